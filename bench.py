@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark of the particle-fluid hot path: one step = one solver substep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload dfsph_1m|pbf]
+
+Default workload: DFSPH, 1,000,000 fluid particles (100^3 lattice, spacing 0.01,
+jitter +-0.05 spacing, seed 2002) in a 3-layer 2 x 1.5 x 1 box of 439,467
+boundary particles, dt = 1 ms, thresholds 0.1 %, seeded synthetic input.
+Metric: million fluid-particle substeps per second (whole job, all ranks).
+
+Under torchrun every rank advances its own replica of the scene (the path
+has no exchange step: replicas only); timing is the max over ranks.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "vt-physics_b200"))
+
+METRIC = "M particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["dfsph_1m", "pbf"], default="dfsph_1m")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--block", type=int, default=0)
+    return ap.parse_args()
+
+
+def make_scene(workload):
+    from vtp import scenes
+    return scenes.dfsph_1m() if workload == "dfsph_1m" else scenes.pbf_dam_break()
+
+
+class Clocks:
+    """nvidia-smi sampler running while the timed region runs (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(scene, seconds: float) -> dict:
+    """FP64 OpenMP oracle on the host cores: bounded sample of the same scene."""
+    from oracle import oracle as O
+    O.lib()
+    cores = O.num_threads()
+    t0 = time.perf_counter()
+    o = O.OracleSolver(scene)
+    init_s = time.perf_counter() - t0
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 1000:
+            break
+    nf = scene.n_fluid
+    return {"value": nf * steps / el / 1e6, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"FP64 OpenMP oracle, first {steps} substeps of the same scene after a {init_s:.1f} s "
+                      f"initialization, {el:.1f} s of CPU time"}
+
+
+def run_reference(args) -> dict:
+    """The reference's own CUDA build (oracle/_ref/libvtref.so) on this GPU, through its Solver API."""
+    import numpy as np
+    from oracle.ref import ref as R
+    out = {"impl": "reference", "metric": METRIC, "unit": METRIC, "higher_is_better": True}
+    if not R.available():
+        out["unavailable"] = "oracle/_ref/libvtref.so was not built (the reference sources were not present)"
+        return out
+    sc = make_scene(args.workload)
+    s = R.RefSolver(sc)
+    s.initialize()
+    if args.warmup:
+        s.tick_timed(args.warmup)
+    clk = Clocks(0)
+    clk.start()
+    ms = s.tick_timed(args.steps)
+    clocks = clk.stop()
+    nf = sc.n_fluid
+    value = nf * args.steps / (ms / 1e3) / 1e6
+    # e2e: host positions / velocities in, positions out, one tick per step.
+    fm = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    pos = s.get("pos", 3)
+    vel = s.get("vel", 3)
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set("pos", pos)
+        s.set("vel", vel)
+        s.tick(1)
+        pos = s.get("pos", 3)
+    el = time.perf_counter() - t0
+    out.update({"value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": args.workload, "fluid": nf, "boundary": sc.n_boundary,
+                                                "impl": "reference CUDA build (sm_100a, -O3) via Solver::tickNsteps"},
+                "clocks": clocks,
+                "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
+                                 "sample": "the reference is GPU code: its own CUDA build timed on this B200"},
+                "e2e": {"value": nf * e2e_steps / el / 1e6, "unit": METRIC,
+                        "h2d_bytes_per_step": int(2 * 12 * s.n), "d2h_bytes_per_step": int(12 * s.n)}})
+    return out
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        # one GPU per process: the library and torch both see only this rank's device
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    import numpy as np
+    import torch
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import vtp
+    vtp.lib()
+    sc = make_scene(args.workload)
+    extra = {}
+    if args.block:
+        extra["blockSize"] = args.block
+    s = vtp.solver_from_scene(sc, extra=extra or None)
+    assert s.initialize(), s.last_error
+    if args.warmup:
+        assert s.tickNsteps(args.warmup), s.last_error
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(local if world > 1 else 0)
+    clk.start()
+    t0 = time.perf_counter()
+    ok = s.tickNsteps(args.steps)
+    wall = time.perf_counter() - t0
+    clocks = clk.stop()
+    assert ok, s.last_error
+    torch.cuda.synchronize()
+    dev_ms = s.stage_times()[2]
+    launches = s.launch_count()
+    st = s.stats()
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    nf = sc.n_fluid
+    value = nf * args.steps * world / (max_ms / 1e3) / 1e6
+
+    # Per-kernel device times over a few extra substeps (CUDA events around each launch).
+    prof = s.profile_kernels(args.profile_steps)
+    cnt, nb = None, None
+    k_mean = 0.0
+    try:
+        cnt_all, _ = s.get_neighbors(int(sc.config[sc.solver]["Required"]["maxNeighborNum"]))
+        fmask = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+        k_mean = float(np.mean(cnt_all[fmask].astype(np.float64) - 1.0))
+    except Exception:
+        pass
+    from vtp.bytes_model import kernel_bytes
+    req = sc.config[sc.solver]["Required"]
+    h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
+    dims = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
+    K = dims[2] * dims[1] * dims[0] + dims[1] * dims[0] + dims[0] + 1
+    N = sc.n_total
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_launches) = dom
+    per_launch_ms = dom_ms / max(dom_launches, 1)
+    b = kernel_bytes(sc.solver, dom_name, N, nf, K, k_mean)
+    peak, peak_kind = peaks()
+    achieved = b["state"] / (per_launch_ms / 1e3) / 1e9
+    kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+
+    # e2e through the public API with host buffers (pinned), H2D of inputs and D2H of the result per step.
+    n_all = s.counts()["total"]
+    pos_h = torch.from_numpy(s.get_field("pos")).pin_memory()
+    vel_h = torch.from_numpy(s.get_field("vel")).pin_memory()
+    out_h = torch.empty((n_all, 3), dtype=torch.float32).pin_memory()
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set_field_ptr("pos", pos_h.data_ptr(), pos_h.numel() * 4)
+        s.set_field_ptr("vel", vel_h.data_ptr(), vel_h.numel() * 4)
+        assert s.tickNsteps(1), s.last_error
+        s.get_field_ptr("pos", out_h.data_ptr(), out_h.numel() * 4)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = nf * e2e_steps * world / float(te.item()) / 1e6
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "fluid": nf, "boundary": sc.n_boundary,
+                   "dt": req["timeStep"], "parallelism": f"replicas{world}",
+                   "div_iters_total": st["total_div_iters"], "incomp_iters_total": st["total_incomp_iters"],
+                   "mean_neighbors": round(k_mean, 2),
+                   "l2": "inputs larger than L2 (state + neighbour lists ~0.5 GB per replica)",
+                   "wall_ms_per_step": 1e3 * wall / args.steps},
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch_state": b["state"], "bytes_per_launch_with_lists": b["total"],
+                     "achieved_with_lists": b["total"] / (per_launch_ms / 1e3) / 1e9,
+                     "ms_per_launch": per_launch_ms},
+        "kernels": kernels,
+        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4),
+                "d2h_bytes_per_step": int(out_h.numel() * 4)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc, args.cpu_seconds)
+    s.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,204 @@
+/*
+ * vtp.h - C ABI of the B200 particle-fluid hot path (uniform-grid neighbour
+ * search + PBF / DFSPH / IMM-CT solver steps).
+ *
+ * The entry points replace the reference's solver plugin interface, the
+ * abstract class `VT_Physics::Solver` (Simulator/Runtime/Include/Framework/
+ * Solver.hpp:27-62) and its factory `SolverManager::createSolver`
+ * (Simulator/Runtime/Source/Manager/SolverManager.cpp:19-40).  Each function
+ * below names the virtual it stands in for.  Plain pointers and sizes only;
+ * configs travel as the reference's JSON text.
+ *
+ * Conventions
+ *  - Every function returns a vtp_status (0 = VTP_OK) except destroy/strings.
+ *  - Host pointers are borrowed for the duration of the call.
+ *  - Per-particle fields are exchanged in ATTACH ORDER (the order in which
+ *    objects were attached, then the object's own particle order), exactly
+ *    as the reference stores them; internally particles are kept sorted by
+ *    grid cell.
+ *  - One handle must not be used from two host threads at once.  Each
+ *    handle owns its own CUDA stream.
+ */
+#ifndef VTP_H
+#define VTP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(VTP_BUILD)
+#define VTP_API __attribute__((visibility("default")))
+#else
+#define VTP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vtp_status {
+    VTP_OK = 0,
+    VTP_ERR_CONFIG = 1,      /* missing / invalid JSON key (reference: checkConfig() false) */
+    VTP_ERR_CUDA = 2,        /* a CUDA call failed (reference: m_isCrashed after cudaGetLastError) */
+    VTP_NOT_CONVERGED = 3,   /* a pressure solve exceeded 100 iterations (reference: "crash") */
+    VTP_ERR_NAN = 4,         /* non-finite state detected */
+    VTP_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    VTP_ERR_BOUNDS = 6,      /* size / index outside a documented limit */
+    VTP_ERR_STATE = 7,       /* call out of order (e.g. tick before attach) */
+    VTP_ERR_ARG = 8,         /* null pointer / wrong byte count */
+    VTP_ERR_NOMEM = 9        /* device allocation failed */
+} vtp_status;
+
+/* Same numbering as the reference's eSolverType (Solver.hpp:17-22). */
+typedef enum vtp_solver_type {
+    VTP_SOLVER_PBF = 0,
+    VTP_SOLVER_DFSPH = 1,
+    VTP_SOLVER_IMM = 2,
+    VTP_SOLVER_IMMCT = 3
+} vtp_solver_type;
+
+/* Per-particle fields for vtp_solver_get_field / vtp_solver_set_field. */
+typedef enum vtp_field {
+    VTP_FIELD_POS = 0,            /* float[3] */
+    VTP_FIELD_VEL = 1,            /* float[3] */
+    VTP_FIELD_COLOR = 2,          /* float[3] */
+    VTP_FIELD_MAT = 3,            /* int32 */
+    VTP_FIELD_MASS = 4,           /* float */
+    VTP_FIELD_VOLUME = 5,         /* float */
+    VTP_FIELD_DENSITY = 6,        /* float: PBF density_sph; DFSPH/IMM compression ratio */
+    VTP_FIELD_LAMBDA = 7,         /* float: PBF lambda */
+    VTP_FIELD_ALPHA = 8,          /* float: DFSPH/IMM df_alpha */
+    VTP_FIELD_KAPPA = 9,          /* float: last pressure-solve kappa */
+    VTP_FIELD_REST_DENSITY = 10,  /* float */
+    VTP_FIELD_VOL_FRAC = 11,      /* float[P] (IMM / IMM-CT) */
+    VTP_FIELD_PHASE_VEL = 12,     /* float[P][3] (IMM / IMM-CT) */
+    VTP_FIELD_CONFORMATION = 13,  /* float[9] row-major Q (IMM-CT) */
+    VTP_FIELD_VEL_GRAD = 14,      /* float[9] row-major (IMM-CT) */
+    VTP_FIELD_STRESS = 15,        /* float[9] row-major viscoelastic stress (IMM-CT) */
+    VTP_FIELD_CD = 16,            /* float: momentum-exchange coefficient (IMM-CT) */
+    VTP_FIELD_DELTA = 17          /* float: last compression-ratio residual field */
+} vtp_field;
+
+/* Statistics of the most recent vtp_solver_tick_n_steps call. */
+typedef struct vtp_stats {
+    uint64_t steps_done;          /* substeps completed since initialize */
+    float sim_time;               /* accumulated like the reference: FP32 += dt */
+    uint32_t last_div_iters;      /* DFSPH/IMM: iterations of the last divergence solve */
+    uint32_t last_incomp_iters;   /* DFSPH/IMM: iterations of the last density solve */
+    uint64_t total_div_iters;     /* summed over the last call */
+    uint64_t total_incomp_iters;
+    double last_div_residual;     /* FP64 mean clamped compression-ratio error */
+    double last_incomp_residual;
+    uint32_t neighbor_overflow;   /* particles whose list hit maxNeighborNum (last substep) */
+    uint32_t dead_particles;      /* fluid particles outside the grid (last substep) */
+    uint32_t phase_retries;       /* IMM-CT phase-transfer retries (last substep) */
+    uint32_t status_bits;         /* device status word, bit (1<<vtp_status) per event */
+} vtp_stats;
+
+typedef struct vtp_solver vtp_solver;
+
+/* Human-readable text for a vtp_status. */
+VTP_API const char *vtp_status_string(int status);
+
+/* Library build id, e.g. "vtp 0.1 sm_100a". */
+VTP_API const char *vtp_version(void);
+
+/* Last error message of this thread (empty string if none). */
+VTP_API const char *vtp_last_error(void);
+
+/* Replaces SolverManager::createSolver(eSolverType) (SolverManager.cpp:19-40);
+ * the solver's CUDA stream is created on the current device. */
+VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
+
+/* Replaces Solver::setConfig(json) (PBFSolver.cpp:30-62, DFSPHSolver.cpp:30-64,
+ * IMMCTSolver.cpp:31-99): `json_text` is the reference's solver config
+ * (e.g. {"DFSPH":{"Required":{...},"Optional":{...}},"EXPORT":{...}}).  An
+ * optional top-level "B200" object carries extensions:
+ *   "forceDivIterations" / "forceIncompIterations": run exactly k solver
+ *       iterations instead of testing the residual (parity runs);
+ *   "deviceLoop": false drives the pressure-solve loops from the host;
+ *   "useGraphs": false launches kernels one by one instead of a CUDA graph;
+ *   "blockSize": threads per block of the neighbour passes (32..256);
+ *   "stageTimers": true records CUDA-event stage times. */
+VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
+
+/* Replaces Solver::attachObject(Object*) (PBFSolver.cpp:169-221 and the
+ * other solvers' attachObject): `pos` is the object's particle positions
+ * (n x float[3], what Object::getObjectComponent()->getElements() returns);
+ * `object_json` holds the two per-object configs the reference reads:
+ *   {"name": "...",
+ *    "ObjectComponentConfig": {"epmMaterial": 0|1, ...},
+ *    "SolverObjectComponentConfig": {"solverType": k, "exportFlag": b,
+ *        "velocityStart": [..], "colorStart": [..], "phaseFraction": [..]}}
+ * `vel` may be NULL (velocityStart is used) or n x float[3] per-particle
+ * initial velocities (an extension used by the differentiable scenes). */
+VTP_API int vtp_solver_attach_object(vtp_solver *s, const float *pos, uint32_t n,
+                             const float *vel, const char *object_json);
+
+/* Replaces Solver::initialize() (PBFSolver.cpp:73-125, DFSPHSolver.cpp:75-137). */
+VTP_API int vtp_solver_initialize(vtp_solver *s);
+
+/* Replaces Solver::tickNsteps(n) (PBFSolver.cpp:148-167).  Runs n substeps
+ * (initializing first if needed) and returns after they finished on the GPU. */
+VTP_API int vtp_solver_tick_n_steps(vtp_solver *s, uint32_t n);
+
+/* Replaces Solver::run() (PBFSolver.cpp:127-146): ticks until the FP32
+ * simulated time reaches animationTime. */
+VTP_API int vtp_solver_run(vtp_solver *s);
+
+/* Replaces Solver::reset() (PBFSolver.cpp:233-236): back to the template config. */
+VTP_API int vtp_solver_reset(vtp_solver *s);
+
+/* Replaces Solver::destroy() (PBFSolver.cpp:238-246); frees the handle. */
+VTP_API void vtp_solver_destroy(vtp_solver *s);
+
+/* Copies the solver's config JSON (after defaults) into buf (NUL-terminated);
+ * stands in for Solver::getSolverConfigTemplate() when called before set_config. */
+VTP_API int vtp_solver_get_config(vtp_solver *s, char *buf, size_t buf_bytes, size_t *needed);
+
+VTP_API int vtp_solver_get_stats(vtp_solver *s, vtp_stats *out);
+VTP_API int vtp_solver_particle_counts(vtp_solver *s, uint32_t *n_total, uint32_t *n_fluid,
+                               uint32_t *n_boundary, uint32_t *n_phases);
+
+/* Field I/O in attach order.  `bytes` must equal n_total * element size. */
+VTP_API int vtp_solver_get_field(vtp_solver *s, int field, void *host, size_t bytes);
+VTP_API int vtp_solver_set_field(vtp_solver *s, int field, const void *host, size_t bytes);
+
+/* Neighbour lists in the reference's layout (UniformGridNeighborSearch.hpp:
+ * 39-51): counts[n_total] (self included, 0 for particles outside the grid)
+ * and nbrs[n_total * max_nbr] original indices, self first, UINT32_MAX padded. */
+VTP_API int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr);
+
+/* Sorted order: sorted_ids[k] = attach-order index at sorted position k and
+ * cell_ids[k] its linear cell id (z*gy*gx + y*gx + x), i.e. the reference's
+ * particleIndices_cuData / cellIndices_cuData after sortByHashValue
+ * (UGNSCudaImpl.cu:128-142). */
+VTP_API int vtp_solver_get_sorted_order(vtp_solver *s, uint32_t *sorted_ids, uint32_t *cell_ids);
+
+/* Device timing of the last tick_n_steps call, in milliseconds, per stage:
+ * [0] neighbour search, [1] solver passes, [2] total.  Zero when timing
+ * is disabled ("B200": {"stageTimers": false}). */
+VTP_API int vtp_solver_get_stage_times(vtp_solver *s, float *ms3);
+
+/* Per-kernel device time of vtp_solver_profile_kernels. */
+typedef struct vtp_kernel_time {
+    char name[32];
+    float total_ms;       /* summed CUDA-event time of all launches */
+    uint32_t launches;
+} vtp_kernel_time;
+
+/* Runs n substeps with direct launches (no graph) and a CUDA event pair
+ * around every kernel on the solver's stream; writes one entry per kernel
+ * name (at most cap) and their number to *count.  The substeps advance the
+ * simulation like tick_n_steps. */
+VTP_API int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_time *out, uint32_t cap,
+                                       uint32_t *count);
+
+/* Number of kernel launches (graph kernel nodes included) issued by the last
+ * tick_n_steps call. */
+VTP_API int vtp_solver_get_launch_count(vtp_solver *s, uint64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VTP_H */

@@ -1,0 +1,189 @@
+"""Python front end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, always as the checker: it is never a fallback for the CUDA path.
+State is kept in attach order in FP64; neighbour search runs in FP32 with the
+reference's arithmetic (UGNSCudaImpl.cu:28-203).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_lib = None
+
+
+class OrGrid(C.Structure):
+    _fields_ = [("lb", C.c_float * 3), ("cell", C.c_float), ("dims", C.c_int32 * 3), ("maxnbr", C.c_uint32)]
+
+
+class OrPbf(C.Structure):
+    _fields_ = [("dt", C.c_double), ("h", C.c_double), ("rho0", C.c_double), ("rho_b", C.c_double),
+                ("xsph_k", C.c_double), ("eps", C.c_double), ("g", C.c_double * 3), ("iterations", C.c_int32)]
+
+
+class OrDfsph(C.Structure):
+    _fields_ = [("dt", C.c_double), ("h", C.c_double), ("rho0", C.c_double), ("rho_b", C.c_double),
+                ("vis", C.c_double), ("div_thr", C.c_double), ("inc_thr", C.c_double), ("gamma", C.c_double),
+                ("g", C.c_double * 3), ("force_div", C.c_int32), ("force_inc", C.c_int32),
+                ("max_iters", C.c_int32)]
+
+
+class OrSolveOut(C.Structure):
+    _fields_ = [("div_iters", C.c_int32), ("inc_iters", C.c_int32), ("div_residual", C.c_double),
+                ("inc_residual", C.c_double), ("crashed", C.c_int32)]
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            from . import build as _b  # type: ignore
+            _b.build()
+        L = C.CDLL(str(path))
+        P = C.c_void_p
+        L.or_neighbors.restype = C.c_uint32
+        L.or_neighbors.argtypes = [C.c_uint32, P, C.POINTER(OrGrid), P, P, P, P]
+        L.or_pbf_init.argtypes = [C.c_uint32, P, P, P, P, C.POINTER(OrGrid), C.POINTER(OrPbf)]
+        L.or_pbf_step.argtypes = [C.c_uint32, P, P, P, P, P, C.POINTER(OrGrid), C.POINTER(OrPbf), P, P]
+        L.or_dfsph_init.argtypes = [C.c_uint32, P, P, P, P, C.POINTER(OrGrid), C.POINTER(OrDfsph)]
+        L.or_dfsph_step.argtypes = [C.c_uint32, P, P, C.c_int32, P, P, P, P, P, C.POINTER(OrGrid),
+                                    C.POINTER(OrDfsph), C.POINTER(OrSolveOut), P, P]
+        L.or_num_threads.restype = C.c_int
+        L.or_set_num_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data if a is not None else None
+
+
+def make_grid(required: dict) -> OrGrid:
+    """Grid of UniformGirdNeighborSearcher::setConfig: cell = h = 4 r, dims = ceil(size / h) in FP32."""
+    r = np.float32(required["particleRadius"])
+    h = np.float32(r * np.float32(4))
+    g = OrGrid()
+    for a in range(3):
+        g.lb[a] = float(np.float32(required["simSpaceLB"][a]))
+        g.dims[a] = int(math.ceil(float(np.float32(np.float32(required["simSpaceSize"][a]) / h))))
+    g.cell = float(h)
+    g.maxnbr = int(required["maxNeighborNum"])
+    return g
+
+
+def neighbors(pos: np.ndarray, grid: OrGrid):
+    """Reference-layout neighbour lists, stable (cell, id) order and cell keys."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    n = pos.shape[0]
+    cnt = np.empty(n, np.uint32)
+    nb = np.empty((n, grid.maxnbr), np.uint32)
+    ids = np.empty(n, np.uint32)
+    keys = np.empty(n, np.uint32)
+    alive = lib().or_neighbors(n, _ptr(pos), C.byref(grid), _ptr(cnt), _ptr(nb), _ptr(ids), _ptr(keys))
+    return cnt, nb, ids[:alive], keys[:alive]
+
+
+def set_threads(n: int):
+    lib().or_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+class OracleSolver:
+    """FP64 state machine for one scene (PBF or DFSPH), attach order."""
+
+    def __init__(self, scene, force_div: int = 0, force_inc: int = 0):
+        self.kind = scene.solver
+        req = scene.config[self.kind]["Required"]
+        opt = scene.config[self.kind]["Optional"]
+        self.grid = make_grid(req)
+        objs = scene.objects
+        self.pos = np.concatenate([o.pos for o in objs]).astype(np.float64)
+        vels = []
+        for o in objs:
+            if o.velocity is not None:
+                vels.append(np.asarray(o.velocity, np.float32))
+            else:
+                vels.append(np.tile(np.asarray(o.velocity_start, np.float32), (o.n, 1)))
+        self.vel = np.concatenate(vels).astype(np.float64)
+        self.mat = np.concatenate([np.full(o.n, o.material, np.int32) for o in objs])
+        self.obj = np.concatenate([np.full(o.n, k, np.int32) for k, o in enumerate(objs)])
+        self.obj_is_fluid = np.array([1 if o.material == 0 else 0 for o in objs], np.int32)
+        self.n = self.pos.shape[0]
+        r = np.float32(req["particleRadius"])
+        h = float(np.float32(r * np.float32(4)))
+        vol0 = float(np.float32(np.float32(2) * r) ** np.float32(3))
+        g = [0.0, -9.8, 0.0]
+        if opt["enable"]:
+            g = [float(np.float32(v)) for v in opt["gravity"]]
+        self.vol = np.full(self.n, vol0, np.float64)
+        self.steps = 0
+        if self.kind == "PBF":
+            p = OrPbf()
+            p.dt = float(np.float32(req["timeStep"]))
+            p.h = h
+            p.rho0 = float(np.float32(req["fPartRestDensity"]))
+            p.rho_b = float(np.float32(req["bPartRestDensity"]))
+            p.xsph_k = float(np.float32(req["XSPH_k"]))
+            p.eps = float(np.float32(1e-6))
+            for a in range(3):
+                p.g[a] = g[a]
+            p.iterations = int(req["iterationNum"])
+            self.p = p
+            self.mass = np.full(self.n, p.rho0 * vol0, np.float64)
+            lib().or_pbf_init(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.mass), _ptr(self.vol),
+                              C.byref(self.grid), C.byref(p))
+            self.density = np.zeros(self.n)
+            self.lam = np.zeros(self.n)
+        elif self.kind == "DFSPH":
+            p = OrDfsph()
+            p.dt = float(np.float32(req["timeStep"]))
+            p.h = h
+            p.rho0 = float(np.float32(req["fPartRestDensity"]))
+            p.rho_b = float(np.float32(req["bPartRestDensity"]))
+            p.vis = float(np.float32(req["fPartRestViscosity"]))
+            p.div_thr = float(np.float32(req["divFreeThreshold"]))
+            p.inc_thr = float(np.float32(req["incompThreshold"]))
+            p.gamma = float(np.float32(req["surfaceTensionCoefficient"]))
+            for a in range(3):
+                p.g[a] = g[a]
+            p.force_div = force_div
+            p.force_inc = force_inc
+            p.max_iters = 101
+            self.p = p
+            self.rest_density = np.where(self.mat == 0, p.rho0, 0.0).astype(np.float64)
+            lib().or_dfsph_init(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), _ptr(self.rest_density),
+                                C.byref(self.grid), C.byref(p))
+            self.ratio = np.zeros(self.n)
+            self.alpha = np.zeros(self.n)
+            self.last = OrSolveOut()
+        else:
+            raise NotImplementedError(self.kind)
+
+    def set_forced_iterations(self, div: int, inc: int):
+        self.p.force_div = int(div)
+        self.p.force_inc = int(inc)
+
+    def step(self, n: int = 1):
+        L = lib()
+        for _ in range(n):
+            if self.kind == "PBF":
+                L.or_pbf_step(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), _ptr(self.mass),
+                              _ptr(self.vol), C.byref(self.grid), C.byref(self.p), _ptr(self.density),
+                              _ptr(self.lam))
+            else:
+                out = OrSolveOut()
+                L.or_dfsph_step(self.n, _ptr(self.mat), _ptr(self.obj), len(self.obj_is_fluid),
+                                _ptr(self.obj_is_fluid), _ptr(self.pos), _ptr(self.vel), _ptr(self.vol),
+                                _ptr(self.rest_density), C.byref(self.grid), C.byref(self.p), C.byref(out),
+                                _ptr(self.ratio), _ptr(self.alpha))
+                self.last = out
+            self.steps += 1

@@ -1,0 +1,526 @@
+/*
+ * CPU oracle (test infrastructure; see vtp_oracle.h).  Restates:
+ *   neighbour search  UGNSCudaImpl.cu:28-203, UniformGridNeighborSearch.cpp:33-60
+ *   SPH kernels       KernelFunctions.cuh:13-70
+ *   PBF               PBFCudaImpl.cu:34-194 in the order of PBFSolver.cpp:326-362
+ *   DFSPH             DFSPHCudaImpl.cu:38-611 in the order of DFSPHSolver.cpp:339-391
+ * Build: gcc -O2 -fopenmp -ffp-contract=off -fPIC -shared (oracle/build.py).
+ */
+#include "vtp_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NBR_NONE 0xffffffffu
+
+/* PI as the reference spells it: const float PI = 3.14159265 (KernelFunctions.cuh:16). */
+static const double kPi = (double)3.14159265f;
+
+int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void or_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* ------------------------------------------------------------------ grid */
+
+static void cell_of(const float *p, const or_grid *g, int *c) {
+    for (int a = 0; a < 3; ++a) {
+        float t = (p[a] - g->lb[a]) / g->cell; /* IEEE single sub + div */
+        c[a] = (int)floorf(t);
+    }
+}
+
+static int cell_available(const int *c, const or_grid *g) {
+    return c[0] >= 0 && c[1] >= 0 && c[2] >= 0 && c[0] <= g->dims[0] && c[1] <= g->dims[1] && c[2] <= g->dims[2];
+}
+
+static uint32_t cell_key(const int *c, const or_grid *g) {
+    return (uint32_t)c[2] * (uint32_t)(g->dims[1] * g->dims[0]) + (uint32_t)c[1] * (uint32_t)g->dims[0] +
+           (uint32_t)c[0];
+}
+
+static float dist2_f32(const float *a, const float *b) {
+    float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}
+
+uint32_t or_neighbors(uint32_t n, const float *pos, const or_grid *g, uint32_t *counts, uint32_t *nbrs,
+                      uint32_t *sorted_ids, uint32_t *keys_out) {
+    const uint64_t nkey = (uint64_t)g->dims[2] * g->dims[1] * g->dims[0] + (uint64_t)g->dims[1] * g->dims[0] +
+                          (uint64_t)g->dims[0] + 1;
+    uint32_t *key = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *start = (uint32_t *)calloc(nkey + 1, sizeof(uint32_t));
+    uint32_t *order = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t alive = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        int c[3];
+        cell_of(pos + 3 * (size_t)i, g, c);
+        if (cell_available(c, g)) {
+            key[i] = cell_key(c, g);
+            start[key[i] + 1]++;
+            ++alive;
+        } else {
+            key[i] = NBR_NONE;
+        }
+    }
+    for (uint64_t k = 0; k < nkey; ++k) start[k + 1] += start[k];
+    {
+        uint32_t *fill = (uint32_t *)malloc(sizeof(uint32_t) * nkey);
+        memcpy(fill, start, sizeof(uint32_t) * nkey);
+        for (uint32_t i = 0; i < n; ++i) /* ascending id: stable */
+            if (key[i] != NBR_NONE) order[fill[key[i]]++] = i;
+        free(fill);
+    }
+    if (sorted_ids)
+        for (uint32_t k = 0; k < alive; ++k) sorted_ids[k] = order[k];
+    if (keys_out)
+        for (uint32_t k = 0; k < alive; ++k) keys_out[k] = key[order[k]];
+    const uint32_t M = g->maxnbr;
+    const float cell = g->cell;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        const uint32_t i = (uint32_t)ii;
+        uint32_t *lst = nbrs + (size_t)i * M;
+        for (uint32_t t = 0; t < M; ++t) lst[t] = NBR_NONE;
+        if (key[i] == NBR_NONE) {
+            counts[i] = 0;
+            continue;
+        }
+        uint32_t cnt = 1;
+        lst[0] = i;
+        int c[3];
+        cell_of(pos + 3 * (size_t)i, g, c);
+        for (int t = 0; t < 27; ++t) {
+            int cc[3] = {c[0] + t / 9 - 1, c[1] + (t / 3) % 3 - 1, c[2] + t % 3 - 1};
+            if (!cell_available(cc, g)) continue;
+            uint32_t k = cell_key(cc, g);
+            for (uint32_t s = start[k]; s < start[k + 1]; ++s) {
+                uint32_t j = order[s];
+                if (j == i) continue;
+                float d2 = dist2_f32(pos + 3 * (size_t)i, pos + 3 * (size_t)j);
+                float r = sqrtf(d2);
+                if (r > 0.f && r <= cell) {
+                    if (cnt < M) lst[cnt++] = j;
+                }
+            }
+        }
+        counts[i] = cnt;
+    }
+    free(key);
+    free(start);
+    free(order);
+    return alive;
+}
+
+/* ------------------------------------------------------------------ kernels (FP64) */
+
+typedef struct {
+    double h, sigma;
+} cubic_t;
+
+static cubic_t cubic_make(double h) {
+    cubic_t k;
+    k.h = h;
+    k.sigma = 8.0 / kPi / (h * h * h);
+    return k;
+}
+
+static double cubic_w(const cubic_t *k, double r) {
+    double q = r / k->h;
+    if (q > 1.0) return 0.0;
+    if (q <= 0.5) return k->sigma * (6.0 * q * q * q - 6.0 * q * q + 1.0);
+    double t = 1.0 - q;
+    return 2.0 * k->sigma * t * t * t;
+}
+
+/* gradient factor g with gradW = g * r_vec */
+static double cubic_g(const cubic_t *k, double r) {
+    double q = r / k->h;
+    if (q < 1e-6 || q > 1.0) return 0.0;
+    double f;
+    if (q <= 0.5) f = 6.0 * (3.0 * q * q - 2.0 * q);
+    else f = -6.0 * (1.0 - q) * (1.0 - q);
+    return f * k->sigma / (r * k->h);
+}
+
+static double tension_c(double r, double h) {
+    double cs = 32.0 / kPi / pow(h, 9.0);
+    if (r * 2 > h && r <= h) return cs * pow(h - r, 3) * pow(r, 3);
+    if (r > 0 && r * 2 <= h) return cs * (2 * pow(h - r, 3) * pow(r, 3) - pow(h, 6) / 64);
+    return 0.0;
+}
+
+static void to_f32(uint32_t n, const double *p, float *f) {
+    for (size_t i = 0; i < 3 * (size_t)n; ++i) f[i] = (float)p[i];
+}
+
+typedef struct {
+    uint32_t *cnt, *nbr;
+} lists_t;
+
+static lists_t build_lists(uint32_t n, const double *pos, const or_grid *g) {
+    lists_t L;
+    float *pf = (float *)malloc(sizeof(float) * 3 * (n ? n : 1));
+    to_f32(n, pos, pf);
+    L.cnt = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    L.nbr = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n ? n : 1) * g->maxnbr);
+    or_neighbors(n, pf, g, L.cnt, L.nbr, NULL, NULL);
+    free(pf);
+    return L;
+}
+
+static void free_lists(lists_t *L) {
+    free(L->cnt);
+    free(L->nbr);
+}
+
+#define FOR_NBR(L, g, i, j)                                                              \
+    for (uint32_t t_ = 0, j = 0; t_ < (L).cnt[i] && ((j = (L).nbr[(size_t)(i) * (g)->maxnbr + t_]), 1); ++t_)
+
+static double rdiff(const double *pos, uint32_t i, uint32_t j, double *r) {
+    r[0] = pos[3 * (size_t)i] - pos[3 * (size_t)j];
+    r[1] = pos[3 * (size_t)i + 1] - pos[3 * (size_t)j + 1];
+    r[2] = pos[3 * (size_t)i + 2] - pos[3 * (size_t)j + 2];
+    return sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+}
+
+/* ------------------------------------------------------------------ PBF */
+
+void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass, double *vol, const or_grid *g,
+                 const or_pbf_params *p) {
+    /* init_cuda + compute_rigid_particle_volume_cuda (PBFCudaImpl.cu:34-68). */
+    lists_t L = build_lists(n, pos, g);
+    cubic_t k = cubic_make(p->h);
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 1) continue;
+        double delta = 0, r[3];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] == mat[i]) delta += cubic_w(&k, rdiff(pos, i, j, r));
+        }
+        vol[i] = 1.0 / delta;
+        mass[i] = p->rho_b * vol[i];
+    }
+    free_lists(&L);
+}
+
+void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *vol,
+                 const or_grid *g, const or_pbf_params *p, double *density_out, double *lambda_out) {
+    const double dt = p->dt;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            vel[3 * (size_t)i + a] += p->g[a] * dt;
+            pos[3 * (size_t)i + a] += vel[3 * (size_t)i + a] * dt;
+        }
+    }
+    lists_t L = build_lists(n, pos, g);
+    cubic_t k = cubic_make(p->h);
+    double *lam = (double *)calloc(n ? n : 1, sizeof(double));
+    double *rho = (double *)calloc(n ? n : 1, sizeof(double));
+    double *dx = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    for (int it = 0; it < p->iterations; ++it) {
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double d = 0, gs[3] = {0, 0, 0}, s2 = 0, r[3];
+            FOR_NBR(L, g, i, j) {
+                double rl = rdiff(pos, i, j, r);
+                d += mass[j] * cubic_w(&k, rl);
+                double gg = cubic_g(&k, rl);
+                for (int a = 0; a < 3; ++a) {
+                    double e = gg * r[a];
+                    gs[a] += e;
+                    s2 += (e / p->rho0) * (e / p->rho0);
+                }
+            }
+            if (d < p->rho0) d = p->rho0;
+            double C = d / p->rho0 - 1.0;
+            for (int a = 0; a < 3; ++a) {
+                gs[a] /= p->rho0;
+                s2 += gs[a] * gs[a];
+            }
+            rho[i] = d;
+            lam[i] = -C / (s2 + p->eps);
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double s[3] = {0, 0, 0}, r[3];
+            FOR_NBR(L, g, i, j) {
+                double gg = cubic_g(&k, rdiff(pos, i, j, r));
+                double lj = mat[j] == 0 ? lam[j] : 0.0; /* boundary lambda never set: 0 */
+                for (int a = 0; a < 3; ++a) s[a] += (lam[i] + lj) * gg * r[a];
+            }
+            for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = s[a] / p->rho0;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            if (mat[i] != 0) continue;
+            for (int a = 0; a < 3; ++a) {
+                pos[3 * (size_t)i + a] += dx[3 * (size_t)i + a];
+                vel[3 * (size_t)i + a] += dx[3 * (size_t)i + a] / dt;
+            }
+        }
+    }
+    /* XSPH_cuda + apply_dx_cuda (PBFCudaImpl.cu:172-194). */
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double dv[3] = {0, 0, 0}, r[3];
+        FOR_NBR(L, g, i, j) {
+            double w = cubic_w(&k, rdiff(pos, i, j, r));
+            for (int a = 0; a < 3; ++a) dv[a] += p->xsph_k * vol[j] * (vel[3 * (size_t)j + a] - vel[3 * (size_t)i + a]) * w;
+        }
+        for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = dv[a] * dt;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            pos[3 * (size_t)i + a] += dx[3 * (size_t)i + a];
+            vel[3 * (size_t)i + a] += dx[3 * (size_t)i + a] / dt;
+        }
+    }
+    if (density_out) memcpy(density_out, rho, sizeof(double) * n);
+    if (lambda_out) memcpy(lambda_out, lam, sizeof(double) * n);
+    free(lam);
+    free(rho);
+    free(dx);
+    free_lists(&L);
+}
+
+/* ------------------------------------------------------------------ DFSPH */
+
+void or_dfsph_init(uint32_t n, const int32_t *mat, const double *pos, double *vol, double *rest_density,
+                   const or_grid *g, const or_dfsph_params *p) {
+    /* compute_rigid_volume_cuda (DFSPHCudaImpl.cu:63-83). */
+    lists_t L = build_lists(n, pos, g);
+    cubic_t k = cubic_make(p->h);
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 1) continue;
+        double delta = 0, r[3];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] == mat[i]) delta += cubic_w(&k, rdiff(pos, i, j, r));
+        }
+        vol[i] = 1.0 / delta;
+        rest_density[i] = vol[i] * p->rho_b;
+    }
+    free_lists(&L);
+}
+
+typedef struct {
+    uint32_t n;
+    const int32_t *mat, *obj, *obj_is_fluid;
+    int32_t nobj;
+    const double *pos, *vol, *mass, *ratio, *alpha;
+    const lists_t *L;
+    const or_grid *g;
+    const cubic_t *k;
+    double dt;
+} dfctx;
+
+static int pressure_solve(const dfctx *c, double *vadv, double *kappa, double thr, int force, int max_iters,
+                          double *residual_out) {
+    const uint32_t n = c->n;
+    const or_grid *g = c->g;
+    double *delta = (double *)calloc(n ? n : 1, sizeof(double));
+    double *osum = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
+    double *ocnt = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) ocnt[c->obj[i]] += 1.0;
+    int iter = 0;
+    double residual = 0;
+    for (;;) {
+        ++iter;
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (c->mat[i] != 0) continue;
+            double d = c->ratio[i] - 1.0, r[3];
+            FOR_NBR(*c->L, g, i, j) {
+                double gg = cubic_g(c->k, rdiff(c->pos, i, j, r));
+                double dot = 0;
+                for (int a = 0; a < 3; ++a) dot += gg * r[a] * (vadv[3 * (size_t)i + a] - vadv[3 * (size_t)j + a]);
+                d += dot * c->vol[j] * c->dt;
+            }
+            if (d < 0) d = 0;
+            delta[i] = d;
+        }
+        for (int o = 0; o < c->nobj; ++o) osum[o] = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (c->obj_is_fluid[c->obj[i]]) osum[c->obj[i]] += delta[i];
+        double acc = 0;
+        int nf = 0;
+        for (int o = 0; o < c->nobj; ++o)
+            if (c->obj_is_fluid[o]) {
+                acc += osum[o] / ocnt[o];
+                ++nf;
+            }
+        residual = nf ? acc / nf : 0.0;
+        for (uint32_t i = 0; i < n; ++i)
+            kappa[i] = c->mat[i] == 0 ? delta[i] / c->alpha[i] / (c->dt * c->dt) / c->vol[i] : 0.0;
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (c->mat[i] != 0) continue;
+            double r[3];
+            FOR_NBR(*c->L, g, i, j) {
+                double gg = cubic_g(c->k, rdiff(c->pos, i, j, r));
+                double s = c->dt * c->vol[i] * c->vol[j] / c->mass[i] * (kappa[i] + kappa[j]) * gg;
+                for (int a = 0; a < 3; ++a) vadv[3 * (size_t)i + a] -= s * r[a];
+            }
+        }
+        if (force > 0) {
+            if (iter >= force) break;
+        } else if (residual < thr || iter > max_iters - 1) {
+            break;
+        }
+    }
+    free(delta);
+    free(osum);
+    free(ocnt);
+    *residual_out = residual;
+    return iter;
+}
+
+void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
+                   double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
+                   const or_dfsph_params *p, or_solve_out *out, double *ratio_out, double *alpha_out) {
+    const double dt = p->dt;
+    lists_t L = build_lists(n, pos, g);
+    cubic_t k = cubic_make(p->h);
+    double *mass = (double *)calloc(n ? n : 1, sizeof(double));
+    double *ratio = (double *)calloc(n ? n : 1, sizeof(double));
+    double *alpha = (double *)calloc(n ? n : 1, sizeof(double));
+    double *vadv = (double *)malloc(sizeof(double) * 3 * (n ? n : 1));
+    double *kappa = (double *)calloc(n ? n : 1, sizeof(double));
+    double *acc = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    double *nrm = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) mass[i] = mat[i] == 0 ? rest_density[i] * vol[i] : 0.0;
+    memcpy(vadv, vel, sizeof(double) * 3 * n);
+    /* compute_compression_ratio_cuda + compute_df_beta_cuda (DFSPHCudaImpl.cu:85-140). */
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double rt = 0, a1[3] = {0, 0, 0}, a2 = 1e-6, r[3];
+        FOR_NBR(L, g, i, j) {
+            double rl = rdiff(pos, i, j, r);
+            rt += vol[j] * cubic_w(&k, rl);
+            double gg = cubic_g(&k, rl);
+            for (int a = 0; a < 3; ++a) a1[a] += vol[j] * gg * r[a];
+            if (mat[j] == 0) a2 += gg * gg * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) * vol[j] * vol[j] / mass[j];
+        }
+        double al = (a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2]) / mass[i] + a2;
+        if (al < 1e-6) al = 1e-6;
+        ratio[i] = rt;
+        alpha[i] = al;
+    }
+    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, &k, dt};
+    out->crashed = 0;
+    out->div_iters = pressure_solve(&c, vadv, kappa, p->div_thr, p->force_div, p->max_iters, &out->div_residual);
+    if (p->force_div <= 0 && out->div_iters > p->max_iters - 1) out->crashed = 1;
+    /* apply_pressure_acc: acc = (v* - v)/dt; v += acc dt; v* = v. */
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            size_t q = 3 * (size_t)i + a;
+            vel[q] += (vadv[q] - vel[q]) / dt * dt;
+            vadv[q] = vel[q];
+        }
+    }
+    /* dfsph_gravity_vis_surface (DFSPHCudaImpl.cu:523-554). */
+    const double h2_001 = 0.001 * p->h * p->h;
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double av[3] = {0, 0, 0}, nn[3] = {0, 0, 0}, r[3];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] != mat[i]) continue;
+            double rl = rdiff(pos, i, j, r);
+            double gg = cubic_g(&k, rl);
+            double vij[3], dot = 0;
+            for (int a = 0; a < 3; ++a) {
+                vij[a] = vel[3 * (size_t)i + a] - vel[3 * (size_t)j + a];
+                dot += vij[a] * r[a];
+            }
+            double pi = p->vis * mass[j] / rest_density[j] * dot / (rl * rl + h2_001);
+            for (int a = 0; a < 3; ++a) {
+                av[a] += 10.0 * pi * gg * r[a];
+                nn[a] += p->h * mass[j] / rest_density[j] * gg * r[a];
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            acc[3 * (size_t)i + a] = p->g[a] + av[a];
+            nrm[3 * (size_t)i + a] = nn[a];
+        }
+    }
+    if (p->gamma != 0.0) {
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double at[3] = {0, 0, 0}, r[3];
+            FOR_NBR(L, g, i, j) {
+                if (mat[j] != mat[i] || j == i) continue;
+                double rl = rdiff(pos, i, j, r);
+                double kk = 2 * rest_density[i] / (rest_density[i] + rest_density[j]);
+                double cc = tension_c(rl, p->h);
+                for (int a = 0; a < 3; ++a) {
+                    double a1 = -p->gamma * mass[i] * mass[j] * cc * r[a] / rl;
+                    double a2 = -p->gamma * mass[i] * (nrm[3 * (size_t)i + a] - nrm[3 * (size_t)j + a]);
+                    at[a] += kk * (a1 + a2);
+                }
+            }
+            for (int a = 0; a < 3; ++a) acc[3 * (size_t)i + a] += at[a];
+        }
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            size_t q = 3 * (size_t)i + a;
+            vel[q] += acc[q] * dt;
+            vadv[q] = vel[q];
+        }
+    }
+    out->inc_iters = pressure_solve(&c, vadv, kappa, p->inc_thr, p->force_inc, p->max_iters, &out->inc_residual);
+    if (p->force_inc <= 0 && out->inc_iters > p->max_iters - 1) out->crashed = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            size_t q = 3 * (size_t)i + a;
+            vel[q] += (vadv[q] - vel[q]) / dt * dt;
+            pos[q] += vel[q] * dt;
+        }
+    }
+    if (ratio_out) memcpy(ratio_out, ratio, sizeof(double) * n);
+    if (alpha_out) memcpy(alpha_out, alpha, sizeof(double) * n);
+    free(mass);
+    free(ratio);
+    free(alpha);
+    free(vadv);
+    free(kappa);
+    free(acc);
+    free(nrm);
+    free_lists(&L);
+}

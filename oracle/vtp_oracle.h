@@ -1,0 +1,79 @@
+/*
+ * CPU oracle (test infrastructure only): an FP64 OpenMP restatement of the
+ * reference's uniform-grid neighbour search and PBF / DFSPH substeps, used
+ * by tests/ to check the sm_100a library and by bench.py as the timed CPU
+ * baseline.  Product code never links or calls it.
+ *
+ * Arrays are in attach order (the reference's original particle order).
+ * Neighbour search runs in FP32 exactly as UGNSCudaImpl.cu:28-203 does
+ * (cell keys with IEEE division, membership sqrtf(d2) <= cell with d2 =
+ * fmaf(dz,dz,fmaf(dy,dy,dx*dx))); the physics runs in FP64.
+ */
+#ifndef VTP_ORACLE_H
+#define VTP_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_grid {
+    float lb[3];
+    float cell;        /* gridCellSize = h */
+    int32_t dims[3];   /* ceil(simSpaceSize / cell) */
+    uint32_t maxnbr;
+} or_grid;
+
+typedef struct or_pbf_params {
+    double dt, h, rho0, rho_b, xsph_k, eps;
+    double g[3];
+    int32_t iterations;
+} or_pbf_params;
+
+typedef struct or_dfsph_params {
+    double dt, h, rho0, rho_b, vis, div_thr, inc_thr, gamma;
+    double g[3];
+    int32_t force_div, force_inc;   /* >0: fixed iteration counts */
+    int32_t max_iters;              /* the reference stops after iteration 101 */
+} or_dfsph_params;
+
+typedef struct or_solve_out {
+    int32_t div_iters, inc_iters;
+    double div_residual, inc_residual;
+    int32_t crashed;
+} or_solve_out;
+
+/* Neighbour lists in the reference layout: counts[n] (self included, 0 when
+ * outside the grid), nbrs[n * maxnbr] attach ids, self first, UINT32_MAX
+ * padded.  sorted_ids/keys (may be NULL) receive the stable (cell, id)
+ * order of the particles inside the grid; returns how many are inside. */
+uint32_t or_neighbors(uint32_t n, const float *pos, const or_grid *g, uint32_t *counts, uint32_t *nbrs,
+                      uint32_t *sorted_ids, uint32_t *keys);
+
+/* PBF: initialize boundary volume / mass (PBFCudaImpl.cu:34-68), then substeps
+ * (PBFSolver.cpp:326-376).  pos/vel are FP64 xyz, mass/vol FP64 per particle,
+ * mat 0 = fluid, 1 = boundary.  density/lambda (may be NULL) receive the last
+ * constraint iteration's values. */
+void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass, double *vol,
+                 const or_grid *g, const or_pbf_params *p);
+void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
+                 const double *vol, const or_grid *g, const or_pbf_params *p, double *density, double *lambda);
+
+/* DFSPH (DFSPHSolver.cpp:339-406): obj[n] gives each particle's object index
+ * and obj_is_fluid/obj_count describe the objects (residual = mean over fluid
+ * objects of the object's mean clamped compression error). */
+void or_dfsph_init(uint32_t n, const int32_t *mat, const double *pos, double *vol, double *rest_density,
+                   const or_grid *g, const or_dfsph_params *p);
+void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
+                   double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
+                   const or_dfsph_params *p, or_solve_out *out, double *ratio, double *alpha);
+
+int or_num_threads(void);
+void or_set_num_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

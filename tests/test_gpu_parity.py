@@ -1,0 +1,175 @@
+"""GPU parity: the sm_100a library (through the C ABI) against the CPU oracle.
+
+Bars (from the project's parity rules):
+  * cell keys, stable (cell, id) order and neighbour lists: bit-exact;
+  * one substep: positions and velocities within 1e-5 relative, where the
+    error of a field is max|a - b| / max(max|b|, floor) and the velocity
+    floor is 1e-3 * spacing / dt (a scene starting at rest has |v| ~ g dt);
+  * multi-step runs: density-error / kinetic-energy trajectories.
+"""
+import numpy as np
+import pytest
+
+from util import fluid_mask, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _spacing(scene):
+    return 2 * scene.config[scene.solver]["Required"]["particleRadius"]
+
+
+def _dt(scene):
+    return scene.config[scene.solver]["Required"]["timeStep"]
+
+
+def _vel_floor(scene):
+    return 1e-3 * _spacing(scene) / _dt(scene)
+
+
+def _check_lists(gpu_cnt, gpu_nb, or_cnt, or_nb):
+    assert np.array_equal(gpu_cnt, or_cnt), f"counts differ at {np.flatnonzero(gpu_cnt != or_cnt)[:10]}"
+    assert np.array_equal(gpu_nb, or_nb), "neighbour lists differ"
+
+
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
+def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind):
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break() if kind == "PBF" else vtp.scenes.dam_break("DFSPH", 30000, seed=7)
+    s = vtp.solver_from_scene(sc)
+    assert s.initialize()
+    pos0 = s.get_field("pos")
+    grid = oracle_lib.make_grid(sc.config[kind]["Required"])
+    maxnbr = grid.maxnbr
+    or_cnt, or_nb, or_ids, or_keys = oracle_lib.neighbors(pos0, grid)
+    cnt, nb = s.get_neighbors(maxnbr)
+    _check_lists(cnt, nb, or_cnt, or_nb)
+    ids, keys = s.get_sorted_order()
+    assert np.array_equal(ids, or_ids)
+    assert np.array_equal(keys, or_keys)
+    # After a substep the lists were built on the substep's start positions.
+    if kind == "DFSPH":
+        assert s.tickNsteps(1)
+        p1 = s.get_field("pos")
+        assert s.tickNsteps(1)
+        or_cnt, or_nb, _, _ = oracle_lib.neighbors(p1, grid)
+        cnt, nb = s.get_neighbors(maxnbr)
+        _check_lists(cnt, nb, or_cnt, or_nb)
+    s.destroy()
+
+
+def test_pbf_one_substep_matches_oracle(vtp_gpu, oracle_lib):
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break()
+    s = vtp.solver_from_scene(sc)
+    o = oracle_lib.OracleSolver(sc)
+    assert s.initialize()
+    mass = s.get_field("mass")
+    vol = s.get_field("volume")
+    assert rel_err(mass, o.mass) < TOL
+    assert rel_err(vol, o.vol) < TOL
+    assert s.tickNsteps(1)
+    o.step(1)
+    fm = fluid_mask(sc)
+    ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+    ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+    ed = rel_err(s.get_field("density")[fm], o.density[fm])
+    el = rel_err(s.get_field("lambda")[fm], o.lam[fm])
+    print(f"PBF one substep rel errors: pos {ep:.2e} vel {ev:.2e} density {ed:.2e} lambda {el:.2e}")
+    assert ep < TOL and ev < TOL and ed < TOL
+    s.destroy()
+
+
+def test_pbf_trajectory_statistics(vtp_gpu, oracle_lib):
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break()
+    s = vtp.solver_from_scene(sc)
+    o = oracle_lib.OracleSolver(sc)
+    fm = fluid_mask(sc)
+    m = o.mass[fm]
+    for k in range(4):
+        assert s.tickNsteps(25)
+        o.step(25)
+        ke_g = 0.5 * np.sum(m * np.sum(s.get_field("vel")[fm].astype(np.float64) ** 2, axis=1))
+        ke_o = 0.5 * np.sum(m * np.sum(o.vel[fm] ** 2, axis=1))
+        com_g = s.get_field("pos")[fm].mean(0)
+        com_o = o.pos[fm].mean(0)
+        print(f"step {25 * (k + 1)}: KE gpu {ke_g:.6e} oracle {ke_o:.6e}; com dy {com_g[1] - com_o[1]:.2e}")
+        assert abs(ke_g - ke_o) <= 1e-3 * max(ke_o, 1e-12)
+        assert np.max(np.abs(com_g - com_o)) < 1e-4
+    s.destroy()
+
+
+@pytest.mark.parametrize("tension", [0.0, 0.001])
+def test_dfsph_one_substep_forced_iterations(vtp_gpu, oracle_lib, tension):
+    vtp = vtp_gpu
+    sc = vtp.scenes.dam_break("DFSPH", 20000, seed=11)
+    sc.config["DFSPH"]["Required"]["surfaceTensionCoefficient"] = tension
+    # Fixed iteration counts make the comparison independent of the stop test.
+    s = vtp.solver_from_scene(sc, extra={"forceDivIterations": 2, "forceIncompIterations": 3})
+    o = oracle_lib.OracleSolver(sc, force_div=2, force_inc=3)
+    assert s.initialize()
+    fm = fluid_mask(sc)
+    assert rel_err(s.get_field("volume"), o.vol) < TOL
+    # a few substeps so the state leaves the lattice rest state
+    for step in range(3):
+        assert s.tickNsteps(1)
+        o.step(1)
+        ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+        ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+        er = rel_err(s.get_field("density")[fm], o.ratio[fm])
+        ea = rel_err(s.get_field("alpha")[fm], o.alpha[fm])
+        print(f"DFSPH step {step + 1} (gamma={tension}): pos {ep:.2e} vel {ev:.2e} ratio {er:.2e} alpha {ea:.2e}")
+        assert ep < TOL and ev < TOL and er < TOL and ea < 1e-4
+    st = s.stats()
+    assert st["last_div_iters"] == 2 and st["last_incomp_iters"] == 3
+    s.destroy()
+
+
+def test_dfsph_converged_solve_matches_oracle(vtp_gpu, oracle_lib):
+    vtp = vtp_gpu
+    sc = vtp.scenes.dam_break("DFSPH", 20000, seed=13)
+    s = vtp.solver_from_scene(sc)
+    o = oracle_lib.OracleSolver(sc)
+    fm = fluid_mask(sc)
+    for step in range(5):
+        assert s.tickNsteps(1)
+        o.step(1)
+        st = s.stats()
+        print(f"step {step + 1}: iters gpu ({st['last_div_iters']},{st['last_incomp_iters']}) "
+              f"oracle ({o.last.div_iters},{o.last.inc_iters}); residual gpu {st['last_incomp_residual']:.3e} "
+              f"oracle {o.last.inc_residual:.3e}")
+        assert abs(st["last_div_iters"] - o.last.div_iters) <= 1
+        assert abs(st["last_incomp_iters"] - o.last.inc_iters) <= 1
+    ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+    assert ev < 1e-3
+    s.destroy()
+
+
+def test_graph_and_direct_launch_agree(vtp_gpu):
+    vtp = vtp_gpu
+    sc = vtp.scenes.dam_break("DFSPH", 8000, seed=17)
+    a = vtp.solver_from_scene(sc)
+    b = vtp.solver_from_scene(sc, extra={"useGraphs": False})
+    c = vtp.solver_from_scene(sc, extra={"deviceLoop": False})
+    for s in (a, b, c):
+        assert s.tickNsteps(4)
+    pa, pb, pc = (s.get_field("pos") for s in (a, b, c))
+    assert np.array_equal(pa, pb) and np.array_equal(pa, pc)
+    assert a.stats()["total_incomp_iters"] == b.stats()["total_incomp_iters"]
+    for s in (a, b, c):
+        s.destroy()
+
+
+def test_runs_are_deterministic(vtp_gpu):
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break()
+    out = []
+    for _ in range(2):
+        s = vtp.solver_from_scene(sc)
+        assert s.tickNsteps(10)
+        out.append(s.get_field("pos"))
+        s.destroy()
+    assert np.array_equal(out[0], out[1])

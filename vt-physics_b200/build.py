@@ -1,0 +1,89 @@
+"""Build the sm_100a shared library ``vtp/libvtp.so`` from ``csrc/`` with nvcc.
+
+Usage: ``python build.py [--jobs N] [--force]``.  Objects go to ``_build/``.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+BUILD = HERE / "_build"
+OUT = HERE / "vtp" / "libvtp.so"
+ROOT = HERE.parent
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def json_include() -> str:
+    """Directory holding nlohmann/json.hpp (header-only JSON library shipped in the image)."""
+    cands = []
+    try:
+        import sysconfig
+        sp = Path(sysconfig.get_paths()["purelib"])
+        cands.append(sp / "include" / "cudnn_frontend" / "thirdparty")
+    except Exception:
+        pass
+    cands += [Path("/usr/include"), Path("/usr/local/include")]
+    for c in cands:
+        if (c / "nlohmann" / "json.hpp").exists():
+            return str(c)
+    raise RuntimeError("nlohmann/json.hpp not found")
+
+
+def flags() -> list[str]:
+    return ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+                   "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", json_include(),
+                   "-DVTP_BUILD"]
+
+
+def compile_one(src: Path, force: bool) -> Path:
+    obj = BUILD / (src.stem + ".o")
+    deps = [src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "vtp.h"]
+    if not force and obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return obj
+    cmd = [nvcc()] + flags() + ["-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    srcs = sorted(CSRC.glob("*.cu"))
+    with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 2)) as ex:
+        objs = list(ex.map(lambda s: compile_one(s, force), srcs))
+    if force or not OUT.exists() or any(o.stat().st_mtime > OUT.stat().st_mtime for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", str(OUT)] + [str(o) for o in objs] + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print(f"built {OUT}")
+    return OUT
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    a = ap.parse_args()
+    try:
+        build(force=a.force, jobs=a.jobs, verbose=True)
+    except RuntimeError as e:
+        print(e, file=sys.stderr)
+        sys.exit(1)

@@ -1,0 +1,1077 @@
+// C ABI (include/vtp.h) and the solver driver: config parsing with the
+// reference's JSON keys, object attachment in attach order, device state in
+// cell-sorted float4 SoA, and one CUDA graph per substep (with conditional
+// WHILE nodes for the DFSPH pressure-solve loops).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <nlohmann/json.hpp>
+
+#include "../../include/vtp.h"
+#include "immct.h"
+#include "solver.h"
+
+using json = nlohmann::json;
+
+namespace vtp {
+thread_local std::string g_last_error;
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+}  // namespace vtp
+
+using vtp::fail;
+using vtp::g_last_error;
+
+namespace {
+
+#define CU(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(VTP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+const std::vector<std::string> kPbfRequired = {"animationTime", "timeStep", "particleRadius", "simSpaceLB",
+                                               "simSpaceSize", "maxNeighborNum", "iterationNum", "XSPH_k",
+                                               "fPartRestDensity", "bPartRestDensity"};
+const std::vector<std::string> kDfsphRequired = {"animationTime", "timeStep", "particleRadius", "simSpaceLB",
+                                                 "simSpaceSize", "maxNeighborNum", "fPartRestDensity",
+                                                 "bPartRestDensity", "fPartRestViscosity", "divFreeThreshold",
+                                                 "incompThreshold", "surfaceTensionCoefficient"};
+const std::vector<std::string> kObjRequired = {"solverType", "exportFlag", "velocityStart", "colorStart"};
+const std::vector<std::string> kOptional = {"enable", "gravity"};
+
+const char *solver_key(int type) {
+    switch (type) {
+        case VTP_SOLVER_PBF: return "PBF";
+        case VTP_SOLVER_DFSPH: return "DFSPH";
+        case VTP_SOLVER_IMM: return "IMM";
+        case VTP_SOLVER_IMMCT: return "IMMCT";
+    }
+    return "?";
+}
+
+json default_config(int type) {
+    json exp = {{"Common", {{"exportTargetDir", "path/to/output"}, {"exportFilePrefix", "obj"},
+                            {"exportFileType", "PLY"}}},
+                {"SolverRequired", {{"enable", false}, {"exportFps", 35}, {"exportGroupPolicy", "MERGE"}}}};
+    json opt = {{"enable", false}, {"gravity", {0, -9.81, 0}}};
+    json req;
+    if (type == VTP_SOLVER_PBF) {
+        req = {{"animationTime", 10}, {"timeStep", 0.01}, {"particleRadius", 0.075},
+               {"simSpaceLB", {-1, -1, -1}}, {"simSpaceSize", {2, 2, 2}}, {"maxNeighborNum", 60},
+               {"iterationNum", 10}, {"XSPH_k", 0.02}, {"fPartRestDensity", 1000}, {"bPartRestDensity", 1000}};
+    } else if (type == VTP_SOLVER_DFSPH) {
+        req = {{"animationTime", 10}, {"timeStep", 0.01}, {"particleRadius", 0.075},
+               {"simSpaceLB", {-1, -1, -1}}, {"simSpaceSize", {2, 2, 2}}, {"maxNeighborNum", 60},
+               {"fPartRestDensity", 1000}, {"bPartRestDensity", 1000}, {"fPartRestViscosity", 0.001},
+               {"divFreeThreshold", 1e-4}, {"incompThreshold", 1e-4}, {"surfaceTensionCoefficient", 0.001}};
+    } else {
+        req = immct_default_required(type == VTP_SOLVER_IMMCT);
+    }
+    return {{solver_key(type), {{"Required", req}, {"Optional", opt}}}, {"EXPORT", exp}};
+}
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// Wraps a launch with profiler events when per-kernel timing is active.
+#define PROF(self, name, call)                        \
+    do {                                              \
+        if ((self)->prof) (self)->prof->begin();      \
+        call;                                         \
+        if ((self)->prof) (self)->prof->end_(name);   \
+    } while (0)
+
+// Largest float d2 whose correctly rounded sqrt is <= h.
+float sqrt_threshold(float h) {
+    float t = h * h;
+    while (std::sqrt(t) > h) t = std::nextafter(t, 0.f);
+    for (;;) {
+        float u = std::nextafter(t, INFINITY);
+        if (std::sqrt(u) <= h) t = u;
+        else break;
+    }
+    return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- config
+
+int vtp_solver::parse_config(const json &c) {
+    const char *key = solver_key(type);
+    if (c.is_null() || c.empty()) return fail(VTP_ERR_CONFIG, std::string(key) + " config json is empty.");
+    if (!c.contains(key)) return fail(VTP_ERR_CONFIG, std::string(key) + " config missing main domain: " + key);
+    const json &sc = c[key];
+    if (!sc.contains("Required"))
+        return fail(VTP_ERR_CONFIG, std::string(key) + " config missing necessary domain: Required");
+    std::vector<std::string> required;
+    if (type == VTP_SOLVER_PBF) required = kPbfRequired;
+    else if (type == VTP_SOLVER_DFSPH) required = kDfsphRequired;
+    else required = immct_required_keys(type == VTP_SOLVER_IMMCT);
+    for (auto &k : required)
+        if (!sc["Required"].contains(k))
+            return fail(VTP_ERR_CONFIG, std::string(key) + " config missing Required key: " + k);
+    if (!sc.contains("Optional")) return fail(VTP_ERR_CONFIG, std::string(key) + " config missing Optional");
+    for (auto &k : kOptional)
+        if (!sc["Optional"].contains(k))
+            return fail(VTP_ERR_CONFIG, std::string(key) + " config missing Optional key: " + k);
+    try {
+        const json &r = sc["Required"];
+        dt = r["timeStep"].get<float>();
+        inv_dt = 1.f / dt;
+        inv_dt2 = inv_dt * inv_dt;
+        radius = r["particleRadius"].get<float>();
+        anim_time = r["animationTime"].get<float>();
+        auto lb = r["simSpaceLB"].get<std::vector<float>>();
+        auto size = r["simSpaceSize"].get<std::vector<float>>();
+        if (lb.size() != 3 || size.size() != 3) return fail(VTP_ERR_CONFIG, "simSpaceLB/simSpaceSize need 3 values");
+        lbx = lb[0]; lby = lb[1]; lbz = lb[2];
+        sx = size[0]; sy = size[1]; sz = size[2];
+        maxnbr = r["maxNeighborNum"].get<uint32_t>();
+        if (maxnbr < 1 || maxnbr > 1024) return fail(VTP_ERR_CONFIG, "maxNeighborNum must be in [1, 1024]");
+        // h = 4 r, rest volume (2r)^3 (PBFSolver.cpp:50-51).
+        h = radius * 4;
+        vol0 = std::pow(2 * radius, 3.f);
+        gravity = make_float3(0.f, -9.8f, 0.f);
+        if (sc["Optional"]["enable"].get<bool>()) {
+            auto g = sc["Optional"]["gravity"].get<std::vector<float>>();
+            if (g.size() != 3) return fail(VTP_ERR_CONFIG, "gravity needs 3 values");
+            gravity = make_float3(g[0], g[1], g[2]);
+        }
+        if (type == VTP_SOLVER_PBF) {
+            rho_f = r["fPartRestDensity"].get<float>();
+            rho_b = r["bPartRestDensity"].get<float>();
+            iterations = r["iterationNum"].get<int>();
+            xsph_k = r["XSPH_k"].get<float>();
+        } else if (type == VTP_SOLVER_DFSPH) {
+            rho_f = r["fPartRestDensity"].get<float>();
+            rho_b = r["bPartRestDensity"].get<float>();
+            viscosity = r["fPartRestViscosity"].get<float>();
+            div_thr = r["divFreeThreshold"].get<float>();
+            incomp_thr = r["incompThreshold"].get<float>();
+            gamma = r["surfaceTensionCoefficient"].get<float>();
+        } else {
+            int rc = immct_parse(type == VTP_SOLVER_IMMCT, r, imm);
+            if (rc) return rc;
+            rho_b = r["bPartRestDensity"].get<float>();
+            div_thr = r["divFreeThreshold"].get<float>();
+            incomp_thr = r["incompThreshold"].get<float>();
+            gamma = r["surfaceTensionCoefficient"].get<float>();
+        }
+        if (c.contains("B200")) {
+            const json &b = c["B200"];
+            force_div = b.value("forceDivIterations", 0u);
+            force_inc = b.value("forceIncompIterations", 0u);
+            device_loop = b.value("deviceLoop", true);
+            use_graphs = b.value("useGraphs", true);
+            stage_timers = b.value("stageTimers", false);
+            stop_on_crash = b.value("stopOnNonConvergence", true);
+            block = b.value("blockSize", 128);
+            if (block < 32 || block > 256 || (block & 31)) return fail(VTP_ERR_CONFIG, "blockSize must be 32..256, multiple of 32");
+        }
+    } catch (const std::exception &e) {
+        return fail(VTP_ERR_CONFIG, std::string("config value error: ") + e.what());
+    }
+    cfg = c;
+    configured = true;
+    return VTP_OK;
+}
+
+int vtp_solver::attach(const float *p, uint32_t n, const float *v, const json &o) {
+    if (initialized) return fail(VTP_ERR_STATE, "attach after initialize");
+    json occ = o.value("ObjectComponentConfig", json::object());
+    json socc = o.value("SolverObjectComponentConfig", json::object());
+    if (!occ.contains("epmMaterial")) return fail(VTP_ERR_CONFIG, "object has no epmMaterial");
+    int mat = occ["epmMaterial"].get<int>();
+    if (mat != 0 && mat != 1) return fail(VTP_ERR_CONFIG, std::string(solver_key(type)) + "Solver unsupported material.");
+    for (auto &k : kObjRequired)
+        if (!socc.contains(k))
+            return fail(VTP_ERR_CONFIG, "Object has no " + std::string(solver_key(type)) + " object component config key: " + k);
+    if (socc["solverType"].get<int>() != type)
+        return fail(VTP_ERR_CONFIG, std::string("Object has no ") + solver_key(type) + " object component config.");
+    if (n > 0 && !p) return fail(VTP_ERR_ARG, "null positions");
+    ObjRec rec;
+    rec.name = o.value("name", std::string("obj_") + std::to_string(objs.size()));
+    rec.mat = mat;
+    rec.start = (uint32_t)(hpos.size() / 3);
+    rec.export_flag = socc["exportFlag"].get<bool>();
+    auto v0 = socc["velocityStart"].get<std::vector<float>>();
+    auto c0 = socc["colorStart"].get<std::vector<float>>();
+    for (int a = 0; a < 3; ++a) {
+        rec.vel0[a] = a < (int)v0.size() ? v0[a] : 0.f;
+        rec.color[a] = a < (int)c0.size() ? c0[a] : 0.f;
+    }
+    if (type == VTP_SOLVER_IMM || type == VTP_SOLVER_IMMCT) {
+        if (!socc.contains("phaseFraction")) return fail(VTP_ERR_CONFIG, "Object has no phaseFraction");
+        rec.phase = socc["phaseFraction"].get<std::vector<float>>();
+    }
+    hpos.insert(hpos.end(), p, p + 3 * (size_t)n);
+    for (uint32_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            hvel.push_back(v ? v[3 * (size_t)i + a] : rec.vel0[a]);
+            hcolor.push_back(rec.color[a]);
+        }
+    hmat.insert(hmat.end(), n, mat);
+    if (!rec.phase.empty())
+        for (uint32_t i = 0; i < n; ++i) hphase.insert(hphase.end(), rec.phase.begin(), rec.phase.end());
+    rec.end = (uint32_t)(hpos.size() / 3);
+    objs.push_back(rec);
+    return VTP_OK;
+}
+
+// ---------------------------------------------------------------- args
+
+vtp::PbfArgs vtp_solver::pbf_args() {
+    vtp::PbfArgs a{};
+    a.nf = L.nf; a.nb = L.nb; a.ell_stride = L.ell_stride; a.k = kc;
+    a.rho0 = rho_f; a.inv_rho0 = 1.f / rho_f; a.rho_b = rho_b; a.eps = 1e-6f; a.dt = dt; a.xsph_k = xsph_k;
+    a.nbr = u.nbr; a.ncnt = u.ncnt;
+    a.pos = pos.c(); a.pos_alt = pos.n(); a.vel = vel.c(); a.vel_alt = vel.n();
+    a.vol = vol; a.density = density; a.lambda = lambda;
+    return a;
+}
+
+vtp::DfsphArgs vtp_solver::dfsph_args() {
+    vtp::DfsphArgs a{};
+    a.nf = L.nf; a.nb = L.nb; a.ell_stride = L.ell_stride; a.k = kc;
+    a.dt = dt; a.inv_dt = inv_dt; a.inv_dt2 = inv_dt2;
+    a.rho0 = rho_f; a.rho_b = rho_b; a.vol_f = vol0;
+    a.mass_f = rho_f * vol0;                               // update_mass_cuda: m = rest_density * V
+    a.vis_coef = (viscosity + viscosity) / 2 * a.mass_f / rho_f;
+    a.h2_001 = 0.001f * (h * h);
+    a.gravity = gravity; a.gamma = gamma;
+    a.csigma = 32.f / 3.14159265f / std::pow(h, 9.f);
+    a.h6_64 = std::pow(h, 6.f) / 64;
+    a.nbr = u.nbr; a.ncnt = u.ncnt;
+    a.pos = pos.c(); a.vel = vel.c(); a.vel_alt = vel.n(); a.vadv = vadv.c(); a.vadv_alt = vadv.n();
+    a.ratio = ratio; a.alpha = alpha; a.kappa = kappa; a.delta = delta;
+    a.acc_tmp = acc_tmp; a.normal = normal;
+    a.orig = orig.c(); a.obj_of = obj_of; a.nobj = nobj_fluid; a.partials = partials; a.status = d_status;
+    return a;
+}
+
+vtp::SolveCtl vtp_solver::solve_ctl(int which, cudaGraphConditionalHandle hnd, int use_cond) {
+    vtp::SolveCtl c{};
+    c.state = solve + which;
+    c.inv_count = inv_count;
+    c.nobj = nobj_fluid;
+    c.nblocks = vtp::dfsph_partial_blocks(L.nf, block);
+    if (c.nblocks == 0) c.nblocks = 1;
+    c.threshold = which == 0 ? div_thr : incomp_thr;
+    c.force_iters = which == 0 ? force_div : force_inc;
+    c.max_iters = 101;
+    c.cond = hnd;
+    c.use_cond = use_cond;
+    return c;
+}
+
+// ---------------------------------------------------------------- initialize
+
+int vtp_solver::sort_boundary_and_lists() {
+    // Boundary rows are static: sort them once, build the cell table once.
+    vtp::Carry none{};
+    vtp::ugns_sort(st, grid, L.nf, L.nb, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, 0.f,
+                   make_float3(0, 0, 0), u, u.bstart);
+    // Copy the sorted boundary rows into both buffers of every double buffer.
+    size_t nb = L.nb;
+    CU(cudaMemcpyAsync(pos.c() + L.nf, pos.n() + L.nf, nb * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(vel.c() + L.nf, vel.n() + L.nf, nb * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(orig.c() + L.nf, orig.n() + L.nf, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    return VTP_OK;
+}
+
+int vtp_solver::initialize() {
+    if (!configured) return fail(VTP_ERR_STATE, "initialize before setConfig");
+    if (initialized) return VTP_OK;
+    const uint32_t n = (uint32_t)(hpos.size() / 3);
+    if (n == 0) return fail(VTP_ERR_STATE, "no particles attached");
+    L.n = n;
+    L.nf = 0;
+    for (auto &o : objs)
+        if (o.mat == 0) L.nf += o.end - o.start;
+    L.nb = n - L.nf;
+    L.ell_stride = maxnbr > 1 ? maxnbr - 1 : 1;
+    // Attach ids of fluid vs boundary decide how a cell's two runs interleave.
+    uint32_t fmin = UINT32_MAX, fmax = 0, bmin = UINT32_MAX, bmax = 0;
+    for (auto &o : objs) {
+        if (o.end == o.start) continue;
+        if (o.mat == 0) fmin = std::min(fmin, o.start), fmax = std::max(fmax, o.end - 1);
+        else bmin = std::min(bmin, o.start), bmax = std::max(bmax, o.end - 1);
+    }
+    if (L.nb == 0 || L.nf == 0 || fmax < bmin) L.merge_mode = 0;
+    else if (bmax < fmin) L.merge_mode = 1;
+    else L.merge_mode = 2;
+
+    // Grid as UniformGirdNeighborSearcher::setConfig (UniformGridNeighborSearch.cpp:214-218).
+    grid.lbx = lbx; grid.lby = lby; grid.lbz = lbz;
+    grid.cell = h;
+    grid.gx = (int)std::ceil(sx / h);
+    grid.gy = (int)std::ceil(sy / h);
+    grid.gz = (int)std::ceil(sz / h);
+    if (grid.gx <= 0 || grid.gy <= 0 || grid.gz <= 0) return fail(VTP_ERR_CONFIG, "empty grid");
+    // Keys reach z*gy*gx + y*gx + x with the inclusive upper bound of cellIsAvailable.
+    uint64_t maxkey = (uint64_t)grid.gz * grid.gy * grid.gx + (uint64_t)grid.gy * grid.gx + grid.gx;
+    if (maxkey + 2 > (1ull << 31)) return fail(VTP_ERR_BOUNDS, "grid too large (more than 2^31 cells)");
+    grid.nkey = (uint32_t)(maxkey + 1);
+    grid.d2max = sqrt_threshold(h);
+    grid.maxnbr = maxnbr;
+    kc.h = h;
+    kc.invh = 1.f / h;
+    kc.sigma = 8.f / 3.14159265f / std::pow(h, 3.f);
+    kc.w0 = kc.sigma;
+
+    if (!st) {
+        CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CU(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        for (auto &e : ev) CU(cudaEventCreate(&e));
+        CU(cudaMallocHost((void **)&h_pinned, 8 * sizeof(uint32_t)));
+    }
+    int rc;
+#define AL(p, cnt) \
+    if ((rc = alloc(p, cnt))) return rc
+    for (int k = 0; k < 2; ++k) {
+        AL(&pos.b[k], n);
+        AL(&vel.b[k], n);
+        AL(&orig.b[k], n);
+    }
+    const uint32_t nrows_max = std::max(L.nf, L.nb);
+    AL(&u.key, nrows_max);
+    AL(&u.rank, nrows_max);
+    AL(&u.count, (size_t)grid.nkey + 1);
+    AL(&u.fstart, (size_t)grid.nkey + 2);
+    AL(&u.bstart, (size_t)grid.nkey + 2);
+    AL(&u.tmp_src, nrows_max);
+    AL(&u.tmp_orig, nrows_max);
+    AL(&u.tmp_key, nrows_max);
+    u.scan_tiles = ((size_t)grid.nkey + 1 + 2047) / 2048;
+    if (u.scan_tiles > 1024 * 64) return fail(VTP_ERR_BOUNDS, "grid too large for the cell scan");
+    AL(&u.scan_sums, u.scan_tiles);
+    const size_t fl_rows = ((size_t)L.nf + 31) / 32 * 32, bl_rows = ((size_t)L.nb + 31) / 32 * 32;
+    AL(&u.nbr, fl_rows * L.ell_stride);
+    AL(&u.ncnt, L.nf);
+    AL(&u.bnbr, bl_rows * L.ell_stride);
+    AL(&u.bncnt, L.nb);
+    AL(&d_status, 4);
+    AL(&d_overflow, 4);
+    CU(cudaMemsetAsync(d_status, 0, 4 * sizeof(uint32_t), st));
+    CU(cudaMemsetAsync(d_overflow, 0, 4 * sizeof(uint32_t), st));
+
+    // Upload in attach order, then split into fluid rows [0, nf) and boundary rows [nf, n).
+    std::vector<float4> p4(n), v4(n);
+    std::vector<uint32_t> ids(n);
+    uint32_t fi = 0, bi = L.nf;
+    const float mass_f = rho_f * vol0;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t row = hmat[i] == 0 ? fi++ : bi++;
+        float w = 0.f;
+        if (type == VTP_SOLVER_PBF) w = mass_f;          // PBF: w = mass (init_cuda, PBFCudaImpl.cu:34-45)
+        else w = vol0;                                    // DFSPH / IMM: w = volume
+        p4[row] = make_float4(hpos[3 * i], hpos[3 * i + 1], hpos[3 * i + 2], w);
+        v4[row] = make_float4(hvel[3 * i], hvel[3 * i + 1], hvel[3 * i + 2], 0.f);
+        ids[row] = i;
+    }
+    CU(cudaMemcpyAsync(pos.c(), p4.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(vel.c(), v4.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(orig.c(), ids.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(pos.n(), p4.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(vel.n(), v4.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(orig.n(), ids.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+
+    if ((rc = sort_boundary_and_lists())) return rc;
+
+    // Solver-specific buffers.
+    if (type == VTP_SOLVER_PBF) {
+        AL(&vol, n);
+        AL(&density, L.nf);
+        AL(&lambda, L.nf);
+        std::vector<float> v(n, vol0);
+        CU(cudaMemcpyAsync(vol, v.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+        CU(cudaMemsetAsync(density, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+        CU(cudaMemsetAsync(lambda, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+    } else {
+        for (int k = 0; k < 2; ++k) AL(&vadv.b[k], n);
+        AL(&ratio, L.nf);
+        AL(&alpha, L.nf);
+        AL(&kappa, L.nf);
+        AL(&delta, L.nf);
+        AL(&rest_b, L.nb);
+        AL(&acc_tmp, L.nf);
+        AL(&normal, L.nf);
+        AL(&solve, 2);
+        CU(cudaMemsetAsync(solve, 0, 2 * sizeof(vtp::SolveState), st));
+        CU(cudaMemsetAsync(kappa, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+        CU(cudaMemsetAsync(ratio, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+        CU(cudaMemsetAsync(alpha, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+        CU(cudaMemsetAsync(delta, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
+        // Fluid objects: residual means are taken per object (vfsph_div, DFSPHCudaImpl.cu:471-483).
+        std::vector<uint16_t> objmap(n, 0);
+        std::vector<double> invc;
+        for (auto &o : objs) {
+            if (o.mat != 0) continue;
+            for (uint32_t i = o.start; i < o.end; ++i) objmap[i] = (uint16_t)invc.size();
+            invc.push_back(o.end > o.start ? 1.0 / (double)(o.end - o.start) : 0.0);
+        }
+        if (invc.empty()) invc.push_back(0.0);
+        nobj_fluid = (int)invc.size();
+        if (nobj_fluid > 65535) return fail(VTP_ERR_BOUNDS, "too many fluid objects");
+        AL(&inv_count, invc.size());
+        AL(&obj_of, n);
+        CU(cudaMemcpyAsync(inv_count, invc.data(), invc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(obj_of, objmap.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+        AL(&partials, (size_t)vtp::dfsph_partial_blocks(std::max<uint32_t>(L.nf, 1), block) * nobj_fluid + 1);
+        if (type != VTP_SOLVER_DFSPH) {
+            if ((rc = immct_alloc(*this))) return rc;
+        }
+    }
+    // Neighbour search of the initial state (initialize(): m_neighborSearcher.update(pos)),
+    // then the boundary volumes from the boundary rows' lists.
+    vtp::Carry carry{};
+    if (type != VTP_SOLVER_PBF) {
+        carry.nf4 = 0;
+    }
+    vtp::ugns_sort(st, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
+                   make_float3(0, 0, 0), u, u.fstart);
+    pos.swap(); vel.swap(); orig.swap();
+    vtp::ugns_build_lists(st, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt, d_status, d_overflow, block);
+    vtp::ugns_build_lists(st, grid, L, L.nf, L.nb, pos.c(), orig.c(), u, u.bnbr, u.bncnt, d_status, d_overflow,
+                          block);
+    if (type == VTP_SOLVER_PBF) {
+        vtp::PbfArgs a = pbf_args();
+        vtp::pbf_init_boundary(st, a, u.bncnt, u.bnbr, L.ell_stride);
+        // boundary volumes live in vol[]; masses in pos.w of both buffers (kernel writes both)
+        CU(cudaMemcpyAsync(pos.n() + L.nf, pos.c() + L.nf, (size_t)L.nb * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    } else {
+        // v* = v (init_cuda), boundary v* = boundary v.
+        for (int k = 0; k < 2; ++k)
+            CU(cudaMemcpyAsync(vadv.b[k], vel.c(), (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        vtp::DfsphArgs a = dfsph_args();
+        vtp::dfsph_rigid_volume(st, a, u.bncnt, u.bnbr, rest_b);
+        CU(cudaMemcpyAsync(pos.n() + L.nf, pos.c() + L.nf, (size_t)L.nb * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        if (type != VTP_SOLVER_DFSPH) {
+            if ((rc = immct_init(*this))) return rc;
+        }
+    }
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st));
+    initialized = true;
+    crashed = false;
+    sim_time = 0.f;
+    steps_done = 0;
+    graphs_ready = false;
+    parity = 0;
+#undef AL
+    return VTP_OK;
+}
+
+// ---------------------------------------------------------------- tick
+
+int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
+    vtp::DfsphArgs a = dfsph_args();
+    vtp::dfsph_solve_begin(s, solve + which);
+    launches_per_tick += 1;
+    if (capture && device_loop) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphConditionalHandle hnd;
+        CU(cudaGraphConditionalHandleCreate(&hnd, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CU(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CU(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+        CU(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        if (type == VTP_SOLVER_DFSPH) {
+            vtp::dfsph_solve_a(side, a, block);
+            vtp::dfsph_solve_b(side, a, block);
+        } else {
+            immct_solve_ab(*this, side, which);
+        }
+        vtp::dfsph_solve_end(side, solve_ctl(which, hnd, 1), partials, d_status);
+        cudaGraph_t out;
+        CU(cudaStreamEndCapture(side, &out));
+        return VTP_OK;  // the body's 3 launches per iteration are added from the iteration totals
+    }
+    // Host-driven loop (reference structure, but only 8 bytes cross PCIe per iteration).
+    for (uint32_t it = 0; it < 101; ++it) {
+        if (type == VTP_SOLVER_DFSPH) {
+            PROF(this, "dfsph_solve_a", vtp::dfsph_solve_a(s, a, block));
+            PROF(this, "dfsph_solve_b", vtp::dfsph_solve_b(s, a, block));
+        } else {
+            immct_solve_ab(*this, s, which);
+        }
+        PROF(this, "dfsph_solve_end",
+             vtp::dfsph_solve_end(s, solve_ctl(which, cudaGraphConditionalHandle{}, 0), partials, d_status));
+        launches_per_tick += 3;
+        CU(cudaMemcpyAsync(h_pinned + 2, &solve[which].stopped, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (h_pinned[2]) break;
+    }
+    return VTP_OK;
+}
+
+int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
+    int rc;
+    if (type == VTP_SOLVER_PBF) {
+        vtp::Carry none{};
+        vtp::ugns_sort(s, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt, gravity, u,
+                       u.fstart, prof);
+        pos.swap(); vel.swap(); orig.swap();
+        PROF(this, "ugns_lists", vtp::ugns_build_lists(s, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
+                                                       d_status, d_overflow, block));
+        launches_per_tick += 8;  // hash, 4 scan kernels, scatter, rank/reorder, lists
+        for (int it = 0; it < iterations; ++it) {
+            vtp::PbfArgs a = pbf_args();
+            PROF(this, "pbf_lambda", vtp::pbf_lambda(s, a, block));
+            PROF(this, "pbf_dx", vtp::pbf_dx(s, a, block));
+            pos.swap();
+            launches_per_tick += 2;
+        }
+        vtp::PbfArgs a = pbf_args();
+        PROF(this, "pbf_xsph", vtp::pbf_xsph(s, a, block));
+        pos.swap(); vel.swap();
+        launches_per_tick += 1;
+        return VTP_OK;
+    }
+    if (type != VTP_SOLVER_DFSPH) return immct_enqueue_tick(*this, s, capture);
+    vtp::Carry carry{};
+    carry.nf4 = 1;
+    carry.src4[0] = vadv.c();
+    carry.dst4[0] = vadv.n();
+    vtp::ugns_sort(s, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
+                   make_float3(0, 0, 0), u, u.fstart, prof);
+    pos.swap(); vel.swap(); orig.swap(); vadv.swap();
+    PROF(this, "ugns_lists", vtp::ugns_build_lists(s, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
+                                                   d_status, d_overflow, block));
+    PROF(this, "dfsph_ratio_alpha", vtp::dfsph_ratio_alpha(s, dfsph_args(), block));
+    launches_per_tick += 9;  // neighbour search (8) + ratio/alpha
+    if ((rc = enqueue_solve(s, 0, capture))) return rc;
+    vtp::DfsphArgs a = dfsph_args();
+    if (gamma == 0.f) {
+        // Tension terms are exactly zero when gamma == 0 (-0 * finite); the normal pass is skipped.
+        PROF(this, "dfsph_viscosity", vtp::dfsph_viscosity(s, a, block));
+        launches_per_tick += 1;
+    } else {
+        PROF(this, "dfsph_vis_normal", vtp::dfsph_vis_normal(s, a, block));
+        PROF(this, "dfsph_tension", vtp::dfsph_tension(s, a, block));
+        launches_per_tick += 2;
+    }
+    vel.swap(); vadv.swap();
+    if ((rc = enqueue_solve(s, 1, capture))) return rc;
+    PROF(this, "dfsph_finalize", vtp::dfsph_finalize(s, dfsph_args()));
+    launches_per_tick += 1;
+    return VTP_OK;
+}
+
+int vtp_solver::build_graphs() {
+    // Capture two substep graphs: the double buffers swap an odd number of
+    // times per substep, so the second graph starts where the first ended.
+    int start_state[4] = {pos.cur, vel.cur, orig.cur, vadv.cur};
+    for (int p = 0; p < 2; ++p) {
+        gstate[p][0] = pos.cur; gstate[p][1] = vel.cur; gstate[p][2] = orig.cur; gstate[p][3] = vadv.cur;
+        launches_per_tick = 0;
+        CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        int rc = enqueue_tick(st, true);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(VTP_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&gexec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(VTP_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    }
+    if (pos.cur != start_state[0] || vel.cur != start_state[1] || orig.cur != start_state[2] ||
+        vadv.cur != start_state[3])
+        return fail(VTP_ERR_STATE, "substep buffer parity does not repeat after two substeps");
+    graphs_ready = true;
+    parity = 0;
+    return VTP_OK;
+}
+
+int vtp_solver::sync_parity() {
+    // Direct launches (profiling, host loops) may leave the double buffers in
+    // either state; pick the graph whose start state matches.
+    for (int p = 0; p < 2; ++p) {
+        if (pos.cur == gstate[p][0] && vel.cur == gstate[p][1] && orig.cur == gstate[p][2] &&
+            vadv.cur == gstate[p][3]) {
+            parity = p;
+            return VTP_OK;
+        }
+    }
+    return fail(VTP_ERR_STATE, "double-buffer state matches neither substep graph");
+}
+
+int vtp_solver::check_status() {
+    CU(cudaMemcpyAsync(h_pinned, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h_pinned + 1, d_overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    stats.status_bits |= h_pinned[0];
+    stats.neighbor_overflow = h_pinned[1];
+    if (h_pinned[0] & vtp::ST_NOT_CONVERGED) {
+        crashed = true;
+        return VTP_NOT_CONVERGED;
+    }
+    if (h_pinned[0] & vtp::ST_NAN) {
+        crashed = true;
+        return VTP_ERR_NAN;
+    }
+    return VTP_OK;
+}
+
+int vtp_solver::tick_n(uint32_t n) {
+    int rc;
+    if (!initialized && (rc = initialize())) return rc;
+    if (crashed) return fail(VTP_NOT_CONVERGED, std::string(solver_key(type)) + "Solver is crashed.");
+    const bool solves = type != VTP_SOLVER_PBF;
+    if (solves) CU(cudaMemsetAsync(solve, 0, 2 * sizeof(vtp::SolveState), st));
+    if (use_graphs && !graphs_ready) {
+        if ((rc = build_graphs())) {
+            // A failed capture leaves the stream usable; fall back to direct launches.
+            cudaGetLastError();
+            use_graphs = false;
+            g_last_error.clear();
+        }
+    }
+    if (use_graphs && (rc = sync_parity())) return rc;
+    CU(cudaMemsetAsync(d_overflow, 0, sizeof(uint32_t), st));
+    CU(cudaEventRecord(ev[0], st));
+    uint64_t launches = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (use_graphs) {
+            CU(cudaGraphLaunch(gexec[parity], st));
+            int np = parity ^ 1;
+            pos.cur = gstate[np][0]; vel.cur = gstate[np][1]; orig.cur = gstate[np][2]; vadv.cur = gstate[np][3];
+            parity = np;
+        } else {
+            launches_per_tick = 0;
+            if ((rc = enqueue_tick(st, false))) return rc;
+            launches += launches_per_tick;
+        }
+        sim_time += dt;
+        ++steps_done;
+        if (solves && stop_on_crash) {
+            // The reference stops ticking after a solve ran past 100 iterations.
+            if ((rc = check_status())) {
+                stats.steps_done = steps_done;
+                return fail(rc, std::string(solver_key(type)) + ": pressure solve exceeded 100 iterations");
+            }
+        }
+    }
+    CU(cudaEventRecord(ev[2], st));
+    CU(cudaStreamSynchronize(st));
+    CU(cudaGetLastError());
+    CU(cudaEventElapsedTime(&stage_ms[2], ev[0], ev[2]));
+    if ((rc = check_status())) return fail(rc, "solver status after tick");
+    if (solves) {
+        vtp::SolveState hs[2];
+        CU(cudaMemcpy(hs, solve, sizeof(hs), cudaMemcpyDeviceToHost));
+        stats.last_div_iters = hs[0].last_iters;
+        stats.last_incomp_iters = hs[1].last_iters;
+        stats.total_div_iters = hs[0].total_iters;
+        stats.total_incomp_iters = hs[1].total_iters;
+        stats.last_div_residual = hs[0].residual;
+        stats.last_incomp_residual = hs[1].residual;
+        if (use_graphs) {
+            // per solve iteration: solve_a, solve_b, solve_end
+            launches = (uint64_t)n * launches_per_tick + 3 * (hs[0].total_iters + hs[1].total_iters);
+        }
+    } else if (use_graphs) {
+        launches = (uint64_t)n * launches_per_tick;
+    }
+    last_launches = launches;
+    stats.steps_done = steps_done;
+    stats.sim_time = sim_time;
+    return VTP_OK;
+}
+
+// ---------------------------------------------------------------- fields
+
+static size_t field_elems(const vtp_solver &s, int f) {
+    switch (f) {
+        case VTP_FIELD_POS: case VTP_FIELD_VEL: case VTP_FIELD_COLOR: return 3;
+        case VTP_FIELD_MAT: case VTP_FIELD_MASS: case VTP_FIELD_VOLUME: case VTP_FIELD_DENSITY:
+        case VTP_FIELD_LAMBDA: case VTP_FIELD_ALPHA: case VTP_FIELD_KAPPA: case VTP_FIELD_REST_DENSITY:
+        case VTP_FIELD_CD: case VTP_FIELD_DELTA: return 1;
+        case VTP_FIELD_VOL_FRAC: return s.imm ? immct_phase_count(s) : 0;
+        case VTP_FIELD_PHASE_VEL: return s.imm ? 3 * immct_phase_count(s) : 0;
+        case VTP_FIELD_CONFORMATION: case VTP_FIELD_VEL_GRAD: case VTP_FIELD_STRESS: return s.imm ? 9 : 0;
+    }
+    return 0;
+}
+
+int vtp_solver::get_field(int f, void *host, size_t bytes) {
+    if (!initialized) return fail(VTP_ERR_STATE, "get_field before initialize");
+    const size_t ne = field_elems(*this, f);
+    if (ne == 0) return fail(VTP_ERR_ARG, "field not available for this solver");
+    if (!host || bytes != (size_t)L.n * ne * 4) return fail(VTP_ERR_ARG, "wrong byte count for field");
+    const uint32_t n = L.n;
+    if (f == VTP_FIELD_COLOR) { memcpy(host, hcolor.data(), bytes); return VTP_OK; }
+    if (f == VTP_FIELD_MAT) { memcpy(host, hmat.data(), bytes); return VTP_OK; }
+    int rc = ensure_stage(bytes);
+    if (rc) return rc;
+    float *tmp = stage;
+    auto fluid_scalar = [&](const float *src, float boundary_value) -> int {
+        // fluid rows from src, boundary rows constant
+        std::vector<float> hv(n, boundary_value);
+        std::vector<uint32_t> ids(n);
+        if (L.nf) {
+            std::vector<float> fv(L.nf);
+            if (cudaMemcpy(fv.data(), src, L.nf * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+            if (cudaMemcpy(ids.data(), orig.c(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+            for (uint32_t r = 0; r < L.nf; ++r) hv[ids[r]] = fv[r];
+        }
+        memcpy(host, hv.data(), bytes);
+        return 0;
+    };
+    switch (f) {
+        case VTP_FIELD_POS: vtp::scatter_f4_to_orig(st, n, pos.c(), orig.c(), tmp); break;
+        case VTP_FIELD_VEL: vtp::scatter_f4_to_orig(st, n, vel.c(), orig.c(), tmp); break;
+        case VTP_FIELD_MASS:
+        case VTP_FIELD_VOLUME:
+        case VTP_FIELD_REST_DENSITY: {
+            std::vector<float4> p4(n);
+            std::vector<uint32_t> ids(n);
+            std::vector<float> vv;
+            CU(cudaMemcpy(p4.data(), pos.c(), n * sizeof(float4), cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(ids.data(), orig.c(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            std::vector<float> rb(L.nb);
+            if (type != VTP_SOLVER_PBF && L.nb) CU(cudaMemcpy(rb.data(), rest_b, L.nb * sizeof(float), cudaMemcpyDeviceToHost));
+            if (type == VTP_SOLVER_PBF) {
+                vv.resize(n);
+                CU(cudaMemcpy(vv.data(), vol, n * sizeof(float), cudaMemcpyDeviceToHost));
+            }
+            std::vector<float> out(n);
+            for (uint32_t r = 0; r < n; ++r) {
+                float v = 0.f;
+                bool fl = r < L.nf;
+                if (type == VTP_SOLVER_PBF) {
+                    if (f == VTP_FIELD_MASS) v = p4[r].w;
+                    else if (f == VTP_FIELD_VOLUME) v = vv[r];
+                    else v = fl ? rho_f : rho_b;
+                } else if (type == VTP_SOLVER_DFSPH) {
+                    if (f == VTP_FIELD_VOLUME) v = p4[r].w;
+                    else if (f == VTP_FIELD_MASS) v = fl ? rho_f * vol0 : 0.f;
+                    else v = fl ? rho_f : rb[r - L.nf];
+                } else {
+                    v = immct_scalar_host(*this, f, r, p4[r].w, fl ? 0.f : rb[r - L.nf]);
+                }
+                out[ids[r]] = v;
+            }
+            memcpy(host, out.data(), bytes);
+            return VTP_OK;
+        }
+        case VTP_FIELD_DENSITY:
+            rc = fluid_scalar(type == VTP_SOLVER_PBF ? density : ratio, 0.f);
+            return rc ? fail(VTP_ERR_CUDA, "field copy failed") : VTP_OK;
+        case VTP_FIELD_LAMBDA:
+            if (type != VTP_SOLVER_PBF) return fail(VTP_ERR_ARG, "lambda is a PBF field");
+            rc = fluid_scalar(lambda, 0.f);
+            return rc ? fail(VTP_ERR_CUDA, "field copy failed") : VTP_OK;
+        case VTP_FIELD_ALPHA:
+        case VTP_FIELD_KAPPA:
+        case VTP_FIELD_DELTA:
+            if (type == VTP_SOLVER_PBF) return fail(VTP_ERR_ARG, "not a PBF field");
+            rc = fluid_scalar(f == VTP_FIELD_ALPHA ? alpha : f == VTP_FIELD_KAPPA ? kappa : delta, 0.f);
+            return rc ? fail(VTP_ERR_CUDA, "field copy failed") : VTP_OK;
+        default:
+            rc = immct_get_field(*this, f, tmp, ne);
+            if (rc) return rc;
+            break;
+    }
+    cudaError_t e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+int vtp_solver::set_field(int f, const void *host, size_t bytes) {
+    if (!initialized) return fail(VTP_ERR_STATE, "set_field before initialize");
+    if (f != VTP_FIELD_POS && f != VTP_FIELD_VEL) return fail(VTP_ERR_ARG, "only pos / vel can be set");
+    if (!host || bytes != (size_t)L.n * 12) return fail(VTP_ERR_ARG, "wrong byte count for field");
+    int rc = ensure_stage(bytes);
+    if (rc) return rc;
+    float *tmp = stage;
+    cudaError_t e = cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        // Only fluid rows move; boundary rows are static and stay as sorted at initialize.
+        DB<float4> &d = f == VTP_FIELD_POS ? pos : vel;
+        vtp::gather_orig_to_f4(st, L.nf, tmp, orig.c(), d.c(), 1);
+        if (f == VTP_FIELD_VEL && vadv.c()) vtp::gather_orig_to_f4(st, L.nf, tmp, orig.c(), vadv.c(), 1);
+        e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+const char *vtp_status_string(int s) {
+    switch (s) {
+        case VTP_OK: return "ok";
+        case VTP_ERR_CONFIG: return "invalid config";
+        case VTP_ERR_CUDA: return "CUDA error";
+        case VTP_NOT_CONVERGED: return "pressure solve did not converge within 100 iterations";
+        case VTP_ERR_NAN: return "non-finite state";
+        case VTP_ERR_TIMEOUT: return "device wait timed out";
+        case VTP_ERR_BOUNDS: return "size or index out of bounds";
+        case VTP_ERR_STATE: return "call out of order";
+        case VTP_ERR_ARG: return "invalid argument";
+        case VTP_ERR_NOMEM: return "out of device memory";
+    }
+    return "unknown status";
+}
+
+const char *vtp_version(void) { return "vtp 0.1 sm_100a"; }
+
+const char *vtp_last_error(void) { return g_last_error.c_str(); }
+
+int vtp_solver_create(int solver_type, vtp_solver **out) {
+    if (!out) return fail(VTP_ERR_ARG, "null out");
+    *out = nullptr;
+    if (solver_type < VTP_SOLVER_PBF || solver_type > VTP_SOLVER_IMMCT)
+        return fail(VTP_ERR_ARG, "unknown solver type");
+    auto *s = new (std::nothrow) vtp_solver();
+    if (!s) return fail(VTP_ERR_NOMEM, "host allocation failed");
+    s->type = solver_type;
+    s->cfg = default_config(solver_type);
+    *out = s;
+    return VTP_OK;
+}
+
+int vtp_solver_set_config(vtp_solver *s, const char *json_text) {
+    if (!s || !json_text) return fail(VTP_ERR_ARG, "null argument");
+    json c;
+    try {
+        c = json::parse(json_text);
+    } catch (const std::exception &e) {
+        return fail(VTP_ERR_CONFIG, std::string("JSON parse error: ") + e.what());
+    }
+    if (s->initialized) return fail(VTP_ERR_STATE, "setConfig after initialize");
+    return s->parse_config(c);
+}
+
+int vtp_solver_attach_object(vtp_solver *s, const float *pos, uint32_t n, const float *vel, const char *object_json) {
+    if (!s || !object_json) return fail(VTP_ERR_ARG, "null argument");
+    json o;
+    try {
+        o = json::parse(object_json);
+    } catch (const std::exception &e) {
+        return fail(VTP_ERR_CONFIG, std::string("JSON parse error: ") + e.what());
+    }
+    try {
+        return s->attach(pos, n, vel, o);
+    } catch (const std::exception &e) {
+        return fail(VTP_ERR_CONFIG, std::string("object config error: ") + e.what());
+    }
+}
+
+int vtp_solver_initialize(vtp_solver *s) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    try {
+        int rc = s->initialize();
+        if (rc) s->release();
+        return rc;
+    } catch (const std::exception &e) {
+        s->release();
+        return fail(VTP_ERR_CONFIG, e.what());
+    }
+}
+
+int vtp_solver_tick_n_steps(vtp_solver *s, uint32_t n) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    return s->tick_n(n);
+}
+
+int vtp_solver_run(vtp_solver *s) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    int rc;
+    if (!s->initialized && (rc = s->initialize())) return rc;
+    // while (cur_simTime < animationTime) tick()   (PBFSolver.cpp:134-143)
+    while (s->sim_time < s->anim_time) {
+        if ((rc = s->tick_n(1))) return rc;
+    }
+    return VTP_OK;
+}
+
+int vtp_solver_reset(vtp_solver *s) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    s->cfg = default_config(s->type);
+    return VTP_OK;
+}
+
+void vtp_solver_destroy(vtp_solver *s) { delete s; }
+
+int vtp_solver_get_config(vtp_solver *s, char *buf, size_t buf_bytes, size_t *needed) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    std::string t = s->cfg.dump();
+    if (needed) *needed = t.size() + 1;
+    if (!buf) return VTP_OK;
+    if (buf_bytes < t.size() + 1) return fail(VTP_ERR_ARG, "buffer too small");
+    memcpy(buf, t.c_str(), t.size() + 1);
+    return VTP_OK;
+}
+
+int vtp_solver_get_stats(vtp_solver *s, vtp_stats *out) {
+    if (!s || !out) return fail(VTP_ERR_ARG, "null argument");
+    *out = s->stats;
+    return VTP_OK;
+}
+
+int vtp_solver_particle_counts(vtp_solver *s, uint32_t *n_total, uint32_t *n_fluid, uint32_t *n_boundary,
+                               uint32_t *n_phases) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    uint32_t n = (uint32_t)(s->hpos.size() / 3), nf = 0;
+    for (auto &o : s->objs)
+        if (o.mat == 0) nf += o.end - o.start;
+    if (n_total) *n_total = n;
+    if (n_fluid) *n_fluid = nf;
+    if (n_boundary) *n_boundary = n - nf;
+    if (n_phases) *n_phases = s->imm ? (uint32_t)immct_phase_count(*s) : 0;
+    return VTP_OK;
+}
+
+int vtp_solver_get_field(vtp_solver *s, int field, void *host, size_t bytes) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    return s->get_field(field, host, bytes);
+}
+
+int vtp_solver_set_field(vtp_solver *s, int field, const void *host, size_t bytes) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    return s->set_field(field, host, bytes);
+}
+
+int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
+    if (!s || !counts || !nbrs) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "get_neighbors before initialize");
+    if (max_nbr != s->maxnbr) return fail(VTP_ERR_ARG, "max_nbr must equal maxNeighborNum");
+    const uint32_t n = s->L.n;
+    // Boundary rows' lists are rebuilt here (the substep only needs fluid rows).
+    vtp::ugns_build_lists(s->st, s->grid, s->L, s->L.nf, s->L.nb, s->pos.c(), s->orig.c(), s->u, s->u.bnbr,
+                          s->u.bncnt, s->d_status, s->d_overflow, s->block);
+    uint32_t *dc = nullptr, *dn = nullptr;
+    CU(cudaMalloc(&dc, (size_t)n * 4));
+    cudaError_t e = cudaMalloc(&dn, (size_t)n * max_nbr * 4);
+    if (e != cudaSuccess) { cudaFree(dc); return fail(VTP_ERR_NOMEM, "neighbour export buffer"); }
+    vtp::export_neighbors(s->st, s->L, 0, s->L.nf, s->u.nbr, s->u.ncnt, s->orig.c(), max_nbr, dc, dn);
+    vtp::export_neighbors(s->st, s->L, s->L.nf, s->L.nb, s->u.bnbr, s->u.bncnt, s->orig.c(), max_nbr, dc, dn);
+    e = cudaMemcpyAsync(counts, dc, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nbrs, dn, (size_t)n * max_nbr * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(dc);
+    cudaFree(dn);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+int vtp_solver_get_sorted_order(vtp_solver *s, uint32_t *sorted_ids, uint32_t *cell_ids) {
+    if (!s || !sorted_ids || !cell_ids) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "get_sorted_order before initialize");
+    const uint32_t n = s->L.n;
+    uint32_t *di = nullptr, *dk = nullptr;
+    CU(cudaMalloc(&di, (size_t)n * 4));
+    cudaError_t e = cudaMalloc(&dk, (size_t)n * 4);
+    if (e != cudaSuccess) { cudaFree(di); return fail(VTP_ERR_NOMEM, "sorted export buffer"); }
+    vtp::export_sorted(s->st, s->grid, n, s->pos.c(), s->orig.c(), di, dk);
+    std::vector<uint32_t> ids(n), keys(n);
+    e = cudaMemcpyAsync(ids.data(), di, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(keys.data(), dk, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(di);
+    cudaFree(dk);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    // Global order of all rows by (cell, attach id): fluid and boundary runs interleave.
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+        return keys[a] != keys[b] ? keys[a] < keys[b] : ids[a] < ids[b];
+    });
+    for (uint32_t k = 0; k < n; ++k) {
+        sorted_ids[k] = ids[idx[k]];
+        cell_ids[k] = keys[idx[k]];
+    }
+    return VTP_OK;
+}
+
+int vtp_solver_get_stage_times(vtp_solver *s, float *ms3) {
+    if (!s || !ms3) return fail(VTP_ERR_ARG, "null argument");
+    for (int k = 0; k < 3; ++k) ms3[k] = s->stage_ms[k];
+    return VTP_OK;
+}
+
+int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_time *out, uint32_t cap, uint32_t *count) {
+    if (!s || !out || !count) return fail(VTP_ERR_ARG, "null argument");
+    int rc = VTP_OK;
+    if (!s->initialized && (rc = s->initialize())) return rc;
+    if (s->crashed) return fail(VTP_NOT_CONVERGED, "solver is crashed");
+    auto P = std::make_unique<vtp::Profiler>();
+    P->st = s->st;
+    for (int k = 0; k < vtp::Profiler::kMax; ++k) {
+        CU(cudaEventCreate(&P->beg[k]));
+        CU(cudaEventCreate(&P->end[k]));
+    }
+    P->ready = true;
+    const bool saved_loop = s->device_loop;
+    s->device_loop = false;
+    s->prof = P.get();
+    if (s->type != VTP_SOLVER_PBF) CU(cudaMemsetAsync(s->solve, 0, 2 * sizeof(vtp::SolveState), s->st));
+    for (uint32_t k = 0; k < n && rc == VTP_OK; ++k) {
+        rc = s->enqueue_tick(s->st, false);
+        s->sim_time += s->dt;
+        ++s->steps_done;
+    }
+    s->prof = nullptr;
+    s->device_loop = saved_loop;
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    std::vector<std::string> names;
+    std::vector<float> tot;
+    std::vector<uint32_t> cnt;
+    for (int k = 0; k < P->n && e == cudaSuccess; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, P->beg[k], P->end[k]);
+        size_t idx = std::find(names.begin(), names.end(), std::string(P->names[k])) - names.begin();
+        if (idx == names.size()) names.push_back(P->names[k]), tot.push_back(0.f), cnt.push_back(0);
+        tot[idx] += ms;
+        cnt[idx] += 1;
+    }
+    for (int k = 0; k < vtp::Profiler::kMax; ++k) cudaEventDestroy(P->beg[k]), cudaEventDestroy(P->end[k]);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    if (rc) return rc;
+    uint32_t m = (uint32_t)std::min<size_t>(cap, names.size());
+    for (uint32_t k = 0; k < m; ++k) {
+        memset(out[k].name, 0, sizeof(out[k].name));
+        strncpy(out[k].name, names[k].c_str(), sizeof(out[k].name) - 1);
+        out[k].total_ms = tot[k];
+        out[k].launches = cnt[k];
+    }
+    *count = m;
+    s->stats.steps_done = s->steps_done;
+    return s->check_status();
+}
+
+int vtp_solver_get_launch_count(vtp_solver *s, uint64_t *launches) {
+    if (!s || !launches) return fail(VTP_ERR_ARG, "null argument");
+    *launches = s->last_launches;
+    return VTP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+// Shared device-side definitions: grid geometry, SPH kernel functions, the
+// warp-interleaved neighbour-list layout and the device status word.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vtp {
+
+// Status bits set on the device (bit = 1 << vtp_status value).
+enum : uint32_t {
+    ST_NOT_CONVERGED = 1u << 3,
+    ST_NAN = 1u << 4,
+    ST_TIMEOUT = 1u << 5,
+    ST_BOUNDS = 1u << 6,
+};
+
+// Uniform grid exactly as UniformGirdNeighborSearcher::setConfig builds it
+// (UniformGridNeighborSearch.cpp:190-228): gridSize = ceil(simSpaceSize / cell),
+// linear cell id = z*gy*gx + y*gx + x (UGNSCudaImpl.cu:58-63).
+struct Grid {
+    float lbx, lby, lbz;
+    float cell;        // gridCellSize (= h)
+    int gx, gy, gz;    // gridSize
+    uint32_t nkey;     // number of key buckets; key nkey is the "outside" bucket
+    float d2max;       // largest float d2 with sqrtf(d2) <= cell (IEEE sqrt)
+    uint32_t maxnbr;   // maxNeighborNum (self included)
+};
+
+// Cell coordinate of a position: floor((p - LB) / cell) per component with
+// IEEE division (UGNSCudaImpl.cu:28-48).
+__device__ __forceinline__ int3 cell_of(float x, float y, float z, const Grid &g) {
+    return make_int3((int)floorf(__fdiv_rn(__fsub_rn(x, g.lbx), g.cell)),
+                     (int)floorf(__fdiv_rn(__fsub_rn(y, g.lby), g.cell)),
+                     (int)floorf(__fdiv_rn(__fsub_rn(z, g.lbz), g.cell)));
+}
+
+// cellIsAvailable (UGNSCudaImpl.cu:73-81): the upper bound is inclusive.
+__device__ __forceinline__ bool cell_available(int3 c, const Grid &g) {
+    return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x <= g.gx && c.y <= g.gy && c.z <= g.gz;
+}
+
+__device__ __forceinline__ uint32_t cell_key(int3 c, const Grid &g) {
+    return (uint32_t)c.z * (uint32_t)(g.gy * g.gx) + (uint32_t)c.y * (uint32_t)g.gx + (uint32_t)c.x;
+}
+
+// Squared distance with a fixed FMA pattern; the neighbour-membership test
+// `0 < |x_i - x_j| <= cell` (UGNSCudaImpl.cu:194) is evaluated as
+// d2 > 0 && d2 <= d2max, which is equivalent for a correctly rounded sqrt.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// The 27 neighbour-cell offsets in the reference's order
+// (UniformGridNeighborSearch.cpp:33-60): x slowest, z fastest.
+__device__ __forceinline__ int3 nbr_offset(int t) {
+    return make_int3(t / 9 - 1, (t / 3) % 3 - 1, t % 3 - 1);
+}
+
+// Warp-interleaved ELL neighbour list: for row r, slot t lives at
+// base + (r/32)*32*stride + t*32 + r%32, so a warp reading slot t of 32
+// consecutive rows touches one 128-byte line.
+__device__ __forceinline__ size_t ell_index(uint32_t row, uint32_t t, uint32_t stride) {
+    return (size_t)(row >> 5) * 32u * stride + (size_t)t * 32u + (row & 31u);
+}
+
+// Cubic spline (sph::cubic_value / cubic_gradient, KernelFunctions.cuh:13-57).
+struct Cubic {
+    float h;       // support radius
+    float invh;    // 1 / h
+    float sigma;   // 8 / pi / h^3 (FP32 as the reference computes it)
+    float w0;      // W(0) = sigma
+};
+
+// W(r) from r^2.
+__device__ __forceinline__ float cubic_w(float d2, const Cubic &k) {
+    float r = sqrtf(d2);
+    float q = r * k.invh;
+    if (q > 1.f) return 0.f;
+    if (q <= 0.5f) {
+        float q2 = q * q;
+        return k.sigma * __fmaf_rn(6.f * q2, q - 1.f, 1.f);
+    }
+    float t = 1.f - q;
+    return (k.sigma * 2.f) * (t * t * t);
+}
+
+// Scalar g with gradW(r_vec) = g * r_vec; zero for q < 1e-6 or q > 1.
+__device__ __forceinline__ float cubic_g(float d2, const Cubic &k) {
+    if (!(d2 > 0.f)) return 0.f;   // coincident particles: q < 1e-6 -> 0
+    float rinv = rsqrtf(d2);
+    float r = d2 * rinv;
+    float q = r * k.invh;
+    if (q < 1e-6f || q > 1.f) return 0.f;
+    float f;
+    if (q <= 0.5f) f = 6.f * q * (3.f * q - 2.f);
+    else {
+        float t = 1.f - q;
+        f = -6.f * t * t;
+    }
+    return f * k.sigma * (rinv * k.invh);
+}
+
+// W and g together (shared sqrt).
+__device__ __forceinline__ void cubic_wg(float d2, const Cubic &k, float &w, float &g) {
+    w = 0.f;
+    g = 0.f;
+    if (!(d2 > 0.f)) {
+        if (d2 == 0.f) w = k.w0;
+        return;
+    }
+    float rinv = rsqrtf(d2);
+    float r = d2 * rinv;
+    float q = r * k.invh;
+    if (q > 1.f) return;
+    if (q <= 0.5f) {
+        float q2 = q * q;
+        w = k.sigma * __fmaf_rn(6.f * q2, q - 1.f, 1.f);
+        if (q >= 1e-6f) g = 6.f * q * (3.f * q - 2.f) * k.sigma * (rinv * k.invh);
+    } else {
+        float t = 1.f - q;
+        w = (k.sigma * 2.f) * (t * t * t);
+        g = -6.f * t * t * k.sigma * (rinv * k.invh);
+    }
+}
+
+// Akinci cohesion spline sph::surface_tension_C (KernelFunctions.cuh:59-70).
+__device__ __forceinline__ float tension_c(float r, float h, float csigma, float h6_64) {
+    if (r * 2.f > h && r <= h) {
+        float a = h - r;
+        return csigma * (a * a * a) * (r * r * r);
+    }
+    if (r > 0.f && r * 2.f <= h) {
+        float a = h - r;
+        return csigma * (2.f * (a * a * a) * (r * r * r) - h6_64);
+    }
+    return 0.f;
+}
+
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+
+}  // namespace vtp

@@ -1,0 +1,345 @@
+// DFSPH solver passes for sm_100a (fluid rows only; rows are cell-sorted).
+//
+// Restates DFSPHSolver::tick (DFSPHSolver.cpp:339-406) with the kernels of
+// DFSPHCudaImpl.cu regrouped into neighbour passes:
+//   ratio_alpha : compute_compression_ratio_cuda + compute_df_beta_cuda (:85-140)
+//   solve_a     : compute_delta_compression_ratio_cuda +
+//                 update_delta_compression_ratio_from_vel_adv_cuda +
+//                 compute_kappa_{div,incomp}_... (:142-196, :355-367) and the
+//                 per-block FP64 partial sums of the residual
+//   solve_b     : vf_update_vel_adv_from_kappa_{div,incomp}_cuda (:198-220, :369-391)
+//   solve_end   : the residual (mean over fluid objects of the object's mean
+//                 clamped compression error, as vfsph_div computes it with
+//                 cal_mean, :449-503) in FP64 on the device, the stop test
+//                 (residual < threshold or iteration > 100) and the loop
+//                 condition of the CUDA-graph WHILE node
+//   viscosity   : apply_pressure_acc (:505-521) evaluated on the fly for i
+//                 and j, then clear_acc + add_acc_gravity +
+//                 add_acc_explicit_lap_vis + acc_2_vel (:222-296, :523-554)
+//   vis_normal / tension : the same with compute_surface_normal_cuda and
+//                 add_acc_surface_tension_cuda (:298-353) when gamma != 0
+//   finalize    : apply_pressure_acc + update_pos_cuda (:393-404)
+#include "dfsph.h"
+
+namespace vtp {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sm[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    double s = 0.0;
+    if (wid == 0) {
+        s = lane < nw ? sm[lane] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+__device__ __forceinline__ float4 pressure_applied(float4 v, float4 va, float inv_dt, float dt) {
+    // add_acc_pressure_cuda + acc_2_vel: acc = (v* - v) / dt; v += acc dt.
+    float4 o = v;
+    o.x = __fmaf_rn((va.x - v.x) * inv_dt, dt, v.x);
+    o.y = __fmaf_rn((va.y - v.y) * inv_dt, dt, v.y);
+    o.z = __fmaf_rn((va.z - v.z) * inv_dt, dt, v.z);
+    return o;
+}
+
+__global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_t *__restrict__ bncnt,
+                                                      const uint32_t *__restrict__ bnbr,
+                                                      float *__restrict__ rest_density_b) {
+    // compute_rigid_volume_cuda (DFSPHCudaImpl.cu:63-83): V_b = 1 / sum_{boundary j} W_ij,
+    // boundary rest_density = V_b * rho_b.
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nb) return;
+    uint32_t i = a.nf + r;
+    float4 p = a.pos[i];
+    uint32_t n = bncnt[r];
+    float delta = n > 0 ? a.k.w0 : 0.f;
+    const uint32_t *lst = bnbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        uint32_t j = lst[(size_t)t * 32u];
+        if (j < a.nf) continue;
+        float4 q = a.pos[j];
+        delta += cubic_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a.k);
+    }
+    float vb = 1.f / delta;
+    p.w = vb;
+    a.pos[i] = p;
+    rest_density_b[r] = vb * a.rho_b;
+}
+
+__global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const uint32_t n = a.ncnt[r];
+    float ratio = n > 0 ? p.w * a.k.w0 : 0.f;   // self term V_i W(0)
+    float a1x = 0.f, a1y = 0.f, a1z = 0.f;
+    float a2 = 1e-6f;
+    const float inv_mf = 1.f / a.mass_f;
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = ldg4(a.pos + j);
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        float w, g;
+        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+        ratio = __fmaf_rn(q.w, w, ratio);
+        const float gx = g * dx, gy = g * dy, gz = g * dz;
+        a1x = __fmaf_rn(q.w, gx, a1x);
+        a1y = __fmaf_rn(q.w, gy, a1y);
+        a1z = __fmaf_rn(q.w, gz, a1z);
+        if (j < a.nf) a2 += (gx * gx + gy * gy + gz * gz) * q.w * q.w * inv_mf;
+    }
+    float alpha = (a1x * a1x + a1y * a1y + a1z * a1z) / a.mass_f + a2;
+    if (alpha < 1e-6f) alpha = 1e-6f;
+    a.ratio[r] = ratio;
+    a.alpha[r] = alpha;
+}
+
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    int obj = 0;
+    if (r < a.nf) {
+        const float4 p = a.pos[r];
+        const float4 vi = a.vadv[r];
+        const uint32_t n = a.ncnt[r];
+        float d = a.ratio[r] - 1.f;
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        for (uint32_t t = 0; t + 1 < n; ++t) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = ldg4(a.pos + j);
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float g = cubic_g(dist2(rx, ry, rz), a.k);
+            const float4 vj = ldg4(a.vadv + j);
+            const float dot = g * (rx * (vi.x - vj.x) + ry * (vi.y - vj.y) + rz * (vi.z - vj.z));
+            d = __fmaf_rn(dot * q.w, a.dt, d);
+        }
+        if (d < 0.f) d = 0.f;
+        a.delta[r] = d;
+        a.kappa[r] = d / a.alpha[r] * a.inv_dt2 / p.w;
+        contrib = (double)d;
+        if (MULTI) obj = a.obj_of[a.orig[r]];
+    }
+    if (!MULTI) {
+        double s = block_sum(contrib);
+        if (threadIdx.x == 0) a.partials[blockIdx.x] = s;
+    } else {
+        for (int o = 0; o < a.nobj; ++o) {
+            double s = block_sum(obj == o ? contrib : 0.0);
+            if (threadIdx.x == 0) a.partials[(size_t)blockIdx.x * a.nobj + o] = s;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    float4 v = a.vadv[r];
+    const float ki = a.kappa[r];
+    const uint32_t n = a.ncnt[r];
+    const float ci = a.dt * p.w / a.mass_f;   // dt V_i / m_i
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = ldg4(a.pos + j);
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+        // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
+        const float kj = j < a.nf ? __ldg(a.kappa + j) : 0.f;
+        const float s = ci * q.w * (ki + kj) * g;
+        v.x = __fmaf_rn(-s, rx, v.x);
+        v.y = __fmaf_rn(-s, ry, v.y);
+        v.z = __fmaf_rn(-s, rz, v.z);
+    }
+    a.vadv[r] = v;
+}
+
+__global__ void k_solve_begin(SolveState *s) {
+    if (threadIdx.x == 0) {
+        s->iter = 0;
+        s->stopped = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__restrict__ partials,
+                                                   uint32_t *status) {
+    double acc = 0.0;
+    for (int o = 0; o < c.nobj; ++o) {
+        double s = 0.0;
+        for (uint32_t b = threadIdx.x; b < c.nblocks; b += blockDim.x) s += partials[(size_t)b * c.nobj + o];
+        s = block_sum(s);
+        if (threadIdx.x == 0) acc += s * c.inv_count[o];
+    }
+    if (threadIdx.x != 0) return;
+    SolveState *st = c.state;
+    const double residual = acc / (double)c.nobj;
+    const uint32_t iter = st->iter + 1;
+    st->iter = iter;
+    st->residual = residual;
+    bool stop;
+    if (c.force_iters > 0) stop = iter >= c.force_iters;
+    else stop = (residual < (double)c.threshold) || iter > c.max_iters - 1;
+    if (!(residual == residual)) {  // NaN residual: stop and flag
+        stop = true;
+        atomicOr(status, ST_NAN);
+    }
+    st->stopped = stop ? 1u : 0u;
+    if (stop) {
+        st->last_iters = iter;
+        st->total_iters += iter;
+        // vfsph_div / vfsph_incomp flag a crash whenever the loop ran past 100 iterations.
+        if (c.force_iters == 0 && iter > c.max_iters - 1) atomicOr(status, ST_NOT_CONVERGED);
+    }
+    if (c.use_cond) cudaGraphSetConditional(c.cond, stop ? 0u : 1u);
+}
+
+template <bool TENSION_SPLIT>
+__global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    const uint32_t n = a.ncnt[r];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    float nx = 0.f, ny = 0.f, nz = 0.f;
+    const float ncoef = a.k.h * a.mass_f / a.rho0;   // h m_j / rho_rest_j (fluid)
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        if (j >= a.nf) continue;   // same-material neighbours only
+        const float4 q = ldg4(a.pos + j);
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float d2 = dist2(rx, ry, rz);
+        const float g = cubic_g(d2, a.k);
+        const float4 vj = pressure_applied(ldg4(a.vel + j), ldg4(a.vadv + j), a.inv_dt, a.dt);
+        const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+        const float pi = a.vis_coef * (vx * rx + vy * ry + vz * rz) / (d2 + a.h2_001);
+        const float s = 10.f * pi * g;
+        ax = __fmaf_rn(s, rx, ax);
+        ay = __fmaf_rn(s, ry, ay);
+        az = __fmaf_rn(s, rz, az);
+        if (TENSION_SPLIT) {
+            const float sn = ncoef * g;
+            nx = __fmaf_rn(sn, rx, nx);
+            ny = __fmaf_rn(sn, ry, ny);
+            nz = __fmaf_rn(sn, rz, nz);
+        }
+    }
+    const float accx = a.gravity.x + ax, accy = a.gravity.y + ay, accz = a.gravity.z + az;
+    if (TENSION_SPLIT) {
+        a.acc_tmp[r] = make_float4(accx, accy, accz, 0.f);
+        a.normal[r] = make_float4(nx, ny, nz, 0.f);
+        return;
+    }
+    float4 o = vi;
+    o.x = __fmaf_rn(accx, a.dt, vi.x);
+    o.y = __fmaf_rn(accy, a.dt, vi.y);
+    o.z = __fmaf_rn(accz, a.dt, vi.z);
+    a.vel_alt[r] = o;
+    a.vadv_alt[r] = o;
+}
+
+__global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    const float4 ni = a.normal[r];
+    const uint32_t n = a.ncnt[r];
+    // Fluid rest densities are equal, so k = 2 rho_i / (rho_i + rho_j) is evaluated once.
+    const float kk = 2.f * a.rho0 / (a.rho0 + a.rho0);
+    const float c1 = -a.gamma * a.mass_f * a.mass_f;
+    const float c2 = -a.gamma * a.mass_f;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        if (j >= a.nf) continue;
+        const float4 q = ldg4(a.pos + j);
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float rl = sqrtf(dist2(rx, ry, rz));
+        const float cs = c1 * tension_c(rl, a.k.h, a.csigma, a.h6_64) / rl;
+        const float4 nj = ldg4(a.normal + j);
+        tx += kk * (cs * rx + c2 * (ni.x - nj.x));
+        ty += kk * (cs * ry + c2 * (ni.y - nj.y));
+        tz += kk * (cs * rz + c2 * (ni.z - nj.z));
+    }
+    const float4 acc = a.acc_tmp[r];
+    float4 o = vi;
+    o.x = __fmaf_rn(acc.x + tx, a.dt, vi.x);
+    o.y = __fmaf_rn(acc.y + ty, a.dt, vi.y);
+    o.z = __fmaf_rn(acc.z + tz, a.dt, vi.z);
+    a.vel_alt[r] = o;
+    a.vadv_alt[r] = o;
+}
+
+__global__ void k_finalize(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 v = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    a.vel[r] = v;
+    a.vadv[r] = v;
+    float4 p = a.pos[r];
+    p.x = __fmaf_rn(v.x, a.dt, p.x);
+    p.y = __fmaf_rn(v.y, a.dt, p.y);
+    p.z = __fmaf_rn(v.z, a.dt, p.z);
+    a.pos[r] = p;
+}
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+uint32_t dfsph_partial_blocks(uint32_t nf, int block) { return nblk(nf, block); }
+
+void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
+                        float *rest_density_b) {
+    if (a.nb) k_rigid_volume<<<nblk(a.nb, 256), 256, 0, st>>>(a, bncnt, bnbr, rest_density_b);
+}
+void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.nf) k_ratio_alpha<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void dfsph_solve_begin(cudaStream_t st, SolveState *s) { k_solve_begin<<<1, 32, 0, st>>>(s); }
+void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
+    unsigned nb = nblk(a.nf, block);
+    if (nb == 0) nb = 1;
+    if (a.nobj > 1) k_solve_a<true><<<nb, block, 0, st>>>(a);
+    else k_solve_a<false><<<nb, block, 0, st>>>(a);
+}
+void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.nf) k_solve_b<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
+    k_solve_end<<<1, 256, 0, st>>>(c, partials, status);
+}
+void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.nf) k_viscosity<false><<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.nf) k_viscosity<true><<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.nf) k_tension<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void dfsph_finalize(cudaStream_t st, const DfsphArgs &a) {
+    if (a.nf) k_finalize<<<nblk(a.nf, 256), 256, 0, st>>>(a);
+}
+
+}  // namespace vtp

@@ -1,0 +1,69 @@
+// DFSPH pass launchers (dfsph.cu).
+#pragma once
+
+#include "internal.h"
+
+namespace vtp {
+
+constexpr int kMaxFluidObjects = 8;
+
+// Device-side state of one pressure solve (divergence or density).
+struct SolveState {
+    uint32_t iter;          // iterations done in the current solve
+    uint32_t stopped;       // 1 once the current solve has stopped
+    uint32_t last_iters;    // iterations of the previous completed solve
+    uint32_t pad_;
+    uint64_t total_iters;   // summed since the counters were cleared
+    double residual;        // last FP64 residual
+};
+
+struct DfsphArgs {
+    uint32_t nf, nb;
+    uint32_t ell_stride;
+    Cubic k;
+    float dt, inv_dt, inv_dt2;
+    float rho0, rho_b, mass_f, vol_f;
+    float vis_coef;         // (nu + nu) / 2 * m_f / rho0
+    float h2_001;           // 0.001 h^2
+    float3 gravity;
+    float gamma;            // surface tension coefficient
+    float csigma, h6_64;    // tension spline constants
+    const uint32_t *nbr, *ncnt;
+    float4 *pos;            // w = volume
+    float4 *vel, *vel_alt;
+    float4 *vadv, *vadv_alt;
+    float *ratio, *alpha, *kappa, *delta;
+    float4 *acc_tmp, *normal;   // tension path only
+    const uint32_t *orig;       // sorted row -> attach id
+    const uint16_t *obj_of;     // attach id -> fluid object slot (multi-object only)
+    int nobj;                   // fluid objects (>= 1)
+    double *partials;           // [blocks][nobj]
+    uint32_t *status;
+};
+
+struct SolveCtl {
+    SolveState *state;
+    const double *inv_count;    // [nobj] 1 / object size
+    int nobj;
+    uint32_t nblocks;           // partial rows
+    float threshold;
+    uint32_t force_iters;       // 0 = residual test
+    uint32_t max_iters;         // reference: stop after iteration 101
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+
+void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
+                        float *rest_density_b);
+void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_solve_begin(cudaStream_t st, SolveState *s);
+void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status);
+void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
+void dfsph_finalize(cudaStream_t st, const DfsphArgs &a);
+uint32_t dfsph_partial_blocks(uint32_t nf, int block);
+
+}  // namespace vtp

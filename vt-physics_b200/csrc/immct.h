@@ -1,0 +1,27 @@
+// IMM / IMM-CT (mixture model + conformation tensor) solver hooks used by the driver.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <nlohmann/json.hpp>
+
+#include "internal.h"
+
+struct vtp_solver;
+
+namespace vtp {
+struct ImmState;
+}
+
+nlohmann::json immct_default_required(bool ct);
+std::vector<std::string> immct_required_keys(bool ct);
+int immct_parse(bool ct, const nlohmann::json &required, std::shared_ptr<vtp::ImmState> &imm);
+int immct_alloc(vtp_solver &s);
+int immct_init(vtp_solver &s);
+int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture);
+void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which);
+int immct_phase_count(const vtp_solver &s);
+float immct_scalar_host(vtp_solver &s, int field, uint32_t row, float w, float boundary_value);
+int immct_get_field(vtp_solver &s, int field, float *dev_out, size_t elems);

@@ -1,0 +1,96 @@
+// Internal host-side interfaces between the solver driver (capi.cu) and the
+// kernel translation units (ugns.cu, pbf.cu, dfsph.cu, immct.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace vtp {
+
+// Particles are kept sorted: fluid rows [0, nf) re-sorted by (cell, attach id)
+// every substep, boundary rows [nf, n) sorted once at initialize.
+struct Layout {
+    uint32_t n = 0, nf = 0, nb = 0;
+    uint32_t ell_stride = 0;   // slots per row in the ELL neighbour list (maxnbr - 1 others)
+    int merge_mode = 0;        // 0: fluid ids < boundary ids, 1: boundary ids < fluid ids, 2: general
+};
+
+// Neighbour-search working set (one per solver).
+struct UgnsBuffers {
+    uint32_t *key = nullptr;       // [nf] cell key per old slot
+    uint32_t *rank = nullptr;      // [nf] arrival rank within the cell (atomic)
+    uint32_t *count = nullptr;     // [nkey + 1]
+    uint32_t *fstart = nullptr;    // [nkey + 2] fluid cell starts (absolute rows)
+    uint32_t *bstart = nullptr;    // [nkey + 2] boundary cell starts (absolute rows)
+    uint32_t *tmp_src = nullptr;   // [max(nf, nb)] scattered: old slot
+    uint32_t *tmp_orig = nullptr;  // [max(nf, nb)] scattered: attach id
+    uint32_t *tmp_key = nullptr;   // [max(nf, nb)] scattered: key
+    uint32_t *scan_sums = nullptr; // [tiles]
+    uint32_t *nbr = nullptr;       // ELL list for fluid rows
+    uint32_t *ncnt = nullptr;      // [nf] neighbour count incl. self (0 = outside the grid)
+    uint32_t *bnbr = nullptr;      // ELL list for boundary rows (init / diagnostics)
+    uint32_t *bncnt = nullptr;     // [nb]
+    size_t scan_tiles = 0;
+};
+
+// Fields a reorder carries from old slot to new slot (float4 / float / uint).
+struct Carry {
+    static constexpr int kMaxF4 = 8, kMaxF1 = 8;
+    int nf4 = 0, nf1 = 0;
+    const float4 *src4[kMaxF4];
+    float4 *dst4[kMaxF4];
+    const float *src1[kMaxF1];
+    float *dst1[kMaxF1];
+};
+
+// Optional per-kernel timing: CUDA events recorded around each launch.
+struct Profiler {
+    static constexpr int kMax = 4096;
+    cudaStream_t st = nullptr;
+    int n = 0;
+    const char *names[kMax];
+    cudaEvent_t beg[kMax], end[kMax];
+    bool ready = false;
+    void begin() {
+        if (!ready || n >= kMax) return;
+        cudaEventRecord(beg[n], st);
+    }
+    void end_(const char *name) {
+        if (!ready || n >= kMax) return;
+        cudaEventRecord(end[n], st);
+        names[n++] = name;
+    }
+};
+
+// --- ugns.cu ---
+// Sort rows [row0, row0 + cnt) by (cell, attach id) into the output arrays;
+// `start` receives the cell-start table (absolute rows).  With `force_dt` > 0
+// the rows' positions get v += g dt; x += v dt applied first (PBF external
+// force fused into the sort).
+void ugns_sort(cudaStream_t st, const Grid &g, uint32_t row0, uint32_t cnt,
+               const float4 *pos_in, float4 *pos_out, const float4 *vel_in, float4 *vel_out,
+               const uint32_t *orig_in, uint32_t *orig_out, const Carry &carry,
+               float force_dt, float3 gravity, UgnsBuffers &u, uint32_t *start, Profiler *prof = nullptr);
+
+// Build the neighbour lists of rows [row0, row0 + cnt) (reference order:
+// 27 offsets, then ascending attach id inside a cell).
+void ugns_build_lists(cudaStream_t st, const Grid &g, const Layout &L, uint32_t row0, uint32_t cnt,
+                      const float4 *pos, const uint32_t *orig, const UgnsBuffers &u,
+                      uint32_t *nbr, uint32_t *ncnt, uint32_t *status, uint32_t *overflow, int block);
+
+// Gather/scatter between attach order and sorted rows.
+void scatter_f4_to_orig(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, float *dst3);
+void scatter_f1_to_orig(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst);
+void gather_orig_to_f4(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, float4 *dst,
+                       int keep_w);
+void gather_orig_to_f1(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst);
+void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base);
+void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
+                      const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
+                      uint32_t *out_nbr);
+void export_sorted(cudaStream_t st, const Grid &g, uint32_t n, const float4 *pos, const uint32_t *orig,
+                   uint32_t *out_ids, uint32_t *out_keys);
+
+}  // namespace vtp

@@ -1,0 +1,145 @@
+// PBF solver passes for sm_100a (fluid rows only; rows are cell-sorted).
+//
+// Restates the reference's PBF substep (PBFSolver::tick, PBFSolver.cpp:326-376)
+// with the kernels of PBFCudaImpl.cu:34-194 regrouped:
+//   lambda pass  = compute_sph_density_and_error_cuda + update_lamb_cuda (:70-122)
+//   dx pass      = compute_dx_cuda + apply_dx_cuda (:124-170), positions
+//                  written to the second buffer so the pass stays Jacobi
+//   xsph pass    = XSPH_cuda + apply_dx_cuda (:172-194, :267-281)
+// apply_ext_force_cuda (:146-157) is fused into the neighbour-search sort.
+#include "pbf.h"
+
+namespace vtp {
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_pbf_init_boundary(PbfArgs a, const uint32_t *__restrict__ bncnt,
+                                                           const uint32_t *__restrict__ bnbr,
+                                                           uint32_t ell_stride) {
+    // compute_rigid_particle_volume_cuda (PBFCudaImpl.cu:47-68): V_b = 1 / sum_{boundary j} W_ij
+    // (self included), m_b = rho_b V_b.  Only boundary neighbours count.
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nb) return;
+    uint32_t i = a.nf + r;
+    float4 p = a.pos[i];
+    uint32_t n = bncnt[r];
+    float delta = n > 0 ? a.k.w0 : 0.f;
+    const uint32_t *lst = bnbr + ell_index(r, 0, ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        uint32_t j = lst[(size_t)t * 32u];
+        if (j < a.nf) continue;
+        float4 q = a.pos[j];
+        delta += cubic_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a.k);
+    }
+    float vb = 1.f / delta;
+    a.vol[i] = vb;
+    float mb = a.rho_b * vb;
+    p.w = mb;
+    a.pos[i] = p;
+    a.pos_alt[i] = p;
+}
+
+__global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const uint32_t n = a.ncnt[r];
+    // Self is the first entry of every list: density gets m_i W(0), gradients 0.
+    float rho = n > 0 ? p.w * a.k.w0 : 0.f;
+    float gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = ldg4(a.pos + j);
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        float w, g;
+        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+        rho = __fmaf_rn(q.w, w, rho);
+        const float ex = g * dx, ey = g * dy, ez = g * dz;
+        gx += ex; gy += ey; gz += ez;
+        const float fx = ex * a.inv_rho0, fy = ey * a.inv_rho0, fz = ez * a.inv_rho0;
+        s2 += fx * fx + fy * fy + fz * fz;
+    }
+    if (rho < a.rho0) rho = a.rho0;
+    const float err = rho / a.rho0 - 1.f;
+    gx /= a.rho0; gy /= a.rho0; gz /= a.rho0;
+    s2 += gx * gx + gy * gy + gz * gz;
+    a.density[r] = rho;
+    a.lambda[r] = -err / (s2 + a.eps);
+}
+
+__global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const float li = a.lambda[r];
+    const uint32_t n = a.ncnt[r];
+    float dx = 0.f, dy = 0.f, dz = 0.f;
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = ldg4(a.pos + j);
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+        // Boundary lambda is never written by the reference; it is taken as 0.
+        const float lj = j < a.nf ? __ldg(a.lambda + j) : 0.f;
+        const float s = (li + lj) * g;
+        dx = __fmaf_rn(s, rx, dx);
+        dy = __fmaf_rn(s, ry, dy);
+        dz = __fmaf_rn(s, rz, dz);
+    }
+    dx /= a.rho0; dy /= a.rho0; dz /= a.rho0;
+    float4 o = p;
+    o.x += dx; o.y += dy; o.z += dz;
+    a.pos_alt[r] = o;
+    float4 v = a.vel[r];
+    v.x += dx / a.dt; v.y += dy / a.dt; v.z += dz / a.dt;
+    a.vel[r] = v;
+}
+
+__global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const float4 vi = a.vel[r];
+    const uint32_t n = a.ncnt[r];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = ldg4(a.pos + j);
+        const float w = cubic_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a.k);
+        const float4 vj = ldg4(a.vel + j);
+        const float c = a.xsph_k * __ldg(a.vol + j);
+        ax = __fmaf_rn(c * (vj.x - vi.x), w, ax);
+        ay = __fmaf_rn(c * (vj.y - vi.y), w, ay);
+        az = __fmaf_rn(c * (vj.z - vi.z), w, az);
+    }
+    const float dx = ax * a.dt, dy = ay * a.dt, dz = az * a.dt;
+    float4 o = p;
+    o.x += dx; o.y += dy; o.z += dz;
+    a.pos_alt[r] = o;
+    float4 v = vi;
+    v.x += dx / a.dt; v.y += dy / a.dt; v.z += dz / a.dt;
+    a.vel_alt[r] = v;
+}
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
+                       uint32_t ell_stride) {
+    if (a.nb) k_pbf_init_boundary<<<nblk(a.nb, 256), 256, 0, st>>>(a, bncnt, bnbr, ell_stride);
+}
+void pbf_lambda(cudaStream_t st, const PbfArgs &a, int block) {
+    if (a.nf) k_pbf_lambda<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void pbf_dx(cudaStream_t st, const PbfArgs &a, int block) {
+    if (a.nf) k_pbf_dx<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+void pbf_xsph(cudaStream_t st, const PbfArgs &a, int block) {
+    if (a.nf) k_pbf_xsph<<<nblk(a.nf, block), block, 0, st>>>(a);
+}
+
+}  // namespace vtp

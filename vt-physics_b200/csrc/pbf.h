@@ -1,0 +1,30 @@
+// PBF pass launchers (pbf.cu).
+#pragma once
+
+#include "internal.h"
+
+namespace vtp {
+
+struct PbfArgs {
+    uint32_t nf, nb;
+    uint32_t ell_stride;
+    Cubic k;
+    float rho0, inv_rho0, rho_b, eps, dt, xsph_k;
+    const uint32_t *nbr;   // fluid-row ELL list
+    const uint32_t *ncnt;  // fluid-row counts (self included)
+    float4 *pos;           // current positions, w = mass
+    float4 *pos_alt;       // output positions (second buffer)
+    float4 *vel;           // current velocities
+    float4 *vel_alt;       // output velocities (XSPH pass)
+    float *vol;            // [n] volume (fluid V0, boundary 1/sum W)
+    float *density;        // [nf]
+    float *lambda;         // [nf]
+};
+
+void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
+                       uint32_t ell_stride);
+void pbf_lambda(cudaStream_t st, const PbfArgs &a, int block);
+void pbf_dx(cudaStream_t st, const PbfArgs &a, int block);
+void pbf_xsph(cudaStream_t st, const PbfArgs &a, int block);
+
+}  // namespace vtp

@@ -1,0 +1,155 @@
+// The solver object behind the C ABI handle (shared by capi.cu and immct.cu).
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <nlohmann/json.hpp>
+
+#include "../../include/vtp.h"
+#include "dfsph.h"
+#include "internal.h"
+#include "pbf.h"
+
+namespace vtp {
+struct ImmState;
+int fail(int code, const std::string &msg);
+extern thread_local std::string g_last_error;
+}  // namespace vtp
+
+template <class T>
+struct DB {
+    T *b[2] = {nullptr, nullptr};
+    int cur = 0;
+    T *c() const { return b[cur]; }
+    T *n() const { return b[cur ^ 1]; }
+    void swap() { cur ^= 1; }
+};
+
+struct ObjRec {
+    std::string name;
+    int mat = 0;
+    uint32_t start = 0, end = 0;
+    bool export_flag = false;
+    float vel0[3] = {0, 0, 0};
+    float color[3] = {0, 0, 0};
+    std::vector<float> phase;
+};
+
+struct vtp_solver {
+    int type = 0;
+    nlohmann::json cfg;
+    bool configured = false;
+    bool initialized = false;
+    bool crashed = false;
+
+    // attach-order host data
+    std::vector<ObjRec> objs;
+    std::vector<float> hpos, hvel, hcolor, hphase;
+    std::vector<int> hmat;
+
+    // parsed parameters (same derivations as the reference's setConfig)
+    float dt = 0, inv_dt = 0, inv_dt2 = 0, radius = 0, h = 0, rho_f = 0, rho_b = 0, vol0 = 0;
+    float xsph_k = 0, viscosity = 0, div_thr = 0, incomp_thr = 0, gamma = 0, anim_time = 0;
+    float lbx = 0, lby = 0, lbz = 0, sx = 0, sy = 0, sz = 0;
+    float3 gravity = make_float3(0.f, -9.8f, 0.f);
+    uint32_t maxnbr = 60;
+    int iterations = 1;
+    float sim_time = 0.f;
+
+    // extensions ("B200" block)
+    uint32_t force_div = 0, force_inc = 0;
+    bool device_loop = true, use_graphs = true, stage_timers = false, stop_on_crash = true;
+    int block = 128;
+
+    // device state
+    cudaStream_t st = nullptr, side = nullptr;
+    vtp::Grid grid{};
+    vtp::Layout L{};
+    vtp::Cubic kc{};
+    DB<float4> pos, vel, vadv;
+    DB<uint32_t> orig;
+    float *vol = nullptr, *density = nullptr, *lambda = nullptr;
+    float *ratio = nullptr, *alpha = nullptr, *kappa = nullptr, *delta = nullptr, *rest_b = nullptr;
+    float4 *acc_tmp = nullptr, *normal = nullptr;
+    double *partials = nullptr, *inv_count = nullptr;
+    uint16_t *obj_of = nullptr;
+    vtp::SolveState *solve = nullptr;   // [2]: divergence, density
+    vtp::UgnsBuffers u{};
+    uint32_t *d_status = nullptr, *d_overflow = nullptr;
+    uint32_t *h_pinned = nullptr;       // [4] status, overflow, iter, spare
+    int nobj_fluid = 1;
+    std::shared_ptr<vtp::ImmState> imm;
+
+    // graphs: two parities (double-buffer swaps alternate between substeps)
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int gstate[2][4] = {{0}};
+    int parity = 0;
+    bool graphs_ready = false;
+    uint64_t launches_per_tick = 0, last_launches = 0;
+
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    vtp::Profiler *prof = nullptr;      // set only while vtp_solver_profile_kernels runs
+    float *stage = nullptr;             // device staging buffer for field I/O
+    size_t stage_bytes = 0;
+    float stage_ms[3] = {0, 0, 0};
+
+    uint64_t steps_done = 0;
+    vtp_stats stats{};
+
+    std::vector<void *> allocs;
+
+    ~vtp_solver() { release(); }
+
+    int ensure_stage(size_t bytes) {
+        if (bytes <= stage_bytes) return 0;
+        if (stage) cudaFree(stage), stage = nullptr, stage_bytes = 0;
+        if (cudaMalloc((void **)&stage, bytes) != cudaSuccess) return vtp::fail(VTP_ERR_NOMEM, "staging buffer");
+        stage_bytes = bytes;
+        return 0;
+    }
+
+    void release() {
+        for (int p = 0; p < 2; ++p)
+            if (gexec[p]) cudaGraphExecDestroy(gexec[p]), gexec[p] = nullptr;
+        for (void *a : allocs) cudaFree(a);
+        allocs.clear();
+        if (stage) cudaFree(stage), stage = nullptr, stage_bytes = 0;
+        if (h_pinned) cudaFreeHost(h_pinned), h_pinned = nullptr;
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e), e = nullptr;
+        if (st) cudaStreamDestroy(st), st = nullptr;
+        if (side) cudaStreamDestroy(side), side = nullptr;
+        imm.reset();
+        graphs_ready = false;
+        initialized = false;
+    }
+
+    template <class T>
+    int alloc(T **p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e != cudaSuccess) return vtp::fail(VTP_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(*p);
+        return VTP_OK;
+    }
+
+    int parse_config(const nlohmann::json &c);
+    int attach(const float *p, uint32_t n, const float *v, const nlohmann::json &o);
+    int initialize();
+    int tick_n(uint32_t n);
+    int enqueue_tick(cudaStream_t s, bool capture);
+    int enqueue_solve(cudaStream_t s, int which, bool capture);
+    int build_graphs();
+    int sort_boundary_and_lists();
+    int get_field(int f, void *host, size_t bytes);
+    int set_field(int f, const void *host, size_t bytes);
+    vtp::PbfArgs pbf_args();
+    vtp::DfsphArgs dfsph_args();
+    vtp::SolveCtl solve_ctl(int which, cudaGraphConditionalHandle h, int use_cond);
+    int check_status();
+    int sync_parity();
+};
+

@@ -1,0 +1,432 @@
+// Uniform-grid neighbour search for sm_100a.
+//
+// Replaces UniformGirdNeighborSearcher::update / cu_update
+// (Simulator/Runtime/Source/Modules/NeighborSearch/UGNS/UGNSCudaImpl.cu:96-227).
+// Instead of two thrust::sort_by_key calls, a 27-cell neighbour walk over
+// particles in attach order and a padded N x maxNbr list, each substep does:
+//   hash    : cell key per row + arrival rank inside the cell (atomicAdd)
+//   scan    : exclusive scan of the per-cell counts -> cell start table
+//   scatter : rows placed into their cell's segment (arrival order)
+//   rank    : inside each segment, rank by attach id -> stable (cell, id)
+//             order, identical to the reference's stable radix sort, and
+//             move the particle state to its new row (float4 SoA)
+//   lists   : neighbour list per row in the reference's order (27 offsets
+//             in fixed order, ascending attach id inside a cell), stored as
+//             a warp-interleaved ELL array of sorted row indices.
+#include "internal.h"
+
+namespace vtp {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ float4 apply_force(float4 p, float4 &v, float dt, float3 g) {
+    // apply_ext_force_cuda (PBFCudaImpl.cu:146-157): v += g dt; x += v dt.
+    v.x = __fmaf_rn(g.x, dt, v.x);
+    v.y = __fmaf_rn(g.y, dt, v.y);
+    v.z = __fmaf_rn(g.z, dt, v.z);
+    p.x = __fmaf_rn(v.x, dt, p.x);
+    p.y = __fmaf_rn(v.y, dt, p.y);
+    p.z = __fmaf_rn(v.z, dt, p.z);
+    return p;
+}
+
+__global__ void k_hash(Grid g, uint32_t row0, uint32_t cnt, const float4 *__restrict__ pos,
+                       const float4 *__restrict__ vel, float force_dt, float3 grav,
+                       uint32_t *__restrict__ key, uint32_t *__restrict__ rank, uint32_t *__restrict__ count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    float4 p = pos[row0 + i];
+    if (force_dt > 0.f) {
+        float4 v = vel[row0 + i];
+        p = apply_force(p, v, force_dt, grav);
+    }
+    int3 c = cell_of(p.x, p.y, p.z, g);
+    uint32_t k = cell_available(c, g) ? cell_key(c, g) : g.nkey;
+    key[i] = k;
+    rank[i] = atomicAdd(&count[k], 1u);
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t &total) {
+    __shared__ uint32_t warp_sums[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    if (wid == 0) {
+        uint32_t s = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t warp_off = wid > 0 ? warp_sums[wid - 1] : 0u;
+    total = warp_sums[nw - 1];
+    __syncthreads();
+    return warp_off + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const uint32_t *__restrict__ in, size_t n,
+                                                                 uint32_t *__restrict__ sums) {
+    size_t base = (size_t)blockIdx.x * kScanTile + threadIdx.x;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t idx = base + (size_t)k * kScanThreads;
+        if (idx < n) s += in[idx];
+    }
+    uint32_t total;
+    block_excl_scan(s, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *sums, size_t tiles) {
+    // One block; each thread owns a contiguous run of tiles.
+    const size_t per = (tiles + blockDim.x - 1) / blockDim.x;
+    size_t b = threadIdx.x * per;
+    uint32_t local = 0;
+    for (size_t k = 0; k < per; ++k)
+        if (b + k < tiles) local += sums[b + k];
+    uint32_t total;
+    uint32_t off = block_excl_scan(local, total);
+    for (size_t k = 0; k < per; ++k) {
+        if (b + k < tiles) {
+            uint32_t v = sums[b + k];
+            sums[b + k] = off;
+            off += v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__restrict__ in, size_t n,
+                                                             const uint32_t *__restrict__ sums, uint32_t base_add,
+                                                             uint32_t *__restrict__ out) {
+    // Each thread scans kScanItems consecutive counters.
+    __shared__ uint32_t tile[kScanTile];
+    size_t t0 = (size_t)blockIdx.x * kScanTile;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t idx = t0 + (size_t)k * kScanThreads + threadIdx.x;
+        tile[k * kScanThreads + threadIdx.x] = idx < n ? in[idx] : 0u;
+    }
+    __syncthreads();
+    uint32_t vals[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        vals[k] = tile[threadIdx.x * kScanItems + k];
+        s += vals[k];
+    }
+    uint32_t total;
+    uint32_t off = block_excl_scan(s, total) + sums[blockIdx.x] + base_add;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        tile[threadIdx.x * kScanItems + k] = off;
+        off += vals[k];
+    }
+    __syncthreads();
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t idx = t0 + (size_t)k * kScanThreads + threadIdx.x;
+        if (idx < n) out[idx] = tile[k * kScanThreads + threadIdx.x];
+    }
+}
+
+// The entry past the last counter holds the grand total (plus the base).
+__global__ void k_scan_total(const uint32_t *__restrict__ in, size_t n, uint32_t *__restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) out[n] = out[n - 1] + in[n - 1];
+}
+
+__global__ void k_scatter(uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ key,
+                          const uint32_t *__restrict__ rank, const uint32_t *__restrict__ start,
+                          const uint32_t *__restrict__ orig, uint32_t *__restrict__ tmp_src,
+                          uint32_t *__restrict__ tmp_orig, uint32_t *__restrict__ tmp_key) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    uint32_t k = key[i];
+    uint32_t d = start[k] - row0 + rank[i];
+    tmp_src[d] = i;
+    tmp_orig[d] = orig[row0 + i];
+    tmp_key[d] = k;
+}
+
+__global__ void k_rank_reorder(Grid g, uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ start,
+                               const uint32_t *__restrict__ tmp_src, const uint32_t *__restrict__ tmp_orig,
+                               const uint32_t *__restrict__ tmp_key, const float4 *__restrict__ pos_in,
+                               float4 *__restrict__ pos_out, const float4 *__restrict__ vel_in,
+                               float4 *__restrict__ vel_out, uint32_t *__restrict__ orig_out, Carry carry,
+                               float force_dt, float3 grav) {
+    uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= cnt) return;
+    uint32_t k = tmp_key[d];
+    uint32_t my = tmp_orig[d];
+    uint32_t dst = d;
+    if (k < g.nkey) {
+        // Stable order inside the cell: rank by attach id.
+        uint32_t s0 = start[k] - row0, s1 = start[k + 1] - row0;
+        uint32_t r = 0;
+        for (uint32_t x = s0; x < s1; ++x) r += (tmp_orig[x] < my) ? 1u : 0u;
+        dst = s0 + r;
+    }
+    uint32_t s = tmp_src[d];
+    float4 p = pos_in[row0 + s];
+    float4 v = vel_in[row0 + s];
+    if (force_dt > 0.f) p = apply_force(p, v, force_dt, grav);
+    pos_out[row0 + dst] = p;
+    vel_out[row0 + dst] = v;
+    orig_out[row0 + dst] = my;
+    for (int f = 0; f < carry.nf4; ++f) carry.dst4[f][row0 + dst] = carry.src4[f][row0 + s];
+    for (int f = 0; f < carry.nf1; ++f) carry.dst1[f][row0 + dst] = carry.src1[f][row0 + s];
+}
+
+// One candidate of the neighbour walk (UGNSCudaImpl.cu:189-199).
+struct Walker {
+    float px, py, pz;
+    uint32_t self;
+    uint32_t cnt;        // entries written incl. self
+    uint32_t maxnbr;
+    uint32_t *out;       // ELL base for this row (slot t at out[t*32])
+    bool overflow;
+
+    __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
+        if (j == self) return;
+        float4 q = pos[j];
+        float d2 = dist2(px - q.x, py - q.y, pz - q.z);
+        if (d2 > 0.f && d2 <= d2max) {
+            if (cnt < maxnbr) {
+                out[(size_t)(cnt - 1) * 32u] = j;
+                ++cnt;
+            } else {
+                overflow = true;
+            }
+        }
+    }
+};
+
+template <int MODE>
+__global__ void k_build_lists(Grid g, uint32_t row0, uint32_t cnt, uint32_t ell_stride,
+                              const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
+                              const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
+                              uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt,
+                              uint32_t *__restrict__ status, uint32_t *__restrict__ overflow_count) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cnt) return;
+    uint32_t i = row0 + r;
+    float4 p = pos[i];
+    int3 c = cell_of(p.x, p.y, p.z, g);
+    if (!cell_available(c, g)) {  // outside the grid: no neighbours, not even self
+        ncnt[r] = 0;
+        return;
+    }
+    Walker w;
+    w.px = p.x; w.py = p.y; w.pz = p.z;
+    w.self = i;
+    w.cnt = 1;
+    w.maxnbr = g.maxnbr;
+    w.out = nbr + ell_index(r, 0, ell_stride);
+    w.overflow = false;
+    const float d2max = g.d2max;
+    for (int t = 0; t < 27; ++t) {
+        int3 cc = c;
+        int3 o = nbr_offset(t);
+        cc.x += o.x; cc.y += o.y; cc.z += o.z;
+        if (!cell_available(cc, g)) continue;
+        uint32_t k = cell_key(cc, g);
+        uint32_t f0 = __ldg(fstart + k), f1 = __ldg(fstart + k + 1);
+        uint32_t b0 = __ldg(bstart + k), b1 = __ldg(bstart + k + 1);
+        if (MODE == 0) {
+            for (uint32_t j = f0; j < f1; ++j) w.visit(j, pos, d2max);
+            for (uint32_t j = b0; j < b1; ++j) w.visit(j, pos, d2max);
+        } else if (MODE == 1) {
+            for (uint32_t j = b0; j < b1; ++j) w.visit(j, pos, d2max);
+            for (uint32_t j = f0; j < f1; ++j) w.visit(j, pos, d2max);
+        } else {
+            // Merge the two id-sorted runs by attach id.
+            while (f0 < f1 || b0 < b1) {
+                uint32_t j;
+                if (b0 >= b1) j = f0++;
+                else if (f0 >= f1) j = b0++;
+                else j = (__ldg(orig + f0) < __ldg(orig + b0)) ? f0++ : b0++;
+                w.visit(j, pos, d2max);
+            }
+        }
+    }
+    ncnt[r] = w.cnt;
+    if (w.overflow) {
+        atomicAdd(overflow_count, 1u);
+        atomicOr(status, ST_BOUNDS);
+    }
+}
+
+__global__ void k_scatter_f4(uint32_t n, const float4 *__restrict__ src, const uint32_t *__restrict__ orig,
+                             float *__restrict__ dst3) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = src[i];
+    size_t o = (size_t)orig[i] * 3;
+    dst3[o] = v.x;
+    dst3[o + 1] = v.y;
+    dst3[o + 2] = v.z;
+}
+
+__global__ void k_scatter_f1(uint32_t n, const float *__restrict__ src, const uint32_t *__restrict__ orig,
+                             float *__restrict__ dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[orig[i]] = src[i];
+}
+
+__global__ void k_gather_f4(uint32_t n, const float *__restrict__ src3, const uint32_t *__restrict__ orig,
+                            float4 *__restrict__ dst, int keep_w) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    size_t o = (size_t)orig[i] * 3;
+    float4 v = dst[i];
+    v.x = src3[o];
+    v.y = src3[o + 1];
+    v.z = src3[o + 2];
+    if (!keep_w) v.w = 0.f;
+    dst[i] = v;
+}
+
+__global__ void k_gather_f1(uint32_t n, const float *__restrict__ src, const uint32_t *__restrict__ orig,
+                            float *__restrict__ dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src[orig[i]];
+}
+
+__global__ void k_iota(uint32_t n, uint32_t *dst, uint32_t base) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = base + i;
+}
+
+__global__ void k_export_neighbors(uint32_t row0, uint32_t cnt, uint32_t ell_stride,
+                                   const uint32_t *__restrict__ nbr, const uint32_t *__restrict__ ncnt,
+                                   const uint32_t *__restrict__ orig, uint32_t maxnbr,
+                                   uint32_t *__restrict__ out_cnt, uint32_t *__restrict__ out_nbr) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cnt) return;
+    uint32_t i = row0 + r;
+    uint32_t o = orig[i];
+    uint32_t c = ncnt[r];
+    out_cnt[o] = c;
+    uint32_t *dst = out_nbr + (size_t)o * maxnbr;
+    for (uint32_t t = 0; t < maxnbr; ++t) dst[t] = 0xffffffffu;
+    if (c == 0) return;
+    dst[0] = o;
+    for (uint32_t t = 1; t < c; ++t) dst[t] = orig[nbr[ell_index(r, t - 1, ell_stride)]];
+}
+
+__global__ void k_export_sorted(Grid g, uint32_t n, const float4 *__restrict__ pos,
+                                const uint32_t *__restrict__ orig, uint32_t *__restrict__ ids,
+                                uint32_t *__restrict__ keys) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    int3 c = cell_of(p.x, p.y, p.z, g);
+    ids[i] = orig[i];
+    keys[i] = cell_available(c, g) ? cell_key(c, g) : 0xffffffffu;
+}
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+static void scan_counts(cudaStream_t st, const uint32_t *count, size_t n, uint32_t base_add, uint32_t *out,
+                        UgnsBuffers &u) {
+    size_t tiles = (n + kScanTile - 1) / kScanTile;
+    k_scan_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums);
+    k_scan_sums<<<1, 1024, 0, st>>>(u.scan_sums, tiles);
+    k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums, base_add, out);
+    k_scan_total<<<1, 32, 0, st>>>(count, n, out);
+}
+
+void ugns_sort(cudaStream_t st, const Grid &g, uint32_t row0, uint32_t cnt, const float4 *pos_in, float4 *pos_out,
+               const float4 *vel_in, float4 *vel_out, const uint32_t *orig_in, uint32_t *orig_out,
+               const Carry &carry, float force_dt, float3 gravity, UgnsBuffers &u, uint32_t *start, Profiler *prof) {
+    const size_t nb = (size_t)g.nkey + 1;  // buckets incl. the outside bucket
+    auto B = [&] { if (prof) prof->begin(); };
+    auto E = [&](const char *nm) { if (prof) prof->end_(nm); };
+    B();
+    cudaMemsetAsync(u.count, 0, nb * sizeof(uint32_t), st);
+    if (cnt > 0) {
+        k_hash<<<nblk(cnt, 256), 256, 0, st>>>(g, row0, cnt, pos_in, vel_in, force_dt, gravity, u.key, u.rank,
+                                               u.count);
+    }
+    E("ugns_clear_hash");
+    B();
+    scan_counts(st, u.count, nb, row0, start, u);
+    E("ugns_cell_scan");
+    if (cnt == 0) return;
+    B();
+    k_scatter<<<nblk(cnt, 256), 256, 0, st>>>(row0, cnt, u.key, u.rank, start, orig_in, u.tmp_src, u.tmp_orig,
+                                              u.tmp_key);
+    E("ugns_scatter");
+    B();
+    k_rank_reorder<<<nblk(cnt, 256), 256, 0, st>>>(g, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
+                                                   pos_out, vel_in, vel_out, orig_out, carry, force_dt, gravity);
+    E("ugns_rank_reorder");
+}
+
+void ugns_build_lists(cudaStream_t st, const Grid &g, const Layout &L, uint32_t row0, uint32_t cnt,
+                      const float4 *pos, const uint32_t *orig, const UgnsBuffers &u, uint32_t *nbr, uint32_t *ncnt,
+                      uint32_t *status, uint32_t *overflow, int block) {
+    if (cnt == 0) return;
+    unsigned nb = nblk(cnt, block);
+    switch (L.merge_mode) {
+        case 0:
+            k_build_lists<0><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+                                                    ncnt, status, overflow);
+            break;
+        case 1:
+            k_build_lists<1><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+                                                    ncnt, status, overflow);
+            break;
+        default:
+            k_build_lists<2><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+                                                    ncnt, status, overflow);
+            break;
+    }
+}
+
+void scatter_f4_to_orig(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, float *dst3) {
+    if (n) k_scatter_f4<<<nblk(n, 256), 256, 0, st>>>(n, src, orig, dst3);
+}
+void scatter_f1_to_orig(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst) {
+    if (n) k_scatter_f1<<<nblk(n, 256), 256, 0, st>>>(n, src, orig, dst);
+}
+void gather_orig_to_f4(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, float4 *dst,
+                       int keep_w) {
+    if (n) k_gather_f4<<<nblk(n, 256), 256, 0, st>>>(n, src3, orig, dst, keep_w);
+}
+void gather_orig_to_f1(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst) {
+    if (n) k_gather_f1<<<nblk(n, 256), 256, 0, st>>>(n, src, orig, dst);
+}
+void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base) {
+    if (n) k_iota<<<nblk(n, 256), 256, 0, st>>>(n, dst, base);
+}
+void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
+                      const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
+                      uint32_t *out_nbr) {
+    if (cnt)
+        k_export_neighbors<<<nblk(cnt, 256), 256, 0, st>>>(row0, cnt, L.ell_stride, nbr, ncnt, orig, maxnbr, out_cnt,
+                                                           out_nbr);
+}
+void export_sorted(cudaStream_t st, const Grid &g, uint32_t n, const float4 *pos, const uint32_t *orig,
+                   uint32_t *out_ids, uint32_t *out_keys) {
+    if (n) k_export_sorted<<<nblk(n, 256), 256, 0, st>>>(g, n, pos, orig, out_ids, out_keys);
+}
+
+}  // namespace vtp

@@ -1,0 +1,48 @@
+"""Algorithmic bytes per kernel launch (state arrays touched once; FP32, float4 = 16 B).
+
+N = all rows (fluid + boundary), Nf = fluid rows, K = number of grid key
+buckets, k = mean neighbours per fluid row (self excluded).  "state" bytes
+follow the per-pass accounting of the project's bytes model; "list" adds the
+neighbour-list indices (4 B per stored neighbour), which the list-based
+design reads on top.
+"""
+from __future__ import annotations
+
+
+def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float) -> dict:
+    lst = 4.0 * k * Nf
+    if name == "ugns_clear_hash":
+        state = 4 * (K + 1) + 16 * Nf + 8 * Nf + (16 * Nf if kind == "PBF" else 0)
+        lst = 0
+    elif name == "ugns_cell_scan":
+        state, lst = 12 * (K + 1), 0
+    elif name == "ugns_scatter":
+        state, lst = 28 * Nf, 0
+    elif name == "ugns_rank_reorder":
+        fields = 2 if kind == "PBF" else 3
+        state, lst = 12 * Nf + 2 * 16 * fields * Nf + 8 * Nf, 0
+    elif name == "ugns_lists":
+        state = 16 * N + 16 * K + 4 * Nf
+    elif name == "pbf_lambda":
+        state = 16 * N + 8 * Nf
+    elif name == "pbf_dx":
+        state = 16 * N + 4 * N + 16 * Nf + 32 * Nf
+    elif name == "pbf_xsph":
+        state = 16 * N + 16 * N + 4 * N + 32 * Nf
+    elif name == "dfsph_ratio_alpha":
+        state = 16 * N + 8 * Nf
+    elif name == "dfsph_solve_a":
+        state = 32 * N + 16 * Nf
+    elif name == "dfsph_solve_b":
+        state = 20 * N + 32 * Nf
+    elif name in ("dfsph_viscosity", "dfsph_vis_normal"):
+        state = 48 * N + 32 * Nf
+    elif name == "dfsph_tension":
+        state = 48 * N + 48 * Nf
+    elif name == "dfsph_finalize":
+        state, lst = 96 * Nf, 0
+    elif name == "dfsph_solve_end":
+        state, lst = 8 * ((Nf + 127) // 128), 0
+    else:
+        state, lst = 0, 0
+    return {"state": float(state), "list": float(lst), "total": float(state + lst)}

@@ -1,0 +1,206 @@
+"""Seeded synthetic particle scenes.
+
+The lattice generators restate the arithmetic of the reference's scene
+generators so that particle counts and unjittered coordinates are identical:
+
+* ``cube``  follows ``ModelHandler::generateParticleCubeElements``
+  (Simulator/Library/Source/Model/ModelHandler.cpp:43-67): FP32 running sums
+  ``x += diameter`` starting at ``lb + r``, loop order z (outer), y, x (inner).
+* ``box``   follows ``ModelHandler::generateParticleBoxElements``
+  (ModelHandler.cpp:124-154): per-axis counts ``int((size + r) / (2.0 r))``,
+  indices ``0..n`` inclusive, a particle is kept when it lies in the first
+  ``layerNum`` or the last ``layerNum + 1`` index layers of any axis, loop
+  order x (outer), y, z (inner), coordinates computed in double and rounded
+  to float.
+
+Jitter is the project's own: SplitMix64 per scene seed, one uniform draw per
+component in generation order, ``(2u - 1) * a * spacing`` added in double and
+rounded to float32.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+EPM_FLUID = 0
+EPM_BOUNDARY = 1
+
+_MASK64 = (1 << 64) - 1
+
+
+def splitmix64_uniform(seed: int, count: int) -> np.ndarray:
+    """``count`` doubles in [0, 1) from SplitMix64 started at ``seed``."""
+    idx = np.arange(1, count + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = (np.uint64(seed & _MASK64) + idx * np.uint64(0x9E3779B97F4A7C15))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def _f32_run(start: np.float32, limit: np.float32, step: np.float32) -> np.ndarray:
+    vals = []
+    v = np.float32(start)
+    while v < limit:
+        vals.append(v)
+        v = np.float32(v + step)
+    return np.array(vals, dtype=np.float32)
+
+
+def cube(r: float, lb, size) -> np.ndarray:
+    """Lattice cube, same count and coordinates as the reference generator."""
+    r = np.float32(r)
+    lb = [np.float32(v) for v in lb]
+    size = [np.float32(v) for v in size]
+    d = np.float32(2 * r)
+    xs = _f32_run(np.float32(r + lb[0]), np.float32(lb[0] + size[0]), d)
+    ys = _f32_run(np.float32(r + lb[1]), np.float32(lb[1] + size[1]), d)
+    zs = _f32_run(np.float32(r + lb[2]), np.float32(lb[2] + size[2]), d)
+    z, y, x = np.meshgrid(zs, ys, xs, indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.float32)
+
+
+def box(r: float, lb, size, layer_num: int) -> np.ndarray:
+    """Hollow box shell, same count and coordinates as the reference generator."""
+    r32 = np.float32(r)
+    lb = [np.float32(v) for v in lb]
+    size = [np.float32(v) for v in size]
+    n = [int(float(np.float32(size[a] + r32)) / (2.0 * float(r32))) for a in range(3)]
+    axes = []
+    for a in range(3):
+        base = float(np.float32(lb[a] + r32))
+        idx = np.arange(n[a] + 1, dtype=np.float64)
+        axes.append((base + 2.0 * float(r32) * idx).astype(np.float32))
+    I, J, K = np.meshgrid(np.arange(n[0] + 1), np.arange(n[1] + 1), np.arange(n[2] + 1), indexing="ij")
+    L = layer_num
+    keep = ((I < L) | (I >= n[0] - L) | (J < L) | (J >= n[1] - L) | (K < L) | (K >= n[2] - L))
+    pts = np.stack([axes[0][I[keep]], axes[1][J[keep]], axes[2][K[keep]]], axis=1)
+    return pts.astype(np.float32)
+
+
+def jitter(pos: np.ndarray, amplitude: float, spacing: float, seed: int) -> np.ndarray:
+    """Add SplitMix64 jitter of +-amplitude*spacing per component (double, then float32)."""
+    if amplitude == 0.0:
+        return pos.astype(np.float32).copy()
+    u = splitmix64_uniform(seed, pos.size).reshape(pos.shape)
+    return (pos.astype(np.float64) + (2.0 * u - 1.0) * amplitude * spacing).astype(np.float32)
+
+
+@dataclass
+class SceneObject:
+    """One attached object: particles plus the reference's per-object configs."""
+    name: str
+    pos: np.ndarray                      # (n, 3) float32
+    material: int                        # EPM_FLUID / EPM_BOUNDARY
+    velocity_start: tuple = (0.0, 0.0, 0.0)
+    color_start: tuple = (0.0, 0.0, 0.0)
+    export_flag: bool = False
+    phase_fraction: tuple | None = None  # IMM / IMM-CT only
+    velocity: np.ndarray | None = None   # optional per-particle initial velocity (n, 3)
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+
+@dataclass
+class Scene:
+    solver: str                          # "PBF" | "DFSPH" | "IMM" | "IMMCT"
+    config: dict
+    objects: list = field(default_factory=list)
+
+    @property
+    def n_total(self) -> int:
+        return sum(o.n for o in self.objects)
+
+    @property
+    def n_fluid(self) -> int:
+        return sum(o.n for o in self.objects if o.material == EPM_FLUID)
+
+    @property
+    def n_boundary(self) -> int:
+        return sum(o.n for o in self.objects if o.material == EPM_BOUNDARY)
+
+
+def _export_block():
+    return {"Common": {"exportTargetDir": "out", "exportFilePrefix": "obj", "exportFileType": "PLY"},
+            "SolverRequired": {"enable": False, "exportFps": 35, "exportGroupPolicy": "MERGE"}}
+
+
+def pbf_config(*, dt, r, lb, size, iterations=4, xsph_k=0.01, rho_f=1000.0, rho_b=1000.0,
+               gravity=(0.0, -9.81, 0.0), max_nbr=60, animation_time=10.0):
+    return {"PBF": {"Required": {"animationTime": animation_time, "timeStep": dt, "particleRadius": r,
+                                 "simSpaceLB": list(lb), "simSpaceSize": list(size),
+                                 "maxNeighborNum": max_nbr, "iterationNum": iterations, "XSPH_k": xsph_k,
+                                 "fPartRestDensity": rho_f, "bPartRestDensity": rho_b},
+                    "Optional": {"enable": True, "gravity": list(gravity)}},
+            "EXPORT": _export_block()}
+
+
+def dfsph_config(*, dt, r, lb, size, rho_f=1000.0, rho_b=1000.0, viscosity=1e-6, div_thr=1e-3,
+                 incomp_thr=1e-3, tension=0.0, gravity=(0.0, -9.81, 0.0), max_nbr=60, animation_time=10.0):
+    return {"DFSPH": {"Required": {"animationTime": animation_time, "timeStep": dt, "particleRadius": r,
+                                   "simSpaceLB": list(lb), "simSpaceSize": list(size),
+                                   "maxNeighborNum": max_nbr, "fPartRestDensity": rho_f,
+                                   "bPartRestDensity": rho_b, "fPartRestViscosity": viscosity,
+                                   "divFreeThreshold": div_thr, "incompThreshold": incomp_thr,
+                                   "surfaceTensionCoefficient": tension},
+                      "Optional": {"enable": True, "gravity": list(gravity)}},
+            "EXPORT": _export_block()}
+
+
+def pbf_dam_break(seed: int = 1001, jitter_amp: float = 0.1) -> Scene:
+    """PBF dam break: 20x40x20 fluid lattice (16,000) in a 2-layer box (35,315), h = 0.04."""
+    r = 0.01
+    fluid = jitter(cube(r, (0.04, 0.04, 0.04), (0.4, 0.8, 0.4)), jitter_amp, 2 * r, seed)
+    wall = box(r, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 2)
+    cfg = pbf_config(dt=1.0 / 240.0, r=r, lb=(-0.1, -0.1, -0.1), size=(1.2, 1.2, 1.2))
+    return Scene("PBF", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, color_start=(0, 0, 1)),
+                              SceneObject("box", wall, EPM_BOUNDARY)])
+
+
+def dfsph_1m(seed: int = 2002, jitter_amp: float = 0.05) -> Scene:
+    """DFSPH 1M: 100^3 fluid lattice at spacing 0.01 in a 2x1.5x1 3-layer box (439,467)."""
+    r = 0.005
+    fluid = jitter(cube(r, (0.03, 0.03, 0.03), (1.0, 1.0, 1.0)), jitter_amp, 2 * r, seed)
+    wall = box(r, (0.0, 0.0, 0.0), (2.0, 1.5, 1.0), 3)
+    cfg = dfsph_config(dt=1e-3, r=r, lb=(-0.05, -0.05, -0.05), size=(2.1, 1.6, 1.1))
+    return Scene("DFSPH", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, color_start=(0, 0, 1)),
+                                SceneObject("box", wall, EPM_BOUNDARY)])
+
+
+def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, jitter_amp: float = 0.05) -> Scene:
+    """Dam break of about ``n_target`` particles: fluid block n x 2n x n in a cubic box of side n*spacing/0.4.
+
+    Used for the small parity scenes and the batched scene mix; number density is constant
+    because the box scales with the fluid block.
+    """
+    spacing = 0.02 if solver == "PBF" else 0.01
+    r = spacing / 2
+    n = max(2, int(round((n_target / 2.0) ** (1.0 / 3.0))))
+    side = n * spacing / 0.4
+    layers = 2 if solver == "PBF" else 3
+    off = layers * spacing + spacing
+    fluid = cube(r, (off, off, off), (n * spacing, 2 * n * spacing, n * spacing))
+    fluid = jitter(fluid, jitter_amp, spacing, seed)
+    wall = box(r, (0.0, 0.0, 0.0), (side, max(side, 2 * n * spacing + 2 * off), side), layers)
+    ext = np.float32(max(side, 2 * n * spacing + 2 * off))
+    lb = (-2 * spacing * 2.5,) * 3
+    size = (float(side) + 5 * 2 * spacing * 2.5, float(ext) + 5 * 2 * spacing * 2.5, float(side) + 5 * 2 * spacing * 2.5)
+    g = (0.0, gravity_y, 0.0)
+    if solver == "PBF":
+        cfg = pbf_config(dt=1.0 / 240.0, r=r, lb=lb, size=size, gravity=g)
+    else:
+        cfg = dfsph_config(dt=1e-3, r=r, lb=lb, size=size, gravity=g)
+    return Scene(solver, cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True),
+                               SceneObject("box", wall, EPM_BOUNDARY)])
+
+
+def grid_dims(cfg_block: dict, h: float):
+    """Grid dimensions as ``UniformGirdNeighborSearcher::setConfig`` computes them (ceil(size / h))."""
+    size = cfg_block["Required"]["simSpaceSize"]
+    hh = np.float32(h)
+    return tuple(int(math.ceil(float(np.float32(np.float32(s) / hh)))) for s in size)
