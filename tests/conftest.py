@@ -5,7 +5,7 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
-for p in (ROOT, ROOT / "vt-physics_b200"):
+for p in (ROOT, ROOT / "vt-physics_b200", ROOT / "tests"):
     if str(p) not in sys.path:
         sys.path.insert(0, str(p))
 

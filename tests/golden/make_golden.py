@@ -89,7 +89,7 @@ def run_case(case: str, out_dir: Path):
         cnt, nb = s.neighbors()
         rec[f"nbr_digest_{t}"] = digest(cnt, nb)
         arrays[f"nbr_count_hist_{t}"] = np.bincount(cnt, minlength=s.maxnbr + 1).astype(np.int64)
-        if full:
+        if full and t == 0:
             valid = nb != 0xFFFFFFFF
             arrays[f"nbr_count_{t}"] = cnt.astype(np.uint16)
             arrays[f"nbr_flat_{t}"] = nb[valid].astype(np.uint32)

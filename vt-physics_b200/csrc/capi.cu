@@ -171,6 +171,15 @@ int vtp_solver::parse_config(const json &c) {
             const json &b = c["B200"];
             force_div = b.value("forceDivIterations", 0u);
             force_inc = b.value("forceIncompIterations", 0u);
+            force_seq.clear();
+            if (b.contains("forceIterationsPerTick")) {
+                for (auto &pair : b["forceIterationsPerTick"]) {
+                    auto v = pair.get<std::vector<uint32_t>>();
+                    if (v.size() != 2) return fail(VTP_ERR_CONFIG, "forceIterationsPerTick entries are [div, incomp]");
+                    force_seq.push_back(v[0]);
+                    force_seq.push_back(v[1]);
+                }
+            }
             device_loop = b.value("deviceLoop", true);
             use_graphs = b.value("useGraphs", true);
             stage_timers = b.value("stageTimers", false);
@@ -256,6 +265,7 @@ vtp::DfsphArgs vtp_solver::dfsph_args() {
     a.ratio = ratio; a.alpha = alpha; a.kappa = kappa; a.delta = delta;
     a.acc_tmp = acc_tmp; a.normal = normal;
     a.orig = orig.c(); a.obj_of = obj_of; a.nobj = nobj_fluid; a.partials = partials; a.status = d_status;
+    a.tick = d_tick;
     return a;
 }
 
@@ -268,6 +278,10 @@ vtp::SolveCtl vtp_solver::solve_ctl(int which, cudaGraphConditionalHandle hnd, i
     if (c.nblocks == 0) c.nblocks = 1;
     c.threshold = which == 0 ? div_thr : incomp_thr;
     c.force_iters = which == 0 ? force_div : force_inc;
+    c.force_seq = d_force_seq;
+    c.force_seq_len = (uint32_t)(force_seq.size() / 2);
+    c.tick = d_tick;
+    c.which = which;
     c.max_iters = 101;
     c.cond = hnd;
     c.use_cond = use_cond;
@@ -326,7 +340,7 @@ int vtp_solver::initialize() {
     grid.maxnbr = maxnbr;
     kc.h = h;
     kc.invh = 1.f / h;
-    kc.sigma = 8.f / 3.14159265f / std::pow(h, 3.f);
+    kc.sigma = 8.f / 3.14159265f / std::pow(h, 3.f);  // replaced by the device value below
     kc.w0 = kc.sigma;
 
     if (!st) {
@@ -335,6 +349,8 @@ int vtp_solver::initialize() {
         for (auto &e : ev) CU(cudaEventCreate(&e));
         CU(cudaMallocHost((void **)&h_pinned, 8 * sizeof(uint32_t)));
     }
+    if (vtp::cubic_sigma_device(st, h, &kc.sigma)) return fail(VTP_ERR_CUDA, "cubic sigma kernel failed");
+    kc.w0 = kc.sigma;  // W(0) = sigma * (6*0 - 6*0 + 1)
     int rc;
 #define AL(p, cnt) \
     if ((rc = alloc(p, cnt))) return rc
@@ -408,6 +424,13 @@ int vtp_solver::initialize() {
         AL(&normal, L.nf);
         AL(&solve, 2);
         CU(cudaMemsetAsync(solve, 0, 2 * sizeof(vtp::SolveState), st));
+        AL(&d_tick, 1);
+        CU(cudaMemsetAsync(d_tick, 0, sizeof(uint64_t), st));
+        if (!force_seq.empty()) {
+            AL(&d_force_seq, force_seq.size());
+            CU(cudaMemcpyAsync(d_force_seq, force_seq.data(), force_seq.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, st));
+        }
         CU(cudaMemsetAsync(kappa, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
         CU(cudaMemsetAsync(ratio, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
         CU(cudaMemsetAsync(alpha, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
@@ -965,7 +988,26 @@ int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, ui
     if (!s->initialized) return fail(VTP_ERR_STATE, "get_neighbors before initialize");
     if (max_nbr != s->maxnbr) return fail(VTP_ERR_ARG, "max_nbr must equal maxNeighborNum");
     const uint32_t n = s->L.n;
-    // Boundary rows' lists are rebuilt here (the substep only needs fluid rows).
+    // Neighbour search of the current state, all rows (UniformGirdNeighborSearcher::update on the
+    // current positions): re-sort the fluid rows and rebuild both row ranges' lists.  Every
+    // substep starts with the same search, so the solver state is unaffected.
+    vtp::Carry carry{};
+    if (s->vadv.c()) {
+        carry.nf4 = 1;
+        carry.src4[0] = s->vadv.c();
+        carry.dst4[0] = s->vadv.n();
+    }
+    vtp::ugns_sort(s->st, s->grid, 0, s->L.nf, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(), s->orig.c(),
+                   s->orig.n(), carry, 0.f, make_float3(0, 0, 0), s->u, s->u.fstart);
+    // Copy the re-sorted fluid rows back so the buffer parity the substep graphs expect is kept.
+    const size_t nf = s->L.nf;
+    CU(cudaMemcpyAsync(s->pos.c(), s->pos.n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    CU(cudaMemcpyAsync(s->vel.c(), s->vel.n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    CU(cudaMemcpyAsync(s->orig.c(), s->orig.n(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s->st));
+    if (s->vadv.c())
+        CU(cudaMemcpyAsync(s->vadv.c(), s->vadv.n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    vtp::ugns_build_lists(s->st, s->grid, s->L, 0, s->L.nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
+                          s->d_status, s->d_overflow, s->block);
     vtp::ugns_build_lists(s->st, s->grid, s->L, s->L.nf, s->L.nb, s->pos.c(), s->orig.c(), s->u, s->u.bnbr,
                           s->u.bncnt, s->d_status, s->d_overflow, s->block);
     uint32_t *dc = nullptr, *dn = nullptr;

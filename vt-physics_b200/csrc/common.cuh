@@ -72,17 +72,22 @@ struct Cubic {
     float w0;      // W(0) = sigma
 };
 
-// W(r) from r^2.
+// W(r) from r^2, rounded the way sph::cubic_value rounds it
+// (KernelFunctions.cuh:13-34): IEEE sqrt, q = r * (1/h), the inner branch
+// evaluated in double and rounded once, the outer branch as
+// (sigma * 2) * powf(1 - q, 3).  Density-ratio sums feed `ratio - 1`, where
+// FP32 rounding is amplified ~1e3 times in the pressure solve, so W follows
+// the reference's arithmetic; gradients use the faster form below.
 __device__ __forceinline__ float cubic_w(float d2, const Cubic &k) {
-    float r = sqrtf(d2);
-    float q = r * k.invh;
+    const float r = sqrtf(d2);
+    const float q = r * k.invh;
     if (q > 1.f) return 0.f;
     if (q <= 0.5f) {
-        float q2 = q * q;
-        return k.sigma * __fmaf_rn(6.f * q2, q - 1.f, 1.f);
+        const float q2 = q * q;
+        const float q3 = q2 * q;
+        return static_cast<float>((double)k.sigma * (6.0 * (double)q3 - 6.0 * (double)q2 + 1.0));
     }
-    float t = 1.f - q;
-    return (k.sigma * 2.f) * (t * t * t);
+    return k.sigma * 2.f * powf(1.f - q, 3.f);
 }
 
 // Scalar g with gradW(r_vec) = g * r_vec; zero for q < 1e-6 or q > 1.
@@ -101,28 +106,15 @@ __device__ __forceinline__ float cubic_g(float d2, const Cubic &k) {
     return f * k.sigma * (rinv * k.invh);
 }
 
-// W and g together (shared sqrt).
+// W and g together.
 __device__ __forceinline__ void cubic_wg(float d2, const Cubic &k, float &w, float &g) {
-    w = 0.f;
-    g = 0.f;
-    if (!(d2 > 0.f)) {
-        if (d2 == 0.f) w = k.w0;
-        return;
-    }
-    float rinv = rsqrtf(d2);
-    float r = d2 * rinv;
-    float q = r * k.invh;
-    if (q > 1.f) return;
-    if (q <= 0.5f) {
-        float q2 = q * q;
-        w = k.sigma * __fmaf_rn(6.f * q2, q - 1.f, 1.f);
-        if (q >= 1e-6f) g = 6.f * q * (3.f * q - 2.f) * k.sigma * (rinv * k.invh);
-    } else {
-        float t = 1.f - q;
-        w = (k.sigma * 2.f) * (t * t * t);
-        g = -6.f * t * t * k.sigma * (rinv * k.invh);
-    }
+    w = cubic_w(d2, k);
+    g = cubic_g(d2, k);
 }
+
+// sigma = 8 / pi / powf(h, 3) evaluated on the device, as every reference
+// kernel evaluates it (KernelFunctions.cuh:16-17).
+__global__ void k_cubic_sigma(float h, float *out);
 
 // Akinci cohesion spline sph::surface_tension_C (KernelFunctions.cuh:59-70).
 __device__ __forceinline__ float tension_c(float r, float h, float csigma, float h6_64) {

@@ -193,8 +193,13 @@ __global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__r
     const uint32_t iter = st->iter + 1;
     st->iter = iter;
     st->residual = residual;
+    uint32_t force = c.force_iters;
+    if (c.force_seq && c.tick) {
+        const uint64_t t = *c.tick;
+        if (t < c.force_seq_len) force = c.force_seq[2 * t + c.which];
+    }
     bool stop;
-    if (c.force_iters > 0) stop = iter >= c.force_iters;
+    if (force > 0) stop = iter >= force;
     else stop = (residual < (double)c.threshold) || iter > c.max_iters - 1;
     if (!(residual == residual)) {  // NaN residual: stop and flag
         stop = true;
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__r
         st->last_iters = iter;
         st->total_iters += iter;
         // vfsph_div / vfsph_incomp flag a crash whenever the loop ran past 100 iterations.
-        if (c.force_iters == 0 && iter > c.max_iters - 1) atomicOr(status, ST_NOT_CONVERGED);
+        if (force == 0 && iter > c.max_iters - 1) atomicOr(status, ST_NOT_CONVERGED);
     }
     if (c.use_cond) cudaGraphSetConditional(c.cond, stop ? 0u : 1u);
 }
@@ -296,6 +301,7 @@ __global__ void k_finalize(DfsphArgs a) {
     const float4 v = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
     a.vel[r] = v;
     a.vadv[r] = v;
+    if (r == 0 && a.tick) *a.tick += 1;
     float4 p = a.pos[r];
     p.x = __fmaf_rn(v.x, a.dt, p.x);
     p.y = __fmaf_rn(v.y, a.dt, p.y);

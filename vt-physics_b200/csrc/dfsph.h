@@ -39,6 +39,7 @@ struct DfsphArgs {
     int nobj;                   // fluid objects (>= 1)
     double *partials;           // [blocks][nobj]
     uint32_t *status;
+    uint64_t *tick;             // substep counter, advanced by the finalize pass
 };
 
 struct SolveCtl {
@@ -48,6 +49,10 @@ struct SolveCtl {
     uint32_t nblocks;           // partial rows
     float threshold;
     uint32_t force_iters;       // 0 = residual test
+    const uint32_t *force_seq;  // optional per-substep [div, incomp] counts (device)
+    uint32_t force_seq_len;     // substeps covered by force_seq
+    const uint64_t *tick;       // device substep counter (advanced by dfsph_finalize)
+    int which;                  // 0 divergence solve, 1 density solve
     uint32_t max_iters;         // reference: stop after iteration 101
     cudaGraphConditionalHandle cond;
     int use_cond;

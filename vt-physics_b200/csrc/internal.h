@@ -80,6 +80,9 @@ void ugns_build_lists(cudaStream_t st, const Grid &g, const Layout &L, uint32_t 
                       const float4 *pos, const uint32_t *orig, const UgnsBuffers &u,
                       uint32_t *nbr, uint32_t *ncnt, uint32_t *status, uint32_t *overflow, int block);
 
+// sigma of the cubic spline computed on the device (0 on success).
+int cubic_sigma_device(cudaStream_t st, float h, float *out_host);
+
 // Gather/scatter between attach order and sorted rows.
 void scatter_f4_to_orig(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, float *dst3);
 void scatter_f1_to_orig(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst);

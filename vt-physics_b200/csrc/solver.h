@@ -60,6 +60,9 @@ struct vtp_solver {
 
     // extensions ("B200" block)
     uint32_t force_div = 0, force_inc = 0;
+    std::vector<uint32_t> force_seq;    // per-substep [div, incomp] iteration counts
+    uint32_t *d_force_seq = nullptr;
+    uint64_t *d_tick = nullptr;
     bool device_loop = true, use_graphs = true, stage_timers = false, stop_on_crash = true;
     int block = 128;
 

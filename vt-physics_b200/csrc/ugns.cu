@@ -344,6 +344,21 @@ inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
 
+__global__ void k_cubic_sigma(float h, float *out) {
+    const float PI = 3.14159265f;
+    if (threadIdx.x == 0) out[0] = 8.f / PI / powf(h, 3.f);
+}
+
+int cubic_sigma_device(cudaStream_t st, float h, float *out_host) {
+    float *d = nullptr;
+    if (cudaMalloc(&d, sizeof(float)) != cudaSuccess) return 1;
+    k_cubic_sigma<<<1, 32, 0, st>>>(h, d);
+    cudaError_t e = cudaMemcpyAsync(out_host, d, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : 1;
+}
+
 static void scan_counts(cudaStream_t st, const uint32_t *count, size_t n, uint32_t base_add, uint32_t *out,
                         UgnsBuffers &u) {
     size_t tiles = (n + kScanTile - 1) / kScanTile;

@@ -163,11 +163,18 @@ def pbf_dam_break(seed: int = 1001, jitter_amp: float = 0.1) -> Scene:
 
 
 def dfsph_1m(seed: int = 2002, jitter_amp: float = 0.05) -> Scene:
-    """DFSPH 1M: 100^3 fluid lattice at spacing 0.01 in a 2x1.5x1 3-layer box (439,467)."""
+    """DFSPH 1M: 100^3 fluid lattice at spacing 0.01 (x, y, z in [0.035, 1.025]) in a 3-layer box.
+
+    The box is 2 x 1.5 x 1.06 (outer): a 1 m fluid cube does not fit inside a
+    1 m box whose 3-layer walls are 0.03 m thick, so the z extent is widened until
+    the far wall starts one spacing beyond the fluid (wall layers at z = 1.035 ...
+    1.065).  The grid spans [-0.05, 2.05] x [-0.05, 1.55] x [-0.05, 1.15], leaving
+    at least two empty cell layers beyond every wall.
+    """
     r = 0.005
     fluid = jitter(cube(r, (0.03, 0.03, 0.03), (1.0, 1.0, 1.0)), jitter_amp, 2 * r, seed)
-    wall = box(r, (0.0, 0.0, 0.0), (2.0, 1.5, 1.0), 3)
-    cfg = dfsph_config(dt=1e-3, r=r, lb=(-0.05, -0.05, -0.05), size=(2.1, 1.6, 1.1))
+    wall = box(r, (0.0, 0.0, 0.0), (2.0, 1.5, 1.06), 3)
+    cfg = dfsph_config(dt=1e-3, r=r, lb=(-0.05, -0.05, -0.05), size=(2.1, 1.6, 1.2))
     return Scene("DFSPH", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, color_start=(0, 0, 1)),
                                 SceneObject("box", wall, EPM_BOUNDARY)])
 
