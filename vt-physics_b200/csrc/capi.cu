@@ -185,6 +185,9 @@ int vtp_solver::parse_config(const json &c) {
             stage_timers = b.value("stageTimers", false);
             stop_on_crash = b.value("stopOnNonConvergence", true);
             block = b.value("blockSize", 128);
+            unroll = b.value("unroll", 4);
+            if (unroll != 1 && unroll != 2 && unroll != 4 && unroll != 8)
+                return fail(VTP_ERR_CONFIG, "unroll must be 1, 2, 4 or 8");
             if (block < 32 || block > 256 || (block & 31)) return fail(VTP_ERR_CONFIG, "blockSize must be 32..256, multiple of 32");
         }
     } catch (const std::exception &e) {
@@ -246,6 +249,7 @@ vtp::PbfArgs vtp_solver::pbf_args() {
     a.nbr = u.nbr; a.ncnt = u.ncnt;
     a.pos = pos.c(); a.pos_alt = pos.n(); a.vel = vel.c(); a.vel_alt = vel.n();
     a.vol = vol; a.density = density; a.lambda = lambda;
+    a.unroll = unroll;
     return a;
 }
 
@@ -266,6 +270,7 @@ vtp::DfsphArgs vtp_solver::dfsph_args() {
     a.acc_tmp = acc_tmp; a.normal = normal;
     a.orig = orig.c(); a.obj_of = obj_of; a.nobj = nobj_fluid; a.partials = partials; a.status = d_status;
     a.tick = d_tick;
+    a.unroll = unroll;
     return a;
 }
 

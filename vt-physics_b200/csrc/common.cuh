@@ -131,4 +131,44 @@ __device__ __forceinline__ float tension_c(float r, float h, float csigma, float
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 
+// Walks `cnt` list entries (warp-interleaved ELL, slot t at lst[t * 32]) in
+// order, U at a time: the list indices of the next batch are loaded before the
+// current batch's gathers (`load(j)`) are issued, so each thread keeps U
+// gathers and U index loads in flight.  `use(j, data)` runs in list order,
+// which keeps FP32 accumulation order identical for every U.
+template <int U, class Load, class Use>
+__device__ __forceinline__ void nbr_loop(const uint32_t *__restrict__ lst, uint32_t cnt, Load load, Use use) {
+    if (U <= 1) {
+        for (uint32_t t = 0; t < cnt; ++t) {
+            const uint32_t j = __ldcs(lst + (size_t)t * 32u);
+            use(j, load(j));
+        }
+        return;
+    }
+    using T = decltype(load(0u));
+    uint32_t nxt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) nxt[u] = (uint32_t)u < cnt ? __ldcs(lst + (size_t)u * 32u) : 0u;
+    uint32_t t = 0;
+    for (; t + U <= cnt; t += U) {
+        uint32_t j[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) j[u] = nxt[u];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t tt = t + U + (uint32_t)u;
+            nxt[u] = tt < cnt ? __ldcs(lst + (size_t)tt * 32u) : 0u;
+        }
+        T d[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) d[u] = load(j[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) use(j[u], d[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (t + (uint32_t)u < cnt) use(nxt[u], load(nxt[u]));
+    }
+}
+
 }  // namespace vtp

@@ -81,6 +81,21 @@ __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_
     rest_density_b[r] = vb * a.rho_b;
 }
 
+struct PV {
+    float4 q, v;
+};
+struct PK {
+    float4 q;
+    float k;
+};
+struct PVV {
+    float4 q, v, va;
+};
+struct PN {
+    float4 q, n;
+};
+
+template <int U>
 __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -91,26 +106,25 @@ __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
     float a2 = 1e-6f;
     const float inv_mf = 1.f / a.mass_f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = ldg4(a.pos + j);
-        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-        float w, g;
-        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
-        ratio = __fmaf_rn(q.w, w, ratio);
-        const float gx = g * dx, gy = g * dy, gz = g * dz;
-        a1x = __fmaf_rn(q.w, gx, a1x);
-        a1y = __fmaf_rn(q.w, gy, a1y);
-        a1z = __fmaf_rn(q.w, gz, a1z);
-        if (j < a.nf) a2 += (gx * gx + gy * gy + gz * gz) * q.w * q.w * inv_mf;
-    }
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pos + j); },
+                [&](uint32_t j, const float4 &q) {
+                    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+                    float w, g;
+                    cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+                    ratio = __fmaf_rn(q.w, w, ratio);
+                    const float gx = g * dx, gy = g * dy, gz = g * dz;
+                    a1x = __fmaf_rn(q.w, gx, a1x);
+                    a1y = __fmaf_rn(q.w, gy, a1y);
+                    a1z = __fmaf_rn(q.w, gz, a1z);
+                    if (j < a.nf) a2 += (gx * gx + gy * gy + gz * gz) * q.w * q.w * inv_mf;
+                });
     float alpha = (a1x * a1x + a1y * a1y + a1z * a1z) / a.mass_f + a2;
     if (alpha < 1e-6f) alpha = 1e-6f;
     a.ratio[r] = ratio;
     a.alpha[r] = alpha;
 }
 
-template <bool MULTI>
+template <bool MULTI, int U>
 __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
@@ -121,15 +135,13 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
         const uint32_t n = a.ncnt[r];
         float d = a.ratio[r] - 1.f;
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        for (uint32_t t = 0; t + 1 < n; ++t) {
-            const uint32_t j = lst[(size_t)t * 32u];
-            const float4 q = ldg4(a.pos + j);
-            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-            const float g = cubic_g(dist2(rx, ry, rz), a.k);
-            const float4 vj = ldg4(a.vadv + j);
-            const float dot = g * (rx * (vi.x - vj.x) + ry * (vi.y - vj.y) + rz * (vi.z - vj.z));
-            d = __fmaf_rn(dot * q.w, a.dt, d);
-        }
+        nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return PV{ldg4(a.pos + j), ldg4(a.vadv + j)}; },
+                    [&](uint32_t, const PV &e) {
+                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+                        const float dot = g * (rx * (vi.x - e.v.x) + ry * (vi.y - e.v.y) + rz * (vi.z - e.v.z));
+                        d = __fmaf_rn(dot * e.q.w, a.dt, d);
+                    });
         if (d < 0.f) d = 0.f;
         a.delta[r] = d;
         a.kappa[r] = d / a.alpha[r] * a.inv_dt2 / p.w;
@@ -147,6 +159,7 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
     }
 }
 
+template <int U>
 __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -156,18 +169,17 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     const uint32_t n = a.ncnt[r];
     const float ci = a.dt * p.w / a.mass_f;   // dt V_i / m_i
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = ldg4(a.pos + j);
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float g = cubic_g(dist2(rx, ry, rz), a.k);
-        // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
-        const float kj = j < a.nf ? __ldg(a.kappa + j) : 0.f;
-        const float s = ci * q.w * (ki + kj) * g;
-        v.x = __fmaf_rn(-s, rx, v.x);
-        v.y = __fmaf_rn(-s, ry, v.y);
-        v.z = __fmaf_rn(-s, rz, v.z);
-    }
+    // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) { return PK{ldg4(a.pos + j), j < a.nf ? __ldg(a.kappa + j) : 0.f}; },
+                [&](uint32_t, const PK &e) {
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float g = cubic_g(dist2(rx, ry, rz), a.k);
+                    const float s = ci * e.q.w * (ki + e.k) * g;
+                    v.x = __fmaf_rn(-s, rx, v.x);
+                    v.y = __fmaf_rn(-s, ry, v.y);
+                    v.z = __fmaf_rn(-s, rz, v.z);
+                });
     a.vadv[r] = v;
 }
 
@@ -215,7 +227,7 @@ __global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__r
     if (c.use_cond) cudaGraphSetConditional(c.cond, stop ? 0u : 1u);
 }
 
-template <bool TENSION_SPLIT>
+template <bool TENSION_SPLIT, int U>
 __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -226,27 +238,30 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     float nx = 0.f, ny = 0.f, nz = 0.f;
     const float ncoef = a.k.h * a.mass_f / a.rho0;   // h m_j / rho_rest_j (fluid)
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        if (j >= a.nf) continue;   // same-material neighbours only
-        const float4 q = ldg4(a.pos + j);
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float d2 = dist2(rx, ry, rz);
-        const float g = cubic_g(d2, a.k);
-        const float4 vj = pressure_applied(ldg4(a.vel + j), ldg4(a.vadv + j), a.inv_dt, a.dt);
-        const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-        const float pi = a.vis_coef * (vx * rx + vy * ry + vz * rz) / (d2 + a.h2_001);
-        const float s = 10.f * pi * g;
-        ax = __fmaf_rn(s, rx, ax);
-        ay = __fmaf_rn(s, ry, ay);
-        az = __fmaf_rn(s, rz, az);
-        if (TENSION_SPLIT) {
-            const float sn = ncoef * g;
-            nx = __fmaf_rn(sn, rx, nx);
-            ny = __fmaf_rn(sn, ry, ny);
-            nz = __fmaf_rn(sn, rz, nz);
-        }
-    }
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) {
+                    if (j >= a.nf) return PVV{};   // same-material neighbours only
+                    return PVV{ldg4(a.pos + j), ldg4(a.vel + j), ldg4(a.vadv + j)};
+                },
+                [&](uint32_t j, const PVV &e) {
+                    if (j >= a.nf) return;
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float d2 = dist2(rx, ry, rz);
+                    const float g = cubic_g(d2, a.k);
+                    const float4 vj = pressure_applied(e.v, e.va, a.inv_dt, a.dt);
+                    const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+                    const float pi = a.vis_coef * (vx * rx + vy * ry + vz * rz) / (d2 + a.h2_001);
+                    const float s = 10.f * pi * g;
+                    ax = __fmaf_rn(s, rx, ax);
+                    ay = __fmaf_rn(s, ry, ay);
+                    az = __fmaf_rn(s, rz, az);
+                    if (TENSION_SPLIT) {
+                        const float sn = ncoef * g;
+                        nx = __fmaf_rn(sn, rx, nx);
+                        ny = __fmaf_rn(sn, ry, ny);
+                        nz = __fmaf_rn(sn, rz, nz);
+                    }
+                });
     const float accx = a.gravity.x + ax, accy = a.gravity.y + ay, accz = a.gravity.z + az;
     if (TENSION_SPLIT) {
         a.acc_tmp[r] = make_float4(accx, accy, accz, 0.f);
@@ -261,6 +276,7 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     a.vadv_alt[r] = o;
 }
 
+template <int U>
 __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -274,18 +290,20 @@ __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
     const float c2 = -a.gamma * a.mass_f;
     float tx = 0.f, ty = 0.f, tz = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        if (j >= a.nf) continue;
-        const float4 q = ldg4(a.pos + j);
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float rl = sqrtf(dist2(rx, ry, rz));
-        const float cs = c1 * tension_c(rl, a.k.h, a.csigma, a.h6_64) / rl;
-        const float4 nj = ldg4(a.normal + j);
-        tx += kk * (cs * rx + c2 * (ni.x - nj.x));
-        ty += kk * (cs * ry + c2 * (ni.y - nj.y));
-        tz += kk * (cs * rz + c2 * (ni.z - nj.z));
-    }
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) {
+                    if (j >= a.nf) return PN{};
+                    return PN{ldg4(a.pos + j), ldg4(a.normal + j)};
+                },
+                [&](uint32_t j, const PN &e) {
+                    if (j >= a.nf) return;
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float rl = sqrtf(dist2(rx, ry, rz));
+                    const float cs = c1 * tension_c(rl, a.k.h, a.csigma, a.h6_64) / rl;
+                    tx += kk * (cs * rx + c2 * (ni.x - e.n.x));
+                    ty += kk * (cs * ry + c2 * (ni.y - e.n.y));
+                    tz += kk * (cs * rz + c2 * (ni.z - e.n.z));
+                });
     const float4 acc = a.acc_tmp[r];
     float4 o = vi;
     o.x = __fmaf_rn(acc.x + tx, a.dt, vi.x);
@@ -319,30 +337,38 @@ void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bnc
                         float *rest_density_b) {
     if (a.nb) k_rigid_volume<<<nblk(a.nb, 256), 256, 0, st>>>(a, bncnt, bnbr, rest_density_b);
 }
+#define VTP_UNROLL_DISPATCH(U, ...)          \
+    switch (U) {                                 \
+        case 1: { constexpr int UU = 1; __VA_ARGS__; } break; \
+        case 2: { constexpr int UU = 2; __VA_ARGS__; } break; \
+        case 8: { constexpr int UU = 8; __VA_ARGS__; } break; \
+        default: { constexpr int UU = 4; __VA_ARGS__; } break; \
+    }
+
 void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) k_ratio_alpha<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_ratio_alpha<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void dfsph_solve_begin(cudaStream_t st, SolveState *s) { k_solve_begin<<<1, 32, 0, st>>>(s); }
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
     unsigned nb = nblk(a.nf, block);
     if (nb == 0) nb = 1;
-    if (a.nobj > 1) k_solve_a<true><<<nb, block, 0, st>>>(a);
-    else k_solve_a<false><<<nb, block, 0, st>>>(a);
+    if (a.nobj > 1) VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<true, UU><<<nb, block, 0, st>>>(a))
+    else VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<false, UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) k_solve_b<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
     k_solve_end<<<1, 256, 0, st>>>(c, partials, status);
 }
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) k_viscosity<false><<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_viscosity<false, UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) k_viscosity<true><<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_viscosity<true, UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) k_tension<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_tension<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void dfsph_finalize(cudaStream_t st, const DfsphArgs &a) {
     if (a.nf) k_finalize<<<nblk(a.nf, 256), 256, 0, st>>>(a);

@@ -40,6 +40,7 @@ struct DfsphArgs {
     double *partials;           // [blocks][nobj]
     uint32_t *status;
     uint64_t *tick;             // substep counter, advanced by the finalize pass
+    int unroll;                 // neighbours in flight per thread (1, 2, 4, 8)
 };
 
 struct SolveCtl {

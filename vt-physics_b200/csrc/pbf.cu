@@ -39,6 +39,16 @@ __global__ void __launch_bounds__(256) k_pbf_init_boundary(PbfArgs a, const uint
     a.pos_alt[i] = p;
 }
 
+struct PL {
+    float4 q;
+    float l;
+};
+struct PV2 {
+    float4 q, v;
+    float vol;
+};
+
+template <int U>
 __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -48,18 +58,17 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     float rho = n > 0 ? p.w * a.k.w0 : 0.f;
     float gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = ldg4(a.pos + j);
-        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-        float w, g;
-        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
-        rho = __fmaf_rn(q.w, w, rho);
-        const float ex = g * dx, ey = g * dy, ez = g * dz;
-        gx += ex; gy += ey; gz += ez;
-        const float fx = ex * a.inv_rho0, fy = ey * a.inv_rho0, fz = ez * a.inv_rho0;
-        s2 += fx * fx + fy * fy + fz * fz;
-    }
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pos + j); },
+                [&](uint32_t, const float4 &q) {
+                    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+                    float w, g;
+                    cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+                    rho = __fmaf_rn(q.w, w, rho);
+                    const float ex = g * dx, ey = g * dy, ez = g * dz;
+                    gx += ex; gy += ey; gz += ez;
+                    const float fx = ex * a.inv_rho0, fy = ey * a.inv_rho0, fz = ez * a.inv_rho0;
+                    s2 += fx * fx + fy * fy + fz * fz;
+                });
     if (rho < a.rho0) rho = a.rho0;
     const float err = rho / a.rho0 - 1.f;
     gx /= a.rho0; gy /= a.rho0; gz /= a.rho0;
@@ -68,6 +77,7 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     a.lambda[r] = -err / (s2 + a.eps);
 }
 
+template <int U>
 __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -76,18 +86,17 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     const uint32_t n = a.ncnt[r];
     float dx = 0.f, dy = 0.f, dz = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = ldg4(a.pos + j);
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float g = cubic_g(dist2(rx, ry, rz), a.k);
-        // Boundary lambda is never written by the reference; it is taken as 0.
-        const float lj = j < a.nf ? __ldg(a.lambda + j) : 0.f;
-        const float s = (li + lj) * g;
-        dx = __fmaf_rn(s, rx, dx);
-        dy = __fmaf_rn(s, ry, dy);
-        dz = __fmaf_rn(s, rz, dz);
-    }
+    // Boundary lambda is never written by the reference; it is taken as 0.
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) { return PL{ldg4(a.pos + j), j < a.nf ? __ldg(a.lambda + j) : 0.f}; },
+                [&](uint32_t, const PL &e) {
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float g = cubic_g(dist2(rx, ry, rz), a.k);
+                    const float s = (li + e.l) * g;
+                    dx = __fmaf_rn(s, rx, dx);
+                    dy = __fmaf_rn(s, ry, dy);
+                    dz = __fmaf_rn(s, rz, dz);
+                });
     dx /= a.rho0; dy /= a.rho0; dz /= a.rho0;
     float4 o = p;
     o.x += dx; o.y += dy; o.z += dz;
@@ -97,6 +106,7 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     a.vel[r] = v;
 }
 
+template <int U>
 __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
@@ -105,16 +115,15 @@ __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
     const uint32_t n = a.ncnt[r];
     float ax = 0.f, ay = 0.f, az = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = ldg4(a.pos + j);
-        const float w = cubic_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a.k);
-        const float4 vj = ldg4(a.vel + j);
-        const float c = a.xsph_k * __ldg(a.vol + j);
-        ax = __fmaf_rn(c * (vj.x - vi.x), w, ax);
-        ay = __fmaf_rn(c * (vj.y - vi.y), w, ay);
-        az = __fmaf_rn(c * (vj.z - vi.z), w, az);
-    }
+    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) { return PV2{ldg4(a.pos + j), ldg4(a.vel + j), __ldg(a.vol + j)}; },
+                [&](uint32_t, const PV2 &e) {
+                    const float w = cubic_w(dist2(p.x - e.q.x, p.y - e.q.y, p.z - e.q.z), a.k);
+                    const float c = a.xsph_k * e.vol;
+                    ax = __fmaf_rn(c * (e.v.x - vi.x), w, ax);
+                    ay = __fmaf_rn(c * (e.v.y - vi.y), w, ay);
+                    az = __fmaf_rn(c * (e.v.z - vi.z), w, az);
+                });
     const float dx = ax * a.dt, dy = ay * a.dt, dz = az * a.dt;
     float4 o = p;
     o.x += dx; o.y += dy; o.z += dz;
@@ -132,14 +141,22 @@ void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt,
                        uint32_t ell_stride) {
     if (a.nb) k_pbf_init_boundary<<<nblk(a.nb, 256), 256, 0, st>>>(a, bncnt, bnbr, ell_stride);
 }
+#define VTP_UNROLL_DISPATCH(U, ...)          \
+    switch (U) {                                 \
+        case 1: { constexpr int UU = 1; __VA_ARGS__; } break; \
+        case 2: { constexpr int UU = 2; __VA_ARGS__; } break; \
+        case 8: { constexpr int UU = 8; __VA_ARGS__; } break; \
+        default: { constexpr int UU = 4; __VA_ARGS__; } break; \
+    }
+
 void pbf_lambda(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) k_pbf_lambda<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_lambda<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void pbf_dx(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) k_pbf_dx<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_dx<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 void pbf_xsph(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) k_pbf_xsph<<<nblk(a.nf, block), block, 0, st>>>(a);
+    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_xsph<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
 
 }  // namespace vtp

@@ -19,6 +19,7 @@ struct PbfArgs {
     float *vol;            // [n] volume (fluid V0, boundary 1/sum W)
     float *density;        // [nf]
     float *lambda;         // [nf]
+    int unroll;            // neighbours in flight per thread (1, 2, 4, 8)
 };
 
 void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,

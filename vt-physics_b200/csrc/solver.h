@@ -65,6 +65,7 @@ struct vtp_solver {
     uint64_t *d_tick = nullptr;
     bool device_loop = true, use_graphs = true, stage_timers = false, stop_on_crash = true;
     int block = 128;
+    int unroll = 4;
 
     // device state
     cudaStream_t st = nullptr, side = nullptr;

@@ -199,9 +199,8 @@ struct Walker {
     uint32_t *out;       // ELL base for this row (slot t at out[t*32])
     bool overflow;
 
-    __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
+    __device__ __forceinline__ void accept(uint32_t j, const float4 &q, float d2max) {
         if (j == self) return;
-        float4 q = pos[j];
         float d2 = dist2(px - q.x, py - q.y, pz - q.z);
         if (d2 > 0.f && d2 <= d2max) {
             if (cnt < maxnbr) {
@@ -211,6 +210,25 @@ struct Walker {
                 overflow = true;
             }
         }
+    }
+
+    __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
+        accept(j, __ldg(pos + j), d2max);
+    }
+
+    // Candidates [j0, j1) in order; positions loaded four at a time.
+    __device__ __forceinline__ void visit_run(uint32_t j0, uint32_t j1, const float4 *__restrict__ pos,
+                                              float d2max) {
+        uint32_t j = j0;
+        for (; j + 4 <= j1; j += 4) {
+            const float4 q0 = __ldg(pos + j), q1 = __ldg(pos + j + 1), q2 = __ldg(pos + j + 2),
+                         q3 = __ldg(pos + j + 3);
+            accept(j, q0, d2max);
+            accept(j + 1, q1, d2max);
+            accept(j + 2, q2, d2max);
+            accept(j + 3, q3, d2max);
+        }
+        for (; j < j1; ++j) visit(j, pos, d2max);
     }
 };
 
@@ -246,11 +264,11 @@ __global__ void k_build_lists(Grid g, uint32_t row0, uint32_t cnt, uint32_t ell_
         uint32_t f0 = __ldg(fstart + k), f1 = __ldg(fstart + k + 1);
         uint32_t b0 = __ldg(bstart + k), b1 = __ldg(bstart + k + 1);
         if (MODE == 0) {
-            for (uint32_t j = f0; j < f1; ++j) w.visit(j, pos, d2max);
-            for (uint32_t j = b0; j < b1; ++j) w.visit(j, pos, d2max);
+            w.visit_run(f0, f1, pos, d2max);
+            w.visit_run(b0, b1, pos, d2max);
         } else if (MODE == 1) {
-            for (uint32_t j = b0; j < b1; ++j) w.visit(j, pos, d2max);
-            for (uint32_t j = f0; j < f1; ++j) w.visit(j, pos, d2max);
+            w.visit_run(b0, b1, pos, d2max);
+            w.visit_run(f0, f1, pos, d2max);
         } else {
             // Merge the two id-sorted runs by attach id.
             while (f0 < f1 || b0 < b1) {

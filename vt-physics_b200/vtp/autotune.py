@@ -1,0 +1,57 @@
+"""Launch-configuration autotuner for the neighbour passes.
+
+Sweeps threads per block and the neighbour-loop unroll (neighbours kept in
+flight per thread) on a scene, timing each candidate with the per-kernel
+CUDA-event profiler of the library, and returns the fastest configuration
+for the solver's substep.  Results are plain dicts so callers can cache them
+(``"B200": {"blockSize": b, "unroll": u}`` in the solver config).
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import time
+
+from .solver import solver_from_scene
+
+BLOCKS = (64, 128, 256)
+UNROLLS = (1, 2, 4, 8)
+
+
+def tune(scene, warmup: int = 3, steps: int = 3, blocks=BLOCKS, unrolls=UNROLLS, verbose: bool = False) -> dict:
+    """Return {"best": {...}, "trials": [...]} for one scene."""
+    trials = []
+    for b, u in itertools.product(blocks, unrolls):
+        s = solver_from_scene(scene, extra={"blockSize": b, "unroll": u})
+        s.initialize()
+        if warmup:
+            s.tickNsteps(warmup)
+        prof = s.profile_kernels(steps)
+        s.destroy()
+        total = sum(v[0] for v in prof.values())
+        rec = {"blockSize": b, "unroll": u, "ms_per_step": total / steps,
+               "kernels": {k: v[0] / max(v[1], 1) for k, v in prof.items()}}
+        trials.append(rec)
+        if verbose:
+            print(json.dumps({k: rec[k] for k in ("blockSize", "unroll", "ms_per_step")}), flush=True)
+    best = min(trials, key=lambda r: r["ms_per_step"])
+    return {"best": {"blockSize": best["blockSize"], "unroll": best["unroll"]}, "trials": trials,
+            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+if __name__ == "__main__":
+    import argparse
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    from vtp import scenes
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scene", default="dfsph_1m", choices=["dfsph_1m", "pbf"])
+    a = ap.parse_args()
+    sc = scenes.dfsph_1m() if a.scene == "dfsph_1m" else scenes.pbf_dam_break()
+    res = tune(sc, verbose=True)
+    print(json.dumps({"best": res["best"], "trials": [{k: t[k] for k in t if k != "kernels"} for t in res["trials"]]}))
+    for t in res["trials"]:
+        print(t["blockSize"], t["unroll"], json.dumps({k: round(v, 4) for k, v in sorted(t["kernels"].items())}))
