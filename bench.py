@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["dfsph_1m", "pbf"], default="dfsph_1m")
+    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k"], default="dfsph_1m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile-steps", type=int, default=3)
@@ -49,7 +49,7 @@ def parse():
 
 def make_scene(workload):
     from vtp import scenes
-    return scenes.dfsph_1m() if workload == "dfsph_1m" else scenes.pbf_dam_break()
+    return {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k}[workload]()
 
 
 class Clocks:
@@ -151,8 +151,8 @@ def run_reference(args) -> dict:
     clocks = clk.stop()
     nf = sc.n_fluid
     value = nf * args.steps / (ms / 1e3) / 1e6
-    # e2e: host positions / velocities in, positions out, one tick per step.
-    fm = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    # e2e: the state round-trips through host memory every step (positions and
+    # velocities in, one tick, positions and velocities out).
     pos = s.get("pos", 3)
     vel = s.get("vel", 3)
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
@@ -162,6 +162,7 @@ def run_reference(args) -> dict:
         s.set("vel", vel)
         s.tick(1)
         pos = s.get("pos", 3)
+        vel = s.get("vel", 3)
     el = time.perf_counter() - t0
     out.update({"value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -171,7 +172,7 @@ def run_reference(args) -> dict:
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
                                  "sample": "the reference is GPU code: its own CUDA build timed on this B200"},
                 "e2e": {"value": nf * e2e_steps / el / 1e6, "unit": METRIC,
-                        "h2d_bytes_per_step": int(2 * 12 * s.n), "d2h_bytes_per_step": int(12 * s.n)}})
+                        "h2d_bytes_per_step": int(2 * 12 * s.n), "d2h_bytes_per_step": int(2 * 12 * s.n)}})
     return out
 
 
@@ -250,17 +251,17 @@ def main():
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_launches) = dom
     per_launch_ms = dom_ms / max(dom_launches, 1)
-    b = kernel_bytes(sc.solver, dom_name, N, nf, K, k_mean)
+    P = len(req.get("phaseRestDensity", [])) or 1
+    b = kernel_bytes(sc.solver, dom_name, N, nf, K, k_mean, P)
     peak, peak_kind = peaks()
     achieved = b["state"] / (per_launch_ms / 1e3) / 1e9
     kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
-    # e2e through the public API with host buffers (pinned), H2D of inputs and D2H of the result per step.
-    n_all = s.counts()["total"]
+    # e2e through the public API: the state round-trips through pinned host memory
+    # every step (H2D of positions and velocities, one substep, D2H of both).
     pos_h = torch.from_numpy(s.get_field("pos")).pin_memory()
     vel_h = torch.from_numpy(s.get_field("vel")).pin_memory()
-    out_h = torch.empty((n_all, 3), dtype=torch.float32).pin_memory()
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
     torch.cuda.synchronize()
     if dist:
@@ -270,7 +271,8 @@ def main():
         s.set_field_ptr("pos", pos_h.data_ptr(), pos_h.numel() * 4)
         s.set_field_ptr("vel", vel_h.data_ptr(), vel_h.numel() * 4)
         assert s.tickNsteps(1), s.last_error
-        s.get_field_ptr("pos", out_h.data_ptr(), out_h.numel() * 4)
+        s.get_field_ptr("pos", pos_h.data_ptr(), pos_h.numel() * 4)
+        s.get_field_ptr("vel", vel_h.data_ptr(), vel_h.numel() * 4)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
@@ -296,7 +298,7 @@ def main():
                      "ms_per_launch": per_launch_ms},
         "kernels": kernels,
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4),
-                "d2h_bytes_per_step": int(out_h.numel() * 4)},
+                "d2h_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc, args.cpu_seconds)

@@ -48,6 +48,10 @@ def scene_for(case: str):
         return scenes.dam_break("DFSPH", 8000, seed=22)
     if case.startswith("dfsph_1m"):
         return scenes.dfsph_1m()
+    if case == "immct_small":
+        return scenes.layered_mixture("IMMCT", 24, seed=31)
+    if case == "imm_small":
+        return scenes.layered_mixture("IMM", 24, seed=32)
     raise KeyError(case)
 
 
@@ -58,6 +62,8 @@ CASES = {
     "dfsph_small": ([0, 1, 2, 3, 10], True),
     "dfsph_small_tension": ([0, 1, 2, 3], False),
     "dfsph_1m_ugns": ([0], False),
+    "immct_small": ([0, 1, 2, 5], False),
+    "imm_small": ([0, 1, 2, 5], False),
 }
 
 
@@ -79,7 +85,7 @@ def run_case(case: str, out_dir: Path):
         while done < t:
             ok = s.tick(1)
             done += 1
-            if sc.solver == "DFSPH":
+            if sc.solver != "PBF":
                 means = s.take_means()
                 d, i, _ = R.split_iterations(means, nfo, req["divFreeThreshold"], req["incompThreshold"])
                 iters.append((d, i))
@@ -110,8 +116,14 @@ def run_case(case: str, out_dir: Path):
                     arrays["mass_0"] = s.get("mass")
         if sc.solver == "PBF" and t > 0:
             arrays[f"density_{t}"] = s.get("density_sph")[fm]
-        if sc.solver == "DFSPH" and t > 0 and case != "dfsph_1m_ugns":
+        if sc.solver != "PBF" and t > 0 and case != "dfsph_1m_ugns":
             arrays[f"ratio_{t}"] = s.get("compression_ratio")[fm]
+        if sc.solver in ("IMM", "IMMCT") and t > 0:
+            P = len(req["phaseRestDensity"])
+            arrays[f"frac_{t}"] = s.get("vol_frac", P)[fm]
+            if sc.solver == "IMMCT":
+                arrays[f"Q_{t}"] = s.get("Q", 9)[fm]
+                arrays[f"cd_{t}"] = s.get("Cd")[fm]
     if iters:
         arrays["iters"] = np.array(iters, np.int32)
     rec["ticks"] = ticks

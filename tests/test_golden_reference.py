@@ -21,6 +21,7 @@ from util import fluid_mask, rel_err
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = ["pbf_small", "pbf_full", "dfsph_small", "dfsph_small_tension"]
+MIX_CASES = ["immct_small", "imm_small"]
 TOL = 1e-5
 
 
@@ -105,7 +106,7 @@ def test_oracle_trajectory_close_to_reference(oracle_lib, case):
 # ---------------------------------------------------------------- GPU: library vs the reference
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", CASES + MIX_CASES)
 def test_library_neighbor_search_matches_reference(vtp_gpu, case):
     g, meta = load(case)
     sc = scene(case)
@@ -150,4 +151,43 @@ def test_library_substeps_match_reference(vtp_gpu, case):
             assert ep < TOL and ev < TOL
         else:  # later substeps: both FP32 runs drift apart at the rate each drifts from FP64
             assert ep < TOL * t and ev < 2e-5 * t
+    s.destroy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", MIX_CASES)
+def test_mixture_substeps_match_reference(vtp_gpu, case):
+    """IMM / IMM-CT: positions, velocities, volume fractions (and Q) against the reference."""
+    g, meta = load(case)
+    sc = scene(case)
+    fm = fluid_mask(sc)
+    s = vtp_gpu.solver_from_scene(sc, extra={"forceIterationsPerTick": g["iters"].tolist()})
+    done = 0
+    for t in meta["ticks"]:
+        if t == 0:
+            continue
+        assert s.tickNsteps(t - done)
+        done = t
+        ep = rel_err(s.get_field("pos")[fm], g[f"pos_{t}"])
+        ev = rel_err(s.get_field("vel")[fm], g[f"vel_{t}"], vel_floor(sc))
+        ef = rel_err(s.get_field("vol_frac")[fm], g[f"frac_{t}"])
+        msg = f"{case} t={t}: library vs reference: pos {ep:.2e} vel {ev:.2e} frac {ef:.2e}"
+        eq = ec = 0.0
+        if f"Q_{t}" in g.files:
+            eq = rel_err(s.get_field("conformation")[fm], g[f"Q_{t}"])
+            ec = rel_err(s.get_field("cd")[fm], g[f"cd_{t}"])
+            msg += f" Q {eq:.2e} Cd {ec:.2e}"
+        # trajectory statistics: kinetic energy and per-phase volumes
+        vel = s.get_field("vel")[fm].astype(np.float64)
+        frac = s.get_field("vol_frac")[fm].astype(np.float64)
+        ke, ke_ref = np.sum(vel ** 2), np.sum(g[f"vel_{t}"].astype(np.float64) ** 2)
+        ph, ph_ref = frac.sum(0), g[f"frac_{t}"].astype(np.float64).sum(0)
+        eke = abs(ke - ke_ref) / ke_ref
+        eph = float(np.max(np.abs(ph - ph_ref) / ph_ref.sum()))
+        msg += f"; kinetic energy {eke:.2e} phase volume {eph:.2e}"
+        print(msg)
+        if t == 1:  # one substep: per-particle bar
+            assert ep < TOL and ev < TOL and ef < TOL and eq < TOL and ec < TOL
+        else:       # later substeps: trajectory statistics
+            assert eke < 1e-3 and eph < 1e-5
     s.destroy()

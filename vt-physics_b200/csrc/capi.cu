@@ -162,7 +162,7 @@ int vtp_solver::parse_config(const json &c) {
         } else {
             int rc = immct_parse(type == VTP_SOLVER_IMMCT, r, imm);
             if (rc) return rc;
-            rho_b = r["bPartRestDensity"].get<float>();
+            rho_b = 0.f;   // IMM / IMM-CT boundaries carry volume only
             div_thr = r["divFreeThreshold"].get<float>();
             incomp_thr = r["incompThreshold"].get<float>();
             gamma = r["surfaceTensionCoefficient"].get<float>();
@@ -205,7 +205,10 @@ int vtp_solver::attach(const float *p, uint32_t n, const float *v, const json &o
     if (!occ.contains("epmMaterial")) return fail(VTP_ERR_CONFIG, "object has no epmMaterial");
     int mat = occ["epmMaterial"].get<int>();
     if (mat != 0 && mat != 1) return fail(VTP_ERR_CONFIG, std::string(solver_key(type)) + "Solver unsupported material.");
-    for (auto &k : kObjRequired)
+    const bool mix = type == VTP_SOLVER_IMM || type == VTP_SOLVER_IMMCT;
+    static const std::vector<std::string> kMixObjRequired = {"solverType", "exportFlag", "velocityStart",
+                                                             "phaseFraction"};
+    for (auto &k : (mix ? kMixObjRequired : kObjRequired))
         if (!socc.contains(k))
             return fail(VTP_ERR_CONFIG, "Object has no " + std::string(solver_key(type)) + " object component config key: " + k);
     if (socc["solverType"].get<int>() != type)
@@ -217,14 +220,15 @@ int vtp_solver::attach(const float *p, uint32_t n, const float *v, const json &o
     rec.start = (uint32_t)(hpos.size() / 3);
     rec.export_flag = socc["exportFlag"].get<bool>();
     auto v0 = socc["velocityStart"].get<std::vector<float>>();
-    auto c0 = socc["colorStart"].get<std::vector<float>>();
+    auto c0 = socc.value("colorStart", std::vector<float>{0.f, 0.f, 0.f});
     for (int a = 0; a < 3; ++a) {
         rec.vel0[a] = a < (int)v0.size() ? v0[a] : 0.f;
         rec.color[a] = a < (int)c0.size() ? c0[a] : 0.f;
     }
-    if (type == VTP_SOLVER_IMM || type == VTP_SOLVER_IMMCT) {
-        if (!socc.contains("phaseFraction")) return fail(VTP_ERR_CONFIG, "Object has no phaseFraction");
+    if (mix) {
         rec.phase = socc["phaseFraction"].get<std::vector<float>>();
+        if (!imm || (int)rec.phase.size() != immct_phase_count(*this))
+            return fail(VTP_ERR_CONFIG, "Object phaseFraction size not match with solver.");
     }
     hpos.insert(hpos.end(), p, p + 3 * (size_t)n);
     for (uint32_t i = 0; i < n; ++i)
@@ -626,6 +630,7 @@ int vtp_solver::build_graphs() {
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(VTP_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
     }
+    if (imm) immct_set_parity(*this, orig.cur);
     if (pos.cur != start_state[0] || vel.cur != start_state[1] || orig.cur != start_state[2] ||
         vadv.cur != start_state[3])
         return fail(VTP_ERR_STATE, "substep buffer parity does not repeat after two substeps");
@@ -687,6 +692,7 @@ int vtp_solver::tick_n(uint32_t n) {
             CU(cudaGraphLaunch(gexec[parity], st));
             int np = parity ^ 1;
             pos.cur = gstate[np][0]; vel.cur = gstate[np][1]; orig.cur = gstate[np][2]; vadv.cur = gstate[np][3];
+            if (imm) immct_set_parity(*this, orig.cur);
             parity = np;
         } else {
             launches_per_tick = 0;
@@ -725,6 +731,7 @@ int vtp_solver::tick_n(uint32_t n) {
         launches = (uint64_t)n * launches_per_tick;
     }
     last_launches = launches;
+    if (imm) stats.phase_retries = immct_last_retries(*this);
     stats.steps_done = steps_done;
     stats.sim_time = sim_time;
     return VTP_OK;
@@ -737,10 +744,11 @@ static size_t field_elems(const vtp_solver &s, int f) {
         case VTP_FIELD_POS: case VTP_FIELD_VEL: case VTP_FIELD_COLOR: return 3;
         case VTP_FIELD_MAT: case VTP_FIELD_MASS: case VTP_FIELD_VOLUME: case VTP_FIELD_DENSITY:
         case VTP_FIELD_LAMBDA: case VTP_FIELD_ALPHA: case VTP_FIELD_KAPPA: case VTP_FIELD_REST_DENSITY:
-        case VTP_FIELD_CD: case VTP_FIELD_DELTA: return 1;
+        case VTP_FIELD_DELTA: return 1;
+        case VTP_FIELD_CD: return s.imm ? 1 : 0;
         case VTP_FIELD_VOL_FRAC: return s.imm ? immct_phase_count(s) : 0;
         case VTP_FIELD_PHASE_VEL: return s.imm ? 3 * immct_phase_count(s) : 0;
-        case VTP_FIELD_CONFORMATION: case VTP_FIELD_VEL_GRAD: case VTP_FIELD_STRESS: return s.imm ? 9 : 0;
+        case VTP_FIELD_CONFORMATION: case VTP_FIELD_STRESS: return s.imm ? 9 : 0;
     }
     return 0;
 }
@@ -751,7 +759,28 @@ int vtp_solver::get_field(int f, void *host, size_t bytes) {
     if (ne == 0) return fail(VTP_ERR_ARG, "field not available for this solver");
     if (!host || bytes != (size_t)L.n * ne * 4) return fail(VTP_ERR_ARG, "wrong byte count for field");
     const uint32_t n = L.n;
-    if (f == VTP_FIELD_COLOR) { memcpy(host, hcolor.data(), bytes); return VTP_OK; }
+    if (f == VTP_FIELD_COLOR) {
+        if (imm) {
+            // color = sum_k alpha_k phaseRestColor_k (update_color_cuda, IMMCTCudaImpl.cu:512-524)
+            const int P = immct_phase_count(*this);
+            std::vector<float> fr((size_t)L.n * P);
+            int rc = get_field(VTP_FIELD_VOL_FRAC, fr.data(), fr.size() * 4);
+            if (rc) return rc;
+            immct_color(*this, fr.data(), (float *)host);
+            return VTP_OK;
+        }
+        memcpy(host, hcolor.data(), bytes);
+        return VTP_OK;
+    }
+    if (imm && (f == VTP_FIELD_MASS || f == VTP_FIELD_REST_DENSITY || f == VTP_FIELD_CD ||
+                f == VTP_FIELD_VOL_FRAC || f == VTP_FIELD_PHASE_VEL || f == VTP_FIELD_CONFORMATION ||
+                f == VTP_FIELD_STRESS)) {
+        int rc = ensure_stage(bytes);
+        if (rc) return rc;
+        if ((rc = immct_get_field(*this, f, stage, ne))) return rc;
+        cudaError_t e = cudaMemcpy(host, stage, bytes, cudaMemcpyDeviceToHost);
+        return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    }
     if (f == VTP_FIELD_MAT) { memcpy(host, hmat.data(), bytes); return VTP_OK; }
     int rc = ensure_stage(bytes);
     if (rc) return rc;
@@ -799,7 +828,7 @@ int vtp_solver::get_field(int f, void *host, size_t bytes) {
                     else if (f == VTP_FIELD_MASS) v = fl ? rho_f * vol0 : 0.f;
                     else v = fl ? rho_f : rb[r - L.nf];
                 } else {
-                    v = immct_scalar_host(*this, f, r, p4[r].w, fl ? 0.f : rb[r - L.nf]);
+                    v = p4[r].w;   // IMM / IMM-CT volume (mass and rest density handled above)
                 }
                 out[ids[r]] = v;
             }
@@ -1002,6 +1031,7 @@ int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, ui
         carry.src4[0] = s->vadv.c();
         carry.dst4[0] = s->vadv.n();
     }
+    if (s->imm) immct_fill_carry(*s, carry);
     vtp::ugns_sort(s->st, s->grid, 0, s->L.nf, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(), s->orig.c(),
                    s->orig.n(), carry, 0.f, make_float3(0, 0, 0), s->u, s->u.fstart);
     // Copy the re-sorted fluid rows back so the buffer parity the substep graphs expect is kept.
@@ -1011,6 +1041,10 @@ int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, ui
     CU(cudaMemcpyAsync(s->orig.c(), s->orig.n(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s->st));
     if (s->vadv.c())
         CU(cudaMemcpyAsync(s->vadv.c(), s->vadv.n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    if (s->imm) {
+        int rc = immct_copy_back(*s);
+        if (rc) return rc;
+    }
     vtp::ugns_build_lists(s->st, s->grid, s->L, 0, s->L.nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
                           s->d_status, s->d_overflow, s->block);
     vtp::ugns_build_lists(s->st, s->grid, s->L, s->L.nf, s->L.nb, s->pos.c(), s->orig.c(), s->u, s->u.bnbr,

@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     float4 v = a.vadv[r];
     const float ki = a.kappa[r];
     const uint32_t n = a.ncnt[r];
-    const float ci = a.dt * p.w / a.mass_f;   // dt V_i / m_i
+    const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
+    const float ci = a.dt * p.w / mi;   // dt V_i / m_i
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,

@@ -41,6 +41,7 @@ struct DfsphArgs {
     uint32_t *status;
     uint64_t *tick;             // substep counter, advanced by the finalize pass
     int unroll;                 // neighbours in flight per thread (1, 2, 4, 8)
+    const float *rest_density;  // IMM / IMM-CT: per-row rest density (mass = rest_density * volume)
 };
 
 struct SolveCtl {

@@ -23,5 +23,9 @@ int immct_init(vtp_solver &s);
 int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture);
 void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which);
 int immct_phase_count(const vtp_solver &s);
-float immct_scalar_host(vtp_solver &s, int field, uint32_t row, float w, float boundary_value);
 int immct_get_field(vtp_solver &s, int field, float *dev_out, size_t elems);
+void immct_fill_carry(vtp_solver &s, vtp::Carry &carry);
+int immct_copy_back(vtp_solver &s);
+void immct_set_parity(vtp_solver &s, int cur);
+uint32_t immct_last_retries(vtp_solver &s);
+void immct_color(vtp_solver &s, const float *frac_attach_order, float *rgb);

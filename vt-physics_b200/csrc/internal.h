@@ -37,7 +37,7 @@ struct UgnsBuffers {
 
 // Fields a reorder carries from old slot to new slot (float4 / float / uint).
 struct Carry {
-    static constexpr int kMaxF4 = 8, kMaxF1 = 8;
+    static constexpr int kMaxF4 = 8, kMaxF1 = 16;
     int nf4 = 0, nf1 = 0;
     const float4 *src4[kMaxF4];
     float4 *dst4[kMaxF4];

@@ -1,7 +1,7 @@
 """Algorithmic bytes per kernel launch (state arrays touched once; FP32, float4 = 16 B).
 
 N = all rows (fluid + boundary), Nf = fluid rows, K = number of grid key
-buckets, k = mean neighbours per fluid row (self excluded).  "state" bytes
+buckets, k = mean neighbours per fluid row (self excluded), P = phases.  "state" bytes
 follow the per-pass accounting of the project's bytes model; "list" adds the
 neighbour-list indices (4 B per stored neighbour), which the list-based
 design reads on top.
@@ -9,7 +9,7 @@ design reads on top.
 from __future__ import annotations
 
 
-def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float) -> dict:
+def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float, P: int = 2) -> dict:
     lst = 4.0 * k * Nf
     if name == "ugns_clear_hash":
         state = 4 * (K + 1) + 16 * Nf + 8 * Nf + (16 * Nf if kind == "PBF" else 0)
@@ -43,6 +43,22 @@ def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float) -> dic
         state, lst = 96 * Nf, 0
     elif name == "dfsph_solve_end":
         state, lst = 8 * ((Nf + 127) // 128), 0
+    elif name == "imm_precompute":          # pos, rest density, fraction of phase 1 gathered; 3 outputs
+        state = 16 * N + 8 * Nf + 12 * Nf
+    elif name in ("imm_vis", "imm_vis_normal"):
+        state = 32 * N + (16 * P + 8) * Nf + 16 * P * Nf + 32 * Nf
+    elif name == "imm_tension":
+        state = 36 * N + 16 * P * Nf + 32 * Nf
+    elif name == "immct_ct":                # pos, vel, rest density gathered; Q read+write, tau written
+        state = 36 * N + 16 * Nf + 72 * Nf + 36 * Nf
+    elif name == "immct_pct":               # pos, rest density, tau gathered; phase velocities updated
+        state = 56 * N + 32 * P * Nf + 32 * Nf
+    elif name == "imm_drift_diffuse":       # pos, vel, flag, fractions, phase velocities gathered
+        state = (36 + 20 * P) * N + 8 * P * Nf
+    elif name == "imm_apply_pressure":
+        state = 32 * P * Nf + 4 * P * Nf + 72 * Nf
+    elif name == "imm_phase_finish":
+        state = 12 * P * Nf + 32 * P * Nf + 48 * Nf
     else:
         state, lst = 0, 0
     return {"state": float(state), "list": float(lst), "total": float(state + lst)}

@@ -206,6 +206,88 @@ def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, j
                                SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def immct_config(*, dt, r, lb, size, rho=(1000.0, 1200.0), cf=1e-3, cd0=0.5, solvent_vis=0.01, vis_base=12.0,
+                 vis_max=12.0, relax=0.05, thin=0.6, theta=0.4, div_thr=1e-4, incomp_thr=1e-4, tension=0.001,
+                 colors=((255, 0, 0), (0, 0, 255)), gravity=(0.0, -9.81, 0.0), max_nbr=60, animation_time=5.0):
+    return {"IMMCT": {"Required": {"animationTime": animation_time, "timeStep": dt, "particleRadius": r,
+                                   "simSpaceLB": list(lb), "simSpaceSize": list(size), "maxNeighborNum": max_nbr,
+                                   "divFreeThreshold": div_thr, "incompThreshold": incomp_thr,
+                                   "surfaceTensionCoefficient": tension, "diffusionCoefficientCf": cf,
+                                   "momentumExchangeCoefficientCd0": cd0, "solventViscosity": solvent_vis,
+                                   "phaseRestDensity": list(rho), "phaseRestColor": [list(c) for c in colors],
+                                   "solutionBasicViscosity": vis_base, "solutionMaxViscosity": vis_max,
+                                   "relaxationTime": relax, "shearThinningBasicFactor": thin,
+                                   "rheologicalThreshold": theta},
+                      "Optional": {"enable": True, "gravity": list(gravity)}},
+            "EXPORT": _export_block()}
+
+
+def imm_config(*, dt, r, lb, size, rho=(1000.0, 1000.0, 1000.0), vis=(0.01, 0.01, 0.01), cf=0.1, cd=0.5,
+               div_thr=1e-4, incomp_thr=1e-4, tension=0.001, colors=((255, 0, 0), (0, 255, 0), (0, 0, 255)),
+               gravity=(0.0, -9.81, 0.0), max_nbr=60, animation_time=5.0):
+    return {"IMM": {"Required": {"animationTime": animation_time, "timeStep": dt, "particleRadius": r,
+                                 "simSpaceLB": list(lb), "simSpaceSize": list(size), "maxNeighborNum": max_nbr,
+                                 "divFreeThreshold": div_thr, "incompThreshold": incomp_thr,
+                                 "surfaceTensionCoefficient": tension, "diffusionCoefficientCf": cf,
+                                 "momentumExchangeCoefficientCd": cd, "phaseRestDensity": list(rho),
+                                 "phaseRestViscosity": list(vis), "phaseRestColor": [list(c) for c in colors]},
+                    "Optional": {"enable": True, "gravity": list(gravity)}},
+            "EXPORT": _export_block()}
+
+
+def immct_500k(seed: int = 3003, jitter_amp: float = 0.05) -> Scene:
+    """IMM-CT: two stacked 100 x 25 x 100 layers at spacing 0.01 (phase 1 below, phase 0 on top).
+
+    Phase 1 (rho 1200) is the viscoelastic phase (the conformation-tensor terms read
+    fraction index 1); relaxation time 0.05 s, thinning factor 0.6, Cf 1e-3,
+    dt 0.5 ms.  Walls: 3-layer box 1.06 x 0.8 x 1.06.  Solver thresholds are 0.1 %.
+    Solution viscosities are 8e-5 / 1.2e-4 (the example's 8 : 12 ratio): the
+    reference's stress-divergence sum (add_phase_pct_acc_cuda) carries no neighbour
+    volume, so its strength grows as 1 / V_j; at spacing 0.01 the template values
+    (12) make the reference's own run explode within one substep.
+    """
+    r = 0.005
+    bottom = cube(r, (0.03, 0.03, 0.03), (1.0, 0.25, 1.0))
+    top = cube(r, (0.03, 0.28, 0.03), (1.0, 0.25, 1.0))
+    both = jitter(np.concatenate([bottom, top]), jitter_amp, 2 * r, seed)
+    wall = box(r, (0.0, 0.0, 0.0), (1.06, 0.8, 1.06), 3)
+    cfg = immct_config(dt=5e-4, r=r, lb=(-0.05, -0.05, -0.05), size=(1.16, 0.9, 1.16), div_thr=1e-3,
+                       incomp_thr=1e-3, vis_base=8e-5, vis_max=1.2e-4)
+    nb = bottom.shape[0]
+    return Scene("IMMCT", cfg, [
+        SceneObject("bottom", both[:nb], EPM_FLUID, export_flag=True, phase_fraction=(0.0, 1.0)),
+        SceneObject("top", both[nb:], EPM_FLUID, export_flag=True, phase_fraction=(1.0, 0.0)),
+        SceneObject("box", wall, EPM_BOUNDARY, phase_fraction=(0.0, 1.0))])
+
+
+def layered_mixture(solver: str, n_side: int, seed: int, jitter_amp: float = 0.05) -> Scene:
+    """Small stratified mixture: two fluid layers of n x n/4 x n at spacing 0.01 in a 3-layer box."""
+    r = 0.005
+    sp = 2 * r
+    off = 4 * sp
+    hl = max(1, n_side // 4) * sp
+    w = n_side * sp
+    bottom = cube(r, (off, off, off), (w, hl, w))
+    top = cube(r, (off, off + hl, off), (w, hl, w))
+    both = jitter(np.concatenate([bottom, top]), jitter_amp, sp, seed)
+    side = w + 2 * off
+    height = 2 * hl + 2 * off + 0.1
+    wall = box(r, (0.0, 0.0, 0.0), (side, height, side), 3)
+    lb = (-0.05, -0.05, -0.05)
+    size = (side + 0.1, height + 0.1, side + 0.1)
+    nb = bottom.shape[0]
+    if solver == "IMMCT":
+        cfg = immct_config(dt=5e-4, r=r, lb=lb, size=size, vis_base=8e-5, vis_max=1.2e-4)
+        fr_b, fr_t, fr_w = (0.0, 1.0), (1.0, 0.0), (0.0, 1.0)
+    else:
+        cfg = imm_config(dt=5e-4, r=r, lb=lb, size=size, rho=(1000.0, 1100.0, 1200.0), vis=(0.01, 0.02, 0.03))
+        fr_b, fr_t, fr_w = (0.0, 0.3, 0.7), (0.6, 0.4, 0.0), (0.0, 0.0, 1.0)
+    return Scene(solver, cfg, [
+        SceneObject("bottom", both[:nb], EPM_FLUID, export_flag=True, phase_fraction=fr_b),
+        SceneObject("top", both[nb:], EPM_FLUID, export_flag=True, phase_fraction=fr_t),
+        SceneObject("box", wall, EPM_BOUNDARY, phase_fraction=fr_w)])
+
+
 def grid_dims(cfg_block: dict, h: float):
     """Grid dimensions as ``UniformGirdNeighborSearcher::setConfig`` computes them (ceil(size / h))."""
     size = cfg_block["Required"]["simSpaceSize"]
