@@ -197,6 +197,34 @@ VTP_API int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_tim
  * tick_n_steps call. */
 VTP_API int vtp_solver_get_launch_count(vtp_solver *s, uint64_t *launches);
 
+/* Allocation-free neighbour search (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc when they need neighbour lists:
+ * code recording a CUDA graph by stream capture, hosts that give this
+ * library a fixed memory budget managed by their own allocator, real-time
+ * loops that forbid allocation after start-up.  Inputs and outputs are the
+ * caller's device buffers: d_pos (n x float[3], any order), d_counts[n] and
+ * d_nbrs[n * max_nbr] in the layout of vtp_solver_get_neighbors (self first,
+ * then the 27 cells in the reference's order, ascending index inside a cell,
+ * UINT32_MAX padded; count 0 for particles outside the grid).  The grid is
+ * the reference's: cell size `cell`, lower corner lb, ceil(size / cell)
+ * cells per axis.  All scratch lives in a fixed array inside the library
+ * (VTP_NOALLOC_SCRATCH_BYTES on every GPU that loads it, held until exit),
+ * which limits n to VTP_NOALLOC_MAX_PARTICLES and the grid to
+ * VTP_NOALLOC_MAX_CELLS cell buckets; larger inputs return VTP_ERR_BOUNDS.
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
+ * and the call returns without waiting.  The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture.  Every call on a device shares the array, so calls whose GPU work
+ * overlaps (other streams, unsynchronised threads) race: order them on one
+ * stream. */
+#define VTP_NOALLOC_MAX_PARTICLES 1048576u
+#define VTP_NOALLOC_MAX_CELLS 2097152u
+#define VTP_NOALLOC_SCRATCH_BYTES 50336512ull
+VTP_API int vtp_ugns_neighbors_noalloc(const float *d_pos, uint32_t n, const float lb[3], const float size[3],
+                                       float cell, uint32_t max_nbr, uint32_t *d_counts, uint32_t *d_nbrs,
+                                       void *stream);
+
 #ifdef __cplusplus
 }
 #endif
