@@ -1,0 +1,117 @@
+"""C ABI on the CPU: the library loads, exports every declared entry point, and
+validates configs / objects the way the reference's setConfig / attachObject do.
+No call here touches a GPU."""
+import ctypes as C
+import json
+import re
+from pathlib import Path
+
+import pytest
+
+import vtp
+from vtp import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "vtp.h"
+
+
+def declared_symbols():
+    txt = HEADER.read_text()
+    return sorted(set(re.findall(r"VTP_API\s+[^;(]*?\b(vtp_\w+)\s*\(", txt)))
+
+
+def test_header_declarations_are_all_exported():
+    lib = vtp.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} missing from the ctypes binding"
+
+
+def test_status_strings_and_version():
+    lib = vtp.lib()
+    assert lib.vtp_version().startswith(b"vtp")
+    assert lib.vtp_status_string(0) == b"ok"
+    assert b"100 iterations" in lib.vtp_status_string(3)
+
+
+def _cfg(kind):
+    return vtp.solver.Solver.__new__(vtp.solver._CLASSES[kind]).__class__
+
+
+@pytest.mark.parametrize("kind", [vtp.PBF, vtp.DFSPH, vtp.IMM, vtp.IMMCT])
+def test_templates_round_trip_through_set_config(kind):
+    s = vtp.SolverManager().createSolver(kind)
+    tpl = s.getSolverConfigTemplate()
+    assert s.setConfig(tpl), s.last_error
+    s.destroy()
+
+
+def test_missing_required_key_is_rejected_like_the_reference():
+    s = vtp.PBFSolver()
+    cfg = vtp.scenes.pbf_dam_break().config
+    del cfg["PBF"]["Required"]["XSPH_k"]
+    assert not s.setConfig(cfg)
+    assert "missing Required key: XSPH_k" in s.last_error
+    cfg2 = vtp.scenes.pbf_dam_break().config
+    del cfg2["PBF"]["Optional"]["gravity"]
+    assert not s.setConfig(cfg2)
+    assert not s.setConfig({})
+    s.destroy()
+
+
+def test_object_checks_follow_attach_object():
+    s = vtp.DFSPHSolver()
+    assert s.setConfig(vtp.scenes.dfsph_config(dt=1e-3, r=0.005, lb=(0, 0, 0), size=(1, 1, 1)))
+    o = vtp.Object(vtp.Particle_Common)
+    o.pos = vtp.scenes.cube(0.005, (0.1, 0.1, 0.1), (0.05, 0.05, 0.05))
+    o.getObjectComponentConfig()["epmMaterial"] = 0
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 0, "exportFlag": False,
+                                                 "velocityStart": [0, 0, 0], "colorStart": [0, 0, 0]})
+    assert not s.attachObject(o)                     # solverType of another solver
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 1, "exportFlag": False,
+                                                 "velocityStart": [0, 0, 0]})
+    assert not s.attachObject(o)                     # colorStart missing
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 1, "exportFlag": False,
+                                                 "velocityStart": [0, 0, 0], "colorStart": [0, 0, 0]})
+    o.getObjectComponentConfig()["epmMaterial"] = 7
+    assert not s.attachObject(o)                     # unsupported material
+    o.getObjectComponentConfig()["epmMaterial"] = 0
+    assert s.attachObject(o), s.last_error
+    assert s.counts() == {"total": o.pos.shape[0], "fluid": o.pos.shape[0], "boundary": 0, "phases": 0}
+    s.destroy()
+
+
+def test_mixture_objects_need_matching_phase_fractions():
+    sc = vtp.scenes.layered_mixture("IMMCT", 8, seed=1)
+    s = vtp.IMMCTSolver()
+    assert s.setConfig(sc.config), s.last_error
+    o = vtp.Object(vtp.Particle_Common)
+    o.pos = sc.objects[0].pos
+    o.getObjectComponentConfig()["epmMaterial"] = 0
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 3, "exportFlag": False,
+                                                 "velocityStart": [0, 0, 0], "phaseFraction": [1, 0, 0]})
+    assert not s.attachObject(o) and "phaseFraction" in s.last_error
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 3, "exportFlag": False,
+                                                 "velocityStart": [0, 0, 0], "phaseFraction": [1, 0]})
+    assert s.attachObject(o), s.last_error
+    assert s.counts()["phases"] == 2
+    s.destroy()
+
+
+def test_bad_extension_values_are_rejected():
+    s = vtp.PBFSolver()
+    cfg = vtp.scenes.pbf_dam_break().config
+    cfg["B200"] = {"unroll": 3}
+    assert not s.setConfig(cfg) and "unroll" in s.last_error
+    cfg["B200"] = {"blockSize": 100}
+    assert not s.setConfig(cfg)
+    s.destroy()
+
+
+def test_field_calls_before_initialize_fail_cleanly():
+    s = vtp.PBFSolver()
+    buf = (C.c_float * 3)()
+    rc = vtp.lib().vtp_solver_get_field(s._h, 0, buf, 12)
+    assert rc == _lib.VTP_ERR_STATE
+    s.destroy()
