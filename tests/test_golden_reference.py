@@ -191,3 +191,33 @@ def test_mixture_substeps_match_reference(vtp_gpu, case):
         else:       # later substeps: trajectory statistics
             assert eke < 1e-3 and eph < 1e-5
     s.destroy()
+
+
+# ---------------------------------------------------------------- the 1M-fluid DFSPH scene (1,453,957 particles)
+
+def test_oracle_neighbor_search_1m_matches_reference(oracle_lib):
+    g, meta = load("dfsph_1m_ugns")
+    sc = scene("dfsph_1m_ugns")
+    pos = np.concatenate([o.pos for o in sc.objects])
+    grid = oracle_lib.make_grid(sc.config[sc.solver]["Required"])
+    cnt, nb, _, _ = oracle_lib.neighbors(pos, grid)
+    assert cnt.size == meta["n"]
+    assert np.array_equal(np.bincount(cnt, minlength=grid.maxnbr + 1), g["nbr_count_hist_0"])
+    assert digest(cnt, nb) == meta["nbr_digest_0"]
+
+
+@pytest.mark.gpu
+def test_library_neighbor_search_1m_matches_reference(vtp_gpu):
+    g, meta = load("dfsph_1m_ugns")
+    sc = scene("dfsph_1m_ugns")
+    s = vtp_gpu.solver_from_scene(sc)
+    assert s.initialize()
+    maxnbr = int(sc.config[sc.solver]["Required"]["maxNeighborNum"])
+    cnt, nb = s.get_neighbors(maxnbr)
+    assert np.array_equal(np.bincount(cnt, minlength=maxnbr + 1), g["nbr_count_hist_0"])
+    assert digest(cnt, nb) == meta["nbr_digest_0"]
+    vol = s.get_field("volume").astype(np.float64)[meta["n_fluid"]:]
+    ref = g["volume_0_boundary_stats"]
+    assert abs(vol.sum() - ref[0]) <= 1e-5 * ref[0]
+    assert vol.min() == pytest.approx(ref[1], rel=1e-5) and vol.max() == pytest.approx(ref[2], rel=1e-5)
+    s.destroy()
