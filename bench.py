@@ -38,12 +38,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k"], default="dfsph_1m")
+    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k", "batched"], default="dfsph_1m")
+    ap.add_argument("--no-loop-baseline", action="store_true",
+                    help="batched workload: skip the plain per-scene loop it is compared with")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--scene-index", type=int, default=-1, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -132,6 +135,72 @@ def cpu_baseline(scene, seconds: float) -> dict:
                       f"initialization, {el:.1f} s of CPU time"}
 
 
+def run_reference_batched(args) -> dict:
+    """Reference side of the batched mix: each scene in its own process running the reference's
+    plain solver (its solvers keep function-local statics, so one solver per process), scenes one
+    after another; a time-bounded sample of the 64 scenes, interleaving PBF and DFSPH scenes."""
+    from vtp import scenes
+    mix = scenes.batched_scenes()
+    order = [k for pair in zip(range(48), range(48, 64)) for k in pair] + list(range(16, 48))
+    order = list(dict.fromkeys(order))
+    steps = max(1, min(args.steps, 50))
+    warm = min(args.warmup, 3)
+    budget = 150.0
+    t_start = time.perf_counter()
+    tot_ms, tot_ps, done, e2e = 0.0, 0.0, [], []
+    for k in order:
+        if time.perf_counter() - t_start > budget:
+            break
+        cmd = [sys.executable, str(Path(__file__).resolve()), "--impl", "reference", "--workload", "batched",
+               "--scene-index", str(k), "--steps", str(steps), "--warmup", str(warm), "--e2e-steps", "3"]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        if r.returncode != 0:
+            continue
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        if "ms" not in d:
+            continue
+        tot_ms += d["ms"]
+        tot_ps += mix[k].n_fluid * steps
+        e2e.append((mix[k].n_fluid * 3, d["e2e_s"]))
+        done.append(k)
+    out = {"impl": "reference", "metric": METRIC, "unit": METRIC, "higher_is_better": True}
+    if not done:
+        out["unavailable"] = "no scene of the batched mix ran in the reference build"
+        return out
+    value = tot_ps / (tot_ms / 1e3) / 1e6
+    out.update({"value": value, "n_gpus": 1, "steps": steps, "warmup": warm, "ms_per_step": tot_ms / steps,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched", "scenes_sampled": done, "scenes": len(mix),
+                           "impl": "reference CUDA build (sm_100a, -O3), one process per scene, "
+                                   "Solver::tickNsteps per scene one after another"},
+                "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
+                                 "sample": f"the reference is GPU code: its own CUDA build on this B200, "
+                                           f"{len(done)} of {len(mix)} scenes x {steps} substeps"},
+                "e2e": {"value": sum(a for a, _ in e2e) / sum(b for _, b in e2e) / 1e6, "unit": METRIC,
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return out
+
+
+def run_reference_scene(args) -> dict:
+    """One scene of the batched mix in the reference build (child process of run_reference_batched)."""
+    from oracle.ref import ref as R
+    from vtp import scenes
+    sc = scenes.batched_scenes()[args.scene_index]
+    s = R.RefSolver(sc)
+    s.initialize()
+    if args.warmup:
+        s.tick_timed(args.warmup)
+    ms = s.tick_timed(args.steps)
+    pos, vel = s.get("pos", 3), s.get("vel", 3)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.set("pos", pos)
+        s.set("vel", vel)
+        s.tick(1)
+        pos, vel = s.get("pos", 3), s.get("vel", 3)
+    return {"ms": ms, "e2e_s": time.perf_counter() - t0}
+
+
 def run_reference(args) -> dict:
     """The reference's own CUDA build (oracle/_ref/libvtref.so) on this GPU, through its Solver API."""
     import numpy as np
@@ -140,6 +209,8 @@ def run_reference(args) -> dict:
     if not R.available():
         out["unavailable"] = "oracle/_ref/libvtref.so was not built (the reference sources were not present)"
         return out
+    if args.workload == "batched":
+        return run_reference_scene(args) if args.scene_index >= 0 else run_reference_batched(args)
     sc = make_scene(args.workload)
     s = R.RefSolver(sc)
     s.initialize()
@@ -176,6 +247,136 @@ def run_reference(args) -> dict:
     return out
 
 
+def _batch_cost(sc) -> float:
+    # relative cost per substep: PBF runs 4 constraint iterations, DFSPH ~2x as many neighbour passes
+    return sc.n_fluid * (1.0 if sc.solver == "PBF" else 2.0)
+
+
+def run_batched(args, rank, world, local, dist, torch):
+    """64 independent scenes (48 PBF + 16 DFSPH): one solver per solver type advances all its
+    scenes together (scene-offset kernels, one CUDA graph per substep).  Compared with the plain
+    per-scene loop (one solver per scene, scenes one after another) on the same GPU."""
+    import numpy as np
+    import vtp
+    from vtp.dist import lpt_assign
+    mix = vtp.scenes.batched_scenes()
+    mine = sorted(lpt_assign([_batch_cost(m) for m in mix], world)[rank])
+    extra = {"blockSize": args.block} if args.block else None
+    groups = {}
+    for k in mine:
+        groups.setdefault(mix[k].solver, []).append(k)
+    batches = []
+    for kind in ("PBF", "DFSPH"):
+        if kind not in groups:
+            continue
+        idx = groups[kind]
+        b, ranges = vtp.solver_from_scenes([mix[k] for k in idx], extra)
+        assert b.initialize(), b.last_error
+        batches.append((kind, idx, b, ranges))
+    for _, _, b, _ in batches:
+        if args.warmup:
+            assert b.tickNsteps(args.warmup), b.last_error
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(local if world > 1 else 0)
+    clk.start()
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    launches = 0
+    for _, _, b, _ in batches:
+        assert b.tickNsteps(args.steps), b.last_error
+        dev_ms += b.stage_times()[2]
+        launches += b.launch_count()
+    wall = time.perf_counter() - t0
+    clocks = clk.stop()
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    nf_all = sum(m.n_fluid for m in mix)
+    value = nf_all * args.steps / (max_ms / 1e3) / 1e6
+    final = {}
+    for kind, idx, b, ranges in batches:
+        pos = b.get_field("pos")
+        for k, (lo, hi) in zip(idx, ranges):
+            final[k] = pos[lo:hi].copy()
+
+    # Roofline of the dominant kernel of the heavier batch (per-launch CUDA events).
+    prof = {}
+    for kind, idx, b, _ in batches:
+        for name, (ms, n) in b.profile_kernels(args.profile_steps).items():
+            pm, pn = prof.get(name, (0.0, 0))
+            prof[name] = (pm + ms, pn + n)
+    kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1],
+                   "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+
+    # e2e through the public API: every scene's state round-trips through pinned host memory
+    # each step (H2D positions + velocities, one substep, D2H of both).
+    hbuf = []
+    for _, _, b, _ in batches:
+        hbuf.append((torch.from_numpy(b.get_field("pos")).pin_memory(),
+                     torch.from_numpy(b.get_field("vel")).pin_memory()))
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for (_, _, b, _), (ph, vh) in zip(batches, hbuf):
+            b.set_field_ptr("pos", ph.data_ptr(), ph.numel() * 4)
+            b.set_field_ptr("vel", vh.data_ptr(), vh.numel() * 4)
+            assert b.tickNsteps(1), b.last_error
+            b.get_field_ptr("pos", ph.data_ptr(), ph.numel() * 4)
+            b.get_field_ptr("vel", vh.data_ptr(), vh.numel() * 4)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = nf_all * e2e_steps / float(te.item()) / 1e6
+    io_bytes = int(sum(ph.numel() * 4 + vh.numel() * 4 for ph, vh in hbuf))
+    for _, _, b, _ in batches:
+        b.destroy()
+
+    cfg = {"workload": "batched", "scenes": len(mix), "pbf_scenes": sum(m.solver == "PBF" for m in mix),
+           "fluid": nf_all, "boundary": sum(m.n_boundary for m in mix), "scenes_this_rank": len(mine),
+           "parallelism": f"scenes-lpt{world}", "wall_ms_per_step": 1e3 * wall / args.steps,
+           "l2": "inputs larger than L2 (~9.2M particles of state and neighbour lists)"}
+    if world == 1 and not args.no_loop_baseline:
+        # The plain per-scene loop: one solver per scene, scenes one after another.
+        loop_ms = 0.0
+        same = True
+        for k, m in enumerate(mix):
+            s = vtp.solver_from_scene(m, extra)
+            assert s.initialize(), s.last_error
+            if args.warmup:
+                assert s.tickNsteps(args.warmup), s.last_error
+            assert s.tickNsteps(args.steps), s.last_error
+            loop_ms += s.stage_times()[2]
+            same = same and np.array_equal(s.get_field("pos"), final[k])
+            s.destroy()
+        cfg["per_scene_loop_value"] = nf_all * args.steps / (loop_ms / 1e3) / 1e6
+        cfg["per_scene_loop_ms_per_step"] = loop_ms / args.steps
+        cfg["speedup_vs_per_scene_loop"] = cfg["per_scene_loop_value"] and value / cfg["per_scene_loop_value"]
+        cfg["identical_per_scene"] = bool(same)
+    dom_name, (dom_ms, dom_launches) = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": None, "peak": peak, "unit": "GB/s",
+                     "frac": None, "peak_kind": peak_kind, "traffic": None,
+                     "ms_per_launch": dom_ms / max(dom_launches, 1)},
+        "kernels": kernels,
+        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+    }
+    return line
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -202,6 +403,24 @@ def main():
 
     import vtp
     vtp.lib()
+    if args.workload == "batched":
+        line = run_batched(args, rank, world, local, dist, torch)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            mix = vtp.scenes.batched_scenes()
+            a = cpu_baseline(mix[0], args.cpu_seconds / 2)
+            d = cpu_baseline(mix[48], args.cpu_seconds / 2)
+            # combined rate: fluid particle-steps of both samples over their summed time
+            t_a = 1.0 / a["value"] if a["value"] else 0.0
+            t_d = 1.0 / d["value"] if d["value"] else 0.0
+            line["cpu_baseline"] = {"value": 2.0 / (t_a + t_d) if t_a + t_d else 0.0, "unit": METRIC,
+                                    "cores": a["cores"], "kind": "port",
+                                    "sample": f"scene 0 (PBF): {a['sample']}; scene 48 (DFSPH): {d['sample']}"}
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return 0
     sc = make_scene(args.workload)
     extra = {}
     if args.block:

@@ -134,6 +134,22 @@ VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 VTP_API int vtp_solver_attach_object(vtp_solver *s, const float *pos, uint32_t n,
                              const float *vel, const char *object_json);
 
+/* Scene batching (no counterpart in the reference, which runs one scene per
+ * solver).  Adds scene k >= 1 to a PBF or DFSPH solver after set_config
+ * (which defines scene 0) and before initialize.  `json_text` is a full
+ * solver config; its domain (simSpaceLB / simSpaceSize) and gravity are the
+ * new scene's own, every other parameter must equal scene 0's
+ * (VTP_ERR_CONFIG otherwise).  Objects join a scene through the key
+ * "scene": k at the top level of their object_json (default 0).  All scenes
+ * advance together in the same kernel launches; each scene's results are
+ * those a solver holding that scene alone produces (bit-identical, iteration
+ * counts included).  set_config drops all added scenes. */
+VTP_API int vtp_solver_add_scene(vtp_solver *s, const char *json_text, uint32_t *scene_index);
+
+/* Statistics of one scene of the most recent tick_n_steps call (pressure-solve
+ * iteration counts and residuals are per scene; the rest as get_stats). */
+VTP_API int vtp_solver_get_scene_stats(vtp_solver *s, uint32_t scene, vtp_stats *out);
+
 /* Replaces Solver::initialize() (PBFSolver.cpp:73-125, DFSPHSolver.cpp:75-137). */
 VTP_API int vtp_solver_initialize(vtp_solver *s);
 

@@ -54,6 +54,9 @@ def lib() -> C.CDLL:
         L.or_dfsph_init.argtypes = [C.c_uint32, P, P, P, P, C.POINTER(OrGrid), C.POINTER(OrDfsph)]
         L.or_dfsph_step.argtypes = [C.c_uint32, P, P, C.c_int32, P, P, P, P, P, C.POINTER(OrGrid),
                                     C.POINTER(OrDfsph), C.POINTER(OrSolveOut), P, P]
+        L.or_pbf_step_frozen.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf)]
+        L.or_pbf_step_adjoint.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf), P, P,
+                                          C.POINTER(C.c_double)]
         L.or_num_threads.restype = C.c_int
         L.or_set_num_threads.argtypes = [C.c_int]
         _lib = L
@@ -187,3 +190,63 @@ class OracleSolver:
                                 _ptr(self.ratio), _ptr(self.alpha))
                 self.last = out
             self.steps += 1
+
+
+class PbfDiff:
+    """FP64 differentiable PBF rollout with frozen neighbour lists (test infrastructure).
+
+    ``rollout`` advances (pos, vel) ``steps`` substeps; the lists of substep t are either
+    given (``lists[t]`` = (counts, nbrs) in the reference layout, e.g. the GPU's lists of the
+    same trajectory) or built from the FP32-rounded positions after the external force, as
+    the reference builds them.  ``adjoint`` runs or_pbf_step_adjoint backwards over a recorded
+    rollout and returns dL/d(pos0, vel0, XSPH_k).
+    """
+
+    def __init__(self, scene, xsph_k: float | None = None):
+        self.base = OracleSolver(scene)
+        if xsph_k is not None:
+            self.base.p.xsph_k = float(xsph_k)
+        self.p = self.base.p
+        self.maxnbr = int(self.base.grid.maxnbr)
+
+    @property
+    def fluid(self):
+        return self.base.mat == 0
+
+    def _lists_after_force(self, pos, vel):
+        x = pos.copy()
+        v = vel.copy()
+        f = self.fluid
+        g = np.array([self.p.g[a] for a in range(3)])
+        v[f] += g * self.p.dt
+        x[f] += v[f] * self.p.dt
+        cnt, nb, _, _ = neighbors(x.astype(np.float32), self.base.grid)
+        return cnt, nb
+
+    def rollout(self, pos0, vel0, steps: int, lists=None, record: bool = False):
+        b = self.base
+        pos = np.ascontiguousarray(pos0, np.float64).copy()
+        vel = np.ascontiguousarray(vel0, np.float64).copy()
+        states, used = [], []
+        for t in range(steps):
+            cnt, nb = lists[t] if lists is not None else self._lists_after_force(pos, vel)
+            cnt = np.ascontiguousarray(cnt, np.uint32)
+            nb = np.ascontiguousarray(nb, np.uint32)
+            if record:
+                states.append((pos.copy(), vel.copy()))
+                used.append((cnt, nb))
+            lib().or_pbf_step_frozen(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.mass), _ptr(b.vol), _ptr(cnt),
+                                     _ptr(nb), self.maxnbr, C.byref(self.p))
+        return pos, vel, states, used
+
+    def adjoint(self, states, used, xbar, vbar):
+        b = self.base
+        xb = np.ascontiguousarray(xbar, np.float64).copy()
+        vb = np.ascontiguousarray(vbar, np.float64).copy()
+        kb = C.c_double(0.0)
+        for t in range(len(states) - 1, -1, -1):
+            pos, vel = states[t]
+            cnt, nb = used[t]
+            lib().or_pbf_step_adjoint(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.mass), _ptr(b.vol), _ptr(cnt),
+                                      _ptr(nb), self.maxnbr, C.byref(self.p), _ptr(xb), _ptr(vb), C.byref(kb))
+        return xb, vb, kb.value

@@ -220,17 +220,13 @@ void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass
     free_lists(&L);
 }
 
-void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *vol,
-                 const or_grid *g, const or_pbf_params *p, double *density_out, double *lambda_out) {
+/* Constraint iterations + XSPH of one substep on the lists L (positions
+ * already advanced by the external force). */
+static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
+                     const double *vol, const lists_t *Lp, const or_grid *g, const or_pbf_params *p,
+                     double *density_out, double *lambda_out) {
+    const lists_t L = *Lp;
     const double dt = p->dt;
-    for (uint32_t i = 0; i < n; ++i) {
-        if (mat[i] != 0) continue;
-        for (int a = 0; a < 3; ++a) {
-            vel[3 * (size_t)i + a] += p->g[a] * dt;
-            pos[3 * (size_t)i + a] += vel[3 * (size_t)i + a] * dt;
-        }
-    }
-    lists_t L = build_lists(n, pos, g);
     cubic_t k = cubic_make(p->h);
     double *lam = (double *)calloc(n ? n : 1, sizeof(double));
     double *rho = (double *)calloc(n ? n : 1, sizeof(double));
@@ -304,7 +300,226 @@ void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const
     free(lam);
     free(rho);
     free(dx);
+}
+
+static void pbf_apply_force(uint32_t n, const int32_t *mat, double *pos, double *vel, const or_pbf_params *p) {
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            vel[3 * (size_t)i + a] += p->g[a] * p->dt;
+            pos[3 * (size_t)i + a] += vel[3 * (size_t)i + a] * p->dt;
+        }
+    }
+}
+
+void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *vol,
+                 const or_grid *g, const or_pbf_params *p, double *density_out, double *lambda_out) {
+    pbf_apply_force(n, mat, pos, vel, p);
+    lists_t L = build_lists(n, pos, g);
+    pbf_core(n, mat, pos, vel, mass, vol, &L, g, p, density_out, lambda_out);
     free_lists(&L);
+}
+
+void or_pbf_step_frozen(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
+                        const double *vol, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                        const or_pbf_params *p) {
+    or_grid g;
+    memset(&g, 0, sizeof(g));
+    g.maxnbr = maxnbr;
+    lists_t L = {(uint32_t *)cnt, (uint32_t *)nbr};
+    pbf_apply_force(n, mat, pos, vel, p);
+    pbf_core(n, mat, pos, vel, mass, vol, &L, &g, p, NULL, NULL);
+}
+
+/* g'(r) / r for gradW = g(r) r_vec: d(g r_vec)/d r_vec = g I + hh r_vec r_vec^T. */
+static double cubic_hh(const cubic_t *k, double r) {
+    double q = r / k->h;
+    if (q < 1e-6 || q > 1.0) return 0.0;
+    double h4 = k->h * k->h * k->h * k->h;
+    if (q <= 0.5) return 18.0 * k->sigma / (h4 * q);
+    return 6.0 * k->sigma * (1.0 - q * q) / (h4 * q * q * q);
+}
+
+void or_pbf_step_adjoint(uint32_t n, const int32_t *mat, const double *pos_in, const double *vel_in,
+                         const double *mass, const double *vol, const uint32_t *cnt, const uint32_t *nbr,
+                         uint32_t maxnbr, const or_pbf_params *p, double *xbar, double *vbar, double *kbar) {
+    or_grid gg;
+    memset(&gg, 0, sizeof(gg));
+    gg.maxnbr = maxnbr;
+    const or_grid *g = &gg;
+    lists_t L = {(uint32_t *)cnt, (uint32_t *)nbr};
+    const int I = p->iterations;
+    const double dt = p->dt, rho0 = p->rho0, c = p->xsph_k;
+    cubic_t k = cubic_make(p->h);
+    const size_t n3 = 3 * (size_t)(n ? n : 1);
+    /* ---- forward recompute with tape: X[it] positions before iteration it (X[I] = after), LAM, RHO */
+    double *X = (double *)malloc(sizeof(double) * n3 * (I + 1));
+    double *LAM = (double *)calloc((size_t)(n ? n : 1) * (I ? I : 1), sizeof(double));
+    double *RHO = (double *)calloc((size_t)(n ? n : 1) * (I ? I : 1), sizeof(double));
+    double *S2 = (double *)calloc((size_t)(n ? n : 1) * (I ? I : 1), sizeof(double));
+    double *GS = (double *)calloc(n3 * (I ? I : 1), sizeof(double));
+    double *v = (double *)malloc(sizeof(double) * n3);
+    memcpy(X, pos_in, sizeof(double) * 3 * n);
+    memcpy(v, vel_in, sizeof(double) * 3 * n);
+    pbf_apply_force(n, mat, X, v, p);
+    for (int it = 0; it < I; ++it) {
+        double *x = X + n3 * it, *xn = X + n3 * (it + 1);
+        double *lam = LAM + (size_t)n * it;
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double d = 0, gs[3] = {0, 0, 0}, s2 = 0, r[3];
+            FOR_NBR(L, g, i, j) {
+                double rl = rdiff(x, i, j, r);
+                d += mass[j] * cubic_w(&k, rl);
+                double q = cubic_g(&k, rl);
+                for (int a = 0; a < 3; ++a) {
+                    double e = q * r[a] / rho0;
+                    gs[a] += e;
+                    s2 += e * e;
+                }
+            }
+            RHO[(size_t)n * it + i] = d;
+            if (d < rho0) d = rho0;
+            double C = d / rho0 - 1.0;
+            for (int a = 0; a < 3; ++a) s2 += gs[a] * gs[a];
+            for (int a = 0; a < 3; ++a) GS[n3 * it + 3 * (size_t)i + a] = gs[a];
+            S2[(size_t)n * it + i] = s2;
+            lam[i] = -C / (s2 + p->eps);
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            for (int a = 0; a < 3; ++a) xn[3 * (size_t)i + a] = x[3 * (size_t)i + a];
+            if (mat[i] != 0) continue;
+            double s[3] = {0, 0, 0}, r[3];
+            FOR_NBR(L, g, i, j) {
+                double q = cubic_g(&k, rdiff(x, i, j, r));
+                double lj = mat[j] == 0 ? lam[j] : 0.0;
+                for (int a = 0; a < 3; ++a) s[a] += (lam[i] + lj) * q * r[a] / rho0;
+            }
+            for (int a = 0; a < 3; ++a) {
+                xn[3 * (size_t)i + a] += s[a];
+                v[3 * (size_t)i + a] += s[a] / dt;
+            }
+        }
+    }
+    /* ---- XSPH adjoint: a_i = c sum_j V_j (v_j - v_i) W_ij; x_out = x + a dt; v_out = v + a */
+    const double *xI = X + n3 * I;
+    double *ab = (double *)calloc(n3, sizeof(double));
+    double *xb = (double *)calloc(n3, sizeof(double));
+    double *vb = (double *)calloc(n3, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) ab[3 * (size_t)i + a] = xbar[3 * (size_t)i + a] * dt + vbar[3 * (size_t)i + a];
+    }
+    double ksum = 0.0;
+#pragma omp parallel for reduction(+ : ksum)
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double r[3], xo[3], vo[3];
+        for (int a = 0; a < 3; ++a) {
+            xo[a] = xbar[3 * (size_t)i + a];
+            vo[a] = vbar[3 * (size_t)i + a];
+        }
+        const double *ai = ab + 3 * (size_t)i;
+        FOR_NBR(L, g, i, j) {
+            if (j == i) continue;
+            double rl = rdiff(xI, i, j, r);
+            double w = cubic_w(&k, rl), q = cubic_g(&k, rl);
+            const int fj = mat[j] == 0;
+            const double *aj = ab + 3 * (size_t)j;
+            double dvdot_i = 0, dvdot_j = 0;
+            for (int a = 0; a < 3; ++a) {
+                double dv = v[3 * (size_t)j + a] - v[3 * (size_t)i + a];
+                dvdot_i += dv * ai[a];
+                dvdot_j += dv * (fj ? aj[a] : 0.0);
+                vo[a] += -c * vol[j] * w * ai[a] + (fj ? c * vol[i] * w * aj[a] : 0.0);
+            }
+            for (int a = 0; a < 3; ++a) xo[a] += c * q * r[a] * (vol[j] * dvdot_i - (fj ? vol[i] * dvdot_j : 0.0));
+            ksum += vol[j] * w * dvdot_i;
+        }
+        for (int a = 0; a < 3; ++a) {
+            xb[3 * (size_t)i + a] = xo[a];
+            vb[3 * (size_t)i + a] = vo[a];
+        }
+    }
+    *kbar += ksum;
+    /* ---- constraint iterations, last to first */
+    double *db = (double *)calloc(n3, sizeof(double));  /* Delta-bar */
+    double *sb = (double *)calloc(n ? n : 1, sizeof(double));  /* s2-bar */
+    double *rb = (double *)calloc(n ? n : 1, sizeof(double));  /* rho-bar */
+    double *xn = (double *)calloc(n3, sizeof(double));
+    for (int it = I - 1; it >= 0; --it) {
+        const double *x = X + n3 * it, *lam = LAM + (size_t)n * it, *GSi = GS + n3 * it;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (mat[i] != 0) continue;
+            for (int a = 0; a < 3; ++a) db[3 * (size_t)i + a] = xb[3 * (size_t)i + a] + vb[3 * (size_t)i + a] / dt;
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            sb[i] = rb[i] = 0.0;
+            if (mat[i] != 0) continue;
+            double lb = 0, r[3];
+            FOR_NBR(L, g, i, j) {
+                if (j == i) continue;
+                double q = cubic_g(&k, rdiff(x, i, j, r));
+                const int fj = mat[j] == 0;
+                for (int a = 0; a < 3; ++a)
+                    lb += q * r[a] / rho0 * (db[3 * (size_t)i + a] - (fj ? db[3 * (size_t)j + a] : 0.0));
+            }
+            double den = S2[(size_t)n * it + i] + p->eps;
+            double rho = RHO[(size_t)n * it + i];
+            double Cb = -lb / den;
+            sb[i] = -lb * lam[i] / den;
+            rb[i] = rho < rho0 ? 0.0 : Cb / rho0;
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            for (int a = 0; a < 3; ++a) xn[3 * (size_t)i + a] = xb[3 * (size_t)i + a];
+            if (mat[i] != 0) continue;
+            double r[3], acc[3] = {0, 0, 0};
+            FOR_NBR(L, g, i, j) {
+                if (j == i) continue;
+                double rl = rdiff(x, i, j, r);
+                double q = cubic_g(&k, rl), hh = cubic_hh(&k, rl);
+                const int fj = mat[j] == 0;
+                double lj = fj ? lam[j] : 0.0;
+                double e[3], ebar[3], rdot = 0;
+                for (int a = 0; a < 3; ++a) e[a] = q * r[a] / rho0;
+                for (int a = 0; a < 3; ++a) {
+                    double eij = (lam[i] + lj) * db[3 * (size_t)i + a] + 2.0 * sb[i] * (e[a] + GSi[3 * (size_t)i + a]);
+                    double eji = fj ? (lam[i] + lj) * db[3 * (size_t)j + a] + 2.0 * sb[j] * (-e[a] + GSi[3 * (size_t)j + a])
+                                    : 0.0;
+                    ebar[a] = eij - eji;
+                    rdot += r[a] * ebar[a];
+                }
+                double dens = mass[j] * rb[i] + (fj ? mass[i] * rb[j] : 0.0);
+                for (int a = 0; a < 3; ++a)
+                    acc[a] += q * r[a] * dens + (q * ebar[a] + hh * r[a] * rdot) / rho0;
+            }
+            for (int a = 0; a < 3; ++a) xn[3 * (size_t)i + a] += acc[a];
+        }
+        memcpy(xb, xn, sizeof(double) * 3 * n);
+    }
+    /* ---- external force: x0 = x + dt (v + g dt), v0 = v + g dt */
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            if (mat[i] != 0) {
+                xbar[3 * (size_t)i + a] = 0.0;
+                vbar[3 * (size_t)i + a] = 0.0;
+                continue;
+            }
+            xbar[3 * (size_t)i + a] = xb[3 * (size_t)i + a];
+            vbar[3 * (size_t)i + a] = vb[3 * (size_t)i + a] + dt * xb[3 * (size_t)i + a];
+        }
+    }
+    free(X); free(LAM); free(RHO); free(S2); free(GS); free(v);
+    free(ab); free(xb); free(vb); free(db); free(sb); free(rb); free(xn);
 }
 
 /* ------------------------------------------------------------------ DFSPH */

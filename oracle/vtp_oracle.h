@@ -60,6 +60,18 @@ void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass
 void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
                  const double *vol, const or_grid *g, const or_pbf_params *p, double *density, double *lambda);
 
+/* Differentiable PBF (no counterpart in the reference).  A substep with the
+ * neighbour lists given (frozen: reference layout, attach ids, self first),
+ * and its FP64 adjoint: from the pre-step state (pos, vel) and the same lists,
+ * maps (xbar, vbar) = dL/d(post-step pos, vel) to dL/d(pre-step pos, vel) in
+ * place (boundary rows 0) and adds dL/dXSPH_k to *kbar. */
+void or_pbf_step_frozen(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
+                        const double *vol, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                        const or_pbf_params *p);
+void or_pbf_step_adjoint(uint32_t n, const int32_t *mat, const double *pos, const double *vel, const double *mass,
+                         const double *vol, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                         const or_pbf_params *p, double *xbar, double *vbar, double *kbar);
+
 /* DFSPH (DFSPHSolver.cpp:339-406): obj[n] gives each particle's object index
  * and obj_is_fluid/obj_count describe the objects (residual = mean over fluid
  * objects of the object's mean clamped compression error). */

@@ -1,0 +1,139 @@
+"""Scene batching: one solver advancing several independent scenes.
+
+Each scene of a batched solver must produce exactly (bit for bit, iteration
+counts included) what a solver holding that scene alone produces: the scenes
+share kernel launches, never arithmetic.  CPU tests cover the host-side
+validation of vtp_solver_add_scene.
+"""
+import json
+
+import numpy as np
+import pytest
+
+import vtp
+from vtp import scenes
+
+
+def _pbf_mix():
+    return [scenes.dam_break("PBF", n, seed=70 + k, gravity_y=g)
+            for k, (n, g) in enumerate([(2000, -9.0), (5500, -11.5), (3100, -8.2), (8000, -10.0)])]
+
+
+def _dfsph_mix():
+    return [scenes.dam_break("DFSPH", n, seed=90 + k, gravity_y=g)
+            for k, (n, g) in enumerate([(3000, -9.81), (6000, -8.5), (12000, -11.0)])]
+
+
+# ---------------------------------------------------------------- CPU: host-side validation
+
+def test_add_scene_requires_matching_shared_parameters():
+    a, b = _pbf_mix()[:2]
+    s = vtp.PBFSolver()
+    assert s.setConfig(a.config)
+    assert s.addScene(b.config) == 1
+    bad = json.loads(json.dumps(b.config))
+    bad["PBF"]["Required"]["timeStep"] = 0.002
+    with pytest.raises(vtp.VtpError, match="timeStep"):
+        s.addScene(bad)
+    bad = json.loads(json.dumps(b.config))
+    bad["PBF"]["Required"]["iterationNum"] = 7
+    with pytest.raises(vtp.VtpError, match="iterationNum"):
+        s.addScene(bad)
+    s.destroy()
+
+
+def test_add_scene_rejects_mixture_solvers_and_bad_scene_index():
+    sc = scenes.layered_mixture("IMMCT", 8, seed=1)
+    s = vtp.IMMCTSolver()
+    assert s.setConfig(sc.config)
+    with pytest.raises(vtp.VtpError, match="PBF and DFSPH"):
+        s.addScene(sc.config)
+    s.destroy()
+    p = vtp.PBFSolver()
+    a = _pbf_mix()[0]
+    assert p.setConfig(a.config)
+    o = vtp.Object(vtp.Particle_Common)
+    o.pos = a.objects[0].pos
+    o.getObjectComponentConfig()["epmMaterial"] = 0
+    o.attachSpecificSolverObjectComponentConfig({"solverType": 0, "exportFlag": False, "velocityStart": [0, 0, 0],
+                                                 "colorStart": [0, 0, 0]})
+    assert not p.attachObject(o, scene=1)
+    assert "scene index" in p.last_error
+    p.destroy()
+
+
+def test_set_config_drops_added_scenes():
+    a, b = _pbf_mix()[:2]
+    s = vtp.PBFSolver()
+    s.setConfig(a.config)
+    assert s.addScene(b.config) == 1
+    s.setConfig(a.config)
+    assert s.addScene(b.config) == 1
+    s.destroy()
+
+
+def test_batched_scene_generator():
+    mix = scenes.batched_scenes()
+    assert len(mix) == 64
+    assert [m.solver for m in mix].count("PBF") == 48
+    nf = np.array([m.n_fluid for m in mix])
+    assert nf.min() >= 4000 * 0.8 and nf.max() <= 256000 * 1.1
+    g = np.array([m.config[m.solver]["Optional"]["gravity"][1] for m in mix])
+    assert np.all((g >= -12) & (g <= -8))
+
+
+# ---------------------------------------------------------------- GPU: batched == alone
+
+def _run_alone(sc, steps, extra):
+    s = vtp.solver_from_scene(sc, extra)
+    assert s.initialize()
+    assert s.tickNsteps(steps), s.last_error
+    out = (s.get_field("pos"), s.get_field("vel"), s.stats())
+    s.destroy()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,steps,extra", [
+    ("PBF", 6, None),
+    ("DFSPH", 4, None),
+    ("DFSPH", 3, {"deviceLoop": False}),
+    ("DFSPH", 3, {"useGraphs": False, "blockSize": 64}),
+])
+def test_batched_scenes_match_each_scene_alone(vtp_gpu, kind, steps, extra):
+    mix = _pbf_mix() if kind == "PBF" else _dfsph_mix()
+    b, ranges = vtp.solver_from_scenes(mix, extra)
+    assert b.initialize()
+    assert b.tickNsteps(steps), b.last_error
+    pos, vel = b.get_field("pos"), b.get_field("vel")
+    for k, sc in enumerate(mix):
+        lo, hi = ranges[k]
+        p1, v1, st1 = _run_alone(sc, steps, extra)
+        assert np.array_equal(pos[lo:hi], p1), f"scene {k} positions"
+        assert np.array_equal(vel[lo:hi], v1), f"scene {k} velocities"
+        if kind == "DFSPH":
+            sk = b.scene_stats(k)
+            assert (sk["total_div_iters"], sk["total_incomp_iters"]) == (st1["total_div_iters"],
+                                                                          st1["total_incomp_iters"])
+            assert sk["last_incomp_residual"] == st1["last_incomp_residual"]
+    b.destroy()
+
+
+@pytest.mark.gpu
+def test_batched_neighbor_lists_are_per_scene(vtp_gpu):
+    mix = _dfsph_mix()[:2]
+    b, ranges = vtp.solver_from_scenes(mix)
+    assert b.initialize() and b.tickNsteps(2)
+    maxnbr = int(mix[0].config["DFSPH"]["Required"]["maxNeighborNum"])
+    cnt, nb = b.get_neighbors(maxnbr)
+    for k, sc in enumerate(mix):
+        lo, hi = ranges[k]
+        s = vtp.solver_from_scene(sc)
+        assert s.initialize() and s.tickNsteps(2)
+        c1, n1 = s.get_neighbors(maxnbr)
+        s.destroy()
+        sub = nb[lo:hi].astype(np.int64)
+        sub = np.where(sub == 0xFFFFFFFF, -1, sub - lo)
+        assert np.array_equal(cnt[lo:hi], c1)
+        assert np.array_equal(sub, np.where(n1 == 0xFFFFFFFF, -1, n1.astype(np.int64)))
+    b.destroy()

@@ -195,6 +195,45 @@ int vtp_solver::parse_config(const json &c) {
     }
     cfg = c;
     configured = true;
+    // setConfig (re)defines scene 0 and drops any added scenes.
+    SceneRec s0;
+    s0.lb[0] = lbx; s0.lb[1] = lby; s0.lb[2] = lbz;
+    s0.size[0] = sx; s0.size[1] = sy; s0.size[2] = sz;
+    s0.gravity = gravity;
+    scenes.assign(1, s0);
+    return VTP_OK;
+}
+
+int vtp_solver::add_scene(const json &c, uint32_t *index) {
+    if (!configured) return fail(VTP_ERR_STATE, "add_scene before setConfig");
+    if (initialized) return fail(VTP_ERR_STATE, "add_scene after initialize");
+    if (type != VTP_SOLVER_PBF && type != VTP_SOLVER_DFSPH)
+        return fail(VTP_ERR_CONFIG, "scene batching supports the PBF and DFSPH solvers");
+    if (scenes.size() >= 65535) return fail(VTP_ERR_BOUNDS, "too many scenes");
+    // Parse with a scratch solver, then require every shared parameter to match.
+    vtp_solver t;
+    t.type = type;
+    int rc = t.parse_config(c);
+    if (rc) return rc;
+    std::string diff;
+    auto same = [&](const char *name, double a, double b) {
+        if (a != b && diff.empty()) diff = name;
+    };
+    same("timeStep", t.dt, dt);
+    same("particleRadius", t.radius, radius);
+    same("maxNeighborNum", t.maxnbr, maxnbr);
+    same("fPartRestDensity", t.rho_f, rho_f);
+    same("bPartRestDensity", t.rho_b, rho_b);
+    same("iterationNum", t.iterations, iterations);
+    same("XSPH_k", t.xsph_k, xsph_k);
+    same("fPartRestViscosity", t.viscosity, viscosity);
+    same("divFreeThreshold", t.div_thr, div_thr);
+    same("incompThreshold", t.incomp_thr, incomp_thr);
+    same("surfaceTensionCoefficient", t.gamma, gamma);
+    if (!diff.empty())
+        return fail(VTP_ERR_CONFIG, "scene config differs from scene 0 in a shared parameter: " + diff);
+    scenes.push_back(t.scenes[0]);
+    if (index) *index = (uint32_t)(scenes.size() - 1);
     return VTP_OK;
 }
 
@@ -217,6 +256,8 @@ int vtp_solver::attach(const float *p, uint32_t n, const float *v, const json &o
     ObjRec rec;
     rec.name = o.value("name", std::string("obj_") + std::to_string(objs.size()));
     rec.mat = mat;
+    rec.scene = o.value("scene", 0u);
+    if (rec.scene >= scenes.size()) return fail(VTP_ERR_ARG, "object scene index out of range");
     rec.start = (uint32_t)(hpos.size() / 3);
     rec.export_flag = socc["exportFlag"].get<bool>();
     auto v0 = socc["velocityStart"].get<std::vector<float>>();
@@ -257,7 +298,7 @@ vtp::PbfArgs vtp_solver::pbf_args() {
     return a;
 }
 
-vtp::DfsphArgs vtp_solver::dfsph_args() {
+vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     vtp::DfsphArgs a{};
     a.nf = L.nf; a.nb = L.nb; a.ell_stride = L.ell_stride; a.k = kc;
     a.dt = dt; a.inv_dt = inv_dt; a.inv_dt2 = inv_dt2;
@@ -265,14 +306,17 @@ vtp::DfsphArgs vtp_solver::dfsph_args() {
     a.mass_f = rho_f * vol0;                               // update_mass_cuda: m = rest_density * V
     a.vis_coef = (viscosity + viscosity) / 2 * a.mass_f / rho_f;
     a.h2_001 = 0.001f * (h * h);
-    a.gravity = gravity; a.gamma = gamma;
+    a.gamma = gamma;
     a.csigma = 32.f / 3.14159265f / std::pow(h, 9.f);
     a.h6_64 = std::pow(h, 6.f) / 64;
     a.nbr = u.nbr; a.ncnt = u.ncnt;
     a.pos = pos.c(); a.vel = vel.c(); a.vel_alt = vel.n(); a.vadv = vadv.c(); a.vadv_alt = vadv.n();
     a.ratio = ratio; a.alpha = alpha; a.kappa = kappa; a.delta = delta;
     a.acc_tmp = acc_tmp; a.normal = normal;
-    a.orig = orig.c(); a.obj_of = obj_of; a.nobj = nobj_fluid; a.partials = partials; a.status = d_status;
+    a.orig = orig.c(); a.obj_of = obj_of; a.nobj_max = nobj_max; a.partials = partials; a.status = d_status;
+    a.tiles = d_tiles; a.ntiles = ntiles; a.scene_tiles = d_scene_tiles;
+    a.state = solve ? solve + (size_t)which * scenes.size() : nullptr;
+    a.sc = scn();
     a.tick = d_tick;
     a.unroll = unroll;
     return a;
@@ -280,11 +324,12 @@ vtp::DfsphArgs vtp_solver::dfsph_args() {
 
 vtp::SolveCtl vtp_solver::solve_ctl(int which, cudaGraphConditionalHandle hnd, int use_cond) {
     vtp::SolveCtl c{};
-    c.state = solve + which;
+    c.state = solve + (size_t)which * scenes.size();
+    c.loop = loop + which;
     c.inv_count = inv_count;
-    c.nobj = nobj_fluid;
-    c.nblocks = vtp::dfsph_partial_blocks(L.nf, block);
-    if (c.nblocks == 0) c.nblocks = 1;
+    c.scene_tiles = d_scene_tiles;
+    c.nscenes = nscenes();
+    c.nobj_max = nobj_max;
     c.threshold = which == 0 ? div_thr : incomp_thr;
     c.force_iters = which == 0 ? force_div : force_inc;
     c.force_seq = d_force_seq;
@@ -302,8 +347,8 @@ vtp::SolveCtl vtp_solver::solve_ctl(int which, cudaGraphConditionalHandle hnd, i
 int vtp_solver::sort_boundary_and_lists() {
     // Boundary rows are static: sort them once, build the cell table once.
     vtp::Carry none{};
-    vtp::ugns_sort(st, grid, L.nf, L.nb, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, 0.f,
-                   make_float3(0, 0, 0), u, u.bstart);
+    vtp::ugns_sort(st, scn(), nbuckets, L.nf, L.nb, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, 0.f,
+                   u, u.bstart);
     // Copy the sorted boundary rows into both buffers of every double buffer.
     size_t nb = L.nb;
     CU(cudaMemcpyAsync(pos.c() + L.nf, pos.n() + L.nf, nb * sizeof(float4), cudaMemcpyDeviceToDevice, st));
@@ -317,36 +362,61 @@ int vtp_solver::initialize() {
     if (initialized) return VTP_OK;
     const uint32_t n = (uint32_t)(hpos.size() / 3);
     if (n == 0) return fail(VTP_ERR_STATE, "no particles attached");
+    const int S = nscenes();
     L.n = n;
     L.nf = 0;
-    for (auto &o : objs)
+    for (auto &sc : scenes) sc.nf = sc.nb = 0, sc.attach_lo = UINT32_MAX;
+    for (auto &o : objs) {
+        SceneRec &sc = scenes[o.scene];
+        (o.mat == 0 ? sc.nf : sc.nb) += o.end - o.start;
+        if (o.end > o.start) sc.attach_lo = std::min(sc.attach_lo, o.start);
         if (o.mat == 0) L.nf += o.end - o.start;
+    }
     L.nb = n - L.nf;
     L.ell_stride = maxnbr > 1 ? maxnbr - 1 : 1;
-    // Attach ids of fluid vs boundary decide how a cell's two runs interleave.
-    uint32_t fmin = UINT32_MAX, fmax = 0, bmin = UINT32_MAX, bmax = 0;
-    for (auto &o : objs) {
-        if (o.end == o.start) continue;
-        if (o.mat == 0) fmin = std::min(fmin, o.start), fmax = std::max(fmax, o.end - 1);
-        else bmin = std::min(bmin, o.start), bmax = std::max(bmax, o.end - 1);
+    // Attach ids of fluid vs boundary decide how a cell's two runs interleave
+    // (per scene; scenes that disagree fall back to the general merge).
+    int mode = -1;
+    for (int k = 0; k < S; ++k) {
+        uint32_t fmin = UINT32_MAX, fmax = 0, bmin = UINT32_MAX, bmax = 0;
+        for (auto &o : objs) {
+            if (o.end == o.start || (int)o.scene != k) continue;
+            if (o.mat == 0) fmin = std::min(fmin, o.start), fmax = std::max(fmax, o.end - 1);
+            else bmin = std::min(bmin, o.start), bmax = std::max(bmax, o.end - 1);
+        }
+        int m;
+        if (scenes[k].nb == 0 || scenes[k].nf == 0 || fmax < bmin) m = 0;
+        else if (bmax < fmin) m = 1;
+        else m = 2;
+        if (scenes[k].nf + scenes[k].nb == 0) continue;
+        mode = mode < 0 ? m : (mode == m ? m : 2);
     }
-    if (L.nb == 0 || L.nf == 0 || fmax < bmin) L.merge_mode = 0;
-    else if (bmax < fmin) L.merge_mode = 1;
-    else L.merge_mode = 2;
+    L.merge_mode = mode < 0 ? 0 : mode;
 
-    // Grid as UniformGirdNeighborSearcher::setConfig (UniformGridNeighborSearch.cpp:214-218).
-    grid.lbx = lbx; grid.lby = lby; grid.lbz = lbz;
-    grid.cell = h;
-    grid.gx = (int)std::ceil(sx / h);
-    grid.gy = (int)std::ceil(sy / h);
-    grid.gz = (int)std::ceil(sz / h);
-    if (grid.gx <= 0 || grid.gy <= 0 || grid.gz <= 0) return fail(VTP_ERR_CONFIG, "empty grid");
-    // Keys reach z*gy*gx + y*gx + x with the inclusive upper bound of cellIsAvailable.
-    uint64_t maxkey = (uint64_t)grid.gz * grid.gy * grid.gx + (uint64_t)grid.gy * grid.gx + grid.gx;
-    if (maxkey + 2 > (1ull << 31)) return fail(VTP_ERR_BOUNDS, "grid too large (more than 2^31 cells)");
-    grid.nkey = (uint32_t)(maxkey + 1);
-    grid.d2max = sqrt_threshold(h);
-    grid.maxnbr = maxnbr;
+    // Grids as UniformGirdNeighborSearcher::setConfig (UniformGridNeighborSearch.cpp:214-218),
+    // one per scene, each followed by its own outside bucket.
+    uint64_t key_base = 0;
+    uint32_t fb = 0, bb = L.nf;
+    for (auto &sc : scenes) {
+        vtp::SceneGrid &g = sc.grid;
+        g.lbx = sc.lb[0]; g.lby = sc.lb[1]; g.lbz = sc.lb[2];
+        g.gx = (int)std::ceil(sc.size[0] / h);
+        g.gy = (int)std::ceil(sc.size[1] / h);
+        g.gz = (int)std::ceil(sc.size[2] / h);
+        if (g.gx <= 0 || g.gy <= 0 || g.gz <= 0) return fail(VTP_ERR_CONFIG, "empty grid");
+        // Keys reach z*gy*gx + y*gx + x with the inclusive upper bound of cellIsAvailable.
+        uint64_t maxkey = (uint64_t)g.gz * g.gy * g.gx + (uint64_t)g.gy * g.gx + g.gx;
+        if (maxkey + 2 > (1ull << 31)) return fail(VTP_ERR_BOUNDS, "grid too large (more than 2^31 cells)");
+        g.nkey = (uint32_t)(maxkey + 1);
+        g.key_base = (uint32_t)key_base;
+        g.grav_x = sc.gravity.x; g.grav_y = sc.gravity.y; g.grav_z = sc.gravity.z;
+        key_base += (uint64_t)g.nkey + 1;
+        if (key_base + 1 > (1ull << 31)) return fail(VTP_ERR_BOUNDS, "scene grids too large (more than 2^31 cells)");
+        sc.fbase = fb; fb += sc.nf;
+        sc.bbase = bb; bb += sc.nb;
+    }
+    nbuckets = (uint32_t)key_base;
+    d2max = sqrt_threshold(h);
     kc.h = h;
     kc.invh = 1.f / h;
     kc.sigma = 8.f / 3.14159265f / std::pow(h, 3.f);  // replaced by the device value below
@@ -371,13 +441,13 @@ int vtp_solver::initialize() {
     const uint32_t nrows_max = std::max(L.nf, L.nb);
     AL(&u.key, nrows_max);
     AL(&u.rank, nrows_max);
-    AL(&u.count, (size_t)grid.nkey + 1);
-    AL(&u.fstart, (size_t)grid.nkey + 2);
-    AL(&u.bstart, (size_t)grid.nkey + 2);
+    AL(&u.count, (size_t)nbuckets);
+    AL(&u.fstart, (size_t)nbuckets + 1);
+    AL(&u.bstart, (size_t)nbuckets + 1);
     AL(&u.tmp_src, nrows_max);
     AL(&u.tmp_orig, nrows_max);
     AL(&u.tmp_key, nrows_max);
-    u.scan_tiles = ((size_t)grid.nkey + 1 + 2047) / 2048;
+    u.scan_tiles = ((size_t)nbuckets + 2047) / 2048;
     if (u.scan_tiles > 1024 * 64) return fail(VTP_ERR_BOUNDS, "grid too large for the cell scan");
     AL(&u.scan_sums, u.scan_tiles);
     const size_t fl_rows = ((size_t)L.nf + 31) / 32 * 32, bl_rows = ((size_t)L.nb + 31) / 32 * 32;
@@ -390,13 +460,32 @@ int vtp_solver::initialize() {
     CU(cudaMemsetAsync(d_status, 0, 4 * sizeof(uint32_t), st));
     CU(cudaMemsetAsync(d_overflow, 0, 4 * sizeof(uint32_t), st));
 
-    // Upload in attach order, then split into fluid rows [0, nf) and boundary rows [nf, n).
+    // Scene table and the static row -> scene map.
+    std::vector<vtp::SceneGrid> sg(S);
+    std::vector<uint16_t> rs(n);
+    for (int k = 0; k < S; ++k) {
+        sg[k] = scenes[k].grid;
+        std::fill(rs.begin() + scenes[k].fbase, rs.begin() + scenes[k].fbase + scenes[k].nf, (uint16_t)k);
+        std::fill(rs.begin() + scenes[k].bbase, rs.begin() + scenes[k].bbase + scenes[k].nb, (uint16_t)k);
+    }
+    AL(&d_sg, S);
+    AL(&row_scene, n);
+    CU(cudaMemcpyAsync(d_sg, sg.data(), S * sizeof(vtp::SceneGrid), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(row_scene, rs.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+
+    // Upload in attach order, placing each scene's fluid rows in [fbase, fbase + nf) and its
+    // boundary rows in [bbase, bbase + nb), attach order kept inside each range.
     std::vector<float4> p4(n), v4(n);
     std::vector<uint32_t> ids(n);
-    uint32_t fi = 0, bi = L.nf;
+    std::vector<uint32_t> fnext(S), bnext(S);
+    for (int k = 0; k < S; ++k) fnext[k] = scenes[k].fbase, bnext[k] = scenes[k].bbase;
+    std::vector<int> scene_of(n, 0);
+    for (auto &o : objs)
+        for (uint32_t i = o.start; i < o.end; ++i) scene_of[i] = (int)o.scene;
     const float mass_f = rho_f * vol0;
     for (uint32_t i = 0; i < n; ++i) {
-        uint32_t row = hmat[i] == 0 ? fi++ : bi++;
+        const int k = scene_of[i];
+        uint32_t row = hmat[i] == 0 ? fnext[k]++ : bnext[k]++;
         float w = 0.f;
         if (type == VTP_SOLVER_PBF) w = mass_f;          // PBF: w = mass (init_cuda, PBFCudaImpl.cu:34-45)
         else w = vol0;                                    // DFSPH / IMM: w = volume
@@ -431,8 +520,10 @@ int vtp_solver::initialize() {
         AL(&rest_b, L.nb);
         AL(&acc_tmp, L.nf);
         AL(&normal, L.nf);
-        AL(&solve, 2);
-        CU(cudaMemsetAsync(solve, 0, 2 * sizeof(vtp::SolveState), st));
+        AL(&solve, 2 * (size_t)S);
+        CU(cudaMemsetAsync(solve, 0, 2 * (size_t)S * sizeof(vtp::SolveState), st));
+        AL(&loop, 2);
+        CU(cudaMemsetAsync(loop, 0, 2 * sizeof(vtp::LoopState), st));
         AL(&d_tick, 1);
         CU(cudaMemsetAsync(d_tick, 0, sizeof(uint64_t), st));
         if (!force_seq.empty()) {
@@ -444,22 +535,44 @@ int vtp_solver::initialize() {
         CU(cudaMemsetAsync(ratio, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
         CU(cudaMemsetAsync(alpha, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
         CU(cudaMemsetAsync(delta, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
-        // Fluid objects: residual means are taken per object (vfsph_div, DFSPHCudaImpl.cu:471-483).
+        // Fluid objects: residual means are taken per object (vfsph_div, DFSPHCudaImpl.cu:471-483);
+        // slots are numbered scene by scene so a scene's objects are contiguous.
         std::vector<uint16_t> objmap(n, 0);
         std::vector<double> invc;
-        for (auto &o : objs) {
-            if (o.mat != 0) continue;
-            for (uint32_t i = o.start; i < o.end; ++i) objmap[i] = (uint16_t)invc.size();
-            invc.push_back(o.end > o.start ? 1.0 / (double)(o.end - o.start) : 0.0);
+        std::vector<vtp::SceneTiles> stl(S);
+        nobj_max = 1;
+        for (int k = 0; k < S; ++k) {
+            stl[k].obj0 = (uint32_t)invc.size();
+            for (auto &o : objs) {
+                if (o.mat != 0 || (int)o.scene != k) continue;
+                for (uint32_t i = o.start; i < o.end; ++i) objmap[i] = (uint16_t)invc.size();
+                invc.push_back(o.end > o.start ? 1.0 / (double)(o.end - o.start) : 0.0);
+            }
+            stl[k].nobj = (uint32_t)invc.size() - stl[k].obj0;
+            nobj_max = std::max<int>(nobj_max, (int)stl[k].nobj);
         }
+        if (invc.size() > 65535) return fail(VTP_ERR_BOUNDS, "too many fluid objects");
         if (invc.empty()) invc.push_back(0.0);
-        nobj_fluid = (int)invc.size();
-        if (nobj_fluid > 65535) return fail(VTP_ERR_BOUNDS, "too many fluid objects");
+        // Scene-offset tiles of `block` fluid rows each.
+        std::vector<uint4> tiles;
+        for (int k = 0; k < S; ++k) {
+            stl[k].tile0 = (uint32_t)tiles.size();
+            for (uint32_t r = 0; r < scenes[k].nf; r += (uint32_t)block)
+                tiles.push_back(make_uint4(scenes[k].fbase + r, std::min<uint32_t>(block, scenes[k].nf - r),
+                                           (uint32_t)k, 0u));
+            stl[k].ntiles = (uint32_t)tiles.size() - stl[k].tile0;
+        }
+        ntiles = (uint32_t)tiles.size();
         AL(&inv_count, invc.size());
         AL(&obj_of, n);
+        AL(&d_tiles, std::max<size_t>(tiles.size(), 1));
+        AL(&d_scene_tiles, S);
         CU(cudaMemcpyAsync(inv_count, invc.data(), invc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(obj_of, objmap.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
-        AL(&partials, (size_t)vtp::dfsph_partial_blocks(std::max<uint32_t>(L.nf, 1), block) * nobj_fluid + 1);
+        if (!tiles.empty())
+            CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_scene_tiles, stl.data(), S * sizeof(vtp::SceneTiles), cudaMemcpyHostToDevice, st));
+        AL(&partials, (size_t)std::max<uint32_t>(ntiles, 1) * nobj_max + 1);
         if (type != VTP_SOLVER_DFSPH) {
             if ((rc = immct_alloc(*this))) return rc;
         }
@@ -467,14 +580,11 @@ int vtp_solver::initialize() {
     // Neighbour search of the initial state (initialize(): m_neighborSearcher.update(pos)),
     // then the boundary volumes from the boundary rows' lists.
     vtp::Carry carry{};
-    if (type != VTP_SOLVER_PBF) {
-        carry.nf4 = 0;
-    }
-    vtp::ugns_sort(st, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
-                   make_float3(0, 0, 0), u, u.fstart);
+    vtp::ugns_sort(st, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
+                   u, u.fstart);
     pos.swap(); vel.swap(); orig.swap();
-    vtp::ugns_build_lists(st, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt, d_status, d_overflow, block);
-    vtp::ugns_build_lists(st, grid, L, L.nf, L.nb, pos.c(), orig.c(), u, u.bnbr, u.bncnt, d_status, d_overflow,
+    vtp::ugns_build_lists(st, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt, d_status, d_overflow, block);
+    vtp::ugns_build_lists(st, scn(), L, L.nf, L.nb, pos.c(), orig.c(), u, u.bnbr, u.bncnt, d_status, d_overflow,
                           block);
     if (type == VTP_SOLVER_PBF) {
         vtp::PbfArgs a = pbf_args();
@@ -507,8 +617,8 @@ int vtp_solver::initialize() {
 // ---------------------------------------------------------------- tick
 
 int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
-    vtp::DfsphArgs a = dfsph_args();
-    vtp::dfsph_solve_begin(s, solve + which);
+    vtp::DfsphArgs a = dfsph_args(which);
+    vtp::dfsph_solve_begin(s, solve + (size_t)which * scenes.size(), loop + which, nscenes());
     launches_per_tick += 1;
     if (capture && device_loop) {
         cudaStreamCaptureStatus cs;
@@ -550,9 +660,9 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
         PROF(this, "dfsph_solve_end",
              vtp::dfsph_solve_end(s, solve_ctl(which, cudaGraphConditionalHandle{}, 0), partials, d_status));
         launches_per_tick += 3;
-        CU(cudaMemcpyAsync(h_pinned + 2, &solve[which].stopped, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(h_pinned + 2, &loop[which].running, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
-        if (h_pinned[2]) break;
+        if (!h_pinned[2]) break;
     }
     return VTP_OK;
 }
@@ -561,10 +671,10 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     int rc;
     if (type == VTP_SOLVER_PBF) {
         vtp::Carry none{};
-        vtp::ugns_sort(s, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt, gravity, u,
-                       u.fstart, prof);
+        vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt,
+                       u, u.fstart, prof);
         pos.swap(); vel.swap(); orig.swap();
-        PROF(this, "ugns_lists", vtp::ugns_build_lists(s, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
+        PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
                                                        d_status, d_overflow, block));
         launches_per_tick += 8;  // hash, 4 scan kernels, scatter, rank/reorder, lists
         for (int it = 0; it < iterations; ++it) {
@@ -585,10 +695,10 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     carry.nf4 = 1;
     carry.src4[0] = vadv.c();
     carry.dst4[0] = vadv.n();
-    vtp::ugns_sort(s, grid, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
-                   make_float3(0, 0, 0), u, u.fstart, prof);
+    vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
+                   u, u.fstart, prof);
     pos.swap(); vel.swap(); orig.swap(); vadv.swap();
-    PROF(this, "ugns_lists", vtp::ugns_build_lists(s, grid, L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
+    PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
                                                    d_status, d_overflow, block));
     PROF(this, "dfsph_ratio_alpha", vtp::dfsph_ratio_alpha(s, dfsph_args(), block));
     launches_per_tick += 9;  // neighbour search (8) + ratio/alpha
@@ -674,7 +784,10 @@ int vtp_solver::tick_n(uint32_t n) {
     if (!initialized && (rc = initialize())) return rc;
     if (crashed) return fail(VTP_NOT_CONVERGED, std::string(solver_key(type)) + "Solver is crashed.");
     const bool solves = type != VTP_SOLVER_PBF;
-    if (solves) CU(cudaMemsetAsync(solve, 0, 2 * sizeof(vtp::SolveState), st));
+    if (solves) {
+        CU(cudaMemsetAsync(solve, 0, 2 * scenes.size() * sizeof(vtp::SolveState), st));
+        CU(cudaMemsetAsync(loop, 0, 2 * sizeof(vtp::LoopState), st));
+    }
     if (use_graphs && !graphs_ready) {
         if ((rc = build_graphs())) {
             // A failed capture leaves the stream usable; fall back to direct launches.
@@ -715,17 +828,13 @@ int vtp_solver::tick_n(uint32_t n) {
     CU(cudaEventElapsedTime(&stage_ms[2], ev[0], ev[2]));
     if ((rc = check_status())) return fail(rc, "solver status after tick");
     if (solves) {
-        vtp::SolveState hs[2];
-        CU(cudaMemcpy(hs, solve, sizeof(hs), cudaMemcpyDeviceToHost));
-        stats.last_div_iters = hs[0].last_iters;
-        stats.last_incomp_iters = hs[1].last_iters;
-        stats.total_div_iters = hs[0].total_iters;
-        stats.total_incomp_iters = hs[1].total_iters;
-        stats.last_div_residual = hs[0].residual;
-        stats.last_incomp_residual = hs[1].residual;
+        if ((rc = read_solve_states())) return rc;
+        stats = scene_stats[0];
         if (use_graphs) {
-            // per solve iteration: solve_a, solve_b, solve_end
-            launches = (uint64_t)n * launches_per_tick + 3 * (hs[0].total_iters + hs[1].total_iters);
+            // per solve-loop iteration: solve_a, solve_b, solve_end
+            vtp::LoopState hl[2];
+            CU(cudaMemcpy(hl, loop, sizeof(hl), cudaMemcpyDeviceToHost));
+            launches = (uint64_t)n * launches_per_tick + 3 * (hl[0].total + hl[1].total);
         }
     } else if (use_graphs) {
         launches = (uint64_t)n * launches_per_tick;
@@ -734,6 +843,23 @@ int vtp_solver::tick_n(uint32_t n) {
     if (imm) stats.phase_retries = immct_last_retries(*this);
     stats.steps_done = steps_done;
     stats.sim_time = sim_time;
+    return VTP_OK;
+}
+
+int vtp_solver::read_solve_states() {
+    const size_t S = scenes.size();
+    std::vector<vtp::SolveState> hs(2 * S);
+    CU(cudaMemcpy(hs.data(), solve, hs.size() * sizeof(vtp::SolveState), cudaMemcpyDeviceToHost));
+    scene_stats.assign(S, stats);
+    for (size_t k = 0; k < S; ++k) {
+        vtp_stats &o = scene_stats[k];
+        o.last_div_iters = hs[k].last_iters;
+        o.last_incomp_iters = hs[S + k].last_iters;
+        o.total_div_iters = hs[k].total_iters;
+        o.total_incomp_iters = hs[S + k].total_iters;
+        o.last_div_residual = hs[k].residual;
+        o.last_incomp_residual = hs[S + k].residual;
+    }
     return VTP_OK;
 }
 
@@ -942,6 +1068,33 @@ int vtp_solver_attach_object(vtp_solver *s, const float *pos, uint32_t n, const 
     }
 }
 
+int vtp_solver_add_scene(vtp_solver *s, const char *json_text, uint32_t *scene_index) {
+    if (!s || !json_text) return fail(VTP_ERR_ARG, "null argument");
+    json c;
+    try {
+        c = json::parse(json_text);
+    } catch (const std::exception &e) {
+        return fail(VTP_ERR_CONFIG, std::string("JSON parse error: ") + e.what());
+    }
+    return s->add_scene(c, scene_index);
+}
+
+int vtp_solver_get_scene_stats(vtp_solver *s, uint32_t scene, vtp_stats *out) {
+    if (!s || !out) return fail(VTP_ERR_ARG, "null argument");
+    if (scene >= s->scenes.size()) return fail(VTP_ERR_ARG, "scene index out of range");
+    *out = s->stats;
+    if (scene < s->scene_stats.size()) {
+        const vtp_stats &k = s->scene_stats[scene];
+        out->last_div_iters = k.last_div_iters;
+        out->last_incomp_iters = k.last_incomp_iters;
+        out->total_div_iters = k.total_div_iters;
+        out->total_incomp_iters = k.total_incomp_iters;
+        out->last_div_residual = k.last_div_residual;
+        out->last_incomp_residual = k.last_incomp_residual;
+    }
+    return VTP_OK;
+}
+
 int vtp_solver_initialize(vtp_solver *s) {
     if (!s) return fail(VTP_ERR_ARG, "null solver");
     try {
@@ -1032,8 +1185,8 @@ int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, ui
         carry.dst4[0] = s->vadv.n();
     }
     if (s->imm) immct_fill_carry(*s, carry);
-    vtp::ugns_sort(s->st, s->grid, 0, s->L.nf, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(), s->orig.c(),
-                   s->orig.n(), carry, 0.f, make_float3(0, 0, 0), s->u, s->u.fstart);
+    vtp::ugns_sort(s->st, s->scn(), s->nbuckets, 0, s->L.nf, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(),
+                   s->orig.c(), s->orig.n(), carry, 0.f, s->u, s->u.fstart);
     // Copy the re-sorted fluid rows back so the buffer parity the substep graphs expect is kept.
     const size_t nf = s->L.nf;
     CU(cudaMemcpyAsync(s->pos.c(), s->pos.n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
@@ -1045,9 +1198,9 @@ int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, ui
         int rc = immct_copy_back(*s);
         if (rc) return rc;
     }
-    vtp::ugns_build_lists(s->st, s->grid, s->L, 0, s->L.nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
+    vtp::ugns_build_lists(s->st, s->scn(), s->L, 0, s->L.nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
                           s->d_status, s->d_overflow, s->block);
-    vtp::ugns_build_lists(s->st, s->grid, s->L, s->L.nf, s->L.nb, s->pos.c(), s->orig.c(), s->u, s->u.bnbr,
+    vtp::ugns_build_lists(s->st, s->scn(), s->L, s->L.nf, s->L.nb, s->pos.c(), s->orig.c(), s->u, s->u.bnbr,
                           s->u.bncnt, s->d_status, s->d_overflow, s->block);
     uint32_t *dc = nullptr, *dn = nullptr;
     CU(cudaMalloc(&dc, (size_t)n * 4));
@@ -1072,7 +1225,7 @@ int vtp_solver_get_sorted_order(vtp_solver *s, uint32_t *sorted_ids, uint32_t *c
     CU(cudaMalloc(&di, (size_t)n * 4));
     cudaError_t e = cudaMalloc(&dk, (size_t)n * 4);
     if (e != cudaSuccess) { cudaFree(di); return fail(VTP_ERR_NOMEM, "sorted export buffer"); }
-    vtp::export_sorted(s->st, s->grid, n, s->pos.c(), s->orig.c(), di, dk);
+    vtp::export_sorted(s->st, s->scn(), n, s->pos.c(), s->orig.c(), di, dk);
     std::vector<uint32_t> ids(n), keys(n);
     e = cudaMemcpyAsync(ids.data(), di, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(keys.data(), dk, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
@@ -1080,10 +1233,15 @@ int vtp_solver_get_sorted_order(vtp_solver *s, uint32_t *sorted_ids, uint32_t *c
     cudaFree(di);
     cudaFree(dk);
     if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
-    // Global order of all rows by (cell, attach id): fluid and boundary runs interleave.
+    // Global order of all rows by (scene, cell, attach id): fluid and boundary runs interleave.
+    std::vector<uint32_t> scene_of(n, 0);
+    for (auto &o : s->objs)
+        for (uint32_t i = o.start; i < o.end; ++i) scene_of[i] = o.scene;
     std::vector<uint32_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0u);
     std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+        const uint32_t sa = scene_of[ids[a]], sb = scene_of[ids[b]];
+        if (sa != sb) return sa < sb;
         return keys[a] != keys[b] ? keys[a] < keys[b] : ids[a] < ids[b];
     });
     for (uint32_t k = 0; k < n; ++k) {
@@ -1114,7 +1272,10 @@ int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_time *out, 
     const bool saved_loop = s->device_loop;
     s->device_loop = false;
     s->prof = P.get();
-    if (s->type != VTP_SOLVER_PBF) CU(cudaMemsetAsync(s->solve, 0, 2 * sizeof(vtp::SolveState), s->st));
+    if (s->type != VTP_SOLVER_PBF) {
+        CU(cudaMemsetAsync(s->solve, 0, 2 * s->scenes.size() * sizeof(vtp::SolveState), s->st));
+        CU(cudaMemsetAsync(s->loop, 0, 2 * sizeof(vtp::LoopState), s->st));
+    }
     for (uint32_t k = 0; k < n && rc == VTP_OK; ++k) {
         rc = s->enqueue_tick(s->st, false);
         s->sim_time += s->dt;

@@ -44,6 +44,49 @@ __device__ __forceinline__ uint32_t cell_key(int3 c, const Grid &g) {
     return (uint32_t)c.z * (uint32_t)(g.gy * g.gx) + (uint32_t)c.y * (uint32_t)g.gx + (uint32_t)c.x;
 }
 
+// One scene of a solver.  A solver advances S >= 1 independent scenes that
+// share the particle radius, time step and material constants but have their
+// own domain (simSpaceLB / simSpaceSize) and gravity.  Each scene owns the
+// global key buckets [key_base, key_base + nkey]; the last one is its
+// "outside" bucket, so a scene's rows stay in one fixed contiguous range of
+// the sorted order.  With S = 1 this is exactly the reference's single grid.
+struct SceneGrid {
+    float lbx, lby, lbz;
+    int gx, gy, gz;
+    uint32_t key_base;
+    uint32_t nkey;             // buckets of in-grid cells (outside bucket excluded)
+    float grav_x, grav_y, grav_z;
+    uint32_t pad_;
+};
+
+// Shared neighbour-search constants plus the per-row scene map.
+struct Scenes {
+    const SceneGrid *sg;       // [S]
+    const uint16_t *row_scene; // [n] scene of each row (rows never change scene)
+    float cell;
+    float d2max;
+    uint32_t maxnbr;
+};
+
+__device__ __forceinline__ int3 cell_of(float x, float y, float z, const SceneGrid &g, float cell) {
+    return make_int3((int)floorf(__fdiv_rn(__fsub_rn(x, g.lbx), cell)),
+                     (int)floorf(__fdiv_rn(__fsub_rn(y, g.lby), cell)),
+                     (int)floorf(__fdiv_rn(__fsub_rn(z, g.lbz), cell)));
+}
+
+__device__ __forceinline__ bool cell_available(int3 c, const SceneGrid &g) {
+    return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x <= g.gx && c.y <= g.gy && c.z <= g.gz;
+}
+
+// Scene-local linear cell id (the reference's cell index inside that scene's grid).
+__device__ __forceinline__ uint32_t cell_key(int3 c, const SceneGrid &g) {
+    return (uint32_t)c.z * (uint32_t)(g.gy * g.gx) + (uint32_t)c.y * (uint32_t)g.gx + (uint32_t)c.x;
+}
+
+__device__ __forceinline__ SceneGrid load_scene(const Scenes &sc, uint32_t row) {
+    return sc.sg[sc.row_scene[row]];
+}
+
 // Squared distance with a fixed FMA pattern; the neighbour-membership test
 // `0 < |x_i - x_j| <= cell` (UGNSCudaImpl.cu:194) is evaluated as
 // d2 > 0 && d2 <= d2max, which is equivalent for a correctly rounded sqrt.

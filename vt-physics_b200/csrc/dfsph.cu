@@ -124,108 +124,151 @@ __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
     a.alpha[r] = alpha;
 }
 
+// Tile kernels run a persistent grid over the scene-offset tiles; a tile of a
+// scene whose solve has stopped is skipped (block-uniform test).
 template <bool MULTI, int U>
 __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    double contrib = 0.0;
-    int obj = 0;
-    if (r < a.nf) {
-        const float4 p = a.pos[r];
-        const float4 vi = a.vadv[r];
-        const uint32_t n = a.ncnt[r];
-        float d = a.ratio[r] - 1.f;
-        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return PV{ldg4(a.pos + j), ldg4(a.vadv + j)}; },
-                    [&](uint32_t, const PV &e) {
-                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                        const float g = cubic_g(dist2(rx, ry, rz), a.k);
-                        const float dot = g * (rx * (vi.x - e.v.x) + ry * (vi.y - e.v.y) + rz * (vi.z - e.v.z));
-                        d = __fmaf_rn(dot * e.q.w, a.dt, d);
-                    });
-        if (d < 0.f) d = 0.f;
-        a.delta[r] = d;
-        a.kappa[r] = d / a.alpha[r] * a.inv_dt2 / p.w;
-        contrib = (double)d;
-        if (MULTI) obj = a.obj_of[a.orig[r]];
-    }
-    if (!MULTI) {
-        double s = block_sum(contrib);
-        if (threadIdx.x == 0) a.partials[blockIdx.x] = s;
-    } else {
-        for (int o = 0; o < a.nobj; ++o) {
-            double s = block_sum(obj == o ? contrib : 0.0);
-            if (threadIdx.x == 0) a.partials[(size_t)blockIdx.x * a.nobj + o] = s;
+    for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        const uint4 tile = a.tiles[t];
+        if (a.state[tile.z].stopped) continue;
+        const uint32_t r = tile.x + threadIdx.x;
+        double contrib = 0.0;
+        int obj = 0;
+        if (threadIdx.x < tile.y) {
+            const float4 p = a.pos[r];
+            const float4 vi = a.vadv[r];
+            const uint32_t n = a.ncnt[r];
+            float d = a.ratio[r] - 1.f;
+            const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+            nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                        [&](uint32_t j) { return PV{ldg4(a.pos + j), ldg4(a.vadv + j)}; },
+                        [&](uint32_t, const PV &e) {
+                            const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                            const float g = cubic_g(dist2(rx, ry, rz), a.k);
+                            const float dot =
+                                g * (rx * (vi.x - e.v.x) + ry * (vi.y - e.v.y) + rz * (vi.z - e.v.z));
+                            d = __fmaf_rn(dot * e.q.w, a.dt, d);
+                        });
+            if (d < 0.f) d = 0.f;
+            a.delta[r] = d;
+            a.kappa[r] = d / a.alpha[r] * a.inv_dt2 / p.w;
+            contrib = (double)d;
+            if (MULTI) obj = (int)a.obj_of[a.orig[r]] - (int)a.scene_tiles[tile.z].obj0;
+        }
+        if (!MULTI) {
+            double s = block_sum(contrib);
+            if (threadIdx.x == 0) a.partials[t] = s;
+        } else {
+            const int no = (int)a.scene_tiles[tile.z].nobj;
+            for (int o = 0; o < no; ++o) {
+                double s = block_sum(obj == o ? contrib : 0.0);
+                if (threadIdx.x == 0) a.partials[(size_t)t * a.nobj_max + o] = s;
+            }
         }
     }
 }
 
 template <int U>
 __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const float4 p = a.pos[r];
-    float4 v = a.vadv[r];
-    const float ki = a.kappa[r];
-    const uint32_t n = a.ncnt[r];
-    const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
-    const float ci = a.dt * p.w / mi;   // dt V_i / m_i
-    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
-    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
-                [&](uint32_t j) { return PK{ldg4(a.pos + j), j < a.nf ? __ldg(a.kappa + j) : 0.f}; },
-                [&](uint32_t, const PK &e) {
-                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                    const float g = cubic_g(dist2(rx, ry, rz), a.k);
-                    const float s = ci * e.q.w * (ki + e.k) * g;
-                    v.x = __fmaf_rn(-s, rx, v.x);
-                    v.y = __fmaf_rn(-s, ry, v.y);
-                    v.z = __fmaf_rn(-s, rz, v.z);
-                });
-    a.vadv[r] = v;
-}
-
-__global__ void k_solve_begin(SolveState *s) {
-    if (threadIdx.x == 0) {
-        s->iter = 0;
-        s->stopped = 0;
+    for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        const uint4 tile = a.tiles[t];
+        if (a.state[tile.z].stopped || threadIdx.x >= tile.y) continue;
+        const uint32_t r = tile.x + threadIdx.x;
+        const float4 p = a.pos[r];
+        float4 v = a.vadv[r];
+        const float ki = a.kappa[r];
+        const uint32_t n = a.ncnt[r];
+        const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
+        const float ci = a.dt * p.w / mi;   // dt V_i / m_i
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
+        nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
+                    [&](uint32_t j) { return PK{ldg4(a.pos + j), j < a.nf ? __ldg(a.kappa + j) : 0.f}; },
+                    [&](uint32_t, const PK &e) {
+                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+                        const float s = ci * e.q.w * (ki + e.k) * g;
+                        v.x = __fmaf_rn(-s, rx, v.x);
+                        v.y = __fmaf_rn(-s, ry, v.y);
+                        v.z = __fmaf_rn(-s, rz, v.z);
+                    });
+        a.vadv[r] = v;
     }
 }
 
+__global__ void k_solve_begin(SolveState *s, LoopState *loop, int nscenes) {
+    for (int i = threadIdx.x; i < nscenes; i += blockDim.x) {
+        s[i].iter = 0;
+        s[i].stopped = 0;
+    }
+    if (threadIdx.x == 0) {
+        loop->done = 0;
+        loop->active = 0;
+        loop->running = 1;
+        loop->iters = 0;
+    }
+}
+
+// One block per scene: FP64 residual of the scene from its tiles' partials,
+// the stop test, and (last block to finish) the loop condition.
 __global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__restrict__ partials,
                                                    uint32_t *status) {
-    double acc = 0.0;
-    for (int o = 0; o < c.nobj; ++o) {
-        double s = 0.0;
-        for (uint32_t b = threadIdx.x; b < c.nblocks; b += blockDim.x) s += partials[(size_t)b * c.nobj + o];
-        s = block_sum(s);
-        if (threadIdx.x == 0) acc += s * c.inv_count[o];
+    SolveState *st = c.state + blockIdx.x;
+    const SceneTiles sct = c.scene_tiles[blockIdx.x];
+    __shared__ uint32_t was_stopped;
+    if (threadIdx.x == 0) was_stopped = st->stopped;
+    __syncthreads();
+    bool active = false;
+    if (!was_stopped) {
+        double acc = 0.0;
+        for (uint32_t o = 0; o < sct.nobj; ++o) {
+            double s = 0.0;
+            for (uint32_t b = threadIdx.x; b < sct.ntiles; b += blockDim.x)
+                s += partials[(size_t)(sct.tile0 + b) * c.nobj_max + o];
+            s = block_sum(s);
+            if (threadIdx.x == 0) acc += s * c.inv_count[sct.obj0 + o];
+        }
+        if (threadIdx.x == 0) {
+            const double residual = sct.nobj ? acc / (double)sct.nobj : 0.0;
+            const uint32_t iter = st->iter + 1;
+            st->iter = iter;
+            st->residual = residual;
+            uint32_t force = c.force_iters;
+            if (c.force_seq && c.tick) {
+                const uint64_t t = *c.tick;
+                if (t < c.force_seq_len) force = c.force_seq[2 * t + c.which];
+            }
+            bool stop;
+            if (force > 0) stop = iter >= force;
+            else stop = (residual < (double)c.threshold) || iter > c.max_iters - 1;
+            if (!(residual == residual)) {  // NaN residual: stop and flag
+                stop = true;
+                atomicOr(status, ST_NAN);
+            }
+            st->stopped = stop ? 1u : 0u;
+            if (stop) {
+                st->last_iters = iter;
+                st->total_iters += iter;
+                // vfsph_div / vfsph_incomp flag a crash whenever the loop ran past 100 iterations.
+                if (force == 0 && iter > c.max_iters - 1) atomicOr(status, ST_NOT_CONVERGED);
+            }
+            active = !stop;
+        }
     }
     if (threadIdx.x != 0) return;
-    SolveState *st = c.state;
-    const double residual = acc / (double)c.nobj;
-    const uint32_t iter = st->iter + 1;
-    st->iter = iter;
-    st->residual = residual;
-    uint32_t force = c.force_iters;
-    if (c.force_seq && c.tick) {
-        const uint64_t t = *c.tick;
-        if (t < c.force_seq_len) force = c.force_seq[2 * t + c.which];
+    if (active) atomicAdd(&c.loop->active, 1u);
+    __threadfence();
+    const uint32_t prev = atomicAdd(&c.loop->done, 1u);
+    if (prev + 1 == gridDim.x) {
+        __threadfence();
+        const uint32_t act = atomicAdd(&c.loop->active, 0u);
+        c.loop->done = 0;
+        c.loop->active = 0;
+        c.loop->iters += 1;
+        c.loop->total += 1;
+        c.loop->running = act ? 1u : 0u;
+        if (c.use_cond) cudaGraphSetConditional(c.cond, act ? 1u : 0u);
     }
-    bool stop;
-    if (force > 0) stop = iter >= force;
-    else stop = (residual < (double)c.threshold) || iter > c.max_iters - 1;
-    if (!(residual == residual)) {  // NaN residual: stop and flag
-        stop = true;
-        atomicOr(status, ST_NAN);
-    }
-    st->stopped = stop ? 1u : 0u;
-    if (stop) {
-        st->last_iters = iter;
-        st->total_iters += iter;
-        // vfsph_div / vfsph_incomp flag a crash whenever the loop ran past 100 iterations.
-        if (force == 0 && iter > c.max_iters - 1) atomicOr(status, ST_NOT_CONVERGED);
-    }
-    if (c.use_cond) cudaGraphSetConditional(c.cond, stop ? 0u : 1u);
 }
 
 template <bool TENSION_SPLIT, int U>
@@ -263,7 +306,8 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
                         nz = __fmaf_rn(sn, rz, nz);
                     }
                 });
-    const float accx = a.gravity.x + ax, accy = a.gravity.y + ay, accz = a.gravity.z + az;
+    const SceneGrid &sg = a.sc.sg[a.sc.row_scene[r]];
+    const float accx = sg.grav_x + ax, accy = sg.grav_y + ay, accz = sg.grav_z + az;
     if (TENSION_SPLIT) {
         a.acc_tmp[r] = make_float4(accx, accy, accz, 0.f);
         a.normal[r] = make_float4(nx, ny, nz, 0.f);
@@ -332,7 +376,16 @@ inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
 
-uint32_t dfsph_partial_blocks(uint32_t nf, int block) { return nblk(nf, block); }
+unsigned dfsph_tile_grid(uint32_t ntiles, int block) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const uint32_t resident = (uint32_t)sms * (uint32_t)(2048 / block);
+    return ntiles == 0 ? 1u : (ntiles < resident ? ntiles : resident);
+}
 
 void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
                         float *rest_density_b) {
@@ -349,18 +402,20 @@ void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bnc
 void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block) {
     if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_ratio_alpha<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
 }
-void dfsph_solve_begin(cudaStream_t st, SolveState *s) { k_solve_begin<<<1, 32, 0, st>>>(s); }
+void dfsph_solve_begin(cudaStream_t st, SolveState *s, LoopState *loop, int nscenes) {
+    k_solve_begin<<<1, 256, 0, st>>>(s, loop, nscenes);
+}
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
-    unsigned nb = nblk(a.nf, block);
-    if (nb == 0) nb = 1;
-    if (a.nobj > 1) VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<true, UU><<<nb, block, 0, st>>>(a))
+    const unsigned nb = dfsph_tile_grid(a.ntiles, block);
+    if (a.nobj_max > 1) VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<true, UU><<<nb, block, 0, st>>>(a))
     else VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<false, UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
-    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
+    const unsigned nb = dfsph_tile_grid(a.ntiles, block);
+    VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
-    k_solve_end<<<1, 256, 0, st>>>(c, partials, status);
+    k_solve_end<<<c.nscenes, 256, 0, st>>>(c, partials, status);
 }
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block) {
     if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_viscosity<false, UU><<<nblk(a.nf, block), block, 0, st>>>(a))

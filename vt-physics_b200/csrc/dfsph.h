@@ -5,9 +5,7 @@
 
 namespace vtp {
 
-constexpr int kMaxFluidObjects = 8;
-
-// Device-side state of one pressure solve (divergence or density).
+// Device-side state of one pressure solve (divergence or density) of one scene.
 struct SolveState {
     uint32_t iter;          // iterations done in the current solve
     uint32_t stopped;       // 1 once the current solve has stopped
@@ -15,6 +13,24 @@ struct SolveState {
     uint32_t pad_;
     uint64_t total_iters;   // summed since the counters were cleared
     double residual;        // last FP64 residual
+};
+
+// State of the batched solve loop of one solve kind (all scenes of a solver
+// iterate together; a scene that has stopped is skipped until all have).
+struct LoopState {
+    uint32_t done;          // solve_end blocks finished in the current iteration
+    uint32_t active;        // scenes still iterating after the current iteration
+    uint32_t running;       // 1 while any scene iterates (read by the host loop)
+    uint32_t iters;         // loop iterations of the current solve
+    uint64_t total;         // loop iterations since the counters were cleared
+};
+
+// Scene-offset tiles: tile t covers fluid rows [row0, row0 + rows) of one
+// scene, so per-block residual partial sums never mix scenes and split each
+// scene's rows exactly as a solver holding that scene alone would.
+struct SceneTiles {
+    uint32_t tile0, ntiles; // the scene's tiles
+    uint32_t obj0, nobj;    // the scene's fluid objects (global slots)
 };
 
 struct DfsphArgs {
@@ -25,7 +41,6 @@ struct DfsphArgs {
     float rho0, rho_b, mass_f, vol_f;
     float vis_coef;         // (nu + nu) / 2 * m_f / rho0
     float h2_001;           // 0.001 h^2
-    float3 gravity;
     float gamma;            // surface tension coefficient
     float csigma, h6_64;    // tension spline constants
     const uint32_t *nbr, *ncnt;
@@ -35,9 +50,14 @@ struct DfsphArgs {
     float *ratio, *alpha, *kappa, *delta;
     float4 *acc_tmp, *normal;   // tension path only
     const uint32_t *orig;       // sorted row -> attach id
-    const uint16_t *obj_of;     // attach id -> fluid object slot (multi-object only)
-    int nobj;                   // fluid objects (>= 1)
-    double *partials;           // [blocks][nobj]
+    const uint16_t *obj_of;     // attach id -> fluid object slot (multi-object scenes only)
+    int nobj_max;               // most fluid objects in one scene (>= 1)
+    double *partials;           // [tiles][nobj_max]
+    const uint4 *tiles;         // {row0, rows, scene, 0}
+    uint32_t ntiles;
+    const SceneTiles *scene_tiles;  // [S]
+    const SolveState *state;    // [S] states of the running solve (stopped scenes are skipped)
+    Scenes sc;                  // per-scene gravity
     uint32_t *status;
     uint64_t *tick;             // substep counter, advanced by the finalize pass
     int unroll;                 // neighbours in flight per thread (1, 2, 4, 8)
@@ -45,10 +65,12 @@ struct DfsphArgs {
 };
 
 struct SolveCtl {
-    SolveState *state;
-    const double *inv_count;    // [nobj] 1 / object size
-    int nobj;
-    uint32_t nblocks;           // partial rows
+    SolveState *state;          // [S]
+    LoopState *loop;
+    const double *inv_count;    // [fluid objects] 1 / object size
+    const SceneTiles *scene_tiles;  // [S]
+    int nscenes;
+    int nobj_max;               // partials per tile
     float threshold;
     uint32_t force_iters;       // 0 = residual test
     const uint32_t *force_seq;  // optional per-substep [div, incomp] counts (device)
@@ -63,7 +85,7 @@ struct SolveCtl {
 void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
                         float *rest_density_b);
 void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block);
-void dfsph_solve_begin(cudaStream_t st, SolveState *s);
+void dfsph_solve_begin(cudaStream_t st, SolveState *s, LoopState *loop, int nscenes);
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status);
@@ -71,6 +93,7 @@ void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_finalize(cudaStream_t st, const DfsphArgs &a);
-uint32_t dfsph_partial_blocks(uint32_t nf, int block);
+// Persistent grid for the tile kernels: enough blocks to fill the GPU.
+unsigned dfsph_tile_grid(uint32_t ntiles, int block);
 
 }  // namespace vtp

@@ -854,8 +854,8 @@ void immct_color(vtp_solver &s, const float *frac_attach_order, float *rgb) {
         }
 }
 
-void immct_solve_ab(vtp_solver &s, cudaStream_t st, int /*which*/) {
-    vtp::DfsphArgs a = s.dfsph_args();
+void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which) {
+    vtp::DfsphArgs a = s.dfsph_args(which);
     a.rest_density = s.imm->rd;
     vtp::dfsph_solve_a(st, a, s.block);
     vtp::dfsph_solve_b(st, a, s.block);
@@ -873,8 +873,8 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
     carry.src4[0] = s.vadv.c();
     carry.dst4[0] = s.vadv.n();
     immct_fill_carry(s, carry);
-    vtp::ugns_sort(st, s.grid, 0, nf, s.pos.c(), s.pos.n(), s.vel.c(), s.vel.n(), s.orig.c(), s.orig.n(), carry, 0.f,
-                   make_float3(0, 0, 0), s.u, s.u.fstart, s.prof);
+    vtp::ugns_sort(st, s.scn(), s.nbuckets, 0, nf, s.pos.c(), s.pos.n(), s.vel.c(), s.vel.n(), s.orig.c(),
+                   s.orig.n(), carry, 0.f, s.u, s.u.fstart, s.prof);
     s.pos.swap(); s.vel.swap(); s.orig.swap(); s.vadv.swap();
     for (int k = 0; k < P; ++k) m.vph[k].swap(), m.frac[k].swap();
     for (int c = 0; c < 9; ++c) m.Q[c].swap();
@@ -885,7 +885,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
         s.launches_per_tick += 1;
     };
     P_("ugns_lists", [&] {
-        vtp::ugns_build_lists(st, s.grid, s.L, 0, nf, s.pos.c(), s.orig.c(), s.u, s.u.nbr, s.u.ncnt, s.d_status,
+        vtp::ugns_build_lists(st, s.scn(), s.L, 0, nf, s.pos.c(), s.orig.c(), s.u, s.u.nbr, s.u.ncnt, s.d_status,
                               s.d_overflow, B);
     });
     s.launches_per_tick += 7;

@@ -21,9 +21,9 @@ struct Layout {
 struct UgnsBuffers {
     uint32_t *key = nullptr;       // [nf] cell key per old slot
     uint32_t *rank = nullptr;      // [nf] arrival rank within the cell (atomic)
-    uint32_t *count = nullptr;     // [nkey + 1]
-    uint32_t *fstart = nullptr;    // [nkey + 2] fluid cell starts (absolute rows)
-    uint32_t *bstart = nullptr;    // [nkey + 2] boundary cell starts (absolute rows)
+    uint32_t *count = nullptr;     // [nbuckets] (all scenes' buckets incl. their outside buckets)
+    uint32_t *fstart = nullptr;    // [nbuckets + 1] fluid cell starts (absolute rows)
+    uint32_t *bstart = nullptr;    // [nbuckets + 1] boundary cell starts (absolute rows)
     uint32_t *tmp_src = nullptr;   // [max(nf, nb)] scattered: old slot
     uint32_t *tmp_orig = nullptr;  // [max(nf, nb)] scattered: attach id
     uint32_t *tmp_key = nullptr;   // [max(nf, nb)] scattered: key
@@ -65,18 +65,19 @@ struct Profiler {
 };
 
 // --- ugns.cu ---
-// Sort rows [row0, row0 + cnt) by (cell, attach id) into the output arrays;
-// `start` receives the cell-start table (absolute rows).  With `force_dt` > 0
-// the rows' positions get v += g dt; x += v dt applied first (PBF external
+// Sort rows [row0, row0 + cnt) by (scene, cell, attach id) into the output
+// arrays; `start` receives the cell-start table (absolute rows) over all
+// `nbuckets` buckets.  With `force_dt` > 0 the rows' positions get
+// v += g dt; x += v dt applied first with their scene's gravity (PBF external
 // force fused into the sort).
-void ugns_sort(cudaStream_t st, const Grid &g, uint32_t row0, uint32_t cnt,
+void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t row0, uint32_t cnt,
                const float4 *pos_in, float4 *pos_out, const float4 *vel_in, float4 *vel_out,
                const uint32_t *orig_in, uint32_t *orig_out, const Carry &carry,
-               float force_dt, float3 gravity, UgnsBuffers &u, uint32_t *start, Profiler *prof = nullptr);
+               float force_dt, UgnsBuffers &u, uint32_t *start, Profiler *prof = nullptr);
 
 // Build the neighbour lists of rows [row0, row0 + cnt) (reference order:
 // 27 offsets, then ascending attach id inside a cell).
-void ugns_build_lists(cudaStream_t st, const Grid &g, const Layout &L, uint32_t row0, uint32_t cnt,
+void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32_t row0, uint32_t cnt,
                       const float4 *pos, const uint32_t *orig, const UgnsBuffers &u,
                       uint32_t *nbr, uint32_t *ncnt, uint32_t *status, uint32_t *overflow, int block);
 
@@ -93,7 +94,7 @@ void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base);
 void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
                       const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
                       uint32_t *out_nbr);
-void export_sorted(cudaStream_t st, const Grid &g, uint32_t n, const float4 *pos, const uint32_t *orig,
+void export_sorted(cudaStream_t st, const Scenes &sc, uint32_t n, const float4 *pos, const uint32_t *orig,
                    uint32_t *out_ids, uint32_t *out_keys);
 
 }  // namespace vtp

@@ -30,11 +30,23 @@ struct DB {
 struct ObjRec {
     std::string name;
     int mat = 0;
+    uint32_t scene = 0;
     uint32_t start = 0, end = 0;
     bool export_flag = false;
     float vel0[3] = {0, 0, 0};
     float color[3] = {0, 0, 0};
     std::vector<float> phase;
+};
+
+// One scene of a solver: its own domain and gravity (everything else is shared).
+struct SceneRec {
+    float lb[3] = {0, 0, 0}, size[3] = {0, 0, 0};
+    float3 gravity = make_float3(0.f, -9.8f, 0.f);
+    // filled at initialize
+    uint32_t nf = 0, nb = 0;       // fluid / boundary particles
+    uint32_t fbase = 0, bbase = 0; // first fluid row, first boundary row (absolute)
+    uint32_t attach_lo = 0;        // smallest attach id of the scene's particles
+    vtp::SceneGrid grid{};
 };
 
 struct vtp_solver {
@@ -69,7 +81,16 @@ struct vtp_solver {
 
     // device state
     cudaStream_t st = nullptr, side = nullptr;
-    vtp::Grid grid{};
+    std::vector<SceneRec> scenes;       // scene 0 comes from setConfig, the rest from add_scene
+    vtp::SceneGrid *d_sg = nullptr;     // [S]
+    uint16_t *row_scene = nullptr;      // [n]
+    uint32_t nbuckets = 0;              // cell buckets of all scenes incl. their outside buckets
+    float d2max = 0.f;
+    uint4 *d_tiles = nullptr;           // scene-offset tiles of the fluid rows
+    uint32_t ntiles = 0;
+    vtp::SceneTiles *d_scene_tiles = nullptr;
+    int nobj_max = 1;
+    vtp::LoopState *loop = nullptr;     // [2]: divergence, density
     vtp::Layout L{};
     vtp::Cubic kc{};
     DB<float4> pos, vel, vadv;
@@ -79,11 +100,10 @@ struct vtp_solver {
     float4 *acc_tmp = nullptr, *normal = nullptr;
     double *partials = nullptr, *inv_count = nullptr;
     uint16_t *obj_of = nullptr;
-    vtp::SolveState *solve = nullptr;   // [2]: divergence, density
+    vtp::SolveState *solve = nullptr;   // [2][S]: divergence, density per scene
     vtp::UgnsBuffers u{};
     uint32_t *d_status = nullptr, *d_overflow = nullptr;
     uint32_t *h_pinned = nullptr;       // [4] status, overflow, iter, spare
-    int nobj_fluid = 1;
     std::shared_ptr<vtp::ImmState> imm;
 
     // graphs: two parities (double-buffer swaps alternate between substeps)
@@ -101,6 +121,7 @@ struct vtp_solver {
 
     uint64_t steps_done = 0;
     vtp_stats stats{};
+    std::vector<vtp_stats> scene_stats;
 
     std::vector<void *> allocs;
 
@@ -141,6 +162,9 @@ struct vtp_solver {
     }
 
     int parse_config(const nlohmann::json &c);
+    int add_scene(const nlohmann::json &c, uint32_t *index);
+    int nscenes() const { return (int)scenes.size(); }
+    vtp::Scenes scn() const { return vtp::Scenes{d_sg, row_scene, h, d2max, maxnbr}; }
     int attach(const float *p, uint32_t n, const float *v, const nlohmann::json &o);
     int initialize();
     int tick_n(uint32_t n);
@@ -151,9 +175,10 @@ struct vtp_solver {
     int get_field(int f, void *host, size_t bytes);
     int set_field(int f, const void *host, size_t bytes);
     vtp::PbfArgs pbf_args();
-    vtp::DfsphArgs dfsph_args();
+    vtp::DfsphArgs dfsph_args(int which = 0);
     vtp::SolveCtl solve_ctl(int which, cudaGraphConditionalHandle h, int use_cond);
     int check_status();
+    int read_solve_states();
     int sync_parity();
 };
 

@@ -34,18 +34,19 @@ __device__ __forceinline__ float4 apply_force(float4 p, float4 &v, float dt, flo
     return p;
 }
 
-__global__ void k_hash(Grid g, uint32_t row0, uint32_t cnt, const float4 *__restrict__ pos,
-                       const float4 *__restrict__ vel, float force_dt, float3 grav,
-                       uint32_t *__restrict__ key, uint32_t *__restrict__ rank, uint32_t *__restrict__ count) {
+__global__ void k_hash(Scenes sc, uint32_t row0, uint32_t cnt, const float4 *__restrict__ pos,
+                       const float4 *__restrict__ vel, float force_dt, uint32_t *__restrict__ key,
+                       uint32_t *__restrict__ rank, uint32_t *__restrict__ count) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
+    const SceneGrid g = load_scene(sc, row0 + i);
     float4 p = pos[row0 + i];
     if (force_dt > 0.f) {
         float4 v = vel[row0 + i];
-        p = apply_force(p, v, force_dt, grav);
+        p = apply_force(p, v, force_dt, make_float3(g.grav_x, g.grav_y, g.grav_z));
     }
-    int3 c = cell_of(p.x, p.y, p.z, g);
-    uint32_t k = cell_available(c, g) ? cell_key(c, g) : g.nkey;
+    int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
+    uint32_t k = g.key_base + (cell_available(c, g) ? cell_key(c, g) : g.nkey);
     key[i] = k;
     rank[i] = atomicAdd(&count[k], 1u);
 }
@@ -161,18 +162,20 @@ __global__ void k_scatter(uint32_t row0, uint32_t cnt, const uint32_t *__restric
     tmp_key[d] = k;
 }
 
-__global__ void k_rank_reorder(Grid g, uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ start,
+__global__ void k_rank_reorder(Scenes sc, uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ start,
                                const uint32_t *__restrict__ tmp_src, const uint32_t *__restrict__ tmp_orig,
                                const uint32_t *__restrict__ tmp_key, const float4 *__restrict__ pos_in,
                                float4 *__restrict__ pos_out, const float4 *__restrict__ vel_in,
                                float4 *__restrict__ vel_out, uint32_t *__restrict__ orig_out, Carry carry,
-                               float force_dt, float3 grav) {
+                               float force_dt) {
     uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= cnt) return;
+    // A row keeps its scene: slot d lies in the same scene range as its source row.
+    const SceneGrid g = load_scene(sc, row0 + d);
     uint32_t k = tmp_key[d];
     uint32_t my = tmp_orig[d];
     uint32_t dst = d;
-    if (k < g.nkey) {
+    if (k < g.key_base + g.nkey) {
         // Stable order inside the cell: rank by attach id.
         uint32_t s0 = start[k] - row0, s1 = start[k + 1] - row0;
         uint32_t r = 0;
@@ -182,7 +185,7 @@ __global__ void k_rank_reorder(Grid g, uint32_t row0, uint32_t cnt, const uint32
     uint32_t s = tmp_src[d];
     float4 p = pos_in[row0 + s];
     float4 v = vel_in[row0 + s];
-    if (force_dt > 0.f) p = apply_force(p, v, force_dt, grav);
+    if (force_dt > 0.f) p = apply_force(p, v, force_dt, make_float3(g.grav_x, g.grav_y, g.grav_z));
     pos_out[row0 + dst] = p;
     vel_out[row0 + dst] = v;
     orig_out[row0 + dst] = my;
@@ -233,7 +236,7 @@ struct Walker {
 };
 
 template <int MODE>
-__global__ void k_build_lists(Grid g, uint32_t row0, uint32_t cnt, uint32_t ell_stride,
+__global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t ell_stride,
                               const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
                               const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
                               uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt,
@@ -241,8 +244,9 @@ __global__ void k_build_lists(Grid g, uint32_t row0, uint32_t cnt, uint32_t ell_
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= cnt) return;
     uint32_t i = row0 + r;
+    const SceneGrid g = load_scene(sc, i);
     float4 p = pos[i];
-    int3 c = cell_of(p.x, p.y, p.z, g);
+    int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
     if (!cell_available(c, g)) {  // outside the grid: no neighbours, not even self
         ncnt[r] = 0;
         return;
@@ -251,16 +255,16 @@ __global__ void k_build_lists(Grid g, uint32_t row0, uint32_t cnt, uint32_t ell_
     w.px = p.x; w.py = p.y; w.pz = p.z;
     w.self = i;
     w.cnt = 1;
-    w.maxnbr = g.maxnbr;
+    w.maxnbr = sc.maxnbr;
     w.out = nbr + ell_index(r, 0, ell_stride);
     w.overflow = false;
-    const float d2max = g.d2max;
+    const float d2max = sc.d2max;
     for (int t = 0; t < 27; ++t) {
         int3 cc = c;
         int3 o = nbr_offset(t);
         cc.x += o.x; cc.y += o.y; cc.z += o.z;
         if (!cell_available(cc, g)) continue;
-        uint32_t k = cell_key(cc, g);
+        uint32_t k = g.key_base + cell_key(cc, g);
         uint32_t f0 = __ldg(fstart + k), f1 = __ldg(fstart + k + 1);
         uint32_t b0 = __ldg(bstart + k), b1 = __ldg(bstart + k + 1);
         if (MODE == 0) {
@@ -347,13 +351,14 @@ __global__ void k_export_neighbors(uint32_t row0, uint32_t cnt, uint32_t ell_str
     for (uint32_t t = 1; t < c; ++t) dst[t] = orig[nbr[ell_index(r, t - 1, ell_stride)]];
 }
 
-__global__ void k_export_sorted(Grid g, uint32_t n, const float4 *__restrict__ pos,
+__global__ void k_export_sorted(Scenes sc, uint32_t n, const float4 *__restrict__ pos,
                                 const uint32_t *__restrict__ orig, uint32_t *__restrict__ ids,
                                 uint32_t *__restrict__ keys) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const SceneGrid g = load_scene(sc, i);
     float4 p = pos[i];
-    int3 c = cell_of(p.x, p.y, p.z, g);
+    int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
     ids[i] = orig[i];
     keys[i] = cell_available(c, g) ? cell_key(c, g) : 0xffffffffu;
 }
@@ -386,17 +391,17 @@ static void scan_counts(cudaStream_t st, const uint32_t *count, size_t n, uint32
     k_scan_total<<<1, 32, 0, st>>>(count, n, out);
 }
 
-void ugns_sort(cudaStream_t st, const Grid &g, uint32_t row0, uint32_t cnt, const float4 *pos_in, float4 *pos_out,
-               const float4 *vel_in, float4 *vel_out, const uint32_t *orig_in, uint32_t *orig_out,
-               const Carry &carry, float force_dt, float3 gravity, UgnsBuffers &u, uint32_t *start, Profiler *prof) {
-    const size_t nb = (size_t)g.nkey + 1;  // buckets incl. the outside bucket
+void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t row0, uint32_t cnt,
+               const float4 *pos_in, float4 *pos_out, const float4 *vel_in, float4 *vel_out,
+               const uint32_t *orig_in, uint32_t *orig_out, const Carry &carry, float force_dt, UgnsBuffers &u,
+               uint32_t *start, Profiler *prof) {
+    const size_t nb = nbuckets;  // buckets incl. every scene's outside bucket
     auto B = [&] { if (prof) prof->begin(); };
     auto E = [&](const char *nm) { if (prof) prof->end_(nm); };
     B();
     cudaMemsetAsync(u.count, 0, nb * sizeof(uint32_t), st);
     if (cnt > 0) {
-        k_hash<<<nblk(cnt, 256), 256, 0, st>>>(g, row0, cnt, pos_in, vel_in, force_dt, gravity, u.key, u.rank,
-                                               u.count);
+        k_hash<<<nblk(cnt, 256), 256, 0, st>>>(sc, row0, cnt, pos_in, vel_in, force_dt, u.key, u.rank, u.count);
     }
     E("ugns_clear_hash");
     B();
@@ -408,27 +413,27 @@ void ugns_sort(cudaStream_t st, const Grid &g, uint32_t row0, uint32_t cnt, cons
                                               u.tmp_key);
     E("ugns_scatter");
     B();
-    k_rank_reorder<<<nblk(cnt, 256), 256, 0, st>>>(g, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
-                                                   pos_out, vel_in, vel_out, orig_out, carry, force_dt, gravity);
+    k_rank_reorder<<<nblk(cnt, 256), 256, 0, st>>>(sc, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
+                                                   pos_out, vel_in, vel_out, orig_out, carry, force_dt);
     E("ugns_rank_reorder");
 }
 
-void ugns_build_lists(cudaStream_t st, const Grid &g, const Layout &L, uint32_t row0, uint32_t cnt,
+void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32_t row0, uint32_t cnt,
                       const float4 *pos, const uint32_t *orig, const UgnsBuffers &u, uint32_t *nbr, uint32_t *ncnt,
                       uint32_t *status, uint32_t *overflow, int block) {
     if (cnt == 0) return;
     unsigned nb = nblk(cnt, block);
     switch (L.merge_mode) {
         case 0:
-            k_build_lists<0><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            k_build_lists<0><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
         case 1:
-            k_build_lists<1><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            k_build_lists<1><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
         default:
-            k_build_lists<2><<<nb, block, 0, st>>>(g, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            k_build_lists<2><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
     }
@@ -457,9 +462,9 @@ void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t 
         k_export_neighbors<<<nblk(cnt, 256), 256, 0, st>>>(row0, cnt, L.ell_stride, nbr, ncnt, orig, maxnbr, out_cnt,
                                                            out_nbr);
 }
-void export_sorted(cudaStream_t st, const Grid &g, uint32_t n, const float4 *pos, const uint32_t *orig,
+void export_sorted(cudaStream_t st, const Scenes &sc, uint32_t n, const float4 *pos, const uint32_t *orig,
                    uint32_t *out_ids, uint32_t *out_keys) {
-    if (n) k_export_sorted<<<nblk(n, 256), 256, 0, st>>>(g, n, pos, orig, out_ids, out_keys);
+    if (n) k_export_sorted<<<nblk(n, 256), 256, 0, st>>>(sc, n, pos, orig, out_ids, out_keys);
 }
 
 }  // namespace vtp

@@ -37,6 +37,8 @@ SIGNATURES = {
     "vtp_solver_set_config": (C.c_int, [_P, C.c_char_p]),
     "vtp_solver_attach_object": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_char_p]),
     "vtp_solver_initialize": (C.c_int, [_P]),
+    "vtp_solver_add_scene": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_uint32)]),
+    "vtp_solver_get_scene_stats": (C.c_int, [_P, C.c_uint32, _P]),
     "vtp_solver_tick_n_steps": (C.c_int, [_P, C.c_uint32]),
     "vtp_solver_run": (C.c_int, [_P]),
     "vtp_solver_reset": (C.c_int, [_P]),

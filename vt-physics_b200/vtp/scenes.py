@@ -206,6 +206,21 @@ def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, j
                                SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def batched_scenes(count: int = 64, n_pbf: int = 48, seed: int = 4242, gravity_seed: int = 4243,
+                   n_min: float = 4e3, n_max: float = 2.56e5) -> list:
+    """The batched mix: ``count`` dam breaks, the first ``n_pbf`` PBF and the rest DFSPH.
+
+    Fluid counts are log-uniform in [n_min, n_max] (SplitMix64 stream ``seed``), gravity
+    y is uniform in [-12, -8] (stream ``gravity_seed``), scene k is jittered with seed
+    4000 + k.  Box size scales with the fluid block so number density is constant.
+    """
+    u = splitmix64_uniform(seed, count)
+    ns = np.round(np.exp(np.log(n_min) + u * (np.log(n_max) - np.log(n_min)))).astype(np.int64)
+    g = -12.0 + 4.0 * splitmix64_uniform(gravity_seed, count)
+    return [dam_break("PBF" if k < n_pbf else "DFSPH", int(ns[k]), seed=4000 + k, gravity_y=float(g[k]))
+            for k in range(count)]
+
+
 def immct_config(*, dt, r, lb, size, rho=(1000.0, 1200.0), cf=1e-3, cd0=0.5, solvent_vis=0.01, vis_base=12.0,
                  vis_max=12.0, relax=0.05, thin=0.6, theta=0.4, div_thr=1e-4, incomp_thr=1e-4, tension=0.001,
                  colors=((255, 0, 0), (0, 0, 255)), gravity=(0.0, -9.81, 0.0), max_nbr=60, animation_time=5.0):

@@ -121,7 +121,13 @@ class Solver:
         return {"solverType": self.solver_type, "exportFlag": False, "velocityStart": [0, 0, 0],
                 "colorStart": [0, 1, 0]}
 
-    def attachObject(self, obj: Object) -> bool:
+    def addScene(self, config: dict) -> int:
+        """Add an independent scene (same shared parameters, own domain and gravity); returns its index."""
+        idx = C.c_uint32()
+        check(lib().vtp_solver_add_scene(self._h, json.dumps(config).encode(), C.byref(idx)), "addScene")
+        return idx.value
+
+    def attachObject(self, obj: Object, scene: int = 0) -> bool:
         pos = np.ascontiguousarray(obj.pos, dtype=np.float32).reshape(-1, 3)
         vel = None
         if obj.velocity is not None:
@@ -129,6 +135,8 @@ class Solver:
             assert vel.shape == pos.shape
         meta = {"name": obj.getName(), "ObjectComponentConfig": obj.getObjectComponentConfig(),
                 "SolverObjectComponentConfig": obj.getSolverObjectComponentConfig()}
+        if scene:
+            meta["scene"] = int(scene)
         code = lib().vtp_solver_attach_object(self._h, pos.ctypes.data, pos.shape[0],
                                               None if vel is None else vel.ctypes.data,
                                               json.dumps(meta).encode())
@@ -209,6 +217,11 @@ class Solver:
         check(lib().vtp_solver_get_stats(self._h, C.byref(s)), "get_stats")
         return s.as_dict()
 
+    def scene_stats(self, scene: int) -> dict:
+        s = VtpStats()
+        check(lib().vtp_solver_get_scene_stats(self._h, int(scene), C.byref(s)), "get_scene_stats")
+        return s.as_dict()
+
     def stage_times(self):
         a = (C.c_float * 3)()
         check(lib().vtp_solver_get_stage_times(self._h, a), "stage_times")
@@ -258,13 +271,7 @@ class SolverManager:
         return _CLASSES[solver_type](strict=strict)
 
 
-def solver_from_scene(scene: "scenes.Scene", extra: dict | None = None, strict: bool = True) -> Solver:
-    """Create, configure and attach a scene (convenience for tests and benchmarks)."""
-    s = _CLASSES[SOLVER_TYPES[scene.solver]](strict=strict)
-    cfg = json.loads(json.dumps(scene.config))
-    if extra:
-        cfg["B200"] = dict(extra)
-    s.setConfig(cfg)
+def _attach_scene_objects(s: Solver, scene: "scenes.Scene", index: int = 0):
     for o in scene.objects:
         obj = Object(Particle_Common, o.name)
         obj.getObjectComponentConfig()["epmMaterial"] = o.material
@@ -275,5 +282,41 @@ def solver_from_scene(scene: "scenes.Scene", extra: dict | None = None, strict: 
         obj.attachSpecificSolverObjectComponentConfig(sc)
         obj.pos = o.pos
         obj.velocity = o.velocity
-        s.attachObject(obj)
+        s.attachObject(obj, scene=index)
+
+
+def solver_from_scene(scene: "scenes.Scene", extra: dict | None = None, strict: bool = True) -> Solver:
+    """Create, configure and attach a scene (convenience for tests and benchmarks)."""
+    s = _CLASSES[SOLVER_TYPES[scene.solver]](strict=strict)
+    cfg = json.loads(json.dumps(scene.config))
+    if extra:
+        cfg["B200"] = dict(extra)
+    s.setConfig(cfg)
+    _attach_scene_objects(s, scene)
     return s
+
+
+def solver_from_scenes(scene_list, extra: dict | None = None, strict: bool = True):
+    """One solver advancing several scenes of the same solver type together.
+
+    Returns (solver, ranges) where ranges[k] = (start, end) is scene k's slice of the
+    attach order (objects are attached scene by scene).
+    """
+    kinds = {sc.solver for sc in scene_list}
+    if len(kinds) != 1:
+        raise ValueError("a batched solver holds scenes of one solver type")
+    s = _CLASSES[SOLVER_TYPES[scene_list[0].solver]](strict=strict)
+    ranges = []
+    start = 0
+    for k, sc in enumerate(scene_list):
+        cfg = json.loads(json.dumps(sc.config))
+        if extra:
+            cfg["B200"] = dict(extra)
+        if k == 0:
+            s.setConfig(cfg)
+        else:
+            s.addScene(cfg)
+        _attach_scene_objects(s, sc, k)
+        ranges.append((start, start + sc.n_total))
+        start += sc.n_total
+    return s, ranges
