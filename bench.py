@@ -38,7 +38,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k", "batched"], default="dfsph_1m")
+    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k", "batched", "diff_pbf"],
+                    default="dfsph_1m")
+    ap.add_argument("--checkpoint-every", type=int, default=20)
+    ap.add_argument("--fd-steps", type=int, default=20, help="diff_pbf: horizon of the finite-difference check")
+    ap.add_argument("--fd-directions", type=int, default=4)
     ap.add_argument("--no-loop-baseline", action="store_true",
                     help="batched workload: skip the plain per-scene loop it is compared with")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -46,6 +50,7 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--extra", default="", help='extra "B200" config keys as JSON, e.g. {"unroll": 2}')
     ap.add_argument("--scene-index", type=int, default=-1, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -261,7 +266,10 @@ def run_batched(args, rank, world, local, dist, torch):
     from vtp.dist import lpt_assign
     mix = vtp.scenes.batched_scenes()
     mine = sorted(lpt_assign([_batch_cost(m) for m in mix], world)[rank])
-    extra = {"blockSize": args.block} if args.block else None
+    extra = json.loads(args.extra) if args.extra else {}
+    if args.block:
+        extra["blockSize"] = args.block
+    extra = extra or None
     groups = {}
     for k in mine:
         groups.setdefault(mix[k].solver, []).append(k)
@@ -377,6 +385,103 @@ def run_batched(args, rank, world, local, dist, torch):
     return line
 
 
+def run_diff(args, torch) -> dict:
+    """Differentiable PBF, 64k fluid particles: forward with checkpoints every k substeps, then the
+    adjoint (per-segment recompute + hand-written adjoint passes).  value = adjoint throughput;
+    config carries the forward throughput and the adjoint / forward cost ratio, and an FD check of
+    the adjoint (FP64 CPU oracle, lists frozen to the GPU's) over a shorter horizon."""
+    import numpy as np
+    import vtp
+    from vtp import diff
+    sc = vtp.scenes.diff_pbf()
+    mask = diff.fluid_mask(sc)
+    nf = int(mask.sum())
+    target = np.array([0.8, 0.2, 0.6])
+    extra = json.loads(args.extra) if args.extra else None
+
+    def loss_grad(pos):
+        m = pos[mask].astype(np.float64).mean(0)
+        g = np.zeros(pos.shape, np.float32)
+        g[mask] = 2.0 * (m - target) / nf
+        return float(((m - target) ** 2).sum()), g
+
+    s = diff.pbf_solver(sc, extra=extra)
+    if args.warmup:   # warm the graphs and kernels on a throwaway copy
+        w = diff.pbf_solver(sc, extra=extra)
+        diff.diff_forward(w, min(args.warmup, args.checkpoint_every), args.checkpoint_every)
+        _, g = loss_grad(w.get_field("pos"))
+        diff.diff_backward(w, g, None)
+        w.destroy()
+    # plain forward of the same rollout (no checkpoints): the cost the adjoint is compared with
+    p = diff.pbf_solver(sc, extra=extra)
+    p.tickNsteps(1)
+    p.destroy()
+    p = diff.pbf_solver(sc, extra=extra)
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
+    tp = time.perf_counter()
+    assert p.tickNsteps(args.steps), p.last_error
+    plain_s = time.perf_counter() - tp
+    p.destroy()
+    t0 = time.perf_counter()
+    diff.diff_forward(s, args.steps, args.checkpoint_every)
+    t1 = time.perf_counter()
+    loss, g = loss_grad(s.get_field("pos"))
+    t2 = time.perf_counter()
+    gx, gv, gk = diff.diff_backward(s, g, None)
+    t3 = time.perf_counter()
+    clocks = clk.stop()
+    fwd_s, bwd_s = t1 - t0, t3 - t2
+    s.destroy()
+    value = nf * args.steps / bwd_s / 1e6
+    cfg = {"workload": "diff_pbf", "fluid": nf, "boundary": int((~mask).sum()), "substeps": args.steps,
+           "checkpoint_every": args.checkpoint_every, "loss": loss, "dl_dxsph_k": gk,
+           "forward_value": nf * args.steps / plain_s / 1e6, "recorded_forward_value": nf * args.steps / fwd_s / 1e6,
+           "adjoint_over_forward": bwd_s / plain_s,
+           "grad_v0_norm": float(np.linalg.norm(gv[mask])),
+           "timing": "host wall clock around each synchronous C-ABI call (inputs resident on the device)",
+           "l2": "per-segment tapes (~0.5 GB) larger than L2"}
+    # FD check of the adjoint over a shorter horizon, FP64 CPU oracle with the GPU's frozen lists.
+    if args.fd_steps > 0 and args.fd_directions > 0:
+        from oracle import oracle as O
+        T = min(args.fd_steps, args.steps)
+        s = diff.pbf_solver(sc, extra=extra)
+        maxnbr = int(sc.config["PBF"]["Required"]["maxNeighborNum"])
+        diff.diff_forward(s, T, args.checkpoint_every, keep_lists=True)
+        lists = [diff.diff_lists(s, t, maxnbr) for t in range(T)]
+        _, g = loss_grad(s.get_field("pos"))
+        _, gv, gk = diff.diff_backward(s, g, None)
+        s.destroy()
+        d = O.PbfDiff(sc)
+        x0, v0 = d.base.pos.copy(), d.base.vel.copy()
+        rng = np.random.default_rng(5006)
+        k0 = d.p.xsph_k
+        errs = []
+        for _ in range(args.fd_directions):
+            dv = np.zeros_like(v0)
+            dv[mask] = rng.normal(size=(nf, 3))
+            dk = rng.normal()
+            nrm = np.sqrt((dv ** 2).sum() + dk * dk)
+            dv, dk = dv / nrm, dk / nrm
+
+            def L(e):
+                d.p.xsph_k = k0 + e * dk
+                x, _, _, _ = d.rollout(x0, v0 + e * dv, T, lists=lists)
+                d.p.xsph_k = k0
+                m = x[mask].mean(0)
+                return float(((m - target) ** 2).sum())
+            fd = (L(1e-4) - L(-1e-4)) / 2e-4
+            ad = float((gv.astype(np.float64) * dv).sum() + gk * dk)
+            errs.append(abs(ad - fd) / abs(fd))
+        cfg["fd_check"] = {"substeps": T, "directions": args.fd_directions, "eps": 1e-4,
+                           "max_rel_err": max(errs), "rel_errs": errs, "reference": "FP64 CPU oracle, frozen lists"}
+    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * bwd_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "clocks": clocks}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -403,6 +508,13 @@ def main():
 
     import vtp
     vtp.lib()
+    if args.workload == "diff_pbf":
+        if rank == 0:
+            print(json.dumps(run_diff(args, torch)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     if args.workload == "batched":
         line = run_batched(args, rank, world, local, dist, torch)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -422,7 +534,7 @@ def main():
             print(json.dumps(line), flush=True)
         return 0
     sc = make_scene(args.workload)
-    extra = {}
+    extra = json.loads(args.extra) if args.extra else {}
     if args.block:
         extra["blockSize"] = args.block
     s = vtp.solver_from_scene(sc, extra=extra or None)

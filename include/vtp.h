@@ -118,6 +118,9 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *   "deviceLoop": false drives the pressure-solve loops from the host;
  *   "useGraphs": false launches kernels one by one instead of a CUDA graph;
  *   "blockSize": threads per block of the neighbour passes (32..256);
+ *   "unroll": neighbour-list entries in flight per thread (1, 2, 4, 8);
+ *   "persistentTiles": true runs the pressure-solve passes as a persistent
+ *       grid looping over the scene-offset tiles (default: one block per tile);
  *   "stageTimers": true records CUDA-event stage times. */
 VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 
@@ -212,6 +215,28 @@ VTP_API int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_tim
 /* Number of kernel launches (graph kernel nodes included) issued by the last
  * tick_n_steps call. */
 VTP_API int vtp_solver_get_launch_count(vtp_solver *s, uint64_t *launches);
+
+/* Differentiable PBF (no counterpart in the reference; PBF solver, one scene).
+ *
+ * vtp_solver_diff_forward runs n_steps ordinary substeps from the current
+ * state, saving the fluid state every `checkpoint_every` substeps (and at
+ * the end).  With keep_lists != 0 every substep's neighbour lists are kept
+ * for vtp_solver_diff_lists (finite-difference checks with frozen lists).
+ *
+ * vtp_solver_diff_backward takes dL/d(positions) and dL/d(velocities) of
+ * the state after the recorded substeps (attach order, n_total x float[3];
+ * NULL = zero) and returns dL/d(positions) and dL/d(velocities) of the state
+ * before them (boundary rows 0) and dL/dXSPH_k (any output may be NULL).
+ * Each checkpoint segment is recomputed with the substep kernels into a
+ * tape (lists frozen per substep as the forward built them), then the
+ * hand-written adjoint passes run in reverse.  The solver is left at the
+ * forward's final state. */
+VTP_API int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists);
+VTP_API int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
+                                     float *dl_dvel0, double *dl_dxsph_k);
+/* Neighbour lists of recorded substep `step` in the layout of
+ * vtp_solver_get_neighbors (built after the substep's external force). */
+VTP_API int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr);
 
 /* Allocation-free neighbour search (no counterpart in the reference).
  *

@@ -1,0 +1,146 @@
+"""Differentiable PBF: the sm_100a adjoint against the FP64 CPU adjoint and FP64
+central finite differences, both with the neighbour lists frozen to the ones the
+GPU forward built (tolerance: 1e-3 relative, the differentiable-PBF target)."""
+import numpy as np
+import pytest
+
+from vtp import scenes
+
+TOL = 1e-3
+TARGET = np.array([0.8, 0.2, 0.6])
+
+
+def small_case(seed=7):
+    sc = scenes.dam_break("PBF", 400, seed=seed)
+    f = sc.objects[0]
+    rng = np.random.default_rng(seed)
+    f.velocity = rng.normal(0.0, 0.1, (f.n, 3)).astype(np.float32)
+    return sc
+
+
+def loss_grad(pos, mask, target):
+    m = pos[mask].astype(np.float64).mean(0)
+    g = np.zeros(pos.shape, np.float64)
+    g[mask] = 2.0 * (m - target) / mask.sum()
+    return float(((m - target) ** 2).sum()), g
+
+
+# ---------------------------------------------------------------- CPU: the FP64 adjoint itself
+
+def test_oracle_adjoint_matches_finite_differences(oracle_lib):
+    sc = small_case(3)
+    d = oracle_lib.PbfDiff(sc)
+    f = d.fluid
+    x0, v0 = d.base.pos.copy(), d.base.vel.copy()
+    T = 6
+    target = TARGET * 0.1
+    xT, _, states, used = d.rollout(x0, v0, T, record=True)
+    _, xbar = loss_grad(xT, f, target)
+    gx, gv, gk = d.adjoint(states, used, xbar, np.zeros_like(xbar))
+    rng = np.random.default_rng(11)
+    k0 = d.p.xsph_k
+    for _ in range(3):
+        dv = np.zeros_like(v0)
+        dv[f] = rng.normal(size=(f.sum(), 3))
+        dk = rng.normal()
+        nrm = np.sqrt((dv ** 2).sum() + dk * dk)
+        dv, dk = dv / nrm, dk / nrm
+
+        def L(s):
+            d.p.xsph_k = k0 + s * dk
+            x, _, _, _ = d.rollout(x0, v0 + s * dv, T, lists=used)
+            d.p.xsph_k = k0
+            return loss_grad(x, f, target)[0]
+        fd = (L(1e-4) - L(-1e-4)) / 2e-4
+        ad = float((gv * dv).sum() + gk * dk)
+        assert abs(ad - fd) <= 1e-6 * abs(fd) + 1e-14
+
+
+# ---------------------------------------------------------------- GPU: the library's adjoint
+
+@pytest.mark.gpu
+def test_gpu_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib):
+    from vtp import diff
+    sc = small_case(7)
+    mask = diff.fluid_mask(sc)
+    T, every = 10, 4
+    s = diff.pbf_solver(sc)
+    maxnbr = int(sc.config["PBF"]["Required"]["maxNeighborNum"])
+    diff.diff_forward(s, T, every, keep_lists=True)
+    lists = [diff.diff_lists(s, t, maxnbr) for t in range(T)]
+    target = TARGET * 0.1
+    _, dl = loss_grad(s.get_field("pos"), mask, target)
+    gx, gv, gk = diff.diff_backward(s, dl.astype(np.float32), None)
+    s.destroy()
+
+    d = oracle_lib.PbfDiff(sc)
+    x0, v0 = d.base.pos.copy(), d.base.vel.copy()
+    xT, _, states, used = d.rollout(x0, v0, T, lists=lists, record=True)
+    _, xbar = loss_grad(xT, mask, target)
+    ox, ov, ok = d.adjoint(states, used, xbar, np.zeros_like(xbar))
+    rel_v = np.linalg.norm(gv[mask] - ov[mask]) / np.linalg.norm(ov[mask])
+    rel_x = np.linalg.norm(gx[mask] - ox[mask]) / np.linalg.norm(ox[mask])
+    print(f"adjoint vs FP64 adjoint: vel {rel_v:.2e} pos {rel_x:.2e} k {abs(gk - ok) / abs(ok):.2e}")
+    assert rel_v < TOL and rel_x < TOL
+    assert abs(gk - ok) <= TOL * abs(ok)
+
+    rng = np.random.default_rng(5006)
+    k0 = d.p.xsph_k
+    for _ in range(4):
+        dv = np.zeros_like(v0)
+        dv[mask] = rng.normal(size=(mask.sum(), 3))
+        dk = rng.normal()
+        nrm = np.sqrt((dv ** 2).sum() + dk * dk)
+        dv, dk = dv / nrm, dk / nrm
+
+        def L(e):
+            d.p.xsph_k = k0 + e * dk
+            x, _, _, _ = d.rollout(x0, v0 + e * dv, T, lists=lists)
+            d.p.xsph_k = k0
+            return loss_grad(x, mask, target)[0]
+        fd = (L(1e-4) - L(-1e-4)) / 2e-4
+        ad = float((gv.astype(np.float64) * dv).sum() + gk * dk)
+        print(f"directional: fd {fd:.6e} adjoint {ad:.6e}")
+        assert abs(ad - fd) <= TOL * abs(fd)
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_independent_of_checkpoint_interval(vtp_gpu):
+    from vtp import diff
+    sc = small_case(9)
+    mask = diff.fluid_mask(sc)
+    out = []
+    for every in (1, 3, 8):
+        s = diff.pbf_solver(sc)
+        diff.diff_forward(s, 8, every)
+        pos = s.get_field("pos")
+        _, dl = loss_grad(pos, mask, TARGET)
+        out.append((pos, diff.diff_backward(s, dl.astype(np.float32), None)))
+        # the solver is back at the forward's final state
+        assert np.array_equal(s.get_field("pos"), pos)
+        s.destroy()
+    for pos, (gx, gv, gk) in out[1:]:
+        assert np.array_equal(pos, out[0][0])
+        assert np.array_equal(gv, out[0][1][1]) and np.array_equal(gx, out[0][1][0]) and gk == out[0][1][2]
+
+
+@pytest.mark.gpu
+def test_torch_autograd_wrapper(vtp_gpu):
+    import torch
+    from vtp import diff
+    sc = small_case(12)
+    f = sc.objects[0]
+    roll = diff.make_rollout(sc, steps=6, checkpoint_every=3)
+    v0 = torch.tensor(f.velocity, requires_grad=True)
+    k = torch.tensor(0.01, requires_grad=True)
+    x = roll(v0, k)
+    loss = ((x.double().mean(0) - torch.tensor(TARGET)) ** 2).sum()
+    loss.backward()
+    s = diff.pbf_solver(sc, f.velocity, 0.01)
+    diff.diff_forward(s, 6, 3)
+    mask = diff.fluid_mask(sc)
+    _, dl = loss_grad(s.get_field("pos"), mask, TARGET)
+    _, gv, gk = diff.diff_backward(s, dl.astype(np.float32), None)
+    s.destroy()
+    assert np.allclose(v0.grad.numpy(), gv[mask], rtol=1e-5, atol=1e-12)
+    assert k.grad.item() == pytest.approx(gk, rel=1e-5)

@@ -186,6 +186,7 @@ int vtp_solver::parse_config(const json &c) {
             stop_on_crash = b.value("stopOnNonConvergence", true);
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
+            persistent_tiles = b.value("persistentTiles", false);
             if (unroll != 1 && unroll != 2 && unroll != 4 && unroll != 8)
                 return fail(VTP_ERR_CONFIG, "unroll must be 1, 2, 4 or 8");
             if (block < 32 || block > 256 || (block & 31)) return fail(VTP_ERR_CONFIG, "blockSize must be 32..256, multiple of 32");
@@ -314,7 +315,7 @@ vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     a.ratio = ratio; a.alpha = alpha; a.kappa = kappa; a.delta = delta;
     a.acc_tmp = acc_tmp; a.normal = normal;
     a.orig = orig.c(); a.obj_of = obj_of; a.nobj_max = nobj_max; a.partials = partials; a.status = d_status;
-    a.tiles = d_tiles; a.ntiles = ntiles; a.scene_tiles = d_scene_tiles;
+    a.tiles = d_tiles; a.ntiles = ntiles; a.scene_tiles = d_scene_tiles; a.persistent = persistent_tiles;
     a.state = solve ? solve + (size_t)which * scenes.size() : nullptr;
     a.sc = scn();
     a.tick = d_tick;
@@ -667,29 +668,50 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
     return VTP_OK;
 }
 
+int vtp_solver::enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape) {
+    // PBFSolver::tick (PBFSolver.cpp:326-376): external force fused into the sort, neighbour
+    // lists, `iterations` constraint passes, XSPH.  With `tape` the lists are built into the
+    // tape and the intermediate states are copied out (differentiable mode).
+    const size_t nf = L.nf;
+    vtp::Carry none{};
+    vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt, u,
+                   u.fstart, prof);
+    pos.swap(); vel.swap(); orig.swap();
+    uint32_t *lnbr = tape ? tape->nbr : u.nbr, *lcnt = tape ? tape->ncnt : u.ncnt;
+    PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, lnbr, lcnt,
+                                                   d_status, d_overflow, block));
+    launches_per_tick += 8;  // hash, 4 scan kernels, scatter, rank/reorder, lists
+    if (tape && nf) {
+        CU(cudaMemcpyAsync(tape->orig, orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        CU(cudaMemcpyAsync(tape->x[0], pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+    }
+    for (int it = 0; it < iterations; ++it) {
+        vtp::PbfArgs a = pbf_args();
+        a.nbr = lnbr;
+        a.ncnt = lcnt;
+        if (tape) {
+            a.density = tape->rho[it];
+            a.lambda = tape->lam[it];
+        }
+        PROF(this, "pbf_lambda", vtp::pbf_lambda(s, a, block));
+        PROF(this, "pbf_dx", vtp::pbf_dx(s, a, block));
+        pos.swap();
+        launches_per_tick += 2;
+        if (tape && nf) CU(cudaMemcpyAsync(tape->x[it + 1], pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+    }
+    if (tape && nf) CU(cudaMemcpyAsync(tape->v, vel.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+    vtp::PbfArgs a = pbf_args();
+    a.nbr = lnbr;
+    a.ncnt = lcnt;
+    PROF(this, "pbf_xsph", vtp::pbf_xsph(s, a, block));
+    pos.swap(); vel.swap();
+    launches_per_tick += 1;
+    return VTP_OK;
+}
+
 int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     int rc;
-    if (type == VTP_SOLVER_PBF) {
-        vtp::Carry none{};
-        vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt,
-                       u, u.fstart, prof);
-        pos.swap(); vel.swap(); orig.swap();
-        PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
-                                                       d_status, d_overflow, block));
-        launches_per_tick += 8;  // hash, 4 scan kernels, scatter, rank/reorder, lists
-        for (int it = 0; it < iterations; ++it) {
-            vtp::PbfArgs a = pbf_args();
-            PROF(this, "pbf_lambda", vtp::pbf_lambda(s, a, block));
-            PROF(this, "pbf_dx", vtp::pbf_dx(s, a, block));
-            pos.swap();
-            launches_per_tick += 2;
-        }
-        vtp::PbfArgs a = pbf_args();
-        PROF(this, "pbf_xsph", vtp::pbf_xsph(s, a, block));
-        pos.swap(); vel.swap();
-        launches_per_tick += 1;
-        return VTP_OK;
-    }
+    if (type == VTP_SOLVER_PBF) return enqueue_pbf_substep(s, nullptr);
     if (type != VTP_SOLVER_DFSPH) return immct_enqueue_tick(*this, s, capture);
     vtp::Carry carry{};
     carry.nf4 = 1;

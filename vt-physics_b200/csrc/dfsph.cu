@@ -376,7 +376,9 @@ inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
 
-unsigned dfsph_tile_grid(uint32_t ntiles, int block) {
+unsigned dfsph_tile_grid(uint32_t ntiles, int block, bool persistent) {
+    if (ntiles == 0) return 1u;
+    if (!persistent) return ntiles;
     static int sms = 0;
     if (sms == 0) {
         int dev = 0;
@@ -384,7 +386,7 @@ unsigned dfsph_tile_grid(uint32_t ntiles, int block) {
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
     const uint32_t resident = (uint32_t)sms * (uint32_t)(2048 / block);
-    return ntiles == 0 ? 1u : (ntiles < resident ? ntiles : resident);
+    return ntiles < resident ? ntiles : resident;
 }
 
 void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
@@ -406,12 +408,12 @@ void dfsph_solve_begin(cudaStream_t st, SolveState *s, LoopState *loop, int nsce
     k_solve_begin<<<1, 256, 0, st>>>(s, loop, nscenes);
 }
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
-    const unsigned nb = dfsph_tile_grid(a.ntiles, block);
+    const unsigned nb = dfsph_tile_grid(a.ntiles, block, a.persistent);
     if (a.nobj_max > 1) VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<true, UU><<<nb, block, 0, st>>>(a))
     else VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<false, UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
-    const unsigned nb = dfsph_tile_grid(a.ntiles, block);
+    const unsigned nb = dfsph_tile_grid(a.ntiles, block, a.persistent);
     VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {

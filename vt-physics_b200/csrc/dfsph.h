@@ -55,6 +55,7 @@ struct DfsphArgs {
     double *partials;           // [tiles][nobj_max]
     const uint4 *tiles;         // {row0, rows, scene, 0}
     uint32_t ntiles;
+    bool persistent;            // persistent grid over the tiles
     const SceneTiles *scene_tiles;  // [S]
     const SolveState *state;    // [S] states of the running solve (stopped scenes are skipped)
     Scenes sc;                  // per-scene gravity
@@ -93,7 +94,8 @@ void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_finalize(cudaStream_t st, const DfsphArgs &a);
-// Persistent grid for the tile kernels: enough blocks to fill the GPU.
-unsigned dfsph_tile_grid(uint32_t ntiles, int block);
+// Grid of the tile kernels: one block per tile, or (persistent) just enough
+// blocks to fill the GPU, each looping over tiles.
+unsigned dfsph_tile_grid(uint32_t ntiles, int block, bool persistent);
 
 }  // namespace vtp

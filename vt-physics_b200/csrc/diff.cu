@@ -1,0 +1,520 @@
+// Differentiable PBF: a recorded forward with checkpoints and the hand-written
+// adjoint of the PBF substep (no counterpart in the reference).
+//
+// Forward (vtp_solver_diff_forward): the ordinary substep graphs, with the
+// fluid state (positions, velocities, sorted order) saved every k substeps.
+// Backward (vtp_solver_diff_backward): for each checkpoint segment, last to
+// first, the segment is recomputed from its checkpoint with the substep
+// kernels themselves (so the neighbour lists and every intermediate state are
+// exactly the forward's) into a tape, then the adjoint substeps run in reverse.
+//
+// One substep (PBFSolver::tick, PBFSolver.cpp:326-376, as the library runs it):
+//   v0 = v + g dt, x0 = x + v0 dt                         (apply_ext_force)
+//   for it < I:  rho_i = m_i W0 + sum_j m_j W_ij,  C_i = max(rho_i, rho0)/rho0 - 1
+//                e_ij = g_ij r_ij / rho0,  G_i = sum_j e_ij,  s2_i = sum_j |e_ij|^2 + |G_i|^2
+//                lambda_i = -C_i / (s2_i + eps)
+//                D_i = sum_j (lambda_i + lambda_j) e_ij   (lambda_j = 0 for boundary j)
+//                x <- x + D,  v <- v + D / dt
+//   a_i = c sum_j V_j (v_j - v_i) W_ij,  x <- x + a dt,  v <- v + a       (XSPH)
+// with gradW_ij = g_ij r_ij and d(g r)/dr = g I + hh r r^T (hh = g'(|r|)/|r|).
+// The adjoint of every neighbour sum is evaluated in gather form over the
+// same lists (pair (i, j) is in i's list iff (j, i) is in j's list while no
+// list overflows), so no pass needs atomics: each row reads its neighbours'
+// adjoint values of the previous pass.  Boundary rows are static and get no
+// adjoint.
+#include "solver.h"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+namespace vtp {
+
+struct DiffState {
+    uint32_t steps = 0, every = 0;     // recorded substeps, checkpoint interval
+    bool keep_lists = false;
+    uint32_t nf = 0, n = 0;
+    std::vector<void *> mem;
+    // checkpoints: fluid rows of (pos, vel, orig) at substeps 0, k, 2k, ... and at the end
+    std::vector<float4 *> ck_pos, ck_vel;
+    std::vector<uint32_t *> ck_orig;
+    // tape of one segment
+    std::vector<PbfTapeSlot> tape;
+    // all substeps' lists (keep_lists)
+    std::vector<uint32_t *> kl_orig, kl_nbr, kl_cnt;
+    // adjoint work arrays
+    float4 *xbar_a = nullptr, *vbar_a = nullptr;   // attach order [n]
+    float4 *xbar = nullptr, *vbar = nullptr, *abar = nullptr, *D[2] = {nullptr, nullptr}, *A2 = nullptr;
+    float *sbar = nullptr;
+    double *kpart = nullptr, *kacc = nullptr;
+    uint32_t kblocks = 0;
+
+    ~DiffState() {
+        for (void *p : mem) cudaFree(p);
+    }
+    template <class T>
+    int alloc(T **p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e != cudaSuccess) return fail(VTP_ERR_NOMEM, std::string("differentiable mode: ") + cudaGetErrorString(e));
+        mem.push_back(*p);
+        return VTP_OK;
+    }
+};
+
+namespace {
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// g'(r) / r of the cubic spline's gradient factor (gradW = g r).
+__device__ __forceinline__ float cubic_hh(float d2, const Cubic &k) {
+    if (!(d2 > 0.f)) return 0.f;
+    const float r = sqrtf(d2);
+    const float q = r * k.invh;
+    if (q < 1e-6f || q > 1.f) return 0.f;
+    const float ih2 = k.invh * k.invh, ih4 = ih2 * ih2;
+    if (q <= 0.5f) return 18.f * k.sigma * ih4 / q;
+    return 6.f * k.sigma * ih4 * (1.f - q * q) / (q * q * q);
+}
+
+__device__ __forceinline__ double block_sum_d(double v) {
+    __shared__ double sm[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    double s = 0.0;
+    if (wid == 0) {
+        s = lane < nw ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    return s;
+}
+
+struct AdjArgs {
+    uint32_t nf, ell_stride;
+    Cubic k;
+    float dt, inv_dt, rho0, eps, c;
+    const uint32_t *nbr, *ncnt, *orig;
+    const float4 *x;        // positions of the pass (n rows, w = mass)
+    const float4 *v;        // velocities before XSPH (n rows)
+    const float *vol;       // [n]
+    const float *lam, *rho; // [nf] of the iteration
+    float4 *xbar, *vbar, *abar, *Dcur, *Dnext, *A2;
+    float *sbar;
+    float4 *xbar_a, *vbar_a;
+    double *kpart;
+};
+
+// Attach order -> this substep's rows; abar = xbar dt + vbar (XSPH output adjoint).
+__global__ void k_adj_gather(AdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const uint32_t id = a.orig[r];
+    const float4 xo = a.xbar_a[id], vo = a.vbar_a[id];
+    a.xbar[r] = xo;
+    a.vbar[r] = vo;
+    a.abar[r] = make_float4(xo.x * a.dt + vo.x, xo.y * a.dt + vo.y, xo.z * a.dt + vo.z, 0.f);
+}
+
+// XSPH adjoint; epilogue: Delta-bar of the last constraint iteration.
+__global__ void __launch_bounds__(256) k_adj_xsph(AdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    double kl = 0.0;
+    if (r < a.nf) {
+        const float4 p = a.x[r], vi = a.v[r], ai = a.abar[r];
+        float4 xb = a.xbar[r], vb = a.vbar[r];
+        const float Vi = a.vol[r];
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        float ksum = 0.f;
+        for (uint32_t t = 0; t + 1 < n; ++t) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = a.x[j], vj = a.v[j];
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float d2 = dist2(rx, ry, rz);
+            const float w = cubic_w(d2, a.k), g = cubic_g(d2, a.k);
+            const float Vj = a.vol[j];
+            const bool fj = j < a.nf;
+            const float4 aj = fj ? a.abar[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float dx = vj.x - vi.x, dy = vj.y - vi.y, dz = vj.z - vi.z;
+            const float di = dx * ai.x + dy * ai.y + dz * ai.z;
+            const float dj = dx * aj.x + dy * aj.y + dz * aj.z;
+            const float ci = -a.c * Vj * w, cj = a.c * Vi * w;
+            vb.x += ci * ai.x + cj * aj.x;
+            vb.y += ci * ai.y + cj * aj.y;
+            vb.z += ci * ai.z + cj * aj.z;
+            const float s = a.c * g * (Vj * di - Vi * dj);
+            xb.x += s * rx;
+            xb.y += s * ry;
+            xb.z += s * rz;
+            ksum += Vj * w * di;
+        }
+        a.xbar[r] = xb;
+        a.vbar[r] = vb;
+        a.Dcur[r] = make_float4(xb.x + vb.x * a.inv_dt, xb.y + vb.y * a.inv_dt, xb.z + vb.z * a.inv_dt, 0.f);
+        kl = (double)ksum;
+    }
+    const double s = block_sum_d(kl);
+    if (threadIdx.x == 0) a.kpart[blockIdx.x] = s;
+}
+
+// Constraint iteration adjoint, pass A: lambda-bar -> s2-bar, rho-bar; G recomputed.
+__global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.x[r], di = a.Dcur[r];
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    const float ir = 1.f / a.rho0;
+    float lb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = a.x[j];
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float g = cubic_g(dist2(rx, ry, rz), a.k) * ir;
+        const float ex = g * rx, ey = g * ry, ez = g * rz;
+        gx += ex; gy += ey; gz += ez;
+        s2 += ex * ex + ey * ey + ez * ez;
+        float4 dj = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < a.nf) dj = a.Dcur[j];
+        lb += ex * (di.x - dj.x) + ey * (di.y - dj.y) + ez * (di.z - dj.z);
+    }
+    s2 += gx * gx + gy * gy + gz * gz;
+    const float den = s2 + a.eps;
+    const float lam = a.lam[r];
+    a.sbar[r] = -lb * lam / den;
+    const float rb = a.rho[r] <= a.rho0 ? 0.f : -lb / (den * a.rho0);   // clamped density: no gradient
+    a.A2[r] = make_float4(gx, gy, gz, rb);
+}
+
+// Constraint iteration adjoint, pass B: xbar of the iteration's input positions;
+// epilogue: Delta-bar of the previous iteration.
+__global__ void __launch_bounds__(256) k_adj_dx(AdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.x[r], di = a.Dcur[r], Ai = a.A2[r];
+    const float li = a.lam[r], sbi = a.sbar[r];
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    const float ir = 1.f / a.rho0;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = a.x[j];
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float d2 = dist2(rx, ry, rz);
+        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+        const float ex = g * rx * ir, ey = g * ry * ir, ez = g * rz * ir;
+        const bool fj = j < a.nf;
+        float lj = 0.f, sbj = 0.f;
+        float4 dj = make_float4(0.f, 0.f, 0.f, 0.f), Aj = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (fj) {
+            lj = a.lam[j];
+            sbj = a.sbar[j];
+            dj = a.Dcur[j];
+            Aj = a.A2[j];
+        }
+        const float ll = li + lj;
+        // e-bar of pair (i, j) minus e-bar of pair (j, i) (zero for a boundary j)
+        float bx = ll * di.x + 2.f * sbi * (ex + Ai.x);
+        float by = ll * di.y + 2.f * sbi * (ey + Ai.y);
+        float bz = ll * di.z + 2.f * sbi * (ez + Ai.z);
+        if (fj) {
+            bx -= ll * dj.x + 2.f * sbj * (Aj.x - ex);
+            by -= ll * dj.y + 2.f * sbj * (Aj.y - ey);
+            bz -= ll * dj.z + 2.f * sbj * (Aj.z - ez);
+        }
+        const float rdot = rx * bx + ry * by + rz * bz;
+        const float dens = q.w * Ai.w + (fj ? p.w * Aj.w : 0.f);   // m_j rho-bar_i + m_i rho-bar_j
+        const float cg = g * dens;
+        ax += cg * rx + (g * bx + hh * rx * rdot) * ir;
+        ay += cg * ry + (g * by + hh * ry * rdot) * ir;
+        az += cg * rz + (g * bz + hh * rz * rdot) * ir;
+    }
+    float4 xb = a.xbar[r];
+    xb.x += ax; xb.y += ay; xb.z += az;
+    a.xbar[r] = xb;
+    const float4 vb = a.vbar[r];
+    a.Dnext[r] = make_float4(xb.x + vb.x * a.inv_dt, xb.y + vb.y * a.inv_dt, xb.z + vb.z * a.inv_dt, 0.f);
+}
+
+// External force adjoint, then this substep's rows -> attach order.
+__global__ void k_adj_force_scatter(AdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const uint32_t id = a.orig[r];
+    const float4 xb = a.xbar[r], vb = a.vbar[r];
+    a.xbar_a[id] = xb;
+    a.vbar_a[id] = make_float4(vb.x + a.dt * xb.x, vb.y + a.dt * xb.y, vb.z + a.dt * xb.z, 0.f);
+}
+
+__global__ void k_adj_kreduce(const double *part, uint32_t nb, double *acc) {
+    double s = 0.0;
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
+    s = block_sum_d(s);
+    if (threadIdx.x == 0) *acc += s;
+}
+
+__global__ void k_f3_to_f4(uint32_t n, const float *src, float4 *dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src ? make_float4(src[3 * (size_t)i], src[3 * (size_t)i + 1], src[3 * (size_t)i + 2], 0.f)
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void k_f4_to_f3(uint32_t n, const float4 *src, float *dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = src[i];
+    dst[3 * (size_t)i] = v.x;
+    dst[3 * (size_t)i + 1] = v.y;
+    dst[3 * (size_t)i + 2] = v.z;
+}
+
+}  // namespace
+}  // namespace vtp
+
+using vtp::fail;
+
+#define CU(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(VTP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+int save_fluid(vtp_solver &s, float4 *p, float4 *v, uint32_t *o) {
+    const size_t nf = s.L.nf;
+    if (!nf) return VTP_OK;
+    CU(cudaMemcpyAsync(p, s.pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(v, s.vel.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(o, s.orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s.st));
+    return VTP_OK;
+}
+
+int restore_fluid(vtp_solver &s, const float4 *p, const float4 *v, const uint32_t *o) {
+    const size_t nf = s.L.nf;
+    if (!nf) return VTP_OK;
+    CU(cudaMemcpyAsync(s.pos.c(), p, nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(s.vel.c(), v, nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(s.orig.c(), o, nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s.st));
+    return VTP_OK;
+}
+
+int check_ready(vtp_solver *s) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    if (s->type != VTP_SOLVER_PBF) return fail(VTP_ERR_CONFIG, "differentiable mode supports the PBF solver");
+    if (s->nscenes() != 1) return fail(VTP_ERR_CONFIG, "differentiable mode runs a single scene");
+    return VTP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    if (!s->initialized && (rc = s->initialize())) return rc;
+    if (s->crashed) return fail(VTP_ERR_STATE, "solver is crashed");
+    if (n_steps == 0 || checkpoint_every == 0) return fail(VTP_ERR_ARG, "n_steps and checkpoint_every must be > 0");
+    auto d = std::make_shared<vtp::DiffState>();
+    d->steps = n_steps;
+    d->every = std::min(checkpoint_every, n_steps);
+    d->keep_lists = keep_lists != 0;
+    d->nf = s->L.nf;
+    d->n = s->L.n;
+    const uint32_t nchk = (n_steps + d->every - 1) / d->every;
+    const size_t nf = std::max<uint32_t>(d->nf, 1), n = d->n;
+    const size_t lrows = ((size_t)d->nf + 31) / 32 * 32 * s->L.ell_stride;
+    d->ck_pos.resize(nchk + 1);
+    d->ck_vel.resize(nchk + 1);
+    d->ck_orig.resize(nchk + 1);
+    for (uint32_t c = 0; c <= nchk; ++c) {
+        if ((rc = d->alloc(&d->ck_pos[c], nf)) || (rc = d->alloc(&d->ck_vel[c], nf)) ||
+            (rc = d->alloc(&d->ck_orig[c], nf)))
+            return rc;
+    }
+    if (d->keep_lists) {
+        d->kl_orig.resize(n_steps);
+        d->kl_nbr.resize(n_steps);
+        d->kl_cnt.resize(n_steps);
+        for (uint32_t t = 0; t < n_steps; ++t)
+            if ((rc = d->alloc(&d->kl_orig[t], nf)) || (rc = d->alloc(&d->kl_nbr[t], std::max<size_t>(lrows, 1))) ||
+                (rc = d->alloc(&d->kl_cnt[t], nf)))
+                return rc;
+    }
+    // The tape of one segment: lists and intermediate states of `every` substeps.
+    const int I = s->iterations;
+    d->tape.resize(d->every);
+    for (auto &slot : d->tape) {
+        if ((rc = d->alloc(&slot.orig, nf)) || (rc = d->alloc(&slot.nbr, std::max<size_t>(lrows, 1))) ||
+            (rc = d->alloc(&slot.ncnt, nf)) || (rc = d->alloc(&slot.v, n)))
+            return rc;
+        slot.x.resize(I + 1);
+        slot.lam.resize(I);
+        slot.rho.resize(I);
+        for (auto &x : slot.x) {
+            if ((rc = d->alloc(&x, n))) return rc;
+            // boundary rows are static: copy them once
+            if (s->L.nb)
+                CU(cudaMemcpyAsync(x + s->L.nf, s->pos.c() + s->L.nf, (size_t)s->L.nb * sizeof(float4),
+                                   cudaMemcpyDeviceToDevice, s->st));
+        }
+        if (s->L.nb)
+            CU(cudaMemcpyAsync(slot.v + s->L.nf, s->vel.c() + s->L.nf, (size_t)s->L.nb * sizeof(float4),
+                               cudaMemcpyDeviceToDevice, s->st));
+        for (int it = 0; it < I; ++it)
+            if ((rc = d->alloc(&slot.lam[it], nf)) || (rc = d->alloc(&slot.rho[it], nf))) return rc;
+    }
+    d->kblocks = vtp::nblk(std::max<uint32_t>(d->nf, 1), 256);
+    if ((rc = d->alloc(&d->xbar_a, n)) || (rc = d->alloc(&d->vbar_a, n)) || (rc = d->alloc(&d->xbar, nf)) ||
+        (rc = d->alloc(&d->vbar, nf)) || (rc = d->alloc(&d->abar, nf)) || (rc = d->alloc(&d->D[0], nf)) ||
+        (rc = d->alloc(&d->D[1], nf)) || (rc = d->alloc(&d->A2, nf)) || (rc = d->alloc(&d->sbar, nf)) ||
+        (rc = d->alloc(&d->kpart, d->kblocks)) || (rc = d->alloc(&d->kacc, 1)))
+        return rc;
+    s->diff.reset();
+    // Forward: checkpoint, then the ordinary substeps up to the next checkpoint.
+    for (uint32_t c = 0; c < nchk; ++c) {
+        if ((rc = save_fluid(*s, d->ck_pos[c], d->ck_vel[c], d->ck_orig[c]))) return rc;
+        const uint32_t k = std::min(d->every, n_steps - c * d->every);
+        if (!d->keep_lists) {
+            if ((rc = s->tick_n(k))) return rc;
+            continue;
+        }
+        // keep_lists: direct launches, every substep's lists kept
+        for (uint32_t t = 0; t < k; ++t) {
+            const uint32_t step = c * d->every + t;
+            PbfTapeSlot slot = d->tape[0];
+            slot.nbr = d->kl_nbr[step];
+            slot.ncnt = d->kl_cnt[step];
+            slot.orig = d->kl_orig[step];
+            if ((rc = s->enqueue_pbf_substep(s->st, &slot))) return rc;
+            s->sim_time += s->dt;
+            ++s->steps_done;
+        }
+        CU(cudaStreamSynchronize(s->st));
+        if ((rc = s->check_status())) return rc;
+    }
+    if ((rc = save_fluid(*s, d->ck_pos[nchk], d->ck_vel[nchk], d->ck_orig[nchk]))) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    if ((rc = s->check_status())) return rc;
+    s->diff = d;
+    return VTP_OK;
+}
+
+int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
+                             float *dl_dvel0, double *dl_dxsph_k) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    if (!s->diff) return fail(VTP_ERR_STATE, "diff_backward before diff_forward");
+    vtp::DiffState &d = *s->diff;
+    const uint32_t n = d.n, nf = d.nf;
+    const size_t n3 = (size_t)n * 3 * sizeof(float);
+    const int I = s->iterations;
+    int r2 = s->ensure_stage(n3);
+    if (r2) return r2;
+    // dL/d(final state), attach order
+    if (dl_dpos) CU(cudaMemcpyAsync(s->stage, dl_dpos, n3, cudaMemcpyHostToDevice, s->st));
+    vtp::k_f3_to_f4<<<vtp::nblk(n, 256), 256, 0, s->st>>>(n, dl_dpos ? s->stage : nullptr, d.xbar_a);
+    if (dl_dvel) CU(cudaMemcpyAsync(s->stage, dl_dvel, n3, cudaMemcpyHostToDevice, s->st));
+    vtp::k_f3_to_f4<<<vtp::nblk(n, 256), 256, 0, s->st>>>(n, dl_dvel ? s->stage : nullptr, d.vbar_a);
+    CU(cudaMemsetAsync(d.kacc, 0, sizeof(double), s->st));
+    const uint32_t nchk = (d.steps + d.every - 1) / d.every;
+    const unsigned G = vtp::nblk(std::max<uint32_t>(nf, 1), 256);
+    for (int c = (int)nchk - 1; c >= 0; --c) {
+        const uint32_t t0 = (uint32_t)c * d.every, k = std::min(d.every, d.steps - t0);
+        // Recompute the segment from its checkpoint into the tape.
+        if ((rc = restore_fluid(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
+        for (uint32_t t = 0; t < k; ++t)
+            if ((rc = s->enqueue_pbf_substep(s->st, &d.tape[t]))) return rc;
+        // Adjoint substeps, last to first.
+        for (int t = (int)k - 1; t >= 0 && nf; --t) {
+            const PbfTapeSlot &T = d.tape[t];
+            vtp::AdjArgs a{};
+            a.nf = nf; a.ell_stride = s->L.ell_stride; a.k = s->kc;
+            a.dt = s->dt; a.inv_dt = 1.f / s->dt; a.rho0 = s->rho_f; a.eps = 1e-6f; a.c = s->xsph_k;
+            a.nbr = T.nbr; a.ncnt = T.ncnt; a.orig = T.orig;
+            a.v = T.v; a.vol = s->vol;
+            a.xbar = d.xbar; a.vbar = d.vbar; a.abar = d.abar; a.A2 = d.A2; a.sbar = d.sbar;
+            a.xbar_a = d.xbar_a; a.vbar_a = d.vbar_a; a.kpart = d.kpart;
+            int cur = 0;
+            a.x = T.x[I];
+            a.Dcur = d.D[cur];
+            vtp::k_adj_gather<<<G, 256, 0, s->st>>>(a);
+            vtp::k_adj_xsph<<<G, 256, 0, s->st>>>(a);
+            vtp::k_adj_kreduce<<<1, 256, 0, s->st>>>(d.kpart, G, d.kacc);
+            for (int it = I - 1; it >= 0; --it) {
+                a.x = T.x[it];
+                a.lam = T.lam[it];
+                a.rho = T.rho[it];
+                a.Dcur = d.D[cur];
+                a.Dnext = d.D[cur ^ 1];
+                vtp::k_adj_lambda<<<G, 256, 0, s->st>>>(a);
+                vtp::k_adj_dx<<<G, 256, 0, s->st>>>(a);
+                cur ^= 1;
+            }
+            vtp::k_adj_force_scatter<<<G, 256, 0, s->st>>>(a);
+        }
+    }
+    CU(cudaGetLastError());
+    // Outputs: dL/d(state at the start of the recorded forward), attach order.
+    if (dl_dpos0) {
+        vtp::k_f4_to_f3<<<vtp::nblk(n, 256), 256, 0, s->st>>>(n, d.xbar_a, s->stage);
+        CU(cudaMemcpyAsync(dl_dpos0, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+    }
+    if (dl_dvel0) {
+        vtp::k_f4_to_f3<<<vtp::nblk(n, 256), 256, 0, s->st>>>(n, d.vbar_a, s->stage);
+        CU(cudaMemcpyAsync(dl_dvel0, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+    }
+    double kb = 0.0;
+    CU(cudaMemcpyAsync(&kb, d.kacc, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    // Put the forward's final state back so the solver can continue.
+    if ((rc = restore_fluid(*s, d.ck_pos[nchk], d.ck_vel[nchk], d.ck_orig[nchk]))) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    if (dl_dxsph_k) *dl_dxsph_k = kb;
+    return s->check_status();
+}
+
+int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    if (!s->diff || !s->diff->keep_lists) return fail(VTP_ERR_STATE, "diff_lists needs diff_forward with keep_lists");
+    vtp::DiffState &d = *s->diff;
+    if (step >= d.steps) return fail(VTP_ERR_ARG, "step out of range");
+    if (!counts || !nbrs) return fail(VTP_ERR_ARG, "null argument");
+    if (max_nbr != s->maxnbr) return fail(VTP_ERR_ARG, "max_nbr must equal maxNeighborNum");
+    const uint32_t n = d.n, nf = d.nf;
+    // Row -> attach id map of that substep: fluid rows from the record, boundary rows static.
+    uint32_t *omap = nullptr, *dc = nullptr, *dn = nullptr;
+    CU(cudaMalloc(&omap, (size_t)n * 4));
+    cudaError_t e = cudaMalloc(&dc, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dn, (size_t)n * max_nbr * 4);
+    if (e == cudaSuccess && nf) e = cudaMemcpyAsync(omap, d.kl_orig[step], (size_t)nf * 4, cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess && n > nf)
+        e = cudaMemcpyAsync(omap + nf, s->orig.c() + nf, (size_t)(n - nf) * 4, cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess) {
+        vtp::export_neighbors(s->st, s->L, 0, nf, d.kl_nbr[step], d.kl_cnt[step], omap, max_nbr, dc, dn);
+        vtp::export_neighbors(s->st, s->L, nf, n - nf, s->u.bnbr, s->u.bncnt, omap, max_nbr, dc, dn);
+        e = cudaMemcpyAsync(counts, dc, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nbrs, dn, (size_t)n * max_nbr * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(omap);
+    cudaFree(dc);
+    cudaFree(dn);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+}  // extern "C"

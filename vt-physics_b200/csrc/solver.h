@@ -49,6 +49,20 @@ struct SceneRec {
     vtp::SceneGrid grid{};
 };
 
+// Recording targets of one PBF substep in differentiable mode: the substep's
+// lists are built into the tape and its intermediate states copied out.
+struct PbfTapeSlot {
+    uint32_t *orig = nullptr;            // [nf] sorted fluid row -> attach id
+    uint32_t *nbr = nullptr, *ncnt = nullptr;
+    std::vector<float4 *> x;             // [iterations + 1] positions (n rows; fluid rows recorded)
+    std::vector<float *> lam, rho;       // [iterations] lambda, clamped density
+    float4 *v = nullptr;                 // velocity before XSPH (n rows; fluid rows recorded)
+};
+
+namespace vtp {
+struct DiffState;
+}
+
 struct vtp_solver {
     int type = 0;
     nlohmann::json cfg;
@@ -78,6 +92,7 @@ struct vtp_solver {
     bool device_loop = true, use_graphs = true, stage_timers = false, stop_on_crash = true;
     int block = 128;
     int unroll = 4;
+    bool persistent_tiles = false;
 
     // device state
     cudaStream_t st = nullptr, side = nullptr;
@@ -105,6 +120,7 @@ struct vtp_solver {
     uint32_t *d_status = nullptr, *d_overflow = nullptr;
     uint32_t *h_pinned = nullptr;       // [4] status, overflow, iter, spare
     std::shared_ptr<vtp::ImmState> imm;
+    std::shared_ptr<vtp::DiffState> diff;
 
     // graphs: two parities (double-buffer swaps alternate between substeps)
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -147,6 +163,7 @@ struct vtp_solver {
         if (st) cudaStreamDestroy(st), st = nullptr;
         if (side) cudaStreamDestroy(side), side = nullptr;
         imm.reset();
+        diff.reset();
         graphs_ready = false;
         initialized = false;
     }
@@ -169,6 +186,7 @@ struct vtp_solver {
     int initialize();
     int tick_n(uint32_t n);
     int enqueue_tick(cudaStream_t s, bool capture);
+    int enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape);
     int enqueue_solve(cudaStream_t s, int which, bool capture);
     int build_graphs();
     int sort_boundary_and_lists();

@@ -54,6 +54,9 @@ SIGNATURES = {
     "vtp_solver_get_stage_times": (C.c_int, [_P, _P]),
     "vtp_solver_get_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "vtp_solver_profile_kernels": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "vtp_solver_diff_forward": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int]),
+    "vtp_solver_diff_backward": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(C.c_double)]),
+    "vtp_solver_diff_lists": (C.c_int, [_P, C.c_uint32, _P, _P, C.c_uint32]),
     "vtp_ugns_neighbors_noalloc": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
                                              C.c_uint32, _P, _P, _P]),
 }

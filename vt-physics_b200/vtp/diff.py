@@ -1,0 +1,109 @@
+"""Differentiable PBF through the C ABI, and its torch.autograd wrapper.
+
+The adjoint itself is the library's (vtp_solver_diff_forward / _backward:
+checkpointed forward, per-segment recompute into a tape with the substep
+kernels, hand-written adjoint passes in reverse).  This module moves arrays
+across the boundary and exposes the rollout to torch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+
+import numpy as np
+
+from ._lib import check, lib
+from .solver import Object, Particle_Common, PBFSolver
+
+
+def diff_forward(s, steps: int, checkpoint_every: int = 20, keep_lists: bool = False):
+    check(lib().vtp_solver_diff_forward(s._h, int(steps), int(checkpoint_every), 1 if keep_lists else 0),
+          "diff_forward")
+
+
+def diff_backward(s, dl_dpos=None, dl_dvel=None):
+    """dL/d(final pos, vel) (n x 3, attach order) -> (dL/dpos0, dL/dvel0, dL/dXSPH_k)."""
+    n = s.counts()["total"]
+
+    def arr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, np.float32).reshape(n, 3)
+        return a
+
+    gp, gv = arr(dl_dpos), arr(dl_dvel)
+    op = np.zeros((n, 3), np.float32)
+    ov = np.zeros((n, 3), np.float32)
+    gk = C.c_double()
+    check(lib().vtp_solver_diff_backward(s._h, None if gp is None else gp.ctypes.data,
+                                         None if gv is None else gv.ctypes.data, op.ctypes.data, ov.ctypes.data,
+                                         C.byref(gk)), "diff_backward")
+    return op, ov, gk.value
+
+
+def diff_lists(s, step: int, max_nbr: int):
+    n = s.counts()["total"]
+    cnt = np.empty(n, np.uint32)
+    nb = np.empty((n, max_nbr), np.uint32)
+    check(lib().vtp_solver_diff_lists(s._h, int(step), cnt.ctypes.data, nb.ctypes.data, int(max_nbr)), "diff_lists")
+    return cnt, nb
+
+
+def pbf_solver(scene, v0_fluid=None, xsph_k=None, extra=None):
+    """A PBF solver of `scene` with per-particle initial fluid velocities and an XSPH coefficient."""
+    cfg = json.loads(json.dumps(scene.config))
+    if xsph_k is not None:
+        cfg["PBF"]["Required"]["XSPH_k"] = float(xsph_k)
+    if extra:
+        cfg["B200"] = dict(extra)
+    s = PBFSolver(strict=True)
+    s.setConfig(cfg)
+    k = 0
+    for o in scene.objects:
+        obj = Object(Particle_Common, o.name)
+        obj.getObjectComponentConfig()["epmMaterial"] = o.material
+        obj.attachSpecificSolverObjectComponentConfig({"solverType": 0, "exportFlag": o.export_flag,
+                                                       "velocityStart": list(o.velocity_start),
+                                                       "colorStart": list(o.color_start)})
+        obj.pos = o.pos
+        obj.velocity = o.velocity
+        if o.material == 0 and v0_fluid is not None:
+            obj.velocity = np.asarray(v0_fluid[k:k + o.n], np.float32)
+            k += o.n
+        s.attachObject(obj)
+    s.initialize()
+    return s
+
+
+def fluid_mask(scene) -> np.ndarray:
+    return np.concatenate([np.full(o.n, o.material == 0) for o in scene.objects])
+
+
+def make_rollout(scene, steps: int, checkpoint_every: int = 20, extra=None):
+    """torch.autograd.Function: (v0 of the fluid [nf, 3], XSPH_k []) -> fluid positions after `steps`."""
+    import torch
+
+    mask = fluid_mask(scene)
+
+    class PbfRollout(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, v0, k):
+            s = pbf_solver(scene, v0.detach().cpu().numpy(), float(k.item()), extra)
+            diff_forward(s, steps, checkpoint_every)
+            pos = s.get_field("pos")
+            ctx.solver = s
+            return torch.from_numpy(pos[mask].copy()).to(v0.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            s = ctx.solver
+            n = s.counts()["total"]
+            dl = np.zeros((n, 3), np.float32)
+            dl[mask] = g.detach().cpu().numpy()
+            _, gv, gk = diff_backward(s, dl, None)
+            s.destroy()
+            ctx.solver = None
+            dev = g.device
+            return torch.from_numpy(gv[mask].copy()).to(dev), torch.tensor(gk, dtype=torch.float32, device=dev)
+
+    return PbfRollout.apply

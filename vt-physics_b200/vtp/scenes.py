@@ -206,6 +206,21 @@ def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, j
                                SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def diff_pbf(seed: int = 5005) -> Scene:
+    """The differentiable PBF scene: a 40^3 lattice (spacing 0.02, lb 0.2, no jitter) in a
+    2-layer [0, 1.2]^3 box, initial fluid velocities N(0, 0.1^2) per component (SplitMix64
+    stream ``seed``, Box-Muller), PBF parameters of the dam break, dt 1/240."""
+    r = 0.01
+    fluid = cube(r, (0.2, 0.2, 0.2), (0.8, 0.8, 0.8))
+    wall = box(r, (0.0, 0.0, 0.0), (1.2, 1.2, 1.2), 2)
+    u = splitmix64_uniform(seed, 2 * fluid.shape[0] * 3).reshape(2, -1)
+    z = np.sqrt(-2.0 * np.log1p(-u[0])) * np.cos(2.0 * np.pi * u[1])
+    v0 = (0.1 * z).reshape(-1, 3).astype(np.float32)
+    cfg = pbf_config(dt=1.0 / 240.0, r=r, lb=(-0.1, -0.1, -0.1), size=(1.4, 1.4, 1.4))
+    return Scene("PBF", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, velocity=v0),
+                              SceneObject("box", wall, EPM_BOUNDARY)])
+
+
 def batched_scenes(count: int = 64, n_pbf: int = 48, seed: int = 4242, gravity_seed: int = 4243,
                    n_min: float = 4e3, n_max: float = 2.56e5) -> list:
     """The batched mix: ``count`` dam breaks, the first ``n_pbf`` PBF and the rest DFSPH.
