@@ -238,6 +238,25 @@ VTP_API int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const 
  * vtp_solver_get_neighbors (built after the substep's external force). */
 VTP_API int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr);
 
+/* DFSPH pressure solve as a differentiable operator (no counterpart in the
+ * reference; DFSPH solver, one scene).
+ *
+ * vtp_solver_dfsph_solve_forward runs one pressure solve (which = 0: the
+ * divergence solve, 1: the density solve; DFSPHCudaImpl.cu:142-220) on the
+ * solver's current positions: the neighbour search and compression-ratio /
+ * alpha pass a substep starts with, then the solve loop on v* = v_in (attach
+ * order, n_total x float[3], boundary rows ignored) until the residual test
+ * stops it (or exactly force_iters iterations when > 0).  v_out (may be NULL)
+ * receives v* after the solve, *iterations the iteration count.  The
+ * solver's own state is left unchanged; the lists, the iteration count and
+ * each iteration's clamp pattern (delta > 0) are kept.
+ * vtp_solver_dfsph_solve_backward maps dL/d(v_out) to dL/d(v_in) through the
+ * recorded solve (hand-written adjoint passes, two per iteration), valid
+ * until the solver advances. */
+VTP_API int vtp_solver_dfsph_solve_forward(vtp_solver *s, int which, const float *v_in, float *v_out,
+                                           uint32_t force_iters, uint32_t *iterations);
+VTP_API int vtp_solver_dfsph_solve_backward(vtp_solver *s, const float *vbar_out, float *vbar_in);
+
 /* Allocation-free neighbour search (no counterpart in the reference).
  *
  * For callers that cannot call cudaMalloc when they need neighbour lists:

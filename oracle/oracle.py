@@ -57,6 +57,8 @@ def lib() -> C.CDLL:
         L.or_pbf_step_frozen.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf)]
         L.or_pbf_step_adjoint.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf), P, P,
                                           C.POINTER(C.c_double)]
+        L.or_dfsph_solve_op.argtypes = [C.c_uint32, P, P, P, P, P, P, C.c_uint32, C.c_double, C.c_double, C.c_int,
+                                         P, P]
         L.or_num_threads.restype = C.c_int
         L.or_set_num_threads.argtypes = [C.c_int]
         _lib = L
@@ -250,3 +252,15 @@ class PbfDiff:
             lib().or_pbf_step_adjoint(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.mass), _ptr(b.vol), _ptr(cnt),
                                       _ptr(nb), self.maxnbr, C.byref(self.p), _ptr(xb), _ptr(vb), C.byref(kb))
         return xb, vb, kb.value
+
+
+def dfsph_solve_op(o: "OracleSolver", cnt, nbr, iters: int, vadv, vbar=None):
+    """FP64 pressure-solve operator on the oracle's current positions with the given lists:
+    returns (v* after `iters` iterations, dL/dv* in or None)."""
+    v = np.ascontiguousarray(vadv, np.float64).copy()
+    vb = None if vbar is None else np.ascontiguousarray(vbar, np.float64).copy()
+    cnt = np.ascontiguousarray(cnt, np.uint32)
+    nbr = np.ascontiguousarray(nbr, np.uint32)
+    lib().or_dfsph_solve_op(o.n, _ptr(o.mat), _ptr(o.pos), _ptr(o.vol), _ptr(o.rest_density), _ptr(cnt), _ptr(nbr),
+                            int(o.grid.maxnbr), float(o.p.h), float(o.p.dt), int(iters), _ptr(v), _ptr(vb))
+    return v, vb

@@ -739,3 +739,112 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
     free(nrm);
     free_lists(&L);
 }
+
+/* ------------------------------------------------------------------ DFSPH pressure solve as an operator */
+
+void or_dfsph_solve_op(uint32_t n, const int32_t *mat, const double *pos, const double *vol,
+                       const double *rest_density, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                       double h, double dt, int iters, double *vadv, double *vbar) {
+    or_grid gg;
+    memset(&gg, 0, sizeof(gg));
+    gg.maxnbr = maxnbr;
+    const or_grid *g = &gg;
+    lists_t L = {(uint32_t *)cnt, (uint32_t *)nbr};
+    cubic_t k = cubic_make(h);
+    const size_t nn = n ? n : 1;
+    double *mass = (double *)calloc(nn, sizeof(double));
+    double *ratio = (double *)calloc(nn, sizeof(double));
+    double *alpha = (double *)calloc(nn, sizeof(double));
+    double *kappa = (double *)calloc(nn, sizeof(double));
+    unsigned char *mask = (unsigned char *)calloc(nn * (iters > 0 ? iters : 1), 1);
+    for (uint32_t i = 0; i < n; ++i) mass[i] = mat[i] == 0 ? rest_density[i] * vol[i] : 0.0;
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double rt = 0, a1[3] = {0, 0, 0}, a2 = 1e-6, r[3];
+        FOR_NBR(L, g, i, j) {
+            double rl = rdiff(pos, i, j, r);
+            rt += vol[j] * cubic_w(&k, rl);
+            double q = cubic_g(&k, rl);
+            for (int a = 0; a < 3; ++a) a1[a] += vol[j] * q * r[a];
+            if (mat[j] == 0) a2 += q * q * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) * vol[j] * vol[j] / mass[j];
+        }
+        double al = (a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2]) / mass[i] + a2;
+        if (al < 1e-6) al = 1e-6;
+        ratio[i] = rt;
+        alpha[i] = al;
+    }
+    for (int it = 0; it < iters; ++it) {
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            kappa[i] = 0.0;
+            if (mat[i] != 0) continue;
+            double d = ratio[i] - 1.0, r[3];
+            FOR_NBR(L, g, i, j) {
+                double q = cubic_g(&k, rdiff(pos, i, j, r));
+                double dot = 0;
+                for (int a = 0; a < 3; ++a) dot += q * r[a] * (vadv[3 * (size_t)i + a] - vadv[3 * (size_t)j + a]);
+                d += dot * vol[j] * dt;
+            }
+            mask[(size_t)n * it + i] = d > 0;
+            if (d < 0) d = 0;
+            kappa[i] = d / alpha[i] / (dt * dt) / vol[i];
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double r[3];
+            FOR_NBR(L, g, i, j) {
+                double q = cubic_g(&k, rdiff(pos, i, j, r));
+                double sc = dt * vol[i] * vol[j] / mass[i] * (kappa[i] + kappa[j]) * q;
+                for (int a = 0; a < 3; ++a) vadv[3 * (size_t)i + a] -= sc * r[a];
+            }
+        }
+    }
+    if (vbar) {
+        /* v' = v - B kappa(v), kappa = P mask (c + A v): vbar_in = vbar + A^T P mask (-B^T vbar) */
+        double *kb = (double *)calloc(nn, sizeof(double));
+        for (int it = iters - 1; it >= 0; --it) {
+#pragma omp parallel for
+            for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+                uint32_t i = (uint32_t)ii;
+                kb[i] = 0.0;
+                if (mat[i] != 0) continue;
+                double s = 0, r[3];
+                const double ci = dt * vol[i] / mass[i];
+                FOR_NBR(L, g, i, j) {
+                    if (j == i) continue;
+                    double q = cubic_g(&k, rdiff(pos, i, j, r));
+                    double di = 0, dj = 0;
+                    for (int a = 0; a < 3; ++a) {
+                        di += r[a] * vbar[3 * (size_t)i + a];
+                        dj += r[a] * vbar[3 * (size_t)j + a];
+                    }
+                    s -= q * vol[j] * ci * di;
+                    if (mat[j] == 0) s += q * (dt * vol[j] / mass[j]) * vol[i] * dj;
+                }
+                kb[i] = mask[(size_t)n * it + i] ? s / alpha[i] / (dt * dt) / vol[i] : 0.0;
+            }
+#pragma omp parallel for
+            for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+                uint32_t i = (uint32_t)ii;
+                if (mat[i] != 0) continue;
+                double r[3], acc[3] = {0, 0, 0};
+                FOR_NBR(L, g, i, j) {
+                    if (j == i) continue;
+                    double q = cubic_g(&k, rdiff(pos, i, j, r));
+                    double c = dt * q * (vol[j] * kb[i] + (mat[j] == 0 ? vol[i] * kb[j] : 0.0));
+                    for (int a = 0; a < 3; ++a) acc[a] += c * r[a];
+                }
+                for (int a = 0; a < 3; ++a) vbar[3 * (size_t)i + a] += acc[a];
+            }
+        }
+        for (uint32_t i = 0; i < n; ++i)
+            if (mat[i] != 0) vbar[3 * (size_t)i] = vbar[3 * (size_t)i + 1] = vbar[3 * (size_t)i + 2] = 0.0;
+        free(kb);
+    }
+    free(mass); free(ratio); free(alpha); free(kappa); free(mask);
+}

@@ -72,6 +72,16 @@ void or_pbf_step_adjoint(uint32_t n, const int32_t *mat, const double *pos, cons
                          const double *vol, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
                          const or_pbf_params *p, double *xbar, double *vbar, double *kbar);
 
+/* DFSPH pressure solve as an operator (no counterpart in the reference): with
+ * the lists given and exactly `iters` iterations of the solve loop
+ * (DFSPHCudaImpl.cu:142-220), maps vadv (v*, in place) as the solve does, the
+ * compression ratio and alpha computed from pos / vol first; with vbar
+ * non-NULL it then maps vbar = dL/d(v* out) to dL/d(v* in) in place, each
+ * iteration's clamp pattern (delta > 0) frozen.  mass = rest_density * vol. */
+void or_dfsph_solve_op(uint32_t n, const int32_t *mat, const double *pos, const double *vol,
+                       const double *rest_density, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                       double h, double dt, int iters, double *vadv, double *vbar);
+
 /* DFSPH (DFSPHSolver.cpp:339-406): obj[n] gives each particle's object index
  * and obj_is_fluid/obj_count describe the objects (residual = mean over fluid
  * objects of the object's mean clamped compression error). */

@@ -144,3 +144,88 @@ def test_torch_autograd_wrapper(vtp_gpu):
     s.destroy()
     assert np.allclose(v0.grad.numpy(), gv[mask], rtol=1e-5, atol=1e-12)
     assert k.grad.item() == pytest.approx(gk, rel=1e-5)
+
+
+# ---------------------------------------------------------------- DFSPH pressure solve as an operator
+
+def _dfsph_case(vtp, seed=4):
+    sc = scenes.dam_break("DFSPH", 3000, seed=seed)
+    s = vtp.solver_from_scene(sc)
+    assert s.initialize() and s.tickNsteps(3)
+    return sc, s
+
+
+def test_oracle_dfsph_solve_adjoint_matches_finite_differences(oracle_lib):
+    sc = scenes.dam_break("DFSPH", 3000, seed=4)
+    o = oracle_lib.OracleSolver(sc)
+    o.step(3)
+    cnt, nb, _, _ = oracle_lib.neighbors(o.pos.astype(np.float32), o.grid)
+    f = o.mat == 0
+    rng = np.random.default_rng(1)
+    v = o.vel.copy()
+    v[f] += rng.normal(0, 0.05, (f.sum(), 3))
+    u = np.zeros_like(v)
+    u[f] = rng.normal(size=(f.sum(), 3))
+    _, vb = oracle_lib.dfsph_solve_op(o, cnt, nb, 5, v, u)
+    for _ in range(2):
+        d = np.zeros_like(v)
+        d[f] = rng.normal(size=(f.sum(), 3))
+        fp, _ = oracle_lib.dfsph_solve_op(o, cnt, nb, 5, v + 1e-6 * d)
+        fm, _ = oracle_lib.dfsph_solve_op(o, cnt, nb, 5, v - 1e-6 * d)
+        fd = float(((fp - fm) / 2e-6 * u).sum())
+        assert abs(float((vb * d).sum()) - fd) <= 1e-7 * abs(fd)
+
+
+@pytest.mark.gpu
+def test_gpu_dfsph_solve_vjp_matches_fp64_and_fd(vtp_gpu, oracle_lib):
+    from vtp import diff
+    sc, s = _dfsph_case(vtp_gpu)
+    n = s.counts()["total"]
+    mask = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    rng = np.random.default_rng(2)
+    v = s.get_field("vel")
+    v[mask] += rng.normal(0, 0.05, (mask.sum(), 3)).astype(np.float32)
+    iters = 5
+    vo, it = diff.dfsph_solve(s, v, 0, iters)
+    assert it == iters
+    u = np.zeros((n, 3), np.float32)
+    u[mask] = rng.normal(size=(mask.sum(), 3))
+    vb = diff.dfsph_solve_vjp(s, u)
+    # FP64 oracle operator on the same positions, volumes and lists
+    o = oracle_lib.OracleSolver(sc)
+    o.pos = s.get_field("pos").astype(np.float64)
+    o.vol = s.get_field("volume").astype(np.float64)
+    cnt, nb = s.get_neighbors(int(sc.config["DFSPH"]["Required"]["maxNeighborNum"]))
+    ov, ob = oracle_lib.dfsph_solve_op(o, cnt, nb, iters, v.astype(np.float64), u.astype(np.float64))
+    dv0 = np.linalg.norm(ov[mask] - v[mask])
+    rel_out = np.linalg.norm(vo[mask] - ov[mask]) / dv0
+    rel_vjp = np.linalg.norm(vb[mask] - ob[mask]) / np.linalg.norm(ob[mask])
+    print(f"solve output vs FP64 (relative to the solve's change) {rel_out:.2e}, vjp {rel_vjp:.2e}")
+    assert rel_out < TOL and rel_vjp < TOL
+    # directional derivatives: FP64 central differences of the oracle operator
+    for _ in range(3):
+        d = np.zeros((n, 3), np.float64)
+        d[mask] = rng.normal(size=(mask.sum(), 3))
+        fp, _ = oracle_lib.dfsph_solve_op(o, cnt, nb, iters, v.astype(np.float64) + 1e-6 * d)
+        fm, _ = oracle_lib.dfsph_solve_op(o, cnt, nb, iters, v.astype(np.float64) - 1e-6 * d)
+        fd = float(((fp - fm) / 2e-6 * u).sum())
+        ad = float((vb.astype(np.float64) * d).sum())
+        print(f"directional: fd {fd:.6e} vjp {ad:.6e}")
+        assert abs(ad - fd) <= TOL * abs(fd)
+    s.destroy()
+
+
+@pytest.mark.gpu
+def test_gpu_dfsph_solve_leaves_solver_state_unchanged(vtp_gpu):
+    from vtp import diff
+    sc, a = _dfsph_case(vtp_gpu, seed=6)
+    b = vtp_gpu.solver_from_scene(sc)
+    assert b.initialize() and b.tickNsteps(3)
+    diff.dfsph_solve(a, a.get_field("vel") * 1.1, 1)
+    assert a.tickNsteps(2) and b.tickNsteps(2)
+    assert np.array_equal(a.get_field("pos"), b.get_field("pos"))
+    assert np.array_equal(a.get_field("vel"), b.get_field("vel"))
+    with pytest.raises(vtp_gpu.VtpError, match="advanced"):
+        diff.dfsph_solve_vjp(a, np.zeros((a.counts()["total"], 3), np.float32))
+    a.destroy()
+    b.destroy()

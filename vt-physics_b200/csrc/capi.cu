@@ -194,6 +194,25 @@ int vtp_solver::parse_config(const json &c) {
     } catch (const std::exception &e) {
         return fail(VTP_ERR_CONFIG, std::string("config value error: ") + e.what());
     }
+    // EXPORT block (optional here; the reference's templates always carry it)
+    export_enabled = false;
+    if (c.contains("EXPORT")) {
+        try {
+            const json &ex = c["EXPORT"];
+            export_enabled = ex.at("SolverRequired").at("enable").get<bool>();
+            if (export_enabled) {
+                const float fps = ex.at("SolverRequired").at("exportFps").get<float>();
+                if (!(fps > 0.f)) return fail(VTP_ERR_CONFIG, "exportFps must be > 0");
+                export_gap = 1.f / fps;
+                for (const char *k : {"exportTargetDir", "exportFilePrefix"})
+                    if (!ex.at("Common").contains(k)) return fail(VTP_ERR_CONFIG, std::string("Export Common Config missing key: ") + k);
+                if (!ex.at("SolverRequired").contains("exportGroupPolicy"))
+                    return fail(VTP_ERR_CONFIG, "Export SolverRequired Config missing key: exportGroupPolicy");
+            }
+        } catch (const std::exception &e) {
+            return fail(VTP_ERR_CONFIG, std::string("EXPORT config error: ") + e.what());
+        }
+    }
     cfg = c;
     configured = true;
     // setConfig (re)defines scene 0 and drops any added scenes.
@@ -318,6 +337,8 @@ vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     a.tiles = d_tiles; a.ntiles = ntiles; a.scene_tiles = d_scene_tiles; a.persistent = persistent_tiles;
     a.state = solve ? solve + (size_t)which * scenes.size() : nullptr;
     a.sc = scn();
+    a.pva = pva;
+    a.pk = pk;
     a.tick = d_tick;
     a.unroll = unroll;
     return a;
@@ -514,6 +535,8 @@ int vtp_solver::initialize() {
         CU(cudaMemsetAsync(lambda, 0, std::max<size_t>(L.nf, 1) * sizeof(float), st));
     } else {
         for (int k = 0; k < 2; ++k) AL(&vadv.b[k], n);
+        AL(&pva, 2 * (size_t)n);
+        AL(&pk, n);
         AL(&ratio, L.nf);
         AL(&alpha, L.nf);
         AL(&kappa, L.nf);
@@ -609,6 +632,7 @@ int vtp_solver::initialize() {
     crashed = false;
     sim_time = 0.f;
     steps_done = 0;
+    out_frames = frames_written = 0;
     graphs_ready = false;
     parity = 0;
 #undef AL
@@ -620,7 +644,8 @@ int vtp_solver::initialize() {
 int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
     vtp::DfsphArgs a = dfsph_args(which);
     vtp::dfsph_solve_begin(s, solve + (size_t)which * scenes.size(), loop + which, nscenes());
-    launches_per_tick += 1;
+    PROF(this, "dfsph_solve_pack", vtp::dfsph_solve_pack(s, a));
+    launches_per_tick += 2;
     if (capture && device_loop) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t g;
@@ -836,6 +861,7 @@ int vtp_solver::tick_n(uint32_t n) {
         }
         sim_time += dt;
         ++steps_done;
+        if ((rc = maybe_export())) return rc;
         if (solves && stop_on_crash) {
             // The reference stops ticking after a solve ran past 100 iterations.
             if ((rc = check_status())) {

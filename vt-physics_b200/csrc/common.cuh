@@ -174,6 +174,19 @@ __device__ __forceinline__ float tension_c(float r, float h, float csigma, float
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 
+// Two adjacent float4 (one 32-byte aligned row of a packed array) in one
+// 256-bit read-only load.
+struct F4x2 {
+    float4 a, b;
+};
+__device__ __forceinline__ F4x2 ldg8(const float4 *p) {
+    F4x2 r;
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w), "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z), "=f"(r.b.w)
+        : "l"(p));
+    return r;
+}
+
 // Walks `cnt` list entries (warp-interleaved ELL, slot t at lst[t * 32]) in
 // order, U at a time: the list indices of the next batch are loaded before the
 // current batch's gathers (`load(j)`) are issued, so each thread keeps U

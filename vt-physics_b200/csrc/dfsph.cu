@@ -84,10 +84,6 @@ __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_
 struct PV {
     float4 q, v;
 };
-struct PK {
-    float4 q;
-    float k;
-};
 struct PVV {
     float4 q, v, va;
 };
@@ -140,18 +136,19 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
             const uint32_t n = a.ncnt[r];
             float d = a.ratio[r] - 1.f;
             const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-            nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
-                        [&](uint32_t j) { return PV{ldg4(a.pos + j), ldg4(a.vadv + j)}; },
-                        [&](uint32_t, const PV &e) {
-                            const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+            nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg8(a.pva + 2 * (size_t)j); },
+                        [&](uint32_t, const F4x2 &e) {
+                            const float rx = p.x - e.a.x, ry = p.y - e.a.y, rz = p.z - e.a.z;
                             const float g = cubic_g(dist2(rx, ry, rz), a.k);
                             const float dot =
-                                g * (rx * (vi.x - e.v.x) + ry * (vi.y - e.v.y) + rz * (vi.z - e.v.z));
-                            d = __fmaf_rn(dot * e.q.w, a.dt, d);
+                                g * (rx * (vi.x - e.b.x) + ry * (vi.y - e.b.y) + rz * (vi.z - e.b.z));
+                            d = __fmaf_rn(dot * e.a.w, a.dt, d);
                         });
             if (d < 0.f) d = 0.f;
             a.delta[r] = d;
-            a.kappa[r] = d / a.alpha[r] * a.inv_dt2 / p.w;
+            const float kap = d / a.alpha[r] * a.inv_dt2 / p.w;
+            a.kappa[r] = kap;
+            a.pk[r] = make_float4(p.x, p.y, p.z, kap);
             contrib = (double)d;
             if (MULTI) obj = (int)a.obj_of[a.orig[r]] - (int)a.scene_tiles[tile.z].obj0;
         }
@@ -181,19 +178,31 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
         const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
         const float ci = a.dt * p.w / mi;   // dt V_i / m_i
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary).
-        nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
-                    [&](uint32_t j) { return PK{ldg4(a.pos + j), j < a.nf ? __ldg(a.kappa + j) : 0.f}; },
-                    [&](uint32_t, const PK &e) {
-                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+        // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary); the
+        // packed row carries kappa_j for fluid rows (volume vol_f) and V_j for boundary rows.
+        nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pk + j); },
+                    [&](uint32_t j, const float4 &e) {
+                        const bool fj = j < a.nf;
+                        const float Vj = fj ? a.vol_f : e.w, kj = fj ? e.w : 0.f;
+                        const float rx = p.x - e.x, ry = p.y - e.y, rz = p.z - e.z;
                         const float g = cubic_g(dist2(rx, ry, rz), a.k);
-                        const float s = ci * e.q.w * (ki + e.k) * g;
+                        const float s = ci * Vj * (ki + kj) * g;
                         v.x = __fmaf_rn(-s, rx, v.x);
                         v.y = __fmaf_rn(-s, ry, v.y);
                         v.z = __fmaf_rn(-s, rz, v.z);
                     });
         a.vadv[r] = v;
+        a.pva[2 * (size_t)r + 1] = v;
     }
+}
+
+__global__ void k_solve_pack(DfsphArgs a, uint32_t n) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const float4 p = a.pos[r];
+    a.pva[2 * (size_t)r] = p;
+    a.pva[2 * (size_t)r + 1] = a.vadv[r];
+    a.pk[r] = r < a.nf ? make_float4(p.x, p.y, p.z, 0.f) : p;
 }
 
 __global__ void k_solve_begin(SolveState *s, LoopState *loop, int nscenes) {
@@ -406,6 +415,10 @@ void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block) {
 }
 void dfsph_solve_begin(cudaStream_t st, SolveState *s, LoopState *loop, int nscenes) {
     k_solve_begin<<<1, 256, 0, st>>>(s, loop, nscenes);
+}
+void dfsph_solve_pack(cudaStream_t st, const DfsphArgs &a) {
+    const uint32_t n = a.nf + a.nb;
+    if (n) k_solve_pack<<<nblk(n, 256), 256, 0, st>>>(a, n);
 }
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
     const unsigned nb = dfsph_tile_grid(a.ntiles, block, a.persistent);

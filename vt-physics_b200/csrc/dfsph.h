@@ -63,6 +63,9 @@ struct DfsphArgs {
     uint64_t *tick;             // substep counter, advanced by the finalize pass
     int unroll;                 // neighbours in flight per thread (1, 2, 4, 8)
     const float *rest_density;  // IMM / IMM-CT: per-row rest density (mass = rest_density * volume)
+    // Packed gather rows of the pressure solve (filled by dfsph_solve_pack):
+    float4 *pva;                // [2n] row j = {pos_j, v*_j} (32 B): one 256-bit load per pair in solve_a
+    float4 *pk;                 // [n] {x, y, z, kappa_j} for fluid rows, {x, y, z, V_j} for boundary rows
 };
 
 struct SolveCtl {
@@ -87,6 +90,8 @@ void dfsph_rigid_volume(cudaStream_t st, const DfsphArgs &a, const uint32_t *bnc
                         float *rest_density_b);
 void dfsph_ratio_alpha(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_begin(cudaStream_t st, SolveState *s, LoopState *loop, int nscenes);
+// Packs pva / pk for a pressure solve (after v* and positions are final for it).
+void dfsph_solve_pack(cudaStream_t st, const DfsphArgs &a);
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status);

@@ -48,6 +48,13 @@ struct DiffState {
     float *sbar = nullptr;
     double *kpart = nullptr, *kacc = nullptr;
     uint32_t kblocks = 0;
+    // DFSPH pressure-solve operator: per-iteration delta (clamp pattern) and work arrays
+    int df_which = -1;
+    uint32_t df_iters = 0;
+    uint64_t df_steps = 0;
+    std::vector<float *> df_delta;
+    float4 *df_vb = nullptr, *df_save = nullptr;
+    float *df_kb = nullptr;
 
     ~DiffState() {
         for (void *p : mem) cudaFree(p);
@@ -259,6 +266,69 @@ __global__ void k_adj_kreduce(const double *part, uint32_t nb, double *acc) {
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
     s = block_sum_d(s);
     if (threadIdx.x == 0) *acc += s;
+}
+
+// DFSPH pressure-solve adjoint.  One iteration maps v -> v - B kappa(v) with
+// kappa_i = P_i max(0, c_i + (A v)_i), (A v)_i = dt sum_j V_j g_ij r_ij.(v_i - v_j),
+// (B kappa)_i = c_i sum_j V_j (kappa_i + kappa_j) g_ij r_ij, c_i = dt V_i / m_i,
+// P_i = 1 / (alpha_i dt^2 V_i) (vf_update_vel_adv_from_kappa_*, compute_kappa_*,
+// DFSPHCudaImpl.cu:142-220); the clamp pattern of each iteration is recorded.
+struct DfAdjArgs {
+    uint32_t nf, ell_stride;
+    Cubic k;
+    float dt, inv_dt2, mass_f;
+    const uint32_t *nbr, *ncnt;
+    const float4 *pos;      // w = volume
+    const float *alpha, *delta;
+    float4 *vb;
+    float *kb;
+};
+
+// kappa-bar = -B^T vbar, then delta-bar = P mask kappa-bar (stored in kb).
+__global__ void __launch_bounds__(256) k_dadj_kappa(DfAdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r], vi = a.vb[r];
+    const float ci = a.dt * p.w / a.mass_f;
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    float s = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = a.pos[j];
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+        s -= g * q.w * ci * (rx * vi.x + ry * vi.y + rz * vi.z);
+        if (j < a.nf) {
+            const float4 vj = a.vb[j];
+            s += g * (a.dt * q.w / a.mass_f) * p.w * (rx * vj.x + ry * vj.y + rz * vj.z);
+        }
+    }
+    a.kb[r] = a.delta[r] > 0.f ? s / a.alpha[r] * a.inv_dt2 / p.w : 0.f;
+}
+
+// vbar += A^T delta-bar.
+__global__ void __launch_bounds__(256) k_dadj_vel(DfAdjArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.pos[r];
+    const float ki = a.kb[r];
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = a.pos[j];
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float g = cubic_g(dist2(rx, ry, rz), a.k);
+        const float c = a.dt * g * (q.w * ki + (j < a.nf ? p.w * a.kb[j] : 0.f));
+        ax += c * rx;
+        ay += c * ry;
+        az += c * rz;
+    }
+    float4 v = a.vb[r];
+    v.x += ax; v.y += ay; v.z += az;
+    a.vb[r] = v;
 }
 
 __global__ void k_f3_to_f4(uint32_t n, const float *src, float4 *dst) {
@@ -514,6 +584,129 @@ int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32
     cudaFree(dc);
     cudaFree(dn);
     if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- DFSPH pressure solve as an operator
+
+namespace {
+
+int dfsph_op_ready(vtp_solver *s) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    if (s->type != VTP_SOLVER_DFSPH) return fail(VTP_ERR_CONFIG, "the pressure-solve operator is a DFSPH operator");
+    if (s->nscenes() != 1) return fail(VTP_ERR_CONFIG, "the pressure-solve operator runs a single scene");
+    return VTP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vtp_solver_dfsph_solve_forward(vtp_solver *s, int which, const float *v_in, float *v_out, uint32_t force_iters,
+                                   uint32_t *iterations) {
+    int rc = dfsph_op_ready(s);
+    if (rc) return rc;
+    if (!s->initialized && (rc = s->initialize())) return rc;
+    if (which != 0 && which != 1) return fail(VTP_ERR_ARG, "which must be 0 (divergence) or 1 (density)");
+    if (!v_in) return fail(VTP_ERR_ARG, "null v_in");
+    if (!s->diff) s->diff = std::make_shared<vtp::DiffState>();
+    vtp::DiffState &d = *s->diff;
+    const uint32_t n = s->L.n, nf = s->L.nf;
+    const size_t nfa = std::max<uint32_t>(nf, 1);
+    if (!d.df_vb && ((rc = d.alloc(&d.df_vb, nfa)) || (rc = d.alloc(&d.df_save, nfa)) ||
+                     (rc = d.alloc(&d.df_kb, nfa))))
+        return rc;
+    // Neighbour search of the current state (the next substep's lists), re-sorted rows copied
+    // back so the substep graphs' buffer parity is kept, then compression ratio and alpha.
+    vtp::Carry carry{};
+    carry.nf4 = 1;
+    carry.src4[0] = s->vadv.c();
+    carry.dst4[0] = s->vadv.n();
+    vtp::ugns_sort(s->st, s->scn(), s->nbuckets, 0, nf, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(),
+                   s->orig.c(), s->orig.n(), carry, 0.f, s->u, s->u.fstart);
+    if (nf) {
+        CU(cudaMemcpyAsync(s->pos.c(), s->pos.n(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+        CU(cudaMemcpyAsync(s->vel.c(), s->vel.n(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+        CU(cudaMemcpyAsync(s->orig.c(), s->orig.n(), (size_t)nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s->st));
+        CU(cudaMemcpyAsync(s->vadv.c(), s->vadv.n(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+        CU(cudaMemcpyAsync(d.df_save, s->vadv.c(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    }
+    vtp::ugns_build_lists(s->st, s->scn(), s->L, 0, nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
+                          s->d_status, s->d_overflow, s->block);
+    vtp::dfsph_ratio_alpha(s->st, s->dfsph_args(which), s->block);
+    const size_t n3 = (size_t)n * 3 * sizeof(float);
+    if ((rc = s->ensure_stage(n3))) return rc;
+    CU(cudaMemcpyAsync(s->stage, v_in, n3, cudaMemcpyHostToDevice, s->st));
+    vtp::gather_orig_to_f4(s->st, nf, s->stage, s->orig.c(), s->vadv.c(), 1);
+    // The solve loop, host-driven, with each iteration's delta recorded.
+    vtp::DfsphArgs a = s->dfsph_args(which);
+    vtp::SolveCtl c = s->solve_ctl(which, cudaGraphConditionalHandle{}, 0);
+    c.force_iters = force_iters;
+    c.force_seq = nullptr;
+    vtp::dfsph_solve_begin(s->st, s->solve + (size_t)which * s->scenes.size(), s->loop + which, s->nscenes());
+    vtp::dfsph_solve_pack(s->st, a);
+    uint32_t it = 0;
+    for (; it < 101; ++it) {
+        if (d.df_delta.size() <= it) {
+            float *p = nullptr;
+            if ((rc = d.alloc(&p, nfa))) return rc;
+            d.df_delta.push_back(p);
+        }
+        vtp::dfsph_solve_a(s->st, a, s->block);
+        if (nf) CU(cudaMemcpyAsync(d.df_delta[it], s->delta, (size_t)nf * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+        vtp::dfsph_solve_b(s->st, a, s->block);
+        vtp::dfsph_solve_end(s->st, c, s->partials, s->d_status);
+        CU(cudaMemcpyAsync(s->h_pinned + 2, &s->loop[which].running, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+        if (!s->h_pinned[2]) break;
+    }
+    const uint32_t iters = std::min<uint32_t>(it + 1, 101);
+    if (v_out) {
+        CU(cudaMemsetAsync(s->stage, 0, n3, s->st));
+        vtp::scatter_f4_to_orig(s->st, nf, s->vadv.c(), s->orig.c(), s->stage);
+        CU(cudaMemcpyAsync(v_out, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+    }
+    // Leave v* as the solver had it.
+    if (nf) CU(cudaMemcpyAsync(s->vadv.c(), d.df_save, (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    CU(cudaGetLastError());
+    d.df_which = which;
+    d.df_iters = iters;
+    d.df_steps = s->steps_done;
+    if (iterations) *iterations = iters;
+    return s->check_status();
+}
+
+int vtp_solver_dfsph_solve_backward(vtp_solver *s, const float *vbar_out, float *vbar_in) {
+    int rc = dfsph_op_ready(s);
+    if (rc) return rc;
+    if (!s->diff || s->diff->df_which < 0) return fail(VTP_ERR_STATE, "dfsph_solve_backward before dfsph_solve_forward");
+    vtp::DiffState &d = *s->diff;
+    if (d.df_steps != s->steps_done) return fail(VTP_ERR_STATE, "the solver advanced since dfsph_solve_forward");
+    if (!vbar_out || !vbar_in) return fail(VTP_ERR_ARG, "null argument");
+    const uint32_t n = s->L.n, nf = s->L.nf;
+    const size_t n3 = (size_t)n * 3 * sizeof(float);
+    if ((rc = s->ensure_stage(n3))) return rc;
+    CU(cudaMemcpyAsync(s->stage, vbar_out, n3, cudaMemcpyHostToDevice, s->st));
+    vtp::gather_orig_to_f4(s->st, nf, s->stage, s->orig.c(), d.df_vb, 0);
+    vtp::DfAdjArgs a{};
+    a.nf = nf; a.ell_stride = s->L.ell_stride; a.k = s->kc;
+    a.dt = s->dt; a.inv_dt2 = s->inv_dt2; a.mass_f = s->rho_f * s->vol0;
+    a.nbr = s->u.nbr; a.ncnt = s->u.ncnt; a.pos = s->pos.c(); a.alpha = s->alpha;
+    a.vb = d.df_vb; a.kb = d.df_kb;
+    const unsigned G = vtp::nblk(std::max<uint32_t>(nf, 1), 256);
+    for (int it = (int)d.df_iters - 1; it >= 0 && nf; --it) {
+        a.delta = d.df_delta[it];
+        vtp::k_dadj_kappa<<<G, 256, 0, s->st>>>(a);
+        vtp::k_dadj_vel<<<G, 256, 0, s->st>>>(a);
+    }
+    CU(cudaMemsetAsync(s->stage, 0, n3, s->st));
+    vtp::scatter_f4_to_orig(s->st, nf, d.df_vb, s->orig.c(), s->stage);
+    CU(cudaMemcpyAsync(vbar_in, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    CU(cudaGetLastError());
     return VTP_OK;
 }
 

@@ -113,6 +113,7 @@ struct vtp_solver {
     float *vol = nullptr, *density = nullptr, *lambda = nullptr;
     float *ratio = nullptr, *alpha = nullptr, *kappa = nullptr, *delta = nullptr, *rest_b = nullptr;
     float4 *acc_tmp = nullptr, *normal = nullptr;
+    float4 *pva = nullptr, *pk = nullptr;   // packed gather rows of the pressure solve
     double *partials = nullptr, *inv_count = nullptr;
     uint16_t *obj_of = nullptr;
     vtp::SolveState *solve = nullptr;   // [2][S]: divergence, density per scene
@@ -136,6 +137,10 @@ struct vtp_solver {
     float stage_ms[3] = {0, 0, 0};
 
     uint64_t steps_done = 0;
+    // PLY export (EXPORT block of the config)
+    bool export_enabled = false;
+    float export_gap = 0.f;
+    uint32_t out_frames = 0, frames_written = 0;
     vtp_stats stats{};
     std::vector<vtp_stats> scene_stats;
 
@@ -197,6 +202,8 @@ struct vtp_solver {
     vtp::SolveCtl solve_ctl(int which, cudaGraphConditionalHandle h, int use_cond);
     int check_status();
     int read_solve_states();
+    int export_frame();
+    int maybe_export();
     int sync_parity();
 };
 

@@ -1,10 +1,13 @@
 """Launch-configuration autotuner for the neighbour passes.
 
-Sweeps threads per block and the neighbour-loop unroll (neighbours kept in
-flight per thread) on a scene, timing each candidate with the per-kernel
-CUDA-event profiler of the library, and returns the fastest configuration
-for the solver's substep.  Results are plain dicts so callers can cache them
-(``"B200": {"blockSize": b, "unroll": u}`` in the solver config).
+Sweeps threads per block (= rows per scene-offset tile), the neighbour-loop
+unroll (neighbours kept in flight per thread) and the tile-grid mode of the
+pressure-solve passes (one block per tile, or a persistent grid) on a scene
+or a batch of scenes, timing each candidate with the per-kernel CUDA-event
+profiler of the library, and returns the fastest configuration for the
+substep.  Results are plain dicts so callers can cache them
+(``"B200": {"blockSize": b, "unroll": u, "persistentTiles": p}`` in the
+solver config).
 """
 from __future__ import annotations
 
@@ -12,30 +15,39 @@ import itertools
 import json
 import time
 
-from .solver import solver_from_scene
+from .solver import solver_from_scene, solver_from_scenes
 
 BLOCKS = (64, 128, 256)
 UNROLLS = (1, 2, 4, 8)
+PERSISTENT = (False,)
 
 
-def tune(scene, warmup: int = 3, steps: int = 3, blocks=BLOCKS, unrolls=UNROLLS, verbose: bool = False) -> dict:
-    """Return {"best": {...}, "trials": [...]} for one scene."""
+def tune(scene, warmup: int = 3, steps: int = 3, blocks=BLOCKS, unrolls=UNROLLS, persistent=PERSISTENT,
+         verbose: bool = False) -> dict:
+    """Return {"best": {...}, "trials": [...]} for one scene, or a list of scenes of one
+    solver type (tuned as one batched solver)."""
     trials = []
-    for b, u in itertools.product(blocks, unrolls):
-        s = solver_from_scene(scene, extra={"blockSize": b, "unroll": u})
+    for b, u, pt in itertools.product(blocks, unrolls, persistent):
+        extra = {"blockSize": b, "unroll": u, "persistentTiles": bool(pt)}
+        if isinstance(scene, (list, tuple)):
+            s, _ = solver_from_scenes(list(scene), extra=extra)
+        else:
+            s = solver_from_scene(scene, extra=extra)
         s.initialize()
         if warmup:
             s.tickNsteps(warmup)
         prof = s.profile_kernels(steps)
         s.destroy()
         total = sum(v[0] for v in prof.values())
-        rec = {"blockSize": b, "unroll": u, "ms_per_step": total / steps,
+        rec = {"blockSize": b, "unroll": u, "persistentTiles": bool(pt), "ms_per_step": total / steps,
                "kernels": {k: v[0] / max(v[1], 1) for k, v in prof.items()}}
         trials.append(rec)
         if verbose:
-            print(json.dumps({k: rec[k] for k in ("blockSize", "unroll", "ms_per_step")}), flush=True)
+            print(json.dumps({k: rec[k] for k in ("blockSize", "unroll", "persistentTiles", "ms_per_step")}),
+                  flush=True)
     best = min(trials, key=lambda r: r["ms_per_step"])
-    return {"best": {"blockSize": best["blockSize"], "unroll": best["unroll"]}, "trials": trials,
+    return {"best": {"blockSize": best["blockSize"], "unroll": best["unroll"],
+                     "persistentTiles": best["persistentTiles"]}, "trials": trials,
             "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
 
 
@@ -48,10 +60,16 @@ if __name__ == "__main__":
     from vtp import scenes
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scene", default="dfsph_1m", choices=["dfsph_1m", "pbf"])
+    ap.add_argument("--scene", default="dfsph_1m", choices=["dfsph_1m", "pbf", "batched_pbf", "batched_dfsph"])
+    ap.add_argument("--persistent", action="store_true", help="also try the persistent tile grid")
     a = ap.parse_args()
-    sc = scenes.dfsph_1m() if a.scene == "dfsph_1m" else scenes.pbf_dam_break()
-    res = tune(sc, verbose=True)
+    if a.scene.startswith("batched"):
+        mix = scenes.batched_scenes()
+        sc = [m for m in mix if m.solver == ("PBF" if a.scene == "batched_pbf" else "DFSPH")]
+    else:
+        sc = scenes.dfsph_1m() if a.scene == "dfsph_1m" else scenes.pbf_dam_break()
+    res = tune(sc, persistent=(False, True) if a.persistent else PERSISTENT, verbose=True)
     print(json.dumps({"best": res["best"], "trials": [{k: t[k] for k in t if k != "kernels"} for t in res["trials"]]}))
     for t in res["trials"]:
-        print(t["blockSize"], t["unroll"], json.dumps({k: round(v, 4) for k, v in sorted(t["kernels"].items())}))
+        print(t["blockSize"], t["unroll"], t["persistentTiles"],
+              json.dumps({k: round(v, 4) for k, v in sorted(t["kernels"].items())}))

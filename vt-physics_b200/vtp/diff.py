@@ -107,3 +107,40 @@ def make_rollout(scene, steps: int, checkpoint_every: int = 20, extra=None):
             return torch.from_numpy(gv[mask].copy()).to(dev), torch.tensor(gk, dtype=torch.float32, device=dev)
 
     return PbfRollout.apply
+
+
+def dfsph_solve(s, v_in, which: int = 0, force_iters: int = 0):
+    """One DFSPH pressure solve on the solver's current positions: (v* out, iterations)."""
+    n = s.counts()["total"]
+    vi = np.ascontiguousarray(v_in, np.float32).reshape(n, 3)
+    vo = np.zeros((n, 3), np.float32)
+    it = C.c_uint32()
+    check(lib().vtp_solver_dfsph_solve_forward(s._h, int(which), vi.ctypes.data, vo.ctypes.data, int(force_iters),
+                                               C.byref(it)), "dfsph_solve_forward")
+    return vo, it.value
+
+
+def dfsph_solve_vjp(s, vbar_out):
+    """dL/d(v* in) of the last dfsph_solve, given dL/d(v* out)."""
+    n = s.counts()["total"]
+    vb = np.ascontiguousarray(vbar_out, np.float32).reshape(n, 3)
+    out = np.zeros((n, 3), np.float32)
+    check(lib().vtp_solver_dfsph_solve_backward(s._h, vb.ctypes.data, out.ctypes.data), "dfsph_solve_backward")
+    return out
+
+
+def make_dfsph_solve(s, which: int = 0, force_iters: int = 0):
+    """torch.autograd.Function over the pressure solve of solver `s` at its current state."""
+    import torch
+
+    class DfsphSolve(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, v):
+            out, _ = dfsph_solve(s, v.detach().cpu().numpy(), which, force_iters)
+            return torch.from_numpy(out).to(v.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            return torch.from_numpy(dfsph_solve_vjp(s, g.detach().cpu().numpy())).to(g.device)
+
+    return DfsphSolve.apply
