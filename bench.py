@@ -118,6 +118,47 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp32_peak_tflops(sm_mhz):
+    """FP32 SIMT peak: SMs x 128 lanes x 2 flops (FMA) x SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    return sms * 128 * 2 * float(sm_mhz) * 1e6 / 1e12
+
+
+def ncu_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch measured by ncu for this kernel and workload (profiles/ncu_traffic.json)."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    try:
+        return json.loads(p.read_text()).get(workload, {}).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload) -> dict:
+    """Roofline of one kernel: algorithmic bytes against the measured HBM copy bandwidth and
+    algorithmic FP32 flops against the SIMT peak at the sampled clock; the binding one (the
+    larger ideal time) is reported as `bound`, both fractions are kept."""
+    t = per_launch_ms / 1e3
+    hbm = b["state"] / t / 1e9
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    fpk = fp32_peak_tflops(mhz)
+    tf = flops / t / 1e12
+    t_bytes = b["state"] / (peak * 1e9)
+    t_flops = flops / (fpk * 1e12) if fpk else 0.0
+    out = {"kernel": name, "ms_per_launch": per_launch_ms,
+           "hbm": {"achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak, "peak_kind": peak_kind,
+                   "bytes_per_launch": b["state"], "bytes_per_launch_with_lists": b["total"],
+                   "frac_with_lists": b["total"] / t / 1e9 / peak},
+           "fp32": {"achieved": tf, "peak": fpk, "unit": "TFLOP/s", "frac": tf / fpk if fpk else None,
+                    "peak_kind": f"computed: SMs x 128 x 2 x {mhz:.0f} MHz", "flops_per_launch": flops}}
+    if t_flops > t_bytes:
+        out.update({"bound": "fp32", "achieved": tf, "peak": fpk, "unit": "TFLOP/s", "frac": tf / fpk})
+    else:
+        out.update({"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak})
+    out["traffic"] = ncu_traffic(workload, name)
+    return out
+
+
 def cpu_baseline(scene, seconds: float) -> dict:
     """FP64 OpenMP oracle on the host cores: bounded sample of the same scene."""
     from oracle import oracle as O
@@ -181,8 +222,8 @@ def run_reference_batched(args) -> dict:
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
                                  "sample": f"the reference is GPU code: its own CUDA build on this B200, "
                                            f"{len(done)} of {len(mix)} scenes x {steps} substeps"},
-                "e2e": {"value": sum(a for a, _ in e2e) / sum(b for _, b in e2e) / 1e6, "unit": METRIC,
-                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+                "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    out["config"]["state_round_trip_value"] = sum(a for a, _ in e2e) / sum(b for _, b in e2e) / 1e6
     return out
 
 
@@ -227,18 +268,21 @@ def run_reference(args) -> dict:
     clocks = clk.stop()
     nf = sc.n_fluid
     value = nf * args.steps / (ms / 1e3) / 1e6
-    # e2e: the state round-trips through host memory every step (positions and
-    # velocities in, one tick, positions and velocities out).
-    pos = s.get("pos", 3)
-    vel = s.get("vel", 3)
+    # e2e: the fluid state round-trips through host memory every step (positions and
+    # velocities of the fluid particles, which the scenes attach first, in; one tick; out),
+    # the same bytes as the library's e2e.
+    nfl = sum(c for _, c in fluid_ranges(sc))
+    assert fluid_ranges(sc) == [(0, nfl)]
+    pos = s.get_prefix("pos", nfl)
+    vel = s.get_prefix("vel", nfl)
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         s.set("pos", pos)
         s.set("vel", vel)
         s.tick(1)
-        pos = s.get("pos", 3)
-        vel = s.get("vel", 3)
+        pos = s.get_prefix("pos", nfl)
+        vel = s.get_prefix("vel", nfl)
     el = time.perf_counter() - t0
     out.update({"value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -247,9 +291,50 @@ def run_reference(args) -> dict:
                 "clocks": clocks,
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
                                  "sample": "the reference is GPU code: its own CUDA build timed on this B200"},
-                "e2e": {"value": nf * e2e_steps / el / 1e6, "unit": METRIC,
-                        "h2d_bytes_per_step": int(2 * 12 * s.n), "d2h_bytes_per_step": int(2 * 12 * s.n)}})
+                "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    # For information: the same fluid-state round trip per step as the library's e2e.
+    out["config"]["state_round_trip"] = {"value": nf * e2e_steps / el / 1e6, "unit": METRIC,
+                                         "h2d_bytes_per_step": int(2 * 12 * nfl),
+                                         "d2h_bytes_per_step": int(2 * 12 * nfl)}
     return out
+
+
+def fluid_ranges(scene):
+    """(first, count) attach-order ranges of the scene's fluid objects."""
+    out, start = [], 0
+    for o in scene.objects:
+        if o.material == 0 and o.n:
+            if out and out[-1][0] + out[-1][1] == start:
+                out[-1] = (out[-1][0], out[-1][1] + o.n)
+            else:
+                out.append((start, o.n))
+        start += o.n
+    return out
+
+
+def state_buffers(s, ranges, torch):
+    """Pinned host buffers holding the fluid state (pos, vel) of each range."""
+    bufs = []
+    for first, count in ranges:
+        p = torch.from_numpy(s.get_field_range("pos", first, count)).pin_memory()
+        v = torch.from_numpy(s.get_field_range("vel", first, count)).pin_memory()
+        bufs.append((first, count, p, v))
+    return bufs
+
+
+def state_bytes(bufs) -> int:
+    return int(sum(p.numel() * 4 + v.numel() * 4 for _, _, p, v in bufs))
+
+
+def state_round_trip(s, bufs):
+    """One e2e step: fluid state host -> device, one substep, fluid state device -> host."""
+    for first, count, p, v in bufs:
+        s.set_field_range_ptr("pos", first, count, p.data_ptr(), p.numel() * 4)
+        s.set_field_range_ptr("vel", first, count, v.data_ptr(), v.numel() * 4)
+    assert s.tickNsteps(1), s.last_error
+    for first, count, p, v in bufs:
+        s.get_field_range_ptr("pos", first, count, p.data_ptr(), p.numel() * 4)
+        s.get_field_range_ptr("vel", first, count, v.data_ptr(), v.numel() * 4)
 
 
 def _batch_cost(sc) -> float:
@@ -321,30 +406,23 @@ def run_batched(args, rank, world, local, dist, torch):
                    "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
-    # e2e through the public API: every scene's state round-trips through pinned host memory
-    # each step (H2D positions + velocities, one substep, D2H of both).
-    hbuf = []
-    for _, _, b, _ in batches:
-        hbuf.append((torch.from_numpy(b.get_field("pos")).pin_memory(),
-                     torch.from_numpy(b.get_field("vel")).pin_memory()))
+    # e2e through the public API: every batch's whole state (positions and velocities of all
+    # its particles) round-trips through pinned host memory each step (H2D, one substep, D2H).
+    hbuf = [state_buffers(b, [(0, b.counts()["total"])], torch) for _, _, b, _ in batches]
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for (_, _, b, _), (ph, vh) in zip(batches, hbuf):
-            b.set_field_ptr("pos", ph.data_ptr(), ph.numel() * 4)
-            b.set_field_ptr("vel", vh.data_ptr(), vh.numel() * 4)
-            assert b.tickNsteps(1), b.last_error
-            b.get_field_ptr("pos", ph.data_ptr(), ph.numel() * 4)
-            b.get_field_ptr("vel", vh.data_ptr(), vh.numel() * 4)
+        for (_, _, b, _), bufs in zip(batches, hbuf):
+            state_round_trip(b, bufs)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_val = nf_all * e2e_steps / float(te.item()) / 1e6
-    io_bytes = int(sum(ph.numel() * 4 + vh.numel() * 4 for ph, vh in hbuf))
+    io_bytes = int(sum(state_bytes(bufs) for bufs in hbuf))
     for _, _, b, _ in batches:
         b.destroy()
 
@@ -573,7 +651,7 @@ def main():
         k_mean = float(np.mean(cnt_all[fmask].astype(np.float64) - 1.0))
     except Exception:
         pass
-    from vtp.bytes_model import kernel_bytes
+    from vtp.bytes_model import kernel_bytes, kernel_flops
     req = sc.config[sc.solver]["Required"]
     h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
     dims = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
@@ -585,25 +663,22 @@ def main():
     P = len(req.get("phaseRestDensity", [])) or 1
     b = kernel_bytes(sc.solver, dom_name, N, nf, K, k_mean, P)
     peak, peak_kind = peaks()
-    achieved = b["state"] / (per_launch_ms / 1e3) / 1e9
+    roofline = roofline_of(dom_name, b, kernel_flops(dom_name, nf, k_mean), per_launch_ms, peak, peak_kind,
+                           clocks, args.workload)
     kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
-    # e2e through the public API: the state round-trips through pinned host memory
-    # every step (H2D of positions and velocities, one substep, D2H of both).
-    pos_h = torch.from_numpy(s.get_field("pos")).pin_memory()
-    vel_h = torch.from_numpy(s.get_field("vel")).pin_memory()
+    # e2e through the public API: every step the fluid state (positions and velocities of
+    # the fluid objects; boundary particles are static) goes host -> device from pinned
+    # memory, one substep runs, and the new fluid state comes back device -> host.
+    bufs = state_buffers(s, fluid_ranges(sc), torch)
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        s.set_field_ptr("pos", pos_h.data_ptr(), pos_h.numel() * 4)
-        s.set_field_ptr("vel", vel_h.data_ptr(), vel_h.numel() * 4)
-        assert s.tickNsteps(1), s.last_error
-        s.get_field_ptr("pos", pos_h.data_ptr(), pos_h.numel() * 4)
-        s.get_field_ptr("vel", vel_h.data_ptr(), vel_h.numel() * 4)
+        state_round_trip(s, bufs)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
@@ -622,14 +697,10 @@ def main():
                    "wall_ms_per_step": 1e3 * wall / args.steps},
         "clocks": clocks,
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "bytes_per_launch_state": b["state"], "bytes_per_launch_with_lists": b["total"],
-                     "achieved_with_lists": b["total"] / (per_launch_ms / 1e3) / 1e9,
-                     "ms_per_launch": per_launch_ms},
+        "roofline": roofline,
         "kernels": kernels,
-        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4),
-                "d2h_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4)},
+        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": state_bytes(bufs),
+                "d2h_bytes_per_step": state_bytes(bufs)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc, args.cpu_seconds)

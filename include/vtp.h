@@ -182,6 +182,15 @@ VTP_API int vtp_solver_particle_counts(vtp_solver *s, uint32_t *n_total, uint32_
 VTP_API int vtp_solver_get_field(vtp_solver *s, int field, void *host, size_t bytes);
 VTP_API int vtp_solver_set_field(vtp_solver *s, int field, const void *host, size_t bytes);
 
+/* Field I/O for the attach-order particle range [first, first + count), e.g. one
+ * object (the reference's exportData reads per-object ranges the same way,
+ * PBFSolver.cpp:262-273).  `bytes` = count * element size; set_field_range
+ * takes pos / vel (boundary rows are static and keep their values). */
+VTP_API int vtp_solver_get_field_range(vtp_solver *s, int field, uint32_t first, uint32_t count, void *host,
+                                       size_t bytes);
+VTP_API int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_t count, const void *host,
+                                       size_t bytes);
+
 /* Neighbour lists in the reference's layout (UniformGridNeighborSearch.hpp:
  * 39-51): counts[n_total] (self included, 0 for particles outside the grid)
  * and nbrs[n_total * max_nbr] original indices, self first, UINT32_MAX padded. */

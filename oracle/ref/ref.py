@@ -94,6 +94,14 @@ class RefSolver:
             raise RuntimeError(f"ref_get({field}) failed ({rc})")
         return out
 
+    def get_prefix(self, field: str, count: int) -> np.ndarray:
+        """pos / vel of the first `count` particles (attach order)."""
+        out = np.empty((count, 3), np.float32)
+        rc = lib().ref_get(self.h, field.encode(), out.ctypes.data, out.nbytes)
+        if rc != 0:
+            raise RuntimeError(f"ref_get({field}) failed ({rc})")
+        return out
+
     def set(self, field: str, arr: np.ndarray):
         a = np.ascontiguousarray(arr, np.float32)
         rc = lib().ref_set(self.h, field.encode(), a.ctypes.data, a.nbytes)

@@ -130,7 +130,9 @@ int copy_field(S *s, const std::string &f, void *out, size_t bytes) {
         }
     }
     if (!src) return -2;
-    if (need != bytes) return -3;
+    // pos / vel may be read for a leading range of particles (attach order), the rest whole
+    const bool prefix_ok = (f == "pos" || f == "vel") && bytes <= need && bytes % 12 == 0;
+    if (need != bytes && !prefix_ok) return -3;
     return cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -4;
 }
 
@@ -141,7 +143,7 @@ int set_field(S *s, const std::string &f, const void *in, size_t bytes) {
     void *dst = nullptr;
     if (f == "pos") dst = d->pos;
     else if (f == "vel") dst = d->vel;
-    if (!dst || bytes != n * 12) return -2;
+    if (!dst || bytes > n * 12 || bytes % 12) return -2;   // the leading particles (attach order)
     return cudaMemcpy(dst, in, bytes, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -4;
 }
 

@@ -115,3 +115,24 @@ def test_field_calls_before_initialize_fail_cleanly():
     rc = vtp.lib().vtp_solver_get_field(s._h, 0, buf, 12)
     assert rc == _lib.VTP_ERR_STATE
     s.destroy()
+
+
+def test_range_io_before_initialize_fails_cleanly():
+    s = vtp.PBFSolver()
+    assert s.setConfig(vtp.scenes.pbf_dam_break().config)
+    buf = (C.c_float * 30)()
+    assert vtp.lib().vtp_solver_get_field_range(s._h, 0, 0, 10, buf, 120) == _lib.VTP_ERR_STATE
+    assert vtp.lib().vtp_solver_set_field_range(s._h, 0, 0, 10, buf, 120) == _lib.VTP_ERR_STATE
+    s.destroy()
+
+
+def test_export_config_is_validated():
+    cfg = vtp.scenes.pbf_dam_break().config
+    cfg["EXPORT"]["SolverRequired"]["enable"] = True
+    cfg["EXPORT"]["SolverRequired"]["exportFps"] = 0
+    s = vtp.PBFSolver()
+    assert not s.setConfig(cfg) and "exportFps" in s.last_error
+    cfg["EXPORT"]["SolverRequired"]["exportFps"] = 30
+    del cfg["EXPORT"]["Common"]["exportTargetDir"]
+    assert not s.setConfig(cfg) and "exportTargetDir" in s.last_error
+    s.destroy()

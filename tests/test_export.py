@@ -34,14 +34,15 @@ def _solver(sc, policy, out, fps):
 def test_pbf_export_files(vtp_gpu, tmp_path, policy):
     sc = scenes.dam_break("PBF", 2000, seed=21)
     dt = sc.config["PBF"]["Required"]["timeStep"]
-    s = _solver(sc, policy, tmp_path, fps=1.0 / (2 * dt))     # a frame every second substep
+    # frames advance when simTime >= frame / fps; with 1/fps = 2.4 dt the frames fall on
+    # substeps 1, 3 and 5 whatever the FP32 rounding of the accumulated time
+    s = _solver(sc, policy, tmp_path, fps=1.0 / (2.4 * dt))
     assert s.initialize() and s.tickNsteps(5)
     pos = s.get_field("pos")
     color = s.get_field("color")
     nf = sc.objects[0].n
     if policy == "MERGE":
         files = sorted((tmp_path / "Fluid").glob("*.ply"), key=lambda p: int(p.stem))
-        # frames advance when simTime >= frame / fps: after substeps 1, 3, 5 -> frames 1, 2, 3
         assert [p.stem for p in files] == ["1", "2", "3"]
         props, d = read_ply(files[-1])
         assert props == ["x", "y", "z"]

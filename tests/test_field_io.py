@@ -1,0 +1,31 @@
+"""Field I/O by attach-order particle range (vtp_solver_get/set_field_range)."""
+import numpy as np
+import pytest
+
+import vtp
+from vtp import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
+def test_range_io_matches_full_io(vtp_gpu, kind):
+    sc = scenes.dam_break(kind, 3000, seed=31)
+    s = vtp.solver_from_scene(sc)
+    assert s.initialize() and s.tickNsteps(3)
+    n, nf = sc.n_total, sc.objects[0].n
+    for name in ("pos", "vel", "volume"):
+        full = s.get_field(name)
+        assert np.array_equal(s.get_field_range(name, 0, nf), full[:nf])
+        assert np.array_equal(s.get_field_range(name, nf, n - nf), full[nf:])
+        assert np.array_equal(s.get_field_range(name, 100, 7), full[100:107])
+    # set a sub-range of fluid velocities: only those particles change
+    v = s.get_field("vel")
+    new = (v[10:20] + 0.5).astype(np.float32)
+    s.set_field_range_ptr("vel", 10, 10, np.ascontiguousarray(new).ctypes.data, new.nbytes)
+    v2 = s.get_field("vel")
+    assert np.array_equal(v2[10:20], new)
+    assert np.array_equal(np.delete(v2, np.s_[10:20], axis=0), np.delete(v, np.s_[10:20], axis=0))
+    with pytest.raises(vtp.VtpError):
+        s.get_field_range("pos", n - 5, 10)
+    s.destroy()

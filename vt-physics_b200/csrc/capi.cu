@@ -1218,6 +1218,52 @@ int vtp_solver_set_field(vtp_solver *s, int field, const void *host, size_t byte
     return s->set_field(field, host, bytes);
 }
 
+int vtp_solver_get_field_range(vtp_solver *s, int field, uint32_t first, uint32_t count, void *host, size_t bytes) {
+    if (!s || (!host && count)) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "get_field before initialize");
+    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+    if (field != VTP_FIELD_POS && field != VTP_FIELD_VEL) {
+        // other fields: through the full-size path
+        const size_t ne = bytes / (count ? count : 1) / 4;
+        std::vector<float> all((size_t)s->L.n * ne);
+        int rc = s->get_field(field, all.data(), all.size() * 4);
+        if (rc) return rc;
+        if (bytes != (size_t)count * ne * 4) return fail(VTP_ERR_ARG, "wrong byte count for field");
+        memcpy(host, all.data() + (size_t)first * ne, bytes);
+        return VTP_OK;
+    }
+    if (bytes != (size_t)count * 12) return fail(VTP_ERR_ARG, "wrong byte count for field");
+    if (!count) return VTP_OK;
+    int rc = s->ensure_stage(bytes);
+    if (rc) return rc;
+    const DB<float4> &d = field == VTP_FIELD_POS ? s->pos : s->vel;
+    vtp::scatter_f4_range(s->st, s->L.n, d.c(), s->orig.c(), first, count, s->stage);
+    cudaError_t e = cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_t count, const void *host,
+                               size_t bytes) {
+    if (!s || (!host && count)) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "set_field before initialize");
+    if (field != VTP_FIELD_POS && field != VTP_FIELD_VEL) return fail(VTP_ERR_ARG, "only pos / vel can be set");
+    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+    if (bytes != (size_t)count * 12) return fail(VTP_ERR_ARG, "wrong byte count for field");
+    if (!count) return VTP_OK;
+    int rc = s->ensure_stage(bytes);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) {
+        // Only fluid rows move; boundary rows are static and stay as sorted at initialize.
+        DB<float4> &d = field == VTP_FIELD_POS ? s->pos : s->vel;
+        float4 *also = field == VTP_FIELD_VEL && s->vadv.c() ? s->vadv.c() : nullptr;
+        vtp::gather_f4_range(s->st, s->L.nf, s->stage, s->orig.c(), first, count, d.c(), also);
+        e = cudaStreamSynchronize(s->st);
+    }
+    return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
 int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
     if (!s || !counts || !nbrs) return fail(VTP_ERR_ARG, "null argument");
     if (!s->initialized) return fail(VTP_ERR_STATE, "get_neighbors before initialize");

@@ -91,6 +91,11 @@ void gather_orig_to_f4(cudaStream_t st, uint32_t n, const float *src3, const uin
                        int keep_w);
 void gather_orig_to_f1(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst);
 void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base);
+// Attach-id range [first, first + count) <-> sorted rows [0, n) (float3 compact buffer).
+void scatter_f4_range(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, uint32_t first,
+                      uint32_t count, float *dst3);
+void gather_f4_range(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, uint32_t first,
+                     uint32_t count, float4 *dst, float4 *dst2);
 void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
                       const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
                       uint32_t *out_nbr);

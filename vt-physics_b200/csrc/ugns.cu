@@ -329,6 +329,39 @@ __global__ void k_gather_f1(uint32_t n, const float *__restrict__ src, const uin
     dst[i] = src[orig[i]];
 }
 
+// Rows whose attach id lies in [first, first + count): scatter to / gather from a
+// compact buffer indexed by id - first.
+__global__ void k_scatter_f4_range(uint32_t n, const float4 *__restrict__ src, const uint32_t *__restrict__ orig,
+                                   uint32_t first, uint32_t count, float *__restrict__ dst3) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = orig[i] - first;
+    if (id >= count) return;
+    const float4 v = src[i];
+    dst3[3 * (size_t)id] = v.x;
+    dst3[3 * (size_t)id + 1] = v.y;
+    dst3[3 * (size_t)id + 2] = v.z;
+}
+
+__global__ void k_gather_f4_range(uint32_t n, const float *__restrict__ src3, const uint32_t *__restrict__ orig,
+                                  uint32_t first, uint32_t count, float4 *__restrict__ dst,
+                                  float4 *__restrict__ dst2) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = orig[i] - first;
+    if (id >= count) return;
+    float4 v = dst[i];
+    v.x = src3[3 * (size_t)id];
+    v.y = src3[3 * (size_t)id + 1];
+    v.z = src3[3 * (size_t)id + 2];
+    dst[i] = v;
+    if (dst2) {
+        float4 w = dst2[i];
+        w.x = v.x; w.y = v.y; w.z = v.z;
+        dst2[i] = w;
+    }
+}
+
 __global__ void k_iota(uint32_t n, uint32_t *dst, uint32_t base) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = base + i;
@@ -451,6 +484,14 @@ void gather_orig_to_f4(cudaStream_t st, uint32_t n, const float *src3, const uin
 }
 void gather_orig_to_f1(cudaStream_t st, uint32_t n, const float *src, const uint32_t *orig, float *dst) {
     if (n) k_gather_f1<<<nblk(n, 256), 256, 0, st>>>(n, src, orig, dst);
+}
+void scatter_f4_range(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, uint32_t first,
+                      uint32_t count, float *dst3) {
+    if (n) k_scatter_f4_range<<<nblk(n, 256), 256, 0, st>>>(n, src, orig, first, count, dst3);
+}
+void gather_f4_range(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, uint32_t first,
+                     uint32_t count, float4 *dst, float4 *dst2) {
+    if (n) k_gather_f4_range<<<nblk(n, 256), 256, 0, st>>>(n, src3, orig, first, count, dst, dst2);
 }
 void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base) {
     if (n) k_iota<<<nblk(n, 256), 256, 0, st>>>(n, dst, base);

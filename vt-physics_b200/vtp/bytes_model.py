@@ -62,3 +62,24 @@ def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float, P: int
     else:
         state, lst = 0, 0
     return {"state": float(state), "list": float(lst), "total": float(state + lst)}
+
+
+# FP32 operations per neighbour pair, counted from the kernel sources (an FMA counts 2,
+# sqrt / rsqrt / division 1): W evaluation ~16 and gradient factor ~22 as in the
+# project's work model, plus each pass's own combination terms.
+FLOPS_PER_PAIR = {
+    "dfsph_ratio_alpha": 16 + 22 + 19,   # W, g, ratio fma, gradient sums, alpha_2 term
+    "dfsph_solve_a": 22 + 11,            # g, r.(v_i - v_j) scaled, fma into delta
+    "dfsph_solve_b": 22 + 10,            # g, (k_i + k_j) c_i V_j g, three fma
+    "dfsph_viscosity": 22 + 27,          # g, pressure-applied v_j, r.v_ij / (d2 + eps), three fma
+    "dfsph_vis_normal": 22 + 33,
+    "dfsph_tension": 30 + 24,
+    "pbf_lambda": 16 + 22 + 16,
+    "pbf_dx": 22 + 8,
+    "pbf_xsph": 16 + 13,
+}
+
+
+def kernel_flops(name: str, Nf: int, k: float) -> float:
+    """Algorithmic FP32 flops of one launch (0 for passes without neighbour arithmetic)."""
+    return float(FLOPS_PER_PAIR.get(name, 0)) * k * Nf

@@ -198,6 +198,24 @@ class Solver:
         fid, _ = FIELDS[name]
         check(lib().vtp_solver_get_field(self._h, fid, ptr, nbytes), f"get_field({name})")
 
+    def set_field_range_ptr(self, name: str, first: int, count: int, ptr: int, nbytes: int):
+        """Upload particles [first, first + count) (attach order) from a raw host pointer."""
+        fid, _ = FIELDS[name]
+        check(lib().vtp_solver_set_field_range(self._h, fid, int(first), int(count), ptr, nbytes),
+              f"set_field_range({name})")
+
+    def get_field_range_ptr(self, name: str, first: int, count: int, ptr: int, nbytes: int):
+        fid, _ = FIELDS[name]
+        check(lib().vtp_solver_get_field_range(self._h, fid, int(first), int(count), ptr, nbytes),
+              f"get_field_range({name})")
+
+    def get_field_range(self, name: str, first: int, count: int) -> np.ndarray:
+        fid, width = FIELDS[name]
+        w = width if isinstance(width, int) and width > 0 else 1
+        out = np.empty((count, w) if w > 1 else count, np.float32)
+        self.get_field_range_ptr(name, first, count, out.ctypes.data, out.nbytes)
+        return out
+
     def get_neighbors(self, max_nbr: int):
         n = self.counts()["total"]
         cnt = np.empty(n, np.uint32)
