@@ -1,4 +1,6 @@
-"""Build the sm_100a shared library ``vtp/libvtp.so`` from ``csrc/`` with nvcc.
+"""Build the sm_100a shared library ``vtp/libvtp.so`` from ``csrc/`` with nvcc, and
+the C++ host interface ``vtp/libvtp_host.so`` (``host/``, the reference's Solver /
+Object / SolverManager classes over the C ABI) with g++.
 
 Usage: ``python build.py [--jobs N] [--force]``.  Objects go to ``_build/``.
 """
@@ -16,6 +18,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 OUT = HERE / "vtp" / "libvtp.so"
+HOST_OUT = HERE / "vtp" / "libvtp_host.so"
+HOST = HERE / "host"
 ROOT = HERE.parent
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -72,9 +76,39 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_host(force)
     if verbose:
         print(f"built {OUT}")
     return OUT
+
+
+def host_flags() -> list[str]:
+    return ["-std=c++17", "-O2", "-fPIC", "-I", str(HOST / "include"), "-I", str(ROOT / "include"),
+            "-I", json_include()]
+
+
+def build_host(force: bool = False) -> Path:
+    """libvtp_host.so: the C++ Solver/Object classes, linked against libvtp.so."""
+    srcs = sorted((HOST / "src").glob("*.cpp"))
+    deps = srcs + list((HOST / "include").rglob("*.hpp")) + [ROOT / "include" / "vtp.h", OUT]
+    if not force and HOST_OUT.exists() and all(HOST_OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return HOST_OUT
+    cmd = ["g++"] + host_flags() + ["-shared", "-o", str(HOST_OUT)] + [str(s) for s in srcs] + \
+          ["-L", str(OUT.parent), "-lvtp", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host library build failed:\n{r.stdout}\n{r.stderr}")
+    return HOST_OUT
+
+
+def build_host_program(src: Path, out: Path) -> Path:
+    """Compile a C++ program against the host interface (used by the example and its tests)."""
+    cmd = ["g++"] + host_flags() + ["-o", str(out), str(src), "-L", str(HOST_OUT.parent), "-lvtp_host", "-lvtp",
+                                    f"-Wl,-rpath,{HOST_OUT.parent}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"program build failed:\n{r.stdout}\n{r.stderr}")
+    return out
 
 
 if __name__ == "__main__":
