@@ -35,7 +35,9 @@ METRIC = "M particle-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed substeps (default: 200; 1000 for pbf; 30 for immct_500k, whose scene develops "
+                         "outlier speeds after ~45 substeps in the reference and here alike)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k", "batched", "diff_pbf"],
@@ -560,8 +562,13 @@ def run_diff(args, torch) -> dict:
             "clocks": clocks}
 
 
+DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "immct_500k": 30, "batched": 200, "diff_pbf": 200}
+
+
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = DEFAULT_STEPS[args.workload]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

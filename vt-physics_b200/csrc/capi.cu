@@ -464,6 +464,7 @@ int vtp_solver::initialize() {
     AL(&u.key, nrows_max);
     AL(&u.rank, nrows_max);
     AL(&u.count, (size_t)nbuckets);
+    CU(cudaMemsetAsync(u.count, 0, (size_t)nbuckets * sizeof(uint32_t), st));   // kept zero by the cell scan
     AL(&u.fstart, (size_t)nbuckets + 1);
     AL(&u.bstart, (size_t)nbuckets + 1);
     AL(&u.tmp_src, nrows_max);
@@ -705,7 +706,7 @@ int vtp_solver::enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape) {
     uint32_t *lnbr = tape ? tape->nbr : u.nbr, *lcnt = tape ? tape->ncnt : u.ncnt;
     PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, lnbr, lcnt,
                                                    d_status, d_overflow, block));
-    launches_per_tick += 8;  // hash, 4 scan kernels, scatter, rank/reorder, lists
+    launches_per_tick += 7;  // hash, 3 scan kernels, scatter, rank/reorder, lists
     if (tape && nf) {
         CU(cudaMemcpyAsync(tape->orig, orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         CU(cudaMemcpyAsync(tape->x[0], pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s));
@@ -748,7 +749,7 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
                                                    d_status, d_overflow, block));
     PROF(this, "dfsph_ratio_alpha", vtp::dfsph_ratio_alpha(s, dfsph_args(), block));
-    launches_per_tick += 9;  // neighbour search (8) + ratio/alpha
+    launches_per_tick += 8;  // neighbour search (7) + ratio/alpha
     if ((rc = enqueue_solve(s, 0, capture))) return rc;
     vtp::DfsphArgs a = dfsph_args();
     if (gamma == 0.f) {

@@ -220,7 +220,7 @@ __global__ void k_solve_begin(SolveState *s, LoopState *loop, int nscenes) {
 
 // One block per scene: FP64 residual of the scene from its tiles' partials,
 // the stop test, and (last block to finish) the loop condition.
-__global__ void __launch_bounds__(256) k_solve_end(SolveCtl c, const double *__restrict__ partials,
+__global__ void __launch_bounds__(1024) k_solve_end(SolveCtl c, const double *__restrict__ partials,
                                                    uint32_t *status) {
     SolveState *st = c.state + blockIdx.x;
     const SceneTiles sct = c.scene_tiles[blockIdx.x];
@@ -430,7 +430,7 @@ void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
     VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
-    k_solve_end<<<c.nscenes, 256, 0, st>>>(c, partials, status);
+    k_solve_end<<<c.nscenes, 1024, 0, st>>>(c, partials, status);
 }
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block) {
     if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_viscosity<false, UU><<<nblk(a.nf, block), block, 0, st>>>(a))

@@ -888,7 +888,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
         vtp::ugns_build_lists(st, s.scn(), s.L, 0, nf, s.pos.c(), s.orig.c(), s.u, s.u.nbr, s.u.ncnt, s.d_status,
                               s.d_overflow, B);
     });
-    s.launches_per_tick += 7;
+    s.launches_per_tick += 6;   // hash, 3 scan kernels, scatter, rank/reorder
     if (nf == 0) return VTP_OK;
     const unsigned G = vtp::nblk(nf, B), G256 = vtp::nblk(nf, 256);
     ImmArgs a = imm_args(s);

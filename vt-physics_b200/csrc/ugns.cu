@@ -112,7 +112,10 @@ __global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *sums, size_t tiles
     }
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__restrict__ in, size_t n,
+// Exclusive scan of the counters into `out` (plus `base_add`), out[n] = grand
+// total.  The counters are zeroed after they are read, so the next hash starts
+// from zero without a separate clear.
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t *__restrict__ in, size_t n,
                                                              const uint32_t *__restrict__ sums, uint32_t base_add,
                                                              uint32_t *__restrict__ out) {
     // Each thread scans kScanItems consecutive counters.
@@ -121,6 +124,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__r
     for (int k = 0; k < kScanItems; ++k) {
         size_t idx = t0 + (size_t)k * kScanThreads + threadIdx.x;
         tile[k * kScanThreads + threadIdx.x] = idx < n ? in[idx] : 0u;
+        if (idx < n) in[idx] = 0u;
     }
     __syncthreads();
     uint32_t vals[kScanItems];
@@ -134,6 +138,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__r
     uint32_t off = block_excl_scan(s, total) + sums[blockIdx.x] + base_add;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
+        const size_t idx = t0 + (size_t)threadIdx.x * kScanItems + k;
+        if (idx + 1 == n) out[n] = off + vals[k];
         tile[threadIdx.x * kScanItems + k] = off;
         off += vals[k];
     }
@@ -142,11 +148,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__r
         size_t idx = t0 + (size_t)k * kScanThreads + threadIdx.x;
         if (idx < n) out[idx] = tile[k * kScanThreads + threadIdx.x];
     }
-}
-
-// The entry past the last counter holds the grand total (plus the base).
-__global__ void k_scan_total(const uint32_t *__restrict__ in, size_t n, uint32_t *__restrict__ out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) out[n] = out[n - 1] + in[n - 1];
 }
 
 __global__ void k_scatter(uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ key,
@@ -415,13 +416,12 @@ int cubic_sigma_device(cudaStream_t st, float h, float *out_host) {
     return e == cudaSuccess ? 0 : 1;
 }
 
-static void scan_counts(cudaStream_t st, const uint32_t *count, size_t n, uint32_t base_add, uint32_t *out,
+static void scan_counts(cudaStream_t st, uint32_t *count, size_t n, uint32_t base_add, uint32_t *out,
                         UgnsBuffers &u) {
     size_t tiles = (n + kScanTile - 1) / kScanTile;
     k_scan_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums);
     k_scan_sums<<<1, 1024, 0, st>>>(u.scan_sums, tiles);
     k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums, base_add, out);
-    k_scan_total<<<1, 32, 0, st>>>(count, n, out);
 }
 
 void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t row0, uint32_t cnt,
@@ -432,7 +432,7 @@ void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t ro
     auto B = [&] { if (prof) prof->begin(); };
     auto E = [&](const char *nm) { if (prof) prof->end_(nm); };
     B();
-    cudaMemsetAsync(u.count, 0, nb * sizeof(uint32_t), st);
+    // u.count is all zero here: zeroed once at allocation and by every scan after reading it.
     if (cnt > 0) {
         k_hash<<<nblk(cnt, 256), 256, 0, st>>>(sc, row0, cnt, pos_in, vel_in, force_dt, u.key, u.rank, u.count);
     }
