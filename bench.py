@@ -166,6 +166,9 @@ def cpu_baseline(scene, seconds: float) -> dict:
     from oracle import oracle as O
     O.lib()
     cores = O.num_threads()
+    if scene.solver not in ("PBF", "DFSPH"):
+        return {"value": None, "unit": METRIC, "cores": cores, "kind": "port",
+                "sample": f"none: the FP64 oracle restates the PBF and DFSPH substeps, not {scene.solver}"}
     t0 = time.perf_counter()
     o = O.OracleSolver(scene)
     init_s = time.perf_counter() - t0
@@ -331,12 +334,10 @@ def state_bytes(bufs) -> int:
 def state_round_trip(s, bufs):
     """One e2e step: fluid state host -> device, one substep, fluid state device -> host."""
     for first, count, p, v in bufs:
-        s.set_field_range_ptr("pos", first, count, p.data_ptr(), p.numel() * 4)
-        s.set_field_range_ptr("vel", first, count, v.data_ptr(), v.numel() * 4)
+        s.set_state_range_ptr(first, count, p.data_ptr(), v.data_ptr())
     assert s.tickNsteps(1), s.last_error
     for first, count, p, v in bufs:
-        s.get_field_range_ptr("pos", first, count, p.data_ptr(), p.numel() * 4)
-        s.get_field_range_ptr("vel", first, count, v.data_ptr(), v.numel() * 4)
+        s.get_state_range_ptr(first, count, p.data_ptr(), v.data_ptr())
 
 
 def _batch_cost(sc) -> float:

@@ -191,6 +191,14 @@ VTP_API int vtp_solver_get_field_range(vtp_solver *s, int field, uint32_t first,
 VTP_API int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_t count, const void *host,
                                        size_t bytes);
 
+/* Positions and velocities of the particle range [first, first + count)
+ * together (pos and vel: count x float[3] host buffers each), one device pass
+ * and one synchronisation per call: the state round trip of a host-side
+ * driver loop. */
+VTP_API int vtp_solver_get_state_range(vtp_solver *s, uint32_t first, uint32_t count, float *pos, float *vel);
+VTP_API int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos,
+                                       const float *vel);
+
 /* Neighbour lists in the reference's layout (UniformGridNeighborSearch.hpp:
  * 39-51): counts[n_total] (self included, 0 for particles outside the grid)
  * and nbrs[n_total * max_nbr] original indices, self first, UINT32_MAX padded. */

@@ -29,3 +29,29 @@ def test_range_io_matches_full_io(vtp_gpu, kind):
     with pytest.raises(vtp.VtpError):
         s.get_field_range("pos", n - 5, 10)
     s.destroy()
+
+
+def test_state_range_io_matches_field_io(vtp_gpu):
+    import ctypes as C
+    sc = scenes.dam_break("DFSPH", 3000, seed=32)
+    s = vtp.solver_from_scene(sc)
+    assert s.initialize() and s.tickNsteps(2)
+    nf = sc.objects[0].n
+    p = np.empty((nf, 3), np.float32)
+    v = np.empty((nf, 3), np.float32)
+    s.get_state_range_ptr(0, nf, p.ctypes.data, v.ctypes.data)
+    assert np.array_equal(p, s.get_field_range("pos", 0, nf))
+    assert np.array_equal(v, s.get_field_range("vel", 0, nf))
+    p2, v2 = (p + 0.001).astype(np.float32), (v * 0.5).astype(np.float32)
+    s.set_state_range_ptr(0, nf, p2.ctypes.data, v2.ctypes.data)
+    assert np.array_equal(s.get_field("pos")[:nf], p2)
+    assert np.array_equal(s.get_field("vel")[:nf], v2)
+    # the next substep starts from the new state: same as setting pos / vel one by one
+    t = vtp.solver_from_scene(sc)
+    assert t.initialize() and t.tickNsteps(2)
+    t.set_field_range_ptr("pos", 0, nf, p2.ctypes.data, p2.nbytes)
+    t.set_field_range_ptr("vel", 0, nf, v2.ctypes.data, v2.nbytes)
+    assert s.tickNsteps(1) and t.tickNsteps(1)
+    assert np.array_equal(s.get_field("pos"), t.get_field("pos"))
+    s.destroy()
+    t.destroy()

@@ -1265,6 +1265,42 @@ int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
 }
 
+int vtp_solver_get_state_range(vtp_solver *s, uint32_t first, uint32_t count, float *pos, float *vel) {
+    if (!s || ((!pos || !vel) && count)) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "get_state before initialize");
+    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+    if (!count) return VTP_OK;
+    const size_t b = (size_t)count * 12;
+    int rc = s->ensure_stage(2 * b);
+    if (rc) return rc;
+    float *p3 = s->stage, *v3 = s->stage + (size_t)count * 3;
+    vtp::scatter_state_range(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), first, count, p3, v3);
+    cudaError_t e = cudaMemcpyAsync(pos, p3, b, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vel, v3, b, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos, const float *vel) {
+    if (!s || ((!pos || !vel) && count)) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "set_state before initialize");
+    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+    if (!count) return VTP_OK;
+    const size_t b = (size_t)count * 12;
+    int rc = s->ensure_stage(2 * b);
+    if (rc) return rc;
+    float *p3 = s->stage, *v3 = s->stage + (size_t)count * 3;
+    cudaError_t e = cudaMemcpyAsync(p3, pos, b, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v3, vel, b, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) {
+        // Only fluid rows move; boundary rows are static and stay as sorted at initialize.
+        vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), first, count, s->pos.c(), s->vel.c(),
+                                s->vadv.c());
+        e = cudaStreamSynchronize(s->st);
+    }
+    return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
 int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
     if (!s || !counts || !nbrs) return fail(VTP_ERR_ARG, "null argument");
     if (!s->initialized) return fail(VTP_ERR_STATE, "get_neighbors before initialize");

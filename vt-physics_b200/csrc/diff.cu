@@ -103,6 +103,20 @@ __device__ __forceinline__ double block_sum_d(double v) {
     return s;
 }
 
+// Gathered neighbour data of the adjoint passes.
+struct XN {
+    float4 q, v, a;
+    float vol;
+};
+struct LN {
+    float4 q, d;
+};
+struct DN {
+    float4 q, d, A;
+    float l, s;
+    bool fj;
+};
+
 struct AdjArgs {
     uint32_t nf, ell_stride;
     Cubic k;
@@ -140,28 +154,34 @@ __global__ void __launch_bounds__(256) k_adj_xsph(AdjArgs a) {
         const uint32_t n = a.ncnt[r];
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
         float ksum = 0.f;
-        for (uint32_t t = 0; t + 1 < n; ++t) {
-            const uint32_t j = lst[(size_t)t * 32u];
-            const float4 q = a.x[j], vj = a.v[j];
-            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-            const float d2 = dist2(rx, ry, rz);
-            const float w = cubic_w(d2, a.k), g = cubic_g(d2, a.k);
-            const float Vj = a.vol[j];
-            const bool fj = j < a.nf;
-            const float4 aj = fj ? a.abar[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float dx = vj.x - vi.x, dy = vj.y - vi.y, dz = vj.z - vi.z;
-            const float di = dx * ai.x + dy * ai.y + dz * ai.z;
-            const float dj = dx * aj.x + dy * aj.y + dz * aj.z;
-            const float ci = -a.c * Vj * w, cj = a.c * Vi * w;
-            vb.x += ci * ai.x + cj * aj.x;
-            vb.y += ci * ai.y + cj * aj.y;
-            vb.z += ci * ai.z + cj * aj.z;
-            const float s = a.c * g * (Vj * di - Vi * dj);
-            xb.x += s * rx;
-            xb.y += s * ry;
-            xb.z += s * rz;
-            ksum += Vj * w * di;
-        }
+        // U = 4 neighbours' gathers in flight per thread (same order of accumulation)
+        nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
+                    [&](uint32_t j) {
+                        XN e;
+                        e.q = __ldg(a.x + j);
+                        e.v = __ldg(a.v + j);
+                        e.vol = __ldg(a.vol + j);
+                        e.a = j < a.nf ? __ldg(a.abar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        return e;
+                    },
+                    [&](uint32_t, const XN &e) {
+                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                        const float d2 = dist2(rx, ry, rz);
+                        const float w = cubic_w(d2, a.k), g = cubic_g(d2, a.k);
+                        const float Vj = e.vol;
+                        const float dx = e.v.x - vi.x, dy = e.v.y - vi.y, dz = e.v.z - vi.z;
+                        const float di = dx * ai.x + dy * ai.y + dz * ai.z;
+                        const float dj = dx * e.a.x + dy * e.a.y + dz * e.a.z;
+                        const float ci = -a.c * Vj * w, cj = a.c * Vi * w;
+                        vb.x += ci * ai.x + cj * e.a.x;
+                        vb.y += ci * ai.y + cj * e.a.y;
+                        vb.z += ci * ai.z + cj * e.a.z;
+                        const float s = a.c * g * (Vj * di - Vi * dj);
+                        xb.x += s * rx;
+                        xb.y += s * ry;
+                        xb.z += s * rz;
+                        ksum += Vj * w * di;
+                    });
         a.xbar[r] = xb;
         a.vbar[r] = vb;
         a.Dcur[r] = make_float4(xb.x + vb.x * a.inv_dt, xb.y + vb.y * a.inv_dt, xb.z + vb.z * a.inv_dt, 0.f);
@@ -180,18 +200,21 @@ __global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     const float ir = 1.f / a.rho0;
     float lb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = a.x[j];
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float g = cubic_g(dist2(rx, ry, rz), a.k) * ir;
-        const float ex = g * rx, ey = g * ry, ez = g * rz;
-        gx += ex; gy += ey; gz += ez;
-        s2 += ex * ex + ey * ey + ez * ez;
-        float4 dj = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j < a.nf) dj = a.Dcur[j];
-        lb += ex * (di.x - dj.x) + ey * (di.y - dj.y) + ez * (di.z - dj.z);
-    }
+    nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) {
+                    LN e;
+                    e.q = __ldg(a.x + j);
+                    e.d = j < a.nf ? __ldg(a.Dcur + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    return e;
+                },
+                [&](uint32_t, const LN &e) {
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float g = cubic_g(dist2(rx, ry, rz), a.k) * ir;
+                    const float ex = g * rx, ey = g * ry, ez = g * rz;
+                    gx += ex; gy += ey; gz += ez;
+                    s2 += ex * ex + ey * ey + ez * ez;
+                    lb += ex * (di.x - e.d.x) + ey * (di.y - e.d.y) + ez * (di.z - e.d.z);
+                });
     s2 += gx * gx + gy * gy + gz * gz;
     const float den = s2 + a.eps;
     const float lam = a.lam[r];
@@ -211,39 +234,44 @@ __global__ void __launch_bounds__(256) k_adj_dx(AdjArgs a) {
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     const float ir = 1.f / a.rho0;
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = a.x[j];
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float d2 = dist2(rx, ry, rz);
-        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
-        const float ex = g * rx * ir, ey = g * ry * ir, ez = g * rz * ir;
-        const bool fj = j < a.nf;
-        float lj = 0.f, sbj = 0.f;
-        float4 dj = make_float4(0.f, 0.f, 0.f, 0.f), Aj = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (fj) {
-            lj = a.lam[j];
-            sbj = a.sbar[j];
-            dj = a.Dcur[j];
-            Aj = a.A2[j];
-        }
-        const float ll = li + lj;
-        // e-bar of pair (i, j) minus e-bar of pair (j, i) (zero for a boundary j)
-        float bx = ll * di.x + 2.f * sbi * (ex + Ai.x);
-        float by = ll * di.y + 2.f * sbi * (ey + Ai.y);
-        float bz = ll * di.z + 2.f * sbi * (ez + Ai.z);
-        if (fj) {
-            bx -= ll * dj.x + 2.f * sbj * (Aj.x - ex);
-            by -= ll * dj.y + 2.f * sbj * (Aj.y - ey);
-            bz -= ll * dj.z + 2.f * sbj * (Aj.z - ez);
-        }
-        const float rdot = rx * bx + ry * by + rz * bz;
-        const float dens = q.w * Ai.w + (fj ? p.w * Aj.w : 0.f);   // m_j rho-bar_i + m_i rho-bar_j
-        const float cg = g * dens;
-        ax += cg * rx + (g * bx + hh * rx * rdot) * ir;
-        ay += cg * ry + (g * by + hh * ry * rdot) * ir;
-        az += cg * rz + (g * bz + hh * rz * rdot) * ir;
-    }
+    nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
+                [&](uint32_t j) {
+                    DN e;
+                    e.q = __ldg(a.x + j);
+                    e.fj = j < a.nf;
+                    if (e.fj) {
+                        e.l = __ldg(a.lam + j);
+                        e.s = __ldg(a.sbar + j);
+                        e.d = __ldg(a.Dcur + j);
+                        e.A = __ldg(a.A2 + j);
+                    } else {
+                        e.l = e.s = 0.f;
+                        e.d = e.A = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                    return e;
+                },
+                [&](uint32_t, const DN &e) {
+                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float d2 = dist2(rx, ry, rz);
+                    const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+                    const float ex = g * rx * ir, ey = g * ry * ir, ez = g * rz * ir;
+                    const float ll = li + e.l;
+                    // e-bar of pair (i, j) minus e-bar of pair (j, i) (zero for a boundary j)
+                    float bx = ll * di.x + 2.f * sbi * (ex + Ai.x);
+                    float by = ll * di.y + 2.f * sbi * (ey + Ai.y);
+                    float bz = ll * di.z + 2.f * sbi * (ez + Ai.z);
+                    if (e.fj) {
+                        bx -= ll * e.d.x + 2.f * e.s * (e.A.x - ex);
+                        by -= ll * e.d.y + 2.f * e.s * (e.A.y - ey);
+                        bz -= ll * e.d.z + 2.f * e.s * (e.A.z - ez);
+                    }
+                    const float rdot = rx * bx + ry * by + rz * bz;
+                    const float dens = e.q.w * Ai.w + (e.fj ? p.w * e.A.w : 0.f);   // m_j rho-bar_i + m_i rho-bar_j
+                    const float cg = g * dens;
+                    ax += cg * rx + (g * bx + hh * rx * rdot) * ir;
+                    ay += cg * ry + (g * by + hh * ry * rdot) * ir;
+                    az += cg * rz + (g * bz + hh * rz * rdot) * ir;
+                });
     float4 xb = a.xbar[r];
     xb.x += ax; xb.y += ay; xb.z += az;
     a.xbar[r] = xb;

@@ -96,6 +96,10 @@ void scatter_f4_range(cudaStream_t st, uint32_t n, const float4 *src, const uint
                       uint32_t count, float *dst3);
 void gather_f4_range(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, uint32_t first,
                      uint32_t count, float4 *dst, float4 *dst2);
+void scatter_state_range(cudaStream_t st, uint32_t n, const float4 *pos, const float4 *vel, const uint32_t *orig,
+                         uint32_t first, uint32_t count, float *p3, float *v3);
+void gather_state_range(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
+                        uint32_t first, uint32_t count, float4 *pos, float4 *vel, float4 *vadv);
 void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
                       const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
                       uint32_t *out_nbr);

@@ -203,8 +203,9 @@ struct Walker {
     uint32_t *out;       // ELL base for this row (slot t at out[t*32])
     bool overflow;
 
+    // The row itself (d2 == 0) fails `d2 > 0` like every coincident particle,
+    // as the reference's `0 < |x_i - x_j|` test excludes it.
     __device__ __forceinline__ void accept(uint32_t j, const float4 &q, float d2max) {
-        if (j == self) return;
         float d2 = dist2(px - q.x, py - q.y, pz - q.z);
         if (d2 > 0.f && d2 <= d2max) {
             if (cnt < maxnbr) {
@@ -363,6 +364,42 @@ __global__ void k_gather_f4_range(uint32_t n, const float *__restrict__ src3, co
     }
 }
 
+// Positions and velocities of one attach-id range together (one pass each way).
+__global__ void k_scatter_state_range(uint32_t n, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
+                                      const uint32_t *__restrict__ orig, uint32_t first, uint32_t count,
+                                      float *__restrict__ p3, float *__restrict__ v3) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = orig[i] - first;
+    if (id >= count) return;
+    const float4 p = pos[i], v = vel[i];
+    p3[3 * (size_t)id] = p.x;
+    p3[3 * (size_t)id + 1] = p.y;
+    p3[3 * (size_t)id + 2] = p.z;
+    v3[3 * (size_t)id] = v.x;
+    v3[3 * (size_t)id + 1] = v.y;
+    v3[3 * (size_t)id + 2] = v.z;
+}
+
+__global__ void k_gather_state_range(uint32_t n, const float *__restrict__ p3, const float *__restrict__ v3,
+                                     const uint32_t *__restrict__ orig, uint32_t first, uint32_t count,
+                                     float4 *__restrict__ pos, float4 *__restrict__ vel, float4 *__restrict__ vadv) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = orig[i] - first;
+    if (id >= count) return;
+    float4 p = pos[i], v = vel[i];
+    p.x = p3[3 * (size_t)id]; p.y = p3[3 * (size_t)id + 1]; p.z = p3[3 * (size_t)id + 2];
+    v.x = v3[3 * (size_t)id]; v.y = v3[3 * (size_t)id + 1]; v.z = v3[3 * (size_t)id + 2];
+    pos[i] = p;
+    vel[i] = v;
+    if (vadv) {
+        float4 w = vadv[i];
+        w.x = v.x; w.y = v.y; w.z = v.z;
+        vadv[i] = w;
+    }
+}
+
 __global__ void k_iota(uint32_t n, uint32_t *dst, uint32_t base) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = base + i;
@@ -492,6 +529,14 @@ void scatter_f4_range(cudaStream_t st, uint32_t n, const float4 *src, const uint
 void gather_f4_range(cudaStream_t st, uint32_t n, const float *src3, const uint32_t *orig, uint32_t first,
                      uint32_t count, float4 *dst, float4 *dst2) {
     if (n) k_gather_f4_range<<<nblk(n, 256), 256, 0, st>>>(n, src3, orig, first, count, dst, dst2);
+}
+void scatter_state_range(cudaStream_t st, uint32_t n, const float4 *pos, const float4 *vel, const uint32_t *orig,
+                         uint32_t first, uint32_t count, float *p3, float *v3) {
+    if (n) k_scatter_state_range<<<nblk(n, 256), 256, 0, st>>>(n, pos, vel, orig, first, count, p3, v3);
+}
+void gather_state_range(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
+                        uint32_t first, uint32_t count, float4 *pos, float4 *vel, float4 *vadv) {
+    if (n) k_gather_state_range<<<nblk(n, 256), 256, 0, st>>>(n, p3, v3, orig, first, count, pos, vel, vadv);
 }
 void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base) {
     if (n) k_iota<<<nblk(n, 256), 256, 0, st>>>(n, dst, base);

@@ -209,6 +209,13 @@ class Solver:
         check(lib().vtp_solver_get_field_range(self._h, fid, int(first), int(count), ptr, nbytes),
               f"get_field_range({name})")
 
+    def set_state_range_ptr(self, first: int, count: int, pos_ptr: int, vel_ptr: int):
+        """Upload positions and velocities of particles [first, first + count) from raw host pointers."""
+        check(lib().vtp_solver_set_state_range(self._h, int(first), int(count), pos_ptr, vel_ptr), "set_state_range")
+
+    def get_state_range_ptr(self, first: int, count: int, pos_ptr: int, vel_ptr: int):
+        check(lib().vtp_solver_get_state_range(self._h, int(first), int(count), pos_ptr, vel_ptr), "get_state_range")
+
     def get_field_range(self, name: str, first: int, count: int) -> np.ndarray:
         fid, width = FIELDS[name]
         w = width if isinstance(width, int) and width > 0 else 1
