@@ -318,26 +318,27 @@ def fluid_ranges(scene):
 
 
 def state_buffers(s, ranges, torch):
-    """Pinned host buffers holding the fluid state (pos, vel) of each range."""
+    """Page-locked host buffers (vtp_host_alloc) holding the fluid state (pos, vel) of each range."""
+    import vtp
     bufs = []
     for first, count in ranges:
-        p = torch.from_numpy(s.get_field_range("pos", first, count)).pin_memory()
-        v = torch.from_numpy(s.get_field_range("vel", first, count)).pin_memory()
+        p, v = vtp.HostBuffer((count, 3)), vtp.HostBuffer((count, 3))
+        s.get_state_range_ptr(first, count, p.ptr, v.ptr)
         bufs.append((first, count, p, v))
     return bufs
 
 
 def state_bytes(bufs) -> int:
-    return int(sum(p.numel() * 4 + v.numel() * 4 for _, _, p, v in bufs))
+    return int(sum(p.nbytes + v.nbytes for _, _, p, v in bufs))
 
 
 def state_round_trip(s, bufs):
     """One e2e step: fluid state host -> device, one substep, fluid state device -> host."""
     for first, count, p, v in bufs:
-        s.set_state_range_ptr(first, count, p.data_ptr(), v.data_ptr())
+        s.set_state_range_ptr(first, count, p.ptr, v.ptr)
     assert s.tickNsteps(1), s.last_error
     for first, count, p, v in bufs:
-        s.get_state_range_ptr(first, count, p.data_ptr(), v.data_ptr())
+        s.get_state_range_ptr(first, count, p.ptr, v.ptr)
 
 
 def _batch_cost(sc) -> float:

@@ -23,7 +23,8 @@ class OrGrid(C.Structure):
 
 class OrPbf(C.Structure):
     _fields_ = [("dt", C.c_double), ("h", C.c_double), ("rho0", C.c_double), ("rho_b", C.c_double),
-                ("xsph_k", C.c_double), ("eps", C.c_double), ("g", C.c_double * 3), ("iterations", C.c_int32)]
+                ("xsph_k", C.c_double), ("eps", C.c_double), ("g", C.c_double * 3), ("iterations", C.c_int32),
+                ("form", C.c_int32)]
 
 
 class OrDfsph(C.Structure):
@@ -142,6 +143,10 @@ class OracleSolver:
             for a in range(3):
                 p.g[a] = g[a]
             p.iterations = int(req["iterationNum"])
+            ext = scene.config.get("B200", {})
+            if ext.get("pbfFormulation", "reference") == "standard":
+                p.form = 1
+                p.eps = float(np.float32(ext.get("pbfEpsilon", 100.0)))
             self.p = p
             self.mass = np.full(self.n, p.rho0 * vol0, np.float64)
             lib().or_pbf_init(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.mass), _ptr(self.vol),

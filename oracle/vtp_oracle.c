@@ -201,6 +201,24 @@ static double rdiff(const double *pos, uint32_t i, uint32_t j, double *r) {
 
 /* ------------------------------------------------------------------ PBF */
 
+/* Standard-PBF kernels (Mueller et al. poly6 density, Desbrun spiky gradient). */
+static double poly6_w(double h, double r) {
+    if (r > h) return 0.0;
+    double d = h * h - r * r;
+    return 315.0 / (64.0 * kPi * pow(h, 9.0)) * d * d * d;
+}
+static double spiky_g(double h, double r) {   /* gradW = g * r_vec */
+    if (r > h || r < 1e-6 * h) return 0.0;
+    double d = h - r;
+    return -45.0 / (kPi * pow(h, 6.0)) * d * d / r;
+}
+static double pbf_w(const or_pbf_params *p, const cubic_t *k, double r) {
+    return p->form == 1 ? poly6_w(p->h, r) : cubic_w(k, r);
+}
+static double pbf_g(const or_pbf_params *p, const cubic_t *k, double r) {
+    return p->form == 1 ? spiky_g(p->h, r) : cubic_g(k, r);
+}
+
 void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass, double *vol, const or_grid *g,
                  const or_pbf_params *p) {
     /* init_cuda + compute_rigid_particle_volume_cuda (PBFCudaImpl.cu:34-68). */
@@ -212,7 +230,7 @@ void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass
         if (mat[i] != 1) continue;
         double delta = 0, r[3];
         FOR_NBR(L, g, i, j) {
-            if (mat[j] == mat[i]) delta += cubic_w(&k, rdiff(pos, i, j, r));
+            if (mat[j] == mat[i]) delta += pbf_w(p, &k, rdiff(pos, i, j, r));
         }
         vol[i] = 1.0 / delta;
         mass[i] = p->rho_b * vol[i];
@@ -239,8 +257,8 @@ static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, c
             double d = 0, gs[3] = {0, 0, 0}, s2 = 0, r[3];
             FOR_NBR(L, g, i, j) {
                 double rl = rdiff(pos, i, j, r);
-                d += mass[j] * cubic_w(&k, rl);
-                double gg = cubic_g(&k, rl);
+                d += mass[j] * pbf_w(p, &k, rl);
+                double gg = pbf_g(p, &k, rl) * (p->form == 1 ? mass[j] : 1.0);
                 for (int a = 0; a < 3; ++a) {
                     double e = gg * r[a];
                     gs[a] += e;
@@ -262,9 +280,10 @@ static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, c
             if (mat[i] != 0) continue;
             double s[3] = {0, 0, 0}, r[3];
             FOR_NBR(L, g, i, j) {
-                double gg = cubic_g(&k, rdiff(pos, i, j, r));
+                double gg = pbf_g(p, &k, rdiff(pos, i, j, r));
                 double lj = mat[j] == 0 ? lam[j] : 0.0; /* boundary lambda never set: 0 */
-                for (int a = 0; a < 3; ++a) s[a] += (lam[i] + lj) * gg * r[a];
+                double c = p->form == 1 ? lam[i] * mass[j] + lj * mass[i] : lam[i] + lj;
+                for (int a = 0; a < 3; ++a) s[a] += c * gg * r[a];
             }
             for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = s[a] / p->rho0;
         }
@@ -283,7 +302,7 @@ static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, c
         if (mat[i] != 0) continue;
         double dv[3] = {0, 0, 0}, r[3];
         FOR_NBR(L, g, i, j) {
-            double w = cubic_w(&k, rdiff(pos, i, j, r));
+            double w = pbf_w(p, &k, rdiff(pos, i, j, r));
             for (int a = 0; a < 3; ++a) dv[a] += p->xsph_k * vol[j] * (vel[3 * (size_t)j + a] - vel[3 * (size_t)i + a]) * w;
         }
         for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = dv[a] * dt;

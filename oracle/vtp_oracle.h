@@ -29,6 +29,11 @@ typedef struct or_pbf_params {
     double dt, h, rho0, rho_b, xsph_k, eps;
     double g[3];
     int32_t iterations;
+    /* 0: the reference's formulation (cubic W and gradient, constraint gradients
+     *    without the particle mass, PBFCudaImpl.cu:70-144);
+     * 1: standard PBF (poly6 density, spiky gradient, mass-weighted constraint
+     *    gradients, Delta x_i = (1/rho0) sum_j (lambda_i m_j + lambda_j m_i) gradW). */
+    int32_t form;
 } or_pbf_params;
 
 typedef struct or_dfsph_params {

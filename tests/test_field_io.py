@@ -55,3 +55,20 @@ def test_state_range_io_matches_field_io(vtp_gpu):
     assert np.array_equal(s.get_field("pos"), t.get_field("pos"))
     s.destroy()
     t.destroy()
+
+
+def test_host_buffers_round_trip_state(vtp_gpu):
+    sc = scenes.dam_break("PBF", 2000, seed=33)
+    s = vtp.solver_from_scene(sc)
+    assert s.initialize() and s.tickNsteps(2)
+    nf = sc.objects[0].n
+    p, v = vtp.HostBuffer((nf, 3)), vtp.HostBuffer((nf, 3))
+    s.get_state_range_ptr(0, nf, p.ptr, v.ptr)
+    assert np.array_equal(p.array, s.get_field("pos")[:nf])
+    assert np.array_equal(v.array, s.get_field("vel")[:nf])
+    p.array[:] += 0.01
+    s.set_state_range_ptr(0, nf, p.ptr, v.ptr)
+    assert np.array_equal(s.get_field("pos")[:nf], p.array)
+    p.free()
+    v.free()
+    s.destroy()

@@ -181,3 +181,23 @@ def test_runs_are_deterministic(vtp_gpu):
         out.append(s.get_field("pos"))
         s.destroy()
     assert np.array_equal(out[0], out[1])
+
+
+def test_standard_pbf_matches_oracle_and_holds_the_fluid(vtp_gpu, oracle_lib):
+    """The standard PBF formulation (poly6 / spiky, mass-weighted constraint gradients, eps 100),
+    an extension checked against the FP64 oracle only (the reference has no such mode)."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break()
+    extra = {"pbfFormulation": "standard", "pbfEpsilon": 100.0}
+    sc.config["B200"] = dict(extra)
+    s = vtp.solver_from_scene(sc, extra)
+    assert s.initialize() and s.tickNsteps(1)
+    o = oracle_lib.OracleSolver(sc)
+    o.step(1)
+    f = fluid_mask(sc)
+    assert rel_err(s.get_field("pos")[f], o.pos[f]) < TOL
+    assert rel_err(s.get_field("vel")[f], o.vel[f], floor=_vel_floor(sc)) < TOL
+    assert s.tickNsteps(89)
+    p = s.get_field("pos")[f]
+    assert (p[:, 1] < 0).sum() < 50
+    s.destroy()

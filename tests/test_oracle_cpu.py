@@ -90,3 +90,19 @@ def test_pbf_free_fall_without_neighbours(oracle_lib):
     g = -9.81
     assert o.vel[0, 1] == pytest.approx(3 * g * 0.01, rel=1e-6)
     assert o.pos[0, 1] == pytest.approx(0.5 + g * 0.01 * 0.01 * (1 + 2 + 3), rel=1e-6)
+
+
+def test_standard_pbf_keeps_the_fluid_in_the_box(oracle_lib):
+    # The reference's PBF constraint gradients leave out the particle mass (consistent only for
+    # m = 1); at r = 0.01 (m = 8e-3) the correction is ~125x too weak and the dam-break fluid
+    # passes through the 2-layer floor.  The standard formulation holds it.
+    sc = scenes.pbf_dam_break()
+    ref = oracle_lib.OracleSolver(sc)
+    sc.config["B200"] = {"pbfFormulation": "standard", "pbfEpsilon": 100.0}
+    std = oracle_lib.OracleSolver(sc)
+    f = ref.mat == 0
+    ref.step(90)
+    std.step(90)
+    assert (ref.pos[f, 1] < 0).sum() > 5000
+    assert (std.pos[f, 1] < 0).sum() < 50
+    assert abs(std.density[f].mean() / 1000.0 - 1.0) < 0.02

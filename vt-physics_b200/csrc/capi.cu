@@ -167,6 +167,12 @@ int vtp_solver::parse_config(const json &c) {
             incomp_thr = r["incompThreshold"].get<float>();
             gamma = r["surfaceTensionCoefficient"].get<float>();
         }
+        // extension defaults (a config without a "B200" block restores them)
+        force_div = force_inc = 0;
+        force_seq.clear();
+        device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
+        block = 128; unroll = 4; persistent_tiles = false;
+        pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
             const json &b = c["B200"];
             force_div = b.value("forceDivIterations", 0u);
@@ -187,6 +193,11 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            const std::string form = b.value("pbfFormulation", std::string("reference"));
+            if (form != "reference" && form != "standard")
+                return fail(VTP_ERR_CONFIG, "pbfFormulation must be \"reference\" or \"standard\"");
+            pbf_form = form == "standard" ? 1 : 0;
+            pbf_eps = b.value("pbfEpsilon", pbf_form ? 100.f : 1e-6f);
             if (unroll != 1 && unroll != 2 && unroll != 4 && unroll != 8)
                 return fail(VTP_ERR_CONFIG, "unroll must be 1, 2, 4 or 8");
             if (block < 32 || block > 256 || (block & 31)) return fail(VTP_ERR_CONFIG, "blockSize must be 32..256, multiple of 32");
@@ -310,7 +321,11 @@ int vtp_solver::attach(const float *p, uint32_t n, const float *v, const json &o
 vtp::PbfArgs vtp_solver::pbf_args() {
     vtp::PbfArgs a{};
     a.nf = L.nf; a.nb = L.nb; a.ell_stride = L.ell_stride; a.k = kc;
-    a.rho0 = rho_f; a.inv_rho0 = 1.f / rho_f; a.rho_b = rho_b; a.eps = 1e-6f; a.dt = dt; a.xsph_k = xsph_k;
+    a.rho0 = rho_f; a.inv_rho0 = 1.f / rho_f; a.rho_b = rho_b; a.eps = pbf_eps; a.dt = dt; a.xsph_k = xsph_k;
+    a.form = pbf_form;
+    a.h2 = h * h;
+    a.c6 = (float)(315.0 / (64.0 * 3.14159265358979 * std::pow((double)h, 9.0)));
+    a.cs = (float)(-45.0 / (3.14159265358979 * std::pow((double)h, 6.0)));
     a.nbr = u.nbr; a.ncnt = u.ncnt;
     a.pos = pos.c(); a.pos_alt = pos.n(); a.vel = vel.c(); a.vel_alt = vel.n();
     a.vol = vol; a.density = density; a.lambda = lambda;
@@ -1263,6 +1278,18 @@ int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_
         e = cudaStreamSynchronize(s->st);
     }
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vtp_host_alloc(size_t bytes, void **ptr) {
+    if (!ptr) return fail(VTP_ERR_ARG, "null argument");
+    *ptr = nullptr;
+    cudaError_t e = cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault);
+    if (e != cudaSuccess) return fail(VTP_ERR_NOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    return VTP_OK;
+}
+
+void vtp_host_free(void *ptr) {
+    if (ptr) cudaFreeHost(ptr);
 }
 
 int vtp_solver_get_state_range(vtp_solver *s, uint32_t first, uint32_t count, float *pos, float *vel) {

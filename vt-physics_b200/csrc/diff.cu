@@ -411,6 +411,7 @@ int check_ready(vtp_solver *s) {
     if (!s) return fail(VTP_ERR_ARG, "null solver");
     if (s->type != VTP_SOLVER_PBF) return fail(VTP_ERR_CONFIG, "differentiable mode supports the PBF solver");
     if (s->nscenes() != 1) return fail(VTP_ERR_CONFIG, "differentiable mode runs a single scene");
+    if (s->pbf_form != 0) return fail(VTP_ERR_CONFIG, "differentiable mode follows the reference's PBF formulation");
     return VTP_OK;
 }
 

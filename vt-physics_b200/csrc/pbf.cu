@@ -13,6 +13,24 @@ namespace vtp {
 
 namespace {
 
+// Standard-PBF kernels (form 1): poly6 density, spiky gradient (gradW = g r).
+__device__ __forceinline__ float poly6_w(float d2, const PbfArgs &a) {
+    if (d2 > a.h2) return 0.f;
+    const float d = a.h2 - d2;
+    return a.c6 * d * d * d;
+}
+__device__ __forceinline__ float spiky_g(float d2, const PbfArgs &a) {
+    if (!(d2 > 0.f)) return 0.f;
+    const float r = sqrtf(d2);
+    if (r < 1e-6f * a.k.h || r > a.k.h) return 0.f;
+    const float d = a.k.h - r;
+    return a.cs * d * d / r;
+}
+__device__ __forceinline__ float pbf_w(float d2, const PbfArgs &a) {
+    return a.form ? poly6_w(d2, a) : cubic_w(d2, a.k);
+}
+__device__ __forceinline__ float pbf_w0(const PbfArgs &a) { return a.form ? a.c6 * a.h2 * a.h2 * a.h2 : a.k.w0; }
+
 __global__ void __launch_bounds__(256) k_pbf_init_boundary(PbfArgs a, const uint32_t *__restrict__ bncnt,
                                                            const uint32_t *__restrict__ bnbr,
                                                            uint32_t ell_stride) {
@@ -23,13 +41,13 @@ __global__ void __launch_bounds__(256) k_pbf_init_boundary(PbfArgs a, const uint
     uint32_t i = a.nf + r;
     float4 p = a.pos[i];
     uint32_t n = bncnt[r];
-    float delta = n > 0 ? a.k.w0 : 0.f;
+    float delta = n > 0 ? pbf_w0(a) : 0.f;
     const uint32_t *lst = bnbr + ell_index(r, 0, ell_stride);
     for (uint32_t t = 0; t + 1 < n; ++t) {
         uint32_t j = lst[(size_t)t * 32u];
         if (j < a.nf) continue;
         float4 q = a.pos[j];
-        delta += cubic_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a.k);
+        delta += pbf_w(dist2(p.x - q.x, p.y - q.y, p.z - q.z), a);
     }
     float vb = 1.f / delta;
     a.vol[i] = vb;
@@ -55,14 +73,20 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     const float4 p = a.pos[r];
     const uint32_t n = a.ncnt[r];
     // Self is the first entry of every list: density gets m_i W(0), gradients 0.
-    float rho = n > 0 ? p.w * a.k.w0 : 0.f;
+    float rho = n > 0 ? p.w * pbf_w0(a) : 0.f;
     float gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pos + j); },
                 [&](uint32_t, const float4 &q) {
                     const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
                     float w, g;
-                    cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+                    if (a.form == 0) {
+                        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+                    } else {
+                        const float d2 = dist2(dx, dy, dz);
+                        w = poly6_w(d2, a);
+                        g = spiky_g(d2, a) * q.w;   // mass-weighted constraint gradient
+                    }
                     rho = __fmaf_rn(q.w, w, rho);
                     const float ex = g * dx, ey = g * dy, ez = g * dz;
                     gx += ex; gy += ey; gz += ez;
@@ -91,8 +115,12 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
                 [&](uint32_t j) { return PL{ldg4(a.pos + j), j < a.nf ? __ldg(a.lambda + j) : 0.f}; },
                 [&](uint32_t, const PL &e) {
                     const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                    const float g = cubic_g(dist2(rx, ry, rz), a.k);
-                    const float s = (li + e.l) * g;
+                    float s;
+                    if (a.form == 0) {
+                        s = (li + e.l) * cubic_g(dist2(rx, ry, rz), a.k);
+                    } else {   // (lambda_i m_j + lambda_j m_i) gradW
+                        s = (li * e.q.w + e.l * p.w) * spiky_g(dist2(rx, ry, rz), a);
+                    }
                     dx = __fmaf_rn(s, rx, dx);
                     dy = __fmaf_rn(s, ry, dy);
                     dz = __fmaf_rn(s, rz, dz);
@@ -118,7 +146,7 @@ __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
                 [&](uint32_t j) { return PV2{ldg4(a.pos + j), ldg4(a.vel + j), __ldg(a.vol + j)}; },
                 [&](uint32_t, const PV2 &e) {
-                    const float w = cubic_w(dist2(p.x - e.q.x, p.y - e.q.y, p.z - e.q.z), a.k);
+                    const float w = pbf_w(dist2(p.x - e.q.x, p.y - e.q.y, p.z - e.q.z), a);
                     const float c = a.xsph_k * e.vol;
                     ax = __fmaf_rn(c * (e.v.x - vi.x), w, ax);
                     ay = __fmaf_rn(c * (e.v.y - vi.y), w, ay);

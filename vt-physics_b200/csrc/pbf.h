@@ -10,6 +10,8 @@ struct PbfArgs {
     uint32_t ell_stride;
     Cubic k;
     float rho0, inv_rho0, rho_b, eps, dt, xsph_k;
+    int form;              // 0: the reference's formulation; 1: standard PBF (poly6 / spiky, mass-weighted)
+    float h2, c6, cs;      // standard PBF: h^2, poly6 315/(64 pi h^9), spiky -45/(pi h^6)
     const uint32_t *nbr;   // fluid-row ELL list
     const uint32_t *ncnt;  // fluid-row counts (self included)
     float4 *pos;           // current positions, w = mass

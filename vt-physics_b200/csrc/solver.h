@@ -93,6 +93,8 @@ struct vtp_solver {
     int block = 128;
     int unroll = 4;
     bool persistent_tiles = false;
+    int pbf_form = 0;                   // 0: the reference's PBF formulation, 1: standard PBF
+    float pbf_eps = 1e-6f;
 
     // device state
     cudaStream_t st = nullptr, side = nullptr;

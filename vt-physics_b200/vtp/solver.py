@@ -266,6 +266,37 @@ class Solver:
         return v.value
 
 
+class HostBuffer:
+    """Page-locked host array from vtp_host_alloc (float32, shape (n, 3) by default)."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.shape = tuple(shape)
+        self.dtype = np.dtype(dtype)
+        nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = C.c_void_p()
+        check(lib().vtp_host_alloc(nbytes, C.byref(p)), "host_alloc")
+        self._p = p
+        self.nbytes = nbytes
+        buf = (C.c_char * nbytes).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype).reshape(self.shape)
+
+    @property
+    def ptr(self) -> int:
+        return self._p.value
+
+    def free(self):
+        if self._p is not None and self._p.value:
+            self.array = None
+            lib().vtp_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class PBFSolver(Solver):
     solver_type = PBF
     key = "PBF"
