@@ -121,6 +121,10 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *   "unroll": neighbour-list entries in flight per thread (1, 2, 4, 8);
  *   "persistentTiles": true runs the pressure-solve passes as a persistent
  *       grid looping over the scene-offset tiles (default: one block per tile);
+ *   "pbfFormulation": "reference" (default: the reference's PBF arithmetic,
+ *       PBFCudaImpl.cu:70-194) or "standard" (poly6 density, spiky gradient,
+ *       mass-weighted constraint gradients); "pbfEpsilon": the relaxation
+ *       added to the lambda denominator (default 1e-6 / 100);
  *   "stageTimers": true records CUDA-event stage times. */
 VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 
