@@ -217,23 +217,63 @@ struct Walker {
         }
     }
 
+    // Same test without the capacity check, for a cell whose candidates all fit
+    // in the list.
+    __device__ __forceinline__ void accept_room(uint32_t j, const float4 &q, float d2max) {
+        const float d2 = dist2(px - q.x, py - q.y, pz - q.z);
+        const bool acc = d2 > 0.f && d2 <= d2max;
+        if (acc) out[(size_t)(cnt - 1) * 32u] = j;
+        cnt += acc ? 1u : 0u;
+    }
+
+    template <bool ROOM>
+    __device__ __forceinline__ void test(uint32_t j, const float4 &q, float d2max) {
+        if (ROOM) accept_room(j, q, d2max);
+        else accept(j, q, d2max);
+    }
+
+    template <bool ROOM>
     __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
-        accept(j, __ldg(pos + j), d2max);
+        test<ROOM>(j, __ldg(pos + j), d2max);
     }
 
     // Candidates [j0, j1) in order; positions loaded four at a time.
+    template <bool ROOM>
     __device__ __forceinline__ void visit_run(uint32_t j0, uint32_t j1, const float4 *__restrict__ pos,
                                               float d2max) {
         uint32_t j = j0;
         for (; j + 4 <= j1; j += 4) {
             const float4 q0 = __ldg(pos + j), q1 = __ldg(pos + j + 1), q2 = __ldg(pos + j + 2),
                          q3 = __ldg(pos + j + 3);
-            accept(j, q0, d2max);
-            accept(j + 1, q1, d2max);
-            accept(j + 2, q2, d2max);
-            accept(j + 3, q3, d2max);
+            test<ROOM>(j, q0, d2max);
+            test<ROOM>(j + 1, q1, d2max);
+            test<ROOM>(j + 2, q2, d2max);
+            test<ROOM>(j + 3, q3, d2max);
         }
-        for (; j < j1; ++j) visit(j, pos, d2max);
+        for (; j < j1; ++j) visit<ROOM>(j, pos, d2max);
+    }
+
+    // One cell: fluid run [f0, f1) and boundary run [b0, b1) in MODE's order.
+    template <int MODE, bool ROOM>
+    __device__ __forceinline__ void visit_cell(uint32_t f0, uint32_t f1, uint32_t b0, uint32_t b1,
+                                               const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
+                                               float d2max) {
+        if (MODE == 0) {
+            visit_run<ROOM>(f0, f1, pos, d2max);
+            visit_run<ROOM>(b0, b1, pos, d2max);
+        } else if (MODE == 1) {
+            visit_run<ROOM>(b0, b1, pos, d2max);
+            visit_run<ROOM>(f0, f1, pos, d2max);
+        } else {
+            // Merge the two id-sorted runs by attach id.
+            while (f0 < f1 || b0 < b1) {
+                uint32_t j;
+                if (b0 >= b1) j = f0++;
+                else if (f0 >= f1) j = b0++;
+                else j = (__ldg(orig + f0) < __ldg(orig + b0)) ? f0++ : b0++;
+                visit<ROOM>(j, pos, d2max);
+            }
+        }
     }
 };
 
@@ -269,22 +309,10 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
         uint32_t k = g.key_base + cell_key(cc, g);
         uint32_t f0 = __ldg(fstart + k), f1 = __ldg(fstart + k + 1);
         uint32_t b0 = __ldg(bstart + k), b1 = __ldg(bstart + k + 1);
-        if (MODE == 0) {
-            w.visit_run(f0, f1, pos, d2max);
-            w.visit_run(b0, b1, pos, d2max);
-        } else if (MODE == 1) {
-            w.visit_run(b0, b1, pos, d2max);
-            w.visit_run(f0, f1, pos, d2max);
-        } else {
-            // Merge the two id-sorted runs by attach id.
-            while (f0 < f1 || b0 < b1) {
-                uint32_t j;
-                if (b0 >= b1) j = f0++;
-                else if (f0 >= f1) j = b0++;
-                else j = (__ldg(orig + f0) < __ldg(orig + b0)) ? f0++ : b0++;
-                w.visit(j, pos, d2max);
-            }
-        }
+        // The capacity check is needed only when the cell's candidates could
+        // overflow the list.
+        if (w.cnt + (f1 - f0) + (b1 - b0) <= w.maxnbr) w.visit_cell<MODE, true>(f0, f1, b0, b1, pos, orig, d2max);
+        else w.visit_cell<MODE, false>(f0, f1, b0, b1, pos, orig, d2max);
     }
     ncnt[r] = w.cnt;
     if (w.overflow) {
