@@ -125,6 +125,10 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       PBFCudaImpl.cu:70-194) or "standard" (poly6 density, spiky gradient,
  *       mass-weighted constraint gradients); "pbfEpsilon": the relaxation
  *       added to the lambda denominator (default 1e-6 / 100);
+ *   "cubicCube": "rounded" (default) takes the (1 - q)^3 of the cubic
+ *       kernel's outer branch correctly rounded, at most one ulp from the
+ *       reference's powf(1 - q, 3) (KernelFunctions.cuh:29); "powf" calls powf
+ *       as the reference does, for bit-identical W at a higher cost;
  *   "stageTimers": true records CUDA-event stage times. */
 VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 
@@ -200,6 +204,15 @@ VTP_API int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first,
  * device, against 29 GB/s from PyTorch's pinned-memory allocator). */
 VTP_API int vtp_host_alloc(size_t bytes, void **ptr);
 VTP_API void vtp_host_free(void *ptr);
+
+/* Device self-test of the cubic kernel's outer branch: sph::cubic_value
+ * (KernelFunctions.cuh:29) takes (1 - q)^3 by powf; the library takes it by a
+ * correctly rounded compensated FP32 product unless the "B200" config key
+ * "cubicCube" is "powf".  This compares the two bit for bit over every input
+ * of that branch (t = 1 - q, q in (0.5, 1], i.e. t = k * 2^-24 for k in
+ * [0, 2^23]) on the current device: *mismatches = inputs whose results
+ * differ, *max_ulp = the largest difference in ulps. */
+VTP_API int vtp_selftest_cube(uint32_t *mismatches, uint32_t *max_ulp);
 
 /* Positions and velocities of the particle range [first, first + count)
  * together (pos and vel: count x float[3] host buffers each), one device pass

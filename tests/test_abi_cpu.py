@@ -106,6 +106,10 @@ def test_bad_extension_values_are_rejected():
     assert not s.setConfig(cfg) and "unroll" in s.last_error
     cfg["B200"] = {"blockSize": 100}
     assert not s.setConfig(cfg)
+    cfg["B200"] = {"cubicCube": "cubed"}
+    assert not s.setConfig(cfg) and "cubicCube" in s.last_error
+    cfg["B200"] = {"cubicCube": "powf"}
+    assert s.setConfig(cfg), s.last_error
     s.destroy()
 
 

@@ -204,3 +204,30 @@ def test_standard_pbf_matches_oracle_and_holds_the_fluid(vtp_gpu, oracle_lib):
     p = s.get_field("pos")[f]
     assert (p[:, 1] < 0).sum() < 50
     s.destroy()
+
+
+def test_rounded_cube_is_within_one_ulp_of_powf(vtp_gpu):
+    """The cubic kernel's outer branch takes (1 - q)^3 correctly rounded by a
+    compensated FP32 product; on every input it can see (t = k * 2^-24,
+    k in [0, 2^23]) it must be at most one ulp from CUDA's powf(t, 3.f), which
+    sph::cubic_value calls."""
+    import ctypes as C
+    bad, ulp = C.c_uint32(), C.c_uint32()
+    assert vtp_gpu.lib().vtp_selftest_cube(C.byref(bad), C.byref(ulp)) == 0
+    print(f"cube_rn vs powf: {bad.value} of {2**23 + 1} inputs differ, max {ulp.value} ulp")
+    assert ulp.value <= 1
+
+
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
+def test_powf_cube_option_runs_and_stays_close(vtp_gpu, kind):
+    """"cubicCube": "powf" (the reference's rounding of W) and the default
+    rounded cube give trajectories that agree to FP32 rounding."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break() if kind == "PBF" else vtp.scenes.dam_break("DFSPH", 8000, seed=5)
+    out = []
+    for cube in ("rounded", "powf"):
+        s = vtp.solver_from_scene(sc, extra={"cubicCube": cube})
+        assert s.tickNsteps(4), s.last_error
+        out.append(s.get_field("pos"))
+        s.destroy()
+    assert rel_err(out[0], out[1], 1e-3) < 1e-5

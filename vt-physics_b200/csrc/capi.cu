@@ -171,7 +171,7 @@ int vtp_solver::parse_config(const json &c) {
         force_div = force_inc = 0;
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
-        block = 128; unroll = 4; persistent_tiles = false;
+        block = 128; unroll = 4; persistent_tiles = false; cube_powf = false;
         pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
             const json &b = c["B200"];
@@ -193,6 +193,10 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            const std::string cube = b.value("cubicCube", std::string("rounded"));
+            if (cube != "rounded" && cube != "powf")
+                return fail(VTP_ERR_CONFIG, "cubicCube must be \"rounded\" or \"powf\"");
+            cube_powf = cube == "powf";
             const std::string form = b.value("pbfFormulation", std::string("reference"));
             if (form != "reference" && form != "standard")
                 return fail(VTP_ERR_CONFIG, "pbfFormulation must be \"reference\" or \"standard\"");
@@ -458,6 +462,7 @@ int vtp_solver::initialize() {
     kc.invh = 1.f / h;
     kc.sigma = 8.f / 3.14159265f / std::pow(h, 3.f);  // replaced by the device value below
     kc.w0 = kc.sigma;
+    kc.cube_powf = cube_powf ? 1 : 0;
 
     if (!st) {
         CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -1290,6 +1295,16 @@ int vtp_host_alloc(size_t bytes, void **ptr) {
 
 void vtp_host_free(void *ptr) {
     if (ptr) cudaFreeHost(ptr);
+}
+
+int vtp_selftest_cube(uint32_t *mismatches, uint32_t *max_ulp) {
+    if (!mismatches || !max_ulp) return fail(VTP_ERR_ARG, "null argument");
+    cudaStream_t st;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+    const int rc = vtp::selftest_cube(st, mismatches, max_ulp);
+    cudaStreamDestroy(st);
+    return rc ? fail(VTP_ERR_CUDA, "cube self-test failed to run") : VTP_OK;
 }
 
 int vtp_solver_get_state_range(vtp_solver *s, uint32_t first, uint32_t count, float *pos, float *vel) {

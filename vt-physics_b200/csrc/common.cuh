@@ -113,14 +113,34 @@ struct Cubic {
     float invh;    // 1 / h
     float sigma;   // 8 / pi / h^3 (FP32 as the reference computes it)
     float w0;      // W(0) = sigma
+    int cube_powf = 0;   // outer branch: 1 = powf(1 - q, 3) as the reference, 0 = cube_rn
 };
+
+// t^3 rounded to the nearest float, for t >= 0 (no overflow or underflow in
+// the range used here).  Compensated product (Ogita, Rump & Oishi, "Accurate
+// sum and dot product", SIAM J. Sci. Comput. 2005): t*t = s + es and
+// s*t = p + ep exactly by FMA, so t^3 = p + ep + es*t, and the small terms are
+// folded into p with one rounding.  powf(t, 3.f) is within one ulp of it on
+// the outer-branch domain of cubic_w (t = 1 - q, q in (0.5, 1], i.e.
+// t = k * 2^-24, k in [0, 2^23]) and differs from it on about 6 % of those
+// inputs; vtp_selftest_cube compares the two over all 2^23 + 1 inputs.
+__device__ __forceinline__ float cube_rn(float t) {
+    const float s = t * t;
+    const float es = __fmaf_rn(t, t, -s);
+    const float p = s * t;
+    const float ep = __fmaf_rn(s, t, -p);
+    return p + __fmaf_rn(es, t, ep);
+}
 
 // W(r) from r^2, rounded the way sph::cubic_value rounds it
 // (KernelFunctions.cuh:13-34): IEEE sqrt, q = r * (1/h), the inner branch
 // evaluated in double and rounded once, the outer branch as
-// (sigma * 2) * powf(1 - q, 3).  Density-ratio sums feed `ratio - 1`, where
-// FP32 rounding is amplified ~1e3 times in the pressure solve, so W follows
-// the reference's arithmetic; gradients use the faster form below.
+// (sigma * 2) * (1 - q)^3.  The cube is powf(1 - q, 3) as the reference writes
+// it when `cube_powf` is set (bit-identical W), else the correctly rounded
+// cube_rn, which costs a few FMAs instead of a powf and is at most one ulp
+// from it.  Density-ratio sums feed `ratio - 1`, where FP32 rounding is
+// amplified ~1e3 times in the pressure solve, so W follows the reference's
+// arithmetic; gradients use the faster form below.
 __device__ __forceinline__ float cubic_w(float d2, const Cubic &k) {
     const float r = sqrtf(d2);
     const float q = r * k.invh;
@@ -130,7 +150,8 @@ __device__ __forceinline__ float cubic_w(float d2, const Cubic &k) {
         const float q3 = q2 * q;
         return static_cast<float>((double)k.sigma * (6.0 * (double)q3 - 6.0 * (double)q2 + 1.0));
     }
-    return k.sigma * 2.f * powf(1.f - q, 3.f);
+    const float t = 1.f - q;
+    return k.sigma * 2.f * (k.cube_powf ? powf(t, 3.f) : cube_rn(t));
 }
 
 // Scalar g with gradW(r_vec) = g * r_vec; zero for q < 1e-6 or q > 1.

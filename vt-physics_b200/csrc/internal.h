@@ -83,6 +83,8 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
 
 // sigma of the cubic spline computed on the device (0 on success).
 int cubic_sigma_device(cudaStream_t st, float h, float *out_host);
+// cube_rn(t) vs powf(t, 3.f) over the outer-branch domain of cubic_w (0 on success).
+int selftest_cube(cudaStream_t st, uint32_t *mismatches, uint32_t *max_ulp);
 
 // Gather/scatter between attach order and sorted rows.
 void scatter_f4_to_orig(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, float *dst3);

@@ -471,6 +471,36 @@ __global__ void k_cubic_sigma(float h, float *out) {
     if (threadIdx.x == 0) out[0] = 8.f / PI / powf(h, 3.f);
 }
 
+// cube_rn against powf(t, 3.f) for every t = k * 2^-24, k in [0, 2^23]:
+// number of differing inputs and the largest distance in ulps (both are
+// positive floats, so the distance is the difference of the bit patterns).
+__global__ void k_selftest_cube(uint32_t *mismatches, uint32_t *max_ulp) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > (1u << 23)) return;
+    const float t = (float)k * 0x1p-24f;
+    const int a = (int)__float_as_uint(cube_rn(t)), b = (int)__float_as_uint(powf(t, 3.f));
+    if (a != b) {
+        atomicAdd(mismatches, 1u);
+        atomicMax(max_ulp, (uint32_t)(a > b ? a - b : b - a));
+    }
+}
+
+int selftest_cube(cudaStream_t st, uint32_t *mismatches, uint32_t *max_ulp) {
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, 2 * sizeof(uint32_t)) != cudaSuccess) return 1;
+    uint32_t out[2] = {0u, 0u};
+    cudaError_t e = cudaMemsetAsync(d, 0, 2 * sizeof(uint32_t), st);
+    if (e == cudaSuccess) {
+        k_selftest_cube<<<nblk((1u << 23) + 1u, 256), 256, 0, st>>>(d, d + 1);
+        e = cudaMemcpyAsync(out, d, sizeof(out), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    *mismatches = out[0];
+    *max_ulp = out[1];
+    return e == cudaSuccess ? 0 : 1;
+}
+
 int cubic_sigma_device(cudaStream_t st, float h, float *out_host) {
     float *d = nullptr;
     if (cudaMalloc(&d, sizeof(float)) != cudaSuccess) return 1;

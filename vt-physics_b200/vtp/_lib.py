@@ -53,6 +53,7 @@ SIGNATURES = {
     "vtp_solver_set_field_range": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_uint32, _P, C.c_size_t]),
     "vtp_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "vtp_host_free": (None, [_P]),
+    "vtp_selftest_cube": (C.c_int, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "vtp_solver_get_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_set_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_get_neighbors": (C.c_int, [_P, _P, _P, C.c_uint32]),
