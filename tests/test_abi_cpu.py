@@ -110,6 +110,8 @@ def test_bad_extension_values_are_rejected():
     assert not s.setConfig(cfg) and "cubicCube" in s.last_error
     cfg["B200"] = {"cubicCube": "powf"}
     assert s.setConfig(cfg), s.last_error
+    cfg["B200"] = {"listLanes": 4}
+    assert not s.setConfig(cfg) and "listLanes" in s.last_error
     s.destroy()
 
 

@@ -24,8 +24,8 @@ def _lattice(n, step=0.25, origin=0.0):
     return np.stack([x.ravel(), y.ravel(), z.ravel()], 1).astype(np.float32)
 
 
-def _compare(vtp, oracle_lib, sc, ticks=0):
-    s = vtp.solver_from_scene(sc)
+def _compare(vtp, oracle_lib, sc, ticks=0, lanes=0):
+    s = vtp.solver_from_scene(sc, extra={"listLanes": lanes})
     assert s.initialize(), s.last_error
     if ticks:
         assert s.tickNsteps(ticks), s.last_error
@@ -41,12 +41,13 @@ def _compare(vtp, oracle_lib, sc, ticks=0):
     return s
 
 
+@pytest.mark.parametrize("lanes", [1, 8])
 @pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
-def test_truncated_lists_match_oracle(vtp_gpu, oracle_lib, kind):
+def test_truncated_lists_match_oracle(vtp_gpu, oracle_lib, kind, lanes):
     # 33 neighbours per interior particle (spacing h/2, exact binary fractions) against a cap of 10
     fluid = _lattice(9)
     sc = _scene(kind, [("fluid", fluid, 0)], max_nbr=10)
-    s = _compare(vtp_gpu, oracle_lib, sc)
+    s = _compare(vtp_gpu, oracle_lib, sc, lanes=lanes)
     cnt, _ = s.get_neighbors(10)
     assert cnt.max() == 10
     assert s.tickNsteps(1)
@@ -70,8 +71,9 @@ def test_coincident_particles_are_not_neighbours(vtp_gpu, oracle_lib):
     s.destroy()
 
 
+@pytest.mark.parametrize("lanes", [1, 8])
 @pytest.mark.parametrize("order", ["fluid_first", "boundary_first", "interleaved"])
-def test_attach_orders_match_oracle(vtp_gpu, oracle_lib, order):
+def test_attach_orders_match_oracle(vtp_gpu, oracle_lib, order, lanes):
     sc0 = scenes.dam_break("DFSPH", 2000, seed=40)
     f, b = sc0.objects
     half = f.n // 2
@@ -83,7 +85,7 @@ def test_attach_orders_match_oracle(vtp_gpu, oracle_lib, order):
         objs = [("f1", f.pos[:half], 0), ("b", b.pos, 1), ("f2", f.pos[half:], 0)]
     req = sc0.config["DFSPH"]["Required"]
     sc = _scene("DFSPH", objs, r=req["particleRadius"], lb=req["simSpaceLB"], size=req["simSpaceSize"])
-    s = _compare(vtp_gpu, oracle_lib, sc, ticks=2)
+    s = _compare(vtp_gpu, oracle_lib, sc, ticks=2, lanes=lanes)
     s.destroy()
 
 

@@ -40,11 +40,12 @@ def _check_lists(gpu_cnt, gpu_nb, or_cnt, or_nb):
     assert np.array_equal(gpu_nb, or_nb), "neighbour lists differ"
 
 
+@pytest.mark.parametrize("lanes", [1, 8])
 @pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
-def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind):
+def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind, lanes):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break() if kind == "PBF" else vtp.scenes.dam_break("DFSPH", 30000, seed=7)
-    s = vtp.solver_from_scene(sc)
+    s = vtp.solver_from_scene(sc, extra={"listLanes": lanes})
     assert s.initialize()
     pos0 = s.get_field("pos")
     grid = oracle_lib.make_grid(sc.config[kind]["Required"])
@@ -169,6 +170,23 @@ def test_graph_and_direct_launch_agree(vtp_gpu):
     assert a.stats()["total_incomp_iters"] == b.stats()["total_incomp_iters"]
     for s in (a, b, c):
         s.destroy()
+
+
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH", "IMMCT"])
+def test_list_builders_give_identical_trajectories(vtp_gpu, kind):
+    """One thread per row and eight lanes per row write the same lists, so
+    whole trajectories are bit-identical."""
+    vtp = vtp_gpu
+    sc = {"PBF": lambda: vtp.scenes.pbf_dam_break(),
+          "DFSPH": lambda: vtp.scenes.dam_break("DFSPH", 8000, seed=5),
+          "IMMCT": lambda: vtp.scenes.layered_mixture("IMMCT", 16, seed=3)}[kind]()
+    out = []
+    for lanes in (1, 8):
+        s = vtp.solver_from_scene(sc, extra={"listLanes": lanes})
+        assert s.tickNsteps(6), s.last_error
+        out.append((s.get_field("pos"), s.get_field("vel")))
+        s.destroy()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
 def test_runs_are_deterministic(vtp_gpu):

@@ -171,7 +171,7 @@ int vtp_solver::parse_config(const json &c) {
         force_div = force_inc = 0;
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
-        block = 128; unroll = 4; persistent_tiles = false; cube_powf = false;
+        block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0;
         pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
             const json &b = c["B200"];
@@ -193,6 +193,9 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            list_lanes = b.value("listLanes", 0);
+            if (list_lanes != 0 && list_lanes != 1 && list_lanes != 8)
+                return fail(VTP_ERR_CONFIG, "listLanes must be 0 (by row count), 1 or 8");
             const std::string cube = b.value("cubicCube", std::string("rounded"));
             if (cube != "rounded" && cube != "powf")
                 return fail(VTP_ERR_CONFIG, "cubicCube must be \"rounded\" or \"powf\"");
@@ -433,6 +436,7 @@ int vtp_solver::initialize() {
         mode = mode < 0 ? m : (mode == m ? m : 2);
     }
     L.merge_mode = mode < 0 ? 0 : mode;
+    L.list_lanes = list_lanes;
 
     // Grids as UniformGirdNeighborSearcher::setConfig (UniformGridNeighborSearch.cpp:214-218),
     // one per scene, each followed by its own outside bucket.

@@ -22,6 +22,8 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+// Up to this many rows the list builder runs eight lanes per row.
+constexpr uint32_t kSplitRows = 131072;
 
 __device__ __forceinline__ float4 apply_force(float4 p, float4 &v, float dt, float3 g) {
     // apply_ext_force_cuda (PBFCudaImpl.cu:146-157): v += g dt; x += v dt.
@@ -321,6 +323,121 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
     }
 }
 
+// Lane-split walk for small row counts, where one thread per row leaves most
+// of the GPU idle and the kernel time is one thread's serial walk: L lanes per
+// row, lane l walking the contiguous group [27 l / L, 27 (l+1) / L) of the 27
+// offsets.  Pass 1 counts the lane's accepted candidates, a shuffle scan over
+// the row's lanes gives each lane its first slot, pass 2 walks again and
+// writes.  The concatenation is the one-thread walk's list, truncation at
+// maxNbr included, so both builders write identical lists.
+template <bool WRITE>
+struct SplitSink {
+    float px, py, pz;
+    uint32_t n;       // candidates accepted by this lane so far
+    uint32_t base;    // this lane's first slot
+    uint32_t cap;     // list slots per row (maxNbr - 1)
+    uint32_t *out;    // ELL base of the row
+
+    __device__ __forceinline__ void take(uint32_t j, const float4 &q, float d2max) {
+        const float d2 = dist2(px - q.x, py - q.y, pz - q.z);
+        if (d2 > 0.f && d2 <= d2max) {
+            if (WRITE) {
+                const uint32_t slot = base + n;
+                if (slot < cap) out[(size_t)slot * 32u] = j;
+            }
+            ++n;
+        }
+    }
+
+    __device__ __forceinline__ void run(uint32_t j0, uint32_t j1, const float4 *__restrict__ pos, float d2max) {
+        uint32_t j = j0;
+        for (; j + 4 <= j1; j += 4) {
+            const float4 q0 = __ldg(pos + j), q1 = __ldg(pos + j + 1), q2 = __ldg(pos + j + 2),
+                         q3 = __ldg(pos + j + 3);
+            take(j, q0, d2max);
+            take(j + 1, q1, d2max);
+            take(j + 2, q2, d2max);
+            take(j + 3, q3, d2max);
+        }
+        for (; j < j1; ++j) take(j, __ldg(pos + j), d2max);
+    }
+};
+
+template <int MODE, bool WRITE>
+__device__ __forceinline__ void split_walk(SplitSink<WRITE> &k, int3 c, const SceneGrid &g, int t0, int t1,
+                                           const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
+                                           const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
+                                           float d2max) {
+    for (int t = t0; t < t1; ++t) {
+        int3 cc = c;
+        const int3 o = nbr_offset(t);
+        cc.x += o.x; cc.y += o.y; cc.z += o.z;
+        if (!cell_available(cc, g)) continue;
+        const uint32_t key = g.key_base + cell_key(cc, g);
+        uint32_t f0 = __ldg(fstart + key), f1 = __ldg(fstart + key + 1);
+        uint32_t b0 = __ldg(bstart + key), b1 = __ldg(bstart + key + 1);
+        if (MODE == 0) {
+            k.run(f0, f1, pos, d2max);
+            k.run(b0, b1, pos, d2max);
+        } else if (MODE == 1) {
+            k.run(b0, b1, pos, d2max);
+            k.run(f0, f1, pos, d2max);
+        } else {
+            while (f0 < f1 || b0 < b1) {
+                uint32_t j;
+                if (b0 >= b1) j = f0++;
+                else if (f0 >= f1) j = b0++;
+                else j = (__ldg(orig + f0) < __ldg(orig + b0)) ? f0++ : b0++;
+                k.take(j, __ldg(pos + j), d2max);
+            }
+        }
+    }
+}
+
+template <int MODE, int L>
+__global__ void __launch_bounds__(256) k_build_lists_split(
+    Scenes sc, uint32_t row0, uint32_t cnt, uint32_t ell_stride, const float4 *__restrict__ pos,
+    const uint32_t *__restrict__ orig, const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
+    uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt, uint32_t *__restrict__ status,
+    uint32_t *__restrict__ overflow_count) {
+    static_assert(L >= 2 && L <= 16 && (L & (L - 1)) == 0, "L divides the warp");
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
+    // The L lanes of a row are one aligned group of a warp and leave together.
+    if (r >= cnt) return;
+    const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(L - 1));
+    const uint32_t i = row0 + r;
+    const SceneGrid g = load_scene(sc, i);
+    const float4 p = pos[i];
+    const int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
+    if (!cell_available(c, g)) {  // outside the grid: no neighbours, not even self
+        if (lane == 0) ncnt[r] = 0;
+        return;
+    }
+    const int t0 = 27 * lane / L, t1 = 27 * (lane + 1) / L;
+    const float d2max = sc.d2max;
+    SplitSink<false> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, nullptr};
+    split_walk<MODE>(cnt1, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+    uint32_t x = cnt1.n;
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(gmask, x, o, L);
+        if (lane >= o) x += y;
+    }
+    const uint32_t total = __shfl_sync(gmask, x, L - 1, L);
+    const uint32_t cap = sc.maxnbr - 1u;
+    SplitSink<true> wr{p.x, p.y, p.z, 0u, x - cnt1.n, cap, nbr + ell_index(r, 0, ell_stride)};
+    if (wr.base < cap) split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+    if (lane == 0) {
+        ncnt[r] = total < cap ? total + 1u : sc.maxnbr;
+        if (total > cap) {
+            atomicAdd(overflow_count, 1u);
+            atomicOr(status, ST_BOUNDS);
+        }
+    }
+}
+
 __global__ void k_scatter_f4(uint32_t n, const float4 *__restrict__ src, const uint32_t *__restrict__ orig,
                              float *__restrict__ dst3) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -550,6 +667,28 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
                       const float4 *pos, const uint32_t *orig, const UgnsBuffers &u, uint32_t *nbr, uint32_t *ncnt,
                       uint32_t *status, uint32_t *overflow, int block) {
     if (cnt == 0) return;
+    // Few rows: eight lanes per row (same lists, a quarter to an eighth of the
+    // serial walk per thread).
+    const bool split = L.list_lanes == 8 || (L.list_lanes == 0 && cnt <= kSplitRows);
+    if (split) {
+        constexpr int S = 8;
+        const unsigned ns = nblk(cnt * S, 256);
+        switch (L.merge_mode) {
+            case 0:
+                k_build_lists_split<0, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                                                               u.bstart, nbr, ncnt, status, overflow);
+                break;
+            case 1:
+                k_build_lists_split<1, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                                                               u.bstart, nbr, ncnt, status, overflow);
+                break;
+            default:
+                k_build_lists_split<2, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                                                               u.bstart, nbr, ncnt, status, overflow);
+                break;
+        }
+        return;
+    }
     unsigned nb = nblk(cnt, block);
     switch (L.merge_mode) {
         case 0:
