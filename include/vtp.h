@@ -125,6 +125,12 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       PBFCudaImpl.cu:70-194) or "standard" (poly6 density, spiky gradient,
  *       mass-weighted constraint gradients); "pbfEpsilon": the relaxation
  *       added to the lambda denominator (default 1e-6 / 100);
+ *   "rowLanes": threads per row of the PBF neighbour passes (1 = the list
+ *       walked in order by one thread, default; 4 or 8 = the row's entries
+ *       split over lanes and their sums added by a shuffle butterfly, for
+ *       small scenes);
+ *   "listLanes": neighbour-list builder lanes per row (0 = by row count,
+ *       default; 1 or 8); every setting writes the same lists;
  *   "cubicCube": "rounded" (default) takes the (1 - q)^3 of the cubic
  *       kernel's outer branch correctly rounded, at most one ulp from the
  *       reference's powf(1 - q, 3) (KernelFunctions.cuh:29); "powf" calls powf

@@ -112,6 +112,8 @@ def test_bad_extension_values_are_rejected():
     assert s.setConfig(cfg), s.last_error
     cfg["B200"] = {"listLanes": 4}
     assert not s.setConfig(cfg) and "listLanes" in s.last_error
+    cfg["B200"] = {"rowLanes": 2}
+    assert not s.setConfig(cfg) and "rowLanes" in s.last_error
     s.destroy()
 
 

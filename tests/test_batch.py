@@ -96,6 +96,7 @@ def _run_alone(sc, steps, extra):
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind,steps,extra", [
     ("PBF", 6, None),
+    ("PBF", 6, {"rowLanes": 8}),
     ("DFSPH", 4, None),
     ("DFSPH", 3, {"deviceLoop": False}),
     ("DFSPH", 3, {"useGraphs": False, "blockSize": 64}),

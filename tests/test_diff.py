@@ -59,12 +59,13 @@ def test_oracle_adjoint_matches_finite_differences(oracle_lib):
 # ---------------------------------------------------------------- GPU: the library's adjoint
 
 @pytest.mark.gpu
-def test_gpu_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib):
+@pytest.mark.parametrize("lanes", [1, 8])
+def test_gpu_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib, lanes):
     from vtp import diff
     sc = small_case(7)
     mask = diff.fluid_mask(sc)
     T, every = 10, 4
-    s = diff.pbf_solver(sc)
+    s = diff.pbf_solver(sc, extra={"rowLanes": lanes})
     maxnbr = int(sc.config["PBF"]["Required"]["maxNeighborNum"])
     diff.diff_forward(s, T, every, keep_lists=True)
     lists = [diff.diff_lists(s, t, maxnbr) for t in range(T)]

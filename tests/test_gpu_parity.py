@@ -69,10 +69,11 @@ def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind, lanes):
     s.destroy()
 
 
-def test_pbf_one_substep_matches_oracle(vtp_gpu, oracle_lib):
+@pytest.mark.parametrize("lanes", [1, 4, 8])
+def test_pbf_one_substep_matches_oracle(vtp_gpu, oracle_lib, lanes):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()
-    s = vtp.solver_from_scene(sc)
+    s = vtp.solver_from_scene(sc, extra={"rowLanes": lanes})
     o = oracle_lib.OracleSolver(sc)
     assert s.initialize()
     mass = s.get_field("mass")
@@ -86,7 +87,8 @@ def test_pbf_one_substep_matches_oracle(vtp_gpu, oracle_lib):
     ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
     ed = rel_err(s.get_field("density")[fm], o.density[fm])
     el = rel_err(s.get_field("lambda")[fm], o.lam[fm])
-    print(f"PBF one substep rel errors: pos {ep:.2e} vel {ev:.2e} density {ed:.2e} lambda {el:.2e}")
+    print(f"PBF one substep (rowLanes {lanes}) rel errors: pos {ep:.2e} vel {ev:.2e} density {ed:.2e} "
+          f"lambda {el:.2e}")
     assert ep < TOL and ev < TOL and ed < TOL
     s.destroy()
 
@@ -201,12 +203,13 @@ def test_runs_are_deterministic(vtp_gpu):
     assert np.array_equal(out[0], out[1])
 
 
-def test_standard_pbf_matches_oracle_and_holds_the_fluid(vtp_gpu, oracle_lib):
+@pytest.mark.parametrize("lanes", [1, 8])
+def test_standard_pbf_matches_oracle_and_holds_the_fluid(vtp_gpu, oracle_lib, lanes):
     """The standard PBF formulation (poly6 / spiky, mass-weighted constraint gradients, eps 100),
     an extension checked against the FP64 oracle only (the reference has no such mode)."""
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()
-    extra = {"pbfFormulation": "standard", "pbfEpsilon": 100.0}
+    extra = {"pbfFormulation": "standard", "pbfEpsilon": 100.0, "rowLanes": lanes}
     sc.config["B200"] = dict(extra)
     s = vtp.solver_from_scene(sc, extra)
     assert s.initialize() and s.tickNsteps(1)

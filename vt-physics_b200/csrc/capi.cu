@@ -171,7 +171,7 @@ int vtp_solver::parse_config(const json &c) {
         force_div = force_inc = 0;
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
-        block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0;
+        block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0; row_lanes = 1;
         pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
             const json &b = c["B200"];
@@ -193,6 +193,9 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            row_lanes = b.value("rowLanes", 1);
+            if (row_lanes != 1 && row_lanes != 4 && row_lanes != 8)
+                return fail(VTP_ERR_CONFIG, "rowLanes must be 1, 4 or 8");
             list_lanes = b.value("listLanes", 0);
             if (list_lanes != 0 && list_lanes != 1 && list_lanes != 8)
                 return fail(VTP_ERR_CONFIG, "listLanes must be 0 (by row count), 1 or 8");
@@ -337,6 +340,7 @@ vtp::PbfArgs vtp_solver::pbf_args() {
     a.pos = pos.c(); a.pos_alt = pos.n(); a.vel = vel.c(); a.vel_alt = vel.n();
     a.vol = vol; a.density = density; a.lambda = lambda;
     a.unroll = unroll;
+    a.lanes = row_lanes;
     return a;
 }
 

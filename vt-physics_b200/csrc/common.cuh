@@ -248,4 +248,49 @@ __device__ __forceinline__ void nbr_loop(const uint32_t *__restrict__ lst, uint3
     }
 }
 
+// Lane groups for rows walked by L lanes each (L divides 32; the L lanes of a
+// row are one aligned group of a warp).
+template <int L>
+__device__ __forceinline__ unsigned lane_group_mask() {
+    if constexpr (L >= 32) return 0xffffffffu;
+    else return ((1u << L) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(L - 1));
+}
+
+// Butterfly sum over a row's L lanes; every lane gets the same bits (each
+// step adds the same two values on both partner lanes).
+template <int L>
+__device__ __forceinline__ float lane_sum(float v, unsigned mask) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, L);
+    return v;
+}
+
+// nbr_loop over a row's entries lane, lane + L, lane + 2L, ...: L lanes share
+// one row's list and each keeps U gathers in flight.  With L == 1 this is
+// nbr_loop itself (same order, same results).
+template <int U, int L, class Load, class Use>
+__device__ __forceinline__ void nbr_loop_lanes(const uint32_t *__restrict__ lst, uint32_t cnt, int lane, Load load,
+                                               Use use) {
+    if constexpr (L == 1) {
+        nbr_loop<U>(lst, cnt, load, use);
+    } else {
+        using T = decltype(load(0u));
+        uint32_t t = (uint32_t)lane;
+        for (; t + (uint32_t)((U - 1) * L) < cnt; t += (uint32_t)(U * L)) {
+            uint32_t j[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) j[u] = __ldcs(lst + (size_t)(t + (uint32_t)(u * L)) * 32u);
+            T d[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) d[u] = load(j[u]);
+#pragma unroll
+            for (int u = 0; u < U; ++u) use(j[u], d[u]);
+        }
+        for (; t < cnt; t += (uint32_t)L) {
+            const uint32_t j = __ldcs(lst + (size_t)t * 32u);
+            use(j, load(j));
+        }
+    }
+}
+
 }  // namespace vtp

@@ -66,33 +66,49 @@ struct PV2 {
     float vol;
 };
 
-template <int U>
+// Neighbour passes, U list entries in flight per thread and L lanes per row
+// (L = 1: one thread walks the row's list in order; L > 1: the row's lanes
+// take entries lane, lane + L, ... and their partial sums are added by a
+// butterfly over the group, so a small scene keeps more of the GPU busy; the
+// FP32 sums then group differently from the list order).
+template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
-    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
     const uint32_t n = a.ncnt[r];
     // Self is the first entry of every list: density gets m_i W(0), gradients 0.
-    float rho = n > 0 ? p.w * pbf_w0(a) : 0.f;
+    float rho = (n > 0 && lane == 0) ? p.w * pbf_w0(a) : 0.f;
     float gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pos + j); },
-                [&](uint32_t, const float4 &q) {
-                    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-                    float w, g;
-                    if (a.form == 0) {
-                        cubic_wg(dist2(dx, dy, dz), a.k, w, g);
-                    } else {
-                        const float d2 = dist2(dx, dy, dz);
-                        w = poly6_w(d2, a);
-                        g = spiky_g(d2, a) * q.w;   // mass-weighted constraint gradient
-                    }
-                    rho = __fmaf_rn(q.w, w, rho);
-                    const float ex = g * dx, ey = g * dy, ez = g * dz;
-                    gx += ex; gy += ey; gz += ez;
-                    const float fx = ex * a.inv_rho0, fy = ey * a.inv_rho0, fz = ez * a.inv_rho0;
-                    s2 += fx * fx + fy * fy + fz * fz;
-                });
+    nbr_loop_lanes<U, L>(lst, n > 0 ? n - 1 : 0, lane, [&](uint32_t j) { return ldg4(a.pos + j); },
+                         [&](uint32_t, const float4 &q) {
+                             const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+                             float w, g;
+                             if (a.form == 0) {
+                                 cubic_wg(dist2(dx, dy, dz), a.k, w, g);
+                             } else {
+                                 const float d2 = dist2(dx, dy, dz);
+                                 w = poly6_w(d2, a);
+                                 g = spiky_g(d2, a) * q.w;   // mass-weighted constraint gradient
+                             }
+                             rho = __fmaf_rn(q.w, w, rho);
+                             const float ex = g * dx, ey = g * dy, ez = g * dz;
+                             gx += ex; gy += ey; gz += ez;
+                             const float fx = ex * a.inv_rho0, fy = ey * a.inv_rho0, fz = ez * a.inv_rho0;
+                             s2 += fx * fx + fy * fy + fz * fz;
+                         });
+    if constexpr (L > 1) {
+        const unsigned m = lane_group_mask<L>();
+        rho = lane_sum<L>(rho, m);
+        gx = lane_sum<L>(gx, m);
+        gy = lane_sum<L>(gy, m);
+        gz = lane_sum<L>(gz, m);
+        s2 = lane_sum<L>(s2, m);
+        if (lane != 0) return;
+    }
     if (rho < a.rho0) rho = a.rho0;
     const float err = rho / a.rho0 - 1.f;
     gx /= a.rho0; gy /= a.rho0; gz /= a.rho0;
@@ -101,9 +117,11 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     a.lambda[r] = -err / (s2 + a.eps);
 }
 
-template <int U>
+template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
-    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
     const float li = a.lambda[r];
@@ -111,20 +129,27 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     float dx = 0.f, dy = 0.f, dz = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     // Boundary lambda is never written by the reference; it is taken as 0.
-    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
-                [&](uint32_t j) { return PL{ldg4(a.pos + j), j < a.nf ? __ldg(a.lambda + j) : 0.f}; },
-                [&](uint32_t, const PL &e) {
-                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                    float s;
-                    if (a.form == 0) {
-                        s = (li + e.l) * cubic_g(dist2(rx, ry, rz), a.k);
-                    } else {   // (lambda_i m_j + lambda_j m_i) gradW
-                        s = (li * e.q.w + e.l * p.w) * spiky_g(dist2(rx, ry, rz), a);
-                    }
-                    dx = __fmaf_rn(s, rx, dx);
-                    dy = __fmaf_rn(s, ry, dy);
-                    dz = __fmaf_rn(s, rz, dz);
-                });
+    nbr_loop_lanes<U, L>(lst, n > 0 ? n - 1 : 0, lane,
+                         [&](uint32_t j) { return PL{ldg4(a.pos + j), j < a.nf ? __ldg(a.lambda + j) : 0.f}; },
+                         [&](uint32_t, const PL &e) {
+                             const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                             float s;
+                             if (a.form == 0) {
+                                 s = (li + e.l) * cubic_g(dist2(rx, ry, rz), a.k);
+                             } else {   // (lambda_i m_j + lambda_j m_i) gradW
+                                 s = (li * e.q.w + e.l * p.w) * spiky_g(dist2(rx, ry, rz), a);
+                             }
+                             dx = __fmaf_rn(s, rx, dx);
+                             dy = __fmaf_rn(s, ry, dy);
+                             dz = __fmaf_rn(s, rz, dz);
+                         });
+    if constexpr (L > 1) {
+        const unsigned m = lane_group_mask<L>();
+        dx = lane_sum<L>(dx, m);
+        dy = lane_sum<L>(dy, m);
+        dz = lane_sum<L>(dz, m);
+        if (lane != 0) return;
+    }
     dx /= a.rho0; dy /= a.rho0; dz /= a.rho0;
     float4 o = p;
     o.x += dx; o.y += dy; o.z += dz;
@@ -134,24 +159,33 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     a.vel[r] = v;
 }
 
-template <int U>
+template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
-    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
     const float4 vi = a.vel[r];
     const uint32_t n = a.ncnt[r];
     float ax = 0.f, ay = 0.f, az = 0.f;
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
-                [&](uint32_t j) { return PV2{ldg4(a.pos + j), ldg4(a.vel + j), __ldg(a.vol + j)}; },
-                [&](uint32_t, const PV2 &e) {
-                    const float w = pbf_w(dist2(p.x - e.q.x, p.y - e.q.y, p.z - e.q.z), a);
-                    const float c = a.xsph_k * e.vol;
-                    ax = __fmaf_rn(c * (e.v.x - vi.x), w, ax);
-                    ay = __fmaf_rn(c * (e.v.y - vi.y), w, ay);
-                    az = __fmaf_rn(c * (e.v.z - vi.z), w, az);
-                });
+    nbr_loop_lanes<U, L>(lst, n > 0 ? n - 1 : 0, lane,
+                         [&](uint32_t j) { return PV2{ldg4(a.pos + j), ldg4(a.vel + j), __ldg(a.vol + j)}; },
+                         [&](uint32_t, const PV2 &e) {
+                             const float w = pbf_w(dist2(p.x - e.q.x, p.y - e.q.y, p.z - e.q.z), a);
+                             const float c = a.xsph_k * e.vol;
+                             ax = __fmaf_rn(c * (e.v.x - vi.x), w, ax);
+                             ay = __fmaf_rn(c * (e.v.y - vi.y), w, ay);
+                             az = __fmaf_rn(c * (e.v.z - vi.z), w, az);
+                         });
+    if constexpr (L > 1) {
+        const unsigned m = lane_group_mask<L>();
+        ax = lane_sum<L>(ax, m);
+        ay = lane_sum<L>(ay, m);
+        az = lane_sum<L>(az, m);
+        if (lane != 0) return;
+    }
     const float dx = ax * a.dt, dy = ay * a.dt, dz = az * a.dt;
     float4 o = p;
     o.x += dx; o.y += dy; o.z += dz;
@@ -176,15 +210,24 @@ void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt,
         case 8: { constexpr int UU = 8; __VA_ARGS__; } break; \
         default: { constexpr int UU = 4; __VA_ARGS__; } break; \
     }
+#define VTP_LANES_DISPATCH(L, ...)           \
+    switch (L) {                                 \
+        case 4: { constexpr int LL = 4; __VA_ARGS__; } break; \
+        case 8: { constexpr int LL = 8; __VA_ARGS__; } break; \
+        default: { constexpr int LL = 1; __VA_ARGS__; } break; \
+    }
 
 void pbf_lambda(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_lambda<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
+    if (a.nf)
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_lambda<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
 }
 void pbf_dx(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_dx<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
+    if (a.nf)
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_dx<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
 }
 void pbf_xsph(cudaStream_t st, const PbfArgs &a, int block) {
-    if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_pbf_xsph<UU><<<nblk(a.nf, block), block, 0, st>>>(a))
+    if (a.nf)
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_xsph<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
 }
 
 }  // namespace vtp

@@ -22,6 +22,7 @@ struct PbfArgs {
     float *density;        // [nf]
     float *lambda;         // [nf]
     int unroll;            // neighbours in flight per thread (1, 2, 4, 8)
+    int lanes = 1;         // threads per row of the neighbour passes (1, 4, 8)
 };
 
 void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,
