@@ -565,6 +565,20 @@ def run_diff(args, torch) -> dict:
 
 
 DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "immct_500k": 30, "batched": 200, "diff_pbf": 200}
+# Launch configuration per workload when --extra is not given ("B200" config keys;
+# vtp/autotune.py --lanes picks 8 lanes per row for the 16k-particle PBF scene).
+DEFAULT_EXTRA = {"pbf": {"rowLanes": 8}}
+L2_BYTES = 126e6
+
+
+def l2_note(s, req) -> str:
+    """Working set of one substep (state arrays, both buffers, plus the fluid
+    neighbour lists) against the 126 MB L2; substeps run back to back without a
+    flush, as a simulation runs them."""
+    c = s.counts()
+    ws = c["total"] * 160 + c["fluid"] * int(req["maxNeighborNum"]) * 4
+    rel = "larger than" if ws > L2_BYTES else "smaller than"
+    return f"working set ~{ws / 1e6:.0f} MB per replica, {rel} L2 (126 MB); no flush between substeps"
 
 
 def main():
@@ -621,7 +635,7 @@ def main():
             print(json.dumps(line), flush=True)
         return 0
     sc = make_scene(args.workload)
-    extra = json.loads(args.extra) if args.extra else {}
+    extra = json.loads(args.extra) if args.extra else dict(DEFAULT_EXTRA.get(args.workload, {}))
     if args.block:
         extra["blockSize"] = args.block
     s = vtp.solver_from_scene(sc, extra=extra or None)
@@ -702,7 +716,8 @@ def main():
                    "dt": req["timeStep"], "parallelism": f"replicas{world}",
                    "div_iters_total": st["total_div_iters"], "incomp_iters_total": st["total_incomp_iters"],
                    "mean_neighbors": round(k_mean, 2),
-                   "l2": "inputs larger than L2 (state + neighbour lists ~0.5 GB per replica)",
+                   "l2": l2_note(s, req),
+                   "b200": extra,
                    "wall_ms_per_step": 1e3 * wall / args.steps},
         "clocks": clocks,
         "gpu_launches": int(launches),
