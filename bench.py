@@ -400,15 +400,20 @@ def run_batched(args, rank, world, local, dist, torch):
         for k, (lo, hi) in zip(idx, ranges):
             final[k] = pos[lo:hi].copy()
 
-    # Roofline of the dominant kernel of the heavier batch (per-launch CUDA events).
+    # Roofline of the dominant kernel (per-launch CUDA events), with the work model of the
+    # batch that launches it.
     prof = {}
+    cands = []
     for kind, idx, b, _ in batches:
         for name, (ms, n) in b.profile_kernels(args.profile_steps).items():
             pm, pn = prof.get(name, (0.0, 0))
             prof[name] = (pm + ms, pn + n)
+            cands.append((ms, n, name, kind, idx, b))
     kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1],
                    "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    d_ms, d_n, dom_name, d_kind, d_idx, d_b = max(cands, key=lambda c: c[0])
+    roofline = batch_roofline(d_b, d_kind, [mix[k] for k in d_idx], dom_name, d_ms / max(d_n, 1), clocks)
 
     # e2e through the public API: every batch's whole state (positions and velocities of all
     # its particles) round-trips through pinned host memory each step (H2D, one substep, D2H).
@@ -451,20 +456,45 @@ def run_batched(args, rank, world, local, dist, torch):
         cfg["per_scene_loop_ms_per_step"] = loop_ms / args.steps
         cfg["speedup_vs_per_scene_loop"] = cfg["per_scene_loop_value"] and value / cfg["per_scene_loop_value"]
         cfg["identical_per_scene"] = bool(same)
-    dom_name, (dom_ms, dom_launches) = max(prof.items(), key=lambda kv: kv[1][0])
-    peak, peak_kind = peaks()
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg, "clocks": clocks,
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": None, "peak": peak, "unit": "GB/s",
-                     "frac": None, "peak_kind": peak_kind, "traffic": None,
-                     "ms_per_launch": dom_ms / max(dom_launches, 1)},
+        "roofline": roofline,
         "kernels": kernels,
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
     }
     return line
+
+
+def grid_buckets(req) -> int:
+    """Cell buckets of one scene's grid (the reference's linear key range plus the
+    inclusive upper layers, as the library allocates them)."""
+    import numpy as np
+    h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
+    dims = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
+    return dims[2] * dims[1] * dims[0] + dims[1] * dims[0] + dims[0] + 1
+
+
+def batch_roofline(b, kind, batch_scenes, name, per_launch_ms, clocks) -> dict:
+    """Roofline of kernel `name` of one batched solver: the work model of the whole batch
+    (all its scenes' rows, buckets and measured mean neighbour count)."""
+    import numpy as np
+    from vtp.bytes_model import kernel_bytes, kernel_flops
+    c = b.counts()
+    req = batch_scenes[0].config[kind]["Required"]
+    fluid = np.asarray(b.get_field("mat")).reshape(-1) == 0
+    cnt, _ = b.get_neighbors(int(req["maxNeighborNum"]))
+    k_mean = float(np.mean(cnt[fluid].astype(np.float64) - 1.0)) if fluid.any() else 0.0
+    K = sum(grid_buckets(m.config[kind]["Required"]) for m in batch_scenes)
+    bts = kernel_bytes(kind, name, c["total"], c["fluid"], K, k_mean)
+    peak, peak_kind = peaks()
+    out = roofline_of(name, bts, kernel_flops(name, c["fluid"], k_mean), per_launch_ms, peak, peak_kind, clocks,
+                      "batched")
+    out["batch"] = {"solver": kind, "scenes": len(batch_scenes), "rows": c["total"], "fluid": c["fluid"],
+                    "mean_neighbors": round(k_mean, 2)}
+    return out
 
 
 def run_diff(args, torch) -> dict:
