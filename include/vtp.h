@@ -125,6 +125,10 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       PBFCudaImpl.cu:70-194) or "standard" (poly6 density, spiky gradient,
  *       mass-weighted constraint gradients); "pbfEpsilon": the relaxation
  *       added to the lambda denominator (default 1e-6 / 100);
+ *   "cellOrder": "brick" (default) keeps rows in 4x4x4-cell bricks with
+ *       Morton order inside (compact neighbourhoods for the gathers) or
+ *       "linear" in the reference's linear cell order; lists, exported keys
+ *       and sorted order are the reference's either way;
  *   "rowLanes": threads per row of the PBF neighbour passes (1 = the list
  *       walked in order by one thread, default; 4 or 8 = the row's entries
  *       split over lanes and their sums added by a shuffle butterfly, for

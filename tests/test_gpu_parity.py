@@ -40,12 +40,13 @@ def _check_lists(gpu_cnt, gpu_nb, or_cnt, or_nb):
     assert np.array_equal(gpu_nb, or_nb), "neighbour lists differ"
 
 
+@pytest.mark.parametrize("order", ["brick", "linear"])
 @pytest.mark.parametrize("lanes", [1, 8])
 @pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
-def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind, lanes):
+def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind, lanes, order):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break() if kind == "PBF" else vtp.scenes.dam_break("DFSPH", 30000, seed=7)
-    s = vtp.solver_from_scene(sc, extra={"listLanes": lanes})
+    s = vtp.solver_from_scene(sc, extra={"listLanes": lanes, "cellOrder": order})
     assert s.initialize()
     pos0 = s.get_field("pos")
     grid = oracle_lib.make_grid(sc.config[kind]["Required"])
@@ -189,6 +190,29 @@ def test_list_builders_give_identical_trajectories(vtp_gpu, kind):
         out.append((s.get_field("pos"), s.get_field("vel")))
         s.destroy()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH", "IMMCT"])
+def test_cell_orders_give_identical_trajectories(vtp_gpu, kind):
+    """Bricked and linear bucket orders store rows differently but walk the
+    same lists in the same order, so trajectories (in attach order) are
+    bit-identical; the DFSPH residual partials group rows by tile, which only
+    moves FP64 roundings, so iteration counts agree too."""
+    vtp = vtp_gpu
+    sc = {"PBF": lambda: vtp.scenes.pbf_dam_break(),
+          "DFSPH": lambda: vtp.scenes.dam_break("DFSPH", 8000, seed=5),
+          "IMMCT": lambda: vtp.scenes.layered_mixture("IMMCT", 16, seed=3)}[kind]()
+    out = []
+    for order in ("brick", "linear"):
+        s = vtp.solver_from_scene(sc, extra={"cellOrder": order})
+        assert s.tickNsteps(6), s.last_error
+        out.append((s.get_field("pos"), s.get_field("vel"), s.stats()))
+        s.destroy()
+    if kind == "PBF":
+        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    else:
+        assert rel_err(out[0][0], out[1][0]) < 1e-6
+        assert out[0][2]["total_div_iters"] == out[1][2]["total_div_iters"]
 
 
 def test_runs_are_deterministic(vtp_gpu):

@@ -172,6 +172,7 @@ int vtp_solver::parse_config(const json &c) {
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
         block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0; row_lanes = 1;
+        cell_order_brick = true;
         pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
             const json &b = c["B200"];
@@ -193,6 +194,10 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            const std::string order = b.value("cellOrder", std::string("brick"));
+            if (order != "brick" && order != "linear")
+                return fail(VTP_ERR_CONFIG, "cellOrder must be \"brick\" or \"linear\"");
+            cell_order_brick = order == "brick";
             row_lanes = b.value("rowLanes", 1);
             if (row_lanes != 1 && row_lanes != 4 && row_lanes != 8)
                 return fail(VTP_ERR_CONFIG, "rowLanes must be 1, 4 or 8");
@@ -453,8 +458,16 @@ int vtp_solver::initialize() {
         g.gy = (int)std::ceil(sc.size[1] / h);
         g.gz = (int)std::ceil(sc.size[2] / h);
         if (g.gx <= 0 || g.gy <= 0 || g.gz <= 0) return fail(VTP_ERR_CONFIG, "empty grid");
-        // Keys reach z*gy*gx + y*gx + x with the inclusive upper bound of cellIsAvailable.
-        uint64_t maxkey = (uint64_t)g.gz * g.gy * g.gx + (uint64_t)g.gy * g.gx + g.gx;
+        // Cells 0..g per axis (the inclusive upper bound of cellIsAvailable).  Bricked
+        // bucket order (4^3-cell bricks, Morton inside) unless the grid is under 4
+        // cells wide in x or y; the linear key reaches z*gy*gx + y*gx + x.
+        const uint64_t bx = (uint64_t)(g.gx + 4) / 4, by = (uint64_t)(g.gy + 4) / 4,
+                       bz = (uint64_t)(g.gz + 4) / 4;
+        g.brick = (cell_order_brick && g.gx >= 4 && g.gy >= 4) ? 1 : 0;
+        g.bx = (uint32_t)bx;
+        g.by = (uint32_t)by;
+        uint64_t maxkey = g.brick ? bx * by * bz * 64 - 1
+                                  : (uint64_t)g.gz * g.gy * g.gx + (uint64_t)g.gy * g.gx + g.gx;
         if (maxkey + 2 > (1ull << 31)) return fail(VTP_ERR_BOUNDS, "grid too large (more than 2^31 cells)");
         g.nkey = (uint32_t)(maxkey + 1);
         g.key_base = (uint32_t)key_base;

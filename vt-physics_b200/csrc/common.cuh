@@ -56,7 +56,8 @@ struct SceneGrid {
     uint32_t key_base;
     uint32_t nkey;             // buckets of in-grid cells (outside bucket excluded)
     float grav_x, grav_y, grav_z;
-    uint32_t pad_;
+    int brick;                 // 1: bricked bucket order (cell_key), 0: the reference's linear key
+    uint32_t bx, by;           // bricks along x and y
 };
 
 // Shared neighbour-search constants plus the per-row scene map.
@@ -78,9 +79,32 @@ __device__ __forceinline__ bool cell_available(int3 c, const SceneGrid &g) {
     return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x <= g.gx && c.y <= g.gy && c.z <= g.gz;
 }
 
-// Scene-local linear cell id (the reference's cell index inside that scene's grid).
-__device__ __forceinline__ uint32_t cell_key(int3 c, const SceneGrid &g) {
+// Scene-local linear cell id: the reference's cell index inside that scene's
+// grid (getCellId, UGNSCudaImpl.cu:58-63), used for the exported keys.
+__device__ __forceinline__ uint32_t ref_cell_key(int3 c, const SceneGrid &g) {
     return (uint32_t)c.z * (uint32_t)(g.gy * g.gx) + (uint32_t)c.y * (uint32_t)g.gx + (uint32_t)c.x;
+}
+
+// Bit i of a 2-bit value moved to bit 3i (Morton interleave of 3 coordinates).
+__device__ __forceinline__ uint32_t morton_spread2(uint32_t v) { return (v & 1u) | ((v & 2u) << 2); }
+
+// Scene-local bucket of a cell, the order rows are kept in.  Bricked order:
+// the grid is cut into 4 x 4 x 4-cell bricks taken in linear order (x
+// fastest), and the 64 cells of a brick follow the Morton (Z) curve, so
+// consecutive rows - a warp, a 128-row tile - cover a compact block of cells
+// and their neighbourhoods overlap in cache.  Every in-grid cell has its own
+// bucket; the reference's linear id (ref_cell_key) instead lets cells on the
+// inclusive upper x (y) face share a bucket with the first cell of the next
+// row (plane), which only matters for grids under 4 cells wide in x or y:
+// those keep the linear order (brick == 0), so that the candidates a row
+// visits are the reference's in every grid.  A cell's run is sorted by attach
+// id in either order and lists are walked cell by cell in the reference's
+// offset order, so the lists do not depend on the bucket order.
+__device__ __forceinline__ uint32_t cell_key(int3 c, const SceneGrid &g) {
+    if (!g.brick) return ref_cell_key(c, g);
+    const uint32_t x = (uint32_t)c.x, y = (uint32_t)c.y, z = (uint32_t)c.z;
+    const uint32_t b = ((z >> 2) * g.by + (y >> 2)) * g.bx + (x >> 2);
+    return b * 64u + (morton_spread2(x & 3u) | (morton_spread2(y & 3u) << 1) | (morton_spread2(z & 3u) << 2));
 }
 
 __device__ __forceinline__ SceneGrid load_scene(const Scenes &sc, uint32_t row) {

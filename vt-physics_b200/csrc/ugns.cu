@@ -576,7 +576,7 @@ __global__ void k_export_sorted(Scenes sc, uint32_t n, const float4 *__restrict_
     float4 p = pos[i];
     int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
     ids[i] = orig[i];
-    keys[i] = cell_available(c, g) ? cell_key(c, g) : 0xffffffffu;
+    keys[i] = cell_available(c, g) ? ref_cell_key(c, g) : 0xffffffffu;
 }
 
 inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
