@@ -793,6 +793,8 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     launches_per_tick += 8;  // neighbour search (7) + ratio/alpha
     if ((rc = enqueue_solve(s, 0, capture))) return rc;
     vtp::DfsphArgs a = dfsph_args();
+    PROF(this, "dfsph_pressure_pack", vtp::dfsph_pressure_pack(s, a));
+    launches_per_tick += 1;
     if (gamma == 0.f) {
         // Tension terms are exactly zero when gamma == 0 (-0 * finite); the normal pass is skipped.
         PROF(this, "dfsph_viscosity", vtp::dfsph_viscosity(s, a, block));

@@ -84,9 +84,6 @@ __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_
 struct PV {
     float4 q, v;
 };
-struct PVV {
-    float4 q, v, va;
-};
 struct PN {
     float4 q, n;
 };
@@ -196,6 +193,17 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     }
 }
 
+// After the divergence solve: the packed rows' second half becomes the
+// velocity after apply_pressure_acc (DFSPHCudaImpl.cu:505-521) for fluid
+// rows, so the viscosity pass gathers {x_j, v_j} with one 256-bit load; the
+// first half still holds x_j from dfsph_solve_pack (positions do not change
+// during the solve).
+__global__ void k_pressure_pack(DfsphArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    a.pva[2 * (size_t)r + 1] = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+}
+
 __global__ void k_solve_pack(DfsphArgs a, uint32_t n) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
@@ -293,15 +301,15 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
                 [&](uint32_t j) {
-                    if (j >= a.nf) return PVV{};   // same-material neighbours only
-                    return PVV{ldg4(a.pos + j), ldg4(a.vel + j), ldg4(a.vadv + j)};
+                    if (j >= a.nf) return F4x2{};   // same-material neighbours only
+                    return ldg8(a.pva + 2 * (size_t)j);   // {x_j, v_j after the pressure step}
                 },
-                [&](uint32_t j, const PVV &e) {
+                [&](uint32_t j, const F4x2 &e) {
                     if (j >= a.nf) return;
-                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                    const float rx = p.x - e.a.x, ry = p.y - e.a.y, rz = p.z - e.a.z;
                     const float d2 = dist2(rx, ry, rz);
                     const float g = cubic_g(d2, a.k);
-                    const float4 vj = pressure_applied(e.v, e.va, a.inv_dt, a.dt);
+                    const float4 vj = e.b;
                     const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
                     const float pi = a.vis_coef * (vx * rx + vy * ry + vz * rz) / (d2 + a.h2_001);
                     const float s = 10.f * pi * g;
@@ -431,6 +439,9 @@ void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
     k_solve_end<<<c.nscenes, 1024, 0, st>>>(c, partials, status);
+}
+void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a) {
+    if (a.nf) k_pressure_pack<<<nblk(a.nf, 256), 256, 0, st>>>(a);
 }
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block) {
     if (a.nf) VTP_UNROLL_DISPATCH(a.unroll, k_viscosity<false, UU><<<nblk(a.nf, block), block, 0, st>>>(a))

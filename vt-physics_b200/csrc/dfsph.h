@@ -95,6 +95,9 @@ void dfsph_solve_pack(cudaStream_t st, const DfsphArgs &a);
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status);
+// Packed rows {x, v after the pressure step} for the viscosity pass (after the
+// divergence solve, before dfsph_viscosity / dfsph_vis_normal).
+void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a);
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
