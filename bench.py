@@ -137,9 +137,12 @@ def ncu_traffic(workload: str, kernel: str):
 
 
 def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload) -> dict:
-    """Roofline of one kernel: algorithmic bytes against the measured HBM copy bandwidth and
-    algorithmic FP32 flops against the SIMT peak at the sampled clock; the binding one (the
-    larger ideal time) is reported as `bound`, both fractions are kept."""
+    """Roofline of one kernel against the HBM ceiling (no pass is a contraction, so the tensor
+    ceiling does not apply): algorithmic state bytes per launch (each state array once, the work
+    model of vtp/bytes_model.py) over the CUDA-event launch time, against the measured HBM copy
+    bandwidth.  Kept beside it: the list-inclusive bytes, and algorithmic FP32 flops against the
+    SIMT peak at the sampled clock (`fp32.ideal_over_hbm` > 1 means the flops, not the bytes, set
+    the ideal time)."""
     t = per_launch_ms / 1e3
     hbm = b["state"] / t / 1e9
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
@@ -153,10 +156,8 @@ def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload
                    "frac_with_lists": b["total"] / t / 1e9 / peak},
            "fp32": {"achieved": tf, "peak": fpk, "unit": "TFLOP/s", "frac": tf / fpk if fpk else None,
                     "peak_kind": f"computed: SMs x 128 x 2 x {mhz:.0f} MHz", "flops_per_launch": flops}}
-    if t_flops > t_bytes:
-        out.update({"bound": "fp32", "achieved": tf, "peak": fpk, "unit": "TFLOP/s", "frac": tf / fpk})
-    else:
-        out.update({"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak})
+    out["fp32"]["ideal_over_hbm"] = t_flops / t_bytes if t_bytes else None
+    out.update({"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak})
     out["traffic"] = ncu_traffic(workload, name)
     return out
 
