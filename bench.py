@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile-steps", type=int, default=3)
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="substeps of the end-to-end run (0: the same substeps as the timed run)")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--extra", default="", help='extra "B200" config keys as JSON, e.g. {"unroll": 2}')
     ap.add_argument("--scene-index", type=int, default=-1, help=argparse.SUPPRESS)
@@ -281,7 +282,7 @@ def run_reference(args) -> dict:
     assert fluid_ranges(sc) == [(0, nfl)]
     pos = s.get_prefix("pos", nfl)
     vel = s.get_prefix("vel", nfl)
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 20)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         s.set("pos", pos)
@@ -419,7 +420,7 @@ def run_batched(args, rank, world, local, dist, torch):
     # e2e through the public API: every batch's whole state (positions and velocities of all
     # its particles) round-trips through pinned host memory each step (H2D, one substep, D2H).
     hbuf = [state_buffers(b, [(0, b.counts()["total"])], torch) for _, _, b, _ in batches]
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 20)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -469,13 +470,17 @@ def run_batched(args, rank, world, local, dist, torch):
     return line
 
 
-def grid_buckets(req) -> int:
-    """Cell buckets of one scene's grid (the reference's linear key range plus the
-    inclusive upper layers, as the library allocates them)."""
+def grid_buckets(req, extra=None) -> int:
+    """Cell buckets of one scene's grid as the library allocates them (cells 0..g per axis,
+    the reference's inclusive upper bound): 64-cell bricks, or the reference's linear key range
+    for "cellOrder": "linear" and grids under 4 cells wide in x or y; plus the outside bucket."""
     import numpy as np
     h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
-    dims = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
-    return dims[2] * dims[1] * dims[0] + dims[1] * dims[0] + dims[0] + 1
+    gx, gy, gz = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
+    linear = (extra or {}).get("cellOrder", "brick") == "linear" or gx < 4 or gy < 4
+    if linear:
+        return gz * gy * gx + gy * gx + gx + 1 + 1
+    return 64 * ((gx + 4) // 4) * ((gy + 4) // 4) * ((gz + 4) // 4) + 1
 
 
 def batch_roofline(b, kind, batch_scenes, name, per_launch_ms, clocks) -> dict:
@@ -487,8 +492,8 @@ def batch_roofline(b, kind, batch_scenes, name, per_launch_ms, clocks) -> dict:
     req = batch_scenes[0].config[kind]["Required"]
     fluid = np.asarray(b.get_field("mat")).reshape(-1) == 0
     cnt, _ = b.get_neighbors(int(req["maxNeighborNum"]))
-    k_mean = float(np.mean(cnt[fluid].astype(np.float64) - 1.0)) if fluid.any() else 0.0
-    K = sum(grid_buckets(m.config[kind]["Required"]) for m in batch_scenes)
+    k_mean = float(np.mean(np.maximum(cnt[fluid].astype(np.float64) - 1.0, 0.0))) if fluid.any() else 0.0
+    K = sum(grid_buckets(m.config[kind]["Required"]) for m in batch_scenes)  # default cell order
     bts = kernel_bytes(kind, name, c["total"], c["fluid"], K, k_mean)
     peak, peak_kind = peaks()
     out = roofline_of(name, bts, kernel_flops(name, c["fluid"], k_mean), per_launch_ms, peak, peak_kind, clocks,
@@ -602,6 +607,23 @@ DEFAULT_EXTRA = {"pbf": {"rowLanes": 8}}
 L2_BYTES = 126e6
 
 
+def neighbor_pass(kind, prof, substeps, nf, K, k_mean, peak, peak_kind) -> dict:
+    """The whole neighbour pass of one substep (hash, scan, scatter, rank/reorder, list build:
+    per-kernel CUDA events) against the HBM ceiling, with the bytes of the neighbour-pass work
+    model (fluid re-bin and cell tables; the list writes beside it)."""
+    from vtp.bytes_model import UGNS_KERNELS, neighbor_pass_bytes
+    ms = sum(prof.get(k, (0.0, 0))[0] for k in UGNS_KERNELS) / max(substeps, 1)
+    sort_ms = sum(prof.get(k, (0.0, 0))[0] for k in UGNS_KERNELS[:-1]) / max(substeps, 1)
+    b = neighbor_pass_bytes(kind, nf, K)
+    lists = 4.0 * k_mean * nf
+    gbs = b / (ms / 1e3) / 1e9 if ms else None
+    return {"kernels": list(UGNS_KERNELS), "ms_per_substep": ms, "sort_ms_per_substep": sort_ms,
+            "bytes_per_substep": b, "achieved": gbs, "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+            "frac": gbs / peak if gbs else None, "list_bytes_per_substep": lists,
+            "frac_with_lists": (b + lists) / (ms / 1e3) / 1e9 / peak if ms else None,
+            "sort_frac": b / (sort_ms / 1e3) / 1e9 / peak if sort_ms else None}
+
+
 def l2_note(s, req) -> str:
     """Working set of one substep (state arrays, both buffers, plus the fluid
     neighbour lists) against the 126 MB L2; substeps run back to back without a
@@ -702,14 +724,13 @@ def main():
     try:
         cnt_all, _ = s.get_neighbors(int(sc.config[sc.solver]["Required"]["maxNeighborNum"]))
         fmask = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
-        k_mean = float(np.mean(cnt_all[fmask].astype(np.float64) - 1.0))
+        k_mean = float(np.mean(np.maximum(cnt_all[fmask].astype(np.float64) - 1.0, 0.0)))
     except Exception:
         pass
     from vtp.bytes_model import kernel_bytes, kernel_flops
     req = sc.config[sc.solver]["Required"]
     h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
-    dims = [int(np.ceil(np.float32(np.float32(v) / np.float32(h)))) for v in req["simSpaceSize"]]
-    K = dims[2] * dims[1] * dims[0] + dims[1] * dims[0] + dims[0] + 1
+    K = grid_buckets(req, extra)
     N = sc.n_total
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_launches) = dom
@@ -721,12 +742,21 @@ def main():
                            clocks, args.workload)
     kernels = {k: {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / sum(x[0] for x in prof.values()), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    npass = neighbor_pass(sc.solver, prof, args.profile_steps, nf, K, k_mean, peak, peak_kind)
 
-    # e2e through the public API: every step the fluid state (positions and velocities of
-    # the fluid objects; boundary particles are static) goes host -> device from pinned
+    l2 = l2_note(s, req)
+    s.destroy()
+
+    # e2e through the public API, over the same substeps as the timed run (a fresh solver of
+    # the same scene, the same warm-up): every step the fluid state (positions and velocities
+    # of the fluid objects; boundary particles are static) goes host -> device from pinned
     # memory, one substep runs, and the new fluid state comes back device -> host.
+    s = vtp.solver_from_scene(sc, extra=extra or None)
+    assert s.initialize(), s.last_error
+    if args.warmup:
+        assert s.tickNsteps(args.warmup), s.last_error
     bufs = state_buffers(s, fluid_ranges(sc), torch)
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else args.steps
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -747,15 +777,17 @@ def main():
                    "dt": req["timeStep"], "parallelism": f"replicas{world}",
                    "div_iters_total": st["total_div_iters"], "incomp_iters_total": st["total_incomp_iters"],
                    "mean_neighbors": round(k_mean, 2),
-                   "l2": l2_note(s, req),
+                   "l2": l2,
                    "b200": extra,
                    "wall_ms_per_step": 1e3 * wall / args.steps},
         "clocks": clocks,
         "gpu_launches": int(launches),
         "roofline": roofline,
+        "neighbor_pass": npass,
         "kernels": kernels,
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": state_bytes(bufs),
-                "d2h_bytes_per_step": state_bytes(bufs)},
+                "d2h_bytes_per_step": state_bytes(bufs), "steps": e2e_steps,
+                "substeps": f"{args.warmup + 1}-{args.warmup + e2e_steps} of a fresh solver"},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc, args.cpu_seconds)

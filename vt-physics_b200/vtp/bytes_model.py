@@ -9,6 +9,19 @@ design reads on top.
 from __future__ import annotations
 
 
+UGNS_KERNELS = ("ugns_clear_hash", "ugns_cell_scan", "ugns_scatter", "ugns_rank_reorder", "ugns_lists")
+
+
+def neighbor_pass_bytes(kind: str, Nf: int, K: int) -> float:
+    """Algorithmic bytes of one neighbour pass (re-bin the fluid rows; the static boundary is
+    binned once): Nf (12 key-in + 4 key + 4 key re-read + 4 permutation + 2 S) + 16 K, where S
+    is the reordered per-particle state (28 B: position, velocity, material for PBF / DFSPH;
+    84 B for IMM-CT: position, velocity, two phase velocities, two fractions, symmetric Q,
+    material).  The neighbour-list writes are not in this model."""
+    S = 84 if kind in ("IMM", "IMMCT") else 28
+    return Nf * (12 + 4 + 4 + 4 + 2 * S) + 16.0 * K
+
+
 def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float, P: int = 2) -> dict:
     lst = 4.0 * k * Nf
     if name == "ugns_clear_hash":
