@@ -102,6 +102,16 @@ inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
         default: { constexpr int UU = 4; __VA_ARGS__; } break; \
     }
 
+// Phase count as a compile-time constant for the common mixtures (2: IMM-CT and
+// two-phase IMM, 3: three-phase IMM), so the per-phase arrays of the neighbour
+// passes live in registers; other counts use the runtime loop (PP = 0).
+#define VTP_PHASE_DISPATCH(P, ...)                              \
+    switch (P) {                                                \
+        case 2: { constexpr int PP = 2; __VA_ARGS__; } break;   \
+        case 3: { constexpr int PP = 3; __VA_ARGS__; } break;   \
+        default: { constexpr int PP = 0; __VA_ARGS__; } break;  \
+    }
+
 __device__ __forceinline__ float rest_of(const ImmArgs &a, uint32_t r) {
     float s = 0.f;
     for (int k = 0; k < a.p.P; ++k) s = __fmaf_rn(a.frac[k][r], a.p.rho[k], s);
@@ -207,16 +217,17 @@ struct VisG {
 
 // Gravity + phase viscosity (+ normals when tension is on); without tension the
 // phase and mixture velocities are advanced here as well.
-template <bool SPLIT, int U>
+template <bool SPLIT, int U, int PP>
 __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
     const float4 vi = a.vel[r];
     const float cd = a.cd[r];
-    const int P = a.p.P;
-    float3 acc[kMaxPhases];
-    float4 vk_i[kMaxPhases];
+    const int P = PP > 0 ? PP : a.p.P;
+    float3 acc[PP > 0 ? PP : kMaxPhases];
+    float4 vk_i[PP > 0 ? PP : kMaxPhases];
+#pragma unroll
     for (int k = 0; k < P; ++k) {
         acc[k] = a.g;
         vk_i[k] = a.vph[k][r];
@@ -236,6 +247,7 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
                     const float g = cubic_g(d2, a.k);
                     const float gx = g * rx, gy = g * ry, gz = g * rz;
                     const float vx = vi.x - e.v.x, vy = vi.y - e.v.y, vz = vi.z - e.v.z;
+#pragma unroll
                     for (int k = 0; k < P; ++k) {
                         const float m1 = a.p.mu[k] * (1.f - cd), m2 = a.p.mu[k] * cd;
                         const float ux = m1 * (vk_i[k].x - e.v.x) + m2 * vx;
@@ -254,10 +266,12 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
                     }
                 });
     if (SPLIT) {
+#pragma unroll
         for (int k = 0; k < P; ++k) a.acc_tmp[k][r] = make_float4(acc[k].x, acc[k].y, acc[k].z, 0.f);
         a.normal[r] = make_float4(nx, ny, nz, 0.f);
         return;
     }
+#pragma unroll
     for (int k = 0; k < P; ++k) {
         float4 vk = vk_i[k];
         vk.x = __fmaf_rn(acc[k].x, a.dt, vk.x);
@@ -461,19 +475,22 @@ struct DG {
 // Drift and diffusion volume-fraction exchange (update_phase_change_from_drift_cuda
 // and update_phase_change_from_diffuse_cuda): two walks over the list so that
 // drift terms are accumulated before diffusion terms, as the reference does.
-template <int U>
+template <int U, int PP>
 __global__ void __launch_bounds__(256) k_drift_diffuse(ImmArgs a, int retry) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     if (retry && a.counter[2]) return;   // the retry loop has stopped
-    const int P = a.p.P;
-    float in[kMaxPhases], out[kMaxPhases];
+    constexpr int NP = PP > 0 ? PP : kMaxPhases;
+    const int P = PP > 0 ? PP : a.p.P;
+    float in[NP], out[NP];
+#pragma unroll
     for (int k = 0; k < P; ++k) in[k] = out[k] = 0.f;
     if (a.flag[r] == 0) {
         const float4 p = a.pos[r];
         const float4 vi = a.vel[r];
-        float fi[kMaxPhases];
-        float4 ui[kMaxPhases];
+        float fi[NP];
+        float4 ui[NP];
+#pragma unroll
         for (int k = 0; k < P; ++k) {
             fi[k] = a.frac[k][r];
             const float4 vk = a.vph[k][r];
@@ -493,6 +510,7 @@ __global__ void __launch_bounds__(256) k_drift_diffuse(ImmArgs a, int retry) {
                         const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
                         const float g = cubic_g(dist2(rx, ry, rz), a.k);
                         const float gx = g * rx, gy = g * ry, gz = g * rz;
+#pragma unroll
                         for (int k = 0; k < P; ++k) {
                             const float fj = __ldg(a.frac[k] + j);
                             const float4 vkj = ldg4(a.vph[k] + j);
@@ -518,6 +536,7 @@ __global__ void __launch_bounds__(256) k_drift_diffuse(ImmArgs a, int retry) {
                         const float d2 = dist2(rx, ry, rz);
                         const float g = cubic_g(d2, a.k);
                         const float factor = (g * rx * rx + g * ry * ry + g * rz * rz) / d2;
+#pragma unroll
                         for (int k = 0; k < P; ++k) {
                             const float fij = fi[k] - __ldg(a.frac[k] + j);
                             const float ch = dtcf * fij * e.q.w * factor;
@@ -526,6 +545,7 @@ __global__ void __launch_bounds__(256) k_drift_diffuse(ImmArgs a, int retry) {
                         }
                     });
     }
+#pragma unroll
     for (int k = 0; k < P; ++k) {
         a.fin[k][r] = in[k];
         a.fout[k][r] = out[k];
@@ -898,10 +918,10 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
     a = imm_args(s);
     P_("imm_apply_pressure", [&] { vtp::k_apply_pressure<<<G256, 256, 0, st>>>(a, 0); });
     if (m.have_tension) {
-        P_("imm_vis_normal", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<true, UU><<<G, B, 0, st>>>(a)) });
+        P_("imm_vis_normal", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<true, UU, PP><<<G, B, 0, st>>>(a))) });
         P_("imm_tension", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_tension<UU><<<G, B, 0, st>>>(a)) });
     } else {
-        P_("imm_vis", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<false, UU><<<G, B, 0, st>>>(a)) });
+        P_("imm_vis", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<false, UU, PP><<<G, B, 0, st>>>(a))) });
     }
     s.vel.swap(); s.vadv.swap();
     if (m.p.ct) {
@@ -914,7 +934,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
     P_("imm_apply_pressure", [&] { vtp::k_apply_pressure<<<G256, 256, 0, st>>>(a, 1); });
     // Phase transfer with the negativity retry loop.
     P_("imm_retry_begin", [&] { vtp::k_retry_begin<<<1, 32, 0, st>>>(m.counter); });
-    P_("imm_drift_diffuse", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU><<<G, B, 0, st>>>(a, 0)) });
+    P_("imm_drift_diffuse", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU, PP><<<G, B, 0, st>>>(a, 0))) });
     if (capture && s.device_loop) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t g;
@@ -935,14 +955,14 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
         CUI(cudaStreamBeginCaptureToGraph(s.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         vtp::k_check_negative<<<G256, 256, 0, s.side>>>(a);
         vtp::k_retry_decide<<<1, 32, 0, s.side>>>(a, hnd, 1);
-        VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU><<<G, B, 0, s.side>>>(a, 1))
+        VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU, PP><<<G, B, 0, s.side>>>(a, 1)))
         cudaGraph_t out;
         CUI(cudaStreamEndCapture(s.side, &out));
     } else {
         for (int it = 0; it < 102; ++it) {
             P_("imm_check_negative", [&] { vtp::k_check_negative<<<G256, 256, 0, st>>>(a); });
             P_("imm_retry_decide", [&] { vtp::k_retry_decide<<<1, 32, 0, st>>>(a, cudaGraphConditionalHandle{}, 0); });
-            P_("imm_drift_diffuse", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU><<<G, B, 0, st>>>(a, 1)) });
+            P_("imm_drift_diffuse", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU, PP><<<G, B, 0, st>>>(a, 1))) });
             CUI(cudaMemcpyAsync(s.h_pinned + 5, m.counter + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             CUI(cudaStreamSynchronize(st));
             if (s.h_pinned[5]) break;
