@@ -73,6 +73,10 @@ struct ImmArgs {
     uint32_t *status;
     uint64_t *tick;           // substep counter (per-substep forced iteration schedules)
     int unroll;
+    // IMM-CT: packed rows of the stress-divergence gathers, 4 float4 per fluid row:
+    // {x, V}, then tau_c / rho_rest^2 for c = 0..8 (3 float4, the last 3 floats unused);
+    // written by the conformation-tensor pass, read by the stress-divergence pass.
+    float4 *tpk;
 };
 
 struct ImmState {
@@ -86,6 +90,7 @@ struct ImmState {
     float *rd = nullptr, *cd = nullptr;
     float *fin[kMaxPhases] = {nullptr}, *fout[kMaxPhases] = {nullptr};
     uint32_t *flag = nullptr, *counter = nullptr;
+    float4 *tpk = nullptr;
     std::vector<float> bfrac;        // boundary rows' phase fractions in attach order (host)
     cudaGraphConditionalHandle cond{};
 };
@@ -404,14 +409,25 @@ __global__ void __launch_bounds__(256) k_ct(ImmArgs a) {
     vis = fminf(vis, a.p.vis_max);
     vis = a.p.vis_base + (vis - a.p.vis_base) / (1.f + powf(10.f * shear, 5.f)) *
                              fminf(1.f, f1 / (a.p.theta + 1e-6f));
+    float t[12];
+    const float d = powf(a.rd[r], 2.f);
 #pragma unroll
-    for (int c = 0; c < 9; ++c) a.tau[c][r] = vis * (Q[c] - ((c % 4) == 0 ? 1.f : 0.f));
+    for (int c = 0; c < 9; ++c) {
+        const float tc = vis * (Q[c] - ((c % 4) == 0 ? 1.f : 0.f));
+        a.tau[c][r] = tc;
+        t[c] = tc / d;   // the tau_j / rho_j^2 term of add_phase_pct_acc_cuda, once per row
+    }
+    t[9] = t[10] = t[11] = 0.f;
+    float4 *row = a.tpk + 4 * (size_t)r;
+    row[0] = p;
+    row[1] = make_float4(t[0], t[1], t[2], t[3]);
+    row[2] = make_float4(t[4], t[5], t[6], t[7]);
+    row[3] = make_float4(t[8], t[9], t[10], t[11]);
 }
 
 struct PG {
     float4 q;
-    float rd;
-    float t[9];
+    float t[9];   // tau_j / rho_j^2
 };
 
 // Viscoelastic stress divergence (add_phase_pct_acc_cuda) + phase / mixture velocities.
@@ -432,10 +448,12 @@ __global__ void __launch_bounds__(256) k_pct(ImmArgs a) {
                 [&](uint32_t j) {
                     PG e{};
                     if (j >= a.nf) return e;
-                    e.q = ldg4(a.pos + j);
-                    e.rd = __ldg(a.rd + j);
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) e.t[c] = __ldg(a.tau[c] + j);
+                    // the neighbour's packed row: {x, V}, tau_j / rho_j^2 (two 256-bit loads)
+                    const F4x2 h0 = ldg8(a.tpk + 4 * (size_t)j), h1 = ldg8(a.tpk + 4 * (size_t)j + 2);
+                    e.q = h0.a;
+                    e.t[0] = h0.b.x; e.t[1] = h0.b.y; e.t[2] = h0.b.z; e.t[3] = h0.b.w;
+                    e.t[4] = h1.a.x; e.t[5] = h1.a.y; e.t[6] = h1.a.z; e.t[7] = h1.a.w;
+                    e.t[8] = h1.b.x;
                     return e;
                 },
                 [&](uint32_t j, const PG &e) {
@@ -443,10 +461,9 @@ __global__ void __launch_bounds__(256) k_pct(ImmArgs a) {
                     const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
                     const float g = cubic_g(dist2(rx, ry, rz), a.k);
                     const float w0 = g * rx, w1 = g * ry, w2 = g * rz;
-                    const float dj = powf(e.rd, 2.f);
                     float M[9];
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) M[c] = ti[c] + e.t[c] / dj;
+                    for (int c = 0; c < 9; ++c) M[c] = ti[c] + e.t[c];
                     ax += M[0] * w0 + M[1] * w1 + M[2] * w2;
                     ay += M[3] * w0 + M[4] * w1 + M[5] * w2;
                     az += M[6] * w0 + M[7] * w1 + M[8] * w2;
@@ -736,6 +753,7 @@ int immct_alloc(vtp_solver &s) {
     if ((rc = s.alloc(&m.cd, nf))) return rc;
     if ((rc = s.alloc(&m.flag, nf))) return rc;
     if ((rc = s.alloc(&m.counter, 4))) return rc;
+    if (m.p.ct && (rc = s.alloc(&m.tpk, 4 * (size_t)nf))) return rc;
     CUI(cudaMemsetAsync(m.flag, 0, nf * sizeof(uint32_t), s.st));
     CUI(cudaMemsetAsync(m.counter, 0, 4 * sizeof(uint32_t), s.st));
     return VTP_OK;
@@ -783,6 +801,7 @@ static ImmArgs imm_args(vtp_solver &s) {
     a.status = s.d_status;
     a.tick = s.d_tick;
     a.unroll = s.unroll;
+    a.tpk = m.tpk;
     return a;
 }
 
