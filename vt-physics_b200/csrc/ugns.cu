@@ -48,9 +48,25 @@ __global__ void k_hash(Scenes sc, uint32_t row0, uint32_t cnt, const float4 *__r
         p = apply_force(p, v, force_dt, make_float3(g.grav_x, g.grav_y, g.grav_z));
     }
     int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
-    uint32_t k = g.key_base + (cell_available(c, g) ? cell_key(c, g) : g.nkey);
+    const bool outside = !cell_available(c, g);
+    uint32_t k = g.key_base + (outside ? g.nkey : cell_key(c, g));
     key[i] = k;
-    rank[i] = atomicAdd(&count[k], 1u);
+    const unsigned om = __ballot_sync(__activemask(), outside);
+    if (outside) {
+        // Every row outside its scene's grid counts into the scene's one outside bucket (whole
+        // scenes can leave the box); one atomic per group of lanes with the same bucket keeps
+        // that counter from serialising the kernel.  The order inside the outside bucket is
+        // arbitrary either way: its rows have no neighbours and are nobody's neighbour.
+        const unsigned grp = __match_any_sync(om, k);
+        const unsigned lane = threadIdx.x & 31u;
+        const int leader = __ffs(grp) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(&count[k], (uint32_t)__popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        rank[i] = base + (uint32_t)__popc(grp & ((1u << lane) - 1u));
+    } else {
+        rank[i] = atomicAdd(&count[k], 1u);
+    }
 }
 
 // Block-wide exclusive scan of one value per thread; returns the block total.
