@@ -73,6 +73,10 @@ struct ImmArgs {
     uint32_t *status;
     uint64_t *tick;           // substep counter (per-substep forced iteration schedules)
     int unroll;
+    // Packed gather rows of the viscosity / tension / conformation passes, 2 float4 per
+    // fluid row ({x, V}, then {v, per-row factor} or {n, rest density}): the launch reads
+    // `pk_in` and writes `pk_out` (see immct_enqueue_tick for which pass writes which).
+    float4 *pk_in, *pk_out;
     // IMM-CT: packed rows of the stress-divergence gathers, 4 float4 per fluid row:
     // {x, V}, then tau_c / rho_rest^2 for c = 0..8 (3 float4, the last 3 floats unused);
     // written by the conformation-tensor pass, read by the stress-divergence pass.
@@ -91,6 +95,7 @@ struct ImmState {
     float *fin[kMaxPhases] = {nullptr}, *fout[kMaxPhases] = {nullptr};
     uint32_t *flag = nullptr, *counter = nullptr;
     float4 *tpk = nullptr;
+    float4 *pk2 = nullptr;           // [2 nf] packed gather rows (viscosity -> tension / conformation)
     std::vector<float> bfrac;        // boundary rows' phase fractions in attach order (host)
     cudaGraphConditionalHandle cond{};
 };
@@ -206,6 +211,13 @@ __global__ void k_apply_pressure(ImmArgs a, int update_pos) {
     const float4 o = mix_velocity(a, r, v);
     a.vel[r] = o;
     a.vadv[r] = o;
+    if (!update_pos && a.pk_out) {
+        // rows for the viscosity pass: {x, V}, {v, h m / rho} (the normal's per-neighbour factor,
+        // evaluated as add_phase_acc_vis / compute_surface_normal do per pair)
+        const float4 p = a.pos[r];
+        a.pk_out[2 * (size_t)r] = p;
+        a.pk_out[2 * (size_t)r + 1] = make_float4(o.x, o.y, o.z, a.h * (rd * p.w) / rd);
+    }
     if (update_pos) {
         float4 p = a.pos[r];
         p.x = __fmaf_rn(o.x, a.dt, p.x);
@@ -243,7 +255,8 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
                 [&](uint32_t j) {
                     if (j >= a.nf) return VisG{};
-                    return VisG{ldg4(a.pos + j), ldg4(a.vel + j), SPLIT ? __ldg(a.rd + j) : 0.f};
+                    const F4x2 e = ldg8(a.pk_in + 2 * (size_t)j);   // {x, V}, {v, h m / rho}
+                    return VisG{e.a, e.b, e.b.w};
                 },
                 [&](uint32_t j, const VisG &e) {
                     if (j >= a.nf) return;   // same material, j != i
@@ -264,7 +277,7 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
                         acc[k].z += s * gz / d2;
                     }
                     if (SPLIT) {
-                        const float sn = a.h * (e.rd * e.q.w) / e.rd;   // h m_j / rho_j
+                        const float sn = e.rd;   // h m_j / rho_j, from the packed row
                         nx = __fmaf_rn(sn, gx, nx);
                         ny = __fmaf_rn(sn, gy, ny);
                         nz = __fmaf_rn(sn, gz, nz);
@@ -274,6 +287,9 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
 #pragma unroll
         for (int k = 0; k < P; ++k) a.acc_tmp[k][r] = make_float4(acc[k].x, acc[k].y, acc[k].z, 0.f);
         a.normal[r] = make_float4(nx, ny, nz, 0.f);
+        // rows for the tension pass: {x, V}, {n, rest density}
+        a.pk_out[2 * (size_t)r] = p;
+        a.pk_out[2 * (size_t)r + 1] = make_float4(nx, ny, nz, a.rd[r]);
         return;
     }
 #pragma unroll
@@ -287,6 +303,10 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
     const float4 o = mix_velocity(a, r, vi);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
+    // rows for the conformation pass: {x, V}, {v, m / rho}
+    const float rdr = a.rd[r];
+    a.pk_out[2 * (size_t)r] = p;
+    a.pk_out[2 * (size_t)r + 1] = make_float4(o.x, o.y, o.z, (rdr * p.w) / rdr);
 }
 
 struct TG {
@@ -310,7 +330,8 @@ __global__ void __launch_bounds__(256) k_tension(ImmArgs a) {
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
                 [&](uint32_t j) {
                     if (j >= a.nf) return TG{};
-                    return TG{ldg4(a.pos + j), ldg4(a.normal + j), __ldg(a.rd + j)};
+                    const F4x2 e = ldg8(a.pk_in + 2 * (size_t)j);   // {x, V}, {n, rest density}
+                    return TG{e.a, e.b, e.b.w};
                 },
                 [&](uint32_t j, const TG &e) {
                     if (j >= a.nf) return;
@@ -335,6 +356,9 @@ __global__ void __launch_bounds__(256) k_tension(ImmArgs a) {
     const float4 o = mix_velocity(a, r, vi);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
+    // rows for the conformation pass: {x, V}, {v, m / rho}
+    a.pk_out[2 * (size_t)r] = p;
+    a.pk_out[2 * (size_t)r + 1] = make_float4(o.x, o.y, o.z, (rdi * p.w) / rdi);
 }
 
 struct CG {
@@ -358,14 +382,15 @@ __global__ void __launch_bounds__(256) k_ct(ImmArgs a) {
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0,
                 [&](uint32_t j) {
                     if (j >= a.nf) return CG{};
-                    return CG{ldg4(a.pos + j), ldg4(a.vel + j), __ldg(a.rd + j)};
+                    const F4x2 e = ldg8(a.pk_in + 2 * (size_t)j);   // {x, V}, {v, m / rho}
+                    return CG{e.a, e.b, e.b.w};
                 },
                 [&](uint32_t j, const CG &e) {
                     if (j >= a.nf) return;
                     const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
                     const float g = cubic_g(dist2(rx, ry, rz), a.k);
                     const float w[3] = {g * rx, g * ry, g * rz};
-                    const float vj = (e.rd * e.q.w) / e.rd;   // m_j / rho_j
+                    const float vj = e.rd;   // m_j / rho_j, from the packed row
                     const float d[3] = {e.v.x - vi.x, e.v.y - vi.y, e.v.z - vi.z};
 #pragma unroll
                     for (int row = 0; row < 3; ++row)
@@ -754,6 +779,7 @@ int immct_alloc(vtp_solver &s) {
     if ((rc = s.alloc(&m.flag, nf))) return rc;
     if ((rc = s.alloc(&m.counter, 4))) return rc;
     if (m.p.ct && (rc = s.alloc(&m.tpk, 4 * (size_t)nf))) return rc;
+    if ((rc = s.alloc(&m.pk2, 2 * (size_t)nf))) return rc;
     CUI(cudaMemsetAsync(m.flag, 0, nf * sizeof(uint32_t), s.st));
     CUI(cudaMemsetAsync(m.counter, 0, 4 * sizeof(uint32_t), s.st));
     return VTP_OK;
@@ -934,10 +960,22 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
     P_("imm_rest_density", [&] { vtp::k_rest_density<<<G256, 256, 0, st>>>(a); });
     P_("imm_precompute", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_precompute<UU><<<G, B, 0, st>>>(a)) });
     if ((rc = s.enqueue_solve(st, 0, capture))) return rc;
+    // Packed gather rows between the solves: the pressure apply writes {x, v} rows into the
+    // solver's packed solve rows (free until the next solve re-packs them), the viscosity
+    // pass reads them and writes rows for the tension pass (or, without tension, for the
+    // conformation pass) into m.pk2; the tension pass writes the conformation pass's rows
+    // back into the solve rows.
     a = imm_args(s);
+    a.pk_out = s.pva;
     P_("imm_apply_pressure", [&] { vtp::k_apply_pressure<<<G256, 256, 0, st>>>(a, 0); });
+    a.pk_in = s.pva;
+    a.pk_out = m.pk2;
+    float4 *ct_rows = m.pk2;
     if (m.have_tension) {
         P_("imm_vis_normal", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<true, UU, PP><<<G, B, 0, st>>>(a))) });
+        a.pk_in = m.pk2;
+        a.pk_out = s.pva;
+        ct_rows = s.pva;
         P_("imm_tension", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_tension<UU><<<G, B, 0, st>>>(a)) });
     } else {
         P_("imm_vis", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_vis<false, UU, PP><<<G, B, 0, st>>>(a))) });
@@ -945,6 +983,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
     s.vel.swap(); s.vadv.swap();
     if (m.p.ct) {
         a = imm_args(s);
+        a.pk_in = ct_rows;
         P_("immct_ct", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_ct<UU><<<G, B, 0, st>>>(a)) });
         P_("immct_pct", [&] { VTP_UNROLL_DISPATCH(s.unroll, vtp::k_pct<UU><<<G, B, 0, st>>>(a)) });
     }
