@@ -52,6 +52,11 @@ def scene_for(case: str):
         return scenes.layered_mixture("IMMCT", 24, seed=31)
     if case == "imm_small":
         return scenes.layered_mixture("IMM", 24, seed=32)
+    if case in ("immct_small_notension", "imm_small_notension"):
+        kind = "IMMCT" if case.startswith("immct") else "IMM"
+        sc = scenes.layered_mixture(kind, 24, seed=33 if kind == "IMMCT" else 34)
+        sc.config[kind]["Required"]["surfaceTensionCoefficient"] = 0.0
+        return sc
     raise KeyError(case)
 
 
@@ -64,6 +69,8 @@ CASES = {
     "dfsph_1m_ugns": ([0], False),
     "immct_small": ([0, 1, 2, 5], False),
     "imm_small": ([0, 1, 2, 5], False),
+    "immct_small_notension": ([0, 1, 2, 5], False),
+    "imm_small_notension": ([0, 1, 2, 5], False),
 }
 
 

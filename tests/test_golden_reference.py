@@ -21,7 +21,7 @@ from util import fluid_mask, rel_err
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = ["pbf_small", "pbf_full", "dfsph_small", "dfsph_small_tension"]
-MIX_CASES = ["immct_small", "imm_small"]
+MIX_CASES = ["immct_small", "imm_small", "immct_small_notension", "imm_small_notension"]
 TOL = 1e-5
 
 
