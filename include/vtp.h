@@ -92,6 +92,7 @@ typedef struct vtp_stats {
     uint32_t dead_particles;      /* fluid particles outside the grid (last substep) */
     uint32_t phase_retries;       /* IMM-CT phase-transfer retries (last substep) */
     uint32_t status_bits;         /* device status word, bit (1<<vtp_status) per event */
+    float last_dt;                /* time step of the last substep (the adaptive one with "cfl") */
 } vtp_stats;
 
 typedef struct vtp_solver vtp_solver;
@@ -125,6 +126,10 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       PBFCudaImpl.cu:70-194) or "standard" (poly6 density, spiky gradient,
  *       mass-weighted constraint gradients); "pbfEpsilon": the relaxation
  *       added to the lambda denominator (default 1e-6 / 100);
+ *   "cfl": DFSPH, single scene: an adaptive time step per substep,
+ *       dt = min(timeStep, cfl * 2 particleRadius / max |v_fluid|) (timeStep
+ *       when the fluid is at rest), computed on the device; 0 (default) keeps
+ *       the reference's fixed timeStep (DFSPHSolver.cpp:43-45);
  *   "cellOrder": "brick" (default) keeps rows in 4x4x4-cell bricks with
  *       Morton order inside (compact neighbourhoods for the gathers) or
  *       "linear" in the reference's linear cell order; lists, exported keys

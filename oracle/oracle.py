@@ -169,6 +169,11 @@ class OracleSolver:
             p.force_inc = force_inc
             p.max_iters = 101
             self.p = p
+            # adaptive step (the library's "cfl" extension): dt = min(timeStep, cfl * 2r / max |v|)
+            self.cfl = float(scene.config.get("B200", {}).get("cfl", 0.0))
+            self.dt_max = np.float32(req["timeStep"])
+            self.diameter = np.float32(2) * np.float32(req["particleRadius"])
+            self.dts = []
             self.rest_density = np.where(self.mat == 0, p.rho0, 0.0).astype(np.float64)
             lib().or_dfsph_init(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), _ptr(self.rest_density),
                                 C.byref(self.grid), C.byref(p))
@@ -190,6 +195,17 @@ class OracleSolver:
                               _ptr(self.vol), C.byref(self.grid), C.byref(self.p), _ptr(self.density),
                               _ptr(self.lam))
             else:
+                if self.cfl > 0:
+                    # the library's formula in FP32 on the fluid velocities of this substep
+                    v = self.vel[self.mat == 0].astype(np.float32)
+                    v2 = (v * v).sum(axis=1, dtype=np.float32)
+                    vmax = np.sqrt(np.float32(v2.max())) if v2.size else np.float32(0)
+                    dt = self.dt_max
+                    if vmax > 0:
+                        dt = max(min(self.dt_max, np.float32(np.float32(self.cfl) * self.diameter) / vmax),
+                                 np.float32(self.dt_max * np.float32(1e-4)))
+                    self.p.dt = float(np.float32(dt))
+                    self.dts.append(self.p.dt)
                 out = OrSolveOut()
                 L.or_dfsph_step(self.n, _ptr(self.mat), _ptr(self.obj), len(self.obj_is_fluid),
                                 _ptr(self.obj_is_fluid), _ptr(self.pos), _ptr(self.vel), _ptr(self.vol),

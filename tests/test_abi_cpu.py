@@ -116,6 +116,15 @@ def test_bad_extension_values_are_rejected():
     assert not s.setConfig(cfg) and "rowLanes" in s.last_error
     cfg["B200"] = {"cellOrder": "hilbert"}
     assert not s.setConfig(cfg) and "cellOrder" in s.last_error
+    cfg["B200"] = {"cfl": 0.4}   # a PBF solver: the adaptive step is a DFSPH extension
+    assert not s.setConfig(cfg) and "DFSPH" in s.last_error
+    d = vtp.DFSPHSolver()
+    dcfg = vtp.scenes.dam_break("DFSPH", 500, seed=1).config
+    dcfg["B200"] = {"cfl": 1.5}
+    assert not d.setConfig(dcfg) and "cfl" in d.last_error
+    dcfg["B200"] = {"cfl": 0.4}
+    assert d.setConfig(dcfg), d.last_error
+    d.destroy()
     s.destroy()
 
 

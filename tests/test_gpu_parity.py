@@ -276,3 +276,60 @@ def test_powf_cube_option_runs_and_stays_close(vtp_gpu, kind):
         out.append(s.get_field("pos"))
         s.destroy()
     assert rel_err(out[0], out[1], 1e-3) < 1e-5
+
+
+def _moving_dam_break(vtp, n=8000, seed=41, speed=6.0):
+    """A DFSPH dam break whose fluid starts at `speed` m/s along x, so the CFL
+    step (0.4 * 0.01 m / 6 m/s = 0.67 ms) is below the 1 ms timeStep cap."""
+    sc = vtp.scenes.dam_break("DFSPH", n, seed=seed)
+    for o in sc.objects:
+        if o.material == 0:
+            o.velocity_start = (speed, 0.0, 0.0)
+    return sc
+
+
+def test_dfsph_adaptive_step_matches_oracle(vtp_gpu, oracle_lib):
+    """"cfl": 0.4 — the step dt = min(timeStep, 0.4 * 2r / max|v|) is computed on
+    the device each substep; positions / velocities and the steps themselves
+    follow the FP64 oracle stepping with the same rule."""
+    vtp = vtp_gpu
+    sc = _moving_dam_break(vtp)
+    sc.config["B200"] = {"cfl": 0.4, "forceDivIterations": 2, "forceIncompIterations": 3}
+    s = vtp.solver_from_scene(sc, extra=sc.config["B200"])
+    o = oracle_lib.OracleSolver(sc, force_div=2, force_inc=3)
+    assert o.cfl == 0.4
+    assert s.initialize()
+    fm = fluid_mask(sc)
+    t = 0.0
+    for step in range(3):
+        assert s.tickNsteps(1), s.last_error
+        o.step(1)
+        st = s.stats()
+        t += o.dts[-1]
+        assert abs(st["last_dt"] - o.dts[-1]) <= 1e-6 * o.dts[-1]
+        assert st["last_dt"] < 0.999e-3
+        ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+        ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+        print(f"adaptive step {step + 1}: dt {st['last_dt']:.6e} (oracle {o.dts[-1]:.6e}) pos {ep:.2e} vel {ev:.2e}")
+        assert ep < TOL and ev < TOL_DFSPH_VEL_FP64
+    assert abs(s.stats()["sim_time"] - t) <= 1e-6 * t
+    s.destroy()
+
+
+def test_dfsph_adaptive_step_is_the_cap_at_rest_and_rejected_for_batches(vtp_gpu):
+    vtp = vtp_gpu
+    sc = vtp.scenes.dam_break("DFSPH", 4000, seed=42)
+    fixed = vtp.solver_from_scene(sc)
+    adapt = vtp.solver_from_scene(sc, extra={"cfl": 0.4})
+    for s in (fixed, adapt):
+        assert s.tickNsteps(3), s.last_error
+    # starting at rest the fluid stays far below 4 m/s: the step is the timeStep cap,
+    # so the trajectory is the fixed-step one bit for bit
+    assert adapt.stats()["last_dt"] == fixed.stats()["last_dt"]
+    assert np.array_equal(adapt.get_field("pos"), fixed.get_field("pos"))
+    fixed.destroy()
+    adapt.destroy()
+    b, _ = vtp.solver_from_scenes([sc, vtp.scenes.dam_break("DFSPH", 3000, seed=43)], {"cfl": 0.4},
+                                  strict=False)
+    assert not b.initialize() and "single scene" in b.last_error
+    b.destroy()

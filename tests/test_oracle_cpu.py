@@ -106,3 +106,22 @@ def test_standard_pbf_keeps_the_fluid_in_the_box(oracle_lib):
     assert (ref.pos[f, 1] < 0).sum() > 5000
     assert (std.pos[f, 1] < 0).sum() < 50
     assert abs(std.density[f].mean() / 1000.0 - 1.0) < 0.02
+
+
+def test_oracle_adaptive_step_follows_the_cfl_rule(oracle_lib):
+    """The oracle's adaptive step (the library's "cfl" extension) is
+    min(timeStep, cfl * 2r / max|v_fluid|) on the substep's velocities."""
+    from vtp import scenes
+    sc = scenes.dam_break("DFSPH", 1500, seed=44)
+    for o in sc.objects:
+        if o.material == 0:
+            o.velocity_start = (6.0, 0.0, 0.0)
+    sc.config["B200"] = {"cfl": 0.4}
+    o = oracle_lib.OracleSolver(sc, force_div=1, force_inc=1)
+    fluid = o.mat == 0
+    for _ in range(2):
+        vmax = float(np.sqrt((o.vel[fluid] ** 2).sum(axis=1).max()))
+        o.step(1)
+        expect = min(1e-3, 0.4 * 0.01 / vmax)
+        assert abs(o.dts[-1] - expect) <= 1e-5 * expect
+    assert o.dts[0] < 1e-3

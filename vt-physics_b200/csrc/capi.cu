@@ -172,6 +172,7 @@ int vtp_solver::parse_config(const json &c) {
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
         block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0; row_lanes = 1;
+        cfl = 0.f;
         cell_order_brick = true;
         pbf_form = 0; pbf_eps = 1e-6f;
         if (c.contains("B200")) {
@@ -194,6 +195,10 @@ int vtp_solver::parse_config(const json &c) {
             block = b.value("blockSize", 128);
             unroll = b.value("unroll", 4);
             persistent_tiles = b.value("persistentTiles", false);
+            cfl = b.value("cfl", 0.f);
+            if (!(cfl >= 0.f && cfl <= 1.f)) return fail(VTP_ERR_CONFIG, "cfl must be in [0, 1] (0: fixed timeStep)");
+            if (cfl > 0.f && type != VTP_SOLVER_DFSPH)
+                return fail(VTP_ERR_CONFIG, "cfl (adaptive time step) is a DFSPH extension");
             const std::string order = b.value("cellOrder", std::string("brick"));
             if (order != "brick" && order != "linear")
                 return fail(VTP_ERR_CONFIG, "cellOrder must be \"brick\" or \"linear\"");
@@ -372,6 +377,7 @@ vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     a.pk = pk;
     a.tick = d_tick;
     a.unroll = unroll;
+    a.dtp = cfl > 0.f ? d_cfl : nullptr;
     return a;
 }
 
@@ -416,6 +422,8 @@ int vtp_solver::initialize() {
     const uint32_t n = (uint32_t)(hpos.size() / 3);
     if (n == 0) return fail(VTP_ERR_STATE, "no particles attached");
     const int S = nscenes();
+    if (cfl > 0.f && S != 1)
+        return fail(VTP_ERR_CONFIG, "cfl (adaptive time step) needs a single scene: batched scenes share one step");
     L.n = n;
     L.nf = 0;
     for (auto &sc : scenes) sc.nf = sc.nb = 0, sc.attach_lo = UINT32_MAX;
@@ -591,6 +599,13 @@ int vtp_solver::initialize() {
         AL(&loop, 2);
         CU(cudaMemsetAsync(loop, 0, 2 * sizeof(vtp::LoopState), st));
         AL(&d_tick, 1);
+        if (cfl > 0.f) {
+            AL(&d_cfl, 2);
+            AL(&d_vmax, 1);
+            const float init[2] = {dt, 0.f};
+            CU(cudaMemcpyAsync(d_cfl, init, sizeof(init), cudaMemcpyHostToDevice, st));
+            CU(cudaMemsetAsync(d_vmax, 0, sizeof(uint32_t), st));
+        }
         CU(cudaMemsetAsync(d_tick, 0, sizeof(uint64_t), st));
         if (!force_seq.empty()) {
             AL(&d_force_seq, force_seq.size());
@@ -780,6 +795,10 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     int rc;
     if (type == VTP_SOLVER_PBF) return enqueue_pbf_substep(s, nullptr);
     if (type != VTP_SOLVER_DFSPH) return immct_enqueue_tick(*this, s, capture);
+    if (cfl > 0.f) {
+        PROF(this, "dfsph_cfl", vtp::dfsph_cfl_step(s, dfsph_args(), cfl, 2.f * radius, dt, d_vmax, d_cfl, d_cfl + 1));
+        launches_per_tick += 2;
+    }
     vtp::Carry carry{};
     carry.nf4 = 1;
     carry.src4[0] = vadv.c();
@@ -903,7 +922,16 @@ int vtp_solver::tick_n(uint32_t n) {
             if ((rc = enqueue_tick(st, false))) return rc;
             launches += launches_per_tick;
         }
-        sim_time += dt;
+        if (cfl > 0.f) {
+            // adaptive step: the simulated time lives on the device; read it when an export needs it
+            if (export_enabled) {
+                CU(cudaMemcpyAsync(h_pinned + 6, d_cfl + 1, sizeof(float), cudaMemcpyDeviceToHost, st));
+                CU(cudaStreamSynchronize(st));
+                std::memcpy(&sim_time, h_pinned + 6, sizeof(float));
+            }
+        } else {
+            sim_time += dt;
+        }
         ++steps_done;
         if ((rc = maybe_export())) return rc;
         if (solves && stop_on_crash) {
@@ -918,6 +946,12 @@ int vtp_solver::tick_n(uint32_t n) {
     CU(cudaStreamSynchronize(st));
     CU(cudaGetLastError());
     CU(cudaEventElapsedTime(&stage_ms[2], ev[0], ev[2]));
+    if (cfl > 0.f) {
+        float dev[2];
+        CU(cudaMemcpy(dev, d_cfl, sizeof(dev), cudaMemcpyDeviceToHost));
+        last_dt = dev[0];
+        sim_time = dev[1];
+    }
     if ((rc = check_status())) return fail(rc, "solver status after tick");
     if (solves) {
         if ((rc = read_solve_states())) return rc;
@@ -935,6 +969,7 @@ int vtp_solver::tick_n(uint32_t n) {
     if (imm) stats.phase_retries = immct_last_retries(*this);
     stats.steps_done = steps_done;
     stats.sim_time = sim_time;
+    stats.last_dt = cfl > 0.f ? last_dt : dt;
     return VTP_OK;
 }
 

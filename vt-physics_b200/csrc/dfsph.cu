@@ -21,6 +21,8 @@
 //   finalize    : apply_pressure_acc + update_pos_cuda (:393-404)
 #include "dfsph.h"
 
+#include <algorithm>
+
 namespace vtp {
 
 namespace {
@@ -55,6 +57,18 @@ __device__ __forceinline__ float4 pressure_applied(float4 v, float4 va, float in
     o.y = __fmaf_rn((va.y - v.y) * inv_dt, dt, v.y);
     o.z = __fmaf_rn((va.z - v.z) * inv_dt, dt, v.z);
     return o;
+}
+
+// Time step of the running substep: the fixed dt, or the adaptive one on the device
+// (1/dt and 1/dt^2 formed as the host forms them for the fixed step).
+struct StepDt {
+    float dt, inv_dt, inv_dt2;
+};
+__device__ __forceinline__ StepDt step_dt(const DfsphArgs &a) {
+    if (!a.dtp) return StepDt{a.dt, a.inv_dt, a.inv_dt2};
+    const float dt = *a.dtp;
+    const float inv = 1.f / dt;
+    return StepDt{dt, inv, inv * inv};
 }
 
 __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_t *__restrict__ bncnt,
@@ -121,6 +135,7 @@ __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
 // scene whose solve has stopped is skipped (block-uniform test).
 template <bool MULTI, int U>
 __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const uint4 tile = a.tiles[t];
         if (a.state[tile.z].stopped) continue;
@@ -139,11 +154,11 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
                             const float g = cubic_g(dist2(rx, ry, rz), a.k);
                             const float dot =
                                 g * (rx * (vi.x - e.b.x) + ry * (vi.y - e.b.y) + rz * (vi.z - e.b.z));
-                            d = __fmaf_rn(dot * e.a.w, a.dt, d);
+                            d = __fmaf_rn(dot * e.a.w, T.dt, d);
                         });
             if (d < 0.f) d = 0.f;
             a.delta[r] = d;
-            const float kap = d / a.alpha[r] * a.inv_dt2 / p.w;
+            const float kap = d / a.alpha[r] * T.inv_dt2 / p.w;
             a.kappa[r] = kap;
             a.pk[r] = make_float4(p.x, p.y, p.z, kap);
             contrib = (double)d;
@@ -164,6 +179,7 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
 
 template <int U>
 __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const uint4 tile = a.tiles[t];
         if (a.state[tile.z].stopped || threadIdx.x >= tile.y) continue;
@@ -173,7 +189,7 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
         const float ki = a.kappa[r];
         const uint32_t n = a.ncnt[r];
         const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
-        const float ci = a.dt * p.w / mi;   // dt V_i / m_i
+        const float ci = T.dt * p.w / mi;   // dt V_i / m_i
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
         // Boundary kappa is 0 (kappa_div zeroed; kappa_incomp never written for boundary); the
         // packed row carries kappa_j for fluid rows (volume vol_f) and V_j for boundary rows.
@@ -199,9 +215,10 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
 // first half still holds x_j from dfsph_solve_pack (positions do not change
 // during the solve).
 __global__ void k_pressure_pack(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
-    a.pva[2 * (size_t)r + 1] = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    a.pva[2 * (size_t)r + 1] = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
 }
 
 __global__ void k_solve_pack(DfsphArgs a, uint32_t n) {
@@ -290,10 +307,11 @@ __global__ void __launch_bounds__(1024) k_solve_end(SolveCtl c, const double *__
 
 template <bool TENSION_SPLIT, int U>
 __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
-    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
     const uint32_t n = a.ncnt[r];
     float ax = 0.f, ay = 0.f, az = 0.f;
     float nx = 0.f, ny = 0.f, nz = 0.f;
@@ -331,19 +349,20 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
         return;
     }
     float4 o = vi;
-    o.x = __fmaf_rn(accx, a.dt, vi.x);
-    o.y = __fmaf_rn(accy, a.dt, vi.y);
-    o.z = __fmaf_rn(accz, a.dt, vi.z);
+    o.x = __fmaf_rn(accx, T.dt, vi.x);
+    o.y = __fmaf_rn(accy, T.dt, vi.y);
+    o.z = __fmaf_rn(accz, T.dt, vi.z);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
 }
 
 template <int U>
 __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
-    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    const float4 vi = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
     const float4 ni = a.normal[r];
     const uint32_t n = a.ncnt[r];
     // Fluid rest densities are equal, so k = 2 rho_i / (rho_i + rho_j) is evaluated once.
@@ -368,25 +387,52 @@ __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
                 });
     const float4 acc = a.acc_tmp[r];
     float4 o = vi;
-    o.x = __fmaf_rn(acc.x + tx, a.dt, vi.x);
-    o.y = __fmaf_rn(acc.y + ty, a.dt, vi.y);
-    o.z = __fmaf_rn(acc.z + tz, a.dt, vi.z);
+    o.x = __fmaf_rn(acc.x + tx, T.dt, vi.x);
+    o.y = __fmaf_rn(acc.y + ty, T.dt, vi.y);
+    o.z = __fmaf_rn(acc.z + tz, T.dt, vi.z);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
 }
 
 __global__ void k_finalize(DfsphArgs a) {
+    const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
-    const float4 v = pressure_applied(a.vel[r], a.vadv[r], a.inv_dt, a.dt);
+    const float4 v = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
     a.vel[r] = v;
     a.vadv[r] = v;
     if (r == 0 && a.tick) *a.tick += 1;
     float4 p = a.pos[r];
-    p.x = __fmaf_rn(v.x, a.dt, p.x);
-    p.y = __fmaf_rn(v.y, a.dt, p.y);
-    p.z = __fmaf_rn(v.z, a.dt, p.z);
+    p.x = __fmaf_rn(v.x, T.dt, p.x);
+    p.y = __fmaf_rn(v.y, T.dt, p.y);
+    p.z = __fmaf_rn(v.z, T.dt, p.z);
     a.pos[r] = p;
+}
+
+// Largest |v|^2 over the fluid rows, folded into *vmax_bits (non-negative floats order like
+// their bit patterns, so an unsigned atomicMax is a float max).
+__global__ void __launch_bounds__(256) k_cfl_max(DfsphArgs a, uint32_t *vmax_bits) {
+    float m = 0.f;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < a.nf; r += gridDim.x * blockDim.x) {
+        const float4 v = a.vel[r];
+        m = fmaxf(m, dist2(v.x, v.y, v.z));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31u) == 0 && m > 0.f) atomicMax(vmax_bits, __float_as_uint(m));
+}
+
+// dt = min(dt_max, cfl * diameter / vmax); the scratch word is cleared for the next substep.
+// A step below dt_max * 1e-4 (velocities that have blown up) is held at that floor.
+__global__ void k_cfl_step(uint32_t *vmax_bits, float cfl, float diameter, float dt_max, float *dtp,
+                           float *sim_time) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const float vmax = sqrtf(__uint_as_float(*vmax_bits));
+    *vmax_bits = 0u;
+    float dt = dt_max;
+    if (vmax > 0.f) dt = fmaxf(fminf(dt_max, cfl * diameter / vmax), dt_max * 1e-4f);
+    *dtp = dt;
+    *sim_time += dt;
 }
 
 inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -439,6 +485,14 @@ void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
 }
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
     k_solve_end<<<c.nscenes, 1024, 0, st>>>(c, partials, status);
+}
+void dfsph_cfl_step(cudaStream_t st, const DfsphArgs &a, float cfl, float diameter, float dt_max,
+                    uint32_t *vmax_bits, float *dtp, float *sim_time) {
+    if (a.nf) {
+        const unsigned g = std::min<unsigned>(nblk(a.nf, 256), 148u * 8u);
+        k_cfl_max<<<g, 256, 0, st>>>(a, vmax_bits);
+    }
+    k_cfl_step<<<1, 32, 0, st>>>(vmax_bits, cfl, diameter, dt_max, dtp, sim_time);
 }
 void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a) {
     if (a.nf) k_pressure_pack<<<nblk(a.nf, 256), 256, 0, st>>>(a);

@@ -66,6 +66,7 @@ struct DfsphArgs {
     // Packed gather rows of the pressure solve (filled by dfsph_solve_pack):
     float4 *pva;                // [2n] row j = {pos_j, v*_j} (32 B): one 256-bit load per pair in solve_a
     float4 *pk;                 // [n] {x, y, z, kappa_j} for fluid rows, {x, y, z, V_j} for boundary rows
+    const float *dtp;           // adaptive time step (CFL) on the device; null: the fixed dt above
 };
 
 struct SolveCtl {
@@ -99,6 +100,11 @@ void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials,
 // divergence solve, before dfsph_viscosity / dfsph_vis_normal).
 void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a);
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
+// Adaptive time step: dt = min(dt_max, cfl * diameter / max |v_fluid|) (dt_max when at rest),
+// written to *dtp, added to the FP32 simulated time *sim_time; vmax_bits is a zeroed scratch
+// word (left zeroed).
+void dfsph_cfl_step(cudaStream_t st, const DfsphArgs &a, float cfl, float diameter, float dt_max,
+                    uint32_t *vmax_bits, float *dtp, float *sim_time);
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_finalize(cudaStream_t st, const DfsphArgs &a);

@@ -626,6 +626,7 @@ int dfsph_op_ready(vtp_solver *s) {
     if (!s) return fail(VTP_ERR_ARG, "null solver");
     if (s->type != VTP_SOLVER_DFSPH) return fail(VTP_ERR_CONFIG, "the pressure-solve operator is a DFSPH operator");
     if (s->nscenes() != 1) return fail(VTP_ERR_CONFIG, "the pressure-solve operator runs a single scene");
+    if (s->cfl > 0.f) return fail(VTP_ERR_CONFIG, "the pressure-solve operator takes the fixed time step (no \"cfl\")");
     return VTP_OK;
 }
 

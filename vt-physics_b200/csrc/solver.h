@@ -77,6 +77,12 @@ struct vtp_solver {
 
     // parsed parameters (same derivations as the reference's setConfig)
     float dt = 0, inv_dt = 0, inv_dt2 = 0, radius = 0, h = 0, rho_f = 0, rho_b = 0, vol0 = 0;
+    // DFSPH adaptive time step (extension "cfl"): dt = min(timeStep, cfl * 2r / max |v|) per
+    // substep on the device; d_cfl = {dt, FP32 simulated time}, d_vmax = scratch word.
+    float cfl = 0.f;
+    float last_dt = 0.f;         // step of the last substep (adaptive or fixed)
+    float *d_cfl = nullptr;
+    uint32_t *d_vmax = nullptr;
     float xsph_k = 0, viscosity = 0, div_thr = 0, incomp_thr = 0, gamma = 0, anim_time = 0;
     float lbx = 0, lby = 0, lbz = 0, sx = 0, sy = 0, sz = 0;
     float3 gravity = make_float3(0.f, -9.8f, 0.f);

@@ -80,7 +80,8 @@ class VtpStats(C.Structure):
                 ("last_incomp_iters", C.c_uint32), ("total_div_iters", C.c_uint64),
                 ("total_incomp_iters", C.c_uint64), ("last_div_residual", C.c_double),
                 ("last_incomp_residual", C.c_double), ("neighbor_overflow", C.c_uint32),
-                ("dead_particles", C.c_uint32), ("phase_retries", C.c_uint32), ("status_bits", C.c_uint32)]
+                ("dead_particles", C.c_uint32), ("phase_retries", C.c_uint32), ("status_bits", C.c_uint32),
+                ("last_dt", C.c_float)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
