@@ -378,6 +378,7 @@ vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     a.tick = d_tick;
     a.unroll = unroll;
     a.dtp = cfl > 0.f ? d_cfl : nullptr;
+    a.vmax_bits = cfl > 0.f ? d_vmax : nullptr;
     return a;
 }
 
@@ -687,6 +688,7 @@ int vtp_solver::initialize() {
     CU(cudaStreamSynchronize(st));
     initialized = true;
     crashed = false;
+    if (cfl > 0.f) vtp::dfsph_cfl_refresh(st, dfsph_args(), d_vmax);
     sim_time = 0.f;
     steps_done = 0;
     out_frames = frames_written = 0;
@@ -796,8 +798,8 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     if (type == VTP_SOLVER_PBF) return enqueue_pbf_substep(s, nullptr);
     if (type != VTP_SOLVER_DFSPH) return immct_enqueue_tick(*this, s, capture);
     if (cfl > 0.f) {
-        PROF(this, "dfsph_cfl", vtp::dfsph_cfl_step(s, dfsph_args(), cfl, 2.f * radius, dt, d_vmax, d_cfl, d_cfl + 1));
-        launches_per_tick += 2;
+        PROF(this, "dfsph_cfl", vtp::dfsph_cfl_step(s, cfl, 2.f * radius, dt, d_vmax, d_cfl, d_cfl + 1));
+        launches_per_tick += 1;
     }
     vtp::Carry carry{};
     carry.nf4 = 1;
@@ -1125,6 +1127,7 @@ int vtp_solver::set_field(int f, const void *host, size_t bytes) {
         DB<float4> &d = f == VTP_FIELD_POS ? pos : vel;
         vtp::gather_orig_to_f4(st, L.nf, tmp, orig.c(), d.c(), 1);
         if (f == VTP_FIELD_VEL && vadv.c()) vtp::gather_orig_to_f4(st, L.nf, tmp, orig.c(), vadv.c(), 1);
+        if (f == VTP_FIELD_VEL && cfl > 0.f) vtp::dfsph_cfl_refresh(st, dfsph_args(), d_vmax);
         e = cudaStreamSynchronize(st);
     }
     if (e != cudaSuccess) return fail(VTP_ERR_CUDA, cudaGetErrorString(e));
@@ -1338,6 +1341,7 @@ int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first, uint32_
         DB<float4> &d = field == VTP_FIELD_POS ? s->pos : s->vel;
         float4 *also = field == VTP_FIELD_VEL && s->vadv.c() ? s->vadv.c() : nullptr;
         vtp::gather_f4_range(s->st, s->L.nf, s->stage, s->orig.c(), first, count, d.c(), also);
+        if (field == VTP_FIELD_VEL && s->cfl > 0.f) vtp::dfsph_cfl_refresh(s->st, s->dfsph_args(), s->d_vmax);
         e = cudaStreamSynchronize(s->st);
     }
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
@@ -1396,6 +1400,7 @@ int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, co
         // Only fluid rows move; boundary rows are static and stay as sorted at initialize.
         vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), first, count, s->pos.c(), s->vel.c(),
                                 s->vadv.c());
+        if (s->cfl > 0.f) vtp::dfsph_cfl_refresh(s->st, s->dfsph_args(), s->d_vmax);
         e = cudaStreamSynchronize(s->st);
     }
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));

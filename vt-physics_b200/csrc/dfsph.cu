@@ -407,6 +407,11 @@ __global__ void k_finalize(DfsphArgs a) {
     p.y = __fmaf_rn(v.y, T.dt, p.y);
     p.z = __fmaf_rn(v.z, T.dt, p.z);
     a.pos[r] = p;
+    if (a.vmax_bits) {   // adaptive step: max |v|^2 of the new velocities for the next substep
+        const unsigned m = __activemask();
+        const uint32_t b = __reduce_max_sync(m, __float_as_uint(dist2(v.x, v.y, v.z)));
+        if ((threadIdx.x & 31u) == (unsigned)(__ffs(m) - 1)) atomicMax(a.vmax_bits, b);
+    }
 }
 
 // Largest |v|^2 over the fluid rows, folded into *vmax_bits (non-negative floats order like
@@ -486,13 +491,16 @@ void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
 void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials, uint32_t *status) {
     k_solve_end<<<c.nscenes, 1024, 0, st>>>(c, partials, status);
 }
-void dfsph_cfl_step(cudaStream_t st, const DfsphArgs &a, float cfl, float diameter, float dt_max,
-                    uint32_t *vmax_bits, float *dtp, float *sim_time) {
+void dfsph_cfl_step(cudaStream_t st, float cfl, float diameter, float dt_max, uint32_t *vmax_bits, float *dtp,
+                    float *sim_time) {
+    k_cfl_step<<<1, 32, 0, st>>>(vmax_bits, cfl, diameter, dt_max, dtp, sim_time);
+}
+void dfsph_cfl_refresh(cudaStream_t st, const DfsphArgs &a, uint32_t *vmax_bits) {
+    cudaMemsetAsync(vmax_bits, 0, sizeof(uint32_t), st);
     if (a.nf) {
         const unsigned g = std::min<unsigned>(nblk(a.nf, 256), 148u * 8u);
         k_cfl_max<<<g, 256, 0, st>>>(a, vmax_bits);
     }
-    k_cfl_step<<<1, 32, 0, st>>>(vmax_bits, cfl, diameter, dt_max, dtp, sim_time);
 }
 void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a) {
     if (a.nf) k_pressure_pack<<<nblk(a.nf, 256), 256, 0, st>>>(a);

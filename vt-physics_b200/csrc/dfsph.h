@@ -67,6 +67,7 @@ struct DfsphArgs {
     float4 *pva;                // [2n] row j = {pos_j, v*_j} (32 B): one 256-bit load per pair in solve_a
     float4 *pk;                 // [n] {x, y, z, kappa_j} for fluid rows, {x, y, z, V_j} for boundary rows
     const float *dtp;           // adaptive time step (CFL) on the device; null: the fixed dt above
+    uint32_t *vmax_bits;        // adaptive step: the finalize pass folds max |v|^2 of the new velocities here
 };
 
 struct SolveCtl {
@@ -101,10 +102,12 @@ void dfsph_solve_end(cudaStream_t st, const SolveCtl &c, const double *partials,
 void dfsph_pressure_pack(cudaStream_t st, const DfsphArgs &a);
 void dfsph_viscosity(cudaStream_t st, const DfsphArgs &a, int block);
 // Adaptive time step: dt = min(dt_max, cfl * diameter / max |v_fluid|) (dt_max when at rest),
-// written to *dtp, added to the FP32 simulated time *sim_time; vmax_bits is a zeroed scratch
-// word (left zeroed).
-void dfsph_cfl_step(cudaStream_t st, const DfsphArgs &a, float cfl, float diameter, float dt_max,
-                    uint32_t *vmax_bits, float *dtp, float *sim_time);
+// written to *dtp and added to the FP32 simulated time *sim_time.  max |v|^2 comes from
+// *vmax_bits, which the previous substep's finalize pass filled (and dfsph_cfl_refresh after
+// initialize or a velocity write from the host); the step zeroes it for the next finalize.
+void dfsph_cfl_step(cudaStream_t st, float cfl, float diameter, float dt_max, uint32_t *vmax_bits, float *dtp,
+                    float *sim_time);
+void dfsph_cfl_refresh(cudaStream_t st, const DfsphArgs &a, uint32_t *vmax_bits);
 void dfsph_vis_normal(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_tension(cudaStream_t st, const DfsphArgs &a, int block);
 void dfsph_finalize(cudaStream_t st, const DfsphArgs &a);
