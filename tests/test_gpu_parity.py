@@ -327,6 +327,13 @@ def test_dfsph_adaptive_step_is_the_cap_at_rest_and_rejected_for_batches(vtp_gpu
     # so the trajectory is the fixed-step one bit for bit
     assert adapt.stats()["last_dt"] == fixed.stats()["last_dt"]
     assert np.array_equal(adapt.get_field("pos"), fixed.get_field("pos"))
+    # velocities written from the host set the next step: all fluid at 8 m/s -> 0.4 * 0.01 / 8
+    v = adapt.get_field("vel")
+    fm = fluid_mask(sc)
+    v[fm] = (8.0, 0.0, 0.0)
+    adapt.set_field("vel", v)
+    assert adapt.tickNsteps(1)
+    assert abs(adapt.stats()["last_dt"] - 0.4 * 0.01 / 8.0) <= 1e-6 * 5e-4
     fixed.destroy()
     adapt.destroy()
     b, _ = vtp.solver_from_scenes([sc, vtp.scenes.dam_break("DFSPH", 3000, seed=43)], {"cfl": 0.4},
