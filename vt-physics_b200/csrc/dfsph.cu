@@ -394,23 +394,32 @@ __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
     a.vadv_alt[r] = o;
 }
 
-__global__ void k_finalize(DfsphArgs a) {
+__global__ void __launch_bounds__(256) k_finalize(DfsphArgs a) {
     const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const float4 v = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
-    a.vel[r] = v;
-    a.vadv[r] = v;
-    if (r == 0 && a.tick) *a.tick += 1;
-    float4 p = a.pos[r];
-    p.x = __fmaf_rn(v.x, T.dt, p.x);
-    p.y = __fmaf_rn(v.y, T.dt, p.y);
-    p.z = __fmaf_rn(v.z, T.dt, p.z);
-    a.pos[r] = p;
+    float v2 = 0.f;
+    if (r < a.nf) {
+        const float4 v = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
+        a.vel[r] = v;
+        a.vadv[r] = v;
+        if (r == 0 && a.tick) *a.tick += 1;
+        float4 p = a.pos[r];
+        p.x = __fmaf_rn(v.x, T.dt, p.x);
+        p.y = __fmaf_rn(v.y, T.dt, p.y);
+        p.z = __fmaf_rn(v.z, T.dt, p.z);
+        a.pos[r] = p;
+        v2 = dist2(v.x, v.y, v.z);
+    }
     if (a.vmax_bits) {   // adaptive step: max |v|^2 of the new velocities for the next substep
-        const unsigned m = __activemask();
-        const uint32_t b = __reduce_max_sync(m, __float_as_uint(dist2(v.x, v.y, v.z)));
-        if ((threadIdx.x & 31u) == (unsigned)(__ffs(m) - 1)) atomicMax(a.vmax_bits, b);
+        __shared__ uint32_t wmax[8];
+        uint32_t b = __reduce_max_sync(0xffffffffu, __float_as_uint(v2));
+        if ((threadIdx.x & 31u) == 0) wmax[threadIdx.x >> 5] = b;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            b = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0u;
+            b = __reduce_max_sync(0xffffffffu, b);
+            if (threadIdx.x == 0 && b) atomicMax(a.vmax_bits, b);   // one atomic per block
+        }
     }
 }
 
