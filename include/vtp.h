@@ -220,6 +220,24 @@ VTP_API int vtp_solver_set_field_range(vtp_solver *s, int field, uint32_t first,
 VTP_API int vtp_host_alloc(size_t bytes, void **ptr);
 VTP_API void vtp_host_free(void *ptr);
 
+/* Scene generation on the device, into caller-owned device memory: the
+ * reference's particle generators (ModelHandler.cpp:43-67 lattice cube,
+ * :124-154 hollow box), with the coordinates its host loops produce, bit for
+ * bit (the cube's per-axis FP32 running sums, the box's lb + r + 2 r i in
+ * double), as n x float[3] in the generators' order.  vtp_generate_cube can
+ * add the SplitMix64 jitter the test scenes use: component c of particle p
+ * draws u_(3p+c+1) from `seed` and moves by (2u - 1) * jitter_amp *
+ * jitter_spacing (double, rounded once); jitter_amp = 0 means none.
+ * *count receives the particle count even when it exceeds `capacity` (then
+ * VTP_ERR_BOUNDS and nothing is written), so a first call with capacity 0
+ * sizes the buffer.  Work is enqueued on `stream` (cudaStream_t; NULL =
+ * default stream) and the call returns without waiting. */
+VTP_API int vtp_generate_cube(float radius, const float lb[3], const float size[3], double jitter_amp,
+                              double jitter_spacing, uint64_t seed, float *d_out, uint32_t capacity,
+                              uint32_t *count, void *stream);
+VTP_API int vtp_generate_box(float radius, const float lb[3], const float size[3], int32_t layers, float *d_out,
+                             uint32_t capacity, uint32_t *count, void *stream);
+
 /* Device self-test of the cubic kernel's outer branch: sph::cubic_value
  * (KernelFunctions.cuh:29) takes (1 - q)^3 by powf; the library takes it by a
  * correctly rounded compensated FP32 product unless the "B200" config key

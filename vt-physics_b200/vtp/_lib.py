@@ -54,6 +54,10 @@ SIGNATURES = {
     "vtp_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "vtp_host_free": (None, [_P]),
     "vtp_selftest_cube": (C.c_int, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "vtp_generate_cube": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_double, C.c_double,
+                                    C.c_uint64, _P, C.c_uint32, C.POINTER(C.c_uint32), _P]),
+    "vtp_generate_box": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, _P,
+                                   C.c_uint32, C.POINTER(C.c_uint32), _P]),
     "vtp_solver_get_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_set_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_get_neighbors": (C.c_int, [_P, _P, _P, C.c_uint32]),
