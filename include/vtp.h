@@ -78,6 +78,19 @@ typedef enum vtp_field {
     VTP_FIELD_DELTA = 17          /* float: last compression-ratio residual field */
 } vtp_field;
 
+/* Conservation and density-error sums of the fluid of one scene (or all),
+ * FP64 on the device. */
+typedef struct vtp_conservation {
+    double fluid_mass;            /* sum of fluid masses (PBF m, DFSPH rho0 V, IMM rest density * V) */
+    double momentum[3];           /* sum m v */
+    double kinetic_energy;        /* sum m |v|^2 / 2 */
+    double mean_density_error;    /* mean of rho / rho0 - 1 (PBF, its clamped density) or of the
+                                     compression ratio - 1 (DFSPH, IMM) of the last substep */
+    uint32_t fluid_particles;
+    uint32_t phases;              /* IMM / IMM-CT: phases reported (at most 8); 0 otherwise */
+    double phase_mass[8];         /* IMM / IMM-CT: sum V alpha_k rho_k per phase */
+} vtp_conservation;
+
 /* Statistics of the most recent vtp_solver_tick_n_steps call. */
 typedef struct vtp_stats {
     uint64_t steps_done;          /* substeps completed since initialize */
@@ -237,6 +250,13 @@ VTP_API int vtp_generate_cube(float radius, const float lb[3], const float size[
                               uint32_t *count, void *stream);
 VTP_API int vtp_generate_box(float radius, const float lb[3], const float size[3], int32_t layers, float *d_out,
                              uint32_t capacity, uint32_t *count, void *stream);
+
+/* Trajectory statistics long runs are judged by (no counterpart call in the
+ * reference, which has no such diagnostics): the FP64 sums of
+ * vtp_conservation over the fluid of scene `scene` (-1: every scene of the
+ * solver), summed on the device in a fixed order, so repeated calls on the
+ * same state agree bit for bit.  Synchronous. */
+VTP_API int vtp_solver_get_conservation(vtp_solver *s, int scene, vtp_conservation *out);
 
 /* Device self-test of the cubic kernel's outer branch: sph::cubic_value
  * (KernelFunctions.cuh:29) takes (1 - q)^3 by powf; the library takes it by a

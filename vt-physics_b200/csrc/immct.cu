@@ -747,6 +747,16 @@ int immct_parse(bool ct, const nlohmann::json &r, std::shared_ptr<ImmState> &imm
 
 int immct_phase_count(const vtp_solver &s) { return s.imm ? s.imm->p.P : 0; }
 
+void immct_conservation_inputs(vtp_solver &s, const float **rd, const float **frac, float *rho_k, int *P) {
+    ImmState &m = *s.imm;
+    *rd = m.rd;
+    *P = std::min(m.p.P, vtp::kConsPhases);
+    for (int k = 0; k < *P; ++k) {
+        frac[k] = m.frac[k].c();
+        rho_k[k] = m.p.rho[k];
+    }
+}
+
 #define CUI(call)                                                                               \
     do {                                                                                        \
         cudaError_t e_ = (call);                                                                \

@@ -28,4 +28,7 @@ void immct_fill_carry(vtp_solver &s, vtp::Carry &carry);
 int immct_copy_back(vtp_solver &s);
 void immct_set_parity(vtp_solver &s, int cur);
 uint32_t immct_last_retries(vtp_solver &s);
+// Inputs of the conservation sums: rest density and phase fractions of the fluid rows, the
+// phase rest densities (up to vtp::kConsPhases phases).
+void immct_conservation_inputs(vtp_solver &s, const float **rd, const float **frac, float *rho_k, int *P);
 void immct_color(vtp_solver &s, const float *frac_attach_order, float *rgb);

@@ -9,6 +9,8 @@
 
 namespace vtp {
 
+constexpr int kConsPhases = 8;   // phases the conservation sums report (vtp_conservation.phase_mass)
+
 // Particles are kept sorted: fluid rows [0, nf) re-sorted by (cell, attach id)
 // every substep, boundary rows [nf, n) sorted once at initialize.
 struct Layout {

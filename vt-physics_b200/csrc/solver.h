@@ -79,6 +79,8 @@ struct vtp_solver {
     float dt = 0, inv_dt = 0, inv_dt2 = 0, radius = 0, h = 0, rho_f = 0, rho_b = 0, vol0 = 0;
     // DFSPH adaptive time step (extension "cfl"): dt = min(timeStep, cfl * 2r / max |v|) per
     // substep on the device; d_cfl = {dt, FP32 simulated time}, d_vmax = scratch word.
+    double *d_cons = nullptr;       // conservation sums: totals + per-block partials
+    uint32_t cons_blocks = 0;
     float cfl = 0.f;
     float last_dt = 0.f;         // step of the last substep (adaptive or fixed)
     float *d_cfl = nullptr;
@@ -174,6 +176,7 @@ struct vtp_solver {
         for (void *a : allocs) cudaFree(a);
         allocs.clear();
         if (stage) cudaFree(stage), stage = nullptr, stage_bytes = 0;
+        if (d_cons) cudaFree(d_cons), d_cons = nullptr, cons_blocks = 0;
         if (h_pinned) cudaFreeHost(h_pinned), h_pinned = nullptr;
         for (auto &e : ev)
             if (e) cudaEventDestroy(e), e = nullptr;
@@ -216,6 +219,7 @@ struct vtp_solver {
     int read_solve_states();
     int export_frame();
     int maybe_export();
+    int conservation(int scene, vtp_conservation *out);   // conserve.cu
     int sync_parity();
 };
 

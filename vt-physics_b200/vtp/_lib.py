@@ -54,6 +54,7 @@ SIGNATURES = {
     "vtp_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "vtp_host_free": (None, [_P]),
     "vtp_selftest_cube": (C.c_int, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "vtp_solver_get_conservation": (C.c_int, [_P, C.c_int, _P]),
     "vtp_generate_cube": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_double, C.c_double,
                                     C.c_uint64, _P, C.c_uint32, C.POINTER(C.c_uint32), _P]),
     "vtp_generate_box": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, _P,
@@ -89,6 +90,17 @@ class VtpStats(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VtpConservation(C.Structure):
+    _fields_ = [("fluid_mass", C.c_double), ("momentum", C.c_double * 3), ("kinetic_energy", C.c_double),
+                ("mean_density_error", C.c_double), ("fluid_particles", C.c_uint32), ("phases", C.c_uint32),
+                ("phase_mass", C.c_double * 8)]
+
+    def as_dict(self) -> dict:
+        return {"fluid_mass": self.fluid_mass, "momentum": list(self.momentum),
+                "kinetic_energy": self.kinetic_energy, "mean_density_error": self.mean_density_error,
+                "fluid_particles": self.fluid_particles, "phase_mass": list(self.phase_mass[: self.phases])}
 
 
 class VtpError(RuntimeError):

@@ -16,7 +16,7 @@ from typing import Iterable
 import numpy as np
 
 from . import scenes
-from ._lib import FIELDS, SOLVER_TYPES, VtpError, VtpKernelTime, VtpStats, check, lib
+from ._lib import FIELDS, SOLVER_TYPES, VtpConservation, VtpError, VtpKernelTime, VtpStats, check, lib
 
 PBF, DFSPH, IMM, IMMCT = 0, 1, 2, 3
 EPM_FLUID, EPM_BOUNDARY = 0, 1
@@ -241,6 +241,13 @@ class Solver:
         s = VtpStats()
         check(lib().vtp_solver_get_stats(self._h, C.byref(s)), "get_stats")
         return s.as_dict()
+
+    def conservation(self, scene: int = -1) -> dict:
+        """FP64 device sums of the fluid: mass, momentum, kinetic energy, mean density
+        error and (IMM / IMM-CT) per-phase mass, of one scene or (-1) all."""
+        c = VtpConservation()
+        check(lib().vtp_solver_get_conservation(self._h, int(scene), C.byref(c)), "get_conservation")
+        return c.as_dict()
 
     def scene_stats(self, scene: int) -> dict:
         s = VtpStats()
