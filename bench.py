@@ -748,6 +748,7 @@ def main():
     npass = neighbor_pass(sc.solver, prof, args.profile_steps, nf, K, k_mean, peak, peak_kind)
 
     l2 = l2_note(s, req)
+    cons = s.conservation()
     s.destroy()
 
     # e2e through the public API, over the same substeps as the timed run (a fresh solver of
@@ -780,6 +781,7 @@ def main():
                    "dt": req["timeStep"], "dt_last": st.get("last_dt"), "parallelism": f"replicas{world}",
                    "div_iters_total": st["total_div_iters"], "incomp_iters_total": st["total_incomp_iters"],
                    "mean_neighbors": round(k_mean, 2),
+                   "mean_density_error": cons["mean_density_error"],
                    "l2": l2,
                    "b200": extra,
                    "wall_ms_per_step": 1e3 * wall / args.steps},
