@@ -346,27 +346,57 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
 // the row's lanes gives each lane its first slot, pass 2 walks again and
 // writes.  The concatenation is the one-thread walk's list, truncation at
 // maxNbr included, so both builders write identical lists.
-template <bool WRITE>
+// Passes of the lane-split walk: kCount tests every candidate, counts the
+// accepted ones and records which were accepted (one bit per candidate, for a
+// lane's first 64 candidates); kReplay writes the accepted candidates from
+// those bits without loading a position again; kWrite tests and writes (for a
+// lane with more than 64 candidates).
+enum SplitPass { kCount = 0, kReplay = 1, kWrite = 2 };
+
+template <int PASS>
 struct SplitSink {
     float px, py, pz;
     uint32_t n;       // candidates accepted by this lane so far
     uint32_t base;    // this lane's first slot
     uint32_t cap;     // list slots per row (maxNbr - 1)
     uint32_t *out;    // ELL base of the row
+    uint64_t bits;    // accepted candidates among the lane's first 64 (kCount writes, kReplay reads)
+    uint32_t idx;     // candidates seen
+
+    __device__ __forceinline__ void put(uint32_t j) {
+        const uint32_t slot = base + n;
+        if (slot < cap) out[(size_t)slot * 32u] = j;
+    }
 
     __device__ __forceinline__ void take(uint32_t j, const float4 &q, float d2max) {
         const float d2 = dist2(px - q.x, py - q.y, pz - q.z);
         if (d2 > 0.f && d2 <= d2max) {
-            if (WRITE) {
-                const uint32_t slot = base + n;
-                if (slot < cap) out[(size_t)slot * 32u] = j;
-            }
+            if (PASS == kCount && idx < 64) bits |= 1ull << idx;
+            if (PASS == kWrite) put(j);
             ++n;
+        }
+        ++idx;
+    }
+
+    // One candidate in walk order: tested (kCount, kWrite) or replayed from the bits.
+    __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
+        if (PASS == kReplay) {
+            if ((bits >> idx) & 1ull) {
+                put(j);
+                ++n;
+            }
+            ++idx;
+        } else {
+            take(j, __ldg(pos + j), d2max);
         }
     }
 
     __device__ __forceinline__ void run(uint32_t j0, uint32_t j1, const float4 *__restrict__ pos, float d2max) {
         uint32_t j = j0;
+        if (PASS == kReplay) {
+            for (; j < j1; ++j) visit(j, pos, d2max);
+            return;
+        }
         for (; j + 4 <= j1; j += 4) {
             const float4 q0 = __ldg(pos + j), q1 = __ldg(pos + j + 1), q2 = __ldg(pos + j + 2),
                          q3 = __ldg(pos + j + 3);
@@ -379,8 +409,8 @@ struct SplitSink {
     }
 };
 
-template <int MODE, bool WRITE>
-__device__ __forceinline__ void split_walk(SplitSink<WRITE> &k, int3 c, const SceneGrid &g, int t0, int t1,
+template <int MODE, int PASS>
+__device__ __forceinline__ void split_walk(SplitSink<PASS> &k, int3 c, const SceneGrid &g, int t0, int t1,
                                            const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
                                            const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
                                            float d2max) {
@@ -404,7 +434,7 @@ __device__ __forceinline__ void split_walk(SplitSink<WRITE> &k, int3 c, const Sc
                 if (b0 >= b1) j = f0++;
                 else if (f0 >= f1) j = b0++;
                 else j = (__ldg(orig + f0) < __ldg(orig + b0)) ? f0++ : b0++;
-                k.take(j, __ldg(pos + j), d2max);
+                k.visit(j, pos, d2max);
             }
         }
     }
@@ -433,7 +463,7 @@ __global__ void __launch_bounds__(256) k_build_lists_split(
     }
     const int t0 = 27 * lane / L, t1 = 27 * (lane + 1) / L;
     const float d2max = sc.d2max;
-    SplitSink<false> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, nullptr};
+    SplitSink<kCount> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, nullptr, 0ull, 0u};
     split_walk<MODE>(cnt1, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
     uint32_t x = cnt1.n;
 #pragma unroll
@@ -443,8 +473,17 @@ __global__ void __launch_bounds__(256) k_build_lists_split(
     }
     const uint32_t total = __shfl_sync(gmask, x, L - 1, L);
     const uint32_t cap = sc.maxnbr - 1u;
-    SplitSink<true> wr{p.x, p.y, p.z, 0u, x - cnt1.n, cap, nbr + ell_index(r, 0, ell_stride)};
-    if (wr.base < cap) split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+    uint32_t *const out = nbr + ell_index(r, 0, ell_stride);
+    const uint32_t base = x - cnt1.n;
+    if (base < cap && cnt1.n > 0) {
+        if (cnt1.idx <= 64) {   // the accepted candidates are known: write them without a second test
+            SplitSink<kReplay> wr{p.x, p.y, p.z, 0u, base, cap, out, cnt1.bits, 0u};
+            split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+        } else {
+            SplitSink<kWrite> wr{p.x, p.y, p.z, 0u, base, cap, out, 0ull, 0u};
+            split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+        }
+    }
     if (lane == 0) {
         ncnt[r] = total < cap ? total + 1u : sc.maxnbr;
         if (total > cap) {
