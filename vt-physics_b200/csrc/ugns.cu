@@ -347,56 +347,40 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
 // writes.  The concatenation is the one-thread walk's list, truncation at
 // maxNbr included, so both builders write identical lists.
 // Passes of the lane-split walk: kCount tests every candidate, counts the
-// accepted ones and records which were accepted (one bit per candidate, for a
-// lane's first 64 candidates); kReplay writes the accepted candidates from
-// those bits without loading a position again; kWrite tests and writes (for a
-// lane with more than 64 candidates).
-enum SplitPass { kCount = 0, kReplay = 1, kWrite = 2 };
+// accepted ones and keeps the first kSplitKeep of them in the block's shared
+// buffer; kWrite tests again and writes every accepted candidate into its
+// slot (only for a lane that accepted more than kSplitKeep).
+enum SplitPass { kCount = 0, kWrite = 1 };
+constexpr int kSplitBlock = 256;   // threads per block of the lane-split builder
+constexpr uint32_t kSplitKeep = 16; // accepted candidates a lane keeps for the copy-out
 
 template <int PASS>
 struct SplitSink {
     float px, py, pz;
     uint32_t n;       // candidates accepted by this lane so far
-    uint32_t base;    // this lane's first slot
+    uint32_t base;    // kWrite: this lane's first slot
     uint32_t cap;     // list slots per row (maxNbr - 1)
-    uint32_t *out;    // ELL base of the row
-    uint64_t bits;    // accepted candidates among the lane's first 64 (kCount writes, kReplay reads)
-    uint32_t idx;     // candidates seen
-
-    __device__ __forceinline__ void put(uint32_t j) {
-        const uint32_t slot = base + n;
-        if (slot < cap) out[(size_t)slot * 32u] = j;
-    }
+    uint32_t *out;    // kCount: this thread's column of the shared buffer (stride kSplitBlock); kWrite: ELL row
 
     __device__ __forceinline__ void take(uint32_t j, const float4 &q, float d2max) {
         const float d2 = dist2(px - q.x, py - q.y, pz - q.z);
         if (d2 > 0.f && d2 <= d2max) {
-            if (PASS == kCount && idx < 64) bits |= 1ull << idx;
-            if (PASS == kWrite) put(j);
+            if (PASS == kCount) {
+                if (n < kSplitKeep) out[n * kSplitBlock] = j;
+            } else {
+                const uint32_t slot = base + n;
+                if (slot < cap) out[(size_t)slot * 32u] = j;
+            }
             ++n;
         }
-        ++idx;
     }
 
-    // One candidate in walk order: tested (kCount, kWrite) or replayed from the bits.
     __device__ __forceinline__ void visit(uint32_t j, const float4 *__restrict__ pos, float d2max) {
-        if (PASS == kReplay) {
-            if ((bits >> idx) & 1ull) {
-                put(j);
-                ++n;
-            }
-            ++idx;
-        } else {
-            take(j, __ldg(pos + j), d2max);
-        }
+        take(j, __ldg(pos + j), d2max);
     }
 
     __device__ __forceinline__ void run(uint32_t j0, uint32_t j1, const float4 *__restrict__ pos, float d2max) {
         uint32_t j = j0;
-        if (PASS == kReplay) {
-            for (; j < j1; ++j) visit(j, pos, d2max);
-            return;
-        }
         for (; j + 4 <= j1; j += 4) {
             const float4 q0 = __ldg(pos + j), q1 = __ldg(pos + j + 1), q2 = __ldg(pos + j + 2),
                          q3 = __ldg(pos + j + 3);
@@ -441,12 +425,15 @@ __device__ __forceinline__ void split_walk(SplitSink<PASS> &k, int3 c, const Sce
 }
 
 template <int MODE, int L>
-__global__ void __launch_bounds__(256) k_build_lists_split(
+__global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
     Scenes sc, uint32_t row0, uint32_t cnt, uint32_t ell_stride, const float4 *__restrict__ pos,
     const uint32_t *__restrict__ orig, const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
     uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt, uint32_t *__restrict__ status,
     uint32_t *__restrict__ overflow_count) {
     static_assert(L >= 2 && L <= 16 && (L & (L - 1)) == 0, "L divides the warp");
+    // Accepted candidates of each thread, [kSplitKeep][kSplitBlock] (a thread's column is strided, so
+    // a warp's stores and loads of entry k fall in 32 consecutive words).
+    __shared__ uint32_t keep[kSplitKeep * kSplitBlock];
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
@@ -463,7 +450,7 @@ __global__ void __launch_bounds__(256) k_build_lists_split(
     }
     const int t0 = 27 * lane / L, t1 = 27 * (lane + 1) / L;
     const float d2max = sc.d2max;
-    SplitSink<kCount> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, nullptr, 0ull, 0u};
+    SplitSink<kCount> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, keep + threadIdx.x};
     split_walk<MODE>(cnt1, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
     uint32_t x = cnt1.n;
 #pragma unroll
@@ -476,11 +463,11 @@ __global__ void __launch_bounds__(256) k_build_lists_split(
     uint32_t *const out = nbr + ell_index(r, 0, ell_stride);
     const uint32_t base = x - cnt1.n;
     if (base < cap && cnt1.n > 0) {
-        if (cnt1.idx <= 64) {   // the accepted candidates are known: write them without a second test
-            SplitSink<kReplay> wr{p.x, p.y, p.z, 0u, base, cap, out, cnt1.bits, 0u};
-            split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+        if (cnt1.n <= kSplitKeep) {   // the lane's accepted candidates are in shared memory
+            const uint32_t m = min(cnt1.n, cap - base);
+            for (uint32_t k = 0; k < m; ++k) out[(size_t)(base + k) * 32u] = keep[k * kSplitBlock + threadIdx.x];
         } else {
-            SplitSink<kWrite> wr{p.x, p.y, p.z, 0u, base, cap, out, 0ull, 0u};
+            SplitSink<kWrite> wr{p.x, p.y, p.z, 0u, base, cap, out};
             split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
         }
     }
@@ -727,18 +714,18 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
     const bool split = L.list_lanes == 8 || (L.list_lanes == 0 && cnt <= kSplitRows);
     if (split) {
         constexpr int S = 8;
-        const unsigned ns = nblk(cnt * S, 256);
+        const unsigned ns = nblk(cnt * S, kSplitBlock);
         switch (L.merge_mode) {
             case 0:
-                k_build_lists_split<0, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                k_build_lists_split<0, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
             case 1:
-                k_build_lists_split<1, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                k_build_lists_split<1, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
             default:
-                k_build_lists_split<2, S><<<ns, 256, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                k_build_lists_split<2, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
         }
