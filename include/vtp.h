@@ -157,6 +157,11 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       kernel's outer branch correctly rounded, at most one ulp from the
  *       reference's powf(1 - q, 3) (KernelFunctions.cuh:29); "powf" calls powf
  *       as the reference does, for bit-identical W at a higher cost;
+ *   "phaseRetry": IMM / IMM-CT phase-transfer retries (IMMCTCudaImpl.cu:
+ *       1065-1137): "nearFlagged" (default) recomputes only the particles
+ *       that were just flagged negative or have such a fluid neighbour, the
+ *       only ones whose changes a retry alters; "all" recomputes every
+ *       particle as the reference does; both give the same results;
  *   "stageTimers": true records CUDA-event stage times. */
 VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 

@@ -114,6 +114,8 @@ def test_bad_extension_values_are_rejected():
     assert not s.setConfig(cfg) and "listLanes" in s.last_error
     cfg["B200"] = {"rowLanes": 2}
     assert not s.setConfig(cfg) and "rowLanes" in s.last_error
+    cfg["B200"] = {"phaseRetry": "some"}
+    assert not s.setConfig(cfg) and "phaseRetry" in s.last_error
     cfg["B200"] = {"cellOrder": "hilbert"}
     assert not s.setConfig(cfg) and "cellOrder" in s.last_error
     cfg["B200"] = {"cfl": 0.4}   # a PBF solver: the adaptive step is a DFSPH extension

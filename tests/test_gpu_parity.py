@@ -215,6 +215,28 @@ def test_cell_orders_give_identical_trajectories(vtp_gpu, kind):
         assert out[0][2]["total_div_iters"] == out[1][2]["total_div_iters"]
 
 
+@pytest.mark.parametrize("kind", ["IMMCT", "IMM"])
+def test_phase_retries_near_flags_match_full_retries(vtp_gpu, kind):
+    """Phase-transfer retries (IMMCTCudaImpl.cu:1065-1137) that recompute only
+    the rows next to newly flagged particles give the trajectories of retries
+    that recompute every row, bit for bit; the scenes run the retry loop."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.immct_500k() if kind == "IMMCT" else vtp.scenes.layered_mixture("IMM", 64, seed=5)
+    out = []
+    for mode in ("nearFlagged", "all"):
+        s = vtp.solver_from_scene(sc, extra={"phaseRetry": mode})
+        retries = []
+        for _ in range(40):
+            assert s.tickNsteps(1), s.last_error
+            retries.append(s.stats()["phase_retries"])
+        out.append((retries, s.get_field("pos"), s.get_field("vel"), s.get_field("vol_frac")))
+        s.destroy()
+    print(kind, "retries per substep", out[0][0])
+    assert out[0][0] == out[1][0] and sum(out[0][0]) > 0, (out[0][0], out[1][0])
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
+
+
 def test_runs_are_deterministic(vtp_gpu):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()

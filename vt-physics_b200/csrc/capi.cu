@@ -213,6 +213,10 @@ int vtp_solver::parse_config(const json &c) {
             if (cube != "rounded" && cube != "powf")
                 return fail(VTP_ERR_CONFIG, "cubicCube must be \"rounded\" or \"powf\"");
             cube_powf = cube == "powf";
+            const std::string retry = b.value("phaseRetry", std::string("nearFlagged"));
+            if (retry != "nearFlagged" && retry != "all")
+                return fail(VTP_ERR_CONFIG, "phaseRetry must be \"nearFlagged\" or \"all\"");
+            phase_retry_all = retry == "all";
             const std::string form = b.value("pbfFormulation", std::string("reference"));
             if (form != "reference" && form != "standard")
                 return fail(VTP_ERR_CONFIG, "pbfFormulation must be \"reference\" or \"standard\"");

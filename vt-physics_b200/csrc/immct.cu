@@ -69,7 +69,9 @@ struct ImmArgs {
     float *ratio, *alpha;
     float *fin[kMaxPhases], *fout[kMaxPhases];
     uint32_t *flag;
-    uint32_t *counter;        // [0] newly flagged, [1] retry iteration, [2] stop
+    uint32_t *counter;        // [0] newly flagged, [1] retry iteration, [2] stop, [3] retries, [4] work rows
+    uint32_t *work;           // rows the running retry recomputes (k_drift_mark)
+    int retry_all;            // phase-transfer retries recompute every row (1) or rows near new flags (0)
     uint32_t *status;
     uint64_t *tick;           // substep counter (per-substep forced iteration schedules)
     int unroll;
@@ -94,6 +96,7 @@ struct ImmState {
     float *rd = nullptr, *cd = nullptr;
     float *fin[kMaxPhases] = {nullptr}, *fout[kMaxPhases] = {nullptr};
     uint32_t *flag = nullptr, *counter = nullptr;
+    uint32_t *work = nullptr;        // [nf] rows a phase-transfer retry recomputes
     float4 *tpk = nullptr;
     float4 *pk2 = nullptr;           // [2 nf] packed gather rows (viscosity -> tension / conformation)
     std::vector<float> bfrac;        // boundary rows' phase fractions in attach order (host)
@@ -514,14 +517,57 @@ struct DG {
     uint32_t flag;
 };
 
+// Rows a phase-transfer retry has to recompute.  Between passes only the flags
+// change (fractions, phase velocities and positions are fixed until
+// k_phase_finish), and a pair is skipped when either side is flagged, so a
+// pass changes a row's result only when the row or one of its fluid
+// neighbours was flagged by the check just before it (flag == that check's
+// number); every other row would recompute the values it holds, bit for bit.
+// Those rows are appended to `work` (one atomic per warp; the order does not
+// matter, each row's result depends on its own list only).
+__global__ void __launch_bounds__(256) k_drift_mark(ImmArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.counter[2]) return;   // the retry loop has stopped
+    const uint32_t gen = a.counter[1] - 1u;
+    bool redo = false;
+    if (r < a.nf) {
+        const uint32_t fr = a.flag[r];
+        redo = fr == gen;
+        if (fr == 0) {
+            const uint32_t n = a.ncnt[r];
+            const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+            for (uint32_t t = 0; t + 1 < n && !redo; ++t) {
+                const uint32_t j = lst[(size_t)t * 32u];
+                redo = j < a.nf && __ldg(a.flag + j) == gen;
+            }
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, redo);
+    if (m == 0) return;
+    const int lane = (int)(threadIdx.x & 31u);
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&a.counter[4], (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);   // every lane of the warp is here
+    if (redo) a.work[base + (uint32_t)__popc(m & ((1u << lane) - 1u))] = r;
+}
+
 // Drift and diffusion volume-fraction exchange (update_phase_change_from_drift_cuda
-// and update_phase_change_from_diffuse_cuda): two walks over the list so that
-// drift terms are accumulated before diffusion terms, as the reference does.
+// and update_phase_change_from_diffuse_cuda, IMMCTCudaImpl.cu:541-614): two walks
+// over the list so that drift terms are accumulated before diffusion terms, as
+// the reference does.  Every fluid row on the first pass of a substep; on a
+// retry every row ("phaseRetry": "all") or the rows k_drift_mark listed.
 template <int U, int PP>
 __global__ void __launch_bounds__(256) k_drift_diffuse(ImmArgs a, int retry) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (retry) {
+        if (a.counter[2]) return;   // the retry loop has stopped
+        if (!a.retry_all) {
+            if (r >= a.counter[4]) return;
+            r = a.work[r];
+        }
+    }
     if (r >= a.nf) return;
-    if (retry && a.counter[2]) return;   // the retry loop has stopped
     constexpr int NP = PP > 0 ? PP : kMaxPhases;
     const int P = PP > 0 ? PP : a.p.P;
     float in[NP], out[NP];
@@ -603,7 +649,7 @@ __global__ void k_check_negative(ImmArgs a) {
     for (int k = 0; k < a.p.P; ++k)
         if (a.frac[k][r] + a.fout[k][r] + a.fin[k][r] < 0.f) neg = true;
     if (neg) {
-        a.flag[r] = 1;
+        a.flag[r] = a.counter[1];   // the check's number (>= 1): the next pass recomputes around it
         atomicAdd(&a.counter[0], 1u);
     }
 }
@@ -625,6 +671,7 @@ __global__ void k_retry_decide(ImmArgs a, cudaGraphConditionalHandle h, int use_
         }
     }
     c[0] = 0;
+    c[4] = 0;
     if (use_cond) cudaGraphSetConditional(h, c[2] ? 0u : 1u);
 }
 
@@ -787,11 +834,12 @@ int immct_alloc(vtp_solver &s) {
     if ((rc = s.alloc(&m.rd, nf))) return rc;
     if ((rc = s.alloc(&m.cd, nf))) return rc;
     if ((rc = s.alloc(&m.flag, nf))) return rc;
-    if ((rc = s.alloc(&m.counter, 4))) return rc;
+    if ((rc = s.alloc(&m.counter, 5))) return rc;
+    if ((rc = s.alloc(&m.work, nf))) return rc;
     if (m.p.ct && (rc = s.alloc(&m.tpk, 4 * (size_t)nf))) return rc;
     if ((rc = s.alloc(&m.pk2, 2 * (size_t)nf))) return rc;
     CUI(cudaMemsetAsync(m.flag, 0, nf * sizeof(uint32_t), s.st));
-    CUI(cudaMemsetAsync(m.counter, 0, 4 * sizeof(uint32_t), s.st));
+    CUI(cudaMemsetAsync(m.counter, 0, 5 * sizeof(uint32_t), s.st));
     return VTP_OK;
 }
 
@@ -802,6 +850,7 @@ static ImmArgs imm_args(vtp_solver &s) {
     a.ell_stride = s.L.ell_stride;
     a.k = s.kc;
     a.p = m.p;
+    a.retry_all = s.phase_retry_all ? 1 : 0;
     a.dt = s.dt;
     a.inv_dt = s.inv_dt;
     a.h = s.h;
@@ -834,6 +883,7 @@ static ImmArgs imm_args(vtp_solver &s) {
     a.alpha = s.alpha;
     a.flag = m.flag;
     a.counter = m.counter;
+    a.work = m.work;
     a.status = s.d_status;
     a.tick = s.d_tick;
     a.unroll = s.unroll;
@@ -1023,6 +1073,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
         CUI(cudaStreamBeginCaptureToGraph(s.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         vtp::k_check_negative<<<G256, 256, 0, s.side>>>(a);
         vtp::k_retry_decide<<<1, 32, 0, s.side>>>(a, hnd, 1);
+        if (!s.phase_retry_all) vtp::k_drift_mark<<<G256, 256, 0, s.side>>>(a);
         VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU, PP><<<G, B, 0, s.side>>>(a, 1)))
         cudaGraph_t out;
         CUI(cudaStreamEndCapture(s.side, &out));
@@ -1030,6 +1081,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
         for (int it = 0; it < 102; ++it) {
             P_("imm_check_negative", [&] { vtp::k_check_negative<<<G256, 256, 0, st>>>(a); });
             P_("imm_retry_decide", [&] { vtp::k_retry_decide<<<1, 32, 0, st>>>(a, cudaGraphConditionalHandle{}, 0); });
+            if (!s.phase_retry_all) P_("imm_drift_mark", [&] { vtp::k_drift_mark<<<G256, 256, 0, st>>>(a); });
             P_("imm_drift_diffuse", [&] { VTP_PHASE_DISPATCH(P, VTP_UNROLL_DISPATCH(s.unroll, vtp::k_drift_diffuse<UU, PP><<<G, B, 0, st>>>(a, 1))) });
             CUI(cudaMemcpyAsync(s.h_pinned + 5, m.counter + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             CUI(cudaStreamSynchronize(st));

@@ -105,6 +105,7 @@ struct vtp_solver {
     int row_lanes = 1;        // threads per row of the PBF neighbour passes (1, 4, 8)
     int list_lanes = 0;       // neighbour-list builder lanes per row (0 = by row count)
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn
+    bool phase_retry_all = false;   // IMM phase-transfer retries: every row, or rows near new flags
     int pbf_form = 0;                   // 0: the reference's PBF formulation, 1: standard PBF
     float pbf_eps = 1e-6f;
 
