@@ -535,8 +535,20 @@ __global__ void __launch_bounds__(256) k_drift_mark(ImmArgs a) {
         redo = fr == gen;
         if (fr == 0) {
             const uint32_t n = a.ncnt[r];
+            const uint32_t cnt = n > 0 ? n - 1 : 0;
             const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-            for (uint32_t t = 0; t + 1 < n && !redo; ++t) {
+            // four entries, then their four flags, per round trip (gen >= 1, so rows without a
+            // flag word (boundary rows) read as 0)
+            uint32_t t = 0;
+            for (; t + 4 <= cnt && !redo; t += 4) {
+                uint32_t j[4], f[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) j[u] = lst[(size_t)(t + u) * 32u];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) f[u] = j[u] < a.nf ? __ldg(a.flag + j[u]) : 0u;
+                redo = f[0] == gen || f[1] == gen || f[2] == gen || f[3] == gen;
+            }
+            for (; t < cnt && !redo; ++t) {
                 const uint32_t j = lst[(size_t)t * 32u];
                 redo = j < a.nf && __ldg(a.flag + j) == gen;
             }
