@@ -237,6 +237,29 @@ def test_phase_retries_near_flags_match_full_retries(vtp_gpu, kind):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("kind", ["DFSPH", "IMMCT"])
+def test_launch_count_graphs_match_direct_launches(vtp_gpu, kind):
+    """The launch count of graph substeps, kernels run inside the pressure-solve
+    and phase-retry WHILE nodes included, equals the count of the same
+    substeps launched one by one."""
+    vtp = vtp_gpu
+    sc = (vtp.scenes.dam_break("DFSPH", 8000, seed=17) if kind == "DFSPH"
+          else vtp.scenes.layered_mixture("IMMCT", 64, seed=5))
+    counts, retries = [], []
+    for graphs in (True, False):
+        s = vtp.solver_from_scene(sc, extra={"useGraphs": graphs})
+        n, r = 0, 0
+        for _ in range(10):
+            assert s.tickNsteps(1), s.last_error
+            n += s.launch_count()
+            r += s.stats()["phase_retries"]
+        counts.append(n)
+        retries.append(r)
+        s.destroy()
+    assert retries[0] == retries[1] and (kind == "DFSPH" or retries[0] > 0), retries
+    assert counts[0] == counts[1], counts
+
+
 def test_runs_are_deterministic(vtp_gpu):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()

@@ -971,8 +971,12 @@ int vtp_solver::tick_n(uint32_t n) {
     } else if (use_graphs) {
         launches = (uint64_t)n * launches_per_tick;
     }
+    if (imm) {
+        uint64_t body = 0;
+        stats.phase_retries = immct_last_retries(*this, &body);
+        if (use_graphs) launches += body;   // launched inside the retry loop's WHILE node
+    }
     last_launches = launches;
-    if (imm) stats.phase_retries = immct_last_retries(*this);
     stats.steps_done = steps_done;
     stats.sim_time = sim_time;
     stats.last_dt = cfl > 0.f ? last_dt : dt;

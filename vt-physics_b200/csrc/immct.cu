@@ -69,7 +69,8 @@ struct ImmArgs {
     float *ratio, *alpha;
     float *fin[kMaxPhases], *fout[kMaxPhases];
     uint32_t *flag;
-    uint32_t *counter;        // [0] newly flagged, [1] retry iteration, [2] stop, [3] retries, [4] work rows
+    uint32_t *counter;        // [0] newly flagged, [1] retry iteration, [2] stop, [3] retries, [4] work rows,
+                              // [5] retry-loop bodies run since initialize (wraps)
     uint32_t *work;           // rows the running retry recomputes (k_drift_mark)
     int retry_all;            // phase-transfer retries recompute every row (1) or rows near new flags (0)
     uint32_t *status;
@@ -97,6 +98,7 @@ struct ImmState {
     float *fin[kMaxPhases] = {nullptr}, *fout[kMaxPhases] = {nullptr};
     uint32_t *flag = nullptr, *counter = nullptr;
     uint32_t *work = nullptr;        // [nf] rows a phase-transfer retry recomputes
+    uint32_t bodies_seen = 0;        // counter[5] at the last launch count
     float4 *tpk = nullptr;
     float4 *pk2 = nullptr;           // [2 nf] packed gather rows (viscosity -> tension / conformation)
     std::vector<float> bfrac;        // boundary rows' phase fractions in attach order (host)
@@ -671,6 +673,7 @@ __global__ void k_check_negative(ImmArgs a) {
 __global__ void k_retry_decide(ImmArgs a, cudaGraphConditionalHandle h, int use_cond) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t *c = a.counter;
+    c[5] += 1;   // one per body of the retry loop (launch accounting)
     if (c[2] == 0) {
         const uint32_t iter = c[1];
         const bool stop = c[0] == 0 || iter > 100;
@@ -846,12 +849,12 @@ int immct_alloc(vtp_solver &s) {
     if ((rc = s.alloc(&m.rd, nf))) return rc;
     if ((rc = s.alloc(&m.cd, nf))) return rc;
     if ((rc = s.alloc(&m.flag, nf))) return rc;
-    if ((rc = s.alloc(&m.counter, 5))) return rc;
+    if ((rc = s.alloc(&m.counter, 6))) return rc;
     if ((rc = s.alloc(&m.work, nf))) return rc;
     if (m.p.ct && (rc = s.alloc(&m.tpk, 4 * (size_t)nf))) return rc;
     if ((rc = s.alloc(&m.pk2, 2 * (size_t)nf))) return rc;
     CUI(cudaMemsetAsync(m.flag, 0, nf * sizeof(uint32_t), s.st));
-    CUI(cudaMemsetAsync(m.counter, 0, 5 * sizeof(uint32_t), s.st));
+    CUI(cudaMemsetAsync(m.counter, 0, 6 * sizeof(uint32_t), s.st));
     return VTP_OK;
 }
 
@@ -973,9 +976,14 @@ void immct_set_parity(vtp_solver &s, int cur) {
     for (int c = 0; c < 9; ++c) m.Q[c].cur = cur;
 }
 
-uint32_t immct_last_retries(vtp_solver &s) {
-    uint32_t c[4] = {0, 0, 0, 0};
+uint32_t immct_last_retries(vtp_solver &s, uint64_t *body_launches) {
+    uint32_t c[6] = {0, 0, 0, 0, 0, 0};
+    if (body_launches) *body_launches = 0;
     if (cudaMemcpy(c, s.imm->counter, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    // Kernels of the retry loop's bodies since the last call: check, decide, (mark,) drift/diffuse.
+    const uint32_t bodies = c[5] - s.imm->bodies_seen;
+    s.imm->bodies_seen = c[5];
+    if (body_launches) *body_launches = (uint64_t)bodies * (s.phase_retry_all ? 3u : 4u);
     return c[3];
 }
 

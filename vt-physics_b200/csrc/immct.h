@@ -27,7 +27,9 @@ int immct_get_field(vtp_solver &s, int field, float *dev_out, size_t elems);
 void immct_fill_carry(vtp_solver &s, vtp::Carry &carry);
 int immct_copy_back(vtp_solver &s);
 void immct_set_parity(vtp_solver &s, int cur);
-uint32_t immct_last_retries(vtp_solver &s);
+// Retries of the last substep; *body_launches (optional) receives the kernels
+// the retry loop's bodies launched since the previous call.
+uint32_t immct_last_retries(vtp_solver &s, uint64_t *body_launches = nullptr);
 // Inputs of the conservation sums: rest density and phase fractions of the fluid rows, the
 // phase rest densities (up to vtp::kConsPhases phases).
 void immct_conservation_inputs(vtp_solver &s, const float **rd, const float **frac, float *rho_k, int *P);
