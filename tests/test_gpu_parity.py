@@ -260,6 +260,21 @@ def test_launch_count_graphs_match_direct_launches(vtp_gpu, kind):
     assert counts[0] == counts[1], counts
 
 
+def test_programmatic_launch_gives_identical_trajectories(vtp_gpu):
+    """Programmatic dependent launch between the PBF substep's kernels
+    ("pdl", default on) changes when blocks start, not what they read:
+    trajectories with and without it are bit-identical."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break()
+    out = []
+    for pdl in (True, False):
+        s = vtp.solver_from_scene(sc, extra={"rowLanes": 8, "pdl": pdl})
+        assert s.tickNsteps(20), s.last_error
+        out.append((s.get_field("pos"), s.get_field("vel")))
+        s.destroy()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 def test_runs_are_deterministic(vtp_gpu):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()

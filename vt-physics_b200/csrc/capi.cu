@@ -21,6 +21,10 @@ using json = nlohmann::json;
 
 namespace vtp {
 thread_local std::string g_last_error;
+bool &pdl_flag() {
+    static thread_local bool on = false;
+    return on;
+}
 int fail(int code, const std::string &msg) {
     g_last_error = msg;
     return code;
@@ -203,6 +207,7 @@ int vtp_solver::parse_config(const json &c) {
             if (order != "brick" && order != "linear")
                 return fail(VTP_ERR_CONFIG, "cellOrder must be \"brick\" or \"linear\"");
             cell_order_brick = order == "brick";
+            pdl = b.value("pdl", true);
             row_lanes = b.value("rowLanes", 1);
             if (row_lanes != 1 && row_lanes != 4 && row_lanes != 8)
                 return fail(VTP_ERR_CONFIG, "rowLanes must be 1, 4 or 8");
@@ -761,6 +766,7 @@ int vtp_solver::enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape) {
     // lists, `iterations` constraint passes, XSPH.  With `tape` the lists are built into the
     // tape and the intermediate states are copied out (differentiable mode).
     const size_t nf = L.nf;
+    const vtp::PdlScope pdl_scope(pdl);
     vtp::Carry none{};
     vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), none, dt, u,
                    u.fstart, prof);

@@ -73,6 +73,7 @@ struct PV2 {
 // FP32 sums then group differently from the list order).
 template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
+    pdl_enter();
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
 
 template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
+    pdl_enter();
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
@@ -161,6 +163,7 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
 
 template <int U, int L>
 __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
+    pdl_enter();
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
@@ -219,15 +222,15 @@ void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt,
 
 void pbf_lambda(cudaStream_t st, const PbfArgs &a, int block) {
     if (a.nf)
-        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_lambda<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, launch(k_pbf_lambda<UU, LL>, nblk(a.nf * LL, block), block, 0, st, a)))
 }
 void pbf_dx(cudaStream_t st, const PbfArgs &a, int block) {
     if (a.nf)
-        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_dx<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, launch(k_pbf_dx<UU, LL>, nblk(a.nf * LL, block), block, 0, st, a)))
 }
 void pbf_xsph(cudaStream_t st, const PbfArgs &a, int block) {
     if (a.nf)
-        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, k_pbf_xsph<UU, LL><<<nblk(a.nf * LL, block), block, 0, st>>>(a)))
+        VTP_LANES_DISPATCH(a.lanes, VTP_UNROLL_DISPATCH(a.unroll, launch(k_pbf_xsph<UU, LL>, nblk(a.nf * LL, block), block, 0, st, a)))
 }
 
 }  // namespace vtp

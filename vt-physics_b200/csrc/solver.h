@@ -102,6 +102,7 @@ struct vtp_solver {
     int unroll = 4;
     bool persistent_tiles = false;
     bool cell_order_brick = true;   // bucket order: bricked (4^3 cells, Morton inside) or linear
+    bool pdl = true;                // programmatic dependent launch between the substep's kernels
     int row_lanes = 1;        // threads per row of the PBF neighbour passes (1, 4, 8)
     int list_lanes = 0;       // neighbour-list builder lanes per row (0 = by row count)
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn

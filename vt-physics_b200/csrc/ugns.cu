@@ -39,6 +39,7 @@ __device__ __forceinline__ float4 apply_force(float4 p, float4 &v, float dt, flo
 __global__ void k_hash(Scenes sc, uint32_t row0, uint32_t cnt, const float4 *__restrict__ pos,
                        const float4 *__restrict__ vel, float force_dt, uint32_t *__restrict__ key,
                        uint32_t *__restrict__ rank, uint32_t *__restrict__ count) {
+    pdl_enter();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
     const SceneGrid g = load_scene(sc, row0 + i);
@@ -100,6 +101,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t &total)
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const uint32_t *__restrict__ in, size_t n,
                                                                  uint32_t *__restrict__ sums) {
+    pdl_enter();
     size_t base = (size_t)blockIdx.x * kScanTile + threadIdx.x;
     uint32_t s = 0;
 #pragma unroll
@@ -113,6 +115,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const uint32_t 
 }
 
 __global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *sums, size_t tiles) {
+    pdl_enter();
     // One block; each thread owns a contiguous run of tiles.
     const size_t per = (tiles + blockDim.x - 1) / blockDim.x;
     size_t b = threadIdx.x * per;
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *sums, size_t tiles
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t *__restrict__ in, size_t n,
                                                              const uint32_t *__restrict__ sums, uint32_t base_add,
                                                              uint32_t *__restrict__ out) {
+    pdl_enter();
     // Each thread scans kScanItems consecutive counters.
     __shared__ uint32_t tile[kScanTile];
     size_t t0 = (size_t)blockIdx.x * kScanTile;
@@ -172,6 +176,7 @@ __global__ void k_scatter(uint32_t row0, uint32_t cnt, const uint32_t *__restric
                           const uint32_t *__restrict__ rank, const uint32_t *__restrict__ start,
                           const uint32_t *__restrict__ orig, uint32_t *__restrict__ tmp_src,
                           uint32_t *__restrict__ tmp_orig, uint32_t *__restrict__ tmp_key) {
+    pdl_enter();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
     uint32_t k = key[i];
@@ -187,6 +192,7 @@ __global__ void k_rank_reorder(Scenes sc, uint32_t row0, uint32_t cnt, const uin
                                float4 *__restrict__ pos_out, const float4 *__restrict__ vel_in,
                                float4 *__restrict__ vel_out, uint32_t *__restrict__ orig_out, Carry carry,
                                float force_dt) {
+    pdl_enter();
     uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= cnt) return;
     // A row keeps its scene: slot d lies in the same scene range as its source row.
@@ -301,6 +307,7 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
                               const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
                               uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt,
                               uint32_t *__restrict__ status, uint32_t *__restrict__ overflow_count) {
+    pdl_enter();
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= cnt) return;
     uint32_t i = row0 + r;
@@ -430,6 +437,7 @@ __global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
     const uint32_t *__restrict__ orig, const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
     uint32_t *__restrict__ nbr, uint32_t *__restrict__ ncnt, uint32_t *__restrict__ status,
     uint32_t *__restrict__ overflow_count) {
+    pdl_enter();
     static_assert(L >= 2 && L <= 16 && (L & (L - 1)) == 0, "L divides the warp");
     // Accepted candidates of each thread, [kSplitKeep][kSplitBlock] (a thread's column is strided, so
     // a warp's stores and loads of entry k fall in 32 consecutive words).
@@ -673,9 +681,9 @@ int cubic_sigma_device(cudaStream_t st, float h, float *out_host) {
 static void scan_counts(cudaStream_t st, uint32_t *count, size_t n, uint32_t base_add, uint32_t *out,
                         UgnsBuffers &u) {
     size_t tiles = (n + kScanTile - 1) / kScanTile;
-    k_scan_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums);
-    k_scan_sums<<<1, 1024, 0, st>>>(u.scan_sums, tiles);
-    k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(count, n, u.scan_sums, base_add, out);
+    launch(k_scan_tile_sums, (unsigned)tiles, kScanThreads, 0, st, count, n, u.scan_sums);
+    launch(k_scan_sums, 1, 1024, 0, st, u.scan_sums, tiles);
+    launch(k_scan_tiles, (unsigned)tiles, kScanThreads, 0, st, count, n, u.scan_sums, base_add, out);
 }
 
 void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t row0, uint32_t cnt,
@@ -688,7 +696,7 @@ void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t ro
     B();
     // u.count is all zero here: zeroed once at allocation and by every scan after reading it.
     if (cnt > 0) {
-        k_hash<<<nblk(cnt, 256), 256, 0, st>>>(sc, row0, cnt, pos_in, vel_in, force_dt, u.key, u.rank, u.count);
+        launch(k_hash, nblk(cnt, 256), 256, 0, st, sc, row0, cnt, pos_in, vel_in, force_dt, u.key, u.rank, u.count);
     }
     E("ugns_clear_hash");
     B();
@@ -696,11 +704,11 @@ void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t ro
     E("ugns_cell_scan");
     if (cnt == 0) return;
     B();
-    k_scatter<<<nblk(cnt, 256), 256, 0, st>>>(row0, cnt, u.key, u.rank, start, orig_in, u.tmp_src, u.tmp_orig,
+    launch(k_scatter, nblk(cnt, 256), 256, 0, st, row0, cnt, u.key, u.rank, start, orig_in, u.tmp_src, u.tmp_orig,
                                               u.tmp_key);
     E("ugns_scatter");
     B();
-    k_rank_reorder<<<nblk(cnt, 256), 256, 0, st>>>(sc, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
+    launch(k_rank_reorder, nblk(cnt, 256), 256, 0, st, sc, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
                                                    pos_out, vel_in, vel_out, orig_out, carry, force_dt);
     E("ugns_rank_reorder");
 }
@@ -717,15 +725,15 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
         const unsigned ns = nblk(cnt * S, kSplitBlock);
         switch (L.merge_mode) {
             case 0:
-                k_build_lists_split<0, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                launch(k_build_lists_split<0, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
             case 1:
-                k_build_lists_split<1, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                launch(k_build_lists_split<1, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
             default:
-                k_build_lists_split<2, S><<<ns, kSplitBlock, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
+                launch(k_build_lists_split<2, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
                                                                u.bstart, nbr, ncnt, status, overflow);
                 break;
         }
@@ -734,15 +742,15 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
     unsigned nb = nblk(cnt, block);
     switch (L.merge_mode) {
         case 0:
-            k_build_lists<0><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            launch(k_build_lists<0>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
         case 1:
-            k_build_lists<1><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            launch(k_build_lists<1>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
         default:
-            k_build_lists<2><<<nb, block, 0, st>>>(sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
+            launch(k_build_lists<2>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
                                                     ncnt, status, overflow);
             break;
     }
