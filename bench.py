@@ -168,11 +168,8 @@ def cpu_baseline(scene, seconds: float) -> dict:
     from oracle import oracle as O
     O.lib()
     cores = O.num_threads()
-    if scene.solver not in ("PBF", "DFSPH"):
-        return {"value": None, "unit": METRIC, "cores": cores, "kind": "port",
-                "sample": f"none: the FP64 oracle restates the PBF and DFSPH substeps, not {scene.solver}"}
     t0 = time.perf_counter()
-    o = O.OracleSolver(scene)
+    o = O.OracleSolver(scene) if scene.solver in ("PBF", "DFSPH") else O.ImmOracle(scene)
     init_s = time.perf_counter() - t0
     steps = 0
     t0 = time.perf_counter()

@@ -34,6 +34,20 @@ class OrDfsph(C.Structure):
                 ("max_iters", C.c_int32)]
 
 
+class OrImm(C.Structure):
+    _fields_ = [("dt", C.c_double), ("h", C.c_double), ("vol0", C.c_double), ("gamma", C.c_double),
+                ("Cf", C.c_double), ("Cd0", C.c_double), ("g", C.c_double * 3), ("P", C.c_int32),
+                ("ct", C.c_int32), ("rho", C.c_double * 8), ("mu", C.c_double * 8), ("vis_base", C.c_double),
+                ("vis_max", C.c_double), ("relax", C.c_double), ("thin0", C.c_double), ("theta", C.c_double),
+                ("div_thr", C.c_double), ("inc_thr", C.c_double), ("force_div", C.c_int32),
+                ("force_inc", C.c_int32), ("max_iters", C.c_int32)]
+
+
+class OrImmOut(C.Structure):
+    _fields_ = [("div_iters", C.c_int32), ("inc_iters", C.c_int32), ("div_residual", C.c_double),
+                ("inc_residual", C.c_double), ("retries", C.c_int32), ("crashed", C.c_int32)]
+
+
 class OrSolveOut(C.Structure):
     _fields_ = [("div_iters", C.c_int32), ("inc_iters", C.c_int32), ("div_residual", C.c_double),
                 ("inc_residual", C.c_double), ("crashed", C.c_int32)]
@@ -60,6 +74,9 @@ def lib() -> C.CDLL:
                                           C.POINTER(C.c_double)]
         L.or_dfsph_solve_op.argtypes = [C.c_uint32, P, P, P, P, P, P, C.c_uint32, C.c_double, C.c_double, C.c_int,
                                          P, P]
+        L.or_imm_init.argtypes = [C.c_uint32, P, P, P, C.POINTER(OrGrid), C.POINTER(OrImm)]
+        L.or_imm_step.argtypes = [C.c_uint32, P, P, C.c_int32, P, P, P, P, P, P, P, P, C.POINTER(OrGrid),
+                                  C.POINTER(OrImm), C.POINTER(OrImmOut)]
         L.or_num_threads.restype = C.c_int
         L.or_set_num_threads.argtypes = [C.c_int]
         _lib = L
@@ -212,6 +229,85 @@ class OracleSolver:
                                 _ptr(self.rest_density), C.byref(self.grid), C.byref(self.p), C.byref(out),
                                 _ptr(self.ratio), _ptr(self.alpha))
                 self.last = out
+            self.steps += 1
+
+
+class ImmOracle:
+    """FP64 state machine for one IMM or IMM-CT scene (attach order): positions,
+    mixture and phase velocities, volume fractions, conformation tensor and Cd
+    (IMMCTSolver.cpp:408-477, IMMSolver.cpp:400-466; or_imm_step)."""
+
+    def __init__(self, scene, force_div: int = 0, force_inc: int = 0):
+        self.kind = scene.solver
+        req = scene.config[self.kind]["Required"]
+        opt = scene.config[self.kind]["Optional"]
+        self.grid = make_grid(req)
+        objs = scene.objects
+        self.pos = np.concatenate([o.pos for o in objs]).astype(np.float64)
+        vels = [np.asarray(o.velocity, np.float32) if o.velocity is not None
+                else np.tile(np.asarray(o.velocity_start, np.float32), (o.n, 1)) for o in objs]
+        self.vel = np.concatenate(vels).astype(np.float64)
+        self.mat = np.concatenate([np.full(o.n, o.material, np.int32) for o in objs])
+        self.obj = np.concatenate([np.full(o.n, k, np.int32) for k, o in enumerate(objs)])
+        self.obj_is_fluid = np.array([1 if o.material == 0 else 0 for o in objs], np.int32)
+        self.n = self.pos.shape[0]
+        f32 = lambda v: float(np.float32(v))
+        p = OrImm()
+        r = np.float32(req["particleRadius"])
+        p.dt = f32(req["timeStep"])
+        p.h = f32(r * np.float32(4))
+        p.vol0 = f32((np.float32(2) * r) ** np.float32(3))
+        p.gamma = f32(req["surfaceTensionCoefficient"])
+        p.Cf = f32(req["diffusionCoefficientCf"])
+        g = [0.0, -9.8, 0.0]
+        if opt["enable"]:
+            g = [f32(v) for v in opt["gravity"]]
+        for a in range(3):
+            p.g[a] = g[a]
+        rho = [f32(v) for v in req["phaseRestDensity"]]
+        p.P = len(rho)
+        for k, v in enumerate(rho):
+            p.rho[k] = v
+        p.ct = 1 if self.kind == "IMMCT" else 0
+        if p.ct:
+            for k in range(p.P):   # IMMCTSolver::setConfig copies solventViscosity to every phase
+                p.mu[k] = f32(req["solventViscosity"])
+            p.Cd0 = f32(req["momentumExchangeCoefficientCd0"])
+            p.vis_base = f32(np.float32(req["solutionBasicViscosity"]) * np.float32(1000))
+            p.vis_max = f32(np.float32(req["solutionMaxViscosity"]) * np.float32(1000))
+            p.relax = f32(req["relaxationTime"])
+            p.thin0 = f32(req["shearThinningBasicFactor"])
+            p.theta = f32(req["rheologicalThreshold"])
+        else:
+            for k, v in enumerate(req["phaseRestViscosity"]):
+                p.mu[k] = f32(v)
+            p.Cd0 = f32(req["momentumExchangeCoefficientCd"])
+        p.div_thr = f32(req["divFreeThreshold"])
+        p.inc_thr = f32(req["incompThreshold"])
+        p.force_div, p.force_inc, p.max_iters = force_div, force_inc, 101
+        self.p = p
+        P = p.P
+        self.frac = np.concatenate([np.tile(np.asarray(o.phase_fraction, np.float32)[:P], (o.n, 1))
+                                    for o in objs]).astype(np.float64)
+        self.vph = np.repeat(self.vel[:, None, :], P, axis=1).copy()   # init_data_cuda: v_k = v
+        self.Q = np.tile(np.eye(3).reshape(1, 9), (self.n, 1))
+        self.cd = np.full(self.n, p.Cd0, np.float64)
+        self.vol = np.zeros(self.n)
+        lib().or_imm_init(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), C.byref(self.grid), C.byref(p))
+        self.steps = 0
+        self.last = OrImmOut()
+
+    def set_forced_iterations(self, div: int, inc: int):
+        self.p.force_div = int(div)
+        self.p.force_inc = int(inc)
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            out = OrImmOut()
+            lib().or_imm_step(self.n, _ptr(self.mat), _ptr(self.obj), len(self.obj_is_fluid), _ptr(self.obj_is_fluid),
+                              _ptr(self.pos), _ptr(self.vel), _ptr(self.vph), _ptr(self.frac), _ptr(self.Q),
+                              _ptr(self.cd), _ptr(self.vol), C.byref(self.grid), C.byref(self.p), C.byref(out))
+            self.last = out
             self.steps += 1
 
 

@@ -4,6 +4,9 @@
  *   SPH kernels       KernelFunctions.cuh:13-70
  *   PBF               PBFCudaImpl.cu:34-194 in the order of PBFSolver.cpp:326-362
  *   DFSPH             DFSPHCudaImpl.cu:38-611 in the order of DFSPHSolver.cpp:339-391
+ *   IMM-CT / IMM      IMMCTCudaImpl.cu:52-821 in the order of IMMCTSolver.cpp:408-477 and
+ *                     IMMCTCudaImpl.cu:849-1152; IMM the same without the conformation
+ *                     terms and with a constant Cd (IMMSolver.cpp:400-466, IMMCudaImpl.cu)
  * Build: gcc -O2 -fopenmp -ffp-contract=off -fPIC -shared (oracle/build.py).
  */
 #include "vtp_oracle.h"
@@ -866,4 +869,335 @@ void or_dfsph_solve_op(uint32_t n, const int32_t *mat, const double *pos, const 
         free(kb);
     }
     free(mass); free(ratio); free(alpha); free(kappa); free(mask);
+}
+
+/* ------------------------------------------------------------------ IMM / IMM-CT */
+
+#define V3(a, i) (&(a)[3 * (size_t)(i)])
+#define VPH(i, k) (&vph[3 * ((size_t)(i) * P + (k))])
+#define FR(i, k) (frac[(size_t)(i) * P + (k)])
+
+void or_imm_init(uint32_t n, const int32_t *mat, const double *pos, double *vol, const or_grid *g,
+                 const or_imm_params *p) {
+    /* init_data_cuda (IMMCTCudaImpl.cu:52-81): V = fPart_rest_volume; compute_rigid_volume_cuda
+     * (:108-127): boundary V = 1 / sum over same-material neighbours of W (self included). */
+    lists_t L = build_lists(n, pos, g);
+    cubic_t k = cubic_make(p->h);
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] == 0) {
+            vol[i] = p->vol0;
+            continue;
+        }
+        double delta = 0, r[3];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] == mat[i]) delta += cubic_w(&k, rdiff(pos, i, j, r));
+        }
+        vol[i] = 1.0 / delta;
+    }
+    free_lists(&L);
+}
+
+/* update_rest_density_and_mass_cuda (:83-106): rest density = sum_k alpha_k rho_k.  A boundary
+ * particle's value (the reference's racy max over fluid neighbours) enters no fluid term. */
+static void imm_rest_density(uint32_t n, int P, const double *frac, const or_imm_params *p, const double *vol,
+                             double *rd, double *mass) {
+    for (uint32_t i = 0; i < n; ++i) {
+        double s = 0;
+        for (int k = 0; k < P; ++k) s += FR(i, k) * p->rho[k];
+        rd[i] = s;
+        mass[i] = s * vol[i];
+    }
+}
+
+/* update_vel_from_phase_vel_cuda (:405-424): v = sum_k alpha_k v_k (drift u_k = v_k - v). */
+static void imm_mix_velocity(uint32_t n, const int32_t *mat, int P, const double *frac, const double *vph,
+                             double *vel) {
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        double v[3] = {0, 0, 0};
+        for (int k = 0; k < P; ++k)
+            for (int a = 0; a < 3; ++a) v[a] += VPH(i, k)[a] * FR(i, k);
+        for (int a = 0; a < 3; ++a) V3(vel, i)[a] = v[a];
+    }
+}
+
+/* phase_acc_2_phase_vel_cuda (:392-403) then update_vel_from_phase_vel_cuda. */
+static void imm_apply_phase_acc(uint32_t n, const int32_t *mat, int P, const double *frac, double *vph,
+                                const double *acc, double dt, double *vel) {
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int k = 0; k < P; ++k)
+            for (int a = 0; a < 3; ++a) VPH(i, k)[a] += acc[3 * ((size_t)i * P + k) + a] * dt;
+    }
+    imm_mix_velocity(n, mat, P, frac, vph, vel);
+}
+
+/* A mixture acceleration a_i shared out to the phases with the factor Cd + (1 - Cd) rho_i / rho_k
+ * (distribute_acc_pressure_2_phase_cuda :426-440, add_phase_pct_acc_cuda :772-778). */
+static void imm_share(uint32_t i, int P, const double *a, double cd, double rd, const or_imm_params *p,
+                      double *acc) {
+    for (int k = 0; k < P; ++k) {
+        double f = cd + (1.0 - cd) * (rd / p->rho[k]);
+        for (int a3 = 0; a3 < 3; ++a3) acc[3 * ((size_t)i * P + k) + a3] = a[a3] * f;
+    }
+}
+
+/* apply_pressure_acc (:919-937): acc = (v* - v) / dt distributed to the phases. */
+static void imm_apply_pressure(uint32_t n, const int32_t *mat, int P, const double *frac, double *vph,
+                               const double *vadv, const double *cd, const double *rd, const or_imm_params *p,
+                               double *acc, double *vel) {
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        double a[3];
+        for (int a3 = 0; a3 < 3; ++a3) a[a3] = (V3(vadv, i)[a3] - V3(vel, i)[a3]) / p->dt;
+        imm_share(i, P, a, cd[i], rd[i], p, acc);
+    }
+    imm_apply_phase_acc(n, mat, P, frac, vph, acc, p->dt, vel);
+}
+
+/* One pass of update_phase_change_from_drift_cuda + update_phase_change_from_diffuse_cuda
+ * (:541-614) over the unflagged fluid particles; flagged ones get no change. */
+static void imm_phase_pass(uint32_t n, const int32_t *mat, int P, const double *pos, const double *vel,
+                           const double *vph, const double *frac, const double *vol, const int32_t *flag,
+                           const lists_t *L, const or_grid *g, const cubic_t *kc, const or_imm_params *p,
+                           double *fin, double *fout) {
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        for (int k = 0; k < P; ++k) fin[(size_t)i * P + k] = fout[(size_t)i * P + k] = 0.0;
+        if (flag[i]) continue;
+        double r[3];
+        FOR_NBR(*L, g, i, j) {   /* drift */
+            if (j == i || mat[j] != mat[i] || flag[j]) continue;
+            double gg = cubic_g(kc, rdiff(pos, i, j, r));
+            for (int k = 0; k < P; ++k) {
+                double d = 0;
+                for (int a = 0; a < 3; ++a) {
+                    double ui = VPH(i, k)[a] - V3(vel, i)[a], uj = VPH(j, k)[a] - V3(vel, j)[a];
+                    d += (FR(i, k) * ui + FR(j, k) * uj) * gg * r[a];
+                }
+                double ch = -p->dt * vol[j] * d;
+                if (ch < 0) fout[(size_t)i * P + k] += ch;
+                else fin[(size_t)i * P + k] += ch;
+            }
+        }
+        FOR_NBR(*L, g, i, j) {   /* diffusion */
+            if (j == i || mat[j] != mat[i] || flag[j]) continue;
+            double rl = rdiff(pos, i, j, r);
+            double gg = cubic_g(kc, rl);
+            double factor = gg * rl * rl / (rl * rl);   /* (gradW . x_ij) / |x_ij|^2 */
+            for (int k = 0; k < P; ++k) {
+                double ch = p->dt * p->Cf * (FR(i, k) - FR(j, k)) * vol[j] * factor;
+                if (ch < 0) fout[(size_t)i * P + k] += ch;
+                else fin[(size_t)i * P + k] += ch;
+            }
+        }
+    }
+}
+
+void or_imm_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
+                 double *pos, double *vel, double *vph, double *frac, double *Q, double *cd, const double *vol,
+                 const or_grid *g, const or_imm_params *p, or_imm_out *out) {
+    const int P = p->P;
+    const double dt = p->dt;
+    const size_t nn = n ? n : 1;
+    lists_t L = build_lists(n, pos, g);
+    cubic_t kc = cubic_make(p->h);
+    double *rd = (double *)calloc(nn, sizeof(double)), *mass = (double *)calloc(nn, sizeof(double));
+    double *ratio = (double *)calloc(nn, sizeof(double)), *alpha = (double *)calloc(nn, sizeof(double));
+    double *kappa = (double *)calloc(nn, sizeof(double));
+    double *vadv = (double *)malloc(sizeof(double) * 3 * nn);
+    double *acc = (double *)calloc(3 * nn * P, sizeof(double));
+    double *nrm = (double *)calloc(3 * nn, sizeof(double));
+    double *tau = (double *)calloc(9 * nn, sizeof(double));
+    double *fin = (double *)calloc(nn * P, sizeof(double)), *fout = (double *)calloc(nn * P, sizeof(double));
+    int32_t *flag = (int32_t *)calloc(nn, sizeof(int32_t));
+    imm_rest_density(n, P, frac, p, vol, rd, mass);
+
+    /* sph_precompute (:849-864): compression ratio, alpha (as DFSPH, m_j = rest density_j V_j),
+     * and for IMM-CT update_Cd_cuda (:782-804). */
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double rt = 0, a1[3] = {0, 0, 0}, a2 = 1e-6, blk = 0, r[3];
+        FOR_NBR(L, g, i, j) {
+            double rl = rdiff(pos, i, j, r);
+            double w = cubic_w(&kc, rl);
+            rt += vol[j] * w;
+            double gg = cubic_g(&kc, rl);
+            for (int a = 0; a < 3; ++a) a1[a] += vol[j] * gg * r[a];
+            if (mat[j] == 0) a2 += gg * gg * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) * vol[j] * vol[j] / mass[j];
+            if (p->ct && mat[j] == mat[i] && j != i) blk += vol[j] * FR(j, 1) * w;
+        }
+        double al = (a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2]) / mass[i] + a2;
+        ratio[i] = rt;
+        alpha[i] = al < 1e-6 ? 1e-6 : al;
+        cd[i] = p->ct ? p->Cd0 + (1.0 - p->Cd0) * blk : p->Cd0;
+    }
+    memcpy(vadv, vel, sizeof(double) * 3 * n);
+    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, &kc, dt};
+    out->crashed = 0;
+    out->div_iters = pressure_solve(&c, vadv, kappa, p->div_thr, p->force_div, p->max_iters, &out->div_residual);
+    if (p->force_div <= 0 && out->div_iters > p->max_iters - 1) out->crashed = 1;
+    imm_apply_pressure(n, mat, P, frac, vph, vadv, cd, rd, p, acc, vel);
+
+    /* immct_gravity_vis_surface (:939-964): gravity, phase viscosity (:297-330), surface normal
+     * (:332-355) and surface tension (:357-390) on every phase. */
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double nn3[3] = {0, 0, 0}, r[3];
+        for (int k = 0; k < P; ++k)
+            for (int a = 0; a < 3; ++a) acc[3 * ((size_t)i * P + k) + a] = p->g[a];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] != mat[i]) continue;
+            double rl = rdiff(pos, i, j, r);
+            double gg = cubic_g(&kc, rl);
+            for (int a = 0; a < 3; ++a) nn3[a] += p->h * mass[j] / rd[j] * gg * r[a];
+            if (j == i) continue;
+            for (int k = 0; k < P; ++k) {
+                double d = 0;
+                for (int a = 0; a < 3; ++a) {
+                    double vkmj = VPH(i, k)[a] - V3(vel, j)[a], vij = V3(vel, i)[a] - V3(vel, j)[a];
+                    d += (p->mu[k] * (1.0 - cd[i]) * vkmj + p->mu[k] * cd[i] * vij) * r[a];
+                }
+                for (int a = 0; a < 3; ++a) acc[3 * ((size_t)i * P + k) + a] += 10.0 * vol[j] * d * gg * r[a] / (rl * rl);
+            }
+        }
+        for (int a = 0; a < 3; ++a) V3(nrm, i)[a] = nn3[a];
+    }
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double at[3] = {0, 0, 0}, r[3];
+        FOR_NBR(L, g, i, j) {
+            if (mat[j] != mat[i] || j == i) continue;
+            double rl = rdiff(pos, i, j, r);
+            double kk = 2 * rd[i] / (rd[i] + rd[j]);
+            double cc = tension_c(rl, p->h);
+            for (int a = 0; a < 3; ++a) {
+                double a1 = -p->gamma * mass[i] * mass[j] * cc * r[a] / rl;
+                double a2 = -p->gamma * mass[i] * (V3(nrm, i)[a] - V3(nrm, j)[a]);
+                at[a] += kk * (a1 + a2);
+            }
+        }
+        for (int k = 0; k < P; ++k)
+            for (int a = 0; a < 3; ++a) acc[3 * ((size_t)i * P + k) + a] += at[a];
+    }
+    imm_apply_phase_acc(n, mat, P, frac, vph, acc, dt, vel);
+
+    if (p->ct) {
+        /* immct_pct (:966-995): velocity gradient (:687-714), rheological factors (:806-821),
+         * conformation update (:716-744), stress divergence (:746-780). */
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double G[9] = {0}, r[3];
+            FOR_NBR(L, g, i, j) {
+                if (mat[j] != 0) continue;
+                double gg = cubic_g(&kc, rdiff(pos, i, j, r));
+                double vj = mass[j] / rd[j];
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) G[3 * a + b] += vj * (V3(vel, j)[a] - V3(vel, i)[a]) * gg * r[b];
+            }
+            const double a1f = FR(i, 1);
+            const double thin = p->thin0 * fmax(0.0, p->theta - a1f) / (p->theta + 1e-6);
+            const double vinc = pow(1.0 - a1f, -1.2);
+            double *q = &Q[9 * (size_t)i], dq[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    double qg = 0, gq = 0, qiq = 0;
+                    for (int m = 0; m < 3; ++m) {
+                        qg += q[3 * a + m] * G[3 * m + b];          /* Q gradv */
+                        gq += G[3 * m + a] * q[3 * m + b];          /* gradv^T Q */
+                        qiq += (q[3 * a + m] - (a == m)) * q[3 * m + b];   /* (Q - I) Q */
+                    }
+                    dq[3 * a + b] = (qg + gq - (q[3 * a + b] - (a == b)) / p->relax - thin * qiq) * dt;
+                }
+            for (int m = 0; m < 9; ++m) q[m] += dq[m];
+            double trD = G[0] + G[4] + G[8];   /* trace of D = (gradv + gradv^T) / 2 */
+            double shear = sqrt(0.5 * trD * trD);
+            double vis = fmin(p->vis_base * vinc, p->vis_max);
+            vis = p->vis_base + (vis - p->vis_base) / (1.0 + pow(10.0 * shear, 5.0)) * fmin(1.0, a1f / (p->theta + 1e-6));
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) tau[9 * (size_t)i + 3 * a + b] = vis * (q[3 * a + b] - (a == b));
+        }
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (mat[i] != 0) continue;
+            double a[3] = {0, 0, 0}, r[3];
+            FOR_NBR(L, g, i, j) {
+                if (mat[j] != 0) continue;
+                double gg = cubic_g(&kc, rdiff(pos, i, j, r));
+                for (int x = 0; x < 3; ++x)
+                    for (int y = 0; y < 3; ++y)
+                        a[x] += (tau[9 * (size_t)i + 3 * x + y] / (rd[i] * rd[i]) +
+                                 tau[9 * (size_t)j + 3 * x + y] / (rd[j] * rd[j])) * gg * r[y];
+            }
+            for (int x = 0; x < 3; ++x) a[x] *= FR(i, 1) * rd[i];
+            imm_share(i, P, a, cd[i], rd[i], p, acc);
+        }
+        imm_apply_phase_acc(n, mat, P, frac, vph, acc, dt, vel);
+    }
+    memcpy(vadv, vel, sizeof(double) * 3 * n);
+    out->inc_iters = pressure_solve(&c, vadv, kappa, p->inc_thr, p->force_inc, p->max_iters, &out->inc_residual);
+    if (p->force_inc <= 0 && out->inc_iters > p->max_iters - 1) out->crashed = 1;
+    imm_apply_pressure(n, mat, P, frac, vph, vadv, cd, rd, p, acc, vel);
+    for (uint32_t i = 0; i < n; ++i)   /* update_pos_cuda (:480-491) */
+        if (mat[i] == 0)
+            for (int a = 0; a < 3; ++a) V3(pos, i)[a] += V3(vel, i)[a] * dt;
+
+    /* phase_transfer (:1065-1137): exchange with the lists of the substep's start and the new
+     * positions; particles whose fractions would turn negative are flagged and the exchange is
+     * recomputed without them until no particle is newly flagged (at most 100 passes). */
+    imm_phase_pass(n, mat, P, pos, vel, vph, frac, vol, flag, &L, g, &kc, p, fin, fout);
+    int iter = 1;
+    out->retries = 0;
+    for (;;) {
+        int newly = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (mat[i] != 0 || flag[i]) continue;
+            for (int k = 0; k < P; ++k)
+                if (FR(i, k) + fout[(size_t)i * P + k] + fin[(size_t)i * P + k] < 0) {
+                    flag[i] = 1;
+                    ++newly;
+                    break;
+                }
+        }
+        if (newly == 0 || iter > 100) break;
+        imm_phase_pass(n, mat, P, pos, vel, vph, frac, vol, flag, &L, g, &kc, p, fin, fout);
+        ++iter;
+        ++out->retries;
+    }
+    if (iter > 100) out->crashed = 1;
+    for (uint32_t i = 0; i < n; ++i) {   /* update_phase_change, release_unused_drift_vel, release_negative */
+        if (mat[i] != 0) continue;
+        for (int k = 0; k < P; ++k) FR(i, k) += fout[(size_t)i * P + k] + fin[(size_t)i * P + k];
+        if (flag[i])
+            for (int k = 0; k < P; ++k)
+                for (int a = 0; a < 3; ++a) VPH(i, k)[a] = V3(vel, i)[a];
+    }
+    /* regularize_vol_frac_cuda (:493-510) + rest density + mixture velocity, then
+     * update_mass_and_vel (:1139-1152) does the three again. */
+    for (int pass = 0; pass < 2; ++pass) {
+        for (uint32_t i = 0; i < n; ++i) {
+            if (mat[i] != 0) continue;
+            double s = 0;
+            for (int k = 0; k < P; ++k) s += FR(i, k);
+            for (int k = 0; k < P; ++k) FR(i, k) /= s;
+        }
+        imm_rest_density(n, P, frac, p, vol, rd, mass);
+        imm_mix_velocity(n, mat, P, frac, vph, vel);
+    }
+    free(rd); free(mass); free(ratio); free(alpha); free(kappa); free(vadv); free(acc); free(nrm); free(tau);
+    free(fin); free(fout); free(flag);
+    free_lists(&L);
 }

@@ -1,6 +1,7 @@
 /*
  * CPU oracle (test infrastructure only): an FP64 OpenMP restatement of the
- * reference's uniform-grid neighbour search and PBF / DFSPH substeps, used
+ * reference's uniform-grid neighbour search and PBF / DFSPH / IMM / IMM-CT
+ * substeps, used
  * by tests/ to check the sm_100a library and by bench.py as the timed CPU
  * baseline.  Product code never links or calls it.
  *
@@ -95,6 +96,35 @@ void or_dfsph_init(uint32_t n, const int32_t *mat, const double *pos, double *vo
 void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
                    double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
                    const or_dfsph_params *p, or_solve_out *out, double *ratio, double *alpha);
+
+/* IMM / IMM-CT mixtures (IMMCTSolver.cpp:408-477 with IMMCTCudaImpl.cu:52-1152;
+ * IMMSolver.cpp:400-466 with IMMCudaImpl.cu).  P phases; per particle:
+ * frac[n*P] volume fractions, vph[n*P*3] phase velocities, Q[n*9] conformation
+ * tensor (row-major, IMM-CT), cd[n] momentum-exchange coefficient (IMM-CT:
+ * recomputed every substep from the blocking factor; IMM: p->Cd0 throughout).
+ * vol from or_imm_init (fluid vol0, boundary 1 / sum of same-material W). */
+#define OR_MAX_PHASES 8
+typedef struct or_imm_params {
+    double dt, h, vol0, gamma, Cf, Cd0;
+    double g[3];
+    int32_t P, ct;                          /* phases; 1 = IMM-CT, 0 = IMM */
+    double rho[OR_MAX_PHASES], mu[OR_MAX_PHASES];
+    double vis_base, vis_max;               /* IMM-CT, after init_data_cuda's x1000 */
+    double relax, thin0, theta;             /* relaxationTime, shearThinningBasicFactor, rheologicalThreshold */
+    double div_thr, inc_thr;
+    int32_t force_div, force_inc, max_iters;
+} or_imm_params;
+typedef struct or_imm_out {
+    int32_t div_iters, inc_iters;
+    double div_residual, inc_residual;
+    int32_t retries;                        /* phase-transfer passes after the first */
+    int32_t crashed;
+} or_imm_out;
+void or_imm_init(uint32_t n, const int32_t *mat, const double *pos, double *vol, const or_grid *g,
+                 const or_imm_params *p);
+void or_imm_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
+                 double *pos, double *vel, double *vph, double *frac, double *Q, double *cd, const double *vol,
+                 const or_grid *g, const or_imm_params *p, or_imm_out *out);
 
 int or_num_threads(void);
 void or_set_num_threads(int n);

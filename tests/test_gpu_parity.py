@@ -160,6 +160,36 @@ def test_dfsph_converged_solve_matches_oracle(vtp_gpu, oracle_lib):
     s.destroy()
 
 
+@pytest.mark.parametrize("kind", ["IMMCT", "IMM"])
+def test_mixture_substeps_forced_iterations_match_oracle(vtp_gpu, oracle_lib, kind):
+    """IMM / IMM-CT against the FP64 oracle with 2 divergence and 3 density
+    iterations forced: positions, velocities, volume fractions (IMM-CT: also
+    the conformation tensor and Cd) after each of three substeps."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.layered_mixture(kind, 16, seed=3)
+    s = vtp.solver_from_scene(sc, extra={"forceDivIterations": 2, "forceIncompIterations": 3})
+    o = oracle_lib.ImmOracle(sc, force_div=2, force_inc=3)
+    assert s.initialize()
+    fm = fluid_mask(sc)
+    assert rel_err(s.get_field("volume"), o.vol) < TOL
+    for step in range(1, 4):
+        assert s.tickNsteps(1), s.last_error
+        o.step(1)
+        ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+        ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+        ef = rel_err(s.get_field("vol_frac")[fm].reshape(-1), o.frac[fm].reshape(-1))
+        msg = f"{kind} step {step}: pos {ep:.2e} vel {ev:.2e} frac {ef:.2e}"
+        eq = ec = 0.0
+        if kind == "IMMCT":
+            eq = rel_err(s.get_field("conformation")[fm].reshape(-1), o.Q[fm].reshape(-1))
+            ec = rel_err(s.get_field("cd")[fm].reshape(-1), o.cd[fm])
+            msg += f" Q {eq:.2e} Cd {ec:.2e}"
+        print(msg)
+        assert ep < TOL * step and ev < TOL_DFSPH_VEL_FP64 * step
+        assert ef < TOL * step and eq < TOL * step and ec < TOL * step
+    s.destroy()
+
+
 def test_graph_and_direct_launch_agree(vtp_gpu):
     vtp = vtp_gpu
     sc = vtp.scenes.dam_break("DFSPH", 8000, seed=17)
