@@ -259,7 +259,7 @@ VTP_API int vtp_generate_cube(float radius, const float lb[3], const float size[
 VTP_API int vtp_generate_box(float radius, const float lb[3], const float size[3], int32_t layers, float *d_out,
                              uint32_t capacity, uint32_t *count, void *stream);
 
-/* Trajectory statistics long runs are judged by (no counterpart call in the
+/* Trajectory statistics that long runs are compared by (no counterpart call in the
  * reference, which has no such diagnostics): the FP64 sums of
  * vtp_conservation over the fluid of scene `scene` (-1: every scene of the
  * solver), summed on the device in a fixed order, so repeated calls on the

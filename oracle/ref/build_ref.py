@@ -8,7 +8,8 @@ harness ``ref_harness.cu``.  Nothing is written outside ``oracle/_ref/``.
 The reference's own CMake build is not used (it needs vcpkg and MSVC-only
 flags).  ``CommonFunc.cpp`` is left out: the harness supplies ``cal_mean``.
 
-Run here (no GPU needed); the library then travels to the GPU box.
+Builds without a GPU (nvcc cross-compiles for sm_100a); the library is loaded where the
+golden fixtures are generated.
 """
 from __future__ import annotations
 

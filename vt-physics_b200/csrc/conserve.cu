@@ -1,7 +1,7 @@
 // Conservation and density-error sums of the fluid, in FP64 on the device:
 // total mass, momentum, kinetic energy, per-phase mass (IMM / IMM-CT) and the
 // mean density error of the last substep, for one scene or the whole solver.
-// These are the trajectory statistics long runs are judged by; the sums run
+// These are the trajectory statistics that long runs are compared by; the sums run
 // over the sorted rows in a fixed order (per-block tree sums, then one block
 // over the blocks' partials), so repeated calls on the same state agree bit
 // for bit.
