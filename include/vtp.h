@@ -162,9 +162,10 @@ VTP_API int vtp_solver_create(int solver_type, vtp_solver **out);
  *       that were just flagged negative or have such a fluid neighbour, the
  *       only ones whose changes a retry alters; "all" recomputes every
  *       particle as the reference does; both give the same results;
- *   "pdl": PBF: true (default) launches the substep's kernels with
- *       programmatic dependent launch (each starts as the previous one
- *       exits, results unchanged); false launches them plainly;
+ *   "pdl": PBF: true (default) launches the substep's kernels, and those of
+ *       the differentiable adjoint, with programmatic dependent launch (each
+ *       starts as the previous one exits, results unchanged); false launches
+ *       them plainly;
  *   "stageTimers": true records CUDA-event stage times. */
 VTP_API int vtp_solver_set_config(vtp_solver *s, const char *json_text);
 

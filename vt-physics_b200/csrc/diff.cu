@@ -134,6 +134,7 @@ struct AdjArgs {
 
 // Attach order -> this substep's rows; abar = xbar dt + vbar (XSPH output adjoint).
 __global__ void k_adj_gather(AdjArgs a) {
+    pdl_enter();
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const uint32_t id = a.orig[r];
@@ -145,6 +146,7 @@ __global__ void k_adj_gather(AdjArgs a) {
 
 // XSPH adjoint; epilogue: Delta-bar of the last constraint iteration.
 __global__ void __launch_bounds__(256) k_adj_xsph(AdjArgs a) {
+    pdl_enter();
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     double kl = 0.0;
     if (r < a.nf) {
@@ -193,6 +195,7 @@ __global__ void __launch_bounds__(256) k_adj_xsph(AdjArgs a) {
 
 // Constraint iteration adjoint, pass A: lambda-bar -> s2-bar, rho-bar; G recomputed.
 __global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
+    pdl_enter();
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const float4 p = a.x[r], di = a.Dcur[r];
@@ -226,6 +229,7 @@ __global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
 // Constraint iteration adjoint, pass B: xbar of the iteration's input positions;
 // epilogue: Delta-bar of the previous iteration.
 __global__ void __launch_bounds__(256) k_adj_dx(AdjArgs a) {
+    pdl_enter();
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const float4 p = a.x[r], di = a.Dcur[r], Ai = a.A2[r];
@@ -281,6 +285,7 @@ __global__ void __launch_bounds__(256) k_adj_dx(AdjArgs a) {
 
 // External force adjoint, then this substep's rows -> attach order.
 __global__ void k_adj_force_scatter(AdjArgs a) {
+    pdl_enter();
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nf) return;
     const uint32_t id = a.orig[r];
@@ -290,6 +295,7 @@ __global__ void k_adj_force_scatter(AdjArgs a) {
 }
 
 __global__ void k_adj_kreduce(const double *part, uint32_t nb, double *acc) {
+    pdl_enter();
     double s = 0.0;
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
     s = block_sum_d(s);
@@ -535,7 +541,9 @@ int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *d
         if ((rc = restore_fluid(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
         for (uint32_t t = 0; t < k; ++t)
             if ((rc = s->enqueue_pbf_substep(s->st, &d.tape[t]))) return rc;
-        // Adjoint substeps, last to first.
+        // Adjoint substeps, last to first (programmatic launch between their kernels, as in
+        // the forward substep).
+        const vtp::PdlScope pdl_scope(s->pdl);
         for (int t = (int)k - 1; t >= 0 && nf; --t) {
             const PbfTapeSlot &T = d.tape[t];
             vtp::AdjArgs a{};
@@ -548,20 +556,20 @@ int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *d
             int cur = 0;
             a.x = T.x[I];
             a.Dcur = d.D[cur];
-            vtp::k_adj_gather<<<G, 256, 0, s->st>>>(a);
-            vtp::k_adj_xsph<<<G, 256, 0, s->st>>>(a);
-            vtp::k_adj_kreduce<<<1, 256, 0, s->st>>>(d.kpart, G, d.kacc);
+            vtp::launch(vtp::k_adj_gather, G, 256, 0, s->st, a);
+            vtp::launch(vtp::k_adj_xsph, G, 256, 0, s->st, a);
+            vtp::launch(vtp::k_adj_kreduce, 1, 256, 0, s->st, d.kpart, G, d.kacc);
             for (int it = I - 1; it >= 0; --it) {
                 a.x = T.x[it];
                 a.lam = T.lam[it];
                 a.rho = T.rho[it];
                 a.Dcur = d.D[cur];
                 a.Dnext = d.D[cur ^ 1];
-                vtp::k_adj_lambda<<<G, 256, 0, s->st>>>(a);
-                vtp::k_adj_dx<<<G, 256, 0, s->st>>>(a);
+                vtp::launch(vtp::k_adj_lambda, G, 256, 0, s->st, a);
+                vtp::launch(vtp::k_adj_dx, G, 256, 0, s->st, a);
                 cur ^= 1;
             }
-            vtp::k_adj_force_scatter<<<G, 256, 0, s->st>>>(a);
+            vtp::launch(vtp::k_adj_force_scatter, G, 256, 0, s->st, a);
         }
     }
     CU(cudaGetLastError());
