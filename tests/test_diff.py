@@ -106,6 +106,27 @@ def test_gpu_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib, lanes):
 
 
 @pytest.mark.gpu
+def test_gpu_adjoint_same_with_and_without_programmatic_launch(vtp_gpu):
+    """Programmatic dependent launch ("pdl") between the forward and adjoint
+    kernels changes when blocks start, not what they read: the forward state
+    and every gradient are bit-identical with it on and off."""
+    from vtp import diff
+    sc = small_case(10)
+    mask = diff.fluid_mask(sc)
+    out = []
+    for pdl in (True, False):
+        s = diff.pbf_solver(sc, extra={"pdl": pdl})
+        diff.diff_forward(s, 8, 3)
+        pos = s.get_field("pos")
+        _, dl = loss_grad(pos, mask, TARGET)
+        out.append((pos, diff.diff_backward(s, dl.astype(np.float32), None)))
+        s.destroy()
+    (pa, (xa, va, ka)), (pb, (xb, vb, kb)) = out
+    assert np.array_equal(pa, pb)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb) and ka == kb
+
+
+@pytest.mark.gpu
 def test_gpu_adjoint_independent_of_checkpoint_interval(vtp_gpu):
     from vtp import diff
     sc = small_case(9)
