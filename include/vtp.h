@@ -362,9 +362,10 @@ VTP_API int vtp_solver_dfsph_solve_backward(vtp_solver *s, const float *vbar_out
 /* Allocation-free neighbour search (no counterpart in the reference).
  *
  * For callers that cannot call cudaMalloc when they need neighbour lists:
- * code recording a CUDA graph by stream capture, hosts that give this
- * library a fixed memory budget managed by their own allocator, real-time
- * loops that forbid allocation after start-up.  Inputs and outputs are the
+ * hosts that give this library a fixed memory budget managed by their own
+ * allocator, and real-time loops that forbid allocation after start-up
+ * (an allocation can block on the driver and fail under fragmentation at a
+ * moment the caller cannot recover from).  Inputs and outputs are the
  * caller's device buffers: d_pos (n x float[3], any order), d_counts[n] and
  * d_nbrs[n * max_nbr] in the layout of vtp_solver_get_neighbors (self first,
  * then the 27 cells in the reference's order, ascending index inside a cell,
@@ -375,11 +376,14 @@ VTP_API int vtp_solver_dfsph_solve_backward(vtp_solver *s, const float *vbar_out
  * which limits n to VTP_NOALLOC_MAX_PARTICLES and the grid to
  * VTP_NOALLOC_MAX_CELLS cell buckets; larger inputs return VTP_ERR_BOUNDS.
  * The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
- * and the call returns without waiting.  The first call on a device looks
- * up the array's device address; make that first call before any stream
- * capture.  Every call on a device shares the array, so calls whose GPU work
- * overlaps (other streams, unsynchronised threads) race: order them on one
- * stream. */
+ * and the call returns without waiting.  Every call looks up the array's
+ * device address on the current device (a lookup, not an allocation), so a
+ * device reset that reloads the library's device code is followed; the
+ * first call on a device (and the first after a reset) also loads that code
+ * and the array: make that first call before any stream capture.  Every
+ * call on a device shares the array and it keeps the last call's contents,
+ * so calls whose GPU work overlaps (other streams, unsynchronised threads)
+ * race: order them on one stream. */
 #define VTP_NOALLOC_MAX_PARTICLES 1048576u
 #define VTP_NOALLOC_MAX_CELLS 2097152u
 #define VTP_NOALLOC_SCRATCH_BYTES 50336512ull

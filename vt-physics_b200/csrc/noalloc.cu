@@ -2,10 +2,10 @@
 // library as one call that allocates nothing.
 //
 // Some callers cannot call cudaMalloc at the moment they need neighbour lists:
-// code running while a CUDA stream is being captured into a graph (allocation
-// is not a capturable operation), hosts that hand the GPU to this library
-// under a fixed memory budget with their own pool allocator, and real-time
-// loops that forbid allocation after start-up.  They pass device buffers for
+// hosts that hand the GPU to this library under a fixed memory budget with
+// their own pool allocator, and real-time loops that forbid allocation after
+// start-up (cudaMalloc may synchronise the device and can fail under
+// fragmentation in the middle of a frame).  They pass device buffers for
 // the input positions and the output lists; everything else the search needs
 // lives in the fixed scratch arena below, which every GPU that loads this
 // library holds until the process exits.
@@ -15,7 +15,6 @@
 // ordering) corrupt each other's scratch.  Calls are ordered on one stream.
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/vtp.h"
@@ -69,23 +68,19 @@ Arena arena_at(unsigned char *base) {
     return a;
 }
 
-// Device address of the arena, looked up once per device (host code may not
-// use the symbol itself as a device address).
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char *g_base[kMaxDevices] = {nullptr};
-
-int arena_base(int dev, unsigned char **out) {
-    if (dev < 0 || dev >= kMaxDevices) return vtp::fail(VTP_ERR_BOUNDS, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_base[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return vtp::fail(VTP_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        g_base[dev] = (unsigned char *)p;
-    }
-    *out = g_base[dev];
+// Device address of the arena on the current device.  In host code the
+// symbol is a host-side stand-in, not a device address, so the address comes
+// from cudaGetSymbolAddress.  It is looked up on every call rather than
+// cached: after cudaDeviceReset (or in a new context on the same device) the
+// module is loaded again and the array can sit at another address, and a
+// cached pointer would then send the kernels into freed memory.  The lookup
+// allocates nothing; only the first one in a context loads the module.
+int arena_base(unsigned char **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return vtp::fail(VTP_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    *out = (unsigned char *)p;
     return VTP_OK;
 }
 
@@ -264,15 +259,27 @@ extern "C" VTP_API int vtp_ugns_neighbors_noalloc(const float *d_pos, uint32_t n
         return vtp::fail(VTP_ERR_BOUNDS, "vtp_ugns_neighbors_noalloc: " + std::to_string(n) +
                                              " particles exceed the scratch limit of " +
                                              std::to_string(kMaxParticles));
-    if (!(cell > 0.f) || max_nbr < 1 || max_nbr > 1024)
-        return vtp::fail(VTP_ERR_ARG, "cell must be > 0 and max_nbr in [1, 1024]");
+    if (!(cell > 0.f) || !std::isfinite(cell) || max_nbr < 1 || max_nbr > 1024)
+        return vtp::fail(VTP_ERR_ARG, "cell must be finite and > 0, and max_nbr in [1, 1024]");
+    for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(lb[a]) || !std::isfinite(size[a]) || !(size[a] > 0.f))
+            return vtp::fail(VTP_ERR_ARG, "vtp_ugns_neighbors_noalloc: lb must be finite and size finite and > 0");
+    // Cells per axis, checked before the integer conversion (a tiny cell would
+    // otherwise overflow int).
+    double cells[3];
+    for (int a = 0; a < 3; ++a) {
+        cells[a] = std::ceil((double)(size[a] / cell));
+        if (!(cells[a] >= 1.0) || cells[a] > (double)kMaxKeys)
+            return vtp::fail(VTP_ERR_BOUNDS, "vtp_ugns_neighbors_noalloc: grid of " +
+                                                 std::to_string(cells[a]) + " cells along one axis exceeds the "
+                                                 "scratch limit of " + std::to_string(kMaxKeys) + " cell buckets");
+    }
     vtp::Grid g{};
     g.lbx = lb[0]; g.lby = lb[1]; g.lbz = lb[2];
     g.cell = cell;
-    g.gx = (int)std::ceil(size[0] / cell);
-    g.gy = (int)std::ceil(size[1] / cell);
-    g.gz = (int)std::ceil(size[2] / cell);
-    if (g.gx <= 0 || g.gy <= 0 || g.gz <= 0) return vtp::fail(VTP_ERR_ARG, "empty grid");
+    g.gx = (int)cells[0];
+    g.gy = (int)cells[1];
+    g.gz = (int)cells[2];
     const uint64_t maxkey = (uint64_t)g.gz * g.gy * g.gx + (uint64_t)g.gy * g.gx + g.gx;
     if (maxkey + 2 > kMaxKeys)
         return vtp::fail(VTP_ERR_BOUNDS, "vtp_ugns_neighbors_noalloc: grid of " + std::to_string(maxkey + 2) +
@@ -282,12 +289,10 @@ extern "C" VTP_API int vtp_ugns_neighbors_noalloc(const float *d_pos, uint32_t n
     g.d2max = sqrt_limit(cell);
     g.maxnbr = max_nbr;
     if (n == 0) return VTP_OK;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return vtp::fail(VTP_ERR_CUDA, cudaGetErrorString(e));
     unsigned char *base = nullptr;
-    int rc = arena_base(dev, &base);
+    const int rc = arena_base(&base);
     if (rc) return rc;
+    cudaError_t e;
     const Arena a = arena_at(base);
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nb = g.nkey + 1;
