@@ -48,6 +48,8 @@ def scene_for(case: str):
         return scenes.dam_break("DFSPH", 8000, seed=22)
     if case.startswith("dfsph_1m"):
         return scenes.dfsph_1m()
+    if case.startswith("immct_500k"):
+        return scenes.immct_500k()
     if case == "immct_small":
         return scenes.layered_mixture("IMMCT", 24, seed=31)
     if case == "imm_small":
@@ -71,7 +73,19 @@ CASES = {
     "imm_small": ([0, 1, 2, 5], False),
     "immct_small_notension": ([0, 1, 2, 5], False),
     "imm_small_notension": ([0, 1, 2, 5], False),
+    # the benchmark scenes themselves: per-particle fields on a fixed seeded
+    # subsample of fluid rows (SUBSAMPLE rows, in attach order), lists as digests
+    "dfsph_1m_steps": ([0, 1, 3], False),
+    "immct_500k_step": ([0, 1], False),
 }
+# Fluid rows kept per tick for the large cases: (count, seed of the choice).
+SUBSAMPLE = {"dfsph_1m_steps": (32768, 2025), "immct_500k_step": (32768, 3025)}
+
+
+def subsample(case: str, n_fluid: int):
+    """Sorted fluid-row indices (attach order among fluid rows) stored for a large case."""
+    k, seed = SUBSAMPLE[case]
+    return np.sort(np.random.default_rng(seed).choice(n_fluid, size=k, replace=False)).astype(np.int64)
 
 
 def run_case(case: str, out_dir: Path):
@@ -87,6 +101,14 @@ def run_case(case: str, out_dir: Path):
     req = sc.config[sc.solver]["Required"]
     nfo = sum(1 for o in sc.objects if o.material == 0)
     iters = []
+    sub = subsample(case, int(fm.sum())) if case in SUBSAMPLE else None
+    if sub is not None:
+        arrays["sub_idx"] = sub.astype(np.int32)
+
+    def fl(a):
+        """Fluid rows of a per-particle field (the stored subsample for the large cases)."""
+        a = a[fm]
+        return a if sub is None else a[sub]
     s.take_means()
     for t in ticks:
         while done < t:
@@ -110,11 +132,15 @@ def run_case(case: str, out_dir: Path):
             arrays[f"cell_ids_{t}"] = s.get("cellIndices", 1, np.uint32)
         big = case == "dfsph_1m_ugns"
         if t > 0 and not big:
-            arrays[f"pos_{t}"] = s.get("pos", 3)[fm]
-            arrays[f"vel_{t}"] = s.get("vel", 3)[fm]
+            arrays[f"pos_{t}"] = fl(s.get("pos", 3))
+            arrays[f"vel_{t}"] = fl(s.get("vel", 3))
         if t == 0:
             vol = s.get("volume")
-            if big:
+            if sub is not None:
+                vb = vol[~fm].astype(np.float64)
+                arrays["volume_0_boundary_stats"] = np.array([vb.sum(), vb.min(), vb.max()])
+                arrays["volume_0_fluid"] = fl(vol)
+            elif big:
                 vb = vol[~fm].astype(np.float64)
                 arrays["volume_0_boundary_stats"] = np.array([vb.sum(), vb.min(), vb.max()])
             else:
@@ -122,15 +148,21 @@ def run_case(case: str, out_dir: Path):
                 if sc.solver == "PBF":
                     arrays["mass_0"] = s.get("mass")
         if sc.solver == "PBF" and t > 0:
-            arrays[f"density_{t}"] = s.get("density_sph")[fm]
+            arrays[f"density_{t}"] = fl(s.get("density_sph"))
         if sc.solver != "PBF" and t > 0 and case != "dfsph_1m_ugns":
-            arrays[f"ratio_{t}"] = s.get("compression_ratio")[fm]
+            arrays[f"ratio_{t}"] = fl(s.get("compression_ratio"))
         if sc.solver in ("IMM", "IMMCT") and t > 0:
             P = len(req["phaseRestDensity"])
-            arrays[f"frac_{t}"] = s.get("vol_frac", P)[fm]
+            arrays[f"frac_{t}"] = fl(s.get("vol_frac", P))
             if sc.solver == "IMMCT":
-                arrays[f"Q_{t}"] = s.get("Q", 9)[fm]
-                arrays[f"cd_{t}"] = s.get("Cd")[fm]
+                arrays[f"Q_{t}"] = fl(s.get("Q", 9))
+                arrays[f"cd_{t}"] = fl(s.get("Cd"))
+        if sub is not None and t > 0:
+            # whole-scene statistics in FP64: kinetic energy (sum |v|^2) and per-phase volume
+            v = s.get("vel", 3)[fm].astype(np.float64)
+            arrays[f"sum_v2_{t}"] = np.array([np.sum(v * v)])
+            if sc.solver in ("IMM", "IMMCT"):
+                arrays[f"phase_sum_{t}"] = s.get("vol_frac", P)[fm].astype(np.float64).sum(0)
     if iters:
         arrays["iters"] = np.array(iters, np.int32)
     rec["ticks"] = ticks

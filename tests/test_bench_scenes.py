@@ -1,0 +1,162 @@
+"""GPU parity on the benchmark scenes themselves, against the FP64 CPU oracle.
+
+  * DFSPH 1M (1,000,000 fluid + 453,957 boundary): the first substep from the
+    seeded lattice, and substep 11 started from the library's own state (the
+    oracle takes over the library's positions and velocities after 10
+    substeps), each with the benchmark window's iteration counts forced (3
+    divergence, 1 density iteration), every fluid particle, error per field;
+  * IMM-CT 500k: one substep, every fluid particle: positions, velocities,
+    volume fractions, conformation tensor, Cd;
+  * differentiable PBF 64k (64,000 fluid + 51,365 boundary, 200 substeps,
+    checkpoints every 20): the adjoint's directional derivatives against FP64
+    central finite differences on 32 random unit directions in (v0, XSPH_k),
+    neighbour lists frozen to the GPU's; target 1e-3 relative.
+
+Bars: positions 1e-5 relative; velocities 1e-4 against FP64 for the
+pressure-solved schemes (the FP32 rounding of ratio - 1 ~ 0 is amplified
+~1e3 times in kappa; the reference's own FP32 build is as far from FP64);
+error of a field = max|a - b| / max(max|b|, floor), velocity floor
+1e-3 * spacing / dt.
+"""
+import numpy as np
+import pytest
+
+from util import fluid_mask, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+TOL_VEL_FP64 = 1e-4
+
+
+def _vel_floor(sc):
+    req = sc.config[sc.solver]["Required"]
+    return 1e-3 * 2 * req["particleRadius"] / req["timeStep"]
+
+
+def _dfsph_errors(s, o, sc, fm):
+    ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+    ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+    er = rel_err(s.get_field("density")[fm], o.ratio[fm])
+    ea = rel_err(s.get_field("alpha")[fm], o.alpha[fm])
+    return ep, ev, er, ea
+
+
+def test_dfsph_1m_first_substep_matches_fp64_oracle(vtp_gpu, oracle_lib):
+    """The first substep from the seeded lattice, 3 divergence and 1 density
+    iteration forced, every fluid particle."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.dfsph_1m()
+    s = vtp.solver_from_scene(sc, extra={"forceDivIterations": 3, "forceIncompIterations": 1})
+    o = oracle_lib.OracleSolver(sc, force_div=3, force_inc=1)
+    assert s.initialize()
+    fm = fluid_mask(sc)
+    assert fm.sum() == 1_000_000
+    assert rel_err(s.get_field("volume"), o.vol) < TOL
+    assert s.tickNsteps(1), s.last_error
+    o.step(1)
+    ep, ev, er, ea = _dfsph_errors(s, o, sc, fm)
+    print(f"DFSPH 1M substep 1: library vs FP64 oracle: pos {ep:.2e} vel {ev:.2e} ratio {er:.2e} alpha {ea:.2e}")
+    assert ep < TOL and ev < TOL_VEL_FP64 and er < TOL and ea < 1e-4
+    st = s.stats()
+    assert st["last_div_iters"] == 3 and st["last_incomp_iters"] == 1
+    s.destroy()
+
+
+@pytest.mark.parametrize("staged", [False, True])
+def test_dfsph_1m_substep_in_the_bench_window_matches_fp64_oracle(vtp_gpu, oracle_lib, staged):
+    """Substep 11 of the benchmark scene: the library runs 10 substeps with its
+    own stop test, the FP64 oracle takes over the library's state (positions
+    and velocities of every particle), and both advance one substep with 3
+    divergence and 1 density iteration forced; every fluid particle."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.dfsph_1m()
+    warm = 10
+    force = [[0, 0]] * warm + [[3, 1]]   # 0: the residual test decides
+    s = vtp.solver_from_scene(sc, extra={"forceIterationsPerTick": force, "stagedSolve": staged})
+    assert s.tickNsteps(warm), s.last_error
+    fm = fluid_mask(sc)
+    o = oracle_lib.OracleSolver(sc, force_div=3, force_inc=1)
+    o.pos[:] = s.get_field("pos").astype(np.float64)
+    o.vel[:] = s.get_field("vel").astype(np.float64)
+    assert s.tickNsteps(1), s.last_error
+    o.step(1)
+    ep, ev, er, ea = _dfsph_errors(s, o, sc, fm)
+    st = s.stats()
+    print(f"DFSPH 1M substep {warm + 1} (staged {staged}): library vs FP64 oracle from the library's state: "
+          f"pos {ep:.2e} vel {ev:.2e} ratio {er:.2e} alpha {ea:.2e}")
+    assert st["last_div_iters"] == 3 and st["last_incomp_iters"] == 1
+    assert ep < TOL and ev < TOL_VEL_FP64 and er < TOL and ea < 1e-4
+    s.destroy()
+
+
+def test_immct_500k_substep_matches_fp64_oracle(vtp_gpu, oracle_lib):
+    vtp = vtp_gpu
+    sc = vtp.scenes.immct_500k()
+    s = vtp.solver_from_scene(sc, extra={"forceDivIterations": 2, "forceIncompIterations": 2})
+    o = oracle_lib.ImmOracle(sc, force_div=2, force_inc=2)
+    assert s.initialize()
+    fm = fluid_mask(sc)
+    assert fm.sum() == 500_000
+    assert rel_err(s.get_field("volume"), o.vol) < TOL
+    assert s.tickNsteps(1), s.last_error
+    o.step(1)
+    ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+    ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+    ef = rel_err(s.get_field("vol_frac")[fm].reshape(-1), o.frac[fm].reshape(-1))
+    eq = rel_err(s.get_field("conformation")[fm].reshape(-1), o.Q[fm].reshape(-1))
+    ec = rel_err(s.get_field("cd")[fm], o.cd[fm])
+    print(f"IMM-CT 500k t=1: library vs FP64 oracle: pos {ep:.2e} vel {ev:.2e} frac {ef:.2e} Q {eq:.2e} Cd {ec:.2e}; "
+          f"retries gpu {s.stats()['phase_retries']} oracle {o.last.retries}")
+    assert ep < TOL and ev < TOL_VEL_FP64 and ef < TOL and eq < TOL and ec < TOL
+    s.destroy()
+
+
+FD_SUBSTEPS = 200
+FD_DIRECTIONS = 32
+
+
+def test_diff_pbf_64k_adjoint_matches_fd_32_directions(vtp_gpu, oracle_lib):
+    """The benchmark's differentiable-PBF check at its own size and horizon."""
+    from vtp import diff
+    sc = vtp_gpu.scenes.diff_pbf()
+    mask = diff.fluid_mask(sc)
+    nf = int(mask.sum())
+    assert nf == 64_000
+    target = np.array([0.8, 0.2, 0.6])
+    T = FD_SUBSTEPS
+    s = diff.pbf_solver(sc)
+    maxnbr = int(sc.config["PBF"]["Required"]["maxNeighborNum"])
+    diff.diff_forward(s, T, 20, keep_lists=True)
+    lists = [diff.diff_lists(s, t, maxnbr) for t in range(T)]
+    xT = s.get_field("pos")
+    m = xT[mask].astype(np.float64).mean(0)
+    g = np.zeros(xT.shape, np.float32)
+    g[mask] = 2.0 * (m - target) / nf
+    _, gv, gk = diff.diff_backward(s, g, None)
+    s.destroy()
+
+    d = oracle_lib.PbfDiff(sc)
+    x0, v0 = d.base.pos.copy(), d.base.vel.copy()
+    rng = np.random.default_rng(5006)
+    k0 = d.p.xsph_k
+    errs = []
+    for _ in range(FD_DIRECTIONS):
+        dv = np.zeros_like(v0)
+        dv[mask] = rng.normal(size=(nf, 3))
+        dk = rng.normal()
+        nrm = np.sqrt((dv ** 2).sum() + dk * dk)
+        dv, dk = dv / nrm, dk / nrm
+
+        def L(e):
+            d.p.xsph_k = k0 + e * dk
+            x, _, _, _ = d.rollout(x0, v0 + e * dv, T, lists=lists)
+            d.p.xsph_k = k0
+            mm = x[mask].mean(0)
+            return float(((mm - target) ** 2).sum())
+        fd = (L(1e-4) - L(-1e-4)) / 2e-4
+        ad = float((gv.astype(np.float64) * dv).sum() + gk * dk)
+        errs.append(abs(ad - fd) / abs(fd))
+    print(f"diff PBF 64k, {T} substeps, {FD_DIRECTIONS} directions: max rel err {max(errs):.2e}, "
+          f"median {float(np.median(errs)):.2e}")
+    assert max(errs) < 1e-3
