@@ -260,6 +260,33 @@ VTP_API int vtp_generate_cube(float radius, const float lb[3], const float size[
 VTP_API int vtp_generate_box(float radius, const float lb[3], const float size[3], int32_t layers, float *d_out,
                              uint32_t capacity, uint32_t *count, void *stream);
 
+/* Particle geometry on the host (no device work).
+ *
+ * vtp_generate_particles replaces ModelHandler::generateObjectElements
+ * (Simulator/Library/Source/Model/ModelHandler.cpp:13-175): config_json is
+ * the generator config an object component builds ("genType" 1 sphere
+ * {particleRadius, volumeCenter, volumeRadius}, 2 cube {particleRadius, lb,
+ * size}, 3 cylinder {particleRadius, center, bottomAreaRadius, height},
+ * 4 plane {particleRadius, lb, size, layerNum}, 5 box {particleRadius, lb,
+ * size, layerNum}); the positions are the reference's bit for bit, in its
+ * order, as n x float[3] into `out` (host memory, `capacity` particles).
+ * With out == NULL only *count is set.  Unknown genType: VTP_ERR_CONFIG.
+ *
+ * vtp_read_ply replaces ModelHandler::load_PLY_ParticleElements
+ * (ModelHandler.cpp:207-228): every vertex of the PLY file at `path`
+ * (ASCII or binary, float or double coordinates) is one particle, x y z in
+ * file order.  With out == NULL only *count is set.
+ *
+ * vtp_write_ply replaces ExportUtil::exportAsPly (ExportUtil.cpp:28-88): the
+ * ASCII PLY "x y z [r g b] [p1 .. pk]" with the default iostream float
+ * format, written to dir + "/" + name + ".ply" (directories created; the
+ * reference joins with a backslash).  color (n x 3) and phase (n x n_phase)
+ * may be NULL. */
+VTP_API int vtp_generate_particles(const char *config_json, float *out, uint64_t capacity, uint64_t *count);
+VTP_API int vtp_read_ply(const char *path, float *out, uint64_t capacity, uint64_t *count);
+VTP_API int vtp_write_ply(const char *dir, const char *name, const float *pos, uint64_t n, const float *color,
+                          const float *phase, int32_t n_phase);
+
 /* Trajectory statistics that long runs are compared by (no counterpart call in the
  * reference, which has no such diagnostics): the FP64 sums of
  * vtp_conservation over the fluid of scene `scene` (-1: every scene of the

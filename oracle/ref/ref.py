@@ -36,6 +36,9 @@ def lib() -> C.CDLL:
         L.ref_take_means.argtypes = [P, C.c_uint32]
         L.ref_take_means.restype = C.c_uint32
         L.ref_destroy.argtypes = [C.c_int]
+        L.ref_generate.argtypes = [C.c_char_p, P, C.c_int64]
+        L.ref_generate.restype = C.c_int64
+        L.ref_export_ply.argtypes = [C.c_char_p, C.c_char_p, P, C.c_int64, P, P, C.c_int]
         _lib = L
     return _lib
 
@@ -144,3 +147,52 @@ def split_iterations(means: np.ndarray, n_fluid_objects: int, div_thr: float, in
                 break
         iters.append(it)
     return iters[0], iters[1], pos == len(vals)
+
+
+def split_ticks(means: np.ndarray, n_fluid_objects: int, div_thr: float, inc_thr: float):
+    """(div_iters, incomp_iters) of every tick in a run of consecutive ticks, from the
+    cal_mean values recorded over them (each tick runs both loops at least once, so the
+    sequence splits unambiguously; the same stop rule as split_iterations)."""
+    k = n_fluid_objects
+    vals = [float(np.float32(np.sum(means[i:i + k], dtype=np.float32) / np.float32(k)))
+            for i in range(0, len(means), k)]
+    out, pos = [], 0
+    while pos < len(vals):
+        tick = []
+        for thr in (div_thr, inc_thr):
+            it = 0
+            while pos < len(vals):
+                it += 1
+                v = vals[pos]
+                pos += 1
+                if v < thr or it > 100:
+                    break
+            tick.append(it)
+        out.append(tuple(tick))
+    return out
+
+
+def generate(config: dict) -> np.ndarray:
+    """ModelHandler::generateObjectElements of the reference build (host code) -> (n, 3) float32."""
+    cfg = json.dumps(config).encode()
+    n = lib().ref_generate(cfg, None, 0)
+    if n < 0:
+        raise RuntimeError("ref_generate: bad config")
+    out = np.empty((n, 3), np.float32)
+    if n:
+        lib().ref_generate(cfg, out.ctypes.data, n)
+    return out
+
+
+def export_ply(directory: str, name: str, pos, color=None, phase=None):
+    """ExportUtil::exportData of the reference build; returns the path it wrote
+    (the reference joins directory and name with a backslash)."""
+    p = np.ascontiguousarray(pos, np.float32)
+    c = None if color is None else np.ascontiguousarray(color, np.float32)
+    ph = None if phase is None else np.ascontiguousarray(phase, np.float32)
+    nph = 0 if ph is None else ph.shape[1]
+    rc = lib().ref_export_ply(str(directory).encode(), name.encode(), p.ctypes.data, p.shape[0],
+                              None if c is None else c.ctypes.data, None if ph is None else ph.ctypes.data, nph)
+    if rc != 0:
+        raise RuntimeError("ref_export_ply failed")
+    return f"{directory}\\{name}.ply"

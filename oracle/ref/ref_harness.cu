@@ -33,6 +33,8 @@
 #undef protected
 #include "Framework/Object.hpp"
 #include "Framework/ObjectComponents.hpp"
+#include "Model/ExportUtil.hpp"
+#include "Model/ModelHandler.hpp"
 
 using json = nlohmann::json;
 
@@ -287,6 +289,44 @@ uint32_t ref_take_means(float *out, uint32_t cap) {
 }
 
 uint32_t ref_means_pending(void) { return (uint32_t)g_means.size(); }
+
+// ModelHandler::generateObjectElements (ModelHandler.cpp:13-41) for a generator config
+// (genType 1 sphere, 2 cube, 3 cylinder, 4 plane, 5 box): writes up to `cap` particles
+// (x, y, z) into `out` and returns the count, or -1 on a bad config.  Host code only.
+int64_t ref_generate(const char *cfg_json, float *out, int64_t cap) {
+    json c;
+    try {
+        c = json::parse(cfg_json);
+    } catch (...) {
+        return -1;
+    }
+    const std::vector<float3> v = VT_Physics::ModelHandler::generateObjectElements(c);
+    for (int64_t i = 0; out && i < (int64_t)v.size() && i < cap; ++i) {
+        out[3 * i] = v[i].x;
+        out[3 * i + 1] = v[i].y;
+        out[3 * i + 2] = v[i].z;
+    }
+    return (int64_t)v.size();
+}
+
+// ExportUtil::exportData (ExportUtil.cpp:9-88) of n particles: positions, optional colors
+// (n x 3) and phase fractions (n x nphase), to the path that function forms from `dir` and
+// `name` (directory, a backslash, name, ".ply").  Host code only.
+int ref_export_ply(const char *dir, const char *name, const float *pos, int64_t n, const float *color,
+                   const float *phase, int nphase) {
+    json c = {{"Common", {{"exportTargetDir", dir}, {"exportFilePrefix", name}, {"exportFileType", "PLY"}}}};
+    if (phase) c["Common"]["exportPhaseNum"] = nphase;
+    std::vector<float3> p((size_t)n), col;
+    std::vector<float> ph;
+    for (int64_t i = 0; i < n; ++i) p[i] = make_float3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    if (color) {
+        col.resize((size_t)n);
+        for (int64_t i = 0; i < n; ++i) col[i] = make_float3(color[3 * i], color[3 * i + 1], color[3 * i + 2]);
+    }
+    if (phase) ph.assign(phase, phase + n * nphase);
+    VT_Physics::ExportUtil::exportData(c, p, col, ph);
+    return 0;
+}
 
 int ref_destroy(int h) {
     Entry *e = get(h);

@@ -62,3 +62,68 @@ def test_cpp_program_matches_python_api(vtp_gpu, example, kind):
     s.destroy()
     assert (out["fluid"], out["boundary"]) == (fluid.shape[0], wall.shape[0])
     assert np.allclose(out["mean"], mean, rtol=1e-8, atol=0)
+
+
+_GEOMETRY_PROGRAM = r"""
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include "Framework/Object.hpp"
+using namespace VT_Physics;
+int main(int argc, char **argv) {
+    // argv[1]: output file; argv[2]: a PLY file for the particle-file object
+    std::ofstream out(argv[1], std::ios::binary);
+    auto dump = [&](Object &o) {
+        if (!o.update()) { std::fprintf(stderr, "update failed\n"); std::exit(1); }
+        auto e = o.getObjectComponent()->getElements();
+        uint64_t n = e.size() / 3;
+        out.write((const char *)&n, 8);
+        out.write((const char *)e.data(), e.size() * 4);
+    };
+    Object sphere(Particle_Sphere);
+    sphere.getObjectComponentConfig() = {{"particleRadius", 0.01}, {"volumeCenter", {0.5, 0.5, 0.5}}, {"volumeRadius", 0.2}};
+    dump(sphere);
+    Object cyl(Particle_Cylinder);
+    cyl.getObjectComponentConfig() = {{"particleRadius", 0.01}, {"center", {0.5, 0.5, 0.5}},
+                                      {"bottomAreaRadius", 0.2}, {"height", 0.3}};
+    dump(cyl);
+    Object plane(Particle_Plane);
+    plane.getObjectComponentConfig() = {{"particleRadius", 0.01}, {"lb", {0, 0, 0}}, {"size", {1, 0.1, 1}}, {"layerNum", 2}};
+    dump(plane);
+    Object file(Particle_Common);
+    file.getObjectComponentConfig() = {{"particleRadius", 0.01}, {"particleGeometryPath", std::string(argv[2])}};
+    dump(file);
+    return 0;
+}
+"""
+
+
+def test_cpp_objects_generate_every_particle_type(tmp_path):
+    """Sphere, cylinder and plane objects and a Particle_Common object loaded from a PLY file
+    (the reference's ObjectComponents update paths) through the C++ host interface."""
+    sys.path.insert(0, str(PKG))
+    import build
+    from vtp import model
+    build.build()
+    src = tmp_path / "geometry.cpp"
+    src.write_text(_GEOMETRY_PROGRAM)
+    exe = build.build_host_program(src, tmp_path / "geometry")
+    pts = np.random.default_rng(3).uniform(-1, 1, (50, 3)).astype(np.float32)
+    ply = model.write_ply(tmp_path, "cloud", pts)
+    dump = tmp_path / "out.bin"
+    r = subprocess.run([str(exe), str(dump), str(ply)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    raw = dump.read_bytes()
+    got, off = [], 0
+    while off < len(raw):
+        n = int(np.frombuffer(raw[off:off + 8], np.uint64)[0])
+        got.append(np.frombuffer(raw[off + 8:off + 8 + 12 * n], np.float32).reshape(n, 3))
+        off += 8 + 12 * n
+    want = [model.generate({"genType": 1, "particleRadius": 0.01, "volumeCenter": [0.5, 0.5, 0.5], "volumeRadius": 0.2}),
+            model.generate({"genType": 3, "particleRadius": 0.01, "center": [0.5, 0.5, 0.5],
+                            "bottomAreaRadius": 0.2, "height": 0.3}),
+            model.generate({"genType": 4, "particleRadius": 0.01, "lb": [0, 0, 0], "size": [1, 0.1, 1], "layerNum": 2}),
+            model.read_ply(ply)]
+    assert len(got) == 4
+    for a, b in zip(got, want):
+        assert a.shape == b.shape and a.shape[0] > 0 and np.array_equal(a, b)

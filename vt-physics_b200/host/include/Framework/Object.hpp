@@ -1,10 +1,11 @@
 // Particle objects of the host interface: the same class and method names as
 // the reference's VT_Physics::Object (Simulator/Runtime/Include/Framework/
 // Object.hpp:15-48) and ObjectManager, so programs written against the
-// reference compile against this library.  Cube and box objects generate
-// their particles with the reference generators' arithmetic
-// (ModelHandler.cpp:43-67, 124-154): FP32 running sums from lb + r in steps
-// of 2r; Particle_Common objects take positions through setElements().
+// reference compile against this library.  Sphere, cube, cylinder, plane and
+// box objects generate their particles with the reference generators'
+// arithmetic (ModelHandler.cpp:43-175); Particle_Common objects take
+// positions through setElements() or, with "particleGeometryPath" in their
+// component config, from a PLY file (ModelHandler.cpp:177-228).
 #ifndef VTP_HOST_OBJECT_HPP
 #define VTP_HOST_OBJECT_HPP
 
@@ -21,8 +22,8 @@ namespace VT_Physics {
 
 using json = nlohmann::json;
 
-// Object types (the reference's eObjectType, ObjectComponents.hpp:17-31); the
-// particle generators cover Particle_Cube and Particle_Box.
+// Object types (the reference's eObjectType, ObjectComponents.hpp:17-31), all
+// with their particle generators.
 typedef enum eObjectType : uint8_t {
     Particle_Common = 0,
     Particle_Sphere = 1,
@@ -59,7 +60,7 @@ public:
     long long getID() const;
     void rename(std::string newName);
     std::string getName() const;
-    // Regenerates the particles of Cube / Box objects from the component config.
+    // Regenerates the particles from the component config (generators, or a PLY file).
     bool update();
     void reset();
 

@@ -82,9 +82,35 @@ bool Object::update() {
         if (a.size() != 3) throw std::runtime_error(std::string(k) + " needs 3 values");
         for (int i = 0; i < 3; ++i) v[i] = a[i];
     };
+    // Sphere, cylinder and plane objects, and particle objects with a PLY file, go through the
+    // library's host geometry calls (ModelHandler::generateObjectElements / loadObjectElements).
+    auto from_library = [&](bool ply) {
+        uint64_t n = 0;
+        const std::string arg = ply ? c.at("particleGeometryPath").get<std::string>() : [&] {
+            json g = c;
+            g["genType"] = (int)m_component.getType();
+            return g.dump();
+        }();
+        int rc = ply ? vtp_read_ply(arg.c_str(), nullptr, 0, &n) : vtp_generate_particles(arg.c_str(), nullptr, 0, &n);
+        std::vector<float> xyz(3 * n);
+        if (rc == VTP_OK && n)
+            rc = ply ? vtp_read_ply(arg.c_str(), xyz.data(), n, &n)
+                     : vtp_generate_particles(arg.c_str(), xyz.data(), n, &n);
+        if (rc != VTP_OK) {
+            std::fprintf(stderr, "[vtp] object %s: %s\n", m_name.c_str(), vtp_last_error());
+            return false;
+        }
+        m_component.m_pos = std::move(xyz);
+        return true;
+    };
     try {
         switch (m_component.getType()) {
-            case Particle_Common: return true;
+            case Particle_Common:
+                return c.contains("particleGeometryPath") ? from_library(true) : true;
+            case Particle_Sphere:
+            case Particle_Cylinder:
+            case Particle_Plane:
+                return from_library(false);
             case Particle_Cube: {
                 float lb[3], size[3];
                 vec3("lb", lb);

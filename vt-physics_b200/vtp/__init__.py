@@ -3,7 +3,7 @@
 The compute path is the sm_100a library ``libvtp.so`` behind the C ABI in
 ``include/vtp.h``; this package is its Python host mirror.
 """
-from . import scenes
+from . import model, scenes
 from ._lib import FIELDS, LIB_PATH, VtpError, lib, status_string
 from .solver import (DFSPH, EPM_BOUNDARY, EPM_FLUID, IMM, IMMCT, PBF, DFSPHSolver, HostBuffer, IMMCTSolver,
                      IMMSolver, Object,

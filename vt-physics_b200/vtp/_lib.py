@@ -59,6 +59,9 @@ SIGNATURES = {
                                     C.c_uint64, _P, C.c_uint32, C.POINTER(C.c_uint32), _P]),
     "vtp_generate_box": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, _P,
                                    C.c_uint32, C.POINTER(C.c_uint32), _P]),
+    "vtp_generate_particles": (C.c_int, [C.c_char_p, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "vtp_read_ply": (C.c_int, [C.c_char_p, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "vtp_write_ply": (C.c_int, [C.c_char_p, C.c_char_p, _P, C.c_uint64, _P, _P, C.c_int32]),
     "vtp_solver_get_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_set_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_get_neighbors": (C.c_int, [_P, _P, _P, C.c_uint32]),
