@@ -176,6 +176,7 @@ int vtp_solver::parse_config(const json &c) {
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
         block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0; row_lanes = 1;
+        cell_cull = false; staged_solve = false; stage_rows = 2048;
         cfl = 0.f;
         cell_order_brick = true;
         pbf_form = 0; pbf_eps = 1e-6f;
@@ -211,6 +212,11 @@ int vtp_solver::parse_config(const json &c) {
             row_lanes = b.value("rowLanes", 1);
             if (row_lanes != 1 && row_lanes != 4 && row_lanes != 8)
                 return fail(VTP_ERR_CONFIG, "rowLanes must be 1, 4 or 8");
+            cell_cull = b.value("cellCull", false);
+            staged_solve = b.value("stagedSolve", false);
+            stage_rows = b.value("stageRows", 2048);
+            if (stage_rows < 256 || stage_rows > (int)vtp::kStageMaxRows)
+                return fail(VTP_ERR_CONFIG, "stageRows must be in [256, 32767]");
             list_lanes = b.value("listLanes", 0);
             if (list_lanes != 0 && list_lanes != 1 && list_lanes != 8)
                 return fail(VTP_ERR_CONFIG, "listLanes must be 0 (by row count), 1 or 8");
@@ -386,6 +392,8 @@ vtp::DfsphArgs vtp_solver::dfsph_args(int which) {
     a.pk = pk;
     a.tick = d_tick;
     a.unroll = unroll;
+    a.staged = staged ? 1 : 0;
+    a.stg = stg;
     a.dtp = cfl > 0.f ? d_cfl : nullptr;
     a.vmax_bits = cfl > 0.f ? d_vmax : nullptr;
     return a;
@@ -396,7 +404,7 @@ vtp::SolveCtl vtp_solver::solve_ctl(int which, cudaGraphConditionalHandle hnd, i
     c.state = solve + (size_t)which * scenes.size();
     c.loop = loop + which;
     c.inv_count = inv_count;
-    c.scene_tiles = d_scene_tiles;
+    c.scene_tiles = staged ? d_scene_groups : d_scene_tiles;
     c.nscenes = nscenes();
     c.nobj_max = nobj_max;
     c.threshold = which == 0 ? div_thr : incomp_thr;
@@ -464,6 +472,7 @@ int vtp_solver::initialize() {
     }
     L.merge_mode = mode < 0 ? 0 : mode;
     L.list_lanes = list_lanes;
+    L.cell_cull = cell_cull;
 
     // Grids as UniformGirdNeighborSearcher::setConfig (UniformGridNeighborSearch.cpp:214-218),
     // one per scene, each followed by its own outside bucket.
@@ -663,7 +672,27 @@ int vtp_solver::initialize() {
         if (!tiles.empty())
             CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(d_scene_tiles, stl.data(), S * sizeof(vtp::SceneTiles), cudaMemcpyHostToDevice, st));
-        AL(&partials, (size_t)std::max<uint32_t>(ntiles, 1) * nobj_max + 1);
+        // Staged pressure solve: one scene in bricked order whose cells' fluid and boundary runs
+        // do not interleave; residual partials per cell group (plus one for the rows outside).
+        staged = staged_solve && type == VTP_SOLVER_DFSPH && S == 1 && scenes[0].grid.brick &&
+                 L.merge_mode != 2 && L.nf > 0;
+        size_t npart = std::max<uint32_t>(ntiles, 1);
+        if (staged) {
+            stg.ngroups = scenes[0].grid.nkey / vtp::kStageBuckets;
+            stg.scap = (uint32_t)stage_rows;
+            stg.mode = L.merge_mode;
+            stg.fstart = u.fstart;
+            stg.bstart = u.bstart;
+            const size_t fl_rows = ((size_t)L.nf + 31) / 32 * 32;
+            AL(&stg.snbr, fl_rows * L.ell_stride);
+            vtp::SceneTiles sg = stl[0];
+            sg.tile0 = 0;
+            sg.ntiles = stg.ngroups + 1;
+            AL(&d_scene_groups, 1);
+            CU(cudaMemcpyAsync(d_scene_groups, &sg, sizeof(sg), cudaMemcpyHostToDevice, st));
+            npart = std::max<size_t>(npart, (size_t)stg.ngroups + 1);
+        }
+        AL(&partials, npart * nobj_max + 1);
         if (type != VTP_SOLVER_DFSPH) {
             if ((rc = immct_alloc(*this))) return rc;
         }
@@ -818,8 +847,13 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
                    u, u.fstart, prof);
     pos.swap(); vel.swap(); orig.swap(); vadv.swap();
-    PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
-                                                   d_status, d_overflow, block));
+    if (staged) {
+        PROF(this, "ugns_lists", vtp::ugns_build_lists_staged(s, scn(), L, stg, pos.c(), u.nbr, u.ncnt, d_status,
+                                                              d_overflow));
+    } else {
+        PROF(this, "ugns_lists", vtp::ugns_build_lists(s, scn(), L, 0, L.nf, pos.c(), orig.c(), u, u.nbr, u.ncnt,
+                                                       d_status, d_overflow, block));
+    }
     PROF(this, "dfsph_ratio_alpha", vtp::dfsph_ratio_alpha(s, dfsph_args(), block));
     launches_per_tick += 8;  // neighbour search (7) + ratio/alpha
     if ((rc = enqueue_solve(s, 0, capture))) return rc;

@@ -177,6 +177,156 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
     }
 }
 
+// Staged solve_a: one block per brick (staged.h); the block copies the
+// packed {x, v*} rows of the group's neighbourhood into shared memory and each
+// row gathers through its slot list, in list order, so delta and kappa are
+// the bits the unstaged pass computes.  A group whose neighbourhood exceeds
+// the capacity, and the rows outside the grid (block ngroups), gather from
+// global memory.  The FP64 residual partials are per group.
+template <bool MULTI, int U>
+__global__ void __launch_bounds__(kStageBlock) k_solve_a_staged(DfsphArgs a) {
+    extern __shared__ float4 stage[];   // slot s = {stage[2s], stage[2s + 1]}
+    __shared__ GroupPlan P;
+    if (a.state[0].stopped) return;
+    const StepDt T = step_dt(a);
+    const uint32_t grp = blockIdx.x;
+    const SceneGrid g = a.sc.sg[0];
+    uint32_t r0, r1;
+    bool staged = false;
+    if (grp == a.stg.ngroups) {
+        const uint32_t k = g.key_base + g.nkey;
+        r0 = __ldg(a.stg.fstart + k);
+        r1 = __ldg(a.stg.fstart + k + 1);
+    } else {
+        const uint2 rows = group_rows(grp, g, a.stg);
+        r0 = rows.x;
+        r1 = rows.y;
+        if (r0 != r1) {
+            plan_group(P, grp, g, a.stg);
+            staged = P.total <= a.stg.scap;
+        }
+    }
+    if (staged) {
+        for (uint32_t s = threadIdx.x; s < P.total; s += blockDim.x) {
+            bool b;
+            const uint32_t j = a.stg.mode == 0 ? slot_row<0>(P, slot_cell(P, s), s, b)
+                                               : slot_row<1>(P, slot_cell(P, s), s, b);
+            const F4x2 e = ldg8(a.pva + 2 * (size_t)j);
+            stage[2 * s] = e.a;
+            stage[2 * s + 1] = e.b;
+        }
+        __syncthreads();
+    }
+    double contrib = 0.0;
+    for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        const float4 p = a.pos[r];
+        const float4 vi = a.vadv[r];
+        const uint32_t n = a.ncnt[r];
+        float d = a.ratio[r] - 1.f;
+        auto use = [&](auto, const F4x2 &e) {
+            const float rx = p.x - e.a.x, ry = p.y - e.a.y, rz = p.z - e.a.z;
+            const float gw = cubic_g(dist2(rx, ry, rz), a.k);
+            const float dot = gw * (rx * (vi.x - e.b.x) + ry * (vi.y - e.b.y) + rz * (vi.z - e.b.z));
+            d = __fmaf_rn(dot * e.a.w, T.dt, d);
+        };
+        const uint32_t cnt = n > 0 ? n - 1 : 0;
+        if (staged) {
+            slot_loop<U>(a.stg.snbr + ell_index(r, 0, a.ell_stride), cnt,
+                         [&](uint16_t s) {
+                             const uint32_t q = 2u * (uint32_t)(s & 0x7fffu);
+                             return F4x2{stage[q], stage[q + 1]};
+                         },
+                         use);
+        } else {
+            nbr_loop<U>(a.nbr + ell_index(r, 0, a.ell_stride), cnt,
+                        [&](uint32_t j) { return ldg8(a.pva + 2 * (size_t)j); }, use);
+        }
+        if (d < 0.f) d = 0.f;
+        a.delta[r] = d;
+        const float kap = d / a.alpha[r] * T.inv_dt2 / p.w;
+        a.kappa[r] = kap;
+        a.pk[r] = make_float4(p.x, p.y, p.z, kap);
+        contrib += (double)d;
+    }
+    if (!MULTI) {
+        const double s = block_sum(contrib);
+        if (threadIdx.x == 0) a.partials[grp] = s;
+    } else {
+        const int no = (int)a.scene_tiles[0].nobj;
+        for (int o = 0; o < no; ++o) {
+            double c = 0.0;
+            for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+                if ((int)a.obj_of[a.orig[r]] - (int)a.scene_tiles[0].obj0 == o) c += (double)a.delta[r];
+            const double s = block_sum(c);
+            if (threadIdx.x == 0) a.partials[(size_t)grp * a.nobj_max + o] = s;
+        }
+    }
+}
+
+// Staged solve_b: gathers the packed {x, kappa_j} (fluid) / {x, V_j}
+// (boundary) rows from the group's staged copy; bit 15 of a slot marks a
+// boundary neighbour.
+template <int U>
+__global__ void __launch_bounds__(kStageBlock) k_solve_b_staged(DfsphArgs a) {
+    extern __shared__ float4 stage[];
+    __shared__ GroupPlan P;
+    if (a.state[0].stopped) return;
+    const StepDt T = step_dt(a);
+    const uint32_t grp = blockIdx.x;
+    const SceneGrid g = a.sc.sg[0];
+    uint32_t r0, r1;
+    bool staged = false;
+    if (grp == a.stg.ngroups) {
+        const uint32_t k = g.key_base + g.nkey;
+        r0 = __ldg(a.stg.fstart + k);
+        r1 = __ldg(a.stg.fstart + k + 1);
+    } else {
+        const uint2 rows = group_rows(grp, g, a.stg);
+        r0 = rows.x;
+        r1 = rows.y;
+        if (r0 == r1) return;
+        plan_group(P, grp, g, a.stg);
+        staged = P.total <= a.stg.scap;
+    }
+    if (staged) {
+        for (uint32_t s = threadIdx.x; s < P.total; s += blockDim.x) {
+            bool b;
+            const uint32_t j = a.stg.mode == 0 ? slot_row<0>(P, slot_cell(P, s), s, b)
+                                               : slot_row<1>(P, slot_cell(P, s), s, b);
+            stage[s] = __ldg(a.pk + j);
+        }
+        __syncthreads();
+    }
+    for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        const float4 p = a.pos[r];
+        float4 v = a.vadv[r];
+        const float ki = a.kappa[r];
+        const uint32_t n = a.ncnt[r];
+        const float mi = a.rest_density ? a.rest_density[r] * p.w : a.mass_f;
+        const float ci = T.dt * p.w / mi;
+        auto step = [&](bool fj, const float4 &e) {
+            const float Vj = fj ? a.vol_f : e.w, kj = fj ? e.w : 0.f;
+            const float rx = p.x - e.x, ry = p.y - e.y, rz = p.z - e.z;
+            const float gw = cubic_g(dist2(rx, ry, rz), a.k);
+            const float s = ci * Vj * (ki + kj) * gw;
+            v.x = __fmaf_rn(-s, rx, v.x);
+            v.y = __fmaf_rn(-s, ry, v.y);
+            v.z = __fmaf_rn(-s, rz, v.z);
+        };
+        const uint32_t cnt = n > 0 ? n - 1 : 0;
+        if (staged) {
+            slot_loop<U>(a.stg.snbr + ell_index(r, 0, a.ell_stride), cnt,
+                         [&](uint16_t s) { return stage[s & 0x7fffu]; },
+                         [&](uint16_t s, const float4 &e) { step(!(s & kSlotBoundary), e); });
+        } else {
+            nbr_loop<U>(a.nbr + ell_index(r, 0, a.ell_stride), cnt, [&](uint32_t j) { return ldg4(a.pk + j); },
+                        [&](uint32_t j, const float4 &e) { step(j < a.nf, e); });
+        }
+        a.vadv[r] = v;
+        a.pva[2 * (size_t)r + 1] = v;
+    }
+}
+
 template <int U>
 __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     const StepDt T = step_dt(a);
@@ -488,12 +638,29 @@ void dfsph_solve_pack(cudaStream_t st, const DfsphArgs &a) {
     const uint32_t n = a.nf + a.nb;
     if (n) k_solve_pack<<<nblk(n, 256), 256, 0, st>>>(a, n);
 }
+template <class K>
+static void launch_staged(K kern, cudaStream_t st, const DfsphArgs &a, size_t row_bytes) {
+    const size_t smem = (size_t)a.stg.scap * row_bytes;
+    // the staged rows may exceed the 48 KB of dynamic shared memory a kernel gets by default
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<a.stg.ngroups + 1, kStageBlock, smem, st>>>(a);
+}
+
 void dfsph_solve_a(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.staged) {
+        if (a.nobj_max > 1) VTP_UNROLL_DISPATCH(a.unroll, launch_staged(k_solve_a_staged<true, UU>, st, a, 32))
+        else VTP_UNROLL_DISPATCH(a.unroll, launch_staged(k_solve_a_staged<false, UU>, st, a, 32))
+        return;
+    }
     const unsigned nb = dfsph_tile_grid(a.ntiles, block, a.persistent);
     if (a.nobj_max > 1) VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<true, UU><<<nb, block, 0, st>>>(a))
     else VTP_UNROLL_DISPATCH(a.unroll, k_solve_a<false, UU><<<nb, block, 0, st>>>(a))
 }
 void dfsph_solve_b(cudaStream_t st, const DfsphArgs &a, int block) {
+    if (a.staged) {
+        VTP_UNROLL_DISPATCH(a.unroll, launch_staged(k_solve_b_staged<UU>, st, a, 16))
+        return;
+    }
     const unsigned nb = dfsph_tile_grid(a.ntiles, block, a.persistent);
     VTP_UNROLL_DISPATCH(a.unroll, k_solve_b<UU><<<nb, block, 0, st>>>(a))
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "internal.h"
+#include "staged.h"
 
 namespace vtp {
 
@@ -66,6 +67,12 @@ struct DfsphArgs {
     // Packed gather rows of the pressure solve (filled by dfsph_solve_pack):
     float4 *pva;                // [2n] row j = {pos_j, v*_j} (32 B): one 256-bit load per pair in solve_a
     float4 *pk;                 // [n] {x, y, z, kappa_j} for fluid rows, {x, y, z, V_j} for boundary rows
+    // Staged pressure solve (single scene, bricked order): one block per cell group gathers
+    // its neighbours from a shared-memory copy of the group's neighbourhood through the slot
+    // lists; the residual partials are then per group (ngroups + 1 entries, the last for the
+    // rows outside the grid).
+    int staged;
+    Staging stg;
     const float *dtp;           // adaptive time step (CFL) on the device; null: the fixed dt above
     uint32_t *vmax_bits;        // adaptive step: the finalize pass folds max |v|^2 of the new velocities here
 };

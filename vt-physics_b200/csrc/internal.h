@@ -18,6 +18,7 @@ struct Layout {
     uint32_t ell_stride = 0;   // slots per row in the ELL neighbour list (maxnbr - 1 others)
     int merge_mode = 0;        // 0: fluid ids < boundary ids, 1: boundary ids < fluid ids, 2: general
     int list_lanes = 0;        // list builder lanes per row: 0 = by row count, 1 or 8 = forced
+    bool cell_cull = false;    // list builder skips neighbour cells beyond h of the row (same lists)
 };
 
 // Neighbour-search working set (one per solver).

@@ -9,6 +9,7 @@
 
 #include "../../include/vtp.h"
 #include "dfsph.h"
+#include "staged.h"
 #include "internal.h"
 #include "pbf.h"
 
@@ -105,6 +106,9 @@ struct vtp_solver {
     bool pdl = true;                // programmatic dependent launch between the substep's kernels
     int row_lanes = 1;        // threads per row of the PBF neighbour passes (1, 4, 8)
     int list_lanes = 0;       // neighbour-list builder lanes per row (0 = by row count)
+    bool cell_cull = false;   // list builder skips neighbour cells beyond h (same lists)
+    bool staged_solve = false;      // DFSPH pressure solve gathers from shared-memory cell-group copies
+    int stage_rows = 2048;          // staged rows per brick at most
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn
     bool phase_retry_all = false;   // IMM phase-transfer retries: every row, or rows near new flags
     int pbf_form = 0;                   // 0: the reference's PBF formulation, 1: standard PBF
@@ -120,6 +124,9 @@ struct vtp_solver {
     uint4 *d_tiles = nullptr;           // scene-offset tiles of the fluid rows
     uint32_t ntiles = 0;
     vtp::SceneTiles *d_scene_tiles = nullptr;
+    bool staged = false;                // staged solve in use (DFSPH, one scene, bricked order, merge mode 0 / 1)
+    vtp::Staging stg{};
+    vtp::SceneTiles *d_scene_groups = nullptr;   // residual partials of the staged solve: one per cell group
     int nobj_max = 1;
     vtp::LoopState *loop = nullptr;     // [2]: divergence, density
     vtp::Layout L{};

@@ -14,6 +14,9 @@
 //             in fixed order, ascending attach id inside a cell), stored as
 //             a warp-interleaved ELL array of sorted row indices.
 #include "internal.h"
+#include "staged.h"
+
+#include <type_traits>
 
 namespace vtp {
 
@@ -218,6 +221,37 @@ __global__ void k_rank_reorder(Scenes sc, uint32_t row0, uint32_t cnt, const uin
     for (int f = 0; f < carry.nf1; ++f) carry.dst1[f][row0 + dst] = carry.src1[f][row0 + s];
 }
 
+// Cell culling: distances from a row's position to the six faces of its own
+// cell, shrunk by a safety margin.  A neighbour cell whose nearest point lies
+// farther than h (d2 > d2max) holds no particle the membership test can accept
+// (UGNSCudaImpl.cu:189-199 tests every particle of all 27 cells), so skipping
+// it leaves the list unchanged.  The margin (1e-3 cell plus 1e-6 of the
+// coordinate's magnitude) covers the rounding of the face positions and of
+// the cell assignment floor((x - lb) / cell), both a few ulps of the
+// coordinate; a cell inside the margin is simply walked.
+struct FaceGaps {
+    float lx, hx, ly, hy, lz, hz;   // clearance below / above along each axis (>= 0)
+
+    __device__ __forceinline__ void init(const float4 &p, int3 c, const SceneGrid &g, float cell) {
+        gap(p.x, c.x, g.lbx, cell, lx, hx);
+        gap(p.y, c.y, g.lby, cell, ly, hy);
+        gap(p.z, c.z, g.lbz, cell, lz, hz);
+    }
+    __device__ __forceinline__ static void gap(float x, int c, float lb, float cell, float &lo, float &hi) {
+        const float f0 = __fmaf_rn((float)c, cell, lb);           // lower face of the cell
+        const float m = __fmaf_rn(1e-6f, fabsf(f0) + cell, 1e-3f * cell);
+        lo = fmaxf(x - f0 - m, 0.f);
+        hi = fmaxf(f0 + cell - x - m, 0.f);
+    }
+    // Whether the neighbour cell at offset o can hold a particle within h.
+    __device__ __forceinline__ bool reachable(int3 o, float d2max) const {
+        const float ex = o.x < 0 ? lx : (o.x > 0 ? hx : 0.f);
+        const float ey = o.y < 0 ? ly : (o.y > 0 ? hy : 0.f);
+        const float ez = o.z < 0 ? lz : (o.z > 0 ? hz : 0.f);
+        return dist2(ex, ey, ez) <= d2max;
+    }
+};
+
 // One candidate of the neighbour walk (UGNSCudaImpl.cu:189-199).
 struct Walker {
     float px, py, pz;
@@ -301,7 +335,7 @@ struct Walker {
     }
 };
 
-template <int MODE>
+template <int MODE, bool CULL>
 __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t ell_stride,
                               const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
                               const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
@@ -326,11 +360,14 @@ __global__ void k_build_lists(Scenes sc, uint32_t row0, uint32_t cnt, uint32_t e
     w.out = nbr + ell_index(r, 0, ell_stride);
     w.overflow = false;
     const float d2max = sc.d2max;
+    FaceGaps fg;
+    if (CULL) fg.init(p, c, g, sc.cell);
     for (int t = 0; t < 27; ++t) {
         int3 cc = c;
         int3 o = nbr_offset(t);
         cc.x += o.x; cc.y += o.y; cc.z += o.z;
         if (!cell_available(cc, g)) continue;
+        if (CULL && !fg.reachable(o, d2max)) continue;
         uint32_t k = g.key_base + cell_key(cc, g);
         uint32_t f0 = __ldg(fstart + k), f1 = __ldg(fstart + k + 1);
         uint32_t b0 = __ldg(bstart + k), b1 = __ldg(bstart + k + 1);
@@ -400,16 +437,17 @@ struct SplitSink {
     }
 };
 
-template <int MODE, int PASS>
+template <int MODE, bool CULL, int PASS>
 __device__ __forceinline__ void split_walk(SplitSink<PASS> &k, int3 c, const SceneGrid &g, int t0, int t1,
                                            const float4 *__restrict__ pos, const uint32_t *__restrict__ orig,
                                            const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
-                                           float d2max) {
+                                           float d2max, const FaceGaps &fg) {
     for (int t = t0; t < t1; ++t) {
         int3 cc = c;
         const int3 o = nbr_offset(t);
         cc.x += o.x; cc.y += o.y; cc.z += o.z;
         if (!cell_available(cc, g)) continue;
+        if (CULL && !fg.reachable(o, d2max)) continue;
         const uint32_t key = g.key_base + cell_key(cc, g);
         uint32_t f0 = __ldg(fstart + key), f1 = __ldg(fstart + key + 1);
         uint32_t b0 = __ldg(bstart + key), b1 = __ldg(bstart + key + 1);
@@ -431,7 +469,7 @@ __device__ __forceinline__ void split_walk(SplitSink<PASS> &k, int3 c, const Sce
     }
 }
 
-template <int MODE, int L>
+template <int MODE, bool CULL, int L>
 __global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
     Scenes sc, uint32_t row0, uint32_t cnt, uint32_t ell_stride, const float4 *__restrict__ pos,
     const uint32_t *__restrict__ orig, const uint32_t *__restrict__ fstart, const uint32_t *__restrict__ bstart,
@@ -458,8 +496,10 @@ __global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
     }
     const int t0 = 27 * lane / L, t1 = 27 * (lane + 1) / L;
     const float d2max = sc.d2max;
+    FaceGaps fg;
+    if (CULL) fg.init(p, c, g, sc.cell);
     SplitSink<kCount> cnt1{p.x, p.y, p.z, 0u, 0u, 0u, keep + threadIdx.x};
-    split_walk<MODE>(cnt1, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+    split_walk<MODE, CULL>(cnt1, c, g, t0, t1, pos, orig, fstart, bstart, d2max, fg);
     uint32_t x = cnt1.n;
 #pragma unroll
     for (int o = 1; o < L; o <<= 1) {
@@ -476,12 +516,128 @@ __global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
             for (uint32_t k = 0; k < m; ++k) out[(size_t)(base + k) * 32u] = keep[k * kSplitBlock + threadIdx.x];
         } else {
             SplitSink<kWrite> wr{p.x, p.y, p.z, 0u, base, cap, out};
-            split_walk<MODE>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max);
+            split_walk<MODE, CULL>(wr, c, g, t0, t1, pos, orig, fstart, bstart, d2max, fg);
         }
     }
     if (lane == 0) {
         ncnt[r] = total < cap ? total + 1u : sc.maxnbr;
         if (total > cap) {
+            atomicAdd(overflow_count, 1u);
+            atomicOr(status, ST_BOUNDS);
+        }
+    }
+}
+
+// Staged list builder: one block per brick (staged.h).  The block stages
+// the brick's 6 x 6 x 6-cell neighbourhood - positions, with each row's index
+// in w - in shared memory once, and every row of the group walks its 27 cells
+// (the reference's offset order, a cell's runs in list order, cells beyond h
+// culled) over the staged copy, writing the global list entry and the slot
+// list entry of each accepted candidate.  A group whose neighbourhood exceeds
+// the staging capacity walks global memory with the one-thread walker and
+// writes no slot list (the solve passes then gather it from global memory);
+// block `ngroups` gives the rows outside the grid empty lists.
+template <int MODE, bool CULL>
+__global__ void __launch_bounds__(kStageBlock) k_build_lists_staged(
+    Scenes sc, Staging stg, uint32_t ell_stride, const float4 *__restrict__ pos, uint32_t *__restrict__ nbr,
+    uint32_t *__restrict__ ncnt, uint32_t *__restrict__ status, uint32_t *__restrict__ overflow_count) {
+    pdl_enter();
+    extern __shared__ float4 stage[];
+    __shared__ GroupPlan P;
+    const uint32_t grp = blockIdx.x;
+    const SceneGrid g = sc.sg[0];
+    if (grp == stg.ngroups) {   // rows outside the grid: no neighbours, not even self
+        const uint32_t k = g.key_base + g.nkey;
+        const uint32_t r1 = __ldg(stg.fstart + k + 1);
+        for (uint32_t r = __ldg(stg.fstart + k) + threadIdx.x; r < r1; r += blockDim.x) ncnt[r] = 0;
+        return;
+    }
+    const uint2 rows = group_rows(grp, g, stg);
+    if (rows.x == rows.y) return;
+    plan_group(P, grp, g, stg);
+    const bool staged = P.total <= stg.scap;
+    if (staged) {
+        for (uint32_t s = threadIdx.x; s < P.total; s += blockDim.x) {
+            bool b;
+            const uint32_t j = slot_row<MODE>(P, slot_cell(P, s), s, b);
+            float4 q = __ldg(pos + j);
+            q.w = __uint_as_float(j);
+            stage[s] = q;
+        }
+    }
+    __syncthreads();
+    const float d2max = sc.d2max;
+    const uint32_t maxnbr = sc.maxnbr;
+    for (uint32_t r = P.r0 + threadIdx.x; r < P.r1; r += blockDim.x) {
+        const float4 p = pos[r];
+        const int3 c = cell_of(p.x, p.y, p.z, g, sc.cell);
+        FaceGaps fg;
+        if (CULL) fg.init(p, c, g, sc.cell);
+        if (!staged) {
+            Walker w;
+            w.px = p.x; w.py = p.y; w.pz = p.z;
+            w.self = r;
+            w.cnt = 1;
+            w.maxnbr = maxnbr;
+            w.out = nbr + ell_index(r, 0, ell_stride);
+            w.overflow = false;
+            for (int t = 0; t < 27; ++t) {
+                const int3 o = nbr_offset(t);
+                const int3 cc = make_int3(c.x + o.x, c.y + o.y, c.z + o.z);
+                if (!cell_available(cc, g)) continue;
+                if (CULL && !fg.reachable(o, d2max)) continue;
+                const uint32_t k = g.key_base + cell_key(cc, g);
+                const uint32_t f0 = __ldg(stg.fstart + k), f1 = __ldg(stg.fstart + k + 1);
+                const uint32_t b0 = __ldg(stg.bstart + k), b1 = __ldg(stg.bstart + k + 1);
+                if (w.cnt + (f1 - f0) + (b1 - b0) <= w.maxnbr)
+                    w.visit_cell<MODE, true>(f0, f1, b0, b1, pos, nullptr, d2max);
+                else
+                    w.visit_cell<MODE, false>(f0, f1, b0, b1, pos, nullptr, d2max);
+            }
+            ncnt[r] = w.cnt;
+            if (w.overflow) {
+                atomicAdd(overflow_count, 1u);
+                atomicOr(status, ST_BOUNDS);
+            }
+            continue;
+        }
+        uint32_t *const out = nbr + ell_index(r, 0, ell_stride);
+        uint16_t *const sout = stg.snbr + ell_index(r, 0, ell_stride);
+        uint32_t cnt = 1;
+        bool over = false;
+        for (int t = 0; t < 27; ++t) {
+            const int3 o = nbr_offset(t);
+            const int3 cc = make_int3(c.x + o.x, c.y + o.y, c.z + o.z);
+            if (!cell_available(cc, g)) continue;
+            if (CULL && !fg.reachable(o, d2max)) continue;
+            const int lx = cc.x - P.ox, ly = cc.y - P.oy, lz = cc.z - P.oz;
+            if ((unsigned)lx >= (unsigned)kStageUx || (unsigned)ly >= (unsigned)kStageUy ||
+                (unsigned)lz >= (unsigned)kStageUz) {   // a row outside its group's block: never expected
+                atomicOr(status, ST_BOUNDS);
+                continue;
+            }
+            const int u = (lz * kStageUy + ly) * kStageUx + lx;
+            const uint32_t s0 = P.off[u], s1 = P.off[u + 1];
+            // first boundary slot (mode 0) / first fluid slot (mode 1) of the cell
+            const uint32_t sb = s0 + (MODE == 0 ? P.nfl[u] : P.nbl[u]);
+            const bool room = cnt + (s1 - s0) <= maxnbr;
+            for (uint32_t sl = s0; sl < s1; ++sl) {
+                const float4 q = stage[sl];
+                const float d2 = dist2(p.x - q.x, p.y - q.y, p.z - q.z);
+                if (d2 > 0.f && d2 <= d2max) {
+                    if (room || cnt < maxnbr) {
+                        const bool bnd = MODE == 0 ? sl >= sb : sl < sb;
+                        out[(size_t)(cnt - 1) * 32u] = __float_as_uint(q.w);
+                        sout[(size_t)(cnt - 1) * 32u] = (uint16_t)(sl | (bnd ? kSlotBoundary : 0u));
+                        ++cnt;
+                    } else {
+                        over = true;
+                    }
+                }
+            }
+        }
+        ncnt[r] = cnt;
+        if (over) {
             atomicAdd(overflow_count, 1u);
             atomicOr(status, ST_BOUNDS);
         }
@@ -713,6 +869,20 @@ void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t ro
     E("ugns_rank_reorder");
 }
 
+template <int MODE, bool CULL>
+static void build_lists_as(cudaStream_t st, bool split, const Scenes &sc, const Layout &L, uint32_t row0,
+                           uint32_t cnt, const float4 *pos, const uint32_t *orig, const UgnsBuffers &u, uint32_t *nbr,
+                           uint32_t *ncnt, uint32_t *status, uint32_t *overflow, int block) {
+    if (split) {
+        constexpr int S = 8;
+        launch(k_build_lists_split<MODE, CULL, S>, nblk(cnt * S, kSplitBlock), kSplitBlock, 0, st, sc, row0, cnt,
+               L.ell_stride, pos, orig, u.fstart, u.bstart, nbr, ncnt, status, overflow);
+    } else {
+        launch(k_build_lists<MODE, CULL>, nblk(cnt, block), block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig,
+               u.fstart, u.bstart, nbr, ncnt, status, overflow);
+    }
+}
+
 void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32_t row0, uint32_t cnt,
                       const float4 *pos, const uint32_t *orig, const UgnsBuffers &u, uint32_t *nbr, uint32_t *ncnt,
                       uint32_t *status, uint32_t *overflow, int block) {
@@ -720,39 +890,45 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
     // Few rows: eight lanes per row (same lists, a quarter to an eighth of the
     // serial walk per thread).
     const bool split = L.list_lanes == 8 || (L.list_lanes == 0 && cnt <= kSplitRows);
-    if (split) {
-        constexpr int S = 8;
-        const unsigned ns = nblk(cnt * S, kSplitBlock);
-        switch (L.merge_mode) {
-            case 0:
-                launch(k_build_lists_split<0, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
-                                                               u.bstart, nbr, ncnt, status, overflow);
-                break;
-            case 1:
-                launch(k_build_lists_split<1, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
-                                                               u.bstart, nbr, ncnt, status, overflow);
-                break;
-            default:
-                launch(k_build_lists_split<2, S>, ns, kSplitBlock, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart,
-                                                               u.bstart, nbr, ncnt, status, overflow);
-                break;
-        }
-        return;
-    }
-    unsigned nb = nblk(cnt, block);
+    auto go = [&](auto mode, auto cull) {
+        build_lists_as<decltype(mode)::value, decltype(cull)::value>(st, split, sc, L, row0, cnt, pos, orig, u, nbr,
+                                                                     ncnt, status, overflow, block);
+    };
+    using T = std::true_type;
+    using F = std::false_type;
+    using M0 = std::integral_constant<int, 0>;
+    using M1 = std::integral_constant<int, 1>;
+    using M2 = std::integral_constant<int, 2>;
     switch (L.merge_mode) {
-        case 0:
-            launch(k_build_lists<0>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
-                                                    ncnt, status, overflow);
-            break;
-        case 1:
-            launch(k_build_lists<1>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
-                                                    ncnt, status, overflow);
-            break;
-        default:
-            launch(k_build_lists<2>, nb, block, 0, st, sc, row0, cnt, L.ell_stride, pos, orig, u.fstart, u.bstart, nbr,
-                                                    ncnt, status, overflow);
-            break;
+        case 0: L.cell_cull ? go(M0{}, T{}) : go(M0{}, F{}); break;
+        case 1: L.cell_cull ? go(M1{}, T{}) : go(M1{}, F{}); break;
+        default: L.cell_cull ? go(M2{}, T{}) : go(M2{}, F{}); break;
+    }
+}
+
+void ugns_build_lists_staged(cudaStream_t st, const Scenes &sc, const Layout &L, const Staging &stg,
+                             const float4 *pos, uint32_t *nbr, uint32_t *ncnt, uint32_t *status,
+                             uint32_t *overflow) {
+    const size_t smem = (size_t)stg.scap * sizeof(float4);
+    const unsigned grid = stg.ngroups + 1;
+    // the staged rows may exceed the 48 KB of dynamic shared memory a kernel gets by default
+    auto room = [&](auto kern) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); };
+    if (stg.mode == 0 && L.cell_cull) {
+        room(k_build_lists_staged<0, true>);
+        launch(k_build_lists_staged<0, true>, grid, kStageBlock, smem, st, sc, stg, L.ell_stride, pos, nbr, ncnt,
+               status, overflow);
+    } else if (stg.mode == 0) {
+        room(k_build_lists_staged<0, false>);
+        launch(k_build_lists_staged<0, false>, grid, kStageBlock, smem, st, sc, stg, L.ell_stride, pos, nbr, ncnt,
+               status, overflow);
+    } else if (L.cell_cull) {
+        room(k_build_lists_staged<1, true>);
+        launch(k_build_lists_staged<1, true>, grid, kStageBlock, smem, st, sc, stg, L.ell_stride, pos, nbr, ncnt,
+               status, overflow);
+    } else {
+        room(k_build_lists_staged<1, false>);
+        launch(k_build_lists_staged<1, false>, grid, kStageBlock, smem, st, sc, stg, L.ell_stride, pos, nbr, ncnt,
+               status, overflow);
     }
 }
 
