@@ -56,7 +56,19 @@ struct DiffState {
     float4 *df_vb = nullptr, *df_save = nullptr;
     float *df_kb = nullptr;
 
+    // A full checkpoint segment's two halves, each captured once as a graph and replayed for
+    // every segment of that length (their pointers are all fixed: the tape, the adjoint
+    // arrays, the solver's buffers at the parity a segment starts from): `rec` runs the
+    // segment's substeps recording into the tape, `adj` runs the adjoint substeps over it.
+    cudaGraphExec_t rec_exec = nullptr, adj_exec = nullptr;
+    int rec_parity[3] = {-1, -1, -1};   // pos / vel / orig buffer parity `rec` starts from
+    // Checkpoint segment whose tape the forward recorded (the last one: the backward starts
+    // there without recomputing it); -1 when the tape holds no segment of the forward.
+    int tape_holds = -1;
+
     ~DiffState() {
+        if (rec_exec) cudaGraphExecDestroy(rec_exec);
+        if (adj_exec) cudaGraphExecDestroy(adj_exec);
         for (void *p : mem) cudaFree(p);
     }
     template <class T>
@@ -413,6 +425,86 @@ int restore_fluid(vtp_solver &s, const float4 *p, const float4 *v, const uint32_
     return VTP_OK;
 }
 
+int record_rollout(vtp_solver *s, vtp::DiffState &d);
+
+// The k substeps of a checkpoint segment, recording into the tape.
+int record_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k) {
+    int rc;
+    for (uint32_t t = 0; t < k; ++t)
+        if ((rc = s->enqueue_pbf_substep(s->st, &d.tape[t]))) return rc;
+    return VTP_OK;
+}
+
+// The adjoint substeps of a recorded segment of k substeps, last to first (programmatic
+// launch between their kernels, as in the forward substep).
+int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G) {
+    const uint32_t nf = d.nf;
+    const int I = s->iterations;
+    const vtp::PdlScope pdl_scope(s->pdl);
+    for (int t = (int)k - 1; t >= 0 && nf; --t) {
+        const PbfTapeSlot &T = d.tape[t];
+        vtp::AdjArgs a{};
+        a.nf = nf; a.ell_stride = s->L.ell_stride; a.k = s->kc;
+        a.dt = s->dt; a.inv_dt = 1.f / s->dt; a.rho0 = s->rho_f; a.eps = 1e-6f; a.c = s->xsph_k;
+        a.nbr = T.nbr; a.ncnt = T.ncnt; a.orig = T.orig;
+        a.v = T.v; a.vol = s->vol;
+        a.xbar = d.xbar; a.vbar = d.vbar; a.abar = d.abar; a.A2 = d.A2; a.sbar = d.sbar;
+        a.xbar_a = d.xbar_a; a.vbar_a = d.vbar_a; a.kpart = d.kpart;
+        int cur = 0;
+        a.x = T.x[I];
+        a.Dcur = d.D[cur];
+        vtp::launch(vtp::k_adj_gather, G, 256, 0, s->st, a);
+        vtp::launch(vtp::k_adj_xsph, G, 256, 0, s->st, a);
+        vtp::launch(vtp::k_adj_kreduce, 1, 256, 0, s->st, d.kpart, G, d.kacc);
+        for (int it = I - 1; it >= 0; --it) {
+            a.x = T.x[it];
+            a.lam = T.lam[it];
+            a.rho = T.rho[it];
+            a.Dcur = d.D[cur];
+            a.Dnext = d.D[cur ^ 1];
+            vtp::launch(vtp::k_adj_lambda, G, 256, 0, s->st, a);
+            vtp::launch(vtp::k_adj_dx, G, 256, 0, s->st, a);
+            cur ^= 1;
+        }
+        vtp::launch(vtp::k_adj_force_scatter, G, 256, 0, s->st, a);
+    }
+    return VTP_OK;
+}
+
+// Runs `body` (enqueueing a full segment's work on s->st) through the graph `exec`, capturing
+// it on first use.  The substep swaps the position buffers 6 times, the velocities twice and
+// the sorted order once, so a segment of even length ends at the parity it started from;
+// `parity` (when given) records the parity the graph was captured at, and a segment starting
+// at another parity, of odd or partial length, or with graphs off, runs `body` directly.
+template <class Body>
+int run_segment_graph(vtp_solver *s, vtp::DiffState &d, uint32_t k, cudaGraphExec_t &exec, int *parity, Body body) {
+    const int par[3] = {s->pos.cur, s->vel.cur, s->orig.cur};
+    const bool graph_ok = s->use_graphs && k == d.every && k % 2 == 0 && d.nf;
+    if (!graph_ok || (exec && parity && !std::equal(par, par + 3, parity))) return body();
+    if (!exec) {
+        CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
+        const int rc = body();
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s->st, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        const bool same = s->pos.cur == par[0] && s->vel.cur == par[1] && s->orig.cur == par[2];
+        cudaError_t e = ec == cudaSuccess && same ? cudaGraphInstantiate(&exec, g, 0) : cudaErrorInvalidValue;
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {   // run the segment with direct launches instead
+            cudaGetLastError();
+            exec = nullptr;
+            s->pos.cur = par[0]; s->vel.cur = par[1]; s->orig.cur = par[2];
+            return body();
+        }
+        if (parity) std::copy(par, par + 3, parity);
+    }
+    CU(cudaGraphLaunch(exec, s->st));
+    return VTP_OK;
+}
+
 int check_ready(vtp_solver *s) {
     if (!s) return fail(VTP_ERR_ARG, "null solver");
     if (s->type != VTP_SOLVER_PBF) return fail(VTP_ERR_CONFIG, "differentiable mode supports the PBF solver");
@@ -431,9 +523,19 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
     if (!s->initialized && (rc = s->initialize())) return rc;
     if (s->crashed) return fail(VTP_ERR_STATE, "solver is crashed");
     if (n_steps == 0 || checkpoint_every == 0) return fail(VTP_ERR_ARG, "n_steps and checkpoint_every must be > 0");
+    // A rollout of the same shape as the previous one reuses its checkpoints, tape and adjoint
+    // arrays (a training loop records the same horizon again and again); device memory is
+    // allocated only when the shape changes.
+    const uint32_t every = std::min(checkpoint_every, n_steps);
+    if (s->diff && s->diff->steps == n_steps && s->diff->every == every && s->diff->keep_lists == (keep_lists != 0) &&
+        s->diff->nf == s->L.nf && s->diff->n == s->L.n && s->diff->tape.size() == every) {
+        std::shared_ptr<vtp::DiffState> d = s->diff;
+        d->df_which = -1;
+        return record_rollout(s, *d);
+    }
     auto d = std::make_shared<vtp::DiffState>();
     d->steps = n_steps;
-    d->every = std::min(checkpoint_every, n_steps);
+    d->every = every;
     d->keep_lists = keep_lists != 0;
     d->nf = s->L.nf;
     d->n = s->L.n;
@@ -487,10 +589,40 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
         (rc = d->alloc(&d->kpart, d->kblocks)) || (rc = d->alloc(&d->kacc, 1)))
         return rc;
     s->diff.reset();
-    // Forward: checkpoint, then the ordinary substeps up to the next checkpoint.
+    if ((rc = record_rollout(s, *d))) return rc;
+    s->diff = d;
+    return VTP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Forward of a recorded rollout: checkpoint, then the ordinary substeps up to the next checkpoint.
+int record_rollout(vtp_solver *s, vtp::DiffState &dd) {
+    vtp::DiffState *d = &dd;
+    const uint32_t n_steps = d->steps;
+    const uint32_t nchk = (n_steps + d->every - 1) / d->every;
+    int rc;
+    d->tape_holds = -1;
     for (uint32_t c = 0; c < nchk; ++c) {
         if ((rc = save_fluid(*s, d->ck_pos[c], d->ck_vel[c], d->ck_orig[c]))) return rc;
         const uint32_t k = std::min(d->every, n_steps - c * d->every);
+        if (!d->keep_lists && c + 1 == nchk) {
+            // The last segment runs its substeps recording into the tape, so the backward
+            // starts from it without recomputing it.
+            if (!s->initialized && (rc = s->initialize())) return rc;
+            if ((rc = run_segment_graph(s, *d, k, d->rec_exec, d->rec_parity,
+                                        [&] { return record_segment(s, *d, k); })))
+                return rc;
+            for (uint32_t t = 0; t < k; ++t) {   // as tick_n advances them for the segments before
+                s->sim_time += s->dt;
+                ++s->steps_done;
+            }
+            s->stats.steps_done = s->steps_done;
+            s->stats.sim_time = s->sim_time;
+            d->tape_holds = (int)c;
+            continue;
+        }
         if (!d->keep_lists) {
             if ((rc = s->tick_n(k))) return rc;
             continue;
@@ -511,10 +643,11 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
     }
     if ((rc = save_fluid(*s, d->ck_pos[nchk], d->ck_vel[nchk], d->ck_orig[nchk]))) return rc;
     CU(cudaStreamSynchronize(s->st));
-    if ((rc = s->check_status())) return rc;
-    s->diff = d;
-    return VTP_OK;
+    return s->check_status();
 }
+}  // namespace
+
+extern "C" {
 
 int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
                              float *dl_dvel0, double *dl_dxsph_k) {
@@ -537,41 +670,16 @@ int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *d
     const unsigned G = vtp::nblk(std::max<uint32_t>(nf, 1), 256);
     for (int c = (int)nchk - 1; c >= 0; --c) {
         const uint32_t t0 = (uint32_t)c * d.every, k = std::min(d.every, d.steps - t0);
-        // Recompute the segment from its checkpoint into the tape.
-        if ((rc = restore_fluid(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
-        for (uint32_t t = 0; t < k; ++t)
-            if ((rc = s->enqueue_pbf_substep(s->st, &d.tape[t]))) return rc;
-        // Adjoint substeps, last to first (programmatic launch between their kernels, as in
-        // the forward substep).
-        const vtp::PdlScope pdl_scope(s->pdl);
-        for (int t = (int)k - 1; t >= 0 && nf; --t) {
-            const PbfTapeSlot &T = d.tape[t];
-            vtp::AdjArgs a{};
-            a.nf = nf; a.ell_stride = s->L.ell_stride; a.k = s->kc;
-            a.dt = s->dt; a.inv_dt = 1.f / s->dt; a.rho0 = s->rho_f; a.eps = 1e-6f; a.c = s->xsph_k;
-            a.nbr = T.nbr; a.ncnt = T.ncnt; a.orig = T.orig;
-            a.v = T.v; a.vol = s->vol;
-            a.xbar = d.xbar; a.vbar = d.vbar; a.abar = d.abar; a.A2 = d.A2; a.sbar = d.sbar;
-            a.xbar_a = d.xbar_a; a.vbar_a = d.vbar_a; a.kpart = d.kpart;
-            int cur = 0;
-            a.x = T.x[I];
-            a.Dcur = d.D[cur];
-            vtp::launch(vtp::k_adj_gather, G, 256, 0, s->st, a);
-            vtp::launch(vtp::k_adj_xsph, G, 256, 0, s->st, a);
-            vtp::launch(vtp::k_adj_kreduce, 1, 256, 0, s->st, d.kpart, G, d.kacc);
-            for (int it = I - 1; it >= 0; --it) {
-                a.x = T.x[it];
-                a.lam = T.lam[it];
-                a.rho = T.rho[it];
-                a.Dcur = d.D[cur];
-                a.Dnext = d.D[cur ^ 1];
-                vtp::launch(vtp::k_adj_lambda, G, 256, 0, s->st, a);
-                vtp::launch(vtp::k_adj_dx, G, 256, 0, s->st, a);
-                cur ^= 1;
-            }
-            vtp::launch(vtp::k_adj_force_scatter, G, 256, 0, s->st, a);
+        if (c != d.tape_holds) {
+            // Recompute the segment from its checkpoint into the tape.
+            if ((rc = restore_fluid(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
+            if ((rc = run_segment_graph(s, d, k, d.rec_exec, d.rec_parity, [&] { return record_segment(s, d, k); })))
+                return rc;
         }
+        if ((rc = run_segment_graph(s, d, k, d.adj_exec, nullptr, [&] { return adjoint_segment(s, d, k, G); })))
+            return rc;
     }
+    d.tape_holds = -1;   // the tape now holds the first segment's recompute
     CU(cudaGetLastError());
     // Outputs: dL/d(state at the start of the recorded forward), attach order.
     if (dl_dpos0) {
@@ -671,8 +779,12 @@ int vtp_solver_dfsph_solve_forward(vtp_solver *s, int which, const float *v_in, 
         CU(cudaMemcpyAsync(s->vadv.c(), s->vadv.n(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
         CU(cudaMemcpyAsync(d.df_save, s->vadv.c(), (size_t)nf * sizeof(float4), cudaMemcpyDeviceToDevice, s->st));
     }
-    vtp::ugns_build_lists(s->st, s->scn(), s->L, 0, nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
-                          s->d_status, s->d_overflow, s->block);
+    if (s->staged)   // the staged solve passes below read the slot lists too
+        vtp::ugns_build_lists_staged(s->st, s->scn(), s->L, s->stg, s->pos.c(), s->u.nbr, s->u.ncnt, s->d_status,
+                                     s->d_overflow);
+    else
+        vtp::ugns_build_lists(s->st, s->scn(), s->L, 0, nf, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
+                              s->d_status, s->d_overflow, s->block);
     vtp::dfsph_ratio_alpha(s->st, s->dfsph_args(which), s->block);
     const size_t n3 = (size_t)n * 3 * sizeof(float);
     if ((rc = s->ensure_stage(n3))) return rc;
