@@ -266,10 +266,20 @@ def run_reference(args) -> dict:
     s.initialize()
     if args.warmup:
         s.tick_timed(args.warmup)
+    s.take_means()   # residuals recorded so far (initialization, warm-up) are dropped
     clk = Clocks(0)
     clk.start()
     ms = s.tick_timed(args.steps)
     clocks = clk.stop()
+    iters = None
+    if sc.solver != "PBF":
+        # the reference's pressure-solve iterations over the timed substeps, rebuilt from the
+        # residuals its cal_mean returned (one per fluid object per iteration)
+        req = sc.config[sc.solver]["Required"]
+        nfo = sum(1 for o in sc.objects if o.material == 0)
+        per_tick = R.split_ticks(s.take_means(), nfo, req["divFreeThreshold"], req["incompThreshold"])
+        iters = {"div_iters_total": int(sum(d for d, _ in per_tick)),
+                 "incomp_iters_total": int(sum(i for _, i in per_tick)), "substeps_parsed": len(per_tick)}
     nf = sc.n_fluid
     value = nf * args.steps / (ms / 1e3) / 1e6
     # e2e: the fluid state round-trips through host memory every step (positions and
@@ -291,7 +301,8 @@ def run_reference(args) -> dict:
     out.update({"value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": {"workload": args.workload, "fluid": nf, "boundary": sc.n_boundary,
-                                                "impl": "reference CUDA build (sm_100a, -O3) via Solver::tickNsteps"},
+                                                "impl": "reference CUDA build (sm_100a, -O3) via Solver::tickNsteps",
+                                                **(iters or {})},
                 "clocks": clocks,
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
                                  "sample": "the reference is GPU code: its own CUDA build timed on this B200"},
@@ -340,20 +351,15 @@ def state_round_trip(s, bufs):
         s.get_state_range_ptr(first, count, p.ptr, v.ptr)
 
 
-def _batch_cost(sc) -> float:
-    # relative cost per substep: PBF runs 4 constraint iterations, DFSPH ~2x as many neighbour passes
-    return sc.n_fluid * (1.0 if sc.solver == "PBF" else 2.0)
-
-
 def run_batched(args, rank, world, local, dist, torch):
     """64 independent scenes (48 PBF + 16 DFSPH): one solver per solver type advances all its
     scenes together (scene-offset kernels, one CUDA graph per substep).  Compared with the plain
     per-scene loop (one solver per scene, scenes one after another) on the same GPU."""
     import numpy as np
     import vtp
-    from vtp.dist import lpt_assign
+    from vtp.dist import scene_share
     mix = vtp.scenes.batched_scenes()
-    mine = sorted(lpt_assign([_batch_cost(m) for m in mix], world)[rank])
+    mine = scene_share(mix, world, rank)
     extra = json.loads(args.extra) if args.extra else {}
     if args.block:
         extra["blockSize"] = args.block
@@ -520,13 +526,18 @@ def run_diff(args, torch) -> dict:
         g[mask] = 2.0 * (m - target) / nf
         return float(((m - target) ** 2).sum()), g
 
-    s = diff.pbf_solver(sc, extra=extra)
-    if args.warmup:   # warm the graphs and kernels on a throwaway copy
-        w = diff.pbf_solver(sc, extra=extra)
-        diff.diff_forward(w, min(args.warmup, args.checkpoint_every), args.checkpoint_every)
-        _, g = loss_grad(w.get_field("pos"))
-        diff.diff_backward(w, g, None)
-        w.destroy()
+    s = diff.pbf_solver(sc, extra=extra)   # initialized
+    x_init, v_init = s.get_field("pos"), s.get_field("vel")
+    if args.warmup:
+        # One recorded rollout of the timed shape and its adjoint on this solver: it allocates the
+        # checkpoints and the tape, which later rollouts of the same shape reuse, and captures the
+        # backward's segment graph; then the initial state is written back, as a training loop
+        # restarts every rollout from its initial state.
+        diff.diff_forward(s, args.steps, args.checkpoint_every)
+        _, g = loss_grad(s.get_field("pos"))
+        diff.diff_backward(s, g, None)
+        s.set_field("pos", x_init)
+        s.set_field("vel", v_init)
     # plain forward of the same rollout (no checkpoints): the cost the adjoint is compared with
     p = diff.pbf_solver(sc, extra=extra)
     p.tickNsteps(1)
@@ -549,11 +560,14 @@ def run_diff(args, torch) -> dict:
     clocks = clk.stop()
     fwd_s, bwd_s = t1 - t0, t3 - t2
     s.destroy()
-    value = nf * args.steps / bwd_s / 1e6
+    # value: gradients per second in particle-steps, i.e. the recorded forward plus the backward
+    value = nf * args.steps / (fwd_s + bwd_s) / 1e6
     cfg = {"workload": "diff_pbf", "fluid": nf, "boundary": int((~mask).sum()), "substeps": args.steps,
            "checkpoint_every": args.checkpoint_every, "loss": loss, "dl_dxsph_k": gk,
            "forward_value": nf * args.steps / plain_s / 1e6, "recorded_forward_value": nf * args.steps / fwd_s / 1e6,
-           "adjoint_over_forward": bwd_s / plain_s,
+           "adjoint_over_forward": (fwd_s + bwd_s) / plain_s,
+           "adjoint_over_forward_definition": "(recorded forward + backward) / plain forward, wall clock",
+           "recorded_forward_over_forward": fwd_s / plain_s, "backward_over_forward": bwd_s / plain_s,
            "grad_v0_norm": float(np.linalg.norm(gv[mask])),
            "timing": "host wall clock around each synchronous C-ABI call (inputs resident on the device)",
            "l2": "per-segment tapes (~0.5 GB) larger than L2"}
@@ -592,7 +606,7 @@ def run_diff(args, torch) -> dict:
         cfg["fd_check"] = {"substeps": T, "directions": args.fd_directions, "eps": 1e-4,
                            "max_rel_err": max(errs), "rel_errs": errs, "reference": "FP64 CPU oracle, frozen lists"}
     return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * bwd_s / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * (fwd_s + bwd_s) / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "clocks": clocks}
 
@@ -634,10 +648,27 @@ def l2_note(s, req) -> str:
     return f"working set ~{ws / 1e6:.0f} MB per replica, {rel} L2 (126 MB); no flush between substeps"
 
 
+def launch_ranks(n: int) -> int:
+    """`--gpus N` without a launcher: start N ranks of this same command, one process per GPU,
+    through torch.distributed.run on 127.0.0.1 (each rank then initialises NCCL and reads
+    RANK / LOCAL_RANK / WORLD_SIZE like under an outer torchrun).  Rank 0 prints the line; the
+    process group's own timeout ends ranks that wait for one another, `timeout` bounds the rest."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
     if args.steps is None:
         args.steps = DEFAULT_STEPS[args.workload]
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.scene_index < 0:
+        return launch_ranks(args.gpus)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

@@ -44,3 +44,31 @@ def lpt_assign(costs, n_ranks: int) -> list[list[int]]:
         out[r].append(i)
         heapq.heappush(heap, (load + float(costs[i]), r))
     return out
+
+
+def scene_cost(scene) -> float:
+    """Relative cost of one substep of a scene: fluid particles, times 2 for the pressure-solved
+    schemes (DFSPH / IMM run about twice as many neighbour passes as PBF's 4 iterations)."""
+    return scene.n_fluid * (1.0 if scene.solver == "PBF" else 2.0)
+
+
+def scene_share(scenes, n_ranks: int, rank: int) -> list[int]:
+    """Indices of the scenes rank `rank` advances (LPT on scene_cost), ascending."""
+    return sorted(lpt_assign([scene_cost(s) for s in scenes], n_ranks)[rank])
+
+
+def gather_scene_results(local: dict, group=None) -> dict:
+    """Merge every rank's {scene index: result} (any picklable result) on every rank.  The
+    only exchange of a sharded batch, once, after the run."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return dict(local)
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, local, group=group)
+    out = {}
+    for p in parts:
+        overlap = set(out) & set(p)
+        if overlap:
+            raise RuntimeError(f"scenes {sorted(overlap)} were advanced by more than one rank")
+        out.update(p)
+    return out
