@@ -35,6 +35,16 @@ namespace vtp {
 
 constexpr int kMaxPhases = 7;
 
+// The conformation tensor Q and the stress tau are symmetric (the reference keeps full 3x3
+// matrices, IMMCTrtData.hpp:79; its update keeps Q symmetric in exact arithmetic): six
+// components are stored, in the order 00, 01, 02, 11, 12, 22, and the 3x3 row-major
+// component c = 3 row + col is symmetric component sym_of(c).
+constexpr int kSym = 6;
+__host__ __device__ constexpr int sym_of(int c) {
+    return c == 0 ? 0 : c == 1 || c == 3 ? 1 : c == 2 || c == 6 ? 2 : c == 4 ? 3 : c == 5 || c == 7 ? 4 : 5;
+}
+__host__ __device__ constexpr bool sym_diag(int k) { return k == 0 || k == 3 || k == 5; }
+
 struct ImmParams {
     int P;
     int ct;                   // 1: IMM-CT, 0: IMM
@@ -60,8 +70,8 @@ struct ImmArgs {
     float4 *vel, *vel_alt, *vadv, *vadv_alt;
     float4 *vph[kMaxPhases];  // phase velocities (fluid rows)
     float *frac[kMaxPhases];  // volume fractions
-    float *Q[9];              // conformation tensor, row-major components
-    float *tau[9];            // viscoelastic stress, row-major components
+    float *Q[kSym];           // conformation tensor, symmetric components (kSymOrder)
+    float *tau[kSym];         // viscoelastic stress, symmetric components
     float4 *acc_tmp[kMaxPhases];
     float4 *normal;
     float *rd;                // rest density
@@ -80,9 +90,9 @@ struct ImmArgs {
     // fluid row ({x, V}, then {v, per-row factor} or {n, rest density}): the launch reads
     // `pk_in` and writes `pk_out` (see immct_enqueue_tick for which pass writes which).
     float4 *pk_in, *pk_out;
-    // IMM-CT: packed rows of the stress-divergence gathers, 4 float4 per fluid row:
-    // {x, V}, then tau_c / rho_rest^2 for c = 0..8 (3 float4, the last 3 floats unused);
-    // written by the conformation-tensor pass, read by the stress-divergence pass.
+    // IMM-CT: packed rows of the stress-divergence gathers, 3 float4 per fluid row:
+    // {x, V}, then tau_c / rho_rest^2 for the 6 symmetric components (the last 2 floats
+    // unused); written by the conformation-tensor pass, read by the stress-divergence pass.
     float4 *tpk;
 };
 
@@ -91,8 +101,8 @@ struct ImmState {
     bool have_tension = false;
     DB<float4> vph[kMaxPhases];
     DB<float> frac[kMaxPhases];
-    DB<float> Q[9];
-    float *tau[9] = {nullptr};
+    DB<float> Q[kSym];
+    float *tau[kSym] = {nullptr};
     float4 *acc_tmp[kMaxPhases] = {nullptr};
     float *rd = nullptr, *cd = nullptr;
     float *fin[kMaxPhases] = {nullptr}, *fout[kMaxPhases] = {nullptr};
@@ -408,7 +418,7 @@ __global__ void __launch_bounds__(256) k_ct(ImmArgs a) {
     const float kap = powf(1.f - f1, -1.2f);
     float Q[9];
 #pragma unroll
-    for (int c = 0; c < 9; ++c) Q[c] = a.Q[c][r];
+    for (int c = 0; c < 9; ++c) Q[c] = a.Q[sym_of(c)][r];
     float QmI[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) QmI[c] = Q[c] - ((c % 4) == 0 ? 1.f : 0.f);
@@ -428,36 +438,41 @@ __global__ void __launch_bounds__(256) k_ct(ImmArgs a) {
             dQ[c] = (qg + gq - a.p.inv_relax * QmI[c] - beta * qq) * a.dt;
         }
     }
+    // update_ct_cuda (IMMCTCudaImpl.cu:716-744) element by element; the upper triangle is kept
+    // (the lower one differs from it only by the rounding of the (Q - I) Q products)
+    float Qn[kSym];
 #pragma unroll
-    for (int c = 0; c < 9; ++c) {
-        Q[c] += dQ[c];
-        a.Q[c][r] = Q[c];
-    }
+    for (int row = 0; row < 3; ++row)
+#pragma unroll
+        for (int col = row; col < 3; ++col) {
+            const int c = row * 3 + col;
+            Qn[sym_of(c)] = Q[c] + dQ[c];
+        }
+#pragma unroll
+    for (int k = 0; k < kSym; ++k) a.Q[k][r] = Qn[k];
     const float trD = 0.5f * (G[0] + G[0]) + 0.5f * (G[4] + G[4]) + 0.5f * (G[8] + G[8]);
     const float shear = sqrtf(0.5f * trD * trD);
     float vis = a.p.vis_base * kap;
     vis = fminf(vis, a.p.vis_max);
     vis = a.p.vis_base + (vis - a.p.vis_base) / (1.f + powf(10.f * shear, 5.f)) *
                              fminf(1.f, f1 / (a.p.theta + 1e-6f));
-    float t[12];
+    float t[kSym];
     const float d = powf(a.rd[r], 2.f);
 #pragma unroll
-    for (int c = 0; c < 9; ++c) {
-        const float tc = vis * (Q[c] - ((c % 4) == 0 ? 1.f : 0.f));
-        a.tau[c][r] = tc;
-        t[c] = tc / d;   // the tau_j / rho_j^2 term of add_phase_pct_acc_cuda, once per row
+    for (int k = 0; k < kSym; ++k) {
+        const float tc = vis * (Qn[k] - (sym_diag(k) ? 1.f : 0.f));
+        a.tau[k][r] = tc;
+        t[k] = tc / d;   // the tau_j / rho_j^2 term of add_phase_pct_acc_cuda, once per row
     }
-    t[9] = t[10] = t[11] = 0.f;
-    float4 *row = a.tpk + 4 * (size_t)r;
+    float4 *row = a.tpk + 3 * (size_t)r;
     row[0] = p;
     row[1] = make_float4(t[0], t[1], t[2], t[3]);
-    row[2] = make_float4(t[4], t[5], t[6], t[7]);
-    row[3] = make_float4(t[8], t[9], t[10], t[11]);
+    row[2] = make_float4(t[4], t[5], 0.f, 0.f);
 }
 
 struct PG {
     float4 q;
-    float t[9];   // tau_j / rho_j^2
+    float t[kSym];   // tau_j / rho_j^2, symmetric components
 };
 
 // Viscoelastic stress divergence (add_phase_pct_acc_cuda) + phase / mixture velocities.
@@ -468,9 +483,9 @@ __global__ void __launch_bounds__(256) k_pct(ImmArgs a) {
     const float4 p = a.pos[r];
     const float rdi = a.rd[r];
     const float inv_i = powf(rdi, 2.f);
-    float ti[9];
+    float ti[kSym];
 #pragma unroll
-    for (int c = 0; c < 9; ++c) ti[c] = a.tau[c][r] / inv_i;
+    for (int k = 0; k < kSym; ++k) ti[k] = a.tau[k][r] / inv_i;
     float ax = 0.f, ay = 0.f, az = 0.f;
     const uint32_t n = a.ncnt[r];
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
@@ -478,12 +493,12 @@ __global__ void __launch_bounds__(256) k_pct(ImmArgs a) {
                 [&](uint32_t j) {
                     PG e{};
                     if (j >= a.nf) return e;
-                    // the neighbour's packed row: {x, V}, tau_j / rho_j^2 (two 256-bit loads)
-                    const F4x2 h0 = ldg8(a.tpk + 4 * (size_t)j), h1 = ldg8(a.tpk + 4 * (size_t)j + 2);
-                    e.q = h0.a;
-                    e.t[0] = h0.b.x; e.t[1] = h0.b.y; e.t[2] = h0.b.z; e.t[3] = h0.b.w;
-                    e.t[4] = h1.a.x; e.t[5] = h1.a.y; e.t[6] = h1.a.z; e.t[7] = h1.a.w;
-                    e.t[8] = h1.b.x;
+                    // the neighbour's packed row: {x, V}, tau_j / rho_j^2 (48 bytes)
+                    const float4 *row = a.tpk + 3 * (size_t)j;
+                    const float4 h1 = ldg4(row + 1), h2 = ldg4(row + 2);
+                    e.q = ldg4(row);
+                    e.t[0] = h1.x; e.t[1] = h1.y; e.t[2] = h1.z; e.t[3] = h1.w;
+                    e.t[4] = h2.x; e.t[5] = h2.y;
                     return e;
                 },
                 [&](uint32_t j, const PG &e) {
@@ -491,12 +506,12 @@ __global__ void __launch_bounds__(256) k_pct(ImmArgs a) {
                     const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
                     const float g = cubic_g(dist2(rx, ry, rz), a.k);
                     const float w0 = g * rx, w1 = g * ry, w2 = g * rz;
-                    float M[9];
+                    float M[kSym];
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) M[c] = ti[c] + e.t[c];
+                    for (int k = 0; k < kSym; ++k) M[k] = ti[k] + e.t[k];
                     ax += M[0] * w0 + M[1] * w1 + M[2] * w2;
-                    ay += M[3] * w0 + M[4] * w1 + M[5] * w2;
-                    az += M[6] * w0 + M[7] * w1 + M[8] * w2;
+                    ay += M[1] * w0 + M[3] * w1 + M[4] * w2;
+                    az += M[2] * w0 + M[4] * w1 + M[5] * w2;
                 });
     const float s = a.frac[1][r] * rdi;
     ax *= s; ay *= s; az *= s;
@@ -840,7 +855,7 @@ int immct_alloc(vtp_solver &s) {
         if ((rc = s.alloc(&m.fin[k], nf))) return rc;
         if ((rc = s.alloc(&m.fout[k], nf))) return rc;
     }
-    for (int c = 0; c < 9; ++c) {
+    for (int c = 0; c < vtp::kSym; ++c) {
         for (int b = 0; b < 2; ++b)
             if ((rc = s.alloc(&m.Q[c].b[b], nf))) return rc;
         if ((rc = s.alloc(&m.tau[c], nf))) return rc;
@@ -851,7 +866,7 @@ int immct_alloc(vtp_solver &s) {
     if ((rc = s.alloc(&m.flag, nf))) return rc;
     if ((rc = s.alloc(&m.counter, 6))) return rc;
     if ((rc = s.alloc(&m.work, nf))) return rc;
-    if (m.p.ct && (rc = s.alloc(&m.tpk, 4 * (size_t)nf))) return rc;
+    if (m.p.ct && (rc = s.alloc(&m.tpk, 3 * (size_t)nf))) return rc;
     if ((rc = s.alloc(&m.pk2, 2 * (size_t)nf))) return rc;
     CUI(cudaMemsetAsync(m.flag, 0, nf * sizeof(uint32_t), s.st));
     CUI(cudaMemsetAsync(m.counter, 0, 6 * sizeof(uint32_t), s.st));
@@ -887,7 +902,7 @@ static ImmArgs imm_args(vtp_solver &s) {
         a.fin[k] = m.fin[k];
         a.fout[k] = m.fout[k];
     }
-    for (int c = 0; c < 9; ++c) {
+    for (int c = 0; c < vtp::kSym; ++c) {
         a.Q[c] = m.Q[c].c();
         a.tau[c] = m.tau[c];
     }
@@ -926,9 +941,9 @@ int immct_init(vtp_solver &s) {
         CUI(cudaStreamSynchronize(s.st));
     }
     std::vector<float> one(nf, 1.f), zero(nf, 0.f);
-    for (int c = 0; c < 9; ++c)
+    for (int c = 0; c < vtp::kSym; ++c)
         for (int b = 0; b < 2; ++b)
-            CUI(cudaMemcpyAsync(m.Q[c].b[b], (c % 4) == 0 ? one.data() : zero.data(), nf * sizeof(float),
+            CUI(cudaMemcpyAsync(m.Q[c].b[b], vtp::sym_diag(c) ? one.data() : zero.data(), nf * sizeof(float),
                                 cudaMemcpyHostToDevice, s.st));
     m.bfrac.assign(s.hphase.begin(), s.hphase.end());
     m.have_tension = s.gamma != 0.f;
@@ -950,7 +965,7 @@ void immct_fill_carry(vtp_solver &s, vtp::Carry &carry) {
         carry.src1[carry.nf1] = m.frac[k].c();
         carry.dst1[carry.nf1++] = m.frac[k].n();
     }
-    for (int c = 0; c < 9; ++c) {
+    for (int c = 0; c < vtp::kSym; ++c) {
         carry.src1[carry.nf1] = m.Q[c].c();
         carry.dst1[carry.nf1++] = m.Q[c].n();
     }
@@ -964,7 +979,7 @@ int immct_copy_back(vtp_solver &s) {
         CUI(cudaMemcpyAsync(m.vph[k].c(), m.vph[k].n(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
         CUI(cudaMemcpyAsync(m.frac[k].c(), m.frac[k].n(), nf * sizeof(float), cudaMemcpyDeviceToDevice, s.st));
     }
-    for (int c = 0; c < 9; ++c)
+    for (int c = 0; c < vtp::kSym; ++c)
         CUI(cudaMemcpyAsync(m.Q[c].c(), m.Q[c].n(), nf * sizeof(float), cudaMemcpyDeviceToDevice, s.st));
     return VTP_OK;
 }
@@ -973,7 +988,7 @@ void immct_set_parity(vtp_solver &s, int cur) {
     // Phase arrays swap together with the row order once per substep.
     ImmState &m = *s.imm;
     for (int k = 0; k < m.p.P; ++k) m.vph[k].cur = cur, m.frac[k].cur = cur;
-    for (int c = 0; c < 9; ++c) m.Q[c].cur = cur;
+    for (int c = 0; c < vtp::kSym; ++c) m.Q[c].cur = cur;
 }
 
 uint32_t immct_last_retries(vtp_solver &s, uint64_t *body_launches) {
@@ -1007,6 +1022,7 @@ void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which) {
 }
 
 int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
+    const vtp::NvtxRange nvtx_range("vtp IMM substep");
     ImmState &m = *s.imm;
     const int P = m.p.P;
     const int B = s.block;
@@ -1022,7 +1038,7 @@ int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture) {
                    s.orig.n(), carry, 0.f, s.u, s.u.fstart, s.prof);
     s.pos.swap(); s.vel.swap(); s.orig.swap(); s.vadv.swap();
     for (int k = 0; k < P; ++k) m.vph[k].swap(), m.frac[k].swap();
-    for (int c = 0; c < 9; ++c) m.Q[c].swap();
+    for (int c = 0; c < vtp::kSym; ++c) m.Q[c].swap();
     auto P_ = [&](const char *nm, auto &&fn) {
         if (s.prof) s.prof->begin();
         fn();
@@ -1154,9 +1170,12 @@ int immct_get_field(vtp_solver &s, int field, float *dev_out, size_t elems) {
         for (uint32_t r = nf; r < n; ++r)
             if (field == VTP_FIELD_CONFORMATION)
                 for (int c = 0; c < 9; ++c) out[(size_t)ids[r] * 9 + c] = (c % 4) == 0 ? 1.f : 0.f;
-        for (int c = 0; c < 9; ++c) {
-            if ((rc = fetch(field == VTP_FIELD_CONFORMATION ? m.Q[c].c() : m.tau[c], tmp))) return rc;
-            for (uint32_t r = 0; r < nf; ++r) out[(size_t)ids[r] * 9 + c] = tmp[r];
+        // returned as full 3x3 row-major matrices, as the reference stores them
+        for (int k = 0; k < vtp::kSym; ++k) {
+            if ((rc = fetch(field == VTP_FIELD_CONFORMATION ? m.Q[k].c() : m.tau[k], tmp))) return rc;
+            for (int c = 0; c < 9; ++c)
+                if (vtp::sym_of(c) == k)
+                    for (uint32_t r = 0; r < nf; ++r) out[(size_t)ids[r] * 9 + c] = tmp[r];
         }
     } else if (field == VTP_FIELD_CD || field == VTP_FIELD_REST_DENSITY || field == VTP_FIELD_MASS) {
         std::vector<float> rdv, cdv;

@@ -62,10 +62,12 @@ def kernel_bytes(kind: str, name: str, N: int, Nf: int, K: int, k: float, P: int
         state = 32 * N + (16 * P + 8) * Nf + 16 * P * Nf + 32 * Nf
     elif name == "imm_tension":
         state = 36 * N + 16 * P * Nf + 32 * Nf
-    elif name == "immct_ct":                # pos, vel, rest density gathered; Q read+write, tau written
-        state = 36 * N + 16 * Nf + 72 * Nf + 36 * Nf
-    elif name == "immct_pct":               # pos, rest density, tau gathered; phase velocities updated
-        state = 56 * N + 32 * P * Nf + 32 * Nf
+    elif name == "immct_ct":                # pos, vel, rest density gathered; symmetric Q read + write (6
+        # floats each), symmetric tau written, the 48-byte packed stress row written
+        state = 36 * N + 16 * Nf + 48 * Nf + 24 * Nf + 48 * Nf
+    elif name == "immct_pct":               # packed {x, V, tau / rho^2} rows (48 B) gathered, own tau read,
+        # phase velocities updated
+        state = 48 * N + 24 * Nf + 32 * P * Nf + 32 * Nf
     elif name == "imm_drift_diffuse":       # pos, vel, flag, fractions, phase velocities gathered
         state = (36 + 20 * P) * N + 8 * P * Nf
     elif name == "imm_apply_pressure":
