@@ -360,10 +360,13 @@ def run_batched(args, rank, world, local, dist, torch):
     from vtp.dist import scene_share
     mix = vtp.scenes.batched_scenes()
     mine = scene_share(mix, world, rank)
-    extra = json.loads(args.extra) if args.extra else {}
-    if args.block:
-        extra["blockSize"] = args.block
-    extra = extra or None
+    # per solver type: --extra, or the autotuned block of that half of the mix
+    extras = {}
+    for kind in ("PBF", "DFSPH"):
+        e = json.loads(args.extra) if args.extra else default_extra(f"batched_{kind.lower()}")
+        if args.block:
+            e["blockSize"] = args.block
+        extras[kind] = e or None
     groups = {}
     for k in mine:
         groups.setdefault(mix[k].solver, []).append(k)
@@ -372,7 +375,7 @@ def run_batched(args, rank, world, local, dist, torch):
         if kind not in groups:
             continue
         idx = groups[kind]
-        b, ranges = vtp.solver_from_scenes([mix[k] for k in idx], extra)
+        b, ranges = vtp.solver_from_scenes([mix[k] for k in idx], extras[kind])
         assert b.initialize(), b.last_error
         batches.append((kind, idx, b, ranges))
     for _, _, b, _ in batches:
@@ -442,14 +445,14 @@ def run_batched(args, rank, world, local, dist, torch):
 
     cfg = {"workload": "batched", "scenes": len(mix), "pbf_scenes": sum(m.solver == "PBF" for m in mix),
            "fluid": nf_all, "boundary": sum(m.n_boundary for m in mix), "scenes_this_rank": len(mine),
-           "parallelism": f"scenes-lpt{world}", "wall_ms_per_step": 1e3 * wall / args.steps,
+           "parallelism": f"scenes-lpt{world}", "wall_ms_per_step": 1e3 * wall / args.steps, "b200": extras,
            "l2": "inputs larger than L2 (~9.2M particles of state and neighbour lists)"}
     if world == 1 and not args.no_loop_baseline:
         # The plain per-scene loop: one solver per scene, scenes one after another.
         loop_ms = 0.0
         same = True
         for k, m in enumerate(mix):
-            s = vtp.solver_from_scene(m, extra)
+            s = vtp.solver_from_scene(m, extras[m.solver])
             assert s.initialize(), s.last_error
             if args.warmup:
                 assert s.tickNsteps(args.warmup), s.last_error
@@ -612,12 +615,23 @@ def run_diff(args, torch) -> dict:
 
 
 DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "immct_500k": 30, "batched": 200, "diff_pbf": 200}
-# "B200" config keys per workload when --extra is not given: 8 lanes per row for the
-# 16k-particle PBF scene (vtp/autotune.py --lanes picks it); the DFSPH 1M scene steps with the
-# adaptive CFL 0.4 rule capped at its 1 ms timeStep, as the benchmark's configuration states
-# (the dam break stays below 4 m/s over the timed substeps, so the step is the cap throughout,
-# the same work as the reference's fixed step).
-DEFAULT_EXTRA = {"pbf": {"rowLanes": 8}, "dfsph_1m": {"cfl": 0.4}}
+# "B200" keys a workload always runs with, beside the autotuned ones: the DFSPH 1M scene steps
+# with the adaptive CFL 0.4 rule capped at its 1 ms timeStep, as the benchmark's configuration
+# states (the dam break stays below 4 m/s over the timed substeps, so the step is the cap
+# throughout, the same work as the reference's fixed step).
+FIXED_EXTRA = {"dfsph_1m": {"cfl": 0.4}}
+
+
+def default_extra(workload: str) -> dict:
+    """The "B200" block a workload runs with when --extra is not given: the autotuner's cached
+    launch configuration for it on this GPU (vtp/tuned.json, written by vtp/autotune.py --write)
+    plus the workload's fixed keys."""
+    from vtp import autotune
+    extra = autotune.tuned_extra(workload)
+    extra.update(FIXED_EXTRA.get(workload, {}))
+    return extra
+
+
 L2_BYTES = 126e6
 
 
@@ -719,7 +733,7 @@ def main():
             print(json.dumps(line), flush=True)
         return 0
     sc = make_scene(args.workload)
-    extra = json.loads(args.extra) if args.extra else dict(DEFAULT_EXTRA.get(args.workload, {}))
+    extra = json.loads(args.extra) if args.extra else default_extra(args.workload)
     if args.block:
         extra["blockSize"] = args.block
     s = vtp.solver_from_scene(sc, extra=extra or None)

@@ -1,80 +1,219 @@
-"""Launch-configuration autotuner for the neighbour passes.
+"""Launch-configuration autotuner for the neighbour passes, and its cache.
 
-Sweeps threads per block (= rows per scene-offset tile), the neighbour-loop
-unroll (neighbours kept in flight per thread), the lanes per row of the PBF
-passes and the tile-grid mode of the pressure-solve passes (one block per
-tile, or a persistent grid) on a scene
-or a batch of scenes, timing each candidate with the per-kernel CUDA-event
-profiler of the library, and returns the fastest configuration for the
-substep.  Results are plain dicts so callers can cache them
-(``"B200": {"blockSize": b, "unroll": u, "persistentTiles": p, "rowLanes": l}``
-in the solver config).
+Tuned dimensions (keys of the solver config's "B200" block):
+  * blockSize  - threads per block = fluid rows per scene-offset tile of the
+                 pressure solve (32..256);
+  * unroll     - neighbour-list entries whose gathers a thread keeps in
+                 flight (1, 2, 4, 8);
+  * cell tile  - how rows are grouped into cells and cell tiles: "linear"
+                 (the reference's cell order), "brick" (4 x 4 x 4-cell
+                 bricks, Morton order inside) or, for DFSPH, "staged" (bricks
+                 whose neighbourhoods the pressure solve copies into shared
+                 memory; "cellOrder" / "stagedSolve" / "stageRows");
+  * rowLanes   - threads per row of the PBF neighbour passes (1, 4, 8);
+  * listLanes  - threads per row of the list builder (0: by row count, 1, 8).
+Every candidate is timed with the library's per-kernel CUDA-event profiler
+(the substep's kernel time), by coordinate descent from the current best:
+each dimension in turn is swept with the others fixed, until a full pass
+changes nothing.  `tune` takes the measurement as a function, so the search
+itself runs without a GPU (tests/test_autotune.py).
+
+Results are cached in vtp/tuned.json, keyed by the GPU's name and a workload
+key (solver type and fluid-particle count rounded to a power of two, or a
+named workload); `tuned_extra` returns the cached "B200" block, which
+bench.py and batched runs apply by default.  Keys that change FP32 arithmetic
+(rowLanes) are tuned only when the caller allows it: a batched run and the
+per-scene runs it is compared with must share them.
 """
 from __future__ import annotations
 
-import itertools
 import json
+import math
 import time
+from pathlib import Path
 
-from .solver import solver_from_scene, solver_from_scenes
+CACHE = Path(__file__).resolve().parent / "tuned.json"
 
-BLOCKS = (64, 128, 256)
-UNROLLS = (1, 2, 4, 8)
-PERSISTENT = (False,)
-ROW_LANES = (1,)
+DIMENSIONS = {
+    "blockSize": (64, 128, 256),
+    "unroll": (1, 2, 4, 8),
+    "cellTile": ("brick", "linear", "staged"),
+    "rowLanes": (1, 4, 8),
+    "listLanes": (0, 1, 8),
+}
+DEFAULTS = {"blockSize": 128, "unroll": 4, "cellTile": "brick", "rowLanes": 1, "listLanes": 0}
+# Dimensions each solver type has (the others leave its kernels unchanged).
+SOLVER_DIMS = {
+    "PBF": ("blockSize", "unroll", "cellTile", "rowLanes", "listLanes"),
+    "DFSPH": ("blockSize", "unroll", "cellTile", "listLanes"),
+    "IMM": ("blockSize", "unroll", "cellTile", "listLanes"),
+    "IMMCT": ("blockSize", "unroll", "cellTile", "listLanes"),
+}
 
 
-def tune(scene, warmup: int = 3, steps: int = 3, blocks=BLOCKS, unrolls=UNROLLS, persistent=PERSISTENT,
-         lanes=ROW_LANES, verbose: bool = False) -> dict:
-    """Return {"best": {...}, "trials": [...]} for one scene, or a list of scenes of one
-    solver type (tuned as one batched solver)."""
-    trials = []
-    for b, u, pt, ln in itertools.product(blocks, unrolls, persistent, lanes):
-        extra = {"blockSize": b, "unroll": u, "persistentTiles": bool(pt), "rowLanes": ln}
+def to_config(point: dict) -> dict:
+    """The "B200" config keys of a search point."""
+    out = {k: point[k] for k in ("blockSize", "unroll", "rowLanes", "listLanes") if k in point}
+    tile = point.get("cellTile", "brick")
+    out["cellOrder"] = "linear" if tile == "linear" else "brick"
+    out["stagedSolve"] = tile == "staged"
+    return out
+
+
+def dims_for(solver: str, allow_arithmetic: bool = True) -> tuple:
+    """Tuned dimensions of a solver type; without `allow_arithmetic`, only those that leave the
+    FP32 results unchanged."""
+    d = SOLVER_DIMS[solver]
+    if not allow_arithmetic:
+        d = tuple(x for x in d if x != "rowLanes")
+    return d
+
+
+def candidates(dim: str, solver: str) -> tuple:
+    vals = DIMENSIONS[dim]
+    if dim == "cellTile" and solver != "DFSPH":
+        vals = tuple(v for v in vals if v != "staged")
+    return vals
+
+
+def tune(measure, solver: str, dims=None, start: dict | None = None, max_passes: int = 3,
+         verbose: bool = False) -> dict:
+    """Coordinate descent over `dims`: measure(config) -> milliseconds per substep (inf for a
+    configuration that fails).  Returns {"best": point, "ms_per_step", "trials": [...]}; every
+    configuration is measured once."""
+    dims = tuple(dims or SOLVER_DIMS[solver])
+    best = dict(DEFAULTS)
+    best.update(start or {})
+    best = {k: best[k] for k in dims}
+    seen = {}
+
+    def cost(point):
+        key = json.dumps(point, sort_keys=True)
+        if key not in seen:
+            try:
+                ms = float(measure(to_config(point)))
+            except Exception:   # a configuration the solver rejects
+                ms = math.inf
+            seen[key] = ms
+            if verbose:
+                print(json.dumps({"point": point, "ms_per_step": ms}), flush=True)
+        return seen[key]
+
+    best_ms = cost(best)
+    for _ in range(max_passes):
+        changed = False
+        for dim in dims:
+            for v in candidates(dim, solver):
+                if v == best[dim]:
+                    continue
+                p = dict(best)
+                p[dim] = v
+                ms = cost(p)
+                if ms < best_ms:
+                    best, best_ms, changed = p, ms, True
+        if not changed:
+            break
+    trials = [{"point": json.loads(k), "ms_per_step": v} for k, v in seen.items()]
+    return {"best": best, "config": to_config(best), "ms_per_step": best_ms, "trials": trials,
+            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+def library_measure(scene, warmup: int = 3, steps: int = 3, base_extra: dict | None = None):
+    """measure(config) for `tune`: the substep's kernel time of `scene` (or a list of scenes of
+    one solver type, run as one batched solver) with the per-kernel CUDA-event profiler."""
+    from .solver import solver_from_scene, solver_from_scenes
+
+    def measure(cfg: dict) -> float:
+        extra = dict(base_extra or {})
+        extra.update(cfg)
         if isinstance(scene, (list, tuple)):
             s, _ = solver_from_scenes(list(scene), extra=extra)
         else:
             s = solver_from_scene(scene, extra=extra)
-        s.initialize()
-        if warmup:
-            s.tickNsteps(warmup)
-        prof = s.profile_kernels(steps)
-        s.destroy()
-        total = sum(v[0] for v in prof.values())
-        rec = {"blockSize": b, "unroll": u, "persistentTiles": bool(pt), "rowLanes": ln, "ms_per_step": total / steps,
-               "kernels": {k: v[0] / max(v[1], 1) for k, v in prof.items()}}
-        trials.append(rec)
-        if verbose:
-            print(json.dumps({k: rec[k] for k in ("blockSize", "unroll", "persistentTiles", "rowLanes",
-                                                  "ms_per_step")}),
-                  flush=True)
-    best = min(trials, key=lambda r: r["ms_per_step"])
-    return {"best": {"blockSize": best["blockSize"], "unroll": best["unroll"],
-                     "persistentTiles": best["persistentTiles"], "rowLanes": best["rowLanes"]}, "trials": trials,
-            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+        try:
+            if not s.initialize():
+                return math.inf
+            if warmup and not s.tickNsteps(warmup):
+                return math.inf
+            prof = s.profile_kernels(steps)
+            return sum(v[0] for v in prof.values()) / steps
+        finally:
+            s.destroy()
+    return measure
+
+
+def workload_key(solver: str, n_fluid: int, name: str | None = None) -> str:
+    """Cache key of a workload: a named workload, or the solver type and the fluid-particle
+    count rounded to the nearest power of two."""
+    if name:
+        return name
+    return f"{solver}:2^{max(0, round(math.log2(max(n_fluid, 1))))}"
+
+
+def gpu_name() -> str:
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name(0)
+    except Exception:
+        pass
+    return "unknown"
+
+
+def load_cache(path: Path = CACHE) -> dict:
+    try:
+        return json.loads(Path(path).read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def store(key: str, result: dict, gpu: str | None = None, path: Path = CACHE) -> dict:
+    """Record a tuning result (its "B200" config keys and timing) in the cache file."""
+    cache = load_cache(path)
+    cache.setdefault(gpu or gpu_name(), {})[key] = {"B200": result["config"], "ms_per_step": result["ms_per_step"],
+                                                    "when": result.get("when")}
+    Path(path).write_text(json.dumps(cache, indent=1, sort_keys=True) + "\n")
+    return cache
+
+
+def tuned_extra(key: str, gpu: str | None = None, path: Path = CACHE) -> dict:
+    """The cached "B200" block for a workload key on this GPU ({} when none is cached).  A
+    B200 whose name string is not in the cache takes the entry of another B200 name."""
+    cache = load_cache(path)
+    g = gpu or gpu_name()
+    entry = cache.get(g, {}).get(key)
+    if entry is None and "B200" in g:
+        for name, table in cache.items():
+            if "B200" in name and key in table:
+                entry = table[key]
+                break
+    return dict(entry["B200"]) if entry else {}
 
 
 if __name__ == "__main__":
     import argparse
     import sys
-    from pathlib import Path
 
     sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
     from vtp import scenes
 
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--scene", default="dfsph_1m", choices=["dfsph_1m", "pbf", "batched_pbf", "batched_dfsph"])
-    ap.add_argument("--persistent", action="store_true", help="also try the persistent tile grid")
-    ap.add_argument("--lanes", action="store_true", help="also try 4 and 8 lanes per row (PBF passes)")
+    ap = argparse.ArgumentParser(description="tune a workload on this GPU and record it in vtp/tuned.json")
+    ap.add_argument("--workload", default="dfsph_1m",
+                    choices=["dfsph_1m", "pbf", "immct_500k", "batched_pbf", "batched_dfsph"])
+    ap.add_argument("--write", action="store_true", help="record the result in the cache")
+    ap.add_argument("--no-arithmetic", action="store_true",
+                    help="leave out keys that change FP32 arithmetic (rowLanes)")
     a = ap.parse_args()
-    if a.scene.startswith("batched"):
-        mix = scenes.batched_scenes()
-        sc = [m for m in mix if m.solver == ("PBF" if a.scene == "batched_pbf" else "DFSPH")]
+    base = {}
+    if a.workload.startswith("batched"):
+        kind = "PBF" if a.workload == "batched_pbf" else "DFSPH"
+        sc = [m for m in scenes.batched_scenes() if m.solver == kind]
     else:
-        sc = scenes.dfsph_1m() if a.scene == "dfsph_1m" else scenes.pbf_dam_break()
-    res = tune(sc, persistent=(False, True) if a.persistent else PERSISTENT,
-               lanes=(1, 4, 8) if a.lanes else ROW_LANES, verbose=True)
-    print(json.dumps({"best": res["best"], "trials": [{k: t[k] for k in t if k != "kernels"} for t in res["trials"]]}))
-    for t in res["trials"]:
-        print(t["blockSize"], t["unroll"], t["persistentTiles"], t["rowLanes"],
-              json.dumps({k: round(v, 4) for k, v in sorted(t["kernels"].items())}))
+        sc = {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k}[a.workload]()
+        kind = sc.solver
+        if a.workload == "dfsph_1m":
+            base = {"cfl": 0.4}
+    res = tune(library_measure(sc, base_extra=base), kind, dims_for(kind, not a.no_arithmetic), verbose=True)
+    print(json.dumps({k: res[k] for k in ("best", "config", "ms_per_step")}))
+    if a.write:
+        store(a.workload, res)
