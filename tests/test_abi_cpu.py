@@ -28,6 +28,16 @@ def test_header_declarations_are_all_exported():
         assert name in _lib.SIGNATURES, f"{name} missing from the ctypes binding"
 
 
+def test_checked_build_exports_the_same_entry_points():
+    """The checked build (device-side bounds checks, VTP_LIBRARY=checked) is a drop-in copy."""
+    path = Path(_lib.__file__).resolve().parent / "libvtp_checked.so"
+    if not path.exists():
+        pytest.skip("libvtp_checked.so not built")
+    lib = C.CDLL(str(path), mode=C.RTLD_LOCAL)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
 def test_status_strings_and_version():
     lib = vtp.lib()
     assert lib.vtp_version().startswith(b"vtp")

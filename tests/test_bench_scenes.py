@@ -117,7 +117,23 @@ FD_DIRECTIONS = 32
 
 
 def test_diff_pbf_64k_adjoint_matches_fd_32_directions(vtp_gpu, oracle_lib):
-    """The benchmark's differentiable-PBF check at its own size and horizon."""
+    """The benchmark's differentiable-PBF check at its own size and horizon:
+    64,000 fluid particles, 200 substeps, checkpoints every 20, 32 random unit
+    directions in (v0, XSPH_k), neighbour lists frozen to the GPU's.
+
+    Three derivatives per direction: the GPU adjoint (FP32), the FP64 oracle's
+    adjoint of the same discrete map (or_pbf_step_adjoint over an FP64 rollout),
+    and FP64 central finite differences (eps 1e-4).  The loss is only piecewise
+    smooth: the density clamp rho = max(rho, rho0) switches particles in and out
+    of the constraint, and over 200 substeps many switch within any finite eps,
+    so a secant can differ from the derivative at eps = 0 (the probe that led
+    to this test measured, on its worst direction, FD 1.27e-3 from the FP64
+    adjoint at eps 1e-4 and 1e-6, 1.17e-3 at 1e-7).  The bars: the GPU adjoint
+    within 1e-3 of the FP64 adjoint on every direction (measured <= 7.4e-5);
+    the GPU adjoint within 1e-3 of FD on every direction where the FP64
+    adjoint is (measured: all but one of 32, median 2.7e-4); and where it is
+    not, the GPU adjoint is as close to FD as the FP64 adjoint (within 1e-3
+    of the same secant, with the FD excess shared)."""
     from vtp import diff
     sc = vtp_gpu.scenes.diff_pbf()
     mask = diff.fluid_mask(sc)
@@ -138,9 +154,15 @@ def test_diff_pbf_64k_adjoint_matches_fd_32_directions(vtp_gpu, oracle_lib):
 
     d = oracle_lib.PbfDiff(sc)
     x0, v0 = d.base.pos.copy(), d.base.vel.copy()
+    x64, _, states, used = d.rollout(x0, v0, T, lists=lists, record=True)
+    m64 = x64[mask].mean(0)
+    xbar = np.zeros_like(x64)
+    xbar[mask] = 2.0 * (m64 - target) / nf
+    _, ov, ok = d.adjoint(states, used, xbar, np.zeros_like(xbar))
+    del states, used
     rng = np.random.default_rng(5006)
     k0 = d.p.xsph_k
-    errs = []
+    e_gpu_adj, e_gpu_fd, e_adj_fd = [], [], []
     for _ in range(FD_DIRECTIONS):
         dv = np.zeros_like(v0)
         dv[mask] = rng.normal(size=(nf, 3))
@@ -156,7 +178,17 @@ def test_diff_pbf_64k_adjoint_matches_fd_32_directions(vtp_gpu, oracle_lib):
             return float(((mm - target) ** 2).sum())
         fd = (L(1e-4) - L(-1e-4)) / 2e-4
         ad = float((gv.astype(np.float64) * dv).sum() + gk * dk)
-        errs.append(abs(ad - fd) / abs(fd))
-    print(f"diff PBF 64k, {T} substeps, {FD_DIRECTIONS} directions: max rel err {max(errs):.2e}, "
-          f"median {float(np.median(errs)):.2e}")
-    assert max(errs) < 1e-3
+        a64 = float((ov * dv).sum() + ok * dk)
+        e_gpu_adj.append(abs(ad - a64) / abs(a64))
+        e_gpu_fd.append(abs(ad - fd) / abs(fd))
+        e_adj_fd.append(abs(a64 - fd) / abs(fd))
+    e_gpu_adj, e_gpu_fd, e_adj_fd = map(np.array, (e_gpu_adj, e_gpu_fd, e_adj_fd))
+    print(f"diff PBF 64k, {T} substeps, {FD_DIRECTIONS} directions: GPU adjoint vs FP64 adjoint max "
+          f"{e_gpu_adj.max():.2e}; GPU adjoint vs FD max {e_gpu_fd.max():.2e} median {np.median(e_gpu_fd):.2e} "
+          f"({int((e_gpu_fd > 1e-3).sum())} over 1e-3); FP64 adjoint vs FD max {e_adj_fd.max():.2e}")
+    assert e_gpu_adj.max() < 1e-3
+    smooth = e_adj_fd < 1e-3
+    assert smooth.sum() >= FD_DIRECTIONS - 2
+    assert np.all(e_gpu_fd[smooth] < 1e-3)
+    assert np.all(np.abs(e_gpu_fd - e_adj_fd)[~smooth] < 1e-3)
+    assert np.median(e_gpu_fd) < 5e-4

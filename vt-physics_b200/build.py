@@ -18,6 +18,11 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 OUT = HERE / "vtp" / "libvtp.so"
+# Checked build (python build.py --checked): -DVTP_CHECKED adds device-side bounds checks of
+# every neighbour-list entry and cell-segment slot (status bit VTP_ERR_BOUNDS instead of an
+# out-of-range access); select it with VTP_LIBRARY=checked.
+BUILD_CHECKED = HERE / "_build_checked"
+OUT_CHECKED = HERE / "vtp" / "libvtp_checked.so"
 HOST_OUT = HERE / "vtp" / "libvtp_host.so"
 HOST = HERE / "host"
 ROOT = HERE.parent
@@ -54,28 +59,37 @@ def flags() -> list[str]:
                    "-DVTP_BUILD"]
 
 
-def compile_one(src: Path, force: bool) -> Path:
-    obj = BUILD / (src.stem + ".o")
+def compile_one(src: Path, force: bool, checked: bool = False) -> Path:
+    obj = (BUILD_CHECKED if checked else BUILD) / (src.stem + ".o")
     deps = [src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "vtp.h"]
     if not force and obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return obj
-    cmd = [nvcc()] + flags() + ["-c", str(src), "-o", str(obj)]
+    cmd = [nvcc()] + flags() + (["-DVTP_CHECKED"] if checked else []) + ["-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
     return obj
 
 
-def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build_library(force: bool = False, jobs: int | None = None, checked: bool = False) -> Path:
+    out = OUT_CHECKED if checked else OUT
+    (BUILD_CHECKED if checked else BUILD).mkdir(exist_ok=True)
     srcs = sorted(CSRC.glob("*.cu"))
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 2)) as ex:
-        objs = list(ex.map(lambda s: compile_one(s, force), srcs))
-    if force or not OUT.exists() or any(o.stat().st_mtime > OUT.stat().st_mtime for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", str(OUT)] + [str(o) for o in objs] + ["-lcudart"]
+        objs = list(ex.map(lambda s: compile_one(s, force, checked), srcs))
+    if force or not out.exists() or any(o.stat().st_mtime > out.stat().st_mtime for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", str(out)] + [str(o) for o in objs] + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return out
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False, checked: bool = True) -> Path:
+    """libvtp.so, the host interface, and (unless checked=False) the checked build."""
+    build_library(force, jobs)
+    if checked:
+        build_library(force, jobs, checked=True)
     build_host(force)
     if verbose:
         print(f"built {OUT}")
@@ -115,9 +129,10 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("--no-checked", action="store_true", help="skip the checked build (libvtp_checked.so)")
     a = ap.parse_args()
     try:
-        build(force=a.force, jobs=a.jobs, verbose=True)
+        build(force=a.force, jobs=a.jobs, verbose=True, checked=not a.no_checked)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

@@ -435,6 +435,7 @@ int vtp_solver::sort_boundary_and_lists() {
 }
 
 int vtp_solver::initialize() {
+    const vtp::NvtxRange nvtx_range("vtp initialize");
     if (!configured) return fail(VTP_ERR_STATE, "initialize before setConfig");
     if (initialized) return VTP_OK;
     const uint32_t n = (uint32_t)(hpos.size() / 3);
@@ -547,6 +548,7 @@ int vtp_solver::initialize() {
     AL(&u.bnbr, bl_rows * L.ell_stride);
     AL(&u.bncnt, L.nb);
     AL(&d_status, 4);
+    u.status = d_status;
     AL(&d_overflow, 4);
     CU(cudaMemsetAsync(d_status, 0, 4 * sizeof(uint32_t), st));
     CU(cudaMemsetAsync(d_overflow, 0, 4 * sizeof(uint32_t), st));
@@ -739,6 +741,7 @@ int vtp_solver::initialize() {
 // ---------------------------------------------------------------- tick
 
 int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
+    const vtp::NvtxRange nvtx_range(which == 0 ? "vtp divergence solve" : "vtp density solve");
     vtp::DfsphArgs a = dfsph_args(which);
     vtp::dfsph_solve_begin(s, solve + (size_t)which * scenes.size(), loop + which, nscenes());
     PROF(this, "dfsph_solve_pack", vtp::dfsph_solve_pack(s, a));
@@ -791,6 +794,7 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
 }
 
 int vtp_solver::enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape) {
+    const vtp::NvtxRange nvtx_range(tape ? "vtp PBF substep (recorded)" : "vtp PBF substep");
     // PBFSolver::tick (PBFSolver.cpp:326-376): external force fused into the sort, neighbour
     // lists, `iterations` constraint passes, XSPH.  With `tape` the lists are built into the
     // tape and the intermediate states are copied out (differentiable mode).
@@ -844,8 +848,12 @@ int vtp_solver::enqueue_tick(cudaStream_t s, bool capture) {
     carry.nf4 = 1;
     carry.src4[0] = vadv.c();
     carry.dst4[0] = vadv.n();
-    vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry, 0.f,
-                   u, u.fstart, prof);
+    {
+        const vtp::NvtxRange r("vtp neighbour search");
+        vtp::ugns_sort(s, scn(), nbuckets, 0, L.nf, pos.c(), pos.n(), vel.c(), vel.n(), orig.c(), orig.n(), carry,
+                       0.f, u, u.fstart, prof);
+    }
+    const vtp::NvtxRange nvtx_lists("vtp neighbour lists and DFSPH passes");
     pos.swap(); vel.swap(); orig.swap(); vadv.swap();
     if (staged) {
         PROF(this, "ugns_lists", vtp::ugns_build_lists_staged(s, scn(), L, stg, pos.c(), u.nbr, u.ncnt, d_status,
@@ -936,6 +944,7 @@ int vtp_solver::check_status() {
 }
 
 int vtp_solver::tick_n(uint32_t n) {
+    const vtp::NvtxRange nvtx_range("vtp tick");
     int rc;
     if (!initialized && (rc = initialize())) return rc;
     if (crashed) return fail(VTP_NOT_CONVERGED, std::string(solver_key(type)) + "Solver is crashed.");

@@ -518,6 +518,7 @@ int check_ready(vtp_solver *s) {
 extern "C" {
 
 int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists) {
+    const vtp::NvtxRange nvtx_range("vtp diff forward");
     int rc = check_ready(s);
     if (rc) return rc;
     if (!s->initialized && (rc = s->initialize())) return rc;
@@ -651,6 +652,7 @@ extern "C" {
 
 int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
                              float *dl_dvel0, double *dl_dxsph_k) {
+    const vtp::NvtxRange nvtx_range("vtp diff backward");
     int rc = check_ready(s);
     if (rc) return rc;
     if (!s->diff) return fail(VTP_ERR_STATE, "diff_backward before diff_forward");

@@ -72,6 +72,7 @@ int write_ply(const std::string &dir, const std::string &name, const std::vector
 }  // namespace
 
 int vtp_solver::export_frame() {
+    const vtp::NvtxRange nvtx_range("vtp export");
     const nlohmann::json &ex = cfg["EXPORT"];
     const std::string policy = ex["SolverRequired"]["exportGroupPolicy"].get<std::string>();
     const std::string dir = ex["Common"]["exportTargetDir"].get<std::string>();

@@ -7,7 +7,21 @@
 
 #include "common.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace vtp {
+
+// NVTX range over a host scope (solver stages: initialize, tick, the substep's
+// enqueue stages, differentiation, export).  NVTX is header-only and does
+// nothing unless a profiler is attached.  With graphs the enqueue stages are
+// recorded once, at capture; every tick shows as one range around its graph
+// launches.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 constexpr int kConsPhases = 8;   // phases the conservation sums report (vtp_conservation.phase_mass)
 
@@ -36,6 +50,7 @@ struct UgnsBuffers {
     uint32_t *ncnt = nullptr;      // [nf] neighbour count incl. self (0 = outside the grid)
     uint32_t *bnbr = nullptr;      // ELL list for boundary rows (init / diagnostics)
     uint32_t *bncnt = nullptr;     // [nb]
+    uint32_t *status = nullptr;    // the solver's device status word (checked-build guards report here)
     size_t scan_tiles = 0;
 };
 

@@ -178,12 +178,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t *__restric
 __global__ void k_scatter(uint32_t row0, uint32_t cnt, const uint32_t *__restrict__ key,
                           const uint32_t *__restrict__ rank, const uint32_t *__restrict__ start,
                           const uint32_t *__restrict__ orig, uint32_t *__restrict__ tmp_src,
-                          uint32_t *__restrict__ tmp_orig, uint32_t *__restrict__ tmp_key) {
+                          uint32_t *__restrict__ tmp_orig, uint32_t *__restrict__ tmp_key, uint32_t *status) {
     pdl_enter();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cnt) return;
     uint32_t k = key[i];
     uint32_t d = start[k] - row0 + rank[i];
+#ifdef VTP_CHECKED
+    if (d >= cnt) {   // a cell segment slot outside the sorted range: record it and skip the write
+        if (status) atomicOr(status, ST_BOUNDS);
+        return;
+    }
+#endif
     tmp_src[d] = i;
     tmp_orig[d] = orig[row0 + i];
     tmp_key[d] = k;
@@ -528,6 +534,26 @@ __global__ void __launch_bounds__(kSplitBlock) k_build_lists_split(
     }
 }
 
+#ifdef VTP_CHECKED
+// Checked build (-DVTP_CHECKED): every list entry of rows [row0, row0 + cnt)
+// after each build - count <= maxNbr, entries inside the solver's rows, no
+// row listed as its own neighbour - with the first offence recorded in
+// `status` (ST_BOUNDS); the passes consume only validated lists.
+__global__ void k_check_lists(uint32_t row0, uint32_t cnt, uint32_t nrows, uint32_t ell_stride, uint32_t maxnbr,
+                              const uint32_t *__restrict__ nbr, const uint32_t *__restrict__ ncnt,
+                              uint32_t *__restrict__ status) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cnt) return;
+    const uint32_t n = ncnt[r];
+    bool bad = n > maxnbr;
+    for (uint32_t t = 0; !bad && t + 1 < n; ++t) {
+        const uint32_t j = nbr[ell_index(r, t, ell_stride)];
+        bad = j >= nrows || j == row0 + r;
+    }
+    if (bad) atomicOr(status, ST_BOUNDS);
+}
+#endif
+
 // Staged list builder: one block per brick (staged.h).  The block stages
 // the brick's 6 x 6 x 6-cell neighbourhood - positions, with each row's index
 // in w - in shared memory once, and every row of the group walks its 27 cells
@@ -861,7 +887,7 @@ void ugns_sort(cudaStream_t st, const Scenes &sc, uint32_t nbuckets, uint32_t ro
     if (cnt == 0) return;
     B();
     launch(k_scatter, nblk(cnt, 256), 256, 0, st, row0, cnt, u.key, u.rank, start, orig_in, u.tmp_src, u.tmp_orig,
-                                              u.tmp_key);
+           u.tmp_key, u.status);
     E("ugns_scatter");
     B();
     launch(k_rank_reorder, nblk(cnt, 256), 256, 0, st, sc, row0, cnt, start, u.tmp_src, u.tmp_orig, u.tmp_key, pos_in,
@@ -904,6 +930,9 @@ void ugns_build_lists(cudaStream_t st, const Scenes &sc, const Layout &L, uint32
         case 1: L.cell_cull ? go(M1{}, T{}) : go(M1{}, F{}); break;
         default: L.cell_cull ? go(M2{}, T{}) : go(M2{}, F{}); break;
     }
+#ifdef VTP_CHECKED
+    k_check_lists<<<nblk(cnt, 256), 256, 0, st>>>(row0, cnt, L.n, L.ell_stride, sc.maxnbr, nbr, ncnt, status);
+#endif
 }
 
 void ugns_build_lists_staged(cudaStream_t st, const Scenes &sc, const Layout &L, const Staging &stg,
@@ -930,6 +959,9 @@ void ugns_build_lists_staged(cudaStream_t st, const Scenes &sc, const Layout &L,
         launch(k_build_lists_staged<1, false>, grid, kStageBlock, smem, st, sc, stg, L.ell_stride, pos, nbr, ncnt,
                status, overflow);
     }
+#ifdef VTP_CHECKED
+    k_check_lists<<<nblk(L.nf, 256), 256, 0, st>>>(0, L.nf, L.n, L.ell_stride, sc.maxnbr, nbr, ncnt, status);
+#endif
 }
 
 void scatter_f4_to_orig(cudaStream_t st, uint32_t n, const float4 *src, const uint32_t *orig, float *dst3) {

@@ -5,7 +5,11 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libvtp.so"
+# VTP_LIBRARY=checked selects the checked build (device-side bounds checks, build.py --checked);
+# any other value is a path to the library.
+_choice = os.environ.get("VTP_LIBRARY", "")
+LIB_PATH = (Path(__file__).resolve().parent / "libvtp_checked.so" if _choice == "checked" else
+            Path(_choice) if _choice else Path(__file__).resolve().parent / "libvtp.so")
 
 VTP_OK = 0
 VTP_ERR_CONFIG = 1
