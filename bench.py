@@ -521,7 +521,7 @@ def run_diff(args, torch) -> dict:
     mask = diff.fluid_mask(sc)
     nf = int(mask.sum())
     target = np.array([0.8, 0.2, 0.6])
-    extra = json.loads(args.extra) if args.extra else None
+    extra = json.loads(args.extra) if args.extra else (default_extra("diff_pbf") or None)
 
     def loss_grad(pos):
         m = pos[mask].astype(np.float64).mean(0)
@@ -565,7 +565,7 @@ def run_diff(args, torch) -> dict:
     s.destroy()
     # value: gradients per second in particle-steps, i.e. the recorded forward plus the backward
     value = nf * args.steps / (fwd_s + bwd_s) / 1e6
-    cfg = {"workload": "diff_pbf", "fluid": nf, "boundary": int((~mask).sum()), "substeps": args.steps,
+    cfg = {"workload": "diff_pbf", "fluid": nf, "boundary": int((~mask).sum()), "substeps": args.steps, "b200": extra,
            "checkpoint_every": args.checkpoint_every, "loss": loss, "dl_dxsph_k": gk,
            "forward_value": nf * args.steps / plain_s / 1e6, "recorded_forward_value": nf * args.steps / fwd_s / 1e6,
            "adjoint_over_forward": (fwd_s + bwd_s) / plain_s,

@@ -41,12 +41,17 @@ def _check_lists(gpu_cnt, gpu_nb, or_cnt, or_nb):
 
 
 @pytest.mark.parametrize("order", ["brick", "linear"])
-@pytest.mark.parametrize("lanes", [1, 8])
+@pytest.mark.parametrize("lanes", [1, 8, "culled"])
 @pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
 def test_neighbor_lists_and_order_bit_exact(vtp_gpu, oracle_lib, kind, lanes, order):
+    """Every list builder: one thread per row (1), one thread per row with cell culling
+    ("culled"), and eight lanes per row (8)."""
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break() if kind == "PBF" else vtp.scenes.dam_break("DFSPH", 30000, seed=7)
-    s = vtp.solver_from_scene(sc, extra={"listLanes": lanes, "cellOrder": order})
+    extra = {"listLanes": lanes if lanes in (1, 8) else 1, "cellOrder": order}
+    if lanes == "culled":
+        extra["cellCull"] = True
+    s = vtp.solver_from_scene(sc, extra=extra)
     assert s.initialize()
     pos0 = s.get_field("pos")
     grid = oracle_lib.make_grid(sc.config[kind]["Required"])
@@ -214,12 +219,13 @@ def test_list_builders_give_identical_trajectories(vtp_gpu, kind):
           "DFSPH": lambda: vtp.scenes.dam_break("DFSPH", 8000, seed=5),
           "IMMCT": lambda: vtp.scenes.layered_mixture("IMMCT", 16, seed=3)}[kind]()
     out = []
-    for lanes in (1, 8):
-        s = vtp.solver_from_scene(sc, extra={"listLanes": lanes})
+    for extra in ({"listLanes": 1}, {"listLanes": 8}, {"listLanes": 1, "cellCull": True}):
+        s = vtp.solver_from_scene(sc, extra=extra)
         assert s.tickNsteps(6), s.last_error
         out.append((s.get_field("pos"), s.get_field("vel")))
         s.destroy()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
 
 
 @pytest.mark.parametrize("kind", ["PBF", "DFSPH", "IMMCT"])

@@ -190,26 +190,25 @@ def tuned_extra(key: str, gpu: str | None = None, path: Path = CACHE) -> dict:
     return dict(entry["B200"]) if entry else {}
 
 
-if __name__ == "__main__":
+def main(argv=None):
+    """Tune a workload on this GPU; --write records the result in vtp/tuned.json."""
     import argparse
-    import sys
-
-    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
-    from vtp import scenes
+    from . import scenes
 
     ap = argparse.ArgumentParser(description="tune a workload on this GPU and record it in vtp/tuned.json")
     ap.add_argument("--workload", default="dfsph_1m",
-                    choices=["dfsph_1m", "pbf", "immct_500k", "batched_pbf", "batched_dfsph"])
+                    choices=["dfsph_1m", "pbf", "immct_500k", "batched_pbf", "batched_dfsph", "diff_pbf"])
     ap.add_argument("--write", action="store_true", help="record the result in the cache")
     ap.add_argument("--no-arithmetic", action="store_true",
                     help="leave out keys that change FP32 arithmetic (rowLanes)")
-    a = ap.parse_args()
+    a = ap.parse_args(argv)
     base = {}
     if a.workload.startswith("batched"):
         kind = "PBF" if a.workload == "batched_pbf" else "DFSPH"
         sc = [m for m in scenes.batched_scenes() if m.solver == kind]
     else:
-        sc = {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k}[a.workload]()
+        sc = {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k,
+              "diff_pbf": scenes.diff_pbf}[a.workload]()
         kind = sc.solver
         if a.workload == "dfsph_1m":
             base = {"cfl": 0.4}
@@ -217,3 +216,11 @@ if __name__ == "__main__":
     print(json.dumps({k: res[k] for k in ("best", "config", "ms_per_step")}))
     if a.write:
         store(a.workload, res)
+
+
+if __name__ == "__main__":
+    import sys
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    from vtp.autotune import main as _main   # the package's module, so its relative imports resolve
+    _main()
