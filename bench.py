@@ -40,7 +40,8 @@ def parse():
                          "outlier speeds after ~45 substeps in the reference and here alike)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "immct_500k", "batched", "diff_pbf"],
+    ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "pbf_m1", "immct_500k", "batched", "batched_m1",
+                                           "diff_pbf"],
                     default="dfsph_1m")
     ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--fd-steps", type=int, default=20, help="diff_pbf: horizon of the finite-difference check")
@@ -60,7 +61,16 @@ def parse():
 
 def make_scene(workload):
     from vtp import scenes
-    return {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k}[workload]()
+    return {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "pbf_m1": scenes.pbf_dam_break_m1,
+            "immct_500k": scenes.immct_500k}[workload]()
+
+
+def batched_mix(workload):
+    """The batched mix of a workload: "batched" (PBF scenes at spacing 0.02, whose fluid the
+    reference's PBF formulation lets through the floor) or "batched_m1" (PBF particles of
+    mass 1, fluid kept in the box)."""
+    from vtp import scenes
+    return scenes.batched_scenes(pbf_spacing=0.1 if workload == "batched_m1" else None)
 
 
 class Clocks:
@@ -190,7 +200,7 @@ def run_reference_batched(args) -> dict:
     plain solver (its solvers keep function-local statics, so one solver per process), scenes one
     after another; a time-bounded sample of the 64 scenes, interleaving PBF and DFSPH scenes."""
     from vtp import scenes
-    mix = scenes.batched_scenes()
+    mix = batched_mix(args.workload)
     order = [k for pair in zip(range(48), range(48, 64)) for k in pair] + list(range(16, 48))
     order = list(dict.fromkeys(order))
     steps = max(1, min(args.steps, 50))
@@ -201,7 +211,7 @@ def run_reference_batched(args) -> dict:
     for k in order:
         if time.perf_counter() - t_start > budget:
             break
-        cmd = [sys.executable, str(Path(__file__).resolve()), "--impl", "reference", "--workload", "batched",
+        cmd = [sys.executable, str(Path(__file__).resolve()), "--impl", "reference", "--workload", args.workload,
                "--scene-index", str(k), "--steps", str(steps), "--warmup", str(warm), "--e2e-steps", "3"]
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
         if r.returncode != 0:
@@ -220,7 +230,7 @@ def run_reference_batched(args) -> dict:
     value = tot_ps / (tot_ms / 1e3) / 1e6
     out.update({"value": value, "n_gpus": 1, "steps": steps, "warmup": warm, "ms_per_step": tot_ms / steps,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched", "scenes_sampled": done, "scenes": len(mix),
+                "config": {"workload": args.workload, "scenes_sampled": done, "scenes": len(mix),
                            "impl": "reference CUDA build (sm_100a, -O3), one process per scene, "
                                    "Solver::tickNsteps per scene one after another"},
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": 0, "kind": "reference",
@@ -235,7 +245,7 @@ def run_reference_scene(args) -> dict:
     """One scene of the batched mix in the reference build (child process of run_reference_batched)."""
     from oracle.ref import ref as R
     from vtp import scenes
-    sc = scenes.batched_scenes()[args.scene_index]
+    sc = batched_mix(args.workload)[args.scene_index]
     s = R.RefSolver(sc)
     s.initialize()
     if args.warmup:
@@ -259,7 +269,7 @@ def run_reference(args) -> dict:
     if not R.available():
         out["unavailable"] = "oracle/_ref/libvtref.so was not built (the reference sources were not present)"
         return out
-    if args.workload == "batched":
+    if args.workload in ("batched", "batched_m1"):
         return run_reference_scene(args) if args.scene_index >= 0 else run_reference_batched(args)
     sc = make_scene(args.workload)
     s = R.RefSolver(sc)
@@ -358,7 +368,7 @@ def run_batched(args, rank, world, local, dist, torch):
     import numpy as np
     import vtp
     from vtp.dist import scene_share
-    mix = vtp.scenes.batched_scenes()
+    mix = batched_mix(args.workload)
     mine = scene_share(mix, world, rank)
     # per solver type: --extra, or the autotuned block of that half of the mix
     extras = {}
@@ -443,7 +453,7 @@ def run_batched(args, rank, world, local, dist, torch):
     for _, _, b, _ in batches:
         b.destroy()
 
-    cfg = {"workload": "batched", "scenes": len(mix), "pbf_scenes": sum(m.solver == "PBF" for m in mix),
+    cfg = {"workload": args.workload, "scenes": len(mix), "pbf_scenes": sum(m.solver == "PBF" for m in mix),
            "fluid": nf_all, "boundary": sum(m.n_boundary for m in mix), "scenes_this_rank": len(mine),
            "parallelism": f"scenes-lpt{world}", "wall_ms_per_step": 1e3 * wall / args.steps, "b200": extras,
            "l2": "inputs larger than L2 (~9.2M particles of state and neighbour lists)"}
@@ -614,7 +624,8 @@ def run_diff(args, torch) -> dict:
             "clocks": clocks}
 
 
-DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "immct_500k": 30, "batched": 200, "diff_pbf": 200}
+DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "pbf_m1": 1000, "immct_500k": 30, "batched": 200, "batched_m1": 200,
+                 "diff_pbf": 200}
 # "B200" keys a workload always runs with, beside the autotuned ones: the DFSPH 1M scene steps
 # with the adaptive CFL 0.4 rule capped at its 1 ms timeStep, as the benchmark's configuration
 # states (the dam break stays below 4 m/s over the timed substeps, so the step is the cap
@@ -714,10 +725,10 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return 0
-    if args.workload == "batched":
+    if args.workload in ("batched", "batched_m1"):
         line = run_batched(args, rank, world, local, dist, torch)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            mix = vtp.scenes.batched_scenes()
+            mix = batched_mix(args.workload)
             a = cpu_baseline(mix[0], args.cpu_seconds / 2)
             d = cpu_baseline(mix[48], args.cpu_seconds / 2)
             # combined rate: fluid particle-steps of both samples over their summed time

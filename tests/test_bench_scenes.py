@@ -112,6 +112,37 @@ def test_immct_500k_substep_matches_fp64_oracle(vtp_gpu, oracle_lib):
     s.destroy()
 
 
+def test_pbf_m1_keeps_its_fluid_and_follows_the_fp64_oracle(vtp_gpu, oracle_lib):
+    """The PBF dam break at the reference examples' particle size (mass 1), where the
+    reference's formulation keeps the fluid in its box: one substep per particle against
+    the FP64 oracle, then 300 substeps with no particle leaving the box and the kinetic
+    energy and centre of mass following the oracle's trajectory."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.pbf_dam_break_m1()
+    s = vtp.solver_from_scene(sc)
+    o = oracle_lib.OracleSolver(sc)
+    fm = fluid_mask(sc)
+    assert s.tickNsteps(1), s.last_error
+    o.step(1)
+    ep = rel_err(s.get_field("pos")[fm], o.pos[fm])
+    ev = rel_err(s.get_field("vel")[fm], o.vel[fm], _vel_floor(sc))
+    print(f"PBF m=1 substep 1: library vs FP64 oracle: pos {ep:.2e} vel {ev:.2e}")
+    assert ep < TOL and ev < TOL
+    m = o.mass[fm]
+    for t in (100, 300):
+        assert s.tickNsteps(t - s.stats()["steps_done"]), s.last_error
+        o.step(t - o.steps)
+        p, v = s.get_field("pos")[fm].astype(np.float64), s.get_field("vel")[fm].astype(np.float64)
+        ke, ke_o = 0.5 * np.sum(m * np.sum(v * v, 1)), 0.5 * np.sum(m * np.sum(o.vel[fm] ** 2, 1))
+        dcom = float(np.max(np.abs(p.mean(0) - o.pos[fm].mean(0))))
+        out = int(((p < 0.0) | (p > 5.0)).any(1).sum())
+        print(f"PBF m=1 substep {t}: kinetic energy {ke:.4e} (oracle {ke_o:.4e}), centre of mass offset "
+              f"{dcom:.2e} m, particles outside the box {out}")
+        assert out == 0
+        assert abs(ke - ke_o) <= 0.05 * ke_o and dcom < 0.02
+    s.destroy()
+
+
 FD_SUBSTEPS = 200
 FD_DIRECTIONS = 32
 

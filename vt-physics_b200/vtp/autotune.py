@@ -197,7 +197,7 @@ def main(argv=None):
 
     ap = argparse.ArgumentParser(description="tune a workload on this GPU and record it in vtp/tuned.json")
     ap.add_argument("--workload", default="dfsph_1m",
-                    choices=["dfsph_1m", "pbf", "immct_500k", "batched_pbf", "batched_dfsph", "diff_pbf"])
+                    choices=["dfsph_1m", "pbf", "pbf_m1", "immct_500k", "batched_pbf", "batched_dfsph", "diff_pbf"])
     ap.add_argument("--write", action="store_true", help="record the result in the cache")
     ap.add_argument("--no-arithmetic", action="store_true",
                     help="leave out keys that change FP32 arithmetic (rowLanes)")
@@ -207,8 +207,8 @@ def main(argv=None):
         kind = "PBF" if a.workload == "batched_pbf" else "DFSPH"
         sc = [m for m in scenes.batched_scenes() if m.solver == kind]
     else:
-        sc = {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "immct_500k": scenes.immct_500k,
-              "diff_pbf": scenes.diff_pbf}[a.workload]()
+        sc = {"dfsph_1m": scenes.dfsph_1m, "pbf": scenes.pbf_dam_break, "pbf_m1": scenes.pbf_dam_break_m1,
+              "immct_500k": scenes.immct_500k, "diff_pbf": scenes.diff_pbf}[a.workload]()
         kind = sc.solver
         if a.workload == "dfsph_1m":
             base = {"cfl": 0.4}

@@ -162,6 +162,21 @@ def pbf_dam_break(seed: int = 1001, jitter_amp: float = 0.1) -> Scene:
                               SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def pbf_dam_break_m1(seed: int = 1001, jitter_amp: float = 0.1) -> Scene:
+    """The PBF dam break at the particle size of the reference's own PBF examples
+    (particleRadius 0.05, so the particle mass rho0 (2r)^3 is 1): the same 20x40x20 block
+    (16,000) in a 2-layer box, every length 5 times the benchmark's.  The reference's
+    constraint gradients leave out the particle mass, which is consistent only for m = 1
+    (PBFCudaImpl.cu:95-144); here its fluid stays in the box, where at r = 0.01 it passes
+    through the floor."""
+    r = 0.05
+    fluid = jitter(cube(r, (0.2, 0.2, 0.2), (2.0, 4.0, 2.0)), jitter_amp, 2 * r, seed)
+    wall = box(r, (0.0, 0.0, 0.0), (5.0, 5.0, 5.0), 2)
+    cfg = pbf_config(dt=1.0 / 240.0, r=r, lb=(-0.5, -0.5, -0.5), size=(6.0, 6.0, 6.0))
+    return Scene("PBF", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, color_start=(0, 0, 1)),
+                              SceneObject("box", wall, EPM_BOUNDARY)])
+
+
 def dfsph_1m(seed: int = 2002, jitter_amp: float = 0.05) -> Scene:
     """DFSPH 1M: 100^3 fluid lattice at spacing 0.01 (x, y, z in [0.035, 1.025]) in a 3-layer box.
 
@@ -179,13 +194,15 @@ def dfsph_1m(seed: int = 2002, jitter_amp: float = 0.05) -> Scene:
                                 SceneObject("box", wall, EPM_BOUNDARY)])
 
 
-def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, jitter_amp: float = 0.05) -> Scene:
+def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, jitter_amp: float = 0.05,
+              spacing: float | None = None) -> Scene:
     """Dam break of about ``n_target`` particles: fluid block n x 2n x n in a cubic box of side n*spacing/0.4.
 
     Used for the small parity scenes and the batched scene mix; number density is constant
-    because the box scales with the fluid block.
+    because the box scales with the fluid block.  Spacing 0.02 for PBF and 0.01 for DFSPH
+    unless given (0.1 gives PBF particles of mass 1, the reference examples' size).
     """
-    spacing = 0.02 if solver == "PBF" else 0.01
+    spacing = spacing or (0.02 if solver == "PBF" else 0.01)
     r = spacing / 2
     n = max(2, int(round((n_target / 2.0) ** (1.0 / 3.0))))
     side = n * spacing / 0.4
@@ -222,17 +239,20 @@ def diff_pbf(seed: int = 5005) -> Scene:
 
 
 def batched_scenes(count: int = 64, n_pbf: int = 48, seed: int = 4242, gravity_seed: int = 4243,
-                   n_min: float = 4e3, n_max: float = 2.56e5) -> list:
+                   n_min: float = 4e3, n_max: float = 2.56e5, pbf_spacing: float | None = None) -> list:
     """The batched mix: ``count`` dam breaks, the first ``n_pbf`` PBF and the rest DFSPH.
 
     Fluid counts are log-uniform in [n_min, n_max] (SplitMix64 stream ``seed``), gravity
     y is uniform in [-12, -8] (stream ``gravity_seed``), scene k is jittered with seed
     4000 + k.  Box size scales with the fluid block so number density is constant.
+    ``pbf_spacing`` 0.1 makes the PBF scenes' particles of mass 1, where the reference's
+    PBF formulation keeps the fluid in its box (the default 0.02 lets it through the floor).
     """
     u = splitmix64_uniform(seed, count)
     ns = np.round(np.exp(np.log(n_min) + u * (np.log(n_max) - np.log(n_min)))).astype(np.int64)
     g = -12.0 + 4.0 * splitmix64_uniform(gravity_seed, count)
-    return [dam_break("PBF" if k < n_pbf else "DFSPH", int(ns[k]), seed=4000 + k, gravity_y=float(g[k]))
+    return [dam_break("PBF" if k < n_pbf else "DFSPH", int(ns[k]), seed=4000 + k, gravity_y=float(g[k]),
+                      spacing=pbf_spacing if k < n_pbf else None)
             for k in range(count)]
 
 
