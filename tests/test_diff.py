@@ -148,16 +148,22 @@ def test_gpu_adjoint_independent_of_checkpoint_interval(vtp_gpu):
 
 @pytest.mark.gpu
 def test_gpu_adjoint_same_with_segment_graphs_and_reused_buffers(vtp_gpu):
-    """The backward replays each full checkpoint segment as one captured graph
-    ("useGraphs", default on), and a rollout of the same shape as the last
-    reuses its checkpoints and tape: both leave the forward state and every
-    gradient bit-identical to direct launches on fresh buffers."""
+    """The backward replays each full checkpoint segment as captured graphs
+    ("useGraphs", default on), the forward keeps as many segments' tapes
+    resident as "tapeBudgetMB" allows (the backward recomputes the others), and
+    a rollout of the same shape as the last reuses its checkpoints and tapes:
+    none of it changes the forward state or any gradient, bit for bit."""
     from vtp import diff
     sc = small_case(13)
     mask = diff.fluid_mask(sc)
     out = []
-    for graphs in (True, False):
-        s = diff.pbf_solver(sc, extra={"useGraphs": graphs})
+    # tapeBudgetMB 0: one resident tape (the forward's last segment; the other is recomputed);
+    # the default budget holds both segments' tapes (no recompute)
+    for graphs, budget in ((True, None), (False, None), (True, 0), (False, 0)):
+        extra = {"useGraphs": graphs}
+        if budget is not None:
+            extra["tapeBudgetMB"] = budget
+        s = diff.pbf_solver(sc, extra=extra)
         x0, v0 = s.get_field("pos"), s.get_field("vel")
         runs = []
         for _ in range(2):   # the second rollout restarts from the initial state on reused buffers
@@ -171,8 +177,9 @@ def test_gpu_adjoint_same_with_segment_graphs_and_reused_buffers(vtp_gpu):
         for a, b in zip(runs[0], runs[1]):
             assert np.array_equal(a, b)
         out.append(runs[0])
-    for a, b in zip(out[0], out[1]):
-        assert np.array_equal(a, b)
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            assert np.array_equal(a, b)
 
 
 @pytest.mark.gpu

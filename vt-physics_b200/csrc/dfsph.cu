@@ -233,7 +233,14 @@ __global__ void __launch_bounds__(kStageBlock) k_solve_a_staged(DfsphArgs a) {
         if (staged) {
             slot_loop<U>(a.stg.snbr + ell_index(r, 0, a.ell_stride), cnt,
                          [&](uint16_t s) {
-                             const uint32_t q = 2u * (uint32_t)(s & 0x7fffu);
+                             uint32_t q = (uint32_t)(s & 0x7fffu);
+#ifdef VTP_CHECKED
+                             if (q >= P.total) {   // a slot outside the staged rows: record it, read slot 0
+                                 atomicOr(a.status, ST_BOUNDS);
+                                 q = 0;
+                             }
+#endif
+                             q *= 2u;
                              return F4x2{stage[q], stage[q + 1]};
                          },
                          use);
@@ -316,7 +323,16 @@ __global__ void __launch_bounds__(kStageBlock) k_solve_b_staged(DfsphArgs a) {
         const uint32_t cnt = n > 0 ? n - 1 : 0;
         if (staged) {
             slot_loop<U>(a.stg.snbr + ell_index(r, 0, a.ell_stride), cnt,
-                         [&](uint16_t s) { return stage[s & 0x7fffu]; },
+                         [&](uint16_t s) {
+                             uint32_t q = (uint32_t)(s & 0x7fffu);
+#ifdef VTP_CHECKED
+                             if (q >= P.total) {   // a slot outside the staged rows: record it, read slot 0
+                                 atomicOr(a.status, ST_BOUNDS);
+                                 q = 0;
+                             }
+#endif
+                             return stage[q];
+                         },
                          [&](uint16_t s, const float4 &e) { step(!(s & kSlotBoundary), e); });
         } else {
             nbr_loop<U>(a.nbr + ell_index(r, 0, a.ell_stride), cnt, [&](uint32_t j) { return ldg4(a.pk + j); },

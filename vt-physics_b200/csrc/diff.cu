@@ -25,6 +25,7 @@
 #include "solver.h"
 
 #include <algorithm>
+#include <array>
 #include <string>
 #include <vector>
 
@@ -38,8 +39,12 @@ struct DiffState {
     // checkpoints: fluid rows of (pos, vel, orig) at substeps 0, k, 2k, ... and at the end
     std::vector<float4 *> ck_pos, ck_vel;
     std::vector<uint32_t *> ck_orig;
-    // tape of one segment
-    std::vector<PbfTapeSlot> tape;
+    // Tapes of checkpoint segments (lists and intermediate states of `every` substeps each).
+    // The forward records its last `tapes.size()` segments straight into them (segment c into
+    // tape taped[c]); every other segment is recomputed from its checkpoint into tape 0 by
+    // the backward, after the segments the tapes hold have been consumed.
+    std::vector<std::vector<PbfTapeSlot>> tapes;
+    std::vector<int> taped;
     // all substeps' lists (keep_lists)
     std::vector<uint32_t *> kl_orig, kl_nbr, kl_cnt;
     // adjoint work arrays
@@ -56,19 +61,18 @@ struct DiffState {
     float4 *df_vb = nullptr, *df_save = nullptr;
     float *df_kb = nullptr;
 
-    // A full checkpoint segment's two halves, each captured once as a graph and replayed for
-    // every segment of that length (their pointers are all fixed: the tape, the adjoint
-    // arrays, the solver's buffers at the parity a segment starts from): `rec` runs the
-    // segment's substeps recording into the tape, `adj` runs the adjoint substeps over it.
-    cudaGraphExec_t rec_exec = nullptr, adj_exec = nullptr;
-    int rec_parity[3] = {-1, -1, -1};   // pos / vel / orig buffer parity `rec` starts from
-    // Checkpoint segment whose tape the forward recorded (the last one: the backward starts
-    // there without recomputing it); -1 when the tape holds no segment of the forward.
-    int tape_holds = -1;
+    // A full checkpoint segment's two halves, for each tape, captured once as graphs and
+    // replayed for every segment of that length (their pointers are all fixed: the tape, the
+    // adjoint arrays, the solver's buffers at the parity a segment starts from): `rec` runs
+    // the segment's substeps recording into the tape, `adj` runs the adjoint substeps over it.
+    std::vector<cudaGraphExec_t> rec_exec, adj_exec;
+    std::vector<std::array<int, 3>> rec_parity;   // pos / vel / orig buffer parity `rec` starts from
 
     ~DiffState() {
-        if (rec_exec) cudaGraphExecDestroy(rec_exec);
-        if (adj_exec) cudaGraphExecDestroy(adj_exec);
+        for (auto e : rec_exec)
+            if (e) cudaGraphExecDestroy(e);
+        for (auto e : adj_exec)
+            if (e) cudaGraphExecDestroy(e);
         for (void *p : mem) cudaFree(p);
     }
     template <class T>
@@ -427,22 +431,22 @@ int restore_fluid(vtp_solver &s, const float4 *p, const float4 *v, const uint32_
 
 int record_rollout(vtp_solver *s, vtp::DiffState &d);
 
-// The k substeps of a checkpoint segment, recording into the tape.
-int record_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k) {
+// The k substeps of a checkpoint segment, recording into tape `tp`.
+int record_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, int tp) {
     int rc;
     for (uint32_t t = 0; t < k; ++t)
-        if ((rc = s->enqueue_pbf_substep(s->st, &d.tape[t]))) return rc;
+        if ((rc = s->enqueue_pbf_substep(s->st, &d.tapes[tp][t]))) return rc;
     return VTP_OK;
 }
 
 // The adjoint substeps of a recorded segment of k substeps, last to first (programmatic
 // launch between their kernels, as in the forward substep).
-int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G) {
+int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G, int tp) {
     const uint32_t nf = d.nf;
     const int I = s->iterations;
     const vtp::PdlScope pdl_scope(s->pdl);
     for (int t = (int)k - 1; t >= 0 && nf; --t) {
-        const PbfTapeSlot &T = d.tape[t];
+        const PbfTapeSlot &T = d.tapes[tp][t];
         vtp::AdjArgs a{};
         a.nf = nf; a.ell_stride = s->L.ell_stride; a.k = s->kc;
         a.dt = s->dt; a.inv_dt = 1.f / s->dt; a.rho0 = s->rho_f; a.eps = 1e-6f; a.c = s->xsph_k;
@@ -478,6 +482,7 @@ int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G) {
 // at another parity, of odd or partial length, or with graphs off, runs `body` directly.
 template <class Body>
 int run_segment_graph(vtp_solver *s, vtp::DiffState &d, uint32_t k, cudaGraphExec_t &exec, int *parity, Body body) {
+    // (parity: 3 ints, or null for a graph that does not touch the solver's buffers)
     const int par[3] = {s->pos.cur, s->vel.cur, s->orig.cur};
     const bool graph_ok = s->use_graphs && k == d.every && k % 2 == 0 && d.nf;
     if (!graph_ok || (exec && parity && !std::equal(par, par + 3, parity))) return body();
@@ -524,12 +529,25 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
     if (!s->initialized && (rc = s->initialize())) return rc;
     if (s->crashed) return fail(VTP_ERR_STATE, "solver is crashed");
     if (n_steps == 0 || checkpoint_every == 0) return fail(VTP_ERR_ARG, "n_steps and checkpoint_every must be > 0");
-    // A rollout of the same shape as the previous one reuses its checkpoints, tape and adjoint
+    // Tapes kept in device memory: as many segments' as the budget ("tapeBudgetMB") and half
+    // the free device memory allow, at least one (the recompute tape).
+    const uint32_t every = std::min(checkpoint_every, n_steps);
+    const uint32_t nchk_all = (n_steps + every - 1) / every;
+    const int I_it = s->iterations;
+    const size_t lrows_all = ((size_t)s->L.nf + 31) / 32 * 32 * s->L.ell_stride;
+    const size_t slot_bytes = 4 * (size_t)s->L.nf * 2 + 4 * lrows_all + 16 * (size_t)s->L.n * (I_it + 2) +
+                              8 * (size_t)s->L.nf * I_it;
+    const size_t tape_bytes = std::max<size_t>(slot_bytes * every, 1);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    const size_t budget = std::min<size_t>((size_t)s->tape_budget_mb << 20, free_b / 2);
+    uint32_t ntapes = keep_lists ? 1u : (uint32_t)std::min<size_t>(std::max<size_t>(budget / tape_bytes, 1), nchk_all);
+    // A rollout of the same shape as the previous one reuses its checkpoints, tapes and adjoint
     // arrays (a training loop records the same horizon again and again); device memory is
     // allocated only when the shape changes.
-    const uint32_t every = std::min(checkpoint_every, n_steps);
     if (s->diff && s->diff->steps == n_steps && s->diff->every == every && s->diff->keep_lists == (keep_lists != 0) &&
-        s->diff->nf == s->L.nf && s->diff->n == s->L.n && s->diff->tape.size() == every) {
+        s->diff->nf == s->L.nf && s->diff->n == s->L.n && !s->diff->tapes.empty() &&
+        s->diff->tapes.size() <= ntapes) {
         std::shared_ptr<vtp::DiffState> d = s->diff;
         d->df_which = -1;
         return record_rollout(s, *d);
@@ -560,10 +578,12 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
                 (rc = d->alloc(&d->kl_cnt[t], nf)))
                 return rc;
     }
-    // The tape of one segment: lists and intermediate states of `every` substeps.
+    // The tapes: lists and intermediate states of `every` substeps each.
     const int I = s->iterations;
-    d->tape.resize(d->every);
-    for (auto &slot : d->tape) {
+    d->tapes.resize(ntapes);
+    for (auto &tape : d->tapes) {
+    tape.resize(d->every);
+    for (auto &slot : tape) {
         if ((rc = d->alloc(&slot.orig, nf)) || (rc = d->alloc(&slot.nbr, std::max<size_t>(lrows, 1))) ||
             (rc = d->alloc(&slot.ncnt, nf)) || (rc = d->alloc(&slot.v, n)))
             return rc;
@@ -583,6 +603,10 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
         for (int it = 0; it < I; ++it)
             if ((rc = d->alloc(&slot.lam[it], nf)) || (rc = d->alloc(&slot.rho[it], nf))) return rc;
     }
+    }
+    d->rec_exec.assign(ntapes, nullptr);
+    d->adj_exec.assign(ntapes, nullptr);
+    d->rec_parity.assign(ntapes, {-1, -1, -1});
     d->kblocks = vtp::nblk(std::max<uint32_t>(d->nf, 1), 256);
     if ((rc = d->alloc(&d->xbar_a, n)) || (rc = d->alloc(&d->vbar_a, n)) || (rc = d->alloc(&d->xbar, nf)) ||
         (rc = d->alloc(&d->vbar, nf)) || (rc = d->alloc(&d->abar, nf)) || (rc = d->alloc(&d->D[0], nf)) ||
@@ -604,16 +628,18 @@ int record_rollout(vtp_solver *s, vtp::DiffState &dd) {
     const uint32_t n_steps = d->steps;
     const uint32_t nchk = (n_steps + d->every - 1) / d->every;
     int rc;
-    d->tape_holds = -1;
+    const uint32_t ntapes = (uint32_t)d->tapes.size();
+    d->taped.assign(nchk, -1);
     for (uint32_t c = 0; c < nchk; ++c) {
         if ((rc = save_fluid(*s, d->ck_pos[c], d->ck_vel[c], d->ck_orig[c]))) return rc;
         const uint32_t k = std::min(d->every, n_steps - c * d->every);
-        if (!d->keep_lists && c + 1 == nchk) {
-            // The last segment runs its substeps recording into the tape, so the backward
-            // starts from it without recomputing it.
+        if (!d->keep_lists && c + ntapes >= nchk) {
+            // The last segments run their substeps recording into the tapes, so the backward
+            // starts from them without recomputing them.
+            const int tp = (int)(c + ntapes - nchk);
             if (!s->initialized && (rc = s->initialize())) return rc;
-            if ((rc = run_segment_graph(s, *d, k, d->rec_exec, d->rec_parity,
-                                        [&] { return record_segment(s, *d, k); })))
+            if ((rc = run_segment_graph(s, *d, k, d->rec_exec[tp], d->rec_parity[tp].data(),
+                                        [&] { return record_segment(s, *d, k, tp); })))
                 return rc;
             for (uint32_t t = 0; t < k; ++t) {   // as tick_n advances them for the segments before
                 s->sim_time += s->dt;
@@ -621,7 +647,7 @@ int record_rollout(vtp_solver *s, vtp::DiffState &dd) {
             }
             s->stats.steps_done = s->steps_done;
             s->stats.sim_time = s->sim_time;
-            d->tape_holds = (int)c;
+            d->taped[c] = tp;
             continue;
         }
         if (!d->keep_lists) {
@@ -631,7 +657,7 @@ int record_rollout(vtp_solver *s, vtp::DiffState &dd) {
         // keep_lists: direct launches, every substep's lists kept
         for (uint32_t t = 0; t < k; ++t) {
             const uint32_t step = c * d->every + t;
-            PbfTapeSlot slot = d->tape[0];
+            PbfTapeSlot slot = d->tapes[0][0];
             slot.nbr = d->kl_nbr[step];
             slot.ncnt = d->kl_cnt[step];
             slot.orig = d->kl_orig[step];
@@ -672,16 +698,21 @@ int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *d
     const unsigned G = vtp::nblk(std::max<uint32_t>(nf, 1), 256);
     for (int c = (int)nchk - 1; c >= 0; --c) {
         const uint32_t t0 = (uint32_t)c * d.every, k = std::min(d.every, d.steps - t0);
-        if (c != d.tape_holds) {
-            // Recompute the segment from its checkpoint into the tape.
+        int tp = c < (int)d.taped.size() ? d.taped[c] : -1;
+        if (tp < 0) {
+            // Recompute the segment from its checkpoint into tape 0 (whose own segment, the
+            // earliest one the forward recorded, has been consumed already).
+            tp = 0;
             if ((rc = restore_fluid(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
-            if ((rc = run_segment_graph(s, d, k, d.rec_exec, d.rec_parity, [&] { return record_segment(s, d, k); })))
+            if ((rc = run_segment_graph(s, d, k, d.rec_exec[0], d.rec_parity[0].data(),
+                                        [&] { return record_segment(s, d, k, 0); })))
                 return rc;
         }
-        if ((rc = run_segment_graph(s, d, k, d.adj_exec, nullptr, [&] { return adjoint_segment(s, d, k, G); })))
+        if ((rc = run_segment_graph(s, d, k, d.adj_exec[tp], nullptr,
+                                    [&] { return adjoint_segment(s, d, k, G, tp); })))
             return rc;
     }
-    d.tape_holds = -1;   // the tape now holds the first segment's recompute
+    d.taped.assign(d.taped.size(), -1);   // tape 0 now holds the first segment's recompute
     CU(cudaGetLastError());
     // Outputs: dL/d(state at the start of the recorded forward), attach order.
     if (dl_dpos0) {

@@ -108,6 +108,7 @@ struct vtp_solver {
     int list_lanes = 0;       // neighbour-list builder lanes per row (0 = by row count)
     bool cell_cull = false;   // list builder skips neighbour cells beyond h (same lists)
     bool staged_solve = false;      // DFSPH pressure solve gathers from shared-memory cell-group copies
+    uint32_t tape_budget_mb = 8192;  // differentiable PBF: device memory for resident segment tapes
     int stage_rows = 2048;          // staged rows per brick at most
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn
     bool phase_retry_all = false;   // IMM phase-transfer retries: every row, or rows near new flags
