@@ -41,8 +41,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["dfsph_1m", "pbf", "pbf_m1", "immct_500k", "batched", "batched_m1",
-                                           "diff_pbf"],
+                                           "diff_pbf", "dfsph_1m_dd"],
                     default="dfsph_1m")
+    ap.add_argument("--domains", type=int, default=1,
+                    help="dfsph_1m_dd on one process: slabs run as threads on this GPU (under torchrun: one "
+                         "slab per rank)")
     ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--fd-steps", type=int, default=20, help="diff_pbf: horizon of the finite-difference check")
     ap.add_argument("--fd-directions", type=int, default=4)
@@ -625,12 +628,101 @@ def run_diff(args, torch) -> dict:
 
 
 DEFAULT_STEPS = {"dfsph_1m": 200, "pbf": 1000, "pbf_m1": 1000, "immct_500k": 30, "batched": 200, "batched_m1": 200,
-                 "diff_pbf": 200}
+                 "diff_pbf": 200, "dfsph_1m_dd": 50}
 # "B200" keys a workload always runs with, beside the autotuned ones: the DFSPH 1M scene steps
 # with the adaptive CFL 0.4 rule capped at its 1 ms timeStep, as the benchmark's configuration
 # states (the dam break stays below 4 m/s over the timed substeps, so the step is the cap
 # throughout, the same work as the reference's fixed step).
 FIXED_EXTRA = {"dfsph_1m": {"cfl": 0.4}}
+
+
+def run_domains(args, rank, world, dist, torch) -> dict:
+    """dfsph_1m_dd: the DFSPH 1M scene decomposed into slabs along x (vtp/domain.py), one slab per
+    rank under torchrun (NCCL point-to-point and all-reduce between the GPUs) or, in one process,
+    --domains slabs as threads on this GPU.  Strong scaling: the whole scene's particle-steps over
+    the slowest rank's CUDA-event time.  The fixed 1 ms step (the adaptive rule is not decomposed;
+    the whole-scene run's step stays at its 1 ms cap over these substeps anyway)."""
+    from vtp import domain, scenes
+    sc = scenes.dfsph_1m()
+    extra = json.loads(args.extra) if args.extra else default_extra("dfsph_1m")
+    extra.pop("cfl", None)
+    arrays = domain.scene_arrays(sc)
+    arrays.config = json.loads(json.dumps(arrays.config))
+    arrays.config["B200"] = extra
+    ranks = world if world > 1 else max(1, args.domains)
+    plan = domain.plan_slabs(arrays, ranks)
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else args.steps
+
+    def body(r):
+        r.step(args.warmup)
+        before = r.stages.launches
+        ms = r.timed_steps(args.steps)
+        launches = r.stages.launches - before
+        iters = list(r.iters[-args.steps:])
+        # e2e: every substep the rank's owned state goes device -> page-locked host -> device
+        cap = r.stages.capacity
+        hp = torch.empty((cap, 3), dtype=torch.float32, pin_memory=True)
+        hv = torch.empty((cap, 3), dtype=torch.float32, pin_memory=True)
+        io = 0
+        torch.cuda.current_stream().synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            n = r.pos.shape[0]
+            hp[:n].copy_(r.pos, non_blocking=True)
+            hv[:n].copy_(r.vel, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            r.pos = hp[:n].to(r.pos.device, non_blocking=True)
+            r.vel = hv[:n].to(r.vel.device, non_blocking=True)
+            io += 24 * n
+            r.substep()
+        torch.cuda.current_stream().synchronize()
+        e2e_s = time.perf_counter() - t0
+        return {"ms": ms, "launches": launches, "iters": iters, "owned": int(r.pos.shape[0]), "e2e_s": e2e_s,
+                "io": io}
+
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)) if world > 1 else 0)
+    clk.start()
+    if world > 1:
+        with torch.cuda.stream(torch.cuda.Stream()):
+            res = [body(domain.DomainRank(arrays, plan, domain.TorchComm()))]
+        t = torch.tensor([res[0]["ms"], res[0]["e2e_s"], res[0]["launches"], res[0]["io"]], dtype=torch.float64,
+                         device="cuda")
+        tm = t[:2].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ts = t[2:].clone()
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+        max_ms, e2e_s, launches, io = float(tm[0]), float(tm[1]), int(ts[0]), float(ts[1])
+        owned = None
+    else:
+        res = domain.local_ranks(arrays, plan, body)
+        max_ms = max(x["ms"] for x in res)
+        e2e_s = max(x["e2e_s"] for x in res)
+        launches = sum(x["launches"] for x in res)
+        io = sum(x["io"] for x in res)
+        owned = [x["owned"] for x in res]
+    clocks = clk.stop()
+    nf = sc.n_fluid
+    iters = res[0]["iters"]
+    value = nf * args.steps / (max_ms / 1e3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "dfsph_1m_dd", "fluid": nf, "boundary": sc.n_boundary, "dt": 1e-3,
+                   "parallelism": f"slabs{ranks}" + ("" if world > 1 else " (threads on one GPU)"),
+                   "slab_axis": plan.axis, "slab_bounds": list(plan.bounds), "ghost": plan.ghost,
+                   "owned_at_end": owned,
+                   "div_iters_total": sum(i[0] for i in iters), "incomp_iters_total": sum(i[1] for i in iters),
+                   "b200": extra, "l2": "working set above L2 (1.45M particles); no flush between substeps"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "roofline": None,
+        "e2e": {"value": nf * e2e_steps / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": io / e2e_steps,
+                "d2h_bytes_per_step": io / e2e_steps, "steps": e2e_steps},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc, args.cpu_seconds)
+    return line
 
 
 def default_extra(workload: str) -> dict:
@@ -724,6 +816,14 @@ def main():
         if dist:
             dist.barrier()
             dist.destroy_process_group()
+        return 0
+    if args.workload == "dfsph_1m_dd":
+        line = run_domains(args, rank, world, dist, torch)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
         return 0
     if args.workload in ("batched", "batched_m1"):
         line = run_batched(args, rank, world, local, dist, torch)

@@ -418,6 +418,68 @@ VTP_API int vtp_ugns_neighbors_noalloc(const float *d_pos, uint32_t n, const flo
                                        float cell, uint32_t max_nbr, uint32_t *d_counts, uint32_t *d_nbrs,
                                        void *stream);
 
+/* ---- Single-scene domain decomposition (no counterpart in the reference,
+ * which runs a scene on one device, SolverManager.cpp:11-17).  One worker per
+ * rank runs the DFSPH substep (DFSPHSolver.cpp:339-406) over the fluid rows
+ * the rank owns, ghost copies of other ranks' fluid rows within the ghost
+ * width of its slab, and a band of the scene's boundary; the host calls the
+ * stages in order and replaces ghost values between them:
+ *   load, prepare,
+ *   per pressure solve (divergence, then density): solve_begin, then per
+ *     iteration solve_a (+ kappa to ghosts, residual sums added over ranks),
+ *     solve_b (+ v* to ghosts), the stop test on the summed residual;
+ *   between the solves: forces, [normals to ghosts, tension], velocities to
+ *     ghosts;
+ *   finalize, read.
+ * Every row carries its scene-wide attach id, so an owned row's neighbour
+ * list and arithmetic are those of a solver holding the whole scene.  Device
+ * pointers throughout; the work is enqueued on the worker's stream (the
+ * wrapped solver's, or the one set by vtp_domain_set_stream). */
+typedef struct vtp_domain vtp_domain;
+typedef enum vtp_domain_field {
+    VTP_DOMAIN_KAPPA = 0,    /* float per row: kappa after solve_a */
+    VTP_DOMAIN_VADV = 1,     /* float4 per row: v* after solve_b */
+    VTP_DOMAIN_VEL = 2,      /* float4 per row: velocity after forces / tension */
+    VTP_DOMAIN_NORMAL = 3    /* float4 per row: surface normal after forces (tension on) */
+} vtp_domain_field;
+/* config_json: the scene's DFSPH config (the fixed timeStep: "cfl" must be 0).
+ * fluid_pos: the worker's initial fluid rows (owned and ghost, host xyz,
+ * ascending scene-wide id), used for the boundary volumes at create;
+ * boundary_pos / boundary_ids: the boundary band (host, ids ascending);
+ * boundary_first: 1 when the scene's boundary ids are all below its fluid ids
+ * (0: all above); capacity: most owned + ghost rows a substep may load
+ * (<= 2^24); n_objects: the scene's fluid objects (<= 16, residual means are
+ * per object). */
+VTP_API int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t n_fluid,
+                              const float *boundary_pos, const uint32_t *boundary_ids, uint32_t nb,
+                              int boundary_first, uint32_t capacity, uint32_t n_objects, vtp_domain **out);
+VTP_API void vtp_domain_destroy(vtp_domain *d);
+/* stream: a cudaStream_t the stages are enqueued on from now on (cudaStreamLegacy for the
+ * legacy default stream); NULL returns to the worker's own stream. */
+VTP_API int vtp_domain_set_stream(vtp_domain *d, void *stream);
+VTP_API int vtp_domain_capacity(vtp_domain *d, uint32_t *capacity, uint32_t *n_boundary);
+/* Rows [0, n_own) are owned, [n_own, n_own + n_ghost) ghosts (load slots);
+ * d_pos / d_vel float[3] per row, d_ids scene-wide ids, d_obj the fluid object
+ * of each owned row (may be NULL: object 0). */
+VTP_API int vtp_domain_load(vtp_domain *d, uint32_t n_own, uint32_t n_ghost, const float *d_pos,
+                            const float *d_vel, const uint32_t *d_ids, const uint32_t *d_obj);
+VTP_API int vtp_domain_prepare(vtp_domain *d);
+VTP_API int vtp_domain_solve_begin(vtp_domain *d, int which);
+/* d_sums: double[n_objects], the owned rows' clamped compression errors summed per object. */
+VTP_API int vtp_domain_solve_a(vtp_domain *d, double *d_sums);
+VTP_API int vtp_domain_solve_b(vtp_domain *d);
+VTP_API int vtp_domain_forces(vtp_domain *d);
+VTP_API int vtp_domain_tension(vtp_domain *d);
+VTP_API int vtp_domain_finalize(vtp_domain *d);
+/* Gathers `field` of the rows at load slots d_slots[count] into d_out
+ * (count floats or float4s); unpack writes count values into the ghost rows at
+ * load slots [first_slot, first_slot + count). */
+VTP_API int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t count, float *d_out);
+VTP_API int vtp_domain_unpack(vtp_domain *d, int field, uint32_t first_slot, uint32_t count, const float *d_in);
+/* Owned rows' positions and velocities in load-slot order (float[3] each);
+ * waits for the worker's stream and reports a device-side status. */
+VTP_API int vtp_domain_read(vtp_domain *d, float *d_pos, float *d_vel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,17 @@ def lib() -> C.CDLL:
         L.or_imm_init.argtypes = [C.c_uint32, P, P, P, C.POINTER(OrGrid), C.POINTER(OrImm)]
         L.or_imm_step.argtypes = [C.c_uint32, P, P, C.c_int32, P, P, P, P, P, P, P, P, C.POINTER(OrGrid),
                                   C.POINTER(OrImm), C.POINTER(OrImmOut)]
+        for name in ("or_dfsph_ratio_alpha", "or_dfsph_solve_a", "or_dfsph_solve_b", "or_dfsph_forces",
+                     "or_dfsph_tension"):
+            getattr(L, name).restype = None
+        L.or_dfsph_ratio_alpha.argtypes = [C.c_uint32, P, P, P, P, P, P, C.c_uint32, C.c_double, P, P]
+        L.or_dfsph_solve_a.argtypes = [C.c_uint32, P, P, P, P, P, P, P, P, C.c_uint32, C.c_double, C.c_double, P, P]
+        L.or_dfsph_solve_b.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.c_double, C.c_double, P]
+        L.or_dfsph_pressure_apply.argtypes = [C.c_uint32, P, P, P, C.c_double]
+        L.or_dfsph_forces.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph), P, P]
+        L.or_dfsph_tension.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph), P]
+        L.or_dfsph_accelerate.argtypes = [C.c_uint32, P, P, P, P, C.c_double]
+        L.or_dfsph_advance.argtypes = [C.c_uint32, P, P, P, P, C.c_double]
         L.or_num_threads.restype = C.c_int
         L.or_set_num_threads.argtypes = [C.c_int]
         _lib = L
@@ -381,3 +392,151 @@ def dfsph_solve_op(o: "OracleSolver", cnt, nbr, iters: int, vadv, vbar=None):
     lib().or_dfsph_solve_op(o.n, _ptr(o.mat), _ptr(o.pos), _ptr(o.vol), _ptr(o.rest_density), _ptr(cnt), _ptr(nbr),
                             int(o.grid.maxnbr), float(o.p.h), float(o.p.dt), int(iters), _ptr(v), _ptr(vb))
     return v, vb
+
+
+class DfsphDomainStages:
+    """FP64 DFSPH stages over one rank's particles of a slab-decomposed scene (test
+    infrastructure: the checker of the decomposed run, in the stage interface of
+    ``vtp.domain.LibraryStages``).
+
+    The rank's particles (owned and ghost fluid rows in load-slot order, then its boundary
+    band) are kept sorted by scene-wide id, so the oracle's lists, stable in (cell, index),
+    are the whole-scene lists in the whole-scene order; the stages are the functions
+    ``or_dfsph_step`` is made of (DFSPHSolver.cpp:339-406).  Exchanged values are FP64.
+    """
+
+    def __init__(self, config: dict, fluid_pos0, bnd_pos, bnd_gid, boundary_first: bool, capacity: int,
+                 n_objects: int):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cpu")
+        self.dtype = torch.float64
+        req = config["DFSPH"]["Required"]
+        opt = config["DFSPH"]["Optional"]
+        self.grid = make_grid(req)
+        r = np.float32(req["particleRadius"])
+        self.vol0 = float(np.float32(np.float32(2) * r) ** np.float32(3))
+        p = OrDfsph()
+        p.dt = float(np.float32(req["timeStep"]))
+        p.h = float(np.float32(r * np.float32(4)))
+        p.rho0 = float(np.float32(req["fPartRestDensity"]))
+        p.rho_b = float(np.float32(req["bPartRestDensity"]))
+        p.vis = float(np.float32(req["fPartRestViscosity"]))
+        p.gamma = float(np.float32(req["surfaceTensionCoefficient"]))
+        g = [float(np.float32(v)) for v in opt["gravity"]] if opt["enable"] else [0.0, -9.8, 0.0]
+        for a in range(3):
+            p.g[a] = g[a]
+        p.max_iters = 101
+        self.p = p
+        self.nobj = int(n_objects)
+        self.boundary_first = bool(boundary_first)
+        # Boundary volumes of the band with the rank's initial fluid present, as a solver holding
+        # the whole scene computes them at initialize (or_dfsph_init over every particle).
+        fp0 = np.asarray(fluid_pos0, np.float64).reshape(-1, 3)
+        bp = np.asarray(bnd_pos, np.float64).reshape(-1, 3)
+        parts = [bp, fp0] if boundary_first else [fp0, bp]
+        mats = [np.ones(len(bp), np.int32), np.zeros(len(fp0), np.int32)]
+        if not boundary_first:
+            mats = mats[::-1]
+        pos = np.ascontiguousarray(np.concatenate(parts))
+        mat = np.concatenate(mats)
+        vol = np.full(len(pos), self.vol0)
+        rest = np.where(mat == 0, p.rho0, 0.0)
+        lib().or_dfsph_init(len(pos), _ptr(mat), _ptr(pos), _ptr(vol), _ptr(rest), C.byref(self.grid), C.byref(p))
+        sel = mat == 1
+        self.bnd_pos = bp
+        self.bnd_gid = np.asarray(bnd_gid, np.int64)
+        self.bnd_vol = vol[sel]
+        self.bnd_rest = rest[sel]
+
+    def empty(self, field: int, count: int):
+        shape = (count,) if field == 0 else (count, 3)
+        return self.torch.empty(shape, dtype=self.torch.float64)
+
+    def load(self, n_own, pos, vel, gid, obj):
+        nf = pos.shape[0]
+        nb = len(self.bnd_gid)
+        all_gid = np.concatenate([gid.numpy().astype(np.int64), self.bnd_gid])
+        order = np.argsort(all_gid, kind="stable")
+        inv = np.empty_like(order)
+        inv[order] = np.arange(len(order))
+        self.local_of_slot = inv[:nf]
+        self.n_own = int(n_own)
+        cat = lambda f, b: np.ascontiguousarray(np.concatenate([f, b])[order])
+        self.pos = cat(pos.numpy().astype(np.float64), self.bnd_pos)
+        self.vel = cat(vel.numpy().astype(np.float64), np.zeros((nb, 3)))
+        self.mat = cat(np.zeros(nf, np.int32), np.ones(nb, np.int32))
+        self.vol = cat(np.full(nf, self.vol0), self.bnd_vol)
+        self.rest = cat(np.full(nf, self.p.rho0), self.bnd_rest)
+        self.mass = np.where(self.mat == 0, self.rest * self.vol, 0.0)
+        obj_all = np.full(nf + nb, -1, np.int32)
+        obj_all[self.local_of_slot[: self.n_own]] = obj.numpy()[: self.n_own]
+        self.obj = obj_all
+        self.n = nf + nb
+
+    def prepare(self):
+        cnt, nbr, _, _ = neighbors(self.pos.astype(np.float32), self.grid)
+        self.cnt, self.nbr = cnt, nbr
+        n, M = self.n, int(self.grid.maxnbr)
+        self.M = M
+        self.ratio = np.zeros(n)
+        self.alpha = np.zeros(n)
+        lib().or_dfsph_ratio_alpha(n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), _ptr(self.mass), _ptr(cnt),
+                                   _ptr(nbr), M, self.p.h, _ptr(self.ratio), _ptr(self.alpha))
+        self.vadv = self.vel.copy()
+        self.kappa = np.zeros(n)
+        self.delta = np.zeros(n)
+        self.acc = np.zeros((n, 3))
+        self.nrm = np.zeros((n, 3))
+
+    def solve_begin(self, which: int):
+        pass
+
+    def solve_a(self):
+        lib().or_dfsph_solve_a(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), _ptr(self.ratio),
+                               _ptr(self.alpha), _ptr(self.vadv), _ptr(self.cnt), _ptr(self.nbr), self.M, self.p.h,
+                               self.p.dt, _ptr(self.delta), _ptr(self.kappa))
+        sums = np.zeros(self.nobj)
+        for i in np.nonzero(self.obj >= 0)[0]:   # owned rows, ascending id
+            sums[self.obj[i]] += self.delta[i]
+        return self.torch.tensor(sums, dtype=self.torch.float64)
+
+    def solve_b(self):
+        lib().or_dfsph_solve_b(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vol), _ptr(self.mass),
+                               _ptr(self.kappa), _ptr(self.cnt), _ptr(self.nbr), self.M, self.p.h, self.p.dt,
+                               _ptr(self.vadv))
+
+    def forces(self):
+        L = lib()
+        L.or_dfsph_pressure_apply(self.n, _ptr(self.mat), _ptr(self.vel), _ptr(self.vadv), self.p.dt)
+        L.or_dfsph_forces(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), _ptr(self.mass), _ptr(self.rest),
+                          _ptr(self.cnt), _ptr(self.nbr), self.M, C.byref(self.p), _ptr(self.acc), _ptr(self.nrm))
+        if self.p.gamma == 0.0:
+            L.or_dfsph_accelerate(self.n, _ptr(self.mat), _ptr(self.vel), _ptr(self.vadv), _ptr(self.acc), self.p.dt)
+
+    def tension(self):
+        L = lib()
+        L.or_dfsph_tension(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.mass), _ptr(self.rest), _ptr(self.nrm),
+                           _ptr(self.cnt), _ptr(self.nbr), self.M, C.byref(self.p), _ptr(self.acc))
+        L.or_dfsph_accelerate(self.n, _ptr(self.mat), _ptr(self.vel), _ptr(self.vadv), _ptr(self.acc), self.p.dt)
+
+    def finalize(self):
+        lib().or_dfsph_advance(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), _ptr(self.vadv), self.p.dt)
+
+    def _field(self, field: int):
+        return (self.kappa, self.vadv, self.vel, self.nrm)[field]
+
+    def pack(self, field: int, slots):
+        idx = self.local_of_slot[slots.numpy()]
+        return self.torch.from_numpy(self._field(field)[idx].copy())
+
+    def unpack(self, field: int, first: int, values):
+        idx = self.local_of_slot[first: first + values.shape[0]]
+        v = values.numpy()
+        self._field(field)[idx] = v
+        if field == 2:   # velocities after the forces: v* = v
+            self.vadv[idx] = v
+
+    def read(self):
+        idx = self.local_of_slot[: self.n_own]
+        return self.torch.from_numpy(self.pos[idx].copy()), self.torch.from_numpy(self.vel[idx].copy())

@@ -565,102 +565,24 @@ void or_dfsph_init(uint32_t n, const int32_t *mat, const double *pos, double *vo
     free_lists(&L);
 }
 
-typedef struct {
-    uint32_t n;
-    const int32_t *mat, *obj, *obj_is_fluid;
-    int32_t nobj;
-    const double *pos, *vol, *mass, *ratio, *alpha;
-    const lists_t *L;
-    const or_grid *g;
-    const cubic_t *k;
-    double dt;
-} dfctx;
+/* DFSPH substep stages.  or_dfsph_step runs them over every particle; a
+ * slab-decomposed run runs them over one rank's particles (owned fluid, ghost
+ * fluid, a band of the boundary) and exchanges the ghosts' values between them.
+ * Lists are in the layout of or_neighbors: cnt[n], nbr[n * maxnbr]. */
+#define FOR_LIST(cnt, nbr, M, i, j) \
+    for (uint32_t t_ = 0, j = 0; t_ < (cnt)[i] && ((j = (nbr)[(size_t)(i) * (M) + t_]), 1); ++t_)
 
-static int pressure_solve(const dfctx *c, double *vadv, double *kappa, double thr, int force, int max_iters,
-                          double *residual_out) {
-    const uint32_t n = c->n;
-    const or_grid *g = c->g;
-    double *delta = (double *)calloc(n ? n : 1, sizeof(double));
-    double *osum = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
-    double *ocnt = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
-    for (uint32_t i = 0; i < n; ++i) ocnt[c->obj[i]] += 1.0;
-    int iter = 0;
-    double residual = 0;
-    for (;;) {
-        ++iter;
-#pragma omp parallel for
-        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-            uint32_t i = (uint32_t)ii;
-            if (c->mat[i] != 0) continue;
-            double d = c->ratio[i] - 1.0, r[3];
-            FOR_NBR(*c->L, g, i, j) {
-                double gg = cubic_g(c->k, rdiff(c->pos, i, j, r));
-                double dot = 0;
-                for (int a = 0; a < 3; ++a) dot += gg * r[a] * (vadv[3 * (size_t)i + a] - vadv[3 * (size_t)j + a]);
-                d += dot * c->vol[j] * c->dt;
-            }
-            if (d < 0) d = 0;
-            delta[i] = d;
-        }
-        for (int o = 0; o < c->nobj; ++o) osum[o] = 0;
-        for (uint32_t i = 0; i < n; ++i)
-            if (c->obj_is_fluid[c->obj[i]]) osum[c->obj[i]] += delta[i];
-        double acc = 0;
-        int nf = 0;
-        for (int o = 0; o < c->nobj; ++o)
-            if (c->obj_is_fluid[o]) {
-                acc += osum[o] / ocnt[o];
-                ++nf;
-            }
-        residual = nf ? acc / nf : 0.0;
-        for (uint32_t i = 0; i < n; ++i)
-            kappa[i] = c->mat[i] == 0 ? delta[i] / c->alpha[i] / (c->dt * c->dt) / c->vol[i] : 0.0;
-#pragma omp parallel for
-        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-            uint32_t i = (uint32_t)ii;
-            if (c->mat[i] != 0) continue;
-            double r[3];
-            FOR_NBR(*c->L, g, i, j) {
-                double gg = cubic_g(c->k, rdiff(c->pos, i, j, r));
-                double s = c->dt * c->vol[i] * c->vol[j] / c->mass[i] * (kappa[i] + kappa[j]) * gg;
-                for (int a = 0; a < 3; ++a) vadv[3 * (size_t)i + a] -= s * r[a];
-            }
-        }
-        if (force > 0) {
-            if (iter >= force) break;
-        } else if (residual < thr || iter > max_iters - 1) {
-            break;
-        }
-    }
-    free(delta);
-    free(osum);
-    free(ocnt);
-    *residual_out = residual;
-    return iter;
-}
-
-void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
-                   double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
-                   const or_dfsph_params *p, or_solve_out *out, double *ratio_out, double *alpha_out) {
-    const double dt = p->dt;
-    lists_t L = build_lists(n, pos, g);
-    cubic_t k = cubic_make(p->h);
-    double *mass = (double *)calloc(n ? n : 1, sizeof(double));
-    double *ratio = (double *)calloc(n ? n : 1, sizeof(double));
-    double *alpha = (double *)calloc(n ? n : 1, sizeof(double));
-    double *vadv = (double *)malloc(sizeof(double) * 3 * (n ? n : 1));
-    double *kappa = (double *)calloc(n ? n : 1, sizeof(double));
-    double *acc = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
-    double *nrm = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
-    for (uint32_t i = 0; i < n; ++i) mass[i] = mat[i] == 0 ? rest_density[i] * vol[i] : 0.0;
-    memcpy(vadv, vel, sizeof(double) * 3 * n);
+void or_dfsph_ratio_alpha(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *mass,
+                          const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, double h, double *ratio,
+                          double *alpha) {
     /* compute_compression_ratio_cuda + compute_df_beta_cuda (DFSPHCudaImpl.cu:85-140). */
+    cubic_t k = cubic_make(h);
 #pragma omp parallel for
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         uint32_t i = (uint32_t)ii;
         if (mat[i] != 0) continue;
         double rt = 0, a1[3] = {0, 0, 0}, a2 = 1e-6, r[3];
-        FOR_NBR(L, g, i, j) {
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
             double rl = rdiff(pos, i, j, r);
             rt += vol[j] * cubic_w(&k, rl);
             double gg = cubic_g(&k, rl);
@@ -672,11 +594,56 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
         ratio[i] = rt;
         alpha[i] = al;
     }
-    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, &k, dt};
-    out->crashed = 0;
-    out->div_iters = pressure_solve(&c, vadv, kappa, p->div_thr, p->force_div, p->max_iters, &out->div_residual);
-    if (p->force_div <= 0 && out->div_iters > p->max_iters - 1) out->crashed = 1;
-    /* apply_pressure_acc: acc = (v* - v)/dt; v += acc dt; v* = v. */
+}
+
+void or_dfsph_solve_a(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *ratio,
+                      const double *alpha, const double *vadv, const uint32_t *cnt, const uint32_t *nbr,
+                      uint32_t maxnbr, double h, double dt, double *delta, double *kappa) {
+    /* compute_delta_compression_ratio_cuda + update_delta_compression_ratio_from_vel_adv_cuda
+     * (DFSPHCudaImpl.cu:142-196): the clamped compression error; compute_kappa_{div,incomp}
+     * (:355-367): kappa = delta / alpha / dt^2 / V (0 for boundary particles). */
+    cubic_t k = cubic_make(h);
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) {
+            delta[i] = 0.0;
+            kappa[i] = 0.0;
+            continue;
+        }
+        double d = ratio[i] - 1.0, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            double gg = cubic_g(&k, rdiff(pos, i, j, r));
+            double dot = 0;
+            for (int a = 0; a < 3; ++a) dot += gg * r[a] * (vadv[3 * (size_t)i + a] - vadv[3 * (size_t)j + a]);
+            d += dot * vol[j] * dt;
+        }
+        if (d < 0) d = 0;
+        delta[i] = d;
+        kappa[i] = d / alpha[i] / (dt * dt) / vol[i];
+    }
+}
+
+void or_dfsph_solve_b(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *mass,
+                      const double *kappa, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, double h,
+                      double dt, double *vadv) {
+    /* vf_update_vel_adv_from_kappa_{div,incomp}_cuda (DFSPHCudaImpl.cu:198-220, :369-391). */
+    cubic_t k = cubic_make(h);
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            double gg = cubic_g(&k, rdiff(pos, i, j, r));
+            double s = dt * vol[i] * vol[j] / mass[i] * (kappa[i] + kappa[j]) * gg;
+            for (int a = 0; a < 3; ++a) vadv[3 * (size_t)i + a] -= s * r[a];
+        }
+    }
+}
+
+void or_dfsph_pressure_apply(uint32_t n, const int32_t *mat, double *vel, double *vadv, double dt) {
+    /* apply_pressure_acc (DFSPHCudaImpl.cu:505-521): acc = (v* - v)/dt; v += acc dt; v* = v. */
     for (uint32_t i = 0; i < n; ++i) {
         if (mat[i] != 0) continue;
         for (int a = 0; a < 3; ++a) {
@@ -685,14 +652,24 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
             vadv[q] = vel[q];
         }
     }
-    /* dfsph_gravity_vis_surface (DFSPHCudaImpl.cu:523-554). */
+}
+
+void or_dfsph_forces(uint32_t n, const int32_t *mat, const double *pos, const double *vel, const double *mass,
+                     const double *rest_density, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                     const or_dfsph_params *p, double *acc, double *nrm) {
+    /* dfsph_gravity_vis_surface (DFSPHCudaImpl.cu:523-554): gravity plus explicit Laplacian
+     * viscosity into acc, surface normals into nrm (both 0 for boundary particles). */
+    cubic_t k = cubic_make(p->h);
     const double h2_001 = 0.001 * p->h * p->h;
 #pragma omp parallel for
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         uint32_t i = (uint32_t)ii;
-        if (mat[i] != 0) continue;
+        if (mat[i] != 0) {
+            for (int a = 0; a < 3; ++a) acc[3 * (size_t)i + a] = nrm[3 * (size_t)i + a] = 0.0;
+            continue;
+        }
         double av[3] = {0, 0, 0}, nn[3] = {0, 0, 0}, r[3];
-        FOR_NBR(L, g, i, j) {
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
             if (mat[j] != mat[i]) continue;
             double rl = rdiff(pos, i, j, r);
             double gg = cubic_g(&k, rl);
@@ -712,26 +689,34 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
             nrm[3 * (size_t)i + a] = nn[a];
         }
     }
-    if (p->gamma != 0.0) {
+}
+
+void or_dfsph_tension(uint32_t n, const int32_t *mat, const double *pos, const double *mass,
+                      const double *rest_density, const double *nrm, const uint32_t *cnt, const uint32_t *nbr,
+                      uint32_t maxnbr, const or_dfsph_params *p, double *acc) {
+    /* add_acc_surface_tension_cuda (DFSPHCudaImpl.cu:298-353): cohesion and curvature terms. */
 #pragma omp parallel for
-        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-            uint32_t i = (uint32_t)ii;
-            if (mat[i] != 0) continue;
-            double at[3] = {0, 0, 0}, r[3];
-            FOR_NBR(L, g, i, j) {
-                if (mat[j] != mat[i] || j == i) continue;
-                double rl = rdiff(pos, i, j, r);
-                double kk = 2 * rest_density[i] / (rest_density[i] + rest_density[j]);
-                double cc = tension_c(rl, p->h);
-                for (int a = 0; a < 3; ++a) {
-                    double a1 = -p->gamma * mass[i] * mass[j] * cc * r[a] / rl;
-                    double a2 = -p->gamma * mass[i] * (nrm[3 * (size_t)i + a] - nrm[3 * (size_t)j + a]);
-                    at[a] += kk * (a1 + a2);
-                }
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double at[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            if (mat[j] != mat[i] || j == i) continue;
+            double rl = rdiff(pos, i, j, r);
+            double kk = 2 * rest_density[i] / (rest_density[i] + rest_density[j]);
+            double cc = tension_c(rl, p->h);
+            for (int a = 0; a < 3; ++a) {
+                double a1 = -p->gamma * mass[i] * mass[j] * cc * r[a] / rl;
+                double a2 = -p->gamma * mass[i] * (nrm[3 * (size_t)i + a] - nrm[3 * (size_t)j + a]);
+                at[a] += kk * (a1 + a2);
             }
-            for (int a = 0; a < 3; ++a) acc[3 * (size_t)i + a] += at[a];
         }
+        for (int a = 0; a < 3; ++a) acc[3 * (size_t)i + a] += at[a];
     }
+}
+
+void or_dfsph_accelerate(uint32_t n, const int32_t *mat, double *vel, double *vadv, const double *acc, double dt) {
+    /* acc_2_vel (DFSPHCudaImpl.cu:222-296): v += acc dt; v* = v. */
     for (uint32_t i = 0; i < n; ++i) {
         if (mat[i] != 0) continue;
         for (int a = 0; a < 3; ++a) {
@@ -740,8 +725,10 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
             vadv[q] = vel[q];
         }
     }
-    out->inc_iters = pressure_solve(&c, vadv, kappa, p->inc_thr, p->force_inc, p->max_iters, &out->inc_residual);
-    if (p->force_inc <= 0 && out->inc_iters > p->max_iters - 1) out->crashed = 1;
+}
+
+void or_dfsph_advance(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vadv, double dt) {
+    /* apply_pressure_acc + update_pos_cuda (DFSPHSolver.cpp:393-404). */
     for (uint32_t i = 0; i < n; ++i) {
         if (mat[i] != 0) continue;
         for (int a = 0; a < 3; ++a) {
@@ -750,6 +737,86 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
             pos[q] += vel[q] * dt;
         }
     }
+}
+
+typedef struct {
+    uint32_t n;
+    const int32_t *mat, *obj, *obj_is_fluid;
+    int32_t nobj;
+    const double *pos, *vol, *mass, *ratio, *alpha;
+    const lists_t *L;
+    const or_grid *g;
+    double h, dt;
+} dfctx;
+
+static int pressure_solve(const dfctx *c, double *vadv, double *kappa, double thr, int force, int max_iters,
+                          double *residual_out) {
+    const uint32_t n = c->n, M = c->g->maxnbr;
+    double *delta = (double *)calloc(n ? n : 1, sizeof(double));
+    double *osum = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
+    double *ocnt = (double *)calloc(c->nobj > 0 ? c->nobj : 1, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) ocnt[c->obj[i]] += 1.0;
+    int iter = 0;
+    double residual = 0;
+    for (;;) {
+        ++iter;
+        or_dfsph_solve_a(n, c->mat, c->pos, c->vol, c->ratio, c->alpha, vadv, c->L->cnt, c->L->nbr, M, c->h, c->dt,
+                         delta, kappa);
+        /* vfsph_div / vfsph_incomp residual: mean over fluid objects of the object's mean
+         * clamped error (cal_mean, DFSPHCudaImpl.cu:449-503). */
+        for (int o = 0; o < c->nobj; ++o) osum[o] = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (c->obj_is_fluid[c->obj[i]]) osum[c->obj[i]] += delta[i];
+        double acc = 0;
+        int nf = 0;
+        for (int o = 0; o < c->nobj; ++o)
+            if (c->obj_is_fluid[o]) {
+                acc += osum[o] / ocnt[o];
+                ++nf;
+            }
+        residual = nf ? acc / nf : 0.0;
+        or_dfsph_solve_b(n, c->mat, c->pos, c->vol, c->mass, kappa, c->L->cnt, c->L->nbr, M, c->h, c->dt, vadv);
+        if (force > 0) {
+            if (iter >= force) break;
+        } else if (residual < thr || iter > max_iters - 1) {
+            break;
+        }
+    }
+    free(delta);
+    free(osum);
+    free(ocnt);
+    *residual_out = residual;
+    return iter;
+}
+
+void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nobj, const int32_t *obj_is_fluid,
+                   double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
+                   const or_dfsph_params *p, or_solve_out *out, double *ratio_out, double *alpha_out) {
+    /* DFSPHSolver::tick (DFSPHSolver.cpp:339-406). */
+    const double dt = p->dt;
+    const uint32_t M = g->maxnbr;
+    lists_t L = build_lists(n, pos, g);
+    double *mass = (double *)calloc(n ? n : 1, sizeof(double));
+    double *ratio = (double *)calloc(n ? n : 1, sizeof(double));
+    double *alpha = (double *)calloc(n ? n : 1, sizeof(double));
+    double *vadv = (double *)malloc(sizeof(double) * 3 * (n ? n : 1));
+    double *kappa = (double *)calloc(n ? n : 1, sizeof(double));
+    double *acc = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    double *nrm = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) mass[i] = mat[i] == 0 ? rest_density[i] * vol[i] : 0.0;
+    memcpy(vadv, vel, sizeof(double) * 3 * n);
+    or_dfsph_ratio_alpha(n, mat, pos, vol, mass, L.cnt, L.nbr, M, p->h, ratio, alpha);
+    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, p->h, dt};
+    out->crashed = 0;
+    out->div_iters = pressure_solve(&c, vadv, kappa, p->div_thr, p->force_div, p->max_iters, &out->div_residual);
+    if (p->force_div <= 0 && out->div_iters > p->max_iters - 1) out->crashed = 1;
+    or_dfsph_pressure_apply(n, mat, vel, vadv, dt);
+    or_dfsph_forces(n, mat, pos, vel, mass, rest_density, L.cnt, L.nbr, M, p, acc, nrm);
+    if (p->gamma != 0.0) or_dfsph_tension(n, mat, pos, mass, rest_density, nrm, L.cnt, L.nbr, M, p, acc);
+    or_dfsph_accelerate(n, mat, vel, vadv, acc, dt);
+    out->inc_iters = pressure_solve(&c, vadv, kappa, p->inc_thr, p->force_inc, p->max_iters, &out->inc_residual);
+    if (p->force_inc <= 0 && out->inc_iters > p->max_iters - 1) out->crashed = 1;
+    or_dfsph_advance(n, mat, pos, vel, vadv, dt);
     if (ratio_out) memcpy(ratio_out, ratio, sizeof(double) * n);
     if (alpha_out) memcpy(alpha_out, alpha, sizeof(double) * n);
     free(mass);
@@ -1039,7 +1106,7 @@ void or_imm_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t nob
         cd[i] = p->ct ? p->Cd0 + (1.0 - p->Cd0) * blk : p->Cd0;
     }
     memcpy(vadv, vel, sizeof(double) * 3 * n);
-    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, &kc, dt};
+    dfctx c = {n, mat, obj, obj_is_fluid, nobj, pos, vol, mass, ratio, alpha, &L, g, p->h, dt};
     out->crashed = 0;
     out->div_iters = pressure_solve(&c, vadv, kappa, p->div_thr, p->force_div, p->max_iters, &out->div_residual);
     if (p->force_div <= 0 && out->div_iters > p->max_iters - 1) out->crashed = 1;

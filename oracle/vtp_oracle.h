@@ -97,6 +97,30 @@ void or_dfsph_step(uint32_t n, const int32_t *mat, const int32_t *obj, int32_t n
                    double *pos, double *vel, const double *vol, const double *rest_density, const or_grid *g,
                    const or_dfsph_params *p, or_solve_out *out, double *ratio, double *alpha);
 
+/* The stages or_dfsph_step is made of, over given lists (cnt[n], nbr[n * maxnbr]
+ * in the layout of or_neighbors).  A slab-decomposed run calls them on one
+ * rank's particles and exchanges the ghosts' values in between: kappa after
+ * solve_a, v* after solve_b, velocities after forces / tension and normals
+ * between the two.  mass = rest_density * vol for fluid particles. */
+void or_dfsph_ratio_alpha(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *mass,
+                          const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, double h, double *ratio,
+                          double *alpha);
+void or_dfsph_solve_a(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *ratio,
+                      const double *alpha, const double *vadv, const uint32_t *cnt, const uint32_t *nbr,
+                      uint32_t maxnbr, double h, double dt, double *delta, double *kappa);
+void or_dfsph_solve_b(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *mass,
+                      const double *kappa, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, double h,
+                      double dt, double *vadv);
+void or_dfsph_pressure_apply(uint32_t n, const int32_t *mat, double *vel, double *vadv, double dt);
+void or_dfsph_forces(uint32_t n, const int32_t *mat, const double *pos, const double *vel, const double *mass,
+                     const double *rest_density, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                     const or_dfsph_params *p, double *acc, double *nrm);
+void or_dfsph_tension(uint32_t n, const int32_t *mat, const double *pos, const double *mass,
+                      const double *rest_density, const double *nrm, const uint32_t *cnt, const uint32_t *nbr,
+                      uint32_t maxnbr, const or_dfsph_params *p, double *acc);
+void or_dfsph_accelerate(uint32_t n, const int32_t *mat, double *vel, double *vadv, const double *acc, double dt);
+void or_dfsph_advance(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vadv, double dt);
+
 /* IMM / IMM-CT mixtures (IMMCTSolver.cpp:408-477 with IMMCTCudaImpl.cu:52-1152;
  * IMMSolver.cpp:400-466 with IMMCudaImpl.cu).  P phases; per particle:
  * frac[n*P] volume fractions, vph[n*P*3] phase velocities, Q[n*9] conformation

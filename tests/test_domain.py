@@ -1,0 +1,210 @@
+"""Single-scene domain decomposition (vtp/domain.py, csrc/domain.cu).
+
+The decomposed run must reproduce the whole-scene run bit for bit: every owned row
+sees the whole-scene neighbour list and neighbour values.  On CPU the stages are
+the FP64 oracle's (the functions or_dfsph_step is made of), run as threads of one
+process and as gloo ranks; on the GPU they are the library's, against the library
+solver holding the whole scene.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from vtp import domain, scenes
+
+FORCED = {"forceDivIterations": 3, "forceIncompIterations": 2}
+
+
+def _whole_oracle(sc, steps, force=(0, 0)):
+    from oracle import oracle as O
+    o = O.OracleSolver(sc, force_div=force[0], force_inc=force[1])
+    iters = []
+    for _ in range(steps):
+        o.step(1)
+        iters.append((o.last.div_iters, o.last.inc_iters))
+    fl = o.mat == 0
+    return o.pos[fl], o.vel[fl], iters
+
+
+# ----------------------------------------------------------------------------- host logic
+
+def test_slab_plan_splits_fluid_evenly_and_owns_every_coordinate():
+    a = domain.scene_arrays(scenes.dam_break("DFSPH", 3000, seed=11))
+    for ranks in (1, 2, 3, 5):
+        plan = domain.plan_slabs(a, ranks)
+        assert plan.ranks == ranks
+        size = a.config["DFSPH"]["Required"]["simSpaceSize"]
+        assert plan.axis == int(np.argmax(size))
+        own = plan.owner(a.fluid_pos[:, plan.axis])
+        counts = np.bincount(own, minlength=ranks)
+        assert counts.sum() == len(a.fluid_gid)
+        assert counts.max() - counts.min() <= a.fluid_pos.shape[0] // 20 + 40   # lattice layers tie
+        for k in range(ranks):
+            lo, hi = plan.slab(k)
+            x = a.fluid_pos[own == k, plan.axis]
+            assert np.all(x >= lo) and np.all(x < hi)
+    assert domain.plan_slabs(a, 4).ghost == pytest.approx(1.01 * a.h)
+
+
+def test_scene_arrays_keep_attach_ids_and_reject_interleaved_ids():
+    sc = scenes.colliding_blocks()
+    a = domain.scene_arrays(sc)
+    n0 = sc.objects[0].n
+    assert a.fluid_gid.tolist() == list(range(sc.n_fluid))
+    assert a.bnd_gid[0] == sc.n_fluid and not a.boundary_first
+    assert a.fluid_obj[:n0].max() == 0 and a.fluid_obj[n0:].min() == 1
+    assert a.obj_count.tolist() == [sc.objects[0].n, sc.objects[1].n]
+    assert np.allclose(a.fluid_vel[:n0], [1.5, 0, 0]) and np.allclose(a.fluid_vel[n0:], [-1.5, 0, 0])
+    sc.objects = [sc.objects[0], sc.objects[2], sc.objects[1]]   # fluid, box, fluid
+    with pytest.raises(ValueError, match="fluid ids all below or all above"):
+        domain.scene_arrays(sc)
+    with pytest.raises(ValueError, match="DFSPH"):
+        domain.scene_arrays(scenes.dam_break("PBF", 500, seed=1))
+
+
+def test_decomposed_run_rejects_the_adaptive_step(oracle_lib):
+    with pytest.raises(ValueError, match="cfl"):
+        domain.run_local(scenes.dam_break("DFSPH", 800, seed=12), 2, 1, make_stages=oracle_lib.DfsphDomainStages,
+                         extra={"cfl": 0.4})
+
+
+# ----------------------------------------------------------------------------- oracle stages
+
+@pytest.mark.parametrize("ranks", [1, 2, 3])
+@pytest.mark.parametrize("forced", [True, False])
+def test_decomposed_oracle_equals_whole_scene_oracle(oracle_lib, ranks, forced):
+    sc = scenes.dam_break("DFSPH", 3000, seed=11)
+    force = (3, 2) if forced else (0, 0)
+    pos, vel, iters = _whole_oracle(sc, 4, force)
+    out = domain.run_local(sc, ranks, 4, make_stages=oracle_lib.DfsphDomainStages,
+                           extra=FORCED if forced else None)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+    assert sum(out["owned"]) == sc.n_fluid and min(out["owned"]) > 0
+
+
+@pytest.mark.parametrize("ranks", [2, 4])
+def test_decomposed_oracle_with_migration_tension_and_two_objects(oracle_lib, ranks):
+    """Blocks thrown at each other across slab bounds: particles migrate every few substeps,
+    ghosts carry surface normals for the tension pass, residuals are per fluid object."""
+    sc = scenes.colliding_blocks()
+    steps = 25
+    pos, vel, iters = _whole_oracle(sc, steps)
+    out = domain.run_local(sc, ranks, steps, make_stages=oracle_lib.DfsphDomainStages)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+    plan = out["plan"]
+    start = np.bincount(plan.owner(domain.scene_arrays(sc).fluid_pos[:, plan.axis]), minlength=ranks)
+    assert out["owned"] != start.tolist()   # ownership moved with the particles
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _gloo_rank(rank, world, port, steps, q):
+    import datetime
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    sys.path[:0] = [str(root), str(root / "vt-physics_b200")]
+    import torch.distributed as dist
+    from oracle import oracle as O
+    from vtp import domain as D, scenes as S
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        arrays = D.scene_arrays(S.colliding_blocks())
+        plan = D.plan_slabs(arrays, world)
+        r = D.DomainRank(arrays, plan, D.TorchComm(), O.DfsphDomainStages)
+        r.step(steps)
+        parts = [None] * world
+        dist.all_gather_object(parts, r.state())
+        if rank == 0:
+            q.put(D.merge_states(arrays, parts))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_equal_whole_scene_oracle(oracle_lib, world):
+    steps = 12
+    pos, vel, iters = _whole_oracle(scenes.colliding_blocks(), steps)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, steps, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+# ----------------------------------------------------------------------------- library stages
+
+def _whole_library(sc, steps, extra):
+    import vtp
+    s = vtp.solver_from_scene(sc, extra=extra)
+    assert s.initialize()
+    iters = []
+    for _ in range(steps):
+        assert s.tickNsteps(1)
+        st = s.stats()
+        iters.append((st["last_div_iters"], st["last_incomp_iters"]))
+    fl = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    pos, vel = s.get_field("pos")[fl], s.get_field("vel")[fl]
+    s.destroy()
+    return pos, vel, iters
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+def test_library_domains_equal_whole_scene_library(vtp_gpu, ranks):
+    sc = scenes.dam_break("DFSPH", 8000, seed=22)
+    for extra in (FORCED, {}):
+        pos, vel, iters = _whole_library(sc, 5, extra)
+        out = domain.run_local(sc, ranks, 5, extra=extra)
+        assert out["iters"] == iters
+        assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+def test_library_domains_with_migration_tension_and_two_objects(vtp_gpu):
+    sc = scenes.colliding_blocks()
+    pos, vel, iters = _whole_library(sc, 25, {})
+    out = domain.run_local(sc, 4, 25)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+def test_library_domains_follow_the_decomposed_oracle(vtp_gpu, oracle_lib):
+    """The library's decomposed run against the oracle's decomposed run: FP32 vs FP64 after
+    three substeps with forced iterations (the bars of the whole-scene DFSPH parity test)."""
+    sc = scenes.colliding_blocks()
+    lib_out = domain.run_local(sc, 3, 3, extra=FORCED)
+    ora = domain.run_local(sc, 3, 3, make_stages=oracle_lib.DfsphDomainStages, extra=FORCED)
+    assert np.abs(lib_out["pos"] - ora["pos"]).max() < 1e-6
+    assert np.abs(lib_out["vel"] - ora["vel"]).max() < 1e-4
+
+
+@pytest.mark.gpu
+def test_dfsph_1m_in_four_slabs_equals_the_whole_scene(vtp_gpu):
+    sc = scenes.dfsph_1m()
+    pos, vel, iters = _whole_library(sc, 2, FORCED)
+    out = domain.run_local(sc, 4, 2, extra=FORCED)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)

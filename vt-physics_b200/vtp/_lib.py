@@ -80,6 +80,22 @@ SIGNATURES = {
     "vtp_solver_dfsph_solve_backward": (C.c_int, [_P, _P, _P]),
     "vtp_ugns_neighbors_noalloc": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
                                              C.c_uint32, _P, _P, _P]),
+    "vtp_domain_create": (C.c_int, [C.c_char_p, _P, C.c_uint32, _P, _P, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32,
+                                    C.POINTER(_P)]),
+    "vtp_domain_destroy": (None, [_P]),
+    "vtp_domain_set_stream": (C.c_int, [_P, _P]),
+    "vtp_domain_capacity": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "vtp_domain_load": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P]),
+    "vtp_domain_prepare": (C.c_int, [_P]),
+    "vtp_domain_solve_begin": (C.c_int, [_P, C.c_int]),
+    "vtp_domain_solve_a": (C.c_int, [_P, _P]),
+    "vtp_domain_solve_b": (C.c_int, [_P]),
+    "vtp_domain_forces": (C.c_int, [_P]),
+    "vtp_domain_tension": (C.c_int, [_P]),
+    "vtp_domain_finalize": (C.c_int, [_P]),
+    "vtp_domain_pack": (C.c_int, [_P, C.c_int, _P, C.c_uint32, _P]),
+    "vtp_domain_unpack": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_uint32, _P]),
+    "vtp_domain_read": (C.c_int, [_P, _P, _P]),
 }
 
 

@@ -223,6 +223,26 @@ def dam_break(solver: str, n_target: int, seed: int, gravity_y: float = -9.81, j
                                SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def colliding_blocks(seed: int = 41, tension: float = 0.001, speed: float = 1.5, n_side: int = 12,
+                     jitter_amp: float = 0.05) -> Scene:
+    """Two DFSPH fluid blocks (n_side^3 each, spacing 0.01) thrown at each other along x at
+    +-speed inside a 3-layer box whose longest side is x, so that a decomposition into x slabs
+    sees particles migrate between slabs within a few tens of substeps; surface tension on.
+    Both fluid objects come before the box in attach order."""
+    sp = 0.01
+    r = sp / 2
+    side = n_side * sp
+    a = jitter(cube(r, (0.05, 0.05, 0.05), (side, side, side)), jitter_amp, sp, seed)
+    b = jitter(cube(r, (0.1 + side, 0.06, 0.05), (side, side, side)), jitter_amp, sp, seed + 1)
+    lx = 0.16 + 2 * side
+    wall = box(r, (0.0, 0.0, 0.0), (lx, side + 0.13, side + 0.1), 3)
+    cfg = dfsph_config(dt=1e-3, r=r, lb=(-0.05, -0.05, -0.05), size=(lx + 0.1, side + 0.23, side + 0.2),
+                       tension=tension)
+    return Scene("DFSPH", cfg, [SceneObject("left", a, EPM_FLUID, velocity_start=(speed, 0.0, 0.0)),
+                                SceneObject("right", b, EPM_FLUID, velocity_start=(-speed, 0.0, 0.0)),
+                                SceneObject("box", wall, EPM_BOUNDARY)])
+
+
 def diff_pbf(seed: int = 5005) -> Scene:
     """The differentiable PBF scene: a 40^3 lattice (spacing 0.02, lb 0.2, no jitter) in a
     2-layer [0, 1.2]^3 box, initial fluid velocities N(0, 0.1^2) per component (SplitMix64
