@@ -9,7 +9,9 @@ The reference's own CMake build is not used (it needs vcpkg and MSVC-only
 flags).  ``CommonFunc.cpp`` is left out: the harness supplies ``cal_mean``.
 
 Builds without a GPU (nvcc cross-compiles for sm_100a); the library is loaded where the
-golden fixtures are generated.
+golden fixtures are generated.  The reference checkout is given by the environment
+variable VTP_REFERENCE, the ``reference`` argument of ``build``/``available`` or
+``--reference PATH`` on the command line; there is no default location.
 """
 from __future__ import annotations
 
@@ -22,8 +24,12 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE.parent / "_ref"
-REF = Path(os.environ.get("VTP_REFERENCE", "/root/reference"))
-SIM = REF / "Simulator"
+
+
+def reference_root(reference: str | os.PathLike | None = None) -> Path | None:
+    """The reference checkout: the argument, else VTP_REFERENCE, else none."""
+    p = reference or os.environ.get("VTP_REFERENCE")
+    return Path(p) if p else None
 
 SOURCES = [
     "Runtime/Source/Framework/Object.cpp",
@@ -53,16 +59,19 @@ def json_include() -> str:
     raise RuntimeError("nlohmann/json.hpp not found")
 
 
-def available() -> bool:
-    return SIM.exists()
+def available(reference: str | os.PathLike | None = None) -> bool:
+    ref = reference_root(reference)
+    return ref is not None and (ref / "Simulator").exists()
 
 
-def build(force: bool = False) -> Path:
+def build(force: bool = False, reference: str | os.PathLike | None = None) -> Path:
     out = OUT_DIR / "libvtref.so"
-    if not available():
+    if not available(reference):
         if out.exists():
             return out
-        raise RuntimeError(f"reference sources not found at {REF}")
+        raise RuntimeError(f"reference sources not found (VTP_REFERENCE / --reference: {reference_root(reference)})")
+    REF = reference_root(reference)
+    SIM = REF / "Simulator"
     OUT_DIR.mkdir(exist_ok=True)
     obj_dir = OUT_DIR / "obj"
     obj_dir.mkdir(exist_ok=True)
@@ -107,8 +116,9 @@ def build(force: bool = False) -> Path:
 
 
 if __name__ == "__main__":
+    ref = sys.argv[sys.argv.index("--reference") + 1] if "--reference" in sys.argv else None
     try:
-        print(build(force="--force" in sys.argv))
+        print(build(force="--force" in sys.argv, reference=ref))
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

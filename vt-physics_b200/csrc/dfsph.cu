@@ -95,6 +95,36 @@ __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_
     rest_density_b[r] = vb * a.rho_b;
 }
 
+// DFSPH compression ratio and alpha of one row (compute_compression_ratio_cuda +
+// compute_df_beta_cuda, DFSPHCudaImpl.cu:85-140), accumulated entry by entry in list
+// order, every rounding explicit.
+struct RatioAlpha {
+    float ratio, a1x, a1y, a1z, a2;
+
+    // self_w: the self term V_i W(0) (0 for a row outside the grid, which has no list)
+    __device__ __forceinline__ void begin(float self_w) {
+        ratio = self_w;
+        a1x = a1y = a1z = 0.f;
+        a2 = 1e-6f;
+    }
+    // One list entry j: d2 = |x_i - x_j|^2, (dx, dy, dz) = x_i - x_j, vj = V_j.
+    __device__ __forceinline__ void add(float d2, float dx, float dy, float dz, float vj, bool fluid_j,
+                                        const Cubic &k, float inv_mf) {
+        float w, g;
+        cubic_wg(d2, k, w, g);
+        ratio = __fmaf_rn(vj, w, ratio);
+        const float gx = __fmul_rn(g, dx), gy = __fmul_rn(g, dy), gz = __fmul_rn(g, dz);
+        a1x = __fmaf_rn(vj, gx, a1x);
+        a1y = __fmaf_rn(vj, gy, a1y);
+        a1z = __fmaf_rn(vj, gz, a1z);
+        if (fluid_j) a2 = __fmaf_rn(__fmul_rn(__fmul_rn(dist2(gx, gy, gz), vj), vj), inv_mf, a2);
+    }
+    __device__ __forceinline__ float alpha(float mass_f) const {
+        const float al = __fadd_rn(__fdiv_rn(dist2(a1x, a1y, a1z), mass_f), a2);
+        return al < 1e-6f ? 1e-6f : al;
+    }
+};
+
 struct PV {
     float4 q, v;
 };
@@ -108,27 +138,17 @@ __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
     if (r >= a.nf) return;
     const float4 p = a.pos[r];
     const uint32_t n = a.ncnt[r];
-    float ratio = n > 0 ? p.w * a.k.w0 : 0.f;   // self term V_i W(0)
-    float a1x = 0.f, a1y = 0.f, a1z = 0.f;
-    float a2 = 1e-6f;
-    const float inv_mf = 1.f / a.mass_f;
+    RatioAlpha ra;
+    ra.begin(n > 0 ? __fmul_rn(p.w, a.k.w0) : 0.f);   // self term V_i W(0)
+    const float inv_mf = __fdiv_rn(1.f, a.mass_f);
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     nbr_loop<U>(lst, n > 0 ? n - 1 : 0, [&](uint32_t j) { return ldg4(a.pos + j); },
                 [&](uint32_t j, const float4 &q) {
                     const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-                    float w, g;
-                    cubic_wg(dist2(dx, dy, dz), a.k, w, g);
-                    ratio = __fmaf_rn(q.w, w, ratio);
-                    const float gx = g * dx, gy = g * dy, gz = g * dz;
-                    a1x = __fmaf_rn(q.w, gx, a1x);
-                    a1y = __fmaf_rn(q.w, gy, a1y);
-                    a1z = __fmaf_rn(q.w, gz, a1z);
-                    if (j < a.nf) a2 += (gx * gx + gy * gy + gz * gz) * q.w * q.w * inv_mf;
+                    ra.add(dist2(dx, dy, dz), dx, dy, dz, q.w, j < a.nf, a.k, inv_mf);
                 });
-    float alpha = (a1x * a1x + a1y * a1y + a1z * a1z) / a.mass_f + a2;
-    if (alpha < 1e-6f) alpha = 1e-6f;
-    a.ratio[r] = ratio;
-    a.alpha[r] = alpha;
+    a.ratio[r] = ra.ratio;
+    a.alpha[r] = ra.alpha(a.mass_f);
 }
 
 // Tile kernels run a persistent grid over the scene-offset tiles; a tile of a

@@ -256,7 +256,8 @@ struct vtp_domain {
     DB<float> slot, objf;
     uint32_t *row_of_slot = nullptr;
     double *part = nullptr;
-    uint32_t *h_status = nullptr;
+    uint32_t *status = nullptr;     // the domain kernels' own status word (ST_BOUNDS: a bad slot)
+    uint32_t *h_status = nullptr;   // [2]: the domain word, the wrapped solver's word
     std::vector<void *> allocs;
 
     ~vtp_domain() {
@@ -348,7 +349,9 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         vtp_solver *s = d->s;
         if (s->L.nf != capacity || s->L.nb != nb) return fail(VTP_ERR_STATE, "domain worker layout");
         d->st = s->st;
-        CU(cudaMallocHost((void **)&d->h_status, sizeof(uint32_t)));
+        CU(cudaMallocHost((void **)&d->h_status, 2 * sizeof(uint32_t)));
+        if ((rc = d->alloc(&d->status, 1))) return rc;
+        CU(cudaMemsetAsync(d->status, 0, sizeof(uint32_t), d->st));
         for (int k = 0; k < 2; ++k) {
             if ((rc = d->alloc(&d->slot.b[k], capacity))) return rc;
             if ((rc = d->alloc(&d->objf.b[k], capacity))) return rc;
@@ -361,13 +364,12 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
             CU(cudaMemcpyAsync(gid, boundary_ids, nb * sizeof(uint32_t), cudaMemcpyHostToDevice, d->st));
             const uint32_t local0 = mode == 0 ? capacity : 0u;
             k_dd_band_ids<<<nblk(nb, 256), 256, 0, d->st>>>(nb, capacity, local0, gid, s->orig.b[0], s->orig.b[1],
-                                                            s->d_status);
+                                                            d->status);
             CU(cudaGetLastError());
         }
         // Boundary rows' packed gather rows ({x, V_b}, {x, v*}) never change: pack them once.
         vtp::dfsph_solve_pack(d->st, s->dfsph_args());
         CU(cudaGetLastError());
-        CU(cudaMemsetAsync(s->d_status, 0, sizeof(uint32_t), d->st));
         CU(cudaStreamSynchronize(d->st));
         *out = d.release();
         return VTP_OK;
@@ -437,7 +439,7 @@ int vtp_domain_prepare(vtp_domain *d) {
     vtp::ugns_build_lists(d->st, s->scn(), L, 0, d->n_act, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
                           s->d_status, s->d_overflow, s->block);
     if (d->n_act) {
-        k_dd_row_of_slot<<<nblk(d->n_act, 256), 256, 0, d->st>>>(d->n_act, d->slot.c(), d->row_of_slot, s->d_status);
+        k_dd_row_of_slot<<<nblk(d->n_act, 256), 256, 0, d->st>>>(d->n_act, d->slot.c(), d->row_of_slot, d->status);
         k_dd_tiles<<<nblk(nblk(d->n_act, s->block), 256), 256, 0, d->st>>>(s->d_tiles, d->n_act, (uint32_t)s->block);
     }
     d->which = 0;
@@ -523,7 +525,7 @@ int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t 
     if (count == 0) return VTP_OK;
     if (!d_slots || !d_out) return fail(VTP_ERR_ARG, "null array");
     const vtp::DfsphArgs a = d->args();
-    uint32_t *status = d->s->d_status;
+    uint32_t *status = d->status;
     switch (field) {
         case VTP_DOMAIN_KAPPA:
             k_dd_pack1<<<nblk(count, 256), 256, 0, d->st>>>(count, d->n_act, d_slots, d->row_of_slot, a.kappa, d_out,
@@ -554,7 +556,7 @@ int vtp_domain_unpack(vtp_domain *d, int field, uint32_t first_slot, uint32_t co
     if ((uint64_t)first_slot + count > d->n_act || first_slot < d->n_own)
         return fail(VTP_ERR_BOUNDS, "unpack outside the ghost rows");
     k_dd_unpack<<<nblk(count, 256), 256, 0, d->st>>>(field, count, first_slot, d->n_act, d->row_of_slot, d_in,
-                                                    (const float4 *)d_in, d->args(), d->s->d_status);
+                                                    (const float4 *)d_in, d->args(), d->status);
     CU(cudaGetLastError());
     return VTP_OK;
 }
@@ -566,13 +568,19 @@ int vtp_domain_read(vtp_domain *d, float *d_pos, float *d_vel) {
     if (d->n_own) {
         if (!d_pos || !d_vel) return fail(VTP_ERR_ARG, "null array");
         k_dd_read<<<nblk(d->n_own, 256), 256, 0, d->st>>>(d->n_own, d->n_act, d->row_of_slot, s->pos.c(), s->vel.c(),
-                                                         d_pos, d_vel, s->d_status);
+                                                         d_pos, d_vel, d->status);
     }
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(d->h_status, s->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, d->st));
+    CU(cudaMemcpyAsync(d->h_status, d->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, d->st));
+    CU(cudaMemcpyAsync(d->h_status + 1, s->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, d->st));
     CU(cudaStreamSynchronize(d->st));
-    const uint32_t st = *d->h_status;
-    if (st & vtp::ST_BOUNDS) return fail(VTP_ERR_BOUNDS, "a domain stage addressed a row outside the loaded rows");
-    if (st & vtp::ST_NAN) return fail(VTP_ERR_NAN, "non-finite state in a domain worker");
+    // A list longer than maxNeighborNum is truncated as the reference truncates it (the
+    // solver's word records it, not an error); the checked build's bounds reports are.
+    if (d->h_status[0] & vtp::ST_BOUNDS)
+        return fail(VTP_ERR_BOUNDS, "a domain stage addressed a row outside the loaded rows");
+#ifdef VTP_CHECKED
+    if (d->h_status[1] & vtp::ST_BOUNDS) return fail(VTP_ERR_BOUNDS, "a list entry or cell slot out of range");
+#endif
+    if (d->h_status[1] & vtp::ST_NAN) return fail(VTP_ERR_NAN, "non-finite state in a domain worker");
     return VTP_OK;
 }
