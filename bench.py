@@ -150,6 +150,15 @@ def ncu_traffic(workload: str, kernel: str):
         return None
 
 
+def ncu_instructions(workload: str, kernel: str):
+    """Warp instructions per launch measured by ncu for this kernel and workload, if recorded."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    try:
+        return json.loads(p.read_text()).get("warp_instructions", {}).get(workload, {}).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
 def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload) -> dict:
     """Roofline of one kernel against the HBM ceiling (no pass is a contraction, so the tensor
     ceiling does not apply): algorithmic state bytes per launch (each state array once, the work
@@ -173,6 +182,16 @@ def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload
     out["fp32"]["ideal_over_hbm"] = t_flops / t_bytes if t_bytes else None
     out.update({"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak})
     out["traffic"] = ncu_traffic(workload, name)
+    inst = ncu_instructions(workload, name)
+    if inst:
+        # An issue-bound kernel (the list builder): its warp instructions from one ncu capture
+        # over the live launch time, against 4 issue slots per SM per cycle at the sampled clock.
+        sms = 148
+        rate = inst / t / 1e9
+        cap = 4 * sms * mhz / 1e3
+        out["issue"] = {"achieved": rate, "peak": cap, "unit": "G warp-instructions/s", "frac": rate / cap,
+                        "instructions_per_launch": inst, "peak_kind": f"computed: 4 x {sms} SMs x {mhz:.0f} MHz",
+                        "instructions_from": "profiles/ncu_traffic.json"}
     return out
 
 
@@ -399,14 +418,22 @@ def run_batched(args, rank, world, local, dist, torch):
         dist.barrier()
     clk = Clocks(local if world > 1 else 0)
     clk.start()
+    # The batches advance concurrently, each on its own stream (vtp.solver.tick_together);
+    # the device time is the span between two events recorded on an idle GPU before the first
+    # substep is submitted and after the last one has finished.
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ev0.synchronize()
     t0 = time.perf_counter()
-    dev_ms = 0.0
-    launches = 0
-    for _, _, b, _ in batches:
-        assert b.tickNsteps(args.steps), b.last_error
-        dev_ms += b.stage_times()[2]
-        launches += b.launch_count()
+    from vtp.solver import tick_together
+    assert tick_together([b for _, _, b, _ in batches], args.steps), [b.last_error for _, _, b, _ in batches]
     wall = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    ev1.record()
+    ev1.synchronize()
+    dev_ms = ev0.elapsed_time(ev1)
+    launches = sum(b.launch_count() for _, _, b, _ in batches)
+    batch_ms = {kind: b.stage_times()[2] for kind, _, b, _ in batches}
     clocks = clk.stop()
     t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -444,9 +471,24 @@ def run_batched(args, rank, world, local, dist, torch):
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        for (_, _, b, _), bufs in zip(batches, hbuf):
-            state_round_trip(b, bufs)
+
+    failures = []
+
+    def e2e_run(k):
+        b, bufs = batches[k][2], hbuf[k]
+        try:
+            for _ in range(e2e_steps):
+                state_round_trip(b, bufs)
+        except BaseException as e:
+            failures.append(e)
+
+    threads = [threading.Thread(target=e2e_run, args=(k,)) for k in range(len(batches))]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if failures:
+        raise failures[0]
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
@@ -459,6 +501,8 @@ def run_batched(args, rank, world, local, dist, torch):
     cfg = {"workload": args.workload, "scenes": len(mix), "pbf_scenes": sum(m.solver == "PBF" for m in mix),
            "fluid": nf_all, "boundary": sum(m.n_boundary for m in mix), "scenes_this_rank": len(mine),
            "parallelism": f"scenes-lpt{world}", "wall_ms_per_step": 1e3 * wall / args.steps, "b200": extras,
+           "batches": "PBF and DFSPH batches on their own streams, advanced concurrently",
+           "batch_ms_per_step": {k: v / args.steps for k, v in batch_ms.items()},
            "l2": "inputs larger than L2 (~9.2M particles of state and neighbour lists)"}
     if world == 1 and not args.no_loop_baseline:
         # The plain per-scene loop: one solver per scene, scenes one after another.

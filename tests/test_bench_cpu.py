@@ -38,3 +38,29 @@ def test_gpus_flag_starts_its_own_ranks(bench, monkeypatch):
     assert "--master-addr" in cmd and cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
     assert cmd[-6:] == ["--gpus", "4", "--steps", "5", "--warmup", "3"]
     assert cmd[:3] == ["timeout", "-k", "60"]
+
+
+def test_tick_together_runs_every_solver_at_once_and_reports_failures():
+    """tick_together submits each solver's substeps from its own thread: all run at the same
+    time (a barrier only the whole group passes), results are combined, errors re-raised."""
+    import threading
+    from vtp.solver import tick_together
+
+    gate = threading.Barrier(3, timeout=10)
+
+    class Fake:
+        def __init__(self, ok=True, boom=False):
+            self.ok, self.boom, self.n = ok, boom, 0
+
+        def tickNsteps(self, n):
+            gate.wait()          # returns only when all three are inside their call
+            if self.boom:
+                raise RuntimeError("tick failed")
+            self.n += n
+            return self.ok
+
+    a, b, c = Fake(), Fake(), Fake()
+    assert tick_together([a, b, c], 7) and a.n == b.n == c.n == 7
+    assert not tick_together([Fake(), Fake(ok=False), Fake()], 1)
+    with pytest.raises(RuntimeError, match="tick failed"):
+        tick_together([Fake(), Fake(boom=True), Fake()], 1)

@@ -101,6 +101,17 @@ def test_decomposed_oracle_with_migration_tension_and_two_objects(oracle_lib, ra
     assert out["owned"] != start.tolist()   # ownership moved with the particles
 
 
+@pytest.mark.parametrize("speculate", [False, True])
+def test_queued_solve_a_changes_nothing(oracle_lib, speculate):
+    """The solve loop queues the next iteration's solve_a before it waits for the summed
+    residual and drops it when the solve stops; without the queued pass the run is the same."""
+    sc = scenes.colliding_blocks()
+    pos, vel, iters = _whole_oracle(sc, 6)
+    out = domain.run_local(sc, 2, 6, make_stages=oracle_lib.DfsphDomainStages, speculate=speculate)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))

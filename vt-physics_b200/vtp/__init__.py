@@ -8,9 +8,9 @@ from ._lib import FIELDS, LIB_PATH, VtpError, lib, status_string
 from .solver import (DFSPH, EPM_BOUNDARY, EPM_FLUID, IMM, IMMCT, PBF, DFSPHSolver, HostBuffer, IMMCTSolver,
                      IMMSolver, Object,
                      ObjectManager, PBFSolver, Solver, SolverManager, Particle_Box, Particle_Common, Particle_Cube,
-                     solver_from_scene, solver_from_scenes)
+                     solver_from_scene, solver_from_scenes, tick_together)
 
 __all__ = ["scenes", "FIELDS", "LIB_PATH", "VtpError", "lib", "status_string", "DFSPH", "EPM_BOUNDARY", "EPM_FLUID",
            "IMM", "IMMCT", "PBF", "DFSPHSolver", "IMMCTSolver", "IMMSolver", "Object", "ObjectManager", "PBFSolver",
            "Solver", "SolverManager", "Particle_Box", "Particle_Common", "Particle_Cube", "solver_from_scene",
-           "solver_from_scenes", "HostBuffer"]
+           "solver_from_scenes", "tick_together", "HostBuffer"]

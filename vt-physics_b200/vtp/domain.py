@@ -214,6 +214,8 @@ class LoopbackComm:
             torch.cuda.current_stream(t.device).synchronize()
 
     def exchange(self, sends: dict, recvs: dict) -> dict:
+        if self.size == 1:
+            return recvs
         box, me = self.hub.box, self.rank
         for q, t in sends.items():
             self._settle(t)
@@ -228,6 +230,8 @@ class LoopbackComm:
         return recvs
 
     def counts(self, send_counts: list, device=None) -> list:
+        if self.size == 1:
+            return [0]
         box, me = self.hub.box, self.rank
         box[("c", me)] = list(send_counts)
         self.hub.barrier.wait()
@@ -236,6 +240,8 @@ class LoopbackComm:
         return out
 
     def allreduce_sum(self, t):
+        if self.size == 1:   # nothing to add: no barrier, no stream synchronisation
+            return t
         box, me = self.hub.box, self.rank
         mine = t.clone()
         self._settle(mine)
@@ -374,9 +380,10 @@ class DomainRank:
     worker's stages with the exchanges of the module docstring."""
 
     def __init__(self, arrays: SceneArrays, plan: SlabPlan, comm, make_stages=LibraryStages,
-                 capacity_factor: float = 2.0):
+                 capacity_factor: float = 2.0, speculate: bool = True):
         import torch
         self.torch = torch
+        self.speculate = speculate
         self.a = arrays
         self.plan = plan
         self.comm = comm
@@ -436,6 +443,8 @@ class DomainRank:
         return out, got
 
     def _migrate(self):
+        if self.comm.size == 1:
+            return
         t = self.torch
         dest = self.plan.owner(self.pos[:, self.plan.axis])
         index_of = {q: t.nonzero(dest == q).flatten() for q in self._peers()}
@@ -448,6 +457,9 @@ class DomainRank:
 
     def _ghosts(self):
         t = self.torch
+        if self.comm.size == 1:
+            self.send_slots, self.recv_count, self.ghost_first = {}, [0], {}
+            return self.pos, self.vel, self.gid, self.obj
         x = self.pos[:, self.plan.axis]
         w = self.plan.ghost
         self.send_slots = {}
@@ -473,25 +485,53 @@ class DomainRank:
         for q, buf in recvs.items():
             self.stages.unpack(field, self.ghost_first[q], buf)
 
+    def _fetch(self, t):
+        """Start copying `t` to the host; returns a function that waits for the copy (and only
+        for it) and gives the values as a numpy array."""
+        if not t.is_cuda:
+            a = t.numpy().copy()
+            return lambda: a
+        torch = self.torch
+        if getattr(self, "_host", None) is None or self._host.numel() < t.numel():
+            self._host = torch.empty(max(t.numel(), 16), dtype=t.dtype, pin_memory=True)
+        h = self._host[: t.numel()]
+        h.copy_(t, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+
+        def wait():
+            ev.synchronize()
+            return h.numpy().copy()
+        return wait
+
     def _solve(self, which: int):
         """One pressure solve: the loop of vfsph_div / vfsph_incomp (DFSPHSolver.cpp:355-391) with
-        the residual summed over ranks; every rank takes the same decision from the same sum."""
+        the residual summed over ranks; every rank takes the same decision from the same sum.
+
+        With `speculate` the next iteration's solve_a (and its kappa exchange) is queued before
+        the host waits for the summed residual, so the GPU keeps working through the host round
+        trip; when the test stops the solve, that pass is dropped: solve_a writes only delta,
+        kappa and the packed {x, kappa} rows, which the next stage rewrites before reading."""
         st = self.stages
         st.solve_begin(which)
         force = self.force[which]
         if self.substeps < len(self.force_seq):
             force = self.force_seq[self.substeps][which]
         it = 0
+        sums = st.solve_a()
+        self._exchange(FIELD_KAPPA)
         while True:
             it += 1
-            sums = st.solve_a()
-            self._exchange(FIELD_KAPPA)
             st.solve_b()
             self._exchange(FIELD_VADV)
-            tot = self.comm.allreduce_sum(sums).cpu().numpy()
+            result = self._fetch(self.comm.allreduce_sum(sums))
+            if self.speculate:
+                sums = st.solve_a()
+                self._exchange(FIELD_KAPPA)
+            tot = result()
             acc = 0.0
-            for o, s in enumerate(tot):
-                acc += float(s) * self.inv_count[o]
+            for o, v in enumerate(tot):
+                acc += float(v) * self.inv_count[o]
             residual = acc / len(tot)
             if force > 0:
                 stop = it >= force
@@ -503,6 +543,9 @@ class DomainRank:
                 if force == 0 and it > self.max_iters - 1:
                     self.crashed = True
                 return it, residual
+            if not self.speculate:
+                sums = st.solve_a()
+                self._exchange(FIELD_KAPPA)
 
     # --- the substep
     def step(self, n: int = 1):
@@ -573,7 +616,7 @@ def merge_states(arrays: SceneArrays, states: list) -> dict:
 
 
 def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibraryStages,
-                capacity_factor: float = 2.0) -> list:
+                capacity_factor: float = 2.0, speculate: bool = True) -> list:
     """Run ``body(rank)`` for every domain of `plan` inside this process, one thread (and, with
     the library's stages, one CUDA stream) per domain, exchanging through ``LoopbackComm``;
     returns the bodies' results in rank order.  A failure on one domain releases the others
@@ -589,7 +632,7 @@ def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibrarySt
         try:
             ctx = torch.cuda.stream(torch.cuda.Stream()) if use_cuda else _null()
             with ctx:
-                rank = DomainRank(arrays, plan, LoopbackComm(hub, k), make_stages, capacity_factor)
+                rank = DomainRank(arrays, plan, LoopbackComm(hub, k), make_stages, capacity_factor, speculate)
                 results[k] = body(rank)
         except BaseException as e:   # wake the other domains, report the first failure
             errors.append(e)
@@ -610,7 +653,7 @@ def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibrarySt
 
 
 def run_local(scene, ranks: int, steps: int, make_stages=LibraryStages, axis: int | None = None,
-              capacity_factor: float = 2.0, extra: dict | None = None) -> dict:
+              capacity_factor: float = 2.0, extra: dict | None = None, speculate: bool = True) -> dict:
     """Run `scene` decomposed into `ranks` slabs inside this process (``local_ranks``) for
     `steps` substeps and merge the ranks' owned particles into the scene's fluid order."""
     arrays = scene_arrays(scene)
@@ -623,7 +666,7 @@ def run_local(scene, ranks: int, steps: int, make_stages=LibraryStages, axis: in
         rank.step(steps)
         return rank.state()
 
-    out = merge_states(arrays, local_ranks(arrays, plan, body, make_stages, capacity_factor))
+    out = merge_states(arrays, local_ranks(arrays, plan, body, make_stages, capacity_factor, speculate))
     out["plan"] = plan
     return out
 

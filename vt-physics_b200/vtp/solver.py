@@ -334,6 +334,34 @@ class SolverManager:
         return _CLASSES[solver_type](strict=strict)
 
 
+def tick_together(solvers, n: int) -> bool:
+    """Advance every solver `n` substeps with their CUDA streams running at the same time.
+
+    Each solver runs on its own stream and its tick call holds the calling thread until its
+    substeps finish, so one host thread per solver submits them (the library's calls release
+    the interpreter lock) and independent solvers - the PBF and DFSPH batches of a mixed set
+    of scenes, say - overlap on the GPU.  Returns whether every solver advanced; the first
+    exception a strict solver raises is raised here after all threads have finished."""
+    import threading
+    done = [False] * len(solvers)
+    errors = []
+
+    def run(k):
+        try:
+            done[k] = bool(solvers[k].tickNsteps(n))
+        except BaseException as e:
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(k,)) for k in range(len(solvers))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return all(done)
+
+
 def _attach_scene_objects(s: Solver, scene: "scenes.Scene", index: int = 0):
     for o in scene.objects:
         obj = Object(Particle_Common, o.name)
