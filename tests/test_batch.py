@@ -138,3 +138,33 @@ def test_batched_neighbor_lists_are_per_scene(vtp_gpu):
         assert np.array_equal(cnt[lo:hi], c1)
         assert np.array_equal(sub, np.where(n1 == 0xFFFFFFFF, -1, n1.astype(np.int64)))
     b.destroy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
+def test_batched_scenes_follow_the_fp64_oracle(vtp_gpu, oracle_lib, kind):
+    """Each scene of a batch of the benchmark's mix (log-uniform sizes, per-scene gravity, PBF
+    particles of mass 1) against the FP64 oracle advancing that scene alone, not only against
+    the library's own per-scene runs: positions within 1e-5 and velocities within 1e-4 of the
+    largest value after three substeps (DFSPH with forced iterations, so the comparison does
+    not hinge on the stop test)."""
+    mix = scenes.batched_scenes(count=8, n_pbf=4, n_min=2e3, n_max=1.6e4, pbf_spacing=0.1)
+    part = [m for m in mix if m.solver == kind]
+    force = (2, 3) if kind == "DFSPH" else (0, 0)
+    extra = {"forceDivIterations": force[0], "forceIncompIterations": force[1]} if kind == "DFSPH" else None
+    b, ranges = vtp.solver_from_scenes(part, extra)
+    assert b.initialize()
+    assert b.tickNsteps(3), b.last_error
+    pos, vel = b.get_field("pos"), b.get_field("vel")
+    b.destroy()
+    for k, sc in enumerate(part):
+        lo, hi = ranges[k]
+        o = oracle_lib.OracleSolver(sc, force_div=force[0], force_inc=force[1])
+        o.step(3)
+        fm = np.concatenate([np.full(ob.n, ob.material == 0) for ob in sc.objects])
+        req = sc.config[kind]["Required"]
+        v_floor = 1e-3 * 2 * float(req["particleRadius"]) / float(req["timeStep"])
+        dp = np.abs(pos[lo:hi][fm] - o.pos[fm]).max() / np.abs(o.pos[fm]).max()
+        dv = np.abs(vel[lo:hi][fm] - o.vel[fm]).max() / max(np.abs(o.vel[fm]).max(), v_floor)
+        print(f"{kind} scene {k} ({sc.n_fluid} fluid): pos {dp:.2e} vel {dv:.2e}")
+        assert dp < 1e-5 and dv < 1e-4, f"scene {k}"

@@ -66,6 +66,34 @@ def test_noalloc_neighbors_match_solver_api_twice(vtp_gpu, kind):
         assert np.array_equal(nbr, ref_nbr)
 
 
+def test_noalloc_upper_face_and_outside_particles_match_the_oracle(vtp_gpu, oracle_lib):
+    """Particles in the grid's inclusive upper cell layer (cell index == cells per axis, which
+    the reference's cellIsAvailable accepts and which shares its bucket numbering with the
+    next row of cells), exactly on the upper face, and outside the grid on either side: the
+    lists equal the FP32 restatement of the reference's search (no list, count 0, outside)."""
+    import torch
+    vtp = vtp_gpu
+    torch.cuda.set_device(0)
+    # h = 1/8 and size 1 give exactly 8 cells per axis; [1, 1.125) is the inclusive layer
+    req = {"particleRadius": 0.03125, "simSpaceLB": [0.0, 0.0, 0.0], "simSpaceSize": [1.0, 1.0, 1.0],
+           "maxNeighborNum": 60}
+    ax = np.arange(0.78, 1.2, 0.045, dtype=np.float32)
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    lattice = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    face = np.array([[1.0, 0.9, 0.95], [1.0, 1.0, 1.0], [0.95, 1.0, 1.05], [1.12, 1.124, 0.9],
+                     [1.125, 0.9, 0.9], [-0.01, 0.5, 0.5], [0.5, -1e-7, 0.5], [0.0, 0.0, 0.0],
+                     # cells (0, y + 1, z) share their buckets with the inclusive-layer cells (8, y, z)
+                     [0.01, 1.01, 0.9], [0.05, 1.06, 0.95], [0.03, 1.0, 1.0]], np.float32)
+    pos = np.ascontiguousarray(np.concatenate([lattice, face]), np.float32)
+    ref_cnt, ref_nbr, _, _ = oracle_lib.neighbors(pos, oracle_lib.make_grid(req))
+    assert (ref_cnt == 0).sum() > 0 and (ref_cnt > 1).sum() > 100
+    for _ in range(2):
+        cnt, nbr = _noalloc(vtp, torch, pos, req)
+        assert np.array_equal(cnt, ref_cnt)
+        for i in np.nonzero(ref_cnt)[0]:
+            assert np.array_equal(nbr[i, : ref_cnt[i]], ref_nbr[i, : ref_cnt[i]])
+
+
 def test_noalloc_rejects_oversized_input(vtp_gpu):
     import torch
     vtp = vtp_gpu
