@@ -431,6 +431,10 @@ VTP_API int vtp_ugns_neighbors_noalloc(const float *d_pos, uint32_t n, const flo
  *   between the solves: forces, [normals to ghosts, tension], velocities to
  *     ghosts;
  *   finalize, read.
+ * A PBF worker (PBFSolver::tick, PBFSolver.cpp:326-376) runs load, prepare
+ * (the external force applied in the sort to owned and ghost rows alike),
+ * then per constraint iteration pbf_lambda (+ lambda to ghosts) and pbf_dx
+ * (+ positions and velocities to ghosts), then pbf_xsph and read.
  * Every row carries its scene-wide attach id, so an owned row's neighbour
  * list and arithmetic are those of a solver holding the whole scene.  Device
  * pointers throughout; the work is enqueued on the worker's stream (the
@@ -440,9 +444,11 @@ typedef enum vtp_domain_field {
     VTP_DOMAIN_KAPPA = 0,    /* float per row: kappa after solve_a */
     VTP_DOMAIN_VADV = 1,     /* float4 per row: v* after solve_b */
     VTP_DOMAIN_VEL = 2,      /* float4 per row: velocity after forces / tension */
-    VTP_DOMAIN_NORMAL = 3    /* float4 per row: surface normal after forces (tension on) */
+    VTP_DOMAIN_NORMAL = 3,   /* float4 per row: surface normal after forces (tension on) */
+    VTP_DOMAIN_LAMBDA = 4,   /* PBF, float per row: lambda after a lambda pass */
+    VTP_DOMAIN_POSVEL = 5    /* PBF, 2 float4 per row {position, velocity}: after a correction pass */
 } vtp_domain_field;
-/* config_json: the scene's DFSPH config (the fixed timeStep: "cfl" must be 0).
+/* config_json: the scene's DFSPH or PBF config (DFSPH: the fixed timeStep, "cfl" 0).
  * fluid_pos: the worker's initial fluid rows (owned and ghost, host xyz,
  * ascending scene-wide id), used for the boundary volumes at create;
  * boundary_pos / boundary_ids: the boundary band (host, ids ascending);
@@ -471,9 +477,12 @@ VTP_API int vtp_domain_solve_b(vtp_domain *d);
 VTP_API int vtp_domain_forces(vtp_domain *d);
 VTP_API int vtp_domain_tension(vtp_domain *d);
 VTP_API int vtp_domain_finalize(vtp_domain *d);
+VTP_API int vtp_domain_pbf_lambda(vtp_domain *d);
+VTP_API int vtp_domain_pbf_dx(vtp_domain *d);
+VTP_API int vtp_domain_pbf_xsph(vtp_domain *d);
 /* Gathers `field` of the rows at load slots d_slots[count] into d_out
- * (count floats or float4s); unpack writes count values into the ghost rows at
- * load slots [first_slot, first_slot + count). */
+ * (count values of the field's size); unpack writes count values into the ghost
+ * rows at load slots [first_slot, first_slot + count). */
 VTP_API int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t count, float *d_out);
 VTP_API int vtp_domain_unpack(vtp_domain *d, int field, uint32_t first_slot, uint32_t count, const float *d_in);
 /* Owned rows' positions and velocities in load-slot order (float[3] each);

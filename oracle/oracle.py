@@ -87,6 +87,12 @@ def lib() -> C.CDLL:
         L.or_dfsph_forces.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph), P, P]
         L.or_dfsph_tension.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph), P]
         L.or_dfsph_accelerate.argtypes = [C.c_uint32, P, P, P, P, C.c_double]
+        for name in ("or_pbf_apply_force", "or_pbf_lambda", "or_pbf_dx", "or_pbf_xsph"):
+            getattr(L, name).restype = None
+        L.or_pbf_apply_force.argtypes = [C.c_uint32, P, P, P, C.POINTER(OrPbf)]
+        L.or_pbf_lambda.argtypes = [C.c_uint32, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf), P, P]
+        L.or_pbf_dx.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf), P]
+        L.or_pbf_xsph.argtypes = [C.c_uint32, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrPbf), P]
         L.or_dfsph_advance.argtypes = [C.c_uint32, P, P, P, P, C.c_double]
         L.or_num_threads.restype = C.c_int
         L.or_set_num_threads.argtypes = [C.c_int]
@@ -536,6 +542,118 @@ class DfsphDomainStages:
         self._field(field)[idx] = v
         if field == 2:   # velocities after the forces: v* = v
             self.vadv[idx] = v
+
+    def read(self):
+        idx = self.local_of_slot[: self.n_own]
+        return self.torch.from_numpy(self.pos[idx].copy()), self.torch.from_numpy(self.vel[idx].copy())
+
+
+class PbfDomainStages:
+    """FP64 PBF stages over one rank's particles of a slab-decomposed scene (test
+    infrastructure: the checker of the decomposed run, in the stage interface of
+    ``vtp.domain.LibraryStages``).  Particles are kept sorted by scene-wide id as in
+    ``DfsphDomainStages``; the stages are the functions ``or_pbf_step`` is made of
+    (PBFSolver.cpp:326-376)."""
+
+    def __init__(self, config: dict, fluid_pos0, bnd_pos, bnd_gid, boundary_first: bool, capacity: int,
+                 n_objects: int):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cpu")
+        self.dtype = torch.float64
+        req = config["PBF"]["Required"]
+        opt = config["PBF"]["Optional"]
+        self.grid = make_grid(req)
+        r = np.float32(req["particleRadius"])
+        self.vol0 = float(np.float32(np.float32(2) * r) ** np.float32(3))
+        p = OrPbf()
+        p.dt = float(np.float32(req["timeStep"]))
+        p.h = float(np.float32(r * np.float32(4)))
+        p.rho0 = float(np.float32(req["fPartRestDensity"]))
+        p.rho_b = float(np.float32(req["bPartRestDensity"]))
+        p.xsph_k = float(np.float32(req["XSPH_k"]))
+        p.eps = float(np.float32(1e-6))
+        g = [float(np.float32(v)) for v in opt["gravity"]] if opt["enable"] else [0.0, -9.8, 0.0]
+        for a in range(3):
+            p.g[a] = g[a]
+        p.iterations = int(req["iterationNum"])
+        ext = config.get("B200", {})
+        if ext.get("pbfFormulation", "reference") == "standard":
+            p.form = 1
+            p.eps = float(np.float32(ext.get("pbfEpsilon", 100.0)))
+        self.p = p
+        self.mass0 = p.rho0 * self.vol0
+        # boundary mass / volume of the band with the rank's initial fluid present (or_pbf_init)
+        fp0 = np.asarray(fluid_pos0, np.float64).reshape(-1, 3)
+        bp = np.asarray(bnd_pos, np.float64).reshape(-1, 3)
+        parts = [bp, fp0] if boundary_first else [fp0, bp]
+        mats = [np.ones(len(bp), np.int32), np.zeros(len(fp0), np.int32)]
+        if not boundary_first:
+            mats = mats[::-1]
+        pos = np.ascontiguousarray(np.concatenate(parts))
+        mat = np.concatenate(mats)
+        mass = np.full(len(pos), self.mass0)
+        vol = np.full(len(pos), self.vol0)
+        lib().or_pbf_init(len(pos), _ptr(mat), _ptr(pos), _ptr(mass), _ptr(vol), C.byref(self.grid), C.byref(p))
+        sel = mat == 1
+        self.bnd_pos = bp
+        self.bnd_gid = np.asarray(bnd_gid, np.int64)
+        self.bnd_mass = mass[sel]
+        self.bnd_vol = vol[sel]
+
+    def empty(self, field: int, count: int):
+        return self.torch.empty((count,) if field == 4 else (count, 6), dtype=self.torch.float64)
+
+    def load(self, n_own, pos, vel, gid, obj):
+        nf = pos.shape[0]
+        nb = len(self.bnd_gid)
+        order = np.argsort(np.concatenate([gid.numpy().astype(np.int64), self.bnd_gid]), kind="stable")
+        inv = np.empty_like(order)
+        inv[order] = np.arange(len(order))
+        self.local_of_slot = inv[:nf]
+        self.n_own = int(n_own)
+        cat = lambda f, b: np.ascontiguousarray(np.concatenate([f, b])[order])
+        self.pos = cat(pos.numpy().astype(np.float64), self.bnd_pos)
+        self.vel = cat(vel.numpy().astype(np.float64), np.zeros((nb, 3)))
+        self.mat = cat(np.zeros(nf, np.int32), np.ones(nb, np.int32))
+        self.mass = cat(np.full(nf, self.mass0), self.bnd_mass)
+        self.vol = cat(np.full(nf, self.vol0), self.bnd_vol)
+        self.n = nf + nb
+
+    def prepare(self):
+        lib().or_pbf_apply_force(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), C.byref(self.p))
+        self.cnt, self.nbr, _, _ = neighbors(self.pos.astype(np.float32), self.grid)
+        self.M = int(self.grid.maxnbr)
+        self.rho = np.zeros(self.n)
+        self.lam = np.zeros(self.n)
+        self.dx = np.zeros((self.n, 3))
+
+    def pbf_lambda(self):
+        lib().or_pbf_lambda(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.mass), _ptr(self.cnt), _ptr(self.nbr),
+                            self.M, C.byref(self.p), _ptr(self.rho), _ptr(self.lam))
+
+    def pbf_dx(self):
+        lib().or_pbf_dx(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), _ptr(self.mass), _ptr(self.lam),
+                        _ptr(self.cnt), _ptr(self.nbr), self.M, C.byref(self.p), _ptr(self.dx))
+
+    def pbf_xsph(self):
+        lib().or_pbf_xsph(self.n, _ptr(self.mat), _ptr(self.pos), _ptr(self.vel), _ptr(self.vol), _ptr(self.cnt),
+                          _ptr(self.nbr), self.M, C.byref(self.p), _ptr(self.dx))
+
+    def pack(self, field: int, slots):
+        idx = self.local_of_slot[slots.numpy()]
+        if field == 4:
+            return self.torch.from_numpy(self.lam[idx].copy())
+        return self.torch.from_numpy(np.concatenate([self.pos[idx], self.vel[idx]], axis=1))
+
+    def unpack(self, field: int, first: int, values):
+        idx = self.local_of_slot[first: first + values.shape[0]]
+        v = values.numpy()
+        if field == 4:
+            self.lam[idx] = v
+        else:
+            self.pos[idx] = v[:, :3]
+            self.vel[idx] = v[:, 3:]
 
     def read(self):
         idx = self.local_of_slot[: self.n_own]

@@ -195,6 +195,10 @@ static void free_lists(lists_t *L) {
 #define FOR_NBR(L, g, i, j)                                                              \
     for (uint32_t t_ = 0, j = 0; t_ < (L).cnt[i] && ((j = (L).nbr[(size_t)(i) * (g)->maxnbr + t_]), 1); ++t_)
 
+/* The entries of row i of lists in the layout of or_neighbors (self first). */
+#define FOR_LIST(cnt, nbr, M, i, j) \
+    for (uint32_t t_ = 0, j = 0; t_ < (cnt)[i] && ((j = (nbr)[(size_t)(i) * (M) + t_]), 1); ++t_)
+
 static double rdiff(const double *pos, uint32_t i, uint32_t j, double *r) {
     r[0] = pos[3 * (size_t)i] - pos[3 * (size_t)j];
     r[1] = pos[3 * (size_t)i + 1] - pos[3 * (size_t)j + 1];
@@ -243,68 +247,80 @@ void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass
 
 /* Constraint iterations + XSPH of one substep on the lists L (positions
  * already advanced by the external force). */
-static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
-                     const double *vol, const lists_t *Lp, const or_grid *g, const or_pbf_params *p,
-                     double *density_out, double *lambda_out) {
-    const lists_t L = *Lp;
-    const double dt = p->dt;
+/* PBF substep stages over given lists (layout of or_neighbors).  pbf_core (the
+ * monolithic step) runs them over every particle; a slab-decomposed run runs them
+ * over one rank's particles and replaces the ghosts' lambda after or_pbf_lambda
+ * and their positions and velocities after or_pbf_dx. */
+void or_pbf_lambda(uint32_t n, const int32_t *mat, const double *pos, const double *mass, const uint32_t *cnt,
+                   const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *rho, double *lam) {
+    /* compute_sph_density_and_error_cuda + update_lamb_cuda (PBFCudaImpl.cu:70-122). */
     cubic_t k = cubic_make(p->h);
-    double *lam = (double *)calloc(n ? n : 1, sizeof(double));
-    double *rho = (double *)calloc(n ? n : 1, sizeof(double));
-    double *dx = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
-    for (int it = 0; it < p->iterations; ++it) {
 #pragma omp parallel for
-        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-            uint32_t i = (uint32_t)ii;
-            if (mat[i] != 0) continue;
-            double d = 0, gs[3] = {0, 0, 0}, s2 = 0, r[3];
-            FOR_NBR(L, g, i, j) {
-                double rl = rdiff(pos, i, j, r);
-                d += mass[j] * pbf_w(p, &k, rl);
-                double gg = pbf_g(p, &k, rl) * (p->form == 1 ? mass[j] : 1.0);
-                for (int a = 0; a < 3; ++a) {
-                    double e = gg * r[a];
-                    gs[a] += e;
-                    s2 += (e / p->rho0) * (e / p->rho0);
-                }
-            }
-            if (d < p->rho0) d = p->rho0;
-            double C = d / p->rho0 - 1.0;
-            for (int a = 0; a < 3; ++a) {
-                gs[a] /= p->rho0;
-                s2 += gs[a] * gs[a];
-            }
-            rho[i] = d;
-            lam[i] = -C / (s2 + p->eps);
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) {
+            lam[i] = 0.0;   /* boundary lambda never set: 0 */
+            continue;
         }
+        double d = 0, gs[3] = {0, 0, 0}, s2 = 0, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            double rl = rdiff(pos, i, j, r);
+            d += mass[j] * pbf_w(p, &k, rl);
+            double gg = pbf_g(p, &k, rl) * (p->form == 1 ? mass[j] : 1.0);
+            for (int a = 0; a < 3; ++a) {
+                double e = gg * r[a];
+                gs[a] += e;
+                s2 += (e / p->rho0) * (e / p->rho0);
+            }
+        }
+        if (d < p->rho0) d = p->rho0;
+        double C = d / p->rho0 - 1.0;
+        for (int a = 0; a < 3; ++a) {
+            gs[a] /= p->rho0;
+            s2 += gs[a] * gs[a];
+        }
+        rho[i] = d;
+        lam[i] = -C / (s2 + p->eps);
+    }
+}
+
+void or_pbf_dx(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *lam,
+               const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *dx) {
+    /* compute_dx_cuda + apply_dx_cuda (PBFCudaImpl.cu:124-170): Jacobi, all dx first. */
+    cubic_t k = cubic_make(p->h);
 #pragma omp parallel for
-        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-            uint32_t i = (uint32_t)ii;
-            if (mat[i] != 0) continue;
-            double s[3] = {0, 0, 0}, r[3];
-            FOR_NBR(L, g, i, j) {
-                double gg = pbf_g(p, &k, rdiff(pos, i, j, r));
-                double lj = mat[j] == 0 ? lam[j] : 0.0; /* boundary lambda never set: 0 */
-                double c = p->form == 1 ? lam[i] * mass[j] + lj * mass[i] : lam[i] + lj;
-                for (int a = 0; a < 3; ++a) s[a] += c * gg * r[a];
-            }
-            for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = s[a] / p->rho0;
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double s[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            double gg = pbf_g(p, &k, rdiff(pos, i, j, r));
+            double lj = mat[j] == 0 ? lam[j] : 0.0;
+            double c = p->form == 1 ? lam[i] * mass[j] + lj * mass[i] : lam[i] + lj;
+            for (int a = 0; a < 3; ++a) s[a] += c * gg * r[a];
         }
-        for (uint32_t i = 0; i < n; ++i) {
-            if (mat[i] != 0) continue;
-            for (int a = 0; a < 3; ++a) {
-                pos[3 * (size_t)i + a] += dx[3 * (size_t)i + a];
-                vel[3 * (size_t)i + a] += dx[3 * (size_t)i + a] / dt;
-            }
+        for (int a = 0; a < 3; ++a) dx[3 * (size_t)i + a] = s[a] / p->rho0;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            pos[3 * (size_t)i + a] += dx[3 * (size_t)i + a];
+            vel[3 * (size_t)i + a] += dx[3 * (size_t)i + a] / p->dt;
         }
     }
+}
+
+void or_pbf_xsph(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vol, const uint32_t *cnt,
+                 const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *dx) {
     /* XSPH_cuda + apply_dx_cuda (PBFCudaImpl.cu:172-194). */
+    cubic_t k = cubic_make(p->h);
+    const double dt = p->dt;
 #pragma omp parallel for
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         uint32_t i = (uint32_t)ii;
         if (mat[i] != 0) continue;
         double dv[3] = {0, 0, 0}, r[3];
-        FOR_NBR(L, g, i, j) {
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
             double w = pbf_w(p, &k, rdiff(pos, i, j, r));
             for (int a = 0; a < 3; ++a) dv[a] += p->xsph_k * vol[j] * (vel[3 * (size_t)j + a] - vel[3 * (size_t)i + a]) * w;
         }
@@ -317,6 +333,21 @@ static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, c
             vel[3 * (size_t)i + a] += dx[3 * (size_t)i + a] / dt;
         }
     }
+}
+
+static void pbf_core(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
+                     const double *vol, const lists_t *Lp, const or_grid *g, const or_pbf_params *p,
+                     double *density_out, double *lambda_out) {
+    const lists_t L = *Lp;
+    const uint32_t M = g->maxnbr;
+    double *lam = (double *)calloc(n ? n : 1, sizeof(double));
+    double *rho = (double *)calloc(n ? n : 1, sizeof(double));
+    double *dx = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+    for (int it = 0; it < p->iterations; ++it) {
+        or_pbf_lambda(n, mat, pos, mass, L.cnt, L.nbr, M, p, rho, lam);
+        or_pbf_dx(n, mat, pos, vel, mass, lam, L.cnt, L.nbr, M, p, dx);
+    }
+    or_pbf_xsph(n, mat, pos, vel, vol, L.cnt, L.nbr, M, p, dx);
     if (density_out) memcpy(density_out, rho, sizeof(double) * n);
     if (lambda_out) memcpy(lambda_out, lam, sizeof(double) * n);
     free(lam);
@@ -332,6 +363,10 @@ static void pbf_apply_force(uint32_t n, const int32_t *mat, double *pos, double 
             pos[3 * (size_t)i + a] += vel[3 * (size_t)i + a] * p->dt;
         }
     }
+}
+
+void or_pbf_apply_force(uint32_t n, const int32_t *mat, double *pos, double *vel, const or_pbf_params *p) {
+    pbf_apply_force(n, mat, pos, vel, p);
 }
 
 void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *vol,
@@ -569,8 +604,6 @@ void or_dfsph_init(uint32_t n, const int32_t *mat, const double *pos, double *vo
  * slab-decomposed run runs them over one rank's particles (owned fluid, ghost
  * fluid, a band of the boundary) and exchanges the ghosts' values between them.
  * Lists are in the layout of or_neighbors: cnt[n], nbr[n * maxnbr]. */
-#define FOR_LIST(cnt, nbr, M, i, j) \
-    for (uint32_t t_ = 0, j = 0; t_ < (cnt)[i] && ((j = (nbr)[(size_t)(i) * (M) + t_]), 1); ++t_)
 
 void or_dfsph_ratio_alpha(uint32_t n, const int32_t *mat, const double *pos, const double *vol, const double *mass,
                           const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, double h, double *ratio,

@@ -66,6 +66,19 @@ void or_pbf_init(uint32_t n, const int32_t *mat, const double *pos, double *mass
 void or_pbf_step(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass,
                  const double *vol, const or_grid *g, const or_pbf_params *p, double *density, double *lambda);
 
+/* The stages of a PBF substep over given lists (cnt[n], nbr[n * maxnbr] in the layout of
+ * or_neighbors): the external force (before the lists are built), then per constraint
+ * iteration or_pbf_lambda and or_pbf_dx (dx[3n] scratch; positions and velocities updated
+ * in place), then or_pbf_xsph.  A slab-decomposed run replaces the ghosts' lambda between
+ * lambda and dx, and their positions and velocities after dx. */
+void or_pbf_apply_force(uint32_t n, const int32_t *mat, double *pos, double *vel, const or_pbf_params *p);
+void or_pbf_lambda(uint32_t n, const int32_t *mat, const double *pos, const double *mass, const uint32_t *cnt,
+                   const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *rho, double *lam);
+void or_pbf_dx(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *mass, const double *lam,
+               const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *dx);
+void or_pbf_xsph(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vol, const uint32_t *cnt,
+                 const uint32_t *nbr, uint32_t maxnbr, const or_pbf_params *p, double *dx);
+
 /* Differentiable PBF (no counterpart in the reference).  A substep with the
  * neighbour lists given (frozen: reference layout, attach ids, self first),
  * and its FP64 adjoint: from the pre-step state (pos, vel) and the same lists,

@@ -1,4 +1,4 @@
-"""Single-scene domain decomposition (vtp/domain.py, csrc/domain.cu).
+"""Single-scene domain decomposition of DFSPH and PBF (vtp/domain.py, csrc/domain.cu).
 
 The decomposed run must reproduce the whole-scene run bit for bit: every owned row
 sees the whole-scene neighbour list and neighbour values.  On CPU the stages are
@@ -61,8 +61,8 @@ def test_scene_arrays_keep_attach_ids_and_reject_interleaved_ids():
     sc.objects = [sc.objects[0], sc.objects[2], sc.objects[1]]   # fluid, box, fluid
     with pytest.raises(ValueError, match="fluid ids all below or all above"):
         domain.scene_arrays(sc)
-    with pytest.raises(ValueError, match="DFSPH"):
-        domain.scene_arrays(scenes.dam_break("PBF", 500, seed=1))
+    with pytest.raises(ValueError, match="DFSPH and PBF"):
+        domain.scene_arrays(scenes.layered_mixture("IMMCT", 6, seed=1))
 
 
 def test_decomposed_run_rejects_the_adaptive_step(oracle_lib):
@@ -112,6 +112,39 @@ def test_queued_solve_a_changes_nothing(oracle_lib, speculate):
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
 
 
+def _whole_oracle_fields(sc, steps):
+    from oracle import oracle as O
+    o = O.OracleSolver(sc)
+    o.step(steps)
+    fl = o.mat == 0
+    return o.pos[fl], o.vel[fl]
+
+
+@pytest.mark.parametrize("ranks", [1, 2, 3])
+def test_decomposed_pbf_oracle_equals_whole_scene_oracle(oracle_lib, ranks):
+    """PBF: lambda and the corrected positions / velocities go to the ghosts every constraint
+    iteration; the external force is applied to owned and ghost rows alike."""
+    sc = scenes.pbf_dam_break_m1()
+    pos, vel = _whole_oracle_fields(sc, 4)
+    out = domain.run_local(sc, ranks, 4, make_stages=oracle_lib.PbfDomainStages)
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+    assert out["iters"] == [(4, 0)] * 4
+
+
+@pytest.mark.parametrize("ranks", [2, 4])
+def test_decomposed_pbf_oracle_follows_a_collapsing_column(oracle_lib, ranks):
+    """80 substeps of a mass-1 dam break split across its height: the column collapses through
+    the slab bounds (ownership moves), speeds reach ~5 m/s and ghosts are chosen with the
+    external-force reach added."""
+    sc = scenes.dam_break("PBF", 3000, seed=21, spacing=0.1)
+    pos, vel = _whole_oracle_fields(sc, 80)
+    out = domain.run_local(sc, ranks, 80, make_stages=oracle_lib.PbfDomainStages)
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+    plan = out["plan"]
+    start = np.bincount(plan.owner(domain.scene_arrays(sc).fluid_pos[:, plan.axis]), minlength=ranks)
+    assert out["owned"] != start.tolist()
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -120,7 +153,7 @@ def _free_port():
     return p
 
 
-def _gloo_rank(rank, world, port, steps, q):
+def _gloo_rank(rank, world, port, steps, q, kind="DFSPH"):
     import datetime
     import sys
     from pathlib import Path
@@ -133,9 +166,11 @@ def _gloo_rank(rank, world, port, steps, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
-        arrays = D.scene_arrays(S.colliding_blocks())
+        sc = S.colliding_blocks() if kind == "DFSPH" else S.dam_break("PBF", 3000, seed=21, spacing=0.1)
+        arrays = D.scene_arrays(sc)
         plan = D.plan_slabs(arrays, world)
-        r = D.DomainRank(arrays, plan, D.TorchComm(), O.DfsphDomainStages)
+        stages = O.DfsphDomainStages if kind == "DFSPH" else O.PbfDomainStages
+        r = D.DomainRank(arrays, plan, D.TorchComm(), stages)
         r.step(steps)
         parts = [None] * world
         dist.all_gather_object(parts, r.state())
@@ -146,14 +181,18 @@ def _gloo_rank(rank, world, port, steps, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_equal_whole_scene_oracle(oracle_lib, world):
+@pytest.mark.parametrize("world,kind", [(2, "DFSPH"), (3, "DFSPH"), (2, "PBF")])
+def test_gloo_ranks_equal_whole_scene_oracle(oracle_lib, world, kind):
     steps = 12
-    pos, vel, iters = _whole_oracle(scenes.colliding_blocks(), steps)
+    if kind == "DFSPH":
+        pos, vel, iters = _whole_oracle(scenes.colliding_blocks(), steps)
+    else:
+        pos, vel = _whole_oracle_fields(scenes.dam_break("PBF", 3000, seed=21, spacing=0.1), steps)
+        iters = [(4, 0)] * steps
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, steps, q)) for r in range(world)]
+    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, steps, q, kind)) for r in range(world)]
     for p in procs:
         p.start()
     out = q.get(timeout=300)
@@ -218,4 +257,15 @@ def test_dfsph_1m_in_four_slabs_equals_the_whole_scene(vtp_gpu):
     pos, vel, iters = _whole_library(sc, 2, FORCED)
     out = domain.run_local(sc, 4, 2, extra=FORCED)
     assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+def test_library_pbf_domains_equal_whole_scene_library(vtp_gpu, ranks):
+    """PBF at mass-1 particles, the collapsing column over 40 substeps: the decomposed library
+    run equals the whole-scene library run bit for bit."""
+    sc = scenes.dam_break("PBF", 8000, seed=21, spacing=0.1)
+    pos, vel, _ = _whole_library(sc, 40, {})
+    out = domain.run_local(sc, ranks, 40)
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)

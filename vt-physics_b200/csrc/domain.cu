@@ -1,6 +1,6 @@
 // Single-scene domain decomposition: the worker one rank runs for its slab of
-// a DFSPH scene (no counterpart in the reference, which runs a scene on one
-// device: SolverManager.cpp:11-17).
+// a DFSPH or PBF scene (no counterpart in the reference, which runs a scene on
+// one device: SolverManager.cpp:11-17).
 //
 // A rank holds the fluid particles it owns, copies ("ghosts") of the fluid
 // particles other ranks own within the ghost width of its slab, and the
@@ -10,7 +10,11 @@
 // library's own kernels; between the stages the host replaces the ghosts'
 // values with their owners' (kappa after solve_a, v* after solve_b, the
 // velocities after the viscosity / tension pass and the surface normals
-// between the two) and adds the ranks' FP64 residual sums.
+// between the two) and adds the ranks' FP64 residual sums.  A PBF worker runs
+// PBFSolver::tick (PBFSolver.cpp:326-376) the same way: the external force is
+// applied in the sort to every loaded row (owned and ghost alike), and the host
+// replaces the ghosts' lambda after each lambda pass and their positions and
+// velocities after each position-correction pass.
 //
 // Rows carry their scene-wide attach ids, so the sort by (cell, attach id)
 // and the lists of an owned row are those of a solver holding the whole
@@ -76,15 +80,16 @@ __device__ double block_sum_d(double v) {
 }
 
 __global__ void k_dd_load(uint32_t n, const float *__restrict__ pos3, const float *__restrict__ vel3,
-                          const uint32_t *__restrict__ ids, const uint32_t *__restrict__ obj, float vol0,
+                          const uint32_t *__restrict__ ids, const uint32_t *__restrict__ obj, float w,
                           float4 *__restrict__ pos, float4 *__restrict__ vel, float4 *__restrict__ vadv,
                           uint32_t *__restrict__ orig, float *__restrict__ slot, float *__restrict__ objf) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    pos[r] = make_float4(pos3[3 * (size_t)r], pos3[3 * (size_t)r + 1], pos3[3 * (size_t)r + 2], vol0);
+    // w: the volume (DFSPH) or the mass (PBF) every fluid row carries
+    pos[r] = make_float4(pos3[3 * (size_t)r], pos3[3 * (size_t)r + 1], pos3[3 * (size_t)r + 2], w);
     const float4 v = make_float4(vel3[3 * (size_t)r], vel3[3 * (size_t)r + 1], vel3[3 * (size_t)r + 2], 0.f);
     vel[r] = v;
-    vadv[r] = v;   // v* = v at the start of the substep
+    if (vadv) vadv[r] = v;   // DFSPH: v* = v at the start of the substep
     orig[r] = ids[r];
     slot[r] = (float)r;
     objf[r] = obj ? (float)obj[r] : 0.f;
@@ -177,6 +182,31 @@ __global__ void k_dd_pack1(uint32_t count, uint32_t n, const uint32_t *__restric
     out[k] = src[r];
 }
 
+__global__ void k_dd_pack_posvel(uint32_t count, uint32_t n, const uint32_t *__restrict__ slots,
+                                 const uint32_t *__restrict__ row_of_slot, const float4 *__restrict__ pos,
+                                 const float4 *__restrict__ vel, float4 *__restrict__ out, uint32_t *status) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r;
+    if (k >= count || !slot_row(slots[k], n, row_of_slot, status, r)) return;
+    out[2 * (size_t)k] = pos[r];
+    out[2 * (size_t)k + 1] = vel[r];
+}
+
+__global__ void k_dd_unpack_pbf(int field, uint32_t count, uint32_t first, uint32_t n,
+                                const uint32_t *__restrict__ row_of_slot, const float *__restrict__ in1,
+                                const float4 *__restrict__ in4, float *__restrict__ lambda, float4 *__restrict__ pos,
+                                float4 *__restrict__ vel, uint32_t *status) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r;
+    if (k >= count || !slot_row(first + k, n, row_of_slot, status, r)) return;
+    if (field == VTP_DOMAIN_LAMBDA) {
+        lambda[r] = in1[k];
+    } else {
+        pos[r] = in4[2 * (size_t)k];
+        vel[r] = in4[2 * (size_t)k + 1];
+    }
+}
+
 __global__ void k_dd_pack4(uint32_t count, uint32_t n, const uint32_t *__restrict__ slots,
                            const uint32_t *__restrict__ row_of_slot, const float4 *__restrict__ src,
                            float4 *__restrict__ out, uint32_t *status) {
@@ -235,11 +265,11 @@ __global__ void k_dd_read(uint32_t n_own, uint32_t n, const uint32_t *__restrict
     vel3[3 * (size_t)s + 2] = v.z;
 }
 
-std::string object_json(int material) {
+std::string object_json(int material, int type) {
     json o = {{"name", material == 0 ? "domain fluid" : "domain boundary"},
               {"ObjectComponentConfig", {{"epmMaterial", material}}},
               {"SolverObjectComponentConfig",
-               {{"solverType", (int)VTP_SOLVER_DFSPH}, {"exportFlag", false}, {"velocityStart", {0, 0, 0}},
+               {{"solverType", type}, {"exportFlag", false}, {"velocityStart", {0, 0, 0}},
                 {"colorStart", {0, 0, 0}}}}};
     return o.dump();
 }
@@ -248,6 +278,7 @@ std::string object_json(int material) {
 
 struct vtp_domain {
     vtp_solver *s = nullptr;
+    int type = VTP_SOLVER_DFSPH;   // VTP_SOLVER_DFSPH or VTP_SOLVER_PBF
     uint32_t cap = 0, nb = 0, nobj = 1;
     uint32_t n_own = 0, n_act = 0;
     int which = 0;
@@ -284,6 +315,11 @@ struct vtp_domain {
         a.tick = nullptr;
         return a;
     }
+    vtp::PbfArgs pbf() const {
+        vtp::PbfArgs a = s->pbf_args();
+        a.nf = n_act;
+        return a;
+    }
     vtp::Layout layout() const {
         vtp::Layout L = s->L;
         L.nf = n_act;
@@ -296,6 +332,15 @@ namespace {
 int need_prepared(vtp_domain *d) {
     if (!d) return fail(VTP_ERR_ARG, "null domain");
     if (!d->prepared) return fail(VTP_ERR_STATE, "domain stage before vtp_domain_prepare");
+    return VTP_OK;
+}
+
+int need_type(vtp_domain *d, int type) {
+    int rc;
+    if ((rc = need_prepared(d))) return rc;
+    if (d->type != type)
+        return fail(VTP_ERR_STATE, type == VTP_SOLVER_PBF ? "a PBF stage on a DFSPH domain worker"
+                                                          : "a DFSPH stage on a PBF domain worker");
     return VTP_OK;
 }
 
@@ -314,7 +359,9 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         if (boundary_ids[k] <= boundary_ids[k - 1]) return fail(VTP_ERR_ARG, "boundary ids not ascending");
     try {
         json cfg = json::parse(config_json);
-        if (!cfg.contains("DFSPH")) return fail(VTP_ERR_CONFIG, "domain workers run DFSPH scenes");
+        const bool pbf = cfg.contains("PBF");
+        if (!pbf && !cfg.contains("DFSPH")) return fail(VTP_ERR_CONFIG, "domain workers run DFSPH or PBF scenes");
+        const char *key = pbf ? "PBF" : "DFSPH";
         json ext = cfg.contains("B200") ? cfg["B200"] : json::object();
         if (ext.value("cfl", 0.0) > 0.0) return fail(VTP_ERR_CONFIG, "a domain worker takes the fixed timeStep (cfl 0)");
         const int mode = boundary_first ? 1 : 0;
@@ -322,18 +369,19 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         ext["deviceLoop"] = false;
         ext["stagedSolve"] = false;
         cfg["B200"] = ext;
-        const json &req = cfg["DFSPH"]["Required"];
+        const json &req = cfg[key]["Required"];
         const float r = req.at("particleRadius").get<float>();
         const float h = r * 4.f;
         float park[3];
         for (int a = 0; a < 3; ++a) park[a] = req.at("simSpaceLB")[a].get<float>() - 8.f * h;   // outside the grid
 
         auto d = std::make_unique<vtp_domain>();
+        d->type = pbf ? VTP_SOLVER_PBF : VTP_SOLVER_DFSPH;
         d->cap = capacity;
         d->nb = nb;
         d->nobj = n_objects;
         int rc;
-        if ((rc = vtp_solver_create(VTP_SOLVER_DFSPH, &d->s))) return rc;
+        if ((rc = vtp_solver_create(d->type, &d->s))) return rc;
         if ((rc = vtp_solver_set_config(d->s, cfg.dump().c_str()))) return rc;
         // Fluid rows: the initial owned and ghost particles (ascending scene-wide id, so that
         // the boundary rows' lists at initialize, and with them the boundary volumes, are those
@@ -341,7 +389,7 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         std::vector<float> fl((size_t)capacity * 3);
         for (uint32_t i = 0; i < capacity; ++i)
             for (int a = 0; a < 3; ++a) fl[3 * (size_t)i + a] = i < n_fluid ? fluid_pos[3 * (size_t)i + a] : park[a];
-        const std::string fj = object_json(0), bj = object_json(1);
+        const std::string fj = object_json(0, d->type), bj = object_json(1, d->type);
         if (mode == 1 && nb && (rc = vtp_solver_attach_object(d->s, boundary_pos, nb, nullptr, bj.c_str()))) return rc;
         if ((rc = vtp_solver_attach_object(d->s, fl.data(), capacity, nullptr, fj.c_str()))) return rc;
         if (mode == 0 && nb && (rc = vtp_solver_attach_object(d->s, boundary_pos, nb, nullptr, bj.c_str()))) return rc;
@@ -367,8 +415,8 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
                                                             d->status);
             CU(cudaGetLastError());
         }
-        // Boundary rows' packed gather rows ({x, V_b}, {x, v*}) never change: pack them once.
-        vtp::dfsph_solve_pack(d->st, s->dfsph_args());
+        // DFSPH: the boundary rows' packed gather rows ({x, V_b}, {x, v*}) never change: pack them once.
+        if (!pbf) vtp::dfsph_solve_pack(d->st, s->dfsph_args());
         CU(cudaGetLastError());
         CU(cudaStreamSynchronize(d->st));
         *out = d.release();
@@ -406,9 +454,10 @@ int vtp_domain_load(vtp_domain *d, uint32_t n_own, uint32_t n_ghost, const float
     d->n_own = n_own;
     d->n_act = (uint32_t)n;
     if (n)
-        k_dd_load<<<nblk((uint32_t)n, 256), 256, 0, d->st>>>((uint32_t)n, d_pos, d_vel, d_ids, d_obj, s->vol0,
-                                                           s->pos.c(), s->vel.c(), s->vadv.c(), s->orig.c(),
-                                                           d->slot.c(), d->objf.c());
+        k_dd_load<<<nblk((uint32_t)n, 256), 256, 0, d->st>>>(
+            (uint32_t)n, d_pos, d_vel, d_ids, d_obj, d->type == VTP_SOLVER_PBF ? s->rho_f * s->vol0 : s->vol0,
+            s->pos.c(), s->vel.c(), d->type == VTP_SOLVER_PBF ? nullptr : s->vadv.c(), s->orig.c(), d->slot.c(),
+            d->objf.c());
     CU(cudaGetLastError());
     d->loaded = true;
     d->prepared = false;
@@ -420,38 +469,71 @@ int vtp_domain_prepare(vtp_domain *d) {
     if (!d->loaded) return fail(VTP_ERR_STATE, "vtp_domain_prepare before vtp_domain_load");
     vtp_solver *s = d->s;
     const vtp::NvtxRange r("vtp domain neighbour search");
-    // The UGNS sort of the loaded rows (v*, load slot and object carried along), the lists,
-    // then compression ratio and alpha.
+    // The UGNS sort of the loaded rows (load slot and object carried along; DFSPH: v* too;
+    // PBF: the external force applied on the way, PBFCudaImpl.cu:146-157), the lists, then
+    // (DFSPH) compression ratio and alpha.
+    const bool pbf = d->type == VTP_SOLVER_PBF;
     vtp::Carry carry{};
-    carry.nf4 = 1;
-    carry.src4[0] = s->vadv.c();
-    carry.dst4[0] = s->vadv.n();
+    if (!pbf) {
+        carry.nf4 = 1;
+        carry.src4[0] = s->vadv.c();
+        carry.dst4[0] = s->vadv.n();
+    }
     carry.nf1 = 2;
     carry.src1[0] = d->slot.c();
     carry.dst1[0] = d->slot.n();
     carry.src1[1] = d->objf.c();
     carry.dst1[1] = d->objf.n();
     vtp::ugns_sort(d->st, s->scn(), s->nbuckets, 0, d->n_act, s->pos.c(), s->pos.n(), s->vel.c(), s->vel.n(),
-                   s->orig.c(), s->orig.n(), carry, 0.f, s->u, s->u.fstart);
-    s->pos.swap(); s->vel.swap(); s->orig.swap(); s->vadv.swap();
+                   s->orig.c(), s->orig.n(), carry, pbf ? s->dt : 0.f, s->u, s->u.fstart);
+    s->pos.swap(); s->vel.swap(); s->orig.swap();
+    if (!pbf) s->vadv.swap();
     d->slot.swap(); d->objf.swap();
     const vtp::Layout L = d->layout();
     vtp::ugns_build_lists(d->st, s->scn(), L, 0, d->n_act, s->pos.c(), s->orig.c(), s->u, s->u.nbr, s->u.ncnt,
                           s->d_status, s->d_overflow, s->block);
     if (d->n_act) {
         k_dd_row_of_slot<<<nblk(d->n_act, 256), 256, 0, d->st>>>(d->n_act, d->slot.c(), d->row_of_slot, d->status);
-        k_dd_tiles<<<nblk(nblk(d->n_act, s->block), 256), 256, 0, d->st>>>(s->d_tiles, d->n_act, (uint32_t)s->block);
+        if (!pbf)
+            k_dd_tiles<<<nblk(nblk(d->n_act, s->block), 256), 256, 0, d->st>>>(s->d_tiles, d->n_act,
+                                                                             (uint32_t)s->block);
     }
     d->which = 0;
-    vtp::dfsph_ratio_alpha(d->st, d->args(), s->block);
+    if (!pbf) vtp::dfsph_ratio_alpha(d->st, d->args(), s->block);
     CU(cudaGetLastError());
     d->prepared = true;
     return VTP_OK;
 }
 
+int vtp_domain_pbf_lambda(vtp_domain *d) {
+    int rc;
+    if ((rc = need_type(d, VTP_SOLVER_PBF))) return rc;
+    vtp::pbf_lambda(d->st, d->pbf(), d->s->block);
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+int vtp_domain_pbf_dx(vtp_domain *d) {
+    int rc;
+    if ((rc = need_type(d, VTP_SOLVER_PBF))) return rc;
+    vtp::pbf_dx(d->st, d->pbf(), d->s->block);   // positions into the second buffer, velocities in place
+    d->s->pos.swap();
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+int vtp_domain_pbf_xsph(vtp_domain *d) {
+    int rc;
+    if ((rc = need_type(d, VTP_SOLVER_PBF))) return rc;
+    vtp::pbf_xsph(d->st, d->pbf(), d->s->block);
+    d->s->pos.swap(); d->s->vel.swap();
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
 int vtp_domain_solve_begin(vtp_domain *d, int which) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     if (which != 0 && which != 1) return fail(VTP_ERR_ARG, "which: 0 divergence, 1 density");
     d->which = which;
     vtp_solver *s = d->s;
@@ -465,7 +547,7 @@ int vtp_domain_solve_begin(vtp_domain *d, int which) {
 
 int vtp_domain_solve_a(vtp_domain *d, double *d_sums) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     if (!d_sums) return fail(VTP_ERR_ARG, "null sums");
     const vtp::DfsphArgs a = d->args();
     vtp::dfsph_solve_a(d->st, a, d->s->block);
@@ -478,7 +560,7 @@ int vtp_domain_solve_a(vtp_domain *d, double *d_sums) {
 
 int vtp_domain_solve_b(vtp_domain *d) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     vtp::dfsph_solve_b(d->st, d->args(), d->s->block);
     CU(cudaGetLastError());
     return VTP_OK;
@@ -486,7 +568,7 @@ int vtp_domain_solve_b(vtp_domain *d) {
 
 int vtp_domain_forces(vtp_domain *d) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     vtp_solver *s = d->s;
     const vtp::DfsphArgs a = d->args();
     vtp::dfsph_pressure_pack(d->st, a);
@@ -502,7 +584,7 @@ int vtp_domain_forces(vtp_domain *d) {
 
 int vtp_domain_tension(vtp_domain *d) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     vtp_solver *s = d->s;
     if (s->gamma == 0.f) return fail(VTP_ERR_STATE, "surface tension pass with surfaceTensionCoefficient 0");
     vtp::dfsph_tension(d->st, d->args(), s->block);
@@ -513,7 +595,7 @@ int vtp_domain_tension(vtp_domain *d) {
 
 int vtp_domain_finalize(vtp_domain *d) {
     int rc;
-    if ((rc = need_prepared(d))) return rc;
+    if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     vtp::dfsph_finalize(d->st, d->args());
     CU(cudaGetLastError());
     return VTP_OK;
@@ -524,8 +606,21 @@ int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t 
     if ((rc = need_prepared(d))) return rc;
     if (count == 0) return VTP_OK;
     if (!d_slots || !d_out) return fail(VTP_ERR_ARG, "null array");
-    const vtp::DfsphArgs a = d->args();
     uint32_t *status = d->status;
+    if (d->type == VTP_SOLVER_PBF) {
+        vtp_solver *s = d->s;
+        if (field == VTP_DOMAIN_LAMBDA)
+            k_dd_pack1<<<nblk(count, 256), 256, 0, d->st>>>(count, d->n_act, d_slots, d->row_of_slot, s->lambda,
+                                                           d_out, status);
+        else if (field == VTP_DOMAIN_POSVEL)
+            k_dd_pack_posvel<<<nblk(count, 256), 256, 0, d->st>>>(count, d->n_act, d_slots, d->row_of_slot,
+                                                                 s->pos.c(), s->vel.c(), (float4 *)d_out, status);
+        else
+            return fail(VTP_ERR_ARG, "not a PBF domain field");
+        CU(cudaGetLastError());
+        return VTP_OK;
+    }
+    const vtp::DfsphArgs a = d->args();
     switch (field) {
         case VTP_DOMAIN_KAPPA:
             k_dd_pack1<<<nblk(count, 256), 256, 0, d->st>>>(count, d->n_act, d_slots, d->row_of_slot, a.kappa, d_out,
@@ -550,13 +645,21 @@ int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t 
 int vtp_domain_unpack(vtp_domain *d, int field, uint32_t first_slot, uint32_t count, const float *d_in) {
     int rc;
     if ((rc = need_prepared(d))) return rc;
-    if (field < VTP_DOMAIN_KAPPA || field > VTP_DOMAIN_NORMAL) return fail(VTP_ERR_ARG, "unknown domain field");
+    const bool pbf = d->type == VTP_SOLVER_PBF;
+    if (pbf ? (field != VTP_DOMAIN_LAMBDA && field != VTP_DOMAIN_POSVEL)
+            : (field < VTP_DOMAIN_KAPPA || field > VTP_DOMAIN_NORMAL))
+        return fail(VTP_ERR_ARG, "not a domain field of this solver");
     if (count == 0) return VTP_OK;
     if (!d_in) return fail(VTP_ERR_ARG, "null array");
     if ((uint64_t)first_slot + count > d->n_act || first_slot < d->n_own)
         return fail(VTP_ERR_BOUNDS, "unpack outside the ghost rows");
-    k_dd_unpack<<<nblk(count, 256), 256, 0, d->st>>>(field, count, first_slot, d->n_act, d->row_of_slot, d_in,
-                                                    (const float4 *)d_in, d->args(), d->status);
+    if (pbf)
+        k_dd_unpack_pbf<<<nblk(count, 256), 256, 0, d->st>>>(field, count, first_slot, d->n_act, d->row_of_slot, d_in,
+                                                            (const float4 *)d_in, d->s->lambda, d->s->pos.c(),
+                                                            d->s->vel.c(), d->status);
+    else
+        k_dd_unpack<<<nblk(count, 256), 256, 0, d->st>>>(field, count, first_slot, d->n_act, d->row_of_slot, d_in,
+                                                        (const float4 *)d_in, d->args(), d->status);
     CU(cudaGetLastError());
     return VTP_OK;
 }

@@ -93,6 +93,9 @@ SIGNATURES = {
     "vtp_domain_forces": (C.c_int, [_P]),
     "vtp_domain_tension": (C.c_int, [_P]),
     "vtp_domain_finalize": (C.c_int, [_P]),
+    "vtp_domain_pbf_lambda": (C.c_int, [_P]),
+    "vtp_domain_pbf_dx": (C.c_int, [_P]),
+    "vtp_domain_pbf_xsph": (C.c_int, [_P]),
     "vtp_domain_pack": (C.c_int, [_P, C.c_int, _P, C.c_uint32, _P]),
     "vtp_domain_unpack": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_uint32, _P]),
     "vtp_domain_read": (C.c_int, [_P, _P, _P]),

@@ -1,7 +1,7 @@
-"""Single-scene domain decomposition of DFSPH: one slab of the scene per rank.
+"""Single-scene domain decomposition of DFSPH and PBF: one slab of the scene per rank.
 
 The reference runs a scene on one device (SolverManager.cpp:11-17).  Here a
-DFSPH scene too large for one GPU, or wanted faster than one GPU runs it, is
+DFSPH or PBF scene too large for one GPU, or wanted faster than one GPU runs it, is
 split along one axis into slabs, one per rank, by fluid-particle quantiles at
 the start.  Rank k owns the fluid particles whose coordinate on that axis
 lies in [bounds[k], bounds[k+1]) and holds
@@ -30,6 +30,13 @@ the rank's worker (``vtp_domain_*`` in include/vtp.h) with exchanges between:
    0), then the ghosts' velocities;
 6. finalize (positions advanced) and the owned rows read back.
 
+A PBF substep (PBFSolver::tick, PBFSolver.cpp:326-376) has no residual: after
+migration and the ghosts (chosen with twice the largest move under the
+external force added to the ghost width, since PBF builds its lists on the
+positions after that force), every constraint iteration runs the lambda pass,
+sends lambda to the ghosts, runs the correction pass and sends the corrected
+positions and velocities to the ghosts; XSPH follows.
+
 Rows keep their scene-wide attach ids and a rank holds every particle within
 h of its owned rows, so an owned row's neighbour list, in the reference's
 order, is the one a solver holding the whole scene builds, and every value it
@@ -56,7 +63,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-FIELD_KAPPA, FIELD_VADV, FIELD_VEL, FIELD_NORMAL = 0, 1, 2, 3
+FIELD_KAPPA, FIELD_VADV, FIELD_VEL, FIELD_NORMAL = 0, 1, 2, 3   # DFSPH exchanges
+FIELD_LAMBDA, FIELD_POSVEL = 4, 5                               # PBF exchanges
 GHOST_MARGIN = 1.01   # ghost width / h: covers the FP32 rounding of the membership test r <= h
 
 
@@ -64,7 +72,9 @@ GHOST_MARGIN = 1.01   # ghost width / h: covers the FP32 rounding of the members
 
 @dataclass
 class SceneArrays:
-    """A DFSPH scene in the attach order of a solver holding all of it (ids = attach index)."""
+    """A DFSPH or PBF scene in the attach order of a solver holding all of it (ids = attach
+    index)."""
+    solver: str                # "DFSPH" | "PBF"
     config: dict
     fluid_pos: np.ndarray      # (nf, 3) float32
     fluid_vel: np.ndarray      # (nf, 3) float32
@@ -78,9 +88,9 @@ class SceneArrays:
 
 
 def scene_arrays(scene) -> SceneArrays:
-    """Split a ``vtp.scenes.Scene`` (DFSPH) into fluid and boundary arrays with attach ids."""
-    if scene.solver != "DFSPH":
-        raise ValueError("domain decomposition runs DFSPH scenes")
+    """Split a ``vtp.scenes.Scene`` (DFSPH or PBF) into fluid and boundary arrays with attach ids."""
+    if scene.solver not in ("DFSPH", "PBF"):
+        raise ValueError("domain decomposition runs DFSPH and PBF scenes")
     fp, fv, fg, fo, bp, bg, counts = [], [], [], [], [], [], []
     start = 0
     for o in scene.objects:
@@ -105,9 +115,9 @@ def scene_arrays(scene) -> SceneArrays:
         raise ValueError("domain decomposition needs fluid ids all below or all above the boundary ids")
     if start >= 2 ** 31:
         raise ValueError("more than 2^31 particles")
-    req = scene.config["DFSPH"]["Required"]
+    req = scene.config[scene.solver]["Required"]
     h = float(np.float32(np.float32(req["particleRadius"]) * np.float32(4)))
-    return SceneArrays(scene.config, cat(fp, (0, 3), np.float32), cat(fv, (0, 3), np.float32), fgid,
+    return SceneArrays(scene.solver, scene.config, cat(fp, (0, 3), np.float32), cat(fv, (0, 3), np.float32), fgid,
                        cat(fo, (0,), np.int32), np.asarray(counts, np.int64), cat(bp, (0, 3), np.float32), bgid,
                        bool(bgid.size and bgid.max() < fgid.min()), h)
 
@@ -145,7 +155,7 @@ def plan_slabs(arrays: SceneArrays, ranks: int, axis: int | None = None) -> Slab
     if ranks < 1:
         raise ValueError("ranks must be >= 1")
     if axis is None:
-        size = arrays.config["DFSPH"]["Required"]["simSpaceSize"]
+        size = arrays.config[arrays.solver]["Required"]["simSpaceSize"]
         axis = int(np.argmax(np.asarray(size, np.float64)))
     x = np.sort(arrays.fluid_pos[:, axis])
     n = x.size
@@ -185,6 +195,10 @@ class TorchComm:
 
     def allreduce_sum(self, t):
         self.dist.all_reduce(t)
+        return t
+
+    def allreduce_max(self, t):
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return t
 
 
@@ -239,6 +253,27 @@ class LoopbackComm:
         self.hub.barrier.wait()
         return out
 
+    def allreduce_max(self, t):
+        if self.size == 1:
+            return t
+        box, me = self.hub.box, self.rank
+        mine = t.clone()
+        self._settle(mine)
+        box[("m", me)] = mine
+        self.hub.barrier.wait()
+        total = box[("m", 0)].clone()
+        for q in range(1, self.size):
+            total = self._max(total, box[("m", q)])
+        t.copy_(total)
+        self._settle(t)
+        self.hub.barrier.wait()
+        return t
+
+    @staticmethod
+    def _max(a, b):
+        import torch
+        return torch.maximum(a, b)
+
     def allreduce_sum(self, t):
         if self.size == 1:   # nothing to add: no barrier, no stream synchronisation
             return t
@@ -259,7 +294,7 @@ class LoopbackComm:
 # ----------------------------------------------------------------------------- library stages
 
 class LibraryStages:
-    """One rank's DFSPH stages on the sm_100a library; state in CUDA tensors (FP32)."""
+    """One rank's DFSPH or PBF stages on the sm_100a library; state in CUDA tensors (FP32)."""
 
     def __init__(self, config: dict, fluid_pos0: np.ndarray, bnd_pos: np.ndarray, bnd_gid: np.ndarray,
                  boundary_first: bool, capacity: int, n_objects: int):
@@ -271,6 +306,7 @@ class LibraryStages:
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.dtype = torch.float32
         self.nobj = int(n_objects)
+        self.pbf = "PBF" in config
         fp = np.ascontiguousarray(fluid_pos0, np.float32)
         bp = np.ascontiguousarray(bnd_pos, np.float32)
         bg = np.ascontiguousarray(bnd_gid, np.uint32)
@@ -286,7 +322,6 @@ class LibraryStages:
         handle = torch.cuda.current_stream().cuda_stream or 1
         check(self.L.vtp_domain_set_stream(h, C.c_void_p(handle)), "vtp_domain_set_stream")
         self.n_own = 0
-        self.gamma = float(np.float32(config["DFSPH"]["Required"]["surfaceTensionCoefficient"]))
         self.launches = 0   # library kernels launched by the stage calls so far
 
     def close(self):
@@ -301,7 +336,7 @@ class LibraryStages:
             pass
 
     def empty(self, field: int, count: int):
-        shape = (count,) if field == FIELD_KAPPA else (count, 4)
+        shape = {FIELD_KAPPA: (count,), FIELD_LAMBDA: (count,), FIELD_POSVEL: (count, 8)}.get(field, (count, 4))
         return self.torch.empty(shape, dtype=self.torch.float32, device=self.device)
 
     def load(self, n_own, pos, vel, gid, obj):
@@ -322,7 +357,20 @@ class LibraryStages:
 
     def prepare(self):
         self.check(self.L.vtp_domain_prepare(self.h), "vtp_domain_prepare")
-        self.launches += 10
+        # hash, 3 scan kernels, scatter, rank/reorder, lists, slot map (+ DFSPH: tiles, ratio/alpha)
+        self.launches += 8 if self.pbf else 10
+
+    def pbf_lambda(self):
+        self.check(self.L.vtp_domain_pbf_lambda(self.h), "vtp_domain_pbf_lambda")
+        self.launches += 1
+
+    def pbf_dx(self):
+        self.check(self.L.vtp_domain_pbf_dx(self.h), "vtp_domain_pbf_dx")
+        self.launches += 1
+
+    def pbf_xsph(self):
+        self.check(self.L.vtp_domain_pbf_xsph(self.h), "vtp_domain_pbf_xsph")
+        self.launches += 1
 
     def solve_begin(self, which: int):
         self.check(self.L.vtp_domain_solve_begin(self.h, int(which)), "vtp_domain_solve_begin")
@@ -376,7 +424,7 @@ class LibraryStages:
 # ----------------------------------------------------------------------------- one rank
 
 class DomainRank:
-    """One rank of a decomposed DFSPH scene: owns its slab's fluid particles and drives its
+    """One rank of a decomposed DFSPH or PBF scene: owns its slab's fluid particles and drives its
     worker's stages with the exchanges of the module docstring."""
 
     def __init__(self, arrays: SceneArrays, plan: SlabPlan, comm, make_stages=LibraryStages,
@@ -385,28 +433,42 @@ class DomainRank:
         self.torch = torch
         self.speculate = speculate
         self.a = arrays
+        self.kind = arrays.solver
         self.plan = plan
         self.comm = comm
         self.rank = comm.rank
         if plan.ranks != comm.size:
             raise ValueError(f"plan has {plan.ranks} slabs for {comm.size} ranks")
-        req = arrays.config["DFSPH"]["Required"]
+        req = arrays.config[self.kind]["Required"]
+        opt = arrays.config[self.kind].get("Optional", {})
         ext = arrays.config.get("B200", {})
-        if float(ext.get("cfl", 0.0)) > 0.0:
-            raise ValueError("a decomposed scene takes the fixed timeStep (cfl 0)")
-        self.thr = (float(np.float32(req["divFreeThreshold"])), float(np.float32(req["incompThreshold"])))
-        self.force = (int(ext.get("forceDivIterations", 0)), int(ext.get("forceIncompIterations", 0)))
-        self.force_seq = [tuple(int(v) for v in p) for p in ext.get("forceIterationsPerTick", [])]
-        self.gamma = float(np.float32(req["surfaceTensionCoefficient"]))
+        self.dt = float(np.float32(req["timeStep"]))
+        if self.kind == "DFSPH":
+            if float(ext.get("cfl", 0.0)) > 0.0:
+                raise ValueError("a decomposed scene takes the fixed timeStep (cfl 0)")
+            self.thr = (float(np.float32(req["divFreeThreshold"])), float(np.float32(req["incompThreshold"])))
+            self.force = (int(ext.get("forceDivIterations", 0)), int(ext.get("forceIncompIterations", 0)))
+            self.force_seq = [tuple(int(v) for v in p) for p in ext.get("forceIterationsPerTick", [])]
+            self.gamma = float(np.float32(req["surfaceTensionCoefficient"]))
+            reach = 0.0
+        else:
+            # PBF builds its lists on the positions after the external force, x + dt (v + g dt):
+            # ghosts are chosen on the loaded positions with twice the largest such move added
+            # (`_reach`), within a fixed half-h allowance the boundary band is widened by.
+            self.iterations = int(req["iterationNum"])
+            g = opt.get("gravity", [0.0, -9.8, 0.0]) if opt.get("enable", False) else [0.0, -9.8, 0.0]
+            self.g_norm = float(np.linalg.norm(np.asarray(g, np.float64)))
+            reach = 0.5 * arrays.h
+        self.reach_limit = reach
         self.inv_count = [1.0 / float(c) for c in arrays.obj_count]
         self.max_iters = 101
         ax, w = plan.axis, plan.ghost
         lo, hi = plan.slab(self.rank)
         fx = arrays.fluid_pos[:, ax]
         own = plan.owner(fx) == self.rank
-        near = (fx >= lo - w) & (fx < hi + w)
+        near = (fx >= lo - w - 2 * reach) & (fx < hi + w + 2 * reach)
         bx = arrays.bnd_pos[:, ax]
-        band = (bx >= lo - 2 * w) & (bx < hi + 2 * w)
+        band = (bx >= lo - 2 * w - reach) & (bx < hi + 2 * w + reach)
         n0 = int(near.sum())
         cap = min(max(int(capacity_factor * n0), n0 + 4096), 1 << 24)
         self.stages = make_stages(arrays.config, arrays.fluid_pos[near], arrays.bnd_pos[band], arrays.bnd_gid[band],
@@ -417,7 +479,7 @@ class DomainRank:
         self.gid = torch.as_tensor(arrays.fluid_gid[own], device=dev)
         self.obj = torch.as_tensor(arrays.fluid_obj[own], device=dev)
         self.substeps = 0
-        self.iters = []            # (divergence, density) iterations per substep
+        self.iters = []            # (divergence, density) iterations per substep (PBF: (iterations, 0))
         self.residuals = []
         self.crashed = False
 
@@ -455,13 +517,26 @@ class DomainRank:
         self.gid = t.cat([self.gid[keep]] + gid_in)
         self.obj = t.cat([self.obj[keep]] + obj_in)
 
-    def _ghosts(self):
+    def _reach(self) -> float:
+        """PBF: the largest distance a particle moves under the external force this substep,
+        dt (max |v| + |g| dt) over all ranks (one max all-reduce), with a margin."""
+        t = self.torch
+        v = self.vel.norm(dim=1).max() if self.vel.shape[0] else t.zeros((), dtype=self.vel.dtype,
+                                                                           device=self.vel.device)
+        vmax = float(self.comm.allreduce_max(v.reshape(1).to(t.float64)).cpu().numpy()[0])
+        d = 1.01 * self.dt * (vmax + self.g_norm * self.dt) + 1e-6 * self.a.h
+        if d > self.reach_limit:
+            raise RuntimeError(f"a particle moves {d:.3g} under the external force in one substep, more than the "
+                               f"decomposition's allowance {self.reach_limit:.3g} (h / 2)")
+        return d
+
+    def _ghosts(self, reach: float = 0.0):
         t = self.torch
         if self.comm.size == 1:
             self.send_slots, self.recv_count, self.ghost_first = {}, [0], {}
             return self.pos, self.vel, self.gid, self.obj
         x = self.pos[:, self.plan.axis]
-        w = self.plan.ghost
+        w = self.plan.ghost + 2 * reach
         self.send_slots = {}
         for q in self._peers():
             lo, hi = self.plan.slab(q)
@@ -553,6 +628,8 @@ class DomainRank:
             self.substep()
 
     def substep(self):
+        if self.kind == "PBF":
+            return self._pbf_substep()
         if self.crashed:
             raise RuntimeError("DFSPHSolver is crashed.")
         st = self.stages
@@ -572,6 +649,28 @@ class DomainRank:
         self.pos, self.vel = st.read()
         self.iters.append((div[0], inc[0]))
         self.residuals.append((div[1], inc[1]))
+        self.substeps += 1
+
+    def _pbf_substep(self):
+        """PBFSolver::tick (PBFSolver.cpp:326-376) over the rank's rows: the external force in
+        the sort, `iterationNum` constraint iterations (lambda to the ghosts after each lambda
+        pass, positions and velocities after each correction pass), XSPH."""
+        st = self.stages
+        if self.substeps > 0:
+            self._migrate()
+        reach = self._reach() if self.comm.size > 1 else 0.0
+        pos, vel, gid, obj = self._ghosts(reach)
+        st.load(self.pos.shape[0], pos, vel, gid, obj)
+        st.prepare()
+        for _ in range(self.iterations):
+            st.pbf_lambda()
+            self._exchange(FIELD_LAMBDA)
+            st.pbf_dx()
+            self._exchange(FIELD_POSVEL)
+        st.pbf_xsph()
+        self.pos, self.vel = st.read()
+        self.iters.append((self.iterations, 0))
+        self.residuals.append((0.0, 0.0))
         self.substeps += 1
 
     def timed_steps(self, n: int) -> float:
