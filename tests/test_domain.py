@@ -145,6 +145,26 @@ def test_decomposed_pbf_oracle_follows_a_collapsing_column(oracle_lib, ranks):
     assert out["owned"] != start.tolist()
 
 
+@pytest.mark.parametrize("kind", ["DFSPH", "PBF"])
+def test_decomposed_oracle_with_an_empty_slab(oracle_lib, kind):
+    """A slab that holds no fluid (nor boundary) and one that holds no owned fluid but ghosts:
+    every stage runs on zero rows and the others are unaffected."""
+    if kind == "DFSPH":
+        sc, stages = scenes.dam_break("DFSPH", 3000, seed=11), oracle_lib.DfsphDomainStages
+    else:
+        sc, stages = scenes.dam_break("PBF", 3000, seed=21, spacing=0.1), oracle_lib.PbfDomainStages
+    a = domain.scene_arrays(sc)
+    ax = domain.plan_slabs(a, 2).axis
+    lo = float(a.fluid_pos[:, ax].min())
+    h = a.h
+    # slab 0 far below everything, slab 1 a sliver of ghosts only, slab 2 the rest
+    plan = domain.SlabPlan(ax, (lo - 50 * h, lo - 0.5 * h), domain.GHOST_MARGIN * h)
+    pos, vel = _whole_oracle_fields(sc, 3)
+    out = domain.run_local(sc, 3, 3, make_stages=stages, plan=plan)
+    assert out["owned"][:2] == [0, 0]
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -268,4 +288,19 @@ def test_library_pbf_domains_equal_whole_scene_library(vtp_gpu, ranks):
     sc = scenes.dam_break("PBF", 8000, seed=21, spacing=0.1)
     pos, vel, _ = _whole_library(sc, 40, {})
     out = domain.run_local(sc, ranks, 40)
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["DFSPH", "PBF"])
+def test_library_domains_with_an_empty_slab(vtp_gpu, kind):
+    sc = scenes.dam_break("DFSPH", 8000, seed=22) if kind == "DFSPH" else \
+        scenes.dam_break("PBF", 8000, seed=21, spacing=0.1)
+    a = domain.scene_arrays(sc)
+    ax = domain.plan_slabs(a, 2).axis
+    lo = float(a.fluid_pos[:, ax].min())
+    plan = domain.SlabPlan(ax, (lo - 50 * a.h, lo - 0.5 * a.h), domain.GHOST_MARGIN * a.h)
+    pos, vel, _ = _whole_library(sc, 3, FORCED if kind == "DFSPH" else {})
+    out = domain.run_local(sc, 3, 3, plan=plan, extra=FORCED if kind == "DFSPH" else None)
+    assert out["owned"][:2] == [0, 0]
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)

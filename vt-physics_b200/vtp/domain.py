@@ -752,14 +752,16 @@ def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibrarySt
 
 
 def run_local(scene, ranks: int, steps: int, make_stages=LibraryStages, axis: int | None = None,
-              capacity_factor: float = 2.0, extra: dict | None = None, speculate: bool = True) -> dict:
+              capacity_factor: float = 2.0, extra: dict | None = None, speculate: bool = True,
+              plan: SlabPlan | None = None) -> dict:
     """Run `scene` decomposed into `ranks` slabs inside this process (``local_ranks``) for
-    `steps` substeps and merge the ranks' owned particles into the scene's fluid order."""
+    `steps` substeps and merge the ranks' owned particles into the scene's fluid order.
+    `plan` replaces the quantile slabs of ``plan_slabs``."""
     arrays = scene_arrays(scene)
     if extra:
         arrays.config = json.loads(json.dumps(arrays.config))
         arrays.config["B200"] = dict(extra)
-    plan = plan_slabs(arrays, ranks, axis)
+    plan = plan or plan_slabs(arrays, ranks, axis)
 
     def body(rank):
         rank.step(steps)
