@@ -304,3 +304,15 @@ def test_library_domains_with_an_empty_slab(vtp_gpu, kind):
     out = domain.run_local(sc, 3, 3, plan=plan, extra=FORCED if kind == "DFSPH" else None)
     assert out["owned"][:2] == [0, 0]
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+def test_dfsph_1m_in_eight_slabs_over_25_free_substeps(vtp_gpu):
+    """The benchmark scene from rest, the residual deciding (up to 60 iterations a solve in
+    the first substeps): eight slabs take the whole scene's iteration counts and end on its
+    trajectory bit for bit."""
+    sc = scenes.dfsph_1m()
+    pos, vel, iters = _whole_library(sc, 25, {})
+    out = domain.run_local(sc, 8, 25)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
