@@ -242,20 +242,24 @@ def _whole_library(sc, steps, extra):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("ranks", [1, 2, 4])
-def test_library_domains_equal_whole_scene_library(vtp_gpu, ranks):
+@pytest.mark.parametrize("halo", ["peer", "exchange"])
+def test_library_domains_equal_whole_scene_library(vtp_gpu, ranks, halo):
+    """Ghost values by peer stores (the owners' stage kernels write into the other slabs'
+    ghost rows) and by pack / exchange / unpack give the whole-scene run."""
     sc = scenes.dam_break("DFSPH", 8000, seed=22)
     for extra in (FORCED, {}):
         pos, vel, iters = _whole_library(sc, 5, extra)
-        out = domain.run_local(sc, ranks, 5, extra=extra)
+        out = domain.run_local(sc, ranks, 5, extra=extra, halo=halo)
         assert out["iters"] == iters
         assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
 
 
 @pytest.mark.gpu
-def test_library_domains_with_migration_tension_and_two_objects(vtp_gpu):
+@pytest.mark.parametrize("halo", ["peer", "exchange"])
+def test_library_domains_with_migration_tension_and_two_objects(vtp_gpu, halo):
     sc = scenes.colliding_blocks()
     pos, vel, iters = _whole_library(sc, 25, {})
-    out = domain.run_local(sc, 4, 25)
+    out = domain.run_local(sc, 4, 25, halo=halo)
     assert out["iters"] == iters
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
 

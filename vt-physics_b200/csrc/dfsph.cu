@@ -71,6 +71,21 @@ __device__ __forceinline__ StepDt step_dt(const DfsphArgs &a) {
     return StepDt{dt, inv, inv * inv};
 }
 
+// Peer-store halos (HaloPush in dfsph.h): ghost rows write nothing; an owned row hands each
+// value it writes to `f(peer rows, the peer's row)` for every peer it is a ghost on.
+__device__ __forceinline__ bool halo_ghost(const DfsphArgs &a, uint32_t r) { return a.halo && a.halo->ghost[r]; }
+
+template <class F>
+__device__ __forceinline__ void halo_each(const DfsphArgs &a, uint32_t r, F f) {
+    if (!a.halo) return;
+    const uint32_t n = min(a.halo->ntarget[r], (uint32_t)kMaxHaloTargets);
+    for (uint32_t e = 0; e < n; ++e) {
+        const uint2 t = a.halo->target[(size_t)r * kMaxHaloTargets + e];
+        f(a.halo->peer[t.x], t.y);
+    }
+    if (n) __threadfence_system();   // the stores to other GPUs ordered before what follows
+}
+
 __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_t *__restrict__ bncnt,
                                                       const uint32_t *__restrict__ bnbr,
                                                       float *__restrict__ rest_density_b) {
@@ -135,7 +150,7 @@ struct PN {
 template <int U>
 __global__ void __launch_bounds__(256) k_ratio_alpha(DfsphArgs a) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;
     const float4 p = a.pos[r];
     const uint32_t n = a.ncnt[r];
     RatioAlpha ra;
@@ -162,7 +177,7 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
         const uint32_t r = tile.x + threadIdx.x;
         double contrib = 0.0;
         int obj = 0;
-        if (threadIdx.x < tile.y) {
+        if (threadIdx.x < tile.y && !halo_ghost(a, r)) {
             const float4 p = a.pos[r];
             const float4 vi = a.vadv[r];
             const uint32_t n = a.ncnt[r];
@@ -180,7 +195,12 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
             a.delta[r] = d;
             const float kap = d / a.alpha[r] * T.inv_dt2 / p.w;
             a.kappa[r] = kap;
-            a.pk[r] = make_float4(p.x, p.y, p.z, kap);
+            const float4 pkr = make_float4(p.x, p.y, p.z, kap);
+            a.pk[r] = pkr;
+            halo_each(a, r, [&](const PeerRows &P, uint32_t q) {
+                P.kappa[q] = kap;
+                P.pk[q] = pkr;
+            });
             contrib = (double)d;
             if (MULTI) obj = (int)a.obj_of[a.orig[r]] - (int)a.scene_tiles[tile.z].obj0;
         }
@@ -370,6 +390,7 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
         const uint4 tile = a.tiles[t];
         if (a.state[tile.z].stopped || threadIdx.x >= tile.y) continue;
         const uint32_t r = tile.x + threadIdx.x;
+        if (halo_ghost(a, r)) continue;
         const float4 p = a.pos[r];
         float4 v = a.vadv[r];
         const float ki = a.kappa[r];
@@ -392,6 +413,10 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
                     });
         a.vadv[r] = v;
         a.pva[2 * (size_t)r + 1] = v;
+        halo_each(a, r, [&](const PeerRows &P, uint32_t q) {
+            P.vadv[a.halo_vadv][q] = v;
+            P.pva[2 * (size_t)q + 1] = v;
+        });
     }
 }
 
@@ -495,7 +520,7 @@ template <bool TENSION_SPLIT, int U>
 __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;
     const float4 p = a.pos[r];
     const float4 vi = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
     const uint32_t n = a.ncnt[r];
@@ -531,7 +556,9 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     const float accx = sg.grav_x + ax, accy = sg.grav_y + ay, accz = sg.grav_z + az;
     if (TENSION_SPLIT) {
         a.acc_tmp[r] = make_float4(accx, accy, accz, 0.f);
-        a.normal[r] = make_float4(nx, ny, nz, 0.f);
+        const float4 nrm = make_float4(nx, ny, nz, 0.f);
+        a.normal[r] = nrm;
+        halo_each(a, r, [&](const PeerRows &P, uint32_t q) { P.normal[q] = nrm; });
         return;
     }
     float4 o = vi;
@@ -540,13 +567,17 @@ __global__ void __launch_bounds__(256) k_viscosity(DfsphArgs a) {
     o.z = __fmaf_rn(accz, T.dt, vi.z);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
+    halo_each(a, r, [&](const PeerRows &P, uint32_t q) {
+        P.vel[a.halo_vel ^ 1][q] = o;
+        P.vadv[a.halo_vadv ^ 1][q] = o;
+    });
 }
 
 template <int U>
 __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
     const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;
     const float4 p = a.pos[r];
     const float4 vi = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
     const float4 ni = a.normal[r];
@@ -578,13 +609,17 @@ __global__ void __launch_bounds__(256) k_tension(DfsphArgs a) {
     o.z = __fmaf_rn(acc.z + tz, T.dt, vi.z);
     a.vel_alt[r] = o;
     a.vadv_alt[r] = o;
+    halo_each(a, r, [&](const PeerRows &P, uint32_t q) {
+        P.vel[a.halo_vel ^ 1][q] = o;
+        P.vadv[a.halo_vadv ^ 1][q] = o;
+    });
 }
 
 __global__ void __launch_bounds__(256) k_finalize(DfsphArgs a) {
     const StepDt T = step_dt(a);
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     float v2 = 0.f;
-    if (r < a.nf) {
+    if (r < a.nf && !halo_ghost(a, r)) {
         const float4 v = pressure_applied(a.vel[r], a.vadv[r], T.inv_dt, T.dt);
         a.vel[r] = v;
         a.vadv[r] = v;

@@ -29,6 +29,7 @@
 // each peer's ghosts) travel through the sort so that the exchanges address
 // rows by load slot.
 #include <cmath>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -163,6 +164,12 @@ __global__ void __launch_bounds__(kSumThreads) k_dd_sums_final(int nblocks, int 
     }
 }
 
+__global__ void k_dd_ghost_flags(uint32_t n, uint32_t n_own, const float *__restrict__ slot, uint8_t *__restrict__ ghost) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    ghost[r] = (uint32_t)slot[r] >= n_own ? 1 : 0;
+}
+
 __device__ __forceinline__ bool slot_row(uint32_t s, uint32_t n, const uint32_t *row_of_slot, uint32_t *status,
                                          uint32_t &row) {
     if (s >= n) {
@@ -250,6 +257,35 @@ __global__ void k_dd_unpack(int field, uint32_t count, uint32_t first, uint32_t 
     }
 }
 
+// Targets of peer `peer`: the owned rows at load slots slots[k] are ghosts there at rows
+// dst[k] (below dst_limit, the peer's loaded rows).
+__global__ void k_dd_targets(uint32_t count, uint32_t n, uint32_t n_own, uint32_t peer,
+                             const uint32_t *__restrict__ slots, const uint32_t *__restrict__ dst, uint32_t dst_limit,
+                             const uint32_t *__restrict__ row_of_slot, uint32_t *__restrict__ ntarget,
+                             uint2 *__restrict__ target, uint32_t *status) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r;
+    if (k >= count) return;
+    if (slots[k] >= n_own || dst[k] >= dst_limit || !slot_row(slots[k], n, row_of_slot, status, r)) {
+        atomicOr(status, vtp::ST_BOUNDS);
+        return;
+    }
+    const uint32_t e = atomicAdd(&ntarget[r], 1u);
+    if (e >= (uint32_t)vtp::kMaxHaloTargets) {
+        atomicOr(status, vtp::ST_BOUNDS);
+        return;
+    }
+    target[(size_t)r * vtp::kMaxHaloTargets + e] = make_uint2(peer, dst[k]);
+}
+
+__global__ void k_dd_rows(uint32_t count, uint32_t first, uint32_t n, const uint32_t *__restrict__ row_of_slot,
+                          uint32_t *__restrict__ out, uint32_t *status) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t r;
+    if (k >= count || !slot_row(first + k, n, row_of_slot, status, r)) return;
+    out[k] = r;
+}
+
 __global__ void k_dd_read(uint32_t n_own, uint32_t n, const uint32_t *__restrict__ row_of_slot,
                           const float4 *__restrict__ pos, const float4 *__restrict__ vel, float *__restrict__ pos3,
                           float *__restrict__ vel3, uint32_t *status) {
@@ -289,9 +325,18 @@ struct vtp_domain {
     double *part = nullptr;
     uint32_t *status = nullptr;     // the domain kernels' own status word (ST_BOUNDS: a bad slot)
     uint32_t *h_status = nullptr;   // [2]: the domain word, the wrapped solver's word
+    // Peer-store halos (DFSPH): per sorted row its ghost flag and its targets on peer workers
+    bool halo_on = false;
+    uint8_t *ghost = nullptr;
+    uint32_t *ntarget = nullptr;
+    uint2 *target = nullptr;
+    vtp::HaloPush h_halo{};
+    vtp::HaloPush *d_halo = nullptr;
+    std::vector<void *> ipc_opened;   // peer buffers mapped through CUDA IPC
     std::vector<void *> allocs;
 
     ~vtp_domain() {
+        for (void *p : ipc_opened) cudaIpcCloseMemHandle(p);
         for (void *p : allocs) cudaFree(p);
         if (h_status) cudaFreeHost(h_status);
         if (s) vtp_solver_destroy(s);
@@ -313,6 +358,11 @@ struct vtp_domain {
         a.dtp = nullptr;
         a.vmax_bits = nullptr;
         a.tick = nullptr;
+        if (halo_on) {
+            a.halo = d_halo;
+            a.halo_vadv = s->vadv.cur;
+            a.halo_vel = s->vel.cur;
+        }
         return a;
     }
     vtp::PbfArgs pbf() const {
@@ -406,6 +456,17 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         }
         if ((rc = d->alloc(&d->row_of_slot, capacity))) return rc;
         if ((rc = d->alloc(&d->part, (size_t)kSumBlocks * n_objects))) return rc;
+        if (!pbf) {
+            if ((rc = d->alloc(&d->ghost, capacity))) return rc;
+            if ((rc = d->alloc(&d->ntarget, capacity))) return rc;
+            if ((rc = d->alloc(&d->target, (size_t)capacity * vtp::kMaxHaloTargets))) return rc;
+            if ((rc = d->alloc(&d->d_halo, 1))) return rc;
+            d->h_halo.ghost = d->ghost;
+            d->h_halo.ntarget = d->ntarget;
+            d->h_halo.target = d->target;
+            CU(cudaMemsetAsync(d->ntarget, 0, capacity * sizeof(uint32_t), d->st));
+            CU(cudaMemcpyAsync(d->d_halo, &d->h_halo, sizeof(vtp::HaloPush), cudaMemcpyHostToDevice, d->st));
+        }
         if (nb) {
             uint32_t *gid = nullptr;
             if ((rc = d->alloc(&gid, nb))) return rc;
@@ -494,6 +555,10 @@ int vtp_domain_prepare(vtp_domain *d) {
                           s->d_status, s->d_overflow, s->block);
     if (d->n_act) {
         k_dd_row_of_slot<<<nblk(d->n_act, 256), 256, 0, d->st>>>(d->n_act, d->slot.c(), d->row_of_slot, d->status);
+        if (d->halo_on) {
+            k_dd_ghost_flags<<<nblk(d->n_act, 256), 256, 0, d->st>>>(d->n_act, d->n_own, d->slot.c(), d->ghost);
+            CU(cudaMemsetAsync(d->ntarget, 0, d->n_act * sizeof(uint32_t), d->st));
+        }
         if (!pbf)
             k_dd_tiles<<<nblk(nblk(d->n_act, s->block), 256), 256, 0, d->st>>>(s->d_tiles, d->n_act,
                                                                              (uint32_t)s->block);
@@ -597,6 +662,125 @@ int vtp_domain_finalize(vtp_domain *d) {
     int rc;
     if ((rc = need_type(d, VTP_SOLVER_DFSPH))) return rc;
     vtp::dfsph_finalize(d->st, d->args());
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+namespace {
+
+int need_dfsph_halo(vtp_domain *d) {
+    if (!d) return fail(VTP_ERR_ARG, "null domain");
+    if (d->type != VTP_SOLVER_DFSPH || !d->d_halo) return fail(VTP_ERR_STATE, "peer-store halos are a DFSPH worker's");
+    return VTP_OK;
+}
+
+// The buffers a peer stores ghost values into, in vtp_domain_ipc order.
+void halo_buffers(vtp_domain *d, void *out[VTP_DOMAIN_IPC_BUFFERS]) {
+    vtp_solver *s = d->s;
+    void *b[VTP_DOMAIN_IPC_BUFFERS] = {s->kappa, s->pk, s->pva, s->normal, s->vadv.b[0], s->vadv.b[1],
+                                       s->vel.b[0], s->vel.b[1]};
+    for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) out[k] = b[k];
+}
+
+vtp::PeerRows peer_rows(void *const b[VTP_DOMAIN_IPC_BUFFERS]) {
+    vtp::PeerRows r{};
+    r.kappa = (float *)b[0];
+    r.pk = (float4 *)b[1];
+    r.pva = (float4 *)b[2];
+    r.normal = (float4 *)b[3];
+    r.vadv[0] = (float4 *)b[4];
+    r.vadv[1] = (float4 *)b[5];
+    r.vel[0] = (float4 *)b[6];
+    r.vel[1] = (float4 *)b[7];
+    return r;
+}
+
+}  // namespace
+
+int vtp_domain_export_ipc(vtp_domain *d, vtp_domain_ipc *out) {
+    int rc;
+    if ((rc = need_dfsph_halo(d))) return rc;
+    if (!out) return fail(VTP_ERR_ARG, "null output");
+    void *b[VTP_DOMAIN_IPC_BUFFERS];
+    halo_buffers(d, b);
+    for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) {
+        cudaIpcMemHandle_t h;
+        CU(cudaIpcGetMemHandle(&h, b[k]));
+        static_assert(sizeof(h) <= sizeof(out->handle[0]), "IPC handle size");
+        std::memcpy(out->handle[k], &h, sizeof(h));
+    }
+    out->capacity = d->cap;
+    return VTP_OK;
+}
+
+int vtp_domain_link_peer(vtp_domain *d, int peer, vtp_domain *local_peer) {
+    int rc;
+    if ((rc = need_dfsph_halo(d)) || (rc = need_dfsph_halo(local_peer))) return rc;
+    if (peer < 0 || peer >= vtp::kMaxPeers) return fail(VTP_ERR_BOUNDS, "peer index outside 0..7");
+    void *b[VTP_DOMAIN_IPC_BUFFERS];
+    halo_buffers(local_peer, b);
+    d->h_halo.peer[peer] = peer_rows(b);
+    CU(cudaMemcpyAsync(d->d_halo, &d->h_halo, sizeof(vtp::HaloPush), cudaMemcpyHostToDevice, d->st));
+    CU(cudaStreamSynchronize(d->st));
+    return VTP_OK;
+}
+
+int vtp_domain_link_peer_ipc(vtp_domain *d, int peer, const vtp_domain_ipc *h) {
+    int rc;
+    if ((rc = need_dfsph_halo(d))) return rc;
+    if (!h) return fail(VTP_ERR_ARG, "null handles");
+    if (peer < 0 || peer >= vtp::kMaxPeers) return fail(VTP_ERR_BOUNDS, "peer index outside 0..7");
+    void *b[VTP_DOMAIN_IPC_BUFFERS];
+    for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) {
+        cudaIpcMemHandle_t hk;
+        std::memcpy(&hk, h->handle[k], sizeof(hk));
+        CU(cudaIpcOpenMemHandle(&b[k], hk, cudaIpcMemLazyEnablePeerAccess));
+        d->ipc_opened.push_back(b[k]);
+    }
+    d->h_halo.peer[peer] = peer_rows(b);
+    CU(cudaMemcpyAsync(d->d_halo, &d->h_halo, sizeof(vtp::HaloPush), cudaMemcpyHostToDevice, d->st));
+    CU(cudaStreamSynchronize(d->st));
+    return VTP_OK;
+}
+
+int vtp_domain_set_halo(vtp_domain *d, int on) {
+    int rc;
+    if ((rc = need_dfsph_halo(d))) return rc;
+    d->halo_on = on != 0;
+    d->prepared = false;   // the next prepare sets the ghost flags
+    return VTP_OK;
+}
+
+int vtp_domain_buffer_parity(vtp_domain *d, int32_t *out2) {
+    if (!d || !out2) return fail(VTP_ERR_ARG, "null argument");
+    out2[0] = d->s->vadv.cur;
+    out2[1] = d->s->vel.cur;
+    return VTP_OK;
+}
+
+int vtp_domain_rows(vtp_domain *d, uint32_t first_slot, uint32_t count, uint32_t *d_rows) {
+    int rc;
+    if ((rc = need_prepared(d))) return rc;
+    if (count == 0) return VTP_OK;
+    if (!d_rows) return fail(VTP_ERR_ARG, "null array");
+    if ((uint64_t)first_slot + count > d->n_act) return fail(VTP_ERR_BOUNDS, "rows outside the loaded rows");
+    k_dd_rows<<<nblk(count, 256), 256, 0, d->st>>>(count, first_slot, d->n_act, d->row_of_slot, d_rows, d->status);
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+int vtp_domain_halo_targets(vtp_domain *d, int peer, const uint32_t *d_slots, const uint32_t *d_dst_rows,
+                            uint32_t count, uint32_t peer_capacity) {
+    int rc;
+    if ((rc = need_dfsph_halo(d)) || (rc = need_prepared(d))) return rc;
+    if (!d->halo_on) return fail(VTP_ERR_STATE, "halo targets with peer-store halos off");
+    if (peer < 0 || peer >= vtp::kMaxPeers || !d->h_halo.peer[peer].kappa)
+        return fail(VTP_ERR_STATE, "halo targets on a peer that is not linked");
+    if (count == 0) return VTP_OK;
+    if (!d_slots || !d_dst_rows) return fail(VTP_ERR_ARG, "null array");
+    k_dd_targets<<<nblk(count, 256), 256, 0, d->st>>>(count, d->n_act, d->n_own, (uint32_t)peer, d_slots, d_dst_rows,
+                                                     peer_capacity, d->row_of_slot, d->ntarget, d->target,
+                                                     d->status);
     CU(cudaGetLastError());
     return VTP_OK;
 }

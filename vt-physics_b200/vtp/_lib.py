@@ -99,6 +99,13 @@ SIGNATURES = {
     "vtp_domain_pack": (C.c_int, [_P, C.c_int, _P, C.c_uint32, _P]),
     "vtp_domain_unpack": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_uint32, _P]),
     "vtp_domain_read": (C.c_int, [_P, _P, _P]),
+    "vtp_domain_export_ipc": (C.c_int, [_P, _P]),
+    "vtp_domain_link_peer": (C.c_int, [_P, C.c_int, _P]),
+    "vtp_domain_link_peer_ipc": (C.c_int, [_P, C.c_int, _P]),
+    "vtp_domain_set_halo": (C.c_int, [_P, C.c_int]),
+    "vtp_domain_buffer_parity": (C.c_int, [_P, _P]),
+    "vtp_domain_rows": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P]),
+    "vtp_domain_halo_targets": (C.c_int, [_P, C.c_int, _P, _P, C.c_uint32, C.c_uint32]),
 }
 
 

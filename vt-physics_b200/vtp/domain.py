@@ -197,6 +197,20 @@ class TorchComm:
         self.dist.all_reduce(t)
         return t
 
+    def share(self, obj) -> list:
+        """Every rank's `obj` (host objects, e.g. IPC handles), in rank order."""
+        out = [None] * self.size
+        self.dist.all_gather_object(out, obj)
+        return out
+
+    def fence(self, device):
+        """Orders every rank's later stream work after every rank's earlier stream work (a
+        one-element all-reduce on the stream)."""
+        import torch
+        if getattr(self, "_one", None) is None or self._one.device != device:
+            self._one = torch.zeros(1, dtype=torch.float32, device=device)
+        self.dist.all_reduce(self._one)
+
     def allreduce_max(self, t):
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return t
@@ -252,6 +266,24 @@ class LoopbackComm:
         out = [box[("c", q)][me] for q in range(self.size)]
         self.hub.barrier.wait()
         return out
+
+    def share(self, obj) -> list:
+        if self.size == 1:
+            return [obj]
+        box, me = self.hub.box, self.rank
+        box[("s", me)] = obj
+        self.hub.barrier.wait()
+        out = [box[("s", q)] for q in range(self.size)]
+        self.hub.barrier.wait()
+        return out
+
+    def fence(self, device=None):
+        if self.size == 1:
+            return
+        import torch
+        if device is not None and device.type == "cuda":
+            torch.cuda.current_stream(device).synchronize()
+        self.hub.barrier.wait()
 
     def allreduce_max(self, t):
         if self.size == 1:
@@ -360,6 +392,42 @@ class LibraryStages:
         # hash, 3 scan kernels, scatter, rank/reorder, lists, slot map (+ DFSPH: tiles, ratio/alpha)
         self.launches += 8 if self.pbf else 10
 
+    # --- peer-store halos (DFSPH)
+    def export_ipc(self) -> bytes:
+        """CUDA IPC handles of the buffers peers store ghost values into, for another process."""
+        buf = (C.c_ubyte * (8 * 64 + 4))()
+        self.check(self.L.vtp_domain_export_ipc(self.h, C.cast(buf, C.c_void_p)), "vtp_domain_export_ipc")
+        return bytes(buf)
+
+    def link_local(self, peer: int, other: "LibraryStages"):
+        self.check(self.L.vtp_domain_link_peer(self.h, int(peer), other.h), "vtp_domain_link_peer")
+
+    def link_ipc(self, peer: int, handles: bytes):
+        buf = (C.c_ubyte * len(handles)).from_buffer_copy(handles)
+        self.check(self.L.vtp_domain_link_peer_ipc(self.h, int(peer), C.cast(buf, C.c_void_p)),
+                   "vtp_domain_link_peer_ipc")
+
+    def set_halo(self, on: bool):
+        self.check(self.L.vtp_domain_set_halo(self.h, int(bool(on))), "vtp_domain_set_halo")
+
+    def parity(self) -> tuple:
+        out = (C.c_int32 * 2)()
+        self.check(self.L.vtp_domain_buffer_parity(self.h, out), "vtp_domain_buffer_parity")
+        return int(out[0]), int(out[1])
+
+    def rows(self, first: int, count: int):
+        out = self.torch.empty(count, dtype=self.torch.int32, device=self.device)
+        self.check(self.L.vtp_domain_rows(self.h, int(first), int(count), out.data_ptr()), "vtp_domain_rows")
+        self.launches += 1
+        return out
+
+    def halo_targets(self, peer: int, slots, dst_rows, peer_capacity: int):
+        s = slots.to(self.torch.int32).contiguous()
+        d = dst_rows.to(self.torch.int32).contiguous()
+        self.check(self.L.vtp_domain_halo_targets(self.h, int(peer), s.data_ptr(), d.data_ptr(), s.numel(),
+                                                   int(peer_capacity)), "vtp_domain_halo_targets")
+        self.launches += 1
+
     def pbf_lambda(self):
         self.check(self.L.vtp_domain_pbf_lambda(self.h), "vtp_domain_pbf_lambda")
         self.launches += 1
@@ -428,7 +496,7 @@ class DomainRank:
     worker's stages with the exchanges of the module docstring."""
 
     def __init__(self, arrays: SceneArrays, plan: SlabPlan, comm, make_stages=LibraryStages,
-                 capacity_factor: float = 2.0, speculate: bool = True):
+                 capacity_factor: float = 2.0, speculate: bool = True, halo: str = "auto"):
         import torch
         self.torch = torch
         self.speculate = speculate
@@ -482,6 +550,55 @@ class DomainRank:
         self.iters = []            # (divergence, density) iterations per substep (PBF: (iterations, 0))
         self.residuals = []
         self.crashed = False
+        # Halo transport: "peer" (DFSPH, library stages, at most 8 ranks): the owners' stage
+        # kernels store ghost values straight into the peers' ghost rows and a fence orders the
+        # peers' next stage; "exchange": pack, send / receive, unpack.
+        if halo == "auto":
+            halo = "peer" if (self.kind == "DFSPH" and hasattr(self.stages, "link_local") and 1 < comm.size <= 8
+                              and (isinstance(comm, LoopbackComm) or self._nccl())) else "exchange"
+        if halo not in ("peer", "exchange"):
+            raise ValueError("halo must be 'auto', 'peer' or 'exchange'")
+        self.peer_mode = halo == "peer" and comm.size > 1
+        if self.peer_mode:
+            self._link_peers()
+
+    def _nccl(self) -> bool:
+        try:
+            return self.comm.dist.get_backend() == "nccl"
+        except Exception:
+            return False
+
+    def _link_peers(self):
+        """Map every peer worker's ghost-target buffers: directly within one process, through
+        CUDA IPC handles across processes."""
+        st = self.stages
+        if isinstance(self.comm, LoopbackComm):
+            workers = self.comm.share(st)
+            for q in self._peers():
+                st.link_local(q, workers[q])
+            self.peer_cap = [w.capacity for w in workers]
+        else:
+            shared = self.comm.share((st.export_ipc(), st.capacity))
+            for q in self._peers():
+                st.link_ipc(q, shared[q][0])
+            self.peer_cap = [c for _, c in shared]
+        st.set_halo(True)
+
+    def _halo_targets(self):
+        """Peer mode, after prepare: the rows this rank holds each peer's ghosts at go to that
+        peer; the rows each peer holds this rank's sends at come back and become targets."""
+        t = self.torch
+        dev = self.pos.device
+        sends = {q: self.stages.rows(self.ghost_first[q], self.recv_count[q]) for q in self.ghost_first}
+        recvs = {q: t.empty(idx.numel(), dtype=t.int32, device=dev) for q, idx in self.send_slots.items()
+                 if idx.numel()}
+        self.comm.exchange(sends, recvs)
+        for q, rows in recvs.items():
+            self.stages.halo_targets(q, self.send_slots[q], rows, self.peer_cap[q])
+        if self.substeps == 0:
+            par = self.comm.share(self.stages.parity())
+            if any(p != par[0] for p in par):
+                raise RuntimeError(f"workers' buffer parities differ: {par}")
 
     # --- exchanges
     def _peers(self):
@@ -554,6 +671,12 @@ class DomainRank:
         return t.cat([self.pos] + gpos), t.cat([self.vel] + gvel), t.cat([self.gid] + ggid), t.cat([self.obj, zeros])
 
     def _exchange(self, field: int):
+        if self.peer_mode and field in (FIELD_KAPPA, FIELD_VADV, FIELD_VEL, FIELD_NORMAL):
+            # the stage stored the ghost values into the peers itself; order the peers' next
+            # stage after the stores (after solve_b the residual all-reduce does it)
+            if field != FIELD_VADV:
+                self.comm.fence(self.pos.device)
+            return
         sends = {q: self.stages.pack(field, idx) for q, idx in self.send_slots.items() if idx.numel()}
         recvs = {q: self.stages.empty(field, self.recv_count[q]) for q in self.ghost_first}
         self.comm.exchange(sends, recvs)
@@ -638,6 +761,8 @@ class DomainRank:
         pos, vel, gid, obj = self._ghosts()
         st.load(self.pos.shape[0], pos, vel, gid, obj)
         st.prepare()
+        if self.peer_mode:
+            self._halo_targets()
         div = self._solve(0)
         st.forces()
         if self.gamma != 0.0:
@@ -715,7 +840,7 @@ def merge_states(arrays: SceneArrays, states: list) -> dict:
 
 
 def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibraryStages,
-                capacity_factor: float = 2.0, speculate: bool = True) -> list:
+                capacity_factor: float = 2.0, speculate: bool = True, halo: str = "auto") -> list:
     """Run ``body(rank)`` for every domain of `plan` inside this process, one thread (and, with
     the library's stages, one CUDA stream) per domain, exchanging through ``LoopbackComm``;
     returns the bodies' results in rank order.  A failure on one domain releases the others
@@ -726,25 +851,31 @@ def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibrarySt
     errors = []
     use_cuda = make_stages is LibraryStages
 
+    ranks = [None] * plan.ranks
+
     def work(k):
-        rank = None
         try:
             ctx = torch.cuda.stream(torch.cuda.Stream()) if use_cuda else _null()
             with ctx:
-                rank = DomainRank(arrays, plan, LoopbackComm(hub, k), make_stages, capacity_factor, speculate)
-                results[k] = body(rank)
+                ranks[k] = DomainRank(arrays, plan, LoopbackComm(hub, k), make_stages, capacity_factor, speculate,
+                                      halo)
+                results[k] = body(ranks[k])
         except BaseException as e:   # wake the other domains, report the first failure
             errors.append(e)
             hub.barrier.abort()
-        finally:
-            if rank is not None:
-                rank.close()
 
     threads = [threading.Thread(target=work, args=(k,), daemon=True) for k in range(plan.ranks)]
     for th in threads:
         th.start()
     for th in threads:
         th.join()
+    # Workers are released only once every domain has stopped: with peer-store halos a
+    # domain's kernels write into the others' buffers.
+    if use_cuda:
+        torch.cuda.synchronize()
+    for r in ranks:
+        if r is not None:
+            r.close()
     if errors:
         real = [e for e in errors if not isinstance(e, threading.BrokenBarrierError)]
         raise (real or errors)[0]
@@ -753,7 +884,7 @@ def local_ranks(arrays: SceneArrays, plan: SlabPlan, body, make_stages=LibrarySt
 
 def run_local(scene, ranks: int, steps: int, make_stages=LibraryStages, axis: int | None = None,
               capacity_factor: float = 2.0, extra: dict | None = None, speculate: bool = True,
-              plan: SlabPlan | None = None) -> dict:
+              plan: SlabPlan | None = None, halo: str = "auto") -> dict:
     """Run `scene` decomposed into `ranks` slabs inside this process (``local_ranks``) for
     `steps` substeps and merge the ranks' owned particles into the scene's fluid order.
     `plan` replaces the quantile slabs of ``plan_slabs``."""
@@ -767,7 +898,7 @@ def run_local(scene, ranks: int, steps: int, make_stages=LibraryStages, axis: in
         rank.step(steps)
         return rank.state()
 
-    out = merge_states(arrays, local_ranks(arrays, plan, body, make_stages, capacity_factor, speculate))
+    out = merge_states(arrays, local_ranks(arrays, plan, body, make_stages, capacity_factor, speculate, halo))
     out["plan"] = plan
     return out
 
