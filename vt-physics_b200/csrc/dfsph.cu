@@ -438,6 +438,9 @@ __global__ void k_solve_pack(DfsphArgs a, uint32_t n) {
     const float4 p = a.pos[r];
     a.pva[2 * (size_t)r] = p;
     a.pva[2 * (size_t)r + 1] = a.vadv[r];
+    // With peer-store halos a ghost's {x, kappa} row is written only by its owner's solve_a
+    // (which may already be storing it: no fence separates this pack from the peers' solve_a).
+    if (r < a.nf && halo_ghost(a, r)) return;
     a.pk[r] = r < a.nf ? make_float4(p.x, p.y, p.z, 0.f) : p;
 }
 
