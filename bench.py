@@ -684,12 +684,11 @@ def run_domains(args, rank, world, dist, torch) -> dict:
     """dfsph_1m_dd: the DFSPH 1M scene decomposed into slabs along x (vtp/domain.py), one slab per
     rank under torchrun (NCCL point-to-point and all-reduce between the GPUs) or, in one process,
     --domains slabs as threads on this GPU.  Strong scaling: the whole scene's particle-steps over
-    the slowest rank's CUDA-event time.  The fixed 1 ms step (the adaptive rule is not decomposed;
-    the whole-scene run's step stays at its 1 ms cap over these substeps anyway)."""
+    the slowest rank's CUDA-event time.  The configuration of the dfsph_1m workload, its adaptive
+    step included (one max all-reduce of |v|^2 per substep)."""
     from vtp import domain, scenes
     sc = scenes.dfsph_1m()
     extra = json.loads(args.extra) if args.extra else default_extra("dfsph_1m")
-    extra.pop("cfl", None)
     arrays = domain.scene_arrays(sc)
     arrays.config = json.loads(json.dumps(arrays.config))
     arrays.config["B200"] = extra
@@ -761,6 +760,7 @@ def run_domains(args, rank, world, dist, torch) -> dict:
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "dfsph_1m_dd", "fluid": nf, "boundary": sc.n_boundary, "dt": 1e-3,
+                   "halo": "peer stores" if ranks > 1 else "none (one slab)",
                    "parallelism": f"slabs{ranks}" + ("" if world > 1 else " (threads on one GPU)"),
                    "slab_axis": plan.axis, "slab_bounds": list(plan.bounds), "ghost": plan.ghost,
                    "owned_at_end": owned,

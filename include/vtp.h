@@ -448,7 +448,8 @@ typedef enum vtp_domain_field {
     VTP_DOMAIN_LAMBDA = 4,   /* PBF, float per row: lambda after a lambda pass */
     VTP_DOMAIN_POSVEL = 5    /* PBF, 2 float4 per row {position, velocity}: after a correction pass */
 } vtp_domain_field;
-/* config_json: the scene's DFSPH or PBF config (DFSPH: the fixed timeStep, "cfl" 0).
+/* config_json: the scene's DFSPH or PBF config (a DFSPH "cfl" step is set per substep by
+ * the host: vtp_domain_owned_vmax2 after load, the maximum over ranks, vtp_domain_set_dt).
  * fluid_pos: the worker's initial fluid rows (owned and ghost, host xyz,
  * ascending scene-wide id), used for the boundary volumes at create;
  * boundary_pos / boundary_ids: the boundary band (host, ids ascending);
@@ -470,6 +471,11 @@ VTP_API int vtp_domain_capacity(vtp_domain *d, uint32_t *capacity, uint32_t *n_b
 VTP_API int vtp_domain_load(vtp_domain *d, uint32_t n_own, uint32_t n_ghost, const float *d_pos,
                             const float *d_vel, const uint32_t *d_ids, const uint32_t *d_obj);
 VTP_API int vtp_domain_prepare(vtp_domain *d);
+/* DFSPH adaptive step: max |v|^2 of the owned rows (between load and prepare; waits), and the
+ * step the stages use from now on (dt = min(timeStep, cfl 2r / sqrt(max over ranks)), as the
+ * solver's own adaptive step forms it). */
+VTP_API int vtp_domain_owned_vmax2(vtp_domain *d, float *out);
+VTP_API int vtp_domain_set_dt(vtp_domain *d, float dt);
 VTP_API int vtp_domain_solve_begin(vtp_domain *d, int which);
 /* d_sums: double[n_objects], the owned rows' clamped compression errors summed per object. */
 VTP_API int vtp_domain_solve_a(vtp_domain *d, double *d_sums);

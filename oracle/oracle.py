@@ -495,6 +495,17 @@ class DfsphDomainStages:
         self.acc = np.zeros((n, 3))
         self.nrm = np.zeros((n, 3))
 
+    def vmax2(self) -> float:
+        """Largest |v|^2 of the owned rows, as OracleSolver forms it for the adaptive step."""
+        idx = self.local_of_slot[: self.n_own]
+        if idx.size == 0:
+            return 0.0
+        v = self.vel[idx].astype(np.float32)
+        return float((v * v).sum(axis=1, dtype=np.float32).max())
+
+    def set_dt(self, dt: float):
+        self.p.dt = float(np.float32(dt))
+
     def solve_begin(self, which: int):
         pass
 

@@ -65,10 +65,20 @@ def test_scene_arrays_keep_attach_ids_and_reject_interleaved_ids():
         domain.scene_arrays(scenes.layered_mixture("IMMCT", 6, seed=1))
 
 
-def test_decomposed_run_rejects_the_adaptive_step(oracle_lib):
-    with pytest.raises(ValueError, match="cfl"):
-        domain.run_local(scenes.dam_break("DFSPH", 800, seed=12), 2, 1, make_stages=oracle_lib.DfsphDomainStages,
-                         extra={"cfl": 0.4})
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+def test_decomposed_oracle_with_the_adaptive_step(oracle_lib, ranks):
+    """The CFL step (cfl 0.05 binds at 1.5 m/s: dt ~3.3e-4 against the 1 ms cap, changing every
+    substep): one max all-reduce of the owned |v|^2 per substep gives every rank the
+    whole-scene step, and the trajectories stay bit-identical."""
+    from oracle import oracle as O
+    sc = scenes.colliding_blocks()
+    sc.config = dict(sc.config, B200={"cfl": 0.05})
+    o = O.OracleSolver(sc)
+    o.step(10)
+    fl = o.mat == 0
+    assert max(o.dts) < 1e-3 and len(set(o.dts)) > 3
+    out = domain.run_local(sc, ranks, 10, make_stages=oracle_lib.DfsphDomainStages)
+    assert np.array_equal(out["pos"], o.pos[fl]) and np.array_equal(out["vel"], o.vel[fl])
 
 
 # ----------------------------------------------------------------------------- oracle stages
@@ -318,5 +328,18 @@ def test_dfsph_1m_in_eight_slabs_over_25_free_substeps(vtp_gpu):
     sc = scenes.dfsph_1m()
     pos, vel, iters = _whole_library(sc, 25, {})
     out = domain.run_local(sc, 8, 25)
+    assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("halo", ["peer", "exchange"])
+def test_library_domains_with_the_adaptive_step(vtp_gpu, halo):
+    """The library's adaptive step computed on the device for the whole scene and on the host
+    from the all-reduced |v|^2 for the slabs: the same steps, the same trajectory."""
+    sc = scenes.colliding_blocks()
+    extra = {"cfl": 0.05}
+    pos, vel, iters = _whole_library(sc, 10, extra)
+    out = domain.run_local(sc, 4, 10, extra=extra, halo=halo)
     assert out["iters"] == iters
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)

@@ -28,6 +28,7 @@
 // (j < nf).  Load slots (the order the host loads rows in: owned first, then
 // each peer's ghosts) travel through the sort so that the exchanges address
 // rows by load slot.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -286,6 +287,19 @@ __global__ void k_dd_rows(uint32_t count, uint32_t first, uint32_t n, const uint
     out[k] = r;
 }
 
+// Largest |v|^2 of the owned rows (load order, before the sort), with the arithmetic of the
+// adaptive step's own reduction (k_cfl_max): fmax over dist2, folded by unsigned atomicMax.
+__global__ void k_dd_vmax2(uint32_t n_own, const float4 *__restrict__ vel, uint32_t *__restrict__ out_bits) {
+    float m = 0.f;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_own; r += gridDim.x * blockDim.x) {
+        const float4 v = vel[r];
+        m = fmaxf(m, vtp::dist2(v.x, v.y, v.z));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31u) == 0 && m > 0.f) atomicMax(out_bits, __float_as_uint(m));
+}
+
 __global__ void k_dd_read(uint32_t n_own, uint32_t n, const uint32_t *__restrict__ row_of_slot,
                           const float4 *__restrict__ pos, const float4 *__restrict__ vel, float *__restrict__ pos3,
                           float *__restrict__ vel3, uint32_t *status) {
@@ -326,6 +340,9 @@ struct vtp_domain {
     uint32_t *status = nullptr;     // the domain kernels' own status word (ST_BOUNDS: a bad slot)
     uint32_t *h_status = nullptr;   // [2]: the domain word, the wrapped solver's word
     // Peer-store halos (DFSPH): per sorted row its ghost flag and its targets on peer workers
+    bool dt_set = false;            // adaptive step: this substep's dt from the host
+    float dt_now = 0.f;
+    uint32_t *vmax_bits = nullptr;
     bool halo_on = false;
     uint8_t *ghost = nullptr;
     uint32_t *ntarget = nullptr;
@@ -358,6 +375,12 @@ struct vtp_domain {
         a.dtp = nullptr;
         a.vmax_bits = nullptr;
         a.tick = nullptr;
+        if (dt_set) {   // the adaptive step, 1/dt and 1/dt^2 formed as the device forms them
+            const float inv = 1.f / dt_now;
+            a.dt = dt_now;
+            a.inv_dt = inv;
+            a.inv_dt2 = inv * inv;
+        }
         if (halo_on) {
             a.halo = d_halo;
             a.halo_vadv = s->vadv.cur;
@@ -413,7 +436,7 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         if (!pbf && !cfg.contains("DFSPH")) return fail(VTP_ERR_CONFIG, "domain workers run DFSPH or PBF scenes");
         const char *key = pbf ? "PBF" : "DFSPH";
         json ext = cfg.contains("B200") ? cfg["B200"] : json::object();
-        if (ext.value("cfl", 0.0) > 0.0) return fail(VTP_ERR_CONFIG, "a domain worker takes the fixed timeStep (cfl 0)");
+        ext.erase("cfl");   // the host sets an adaptive step per substep (vtp_domain_set_dt)
         const int mode = boundary_first ? 1 : 0;
         ext["useGraphs"] = false;
         ext["deviceLoop"] = false;
@@ -455,6 +478,7 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
             if ((rc = d->alloc(&d->objf.b[k], capacity))) return rc;
         }
         if ((rc = d->alloc(&d->row_of_slot, capacity))) return rc;
+        if ((rc = d->alloc(&d->vmax_bits, 1))) return rc;
         if ((rc = d->alloc(&d->part, (size_t)kSumBlocks * n_objects))) return rc;
         if (!pbf) {
             if ((rc = d->alloc(&d->ghost, capacity))) return rc;
@@ -782,6 +806,32 @@ int vtp_domain_halo_targets(vtp_domain *d, int peer, const uint32_t *d_slots, co
                                                      peer_capacity, d->row_of_slot, d->ntarget, d->target,
                                                      d->status);
     CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+int vtp_domain_owned_vmax2(vtp_domain *d, float *out) {
+    if (!d || !out) return fail(VTP_ERR_ARG, "null argument");
+    if (!d->loaded) return fail(VTP_ERR_STATE, "vtp_domain_owned_vmax2 before vtp_domain_load");
+    if (d->prepared) return fail(VTP_ERR_STATE, "vtp_domain_owned_vmax2 between load and prepare");
+    CU(cudaMemsetAsync(d->vmax_bits, 0, sizeof(uint32_t), d->st));
+    if (d->n_own) {
+        const unsigned g = std::min<unsigned>(nblk(d->n_own, 256), 148u * 8u);
+        k_dd_vmax2<<<g, 256, 0, d->st>>>(d->n_own, d->s->vel.c(), d->vmax_bits);
+    }
+    CU(cudaGetLastError());
+    uint32_t bits = 0;
+    CU(cudaMemcpyAsync(d->h_status, d->vmax_bits, sizeof(uint32_t), cudaMemcpyDeviceToHost, d->st));
+    CU(cudaStreamSynchronize(d->st));
+    bits = d->h_status[0];
+    std::memcpy(out, &bits, sizeof(float));
+    return VTP_OK;
+}
+
+int vtp_domain_set_dt(vtp_domain *d, float dt) {
+    if (!d) return fail(VTP_ERR_ARG, "null domain");
+    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(VTP_ERR_ARG, "time step must be finite and positive");
+    d->dt_set = true;
+    d->dt_now = dt;
     return VTP_OK;
 }
 

@@ -87,6 +87,8 @@ SIGNATURES = {
     "vtp_domain_capacity": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "vtp_domain_load": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P]),
     "vtp_domain_prepare": (C.c_int, [_P]),
+    "vtp_domain_owned_vmax2": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "vtp_domain_set_dt": (C.c_int, [_P, C.c_float]),
     "vtp_domain_solve_begin": (C.c_int, [_P, C.c_int]),
     "vtp_domain_solve_a": (C.c_int, [_P, _P]),
     "vtp_domain_solve_b": (C.c_int, [_P]),

@@ -387,6 +387,16 @@ class LibraryStages:
                    "vtp_domain_load")
         self.launches += 1
 
+    def vmax2(self) -> float:
+        """Largest |v|^2 of the loaded owned rows (the adaptive step's own arithmetic)."""
+        out = C.c_float()
+        self.check(self.L.vtp_domain_owned_vmax2(self.h, C.byref(out)), "vtp_domain_owned_vmax2")
+        self.launches += 1
+        return float(out.value)
+
+    def set_dt(self, dt: float):
+        self.check(self.L.vtp_domain_set_dt(self.h, float(dt)), "vtp_domain_set_dt")
+
     def prepare(self):
         self.check(self.L.vtp_domain_prepare(self.h), "vtp_domain_prepare")
         # hash, 3 scan kernels, scatter, rank/reorder, lists, slot map (+ DFSPH: tiles, ratio/alpha)
@@ -512,8 +522,10 @@ class DomainRank:
         ext = arrays.config.get("B200", {})
         self.dt = float(np.float32(req["timeStep"]))
         if self.kind == "DFSPH":
-            if float(ext.get("cfl", 0.0)) > 0.0:
-                raise ValueError("a decomposed scene takes the fixed timeStep (cfl 0)")
+            # the adaptive step ("cfl"): one max all-reduce of the owned rows' |v|^2 per substep
+            self.cfl = float(np.float32(ext.get("cfl", 0.0)))
+            self.diameter = np.float32(np.float32(2) * np.float32(req["particleRadius"]))
+            self.dts = []
             self.thr = (float(np.float32(req["divFreeThreshold"])), float(np.float32(req["incompThreshold"])))
             self.force = (int(ext.get("forceDivIterations", 0)), int(ext.get("forceIncompIterations", 0)))
             self.force_seq = [tuple(int(v) for v in p) for p in ext.get("forceIterationsPerTick", [])]
@@ -561,6 +573,22 @@ class DomainRank:
         self.peer_mode = halo == "peer" and comm.size > 1
         if self.peer_mode:
             self._link_peers()
+
+    def _adaptive_step(self):
+        """dt = min(timeStep, cfl 2r / max |v|) over all ranks' fluid, at least timeStep 1e-4,
+        in FP32 with the operations of the solver's adaptive step (k_cfl_step); timeStep when
+        the fluid is at rest."""
+        t = self.torch
+        v2 = t.tensor([self.stages.vmax2()], dtype=t.float32, device=self.pos.device)
+        v2 = np.float32(self.comm.allreduce_max(v2).cpu().numpy()[0])
+        f32 = np.float32
+        dt_max = f32(self.dt)
+        vmax = np.sqrt(v2)
+        dt = dt_max
+        if vmax > 0:
+            dt = max(min(dt_max, f32(f32(self.cfl) * self.diameter) / vmax), f32(dt_max * f32(1e-4)))
+        self.stages.set_dt(float(dt))
+        self.dts.append(float(dt))
 
     def _nccl(self) -> bool:
         try:
@@ -760,6 +788,8 @@ class DomainRank:
             self._migrate()
         pos, vel, gid, obj = self._ghosts()
         st.load(self.pos.shape[0], pos, vel, gid, obj)
+        if self.cfl > 0:
+            self._adaptive_step()
         st.prepare()
         if self.peer_mode:
             self._halo_targets()
