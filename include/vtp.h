@@ -491,27 +491,30 @@ VTP_API int vtp_domain_pbf_xsph(vtp_domain *d);
  * rows at load slots [first_slot, first_slot + count). */
 VTP_API int vtp_domain_pack(vtp_domain *d, int field, const uint32_t *d_slots, uint32_t count, float *d_out);
 VTP_API int vtp_domain_unpack(vtp_domain *d, int field, uint32_t first_slot, uint32_t count, const float *d_in);
-/* Peer-store halos (DFSPH): instead of pack / exchange / unpack, the stage kernels of the
- * owner write each value a ghost needs (kappa and its packed row in solve_a, v* and its
- * packed row in solve_b, velocities in forces / tension, normals in the normal pass)
- * straight into the ghost rows of the peer workers, whose buffers this worker maps: a
+/* Peer-store halos: instead of pack / exchange / unpack, the stage kernels of the owner
+ * write each value a ghost needs (DFSPH: kappa and its packed row in solve_a, v* and its
+ * packed row in solve_b, velocities in forces / tension, normals in the normal pass; PBF:
+ * lambda in pbf_lambda, the corrected position and velocity in pbf_dx) straight into the
+ * ghost rows of the peer workers, whose buffers this worker maps: a
  * worker of the same process (vtp_domain_link_peer) or of another process through CUDA IPC
  * (vtp_domain_export_ipc on the peer, vtp_domain_link_peer_ipc here).  Ghost rows then skip
  * their own writes.  Per substep, after prepare: for each peer the owned load slots that
  * are its ghosts and their rows there (vtp_domain_rows on the peer) go to
  * vtp_domain_halo_targets.  The caller orders each peer's next stage after the stores (a
  * collective on the stream, or a barrier); both sides must have the same buffer parity
- * (vtp_domain_buffer_parity), which the same stage sequence gives. */
+ * (vtp_domain_buffer_parity: v*, velocity, position), which the same stage sequence gives. */
 #define VTP_DOMAIN_IPC_BUFFERS 8
 typedef struct vtp_domain_ipc {
     unsigned char handle[VTP_DOMAIN_IPC_BUFFERS][64];   /* cudaIpcMemHandle_t of each buffer */
-    uint32_t capacity;
+    uint32_t capacity;                                   /* the worker's fluid rows */
+    uint32_t count;                                      /* handles used (DFSPH 8, PBF 5) */
+    uint32_t solver_type;
 } vtp_domain_ipc;
 VTP_API int vtp_domain_export_ipc(vtp_domain *d, vtp_domain_ipc *out);
 VTP_API int vtp_domain_link_peer(vtp_domain *d, int peer, vtp_domain *local_peer);
 VTP_API int vtp_domain_link_peer_ipc(vtp_domain *d, int peer, const vtp_domain_ipc *h);
 VTP_API int vtp_domain_set_halo(vtp_domain *d, int on);
-VTP_API int vtp_domain_buffer_parity(vtp_domain *d, int32_t *out2);
+VTP_API int vtp_domain_buffer_parity(vtp_domain *d, int32_t *out3);
 VTP_API int vtp_domain_rows(vtp_domain *d, uint32_t first_slot, uint32_t count, uint32_t *d_rows);
 VTP_API int vtp_domain_halo_targets(vtp_domain *d, int peer, const uint32_t *d_slots, const uint32_t *d_dst_rows,
                                     uint32_t count, uint32_t peer_capacity);

@@ -296,12 +296,14 @@ def test_dfsph_1m_in_four_slabs_equals_the_whole_scene(vtp_gpu):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("ranks", [1, 2, 4])
-def test_library_pbf_domains_equal_whole_scene_library(vtp_gpu, ranks):
+@pytest.mark.parametrize("halo", ["peer", "exchange"])
+def test_library_pbf_domains_equal_whole_scene_library(vtp_gpu, ranks, halo):
     """PBF at mass-1 particles, the collapsing column over 40 substeps: the decomposed library
-    run equals the whole-scene library run bit for bit."""
+    run equals the whole-scene library run bit for bit, with the ghosts' lambda, positions and
+    velocities stored by the owners' kernels or exchanged."""
     sc = scenes.dam_break("PBF", 8000, seed=21, spacing=0.1)
     pos, vel, _ = _whole_library(sc, 40, {})
-    out = domain.run_local(sc, ranks, 40)
+    out = domain.run_local(sc, ranks, 40, halo=halo)
     assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
 
 

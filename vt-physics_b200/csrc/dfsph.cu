@@ -71,21 +71,6 @@ __device__ __forceinline__ StepDt step_dt(const DfsphArgs &a) {
     return StepDt{dt, inv, inv * inv};
 }
 
-// Peer-store halos (HaloPush in dfsph.h): ghost rows write nothing; an owned row hands each
-// value it writes to `f(peer rows, the peer's row)` for every peer it is a ghost on.
-__device__ __forceinline__ bool halo_ghost(const DfsphArgs &a, uint32_t r) { return a.halo && a.halo->ghost[r]; }
-
-template <class F>
-__device__ __forceinline__ void halo_each(const DfsphArgs &a, uint32_t r, F f) {
-    if (!a.halo) return;
-    const uint32_t n = min(a.halo->ntarget[r], (uint32_t)kMaxHaloTargets);
-    for (uint32_t e = 0; e < n; ++e) {
-        const uint2 t = a.halo->target[(size_t)r * kMaxHaloTargets + e];
-        f(a.halo->peer[t.x], t.y);
-    }
-    if (n) __threadfence_system();   // the stores to other GPUs ordered before what follows
-}
-
 __global__ void __launch_bounds__(256) k_rigid_volume(DfsphArgs a, const uint32_t *__restrict__ bncnt,
                                                       const uint32_t *__restrict__ bnbr,
                                                       float *__restrict__ rest_density_b) {

@@ -3,6 +3,7 @@
 
 #include "internal.h"
 #include "staged.h"
+#include "halo.h"
 
 namespace vtp {
 
@@ -32,27 +33,6 @@ struct LoopState {
 struct SceneTiles {
     uint32_t tile0, ntiles; // the scene's tiles
     uint32_t obj0, nobj;    // the scene's fluid objects (global slots)
-};
-
-// Domain decomposition with peer-store halos (a slab worker of vtp_domain_*).  Rows whose
-// load slot marks them as ghosts skip every write; an owned row that is a ghost on peer
-// workers writes the value it computes (kappa and the packed {x, kappa} row in solve_a, v*
-// and the packed {x, v*} row in solve_b, the new velocity in the viscosity / tension pass,
-// the surface normal in the normal pass) into those workers' ghost rows as well: plain
-// stores to another GPU's memory over NVLink, or to another worker on the same GPU.  The
-// host orders a peer's next stage after the stores (a collective, or a barrier).
-constexpr int kMaxPeers = 8;
-constexpr int kMaxHaloTargets = 4;   // peers a row can be a ghost on
-struct PeerRows {
-    float *kappa;
-    float4 *pk, *pva, *normal;
-    float4 *vadv[2], *vel[2];        // both buffers of the double-buffered fields
-};
-struct HaloPush {
-    const uint8_t *ghost;            // [rows] 1: ghost row (no writes)
-    const uint32_t *ntarget;         // [rows] targets of the row (0..kMaxHaloTargets)
-    const uint2 *target;             // [rows][kMaxHaloTargets] {peer, peer row}
-    PeerRows peer[kMaxPeers];
 };
 
 struct DfsphArgs {

@@ -391,6 +391,11 @@ struct vtp_domain {
     vtp::PbfArgs pbf() const {
         vtp::PbfArgs a = s->pbf_args();
         a.nf = n_act;
+        if (halo_on) {
+            a.halo = d_halo;
+            a.halo_pos = s->pos.cur;
+            a.halo_vel = s->vel.cur;
+        }
         return a;
     }
     vtp::Layout layout() const {
@@ -480,7 +485,7 @@ int vtp_domain_create(const char *config_json, const float *fluid_pos, uint32_t 
         if ((rc = d->alloc(&d->row_of_slot, capacity))) return rc;
         if ((rc = d->alloc(&d->vmax_bits, 1))) return rc;
         if ((rc = d->alloc(&d->part, (size_t)kSumBlocks * n_objects))) return rc;
-        if (!pbf) {
+        {
             if ((rc = d->alloc(&d->ghost, capacity))) return rc;
             if ((rc = d->alloc(&d->ntarget, capacity))) return rc;
             if ((rc = d->alloc(&d->target, (size_t)capacity * vtp::kMaxHaloTargets))) return rc;
@@ -692,22 +697,38 @@ int vtp_domain_finalize(vtp_domain *d) {
 
 namespace {
 
-int need_dfsph_halo(vtp_domain *d) {
+int need_halo(vtp_domain *d) {
     if (!d) return fail(VTP_ERR_ARG, "null domain");
-    if (d->type != VTP_SOLVER_DFSPH || !d->d_halo) return fail(VTP_ERR_STATE, "peer-store halos are a DFSPH worker's");
+    if (!d->d_halo) return fail(VTP_ERR_STATE, "domain worker without halo state");
     return VTP_OK;
 }
 
-// The buffers a peer stores ghost values into, in vtp_domain_ipc order.
-void halo_buffers(vtp_domain *d, void *out[VTP_DOMAIN_IPC_BUFFERS]) {
+// The buffers a peer stores ghost values into, in vtp_domain_ipc order: DFSPH kappa, packed
+// {x, kappa} and {x, v*} rows, normals, both v* and both velocity buffers; PBF lambda, both
+// position and both velocity buffers.  Returns how many.
+int halo_buffers(vtp_domain *d, void *out[VTP_DOMAIN_IPC_BUFFERS]) {
     vtp_solver *s = d->s;
+    if (d->type == VTP_SOLVER_PBF) {
+        void *b[5] = {s->lambda, s->pos.b[0], s->pos.b[1], s->vel.b[0], s->vel.b[1]};
+        for (int k = 0; k < 5; ++k) out[k] = b[k];
+        return 5;
+    }
     void *b[VTP_DOMAIN_IPC_BUFFERS] = {s->kappa, s->pk, s->pva, s->normal, s->vadv.b[0], s->vadv.b[1],
                                        s->vel.b[0], s->vel.b[1]};
     for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) out[k] = b[k];
+    return VTP_DOMAIN_IPC_BUFFERS;
 }
 
-vtp::PeerRows peer_rows(void *const b[VTP_DOMAIN_IPC_BUFFERS]) {
+vtp::PeerRows peer_rows(int type, void *const b[VTP_DOMAIN_IPC_BUFFERS]) {
     vtp::PeerRows r{};
+    if (type == VTP_SOLVER_PBF) {
+        r.lambda = (float *)b[0];
+        r.pos[0] = (float4 *)b[1];
+        r.pos[1] = (float4 *)b[2];
+        r.vel[0] = (float4 *)b[3];
+        r.vel[1] = (float4 *)b[4];
+        return r;
+    }
     r.kappa = (float *)b[0];
     r.pk = (float4 *)b[1];
     r.pva = (float4 *)b[2];
@@ -719,31 +740,37 @@ vtp::PeerRows peer_rows(void *const b[VTP_DOMAIN_IPC_BUFFERS]) {
     return r;
 }
 
+bool linked(const vtp::PeerRows &r) { return r.kappa || r.lambda; }
+
 }  // namespace
 
 int vtp_domain_export_ipc(vtp_domain *d, vtp_domain_ipc *out) {
     int rc;
-    if ((rc = need_dfsph_halo(d))) return rc;
+    if ((rc = need_halo(d))) return rc;
     if (!out) return fail(VTP_ERR_ARG, "null output");
+    std::memset(out, 0, sizeof(*out));
     void *b[VTP_DOMAIN_IPC_BUFFERS];
-    halo_buffers(d, b);
-    for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) {
+    const int nbuf = halo_buffers(d, b);
+    for (int k = 0; k < nbuf; ++k) {
         cudaIpcMemHandle_t h;
         CU(cudaIpcGetMemHandle(&h, b[k]));
         static_assert(sizeof(h) <= sizeof(out->handle[0]), "IPC handle size");
         std::memcpy(out->handle[k], &h, sizeof(h));
     }
     out->capacity = d->cap;
+    out->count = (uint32_t)nbuf;
+    out->solver_type = (uint32_t)d->type;
     return VTP_OK;
 }
 
 int vtp_domain_link_peer(vtp_domain *d, int peer, vtp_domain *local_peer) {
     int rc;
-    if ((rc = need_dfsph_halo(d)) || (rc = need_dfsph_halo(local_peer))) return rc;
+    if ((rc = need_halo(d)) || (rc = need_halo(local_peer))) return rc;
     if (peer < 0 || peer >= vtp::kMaxPeers) return fail(VTP_ERR_BOUNDS, "peer index outside 0..7");
-    void *b[VTP_DOMAIN_IPC_BUFFERS];
+    if (local_peer->type != d->type) return fail(VTP_ERR_STATE, "peer worker of another solver type");
+    void *b[VTP_DOMAIN_IPC_BUFFERS] = {};
     halo_buffers(local_peer, b);
-    d->h_halo.peer[peer] = peer_rows(b);
+    d->h_halo.peer[peer] = peer_rows(d->type, b);
     CU(cudaMemcpyAsync(d->d_halo, &d->h_halo, sizeof(vtp::HaloPush), cudaMemcpyHostToDevice, d->st));
     CU(cudaStreamSynchronize(d->st));
     return VTP_OK;
@@ -751,17 +778,19 @@ int vtp_domain_link_peer(vtp_domain *d, int peer, vtp_domain *local_peer) {
 
 int vtp_domain_link_peer_ipc(vtp_domain *d, int peer, const vtp_domain_ipc *h) {
     int rc;
-    if ((rc = need_dfsph_halo(d))) return rc;
+    if ((rc = need_halo(d))) return rc;
     if (!h) return fail(VTP_ERR_ARG, "null handles");
     if (peer < 0 || peer >= vtp::kMaxPeers) return fail(VTP_ERR_BOUNDS, "peer index outside 0..7");
-    void *b[VTP_DOMAIN_IPC_BUFFERS];
-    for (int k = 0; k < VTP_DOMAIN_IPC_BUFFERS; ++k) {
+    if (h->solver_type != (uint32_t)d->type || h->count > VTP_DOMAIN_IPC_BUFFERS)
+        return fail(VTP_ERR_STATE, "peer handles of another solver type");
+    void *b[VTP_DOMAIN_IPC_BUFFERS] = {};
+    for (uint32_t k = 0; k < h->count; ++k) {
         cudaIpcMemHandle_t hk;
         std::memcpy(&hk, h->handle[k], sizeof(hk));
         CU(cudaIpcOpenMemHandle(&b[k], hk, cudaIpcMemLazyEnablePeerAccess));
         d->ipc_opened.push_back(b[k]);
     }
-    d->h_halo.peer[peer] = peer_rows(b);
+    d->h_halo.peer[peer] = peer_rows(d->type, b);
     CU(cudaMemcpyAsync(d->d_halo, &d->h_halo, sizeof(vtp::HaloPush), cudaMemcpyHostToDevice, d->st));
     CU(cudaStreamSynchronize(d->st));
     return VTP_OK;
@@ -769,16 +798,17 @@ int vtp_domain_link_peer_ipc(vtp_domain *d, int peer, const vtp_domain_ipc *h) {
 
 int vtp_domain_set_halo(vtp_domain *d, int on) {
     int rc;
-    if ((rc = need_dfsph_halo(d))) return rc;
+    if ((rc = need_halo(d))) return rc;
     d->halo_on = on != 0;
     d->prepared = false;   // the next prepare sets the ghost flags
     return VTP_OK;
 }
 
-int vtp_domain_buffer_parity(vtp_domain *d, int32_t *out2) {
-    if (!d || !out2) return fail(VTP_ERR_ARG, "null argument");
-    out2[0] = d->s->vadv.cur;
-    out2[1] = d->s->vel.cur;
+int vtp_domain_buffer_parity(vtp_domain *d, int32_t *out3) {
+    if (!d || !out3) return fail(VTP_ERR_ARG, "null argument");
+    out3[0] = d->s->vadv.cur;
+    out3[1] = d->s->vel.cur;
+    out3[2] = d->s->pos.cur;
     return VTP_OK;
 }
 
@@ -796,9 +826,9 @@ int vtp_domain_rows(vtp_domain *d, uint32_t first_slot, uint32_t count, uint32_t
 int vtp_domain_halo_targets(vtp_domain *d, int peer, const uint32_t *d_slots, const uint32_t *d_dst_rows,
                             uint32_t count, uint32_t peer_capacity) {
     int rc;
-    if ((rc = need_dfsph_halo(d)) || (rc = need_prepared(d))) return rc;
+    if ((rc = need_halo(d)) || (rc = need_prepared(d))) return rc;
     if (!d->halo_on) return fail(VTP_ERR_STATE, "halo targets with peer-store halos off");
-    if (peer < 0 || peer >= vtp::kMaxPeers || !d->h_halo.peer[peer].kappa)
+    if (peer < 0 || peer >= vtp::kMaxPeers || !linked(d->h_halo.peer[peer]))
         return fail(VTP_ERR_STATE, "halo targets on a peer that is not linked");
     if (count == 0) return VTP_OK;
     if (!d_slots || !d_dst_rows) return fail(VTP_ERR_ARG, "null array");

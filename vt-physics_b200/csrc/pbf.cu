@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;   // the same for every lane of the row
     const float4 p = a.pos[r];
     const uint32_t n = a.ncnt[r];
     // Self is the first entry of every list: density gets m_i W(0), gradients 0.
@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(PbfArgs a) {
     gx /= a.rho0; gy /= a.rho0; gz /= a.rho0;
     s2 += gx * gx + gy * gy + gz * gz;
     a.density[r] = rho;
-    a.lambda[r] = -err / (s2 + a.eps);
+    const float lam = -err / (s2 + a.eps);
+    a.lambda[r] = lam;
+    halo_each(a, r, [&](const PeerRows &P, uint32_t q) { P.lambda[q] = lam; });
 }
 
 template <int U, int L>
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;
     const float4 p = a.pos[r];
     const float li = a.lambda[r];
     const uint32_t n = a.ncnt[r];
@@ -159,6 +161,10 @@ __global__ void __launch_bounds__(256) k_pbf_dx(PbfArgs a) {
     float4 v = a.vel[r];
     v.x += dx / a.dt; v.y += dy / a.dt; v.z += dz / a.dt;
     a.vel[r] = v;
+    halo_each(a, r, [&](const PeerRows &P, uint32_t q) {
+        P.pos[a.halo_pos ^ 1][q] = o;   // the peer's second buffer, current after its swap
+        P.vel[a.halo_vel][q] = v;
+    });
 }
 
 template <int U, int L>
@@ -167,7 +173,7 @@ __global__ void __launch_bounds__(256) k_pbf_xsph(PbfArgs a) {
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t r = gt / L;
     const int lane = (int)(gt % L);
-    if (r >= a.nf) return;
+    if (r >= a.nf || halo_ghost(a, r)) return;
     const float4 p = a.pos[r];
     const float4 vi = a.vel[r];
     const uint32_t n = a.ncnt[r];

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "internal.h"
+#include "halo.h"
 
 namespace vtp {
 
@@ -23,6 +24,8 @@ struct PbfArgs {
     float *lambda;         // [nf]
     int unroll;            // neighbours in flight per thread (1, 2, 4, 8)
     int lanes = 1;         // threads per row of the neighbour passes (1, 4, 8)
+    const HaloPush *halo = nullptr;   // peer-store halos of a slab worker (halo.h; null: none)
+    int halo_pos = 0, halo_vel = 0;   // current position / velocity buffer (the peers' parity equals ours)
 };
 
 void pbf_init_boundary(cudaStream_t st, const PbfArgs &a, const uint32_t *bncnt, const uint32_t *bnbr,

@@ -405,7 +405,7 @@ class LibraryStages:
     # --- peer-store halos (DFSPH)
     def export_ipc(self) -> bytes:
         """CUDA IPC handles of the buffers peers store ghost values into, for another process."""
-        buf = (C.c_ubyte * (8 * 64 + 4))()
+        buf = (C.c_ubyte * (8 * 64 + 12))()
         self.check(self.L.vtp_domain_export_ipc(self.h, C.cast(buf, C.c_void_p)), "vtp_domain_export_ipc")
         return bytes(buf)
 
@@ -421,9 +421,9 @@ class LibraryStages:
         self.check(self.L.vtp_domain_set_halo(self.h, int(bool(on))), "vtp_domain_set_halo")
 
     def parity(self) -> tuple:
-        out = (C.c_int32 * 2)()
+        out = (C.c_int32 * 3)()
         self.check(self.L.vtp_domain_buffer_parity(self.h, out), "vtp_domain_buffer_parity")
-        return int(out[0]), int(out[1])
+        return int(out[0]), int(out[1]), int(out[2])
 
     def rows(self, first: int, count: int):
         out = self.torch.empty(count, dtype=self.torch.int32, device=self.device)
@@ -562,11 +562,11 @@ class DomainRank:
         self.iters = []            # (divergence, density) iterations per substep (PBF: (iterations, 0))
         self.residuals = []
         self.crashed = False
-        # Halo transport: "peer" (DFSPH, library stages, at most 8 ranks): the owners' stage
-        # kernels store ghost values straight into the peers' ghost rows and a fence orders the
-        # peers' next stage; "exchange": pack, send / receive, unpack.
+        # Halo transport: "peer" (library stages, at most 8 ranks): the owners' stage kernels
+        # store ghost values straight into the peers' ghost rows and a fence orders the peers'
+        # next stage; "exchange": pack, send / receive, unpack.
         if halo == "auto":
-            halo = "peer" if (self.kind == "DFSPH" and hasattr(self.stages, "link_local") and 1 < comm.size <= 8
+            halo = "peer" if (hasattr(self.stages, "link_local") and 1 < comm.size <= 8
                               and (isinstance(comm, LoopbackComm) or self._nccl())) else "exchange"
         if halo not in ("peer", "exchange"):
             raise ValueError("halo must be 'auto', 'peer' or 'exchange'")
@@ -699,7 +699,7 @@ class DomainRank:
         return t.cat([self.pos] + gpos), t.cat([self.vel] + gvel), t.cat([self.gid] + ggid), t.cat([self.obj, zeros])
 
     def _exchange(self, field: int):
-        if self.peer_mode and field in (FIELD_KAPPA, FIELD_VADV, FIELD_VEL, FIELD_NORMAL):
+        if self.peer_mode:
             # the stage stored the ghost values into the peers itself; order the peers' next
             # stage after the stores (after solve_b the residual all-reduce does it)
             if field != FIELD_VADV:
@@ -817,6 +817,8 @@ class DomainRank:
         pos, vel, gid, obj = self._ghosts(reach)
         st.load(self.pos.shape[0], pos, vel, gid, obj)
         st.prepare()
+        if self.peer_mode:
+            self._halo_targets()
         for _ in range(self.iterations):
             st.pbf_lambda()
             self._exchange(FIELD_LAMBDA)
