@@ -133,23 +133,31 @@ __global__ void k_dd_row_of_slot(uint32_t n, const float *__restrict__ slot, uin
 }
 
 // Per-object sums of the clamped compression error over the owned rows (load slots below
-// n_own), in FP64: block partials in a fixed order, then one block adds them.
+// n_own), in FP64: block partials in a fixed order, then one block adds them.  NOBJ bounds
+// the objects at compile time so the accumulators stay in registers.
+template <int NOBJ>
 __global__ void __launch_bounds__(kSumThreads) k_dd_sums(uint32_t n, uint32_t n_own, const float *__restrict__ delta,
                                                          const float *__restrict__ slot,
                                                          const float *__restrict__ objf, int nobj,
                                                          double *__restrict__ part) {
-    double acc[kMaxObjects];
+    double acc[NOBJ];
 #pragma unroll
-    for (int o = 0; o < (int)kMaxObjects; ++o) acc[o] = 0.0;
+    for (int o = 0; o < NOBJ; ++o) acc[o] = 0.0;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         if ((uint32_t)slot[r] >= n_own) continue;
-        const int o = (int)objf[r];
         const double d = (double)delta[r];
+        if (NOBJ == 1) {
+            acc[0] += d;
+        } else {
+            const int o = (int)objf[r];
 #pragma unroll
-        for (int k = 0; k < (int)kMaxObjects; ++k)
-            if (k == o) acc[k] += d;
+            for (int k = 0; k < NOBJ; ++k)
+                if (k == o) acc[k] += d;
+        }
     }
-    for (int o = 0; o < nobj; ++o) {
+#pragma unroll
+    for (int o = 0; o < NOBJ; ++o) {
+        if (o >= nobj) break;   // block-uniform
         const double s = block_sum_d(acc[o]);
         if (threadIdx.x == 0) part[(size_t)blockIdx.x * nobj + o] = s;
     }
@@ -645,8 +653,15 @@ int vtp_domain_solve_a(vtp_domain *d, double *d_sums) {
     if (!d_sums) return fail(VTP_ERR_ARG, "null sums");
     const vtp::DfsphArgs a = d->args();
     vtp::dfsph_solve_a(d->st, a, d->s->block);
-    k_dd_sums<<<kSumBlocks, kSumThreads, 0, d->st>>>(d->n_act, d->n_own, a.delta, d->slot.c(), d->objf.c(),
-                                                     (int)d->nobj, d->part);
+    if (d->nobj == 1)
+        k_dd_sums<1><<<kSumBlocks, kSumThreads, 0, d->st>>>(d->n_act, d->n_own, a.delta, d->slot.c(), d->objf.c(), 1,
+                                                            d->part);
+    else if (d->nobj <= 4)
+        k_dd_sums<4><<<kSumBlocks, kSumThreads, 0, d->st>>>(d->n_act, d->n_own, a.delta, d->slot.c(), d->objf.c(),
+                                                            (int)d->nobj, d->part);
+    else
+        k_dd_sums<kMaxObjects><<<kSumBlocks, kSumThreads, 0, d->st>>>(d->n_act, d->n_own, a.delta, d->slot.c(),
+                                                                      d->objf.c(), (int)d->nobj, d->part);
     k_dd_sums_final<<<1, kSumThreads, 0, d->st>>>(kSumBlocks, (int)d->nobj, d->part, d_sums);
     CU(cudaGetLastError());
     return VTP_OK;
