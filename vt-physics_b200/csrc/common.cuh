@@ -220,19 +220,21 @@ __device__ __forceinline__ float cubic_w(float d2, const Cubic &k) {
 }
 
 // Scalar g with gradW(r_vec) = g * r_vec; zero for q < 1e-6 or q > 1.
+// Every rounding is explicit, so g is the same bits in every kernel that
+// evaluates it, whatever the compiler contracts around the call.
 __device__ __forceinline__ float cubic_g(float d2, const Cubic &k) {
     if (!(d2 > 0.f)) return 0.f;   // coincident particles: q < 1e-6 -> 0
-    float rinv = rsqrtf(d2);
-    float r = d2 * rinv;
-    float q = r * k.invh;
+    const float rinv = rsqrtf(d2);
+    const float r = __fmul_rn(d2, rinv);
+    const float q = __fmul_rn(r, k.invh);
     if (q < 1e-6f || q > 1.f) return 0.f;
     float f;
-    if (q <= 0.5f) f = 6.f * q * (3.f * q - 2.f);
+    if (q <= 0.5f) f = __fmul_rn(__fmul_rn(6.f, q), __fmaf_rn(3.f, q, -2.f));
     else {
-        float t = 1.f - q;
-        f = -6.f * t * t;
+        const float t = __fsub_rn(1.f, q);
+        f = __fmul_rn(__fmul_rn(-6.f, t), t);
     }
-    return f * k.sigma * (rinv * k.invh);
+    return __fmul_rn(__fmul_rn(f, k.sigma), __fmul_rn(rinv, k.invh));
 }
 
 // W and g together.
