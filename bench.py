@@ -150,11 +150,12 @@ def ncu_traffic(workload: str, kernel: str):
         return None
 
 
-def ncu_instructions(workload: str, kernel: str):
-    """Warp instructions per launch measured by ncu for this kernel and workload, if recorded."""
+def ncu_counter(group: str, workload: str, kernel: str):
+    """A per-launch ncu counter of this kernel and workload recorded in profiles/ncu_traffic.json
+    under `group` ("warp_instructions", "l1_wavefronts"), if any."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     try:
-        return json.loads(p.read_text()).get("warp_instructions", {}).get(workload, {}).get(kernel)
+        return json.loads(p.read_text()).get(group, {}).get(workload, {}).get(kernel)
     except (OSError, ValueError):
         return None
 
@@ -182,7 +183,7 @@ def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload
     out["fp32"]["ideal_over_hbm"] = t_flops / t_bytes if t_bytes else None
     out.update({"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak})
     out["traffic"] = ncu_traffic(workload, name)
-    inst = ncu_instructions(workload, name)
+    inst = ncu_counter("warp_instructions", workload, name)
     if inst:
         # An issue-bound kernel (the list builder): its warp instructions from one ncu capture
         # over the live launch time, against 4 issue slots per SM per cycle at the sampled clock.
@@ -192,6 +193,17 @@ def roofline_of(name, b, flops, per_launch_ms, peak, peak_kind, clocks, workload
         out["issue"] = {"achieved": rate, "peak": cap, "unit": "G warp-instructions/s", "frac": rate / cap,
                         "instructions_per_launch": inst, "peak_kind": f"computed: 4 x {sms} SMs x {mhz:.0f} MHz",
                         "instructions_from": "profiles/ncu_traffic.json"}
+    wf = ncu_counter("l1_wavefronts", workload, name)
+    if wf:
+        # A gather-bound kernel (the pressure solve): its L1 data-pipe wavefronts (global, local
+        # and shared) from one ncu capture over the live launch time, against one wavefront per
+        # SM per cycle at the sampled clock.
+        sms = 148
+        rate = wf / t / 1e9
+        cap = sms * mhz / 1e3
+        out["l1tex"] = {"achieved": rate, "peak": cap, "unit": "G wavefronts/s", "frac": rate / cap,
+                        "wavefronts_per_launch": wf, "peak_kind": f"computed: 1 x {sms} SMs x {mhz:.0f} MHz",
+                        "wavefronts_from": "profiles/ncu_traffic.json"}
     return out
 
 
