@@ -455,9 +455,20 @@ __global__ void __launch_bounds__(1024) k_solve_end(SolveCtl c, const double *__
     if (!was_stopped) {
         double acc = 0.0;
         for (uint32_t o = 0; o < sct.nobj; ++o) {
+            // Each thread adds the partials b = tid, tid + blockDim, ... in that order; the
+            // loads are issued eight at a time so that their latencies overlap.
             double s = 0.0;
-            for (uint32_t b = threadIdx.x; b < sct.ntiles; b += blockDim.x)
-                s += partials[(size_t)(sct.tile0 + b) * c.nobj_max + o];
+            for (uint32_t b = threadIdx.x; b < sct.ntiles; b += 8u * blockDim.x) {
+                double v[8];
+#pragma unroll
+                for (uint32_t u = 0; u < 8; ++u) {
+                    const uint32_t bb = b + u * blockDim.x;
+                    v[u] = bb < sct.ntiles ? partials[(size_t)(sct.tile0 + bb) * c.nobj_max + o] : 0.0;
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < 8; ++u)
+                    if (b + u * blockDim.x < sct.ntiles) s += v[u];
+            }
             s = block_sum(s);
             if (threadIdx.x == 0) acc += s * c.inv_count[sct.obj0 + o];
         }
