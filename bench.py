@@ -387,7 +387,12 @@ def state_bytes(bufs) -> int:
 
 
 def state_round_trip(s, bufs):
-    """One e2e step: fluid state host -> device, one substep, fluid state device -> host."""
+    """One e2e step: fluid state host -> device, one substep, fluid state device -> host (one
+    library call, vtp_solver_step_state_range, when the fluid is one attach-order range)."""
+    if len(bufs) == 1:
+        first, count, p, v = bufs[0]
+        assert s.step_state_range_ptr(first, count, p.ptr, v.ptr, 1, p.ptr, v.ptr), s.last_error
+        return
     for first, count, p, v in bufs:
         s.set_state_range_ptr(first, count, p.ptr, v.ptr)
     assert s.tickNsteps(1), s.last_error

@@ -311,6 +311,16 @@ VTP_API int vtp_solver_get_state_range(vtp_solver *s, uint32_t first, uint32_t c
 VTP_API int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos,
                                        const float *vel);
 
+/* One host-driven frame in one call: set_state_range(first, count, pos_in,
+ * vel_in), tickNsteps(n_steps), get_state_range(first, count, pos_out,
+ * vel_out) (the reference's setter / Solver::tickNsteps / getter sequence,
+ * Solver.hpp and PBFSolver.cpp:326-376), enqueued in stream order behind one
+ * synchronisation.  The input buffers are read and the output buffers hold
+ * the new state when it returns VTP_OK; on an error the outputs are
+ * unspecified.  count = 0 only ticks. */
+VTP_API int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos_in,
+                                        const float *vel_in, uint32_t n_steps, float *pos_out, float *vel_out);
+
 /* Neighbour lists in the reference's layout (UniformGridNeighborSearch.hpp:
  * 39-51): counts[n_total] (self included, 0 for particles outside the grid)
  * and nbrs[n_total * max_nbr] original indices, self first, UINT32_MAX padded. */

@@ -72,3 +72,37 @@ def test_host_buffers_round_trip_state(vtp_gpu):
     p.free()
     v.free()
     s.destroy()
+
+
+@pytest.mark.parametrize("kind,extra,steps", [("PBF", None, 1), ("PBF", None, 3), ("DFSPH", {"cfl": 0.4}, 1),
+                                              ("DFSPH", {"useGraphs": False}, 2)])
+def test_one_call_frame_equals_set_tick_get(vtp_gpu, kind, extra, steps):
+    """vtp_solver_step_state_range (upload, n substeps, read back, one synchronisation) gives
+    what set_state_range, tickNsteps and get_state_range give one after another, frame after
+    frame, with the output buffers also serving as the next frame's input."""
+    sc = scenes.dam_break(kind, 3000, seed=34)
+    nf = sc.objects[0].n
+    a, b = vtp.solver_from_scene(sc, extra=extra), vtp.solver_from_scene(sc, extra=extra)
+    assert a.initialize() and b.initialize() and a.tickNsteps(2) and b.tickNsteps(2)
+    pa, va = vtp.HostBuffer((nf, 3)), vtp.HostBuffer((nf, 3))
+    pb, vb = vtp.HostBuffer((nf, 3)), vtp.HostBuffer((nf, 3))
+    a.get_state_range_ptr(0, nf, pa.ptr, va.ptr)
+    b.get_state_range_ptr(0, nf, pb.ptr, vb.ptr)
+    for frame in range(3):
+        va.array[:5] *= 0.5     # the host edits the state between frames
+        vb.array[:5] *= 0.5
+        assert a.step_state_range_ptr(0, nf, pa.ptr, va.ptr, steps, pa.ptr, va.ptr), a.last_error
+        b.set_state_range_ptr(0, nf, pb.ptr, vb.ptr)
+        assert b.tickNsteps(steps), b.last_error
+        b.get_state_range_ptr(0, nf, pb.ptr, vb.ptr)
+        assert np.array_equal(pa.array, pb.array) and np.array_equal(va.array, vb.array), frame
+        assert a.stats() == b.stats()
+    assert a.step_state_range_ptr(0, 0, 0, 0, 1, 0, 0) and b.tickNsteps(1)   # count 0 only ticks
+    assert np.array_equal(a.get_field("pos"), b.get_field("pos"))
+    with pytest.raises(vtp.VtpError):
+        a.strict = True
+        a.step_state_range_ptr(nf, sc.n_total, pa.ptr, va.ptr, 1, pa.ptr, va.ptr)
+    for buf in (pa, va, pb, vb):
+        buf.free()
+    a.destroy()
+    b.destroy()

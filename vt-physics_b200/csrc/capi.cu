@@ -931,20 +931,24 @@ int vtp_solver::check_status() {
     CU(cudaMemcpyAsync(h_pinned, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CU(cudaMemcpyAsync(h_pinned + 1, d_overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    stats.status_bits |= h_pinned[0];
-    stats.neighbor_overflow = h_pinned[1];
-    if (h_pinned[0] & vtp::ST_NOT_CONVERGED) {
+    return apply_status(h_pinned[0], h_pinned[1]);
+}
+
+int vtp_solver::apply_status(uint32_t status_bits, uint32_t overflow) {
+    stats.status_bits |= status_bits;
+    stats.neighbor_overflow = overflow;
+    if (status_bits & vtp::ST_NOT_CONVERGED) {
         crashed = true;
         return VTP_NOT_CONVERGED;
     }
-    if (h_pinned[0] & vtp::ST_NAN) {
+    if (status_bits & vtp::ST_NAN) {
         crashed = true;
         return VTP_ERR_NAN;
     }
     return VTP_OK;
 }
 
-int vtp_solver::tick_n(uint32_t n) {
+int vtp_solver::tick_n(uint32_t n, const std::function<int()> &tail) {
     const vtp::NvtxRange nvtx_range("vtp tick");
     int rc;
     if (!initialized && (rc = initialize())) return rc;
@@ -990,8 +994,9 @@ int vtp_solver::tick_n(uint32_t n) {
         }
         ++steps_done;
         if ((rc = maybe_export())) return rc;
-        if (solves && stop_on_crash) {
-            // The reference stops ticking after a solve ran past 100 iterations.
+        if (solves && stop_on_crash && k + 1 < n) {
+            // The reference stops ticking after a solve ran past 100 iterations (the last
+            // substep's status comes back with the end-of-tick readback below).
             if ((rc = check_status())) {
                 stats.steps_done = steps_done;
                 return fail(rc, std::string(solver_key(type)) + ": pressure solve exceeded 100 iterations");
@@ -999,25 +1004,48 @@ int vtp_solver::tick_n(uint32_t n) {
         }
     }
     CU(cudaEventRecord(ev[2], st));
+    if (tail && (rc = tail())) return rc;
+    // What the host reports after the tick comes back in one readback behind one
+    // synchronisation: the status words, the adaptive step, the solve and loop states.
+    const size_t S = scenes.size();
+    const size_t off_solve = 16, off_loop = off_solve + 2 * S * sizeof(vtp::SolveState);
+    const size_t need = off_loop + 2 * sizeof(vtp::LoopState);
+    if (need > h_tick_bytes) {
+        if (h_tick) cudaFreeHost(h_tick), h_tick = nullptr, h_tick_bytes = 0;
+        CU(cudaMallocHost((void **)&h_tick, need));
+        h_tick_bytes = need;
+    }
+    uint32_t *hw = reinterpret_cast<uint32_t *>(h_tick);
+    const vtp::SolveState *hs = reinterpret_cast<const vtp::SolveState *>(h_tick + off_solve);
+    const vtp::LoopState *hl = reinterpret_cast<const vtp::LoopState *>(h_tick + off_loop);
+    CU(cudaMemcpyAsync(hw, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(hw + 1, d_overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (cfl > 0.f) CU(cudaMemcpyAsync(hw + 2, d_cfl, 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (solves) {
+        CU(cudaMemcpyAsync(h_tick + off_solve, solve, 2 * S * sizeof(vtp::SolveState), cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(h_tick + off_loop, loop, 2 * sizeof(vtp::LoopState), cudaMemcpyDeviceToHost, st));
+    }
     CU(cudaStreamSynchronize(st));
     CU(cudaGetLastError());
     CU(cudaEventElapsedTime(&stage_ms[2], ev[0], ev[2]));
     if (cfl > 0.f) {
         float dev[2];
-        CU(cudaMemcpy(dev, d_cfl, sizeof(dev), cudaMemcpyDeviceToHost));
+        std::memcpy(dev, hw + 2, sizeof(dev));
         last_dt = dev[0];
         sim_time = dev[1];
     }
-    if ((rc = check_status())) return fail(rc, "solver status after tick");
-    if (solves) {
-        if ((rc = read_solve_states())) return rc;
-        stats = scene_stats[0];
-        if (use_graphs) {
-            // per solve-loop iteration: solve_a, solve_b, solve_end
-            vtp::LoopState hl[2];
-            CU(cudaMemcpy(hl, loop, sizeof(hl), cudaMemcpyDeviceToHost));
-            launches = (uint64_t)n * launches_per_tick + 3 * (hl[0].total + hl[1].total);
+    if ((rc = apply_status(hw[0], hw[1]))) {
+        if (solves && stop_on_crash) {
+            stats.steps_done = steps_done;
+            return fail(rc, std::string(solver_key(type)) + ": pressure solve exceeded 100 iterations");
         }
+        return fail(rc, "solver status after tick");
+    }
+    if (solves) {
+        fill_solve_stats(hs);
+        stats = scene_stats[0];
+        // per solve-loop iteration: solve_a, solve_b, solve_end
+        if (use_graphs) launches = (uint64_t)n * launches_per_tick + 3 * (hl[0].total + hl[1].total);
     } else if (use_graphs) {
         launches = (uint64_t)n * launches_per_tick;
     }
@@ -1033,10 +1061,8 @@ int vtp_solver::tick_n(uint32_t n) {
     return VTP_OK;
 }
 
-int vtp_solver::read_solve_states() {
+void vtp_solver::fill_solve_stats(const vtp::SolveState *hs) {
     const size_t S = scenes.size();
-    std::vector<vtp::SolveState> hs(2 * S);
-    CU(cudaMemcpy(hs.data(), solve, hs.size() * sizeof(vtp::SolveState), cudaMemcpyDeviceToHost));
     scene_stats.assign(S, stats);
     for (size_t k = 0; k < S; ++k) {
         vtp_stats &o = scene_stats[k];
@@ -1047,7 +1073,6 @@ int vtp_solver::read_solve_states() {
         o.last_div_residual = hs[k].residual;
         o.last_incomp_residual = hs[S + k].residual;
     }
-    return VTP_OK;
 }
 
 // ---------------------------------------------------------------- fields
@@ -1462,6 +1487,31 @@ int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, co
         e = cudaStreamSynchronize(s->st);
     }
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos_in,
+                                const float *vel_in, uint32_t n_steps, float *pos_out, float *vel_out) {
+    if (!s || ((!pos_in || !vel_in || !pos_out || !vel_out) && count)) return fail(VTP_ERR_ARG, "null argument");
+    if (!s->initialized) return fail(VTP_ERR_STATE, "step_state before initialize");
+    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+    if (!count) return s->tick_n(n_steps);
+    const size_t b = (size_t)count * 12;
+    int rc = s->ensure_stage(2 * b);
+    if (rc) return rc;
+    float *p3 = s->stage, *v3 = s->stage + (size_t)count * 3;
+    // set_state_range's copies and row gather, the substeps, get_state_range's row scatter and
+    // copies, all in stream order; the tick's end-of-tick readback synchronises once for all.
+    CU(cudaMemcpyAsync(p3, pos_in, b, cudaMemcpyHostToDevice, s->st));
+    CU(cudaMemcpyAsync(v3, vel_in, b, cudaMemcpyHostToDevice, s->st));
+    vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), first, count, s->pos.c(), s->vel.c(), s->vadv.c());
+    if (s->cfl > 0.f) vtp::dfsph_cfl_refresh(s->st, s->dfsph_args(), s->d_vmax);
+    CU(cudaGetLastError());
+    return s->tick_n(n_steps, [&]() -> int {
+        vtp::scatter_state_range(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), first, count, p3, v3);
+        CU(cudaMemcpyAsync(pos_out, p3, b, cudaMemcpyDeviceToHost, s->st));
+        CU(cudaMemcpyAsync(vel_out, v3, b, cudaMemcpyDeviceToHost, s->st));
+        return VTP_OK;
+    });
 }
 
 int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {

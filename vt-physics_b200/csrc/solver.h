@@ -1,6 +1,7 @@
 // The solver object behind the C ABI handle (shared by capi.cu and immct.cu).
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -143,7 +144,9 @@ struct vtp_solver {
     vtp::SolveState *solve = nullptr;   // [2][S]: divergence, density per scene
     vtp::UgnsBuffers u{};
     uint32_t *d_status = nullptr, *d_overflow = nullptr;
-    uint32_t *h_pinned = nullptr;       // [4] status, overflow, iter, spare
+    uint32_t *h_pinned = nullptr;       // [8] status, overflow, iter, spare
+    uint8_t *h_tick = nullptr;          // end-of-tick readback: status, overflow, CFL step, solve + loop states
+    size_t h_tick_bytes = 0;
     std::shared_ptr<vtp::ImmState> imm;
     std::shared_ptr<vtp::DiffState> diff;
 
@@ -188,6 +191,7 @@ struct vtp_solver {
         if (stage) cudaFree(stage), stage = nullptr, stage_bytes = 0;
         if (d_cons) cudaFree(d_cons), d_cons = nullptr, cons_blocks = 0;
         if (h_pinned) cudaFreeHost(h_pinned), h_pinned = nullptr;
+        if (h_tick) cudaFreeHost(h_tick), h_tick = nullptr, h_tick_bytes = 0;
         for (auto &e : ev)
             if (e) cudaEventDestroy(e), e = nullptr;
         if (st) cudaStreamDestroy(st), st = nullptr;
@@ -214,7 +218,9 @@ struct vtp_solver {
     vtp::Scenes scn() const { return vtp::Scenes{d_sg, row_scene, h, d2max, maxnbr}; }
     int attach(const float *p, uint32_t n, const float *v, const nlohmann::json &o);
     int initialize();
-    int tick_n(uint32_t n);
+    // `tail` enqueues work after the substeps and before the end-of-tick readback, so that the
+    // readback's single synchronisation covers it.
+    int tick_n(uint32_t n, const std::function<int()> &tail = nullptr);
     int enqueue_tick(cudaStream_t s, bool capture);
     int enqueue_pbf_substep(cudaStream_t s, const PbfTapeSlot *tape);
     int enqueue_solve(cudaStream_t s, int which, bool capture);
@@ -226,7 +232,8 @@ struct vtp_solver {
     vtp::DfsphArgs dfsph_args(int which = 0);
     vtp::SolveCtl solve_ctl(int which, cudaGraphConditionalHandle h, int use_cond);
     int check_status();
-    int read_solve_states();
+    int apply_status(uint32_t status_bits, uint32_t overflow);
+    void fill_solve_stats(const vtp::SolveState *hs);
     int export_frame();
     int maybe_export();
     int conservation(int scene, vtp_conservation *out);   // conserve.cu

@@ -68,6 +68,7 @@ SIGNATURES = {
     "vtp_write_ply": (C.c_int, [C.c_char_p, C.c_char_p, _P, C.c_uint64, _P, _P, C.c_int32]),
     "vtp_solver_get_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_set_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
+    "vtp_solver_step_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P]),
     "vtp_solver_get_neighbors": (C.c_int, [_P, _P, _P, C.c_uint32]),
     "vtp_solver_get_sorted_order": (C.c_int, [_P, _P, _P]),
     "vtp_solver_get_stage_times": (C.c_int, [_P, _P]),

@@ -216,6 +216,15 @@ class Solver:
     def get_state_range_ptr(self, first: int, count: int, pos_ptr: int, vel_ptr: int):
         check(lib().vtp_solver_get_state_range(self._h, int(first), int(count), pos_ptr, vel_ptr), "get_state_range")
 
+    def step_state_range_ptr(self, first: int, count: int, pos_in: int, vel_in: int, n: int, pos_out: int,
+                             vel_out: int) -> bool:
+        """One host-driven frame in one call: upload the positions and velocities of particles
+        [first, first + count), advance n substeps, read them back (raw host pointers; in and out
+        may be the same buffers).  False, with last_error, when the substeps fail as tickNsteps
+        does."""
+        return self._call(lib().vtp_solver_step_state_range(self._h, int(first), int(count), pos_in, vel_in, int(n),
+                                                            pos_out, vel_out), "step_state_range")
+
     def get_field_range(self, name: str, first: int, count: int) -> np.ndarray:
         fid, width = FIELDS[name]
         w = width if isinstance(width, int) and width > 0 else 1
