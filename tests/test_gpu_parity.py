@@ -311,6 +311,27 @@ def test_programmatic_launch_gives_identical_trajectories(vtp_gpu):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("scene", ["dam_break", "colliding_blocks", "staged"])
+def test_dfsph_solve_loop_graph_equals_host_loop(vtp_gpu, scene):
+    """The one-scene solve-loop graph runs the stop test beside solve_b: trajectories and
+    iteration counts equal the host-driven loops' (stop test after solve_b), bit for bit,
+    with one and two fluid objects and with the staged solve."""
+    vtp = vtp_gpu
+    sc = vtp.scenes.colliding_blocks() if scene == "colliding_blocks" else vtp.scenes.dam_break("DFSPH", 20000, seed=3)
+    base = {"stagedSolve": True} if scene == "staged" else {}
+    out = []
+    for extra in ({}, {"useGraphs": False}, {"useGraphs": False, "deviceLoop": False}):
+        s = vtp.solver_from_scene(sc, extra=dict(base, **extra))
+        assert s.tickNsteps(15), s.last_error
+        st = s.stats()
+        out.append((s.get_field("pos"), s.get_field("vel"), st["total_div_iters"], st["total_incomp_iters"],
+                    st["last_div_residual"]))
+        s.destroy()
+    for o in out[1:]:
+        assert np.array_equal(o[0], out[0][0]) and np.array_equal(o[1], out[0][1])
+        assert o[2:] == out[0][2:]
+
+
 def test_runs_are_deterministic(vtp_gpu):
     vtp = vtp_gpu
     sc = vtp.scenes.pbf_dam_break()

@@ -517,6 +517,9 @@ int vtp_solver::initialize() {
     if (!st) {
         CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CU(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CU(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         for (auto &e : ev) CU(cudaEventCreate(&e));
         CU(cudaMallocHost((void **)&h_pinned, 8 * sizeof(uint32_t)));
     }
@@ -765,13 +768,28 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         CU(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
         CU(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        if (type == VTP_SOLVER_DFSPH) {
+        if (type == VTP_SOLVER_DFSPH && scenes.size() == 1) {
+            // One scene: the stop test reads only solve_a's residual partials, so it runs as
+            // a second branch beside solve_b.  The loop ends when the scene stops, so solve_b
+            // (the iteration's last velocity update, as in vfsph_div) runs unconditionally.
             vtp::dfsph_solve_a(side, a, block);
-            vtp::dfsph_solve_b(side, a, block);
+            CU(cudaEventRecord(ev_fork, side));
+            CU(cudaStreamWaitEvent(side2, ev_fork, 0));
+            vtp::dfsph_solve_end(side2, solve_ctl(which, hnd, 1), partials, d_status);
+            vtp::DfsphArgs b = a;
+            b.state = nullptr;
+            vtp::dfsph_solve_b(side, b, block);
+            CU(cudaEventRecord(ev_join, side2));
+            CU(cudaStreamWaitEvent(side, ev_join, 0));
         } else {
-            immct_solve_ab(*this, side, which);
+            if (type == VTP_SOLVER_DFSPH) {
+                vtp::dfsph_solve_a(side, a, block);
+                vtp::dfsph_solve_b(side, a, block);
+            } else {
+                immct_solve_ab(*this, side, which);
+            }
+            vtp::dfsph_solve_end(side, solve_ctl(which, hnd, 1), partials, d_status);
         }
-        vtp::dfsph_solve_end(side, solve_ctl(which, hnd, 1), partials, d_status);
         cudaGraph_t out;
         CU(cudaStreamEndCapture(side, &out));
         return VTP_OK;  // the body's 3 launches per iteration are added from the iteration totals

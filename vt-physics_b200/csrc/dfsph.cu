@@ -302,7 +302,7 @@ template <int U>
 __global__ void __launch_bounds__(kStageBlock) k_solve_b_staged(DfsphArgs a) {
     extern __shared__ float4 stage[];
     __shared__ GroupPlan P;
-    if (a.state[0].stopped) return;
+    if (a.state && a.state[0].stopped) return;
     const StepDt T = step_dt(a);
     const uint32_t grp = blockIdx.x;
     const SceneGrid g = a.sc.sg[0];
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     const StepDt T = step_dt(a);
     for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const uint4 tile = a.tiles[t];
-        if (a.state[tile.z].stopped || threadIdx.x >= tile.y) continue;
+        if ((a.state && a.state[tile.z].stopped) || threadIdx.x >= tile.y) continue;
         const uint32_t r = tile.x + threadIdx.x;
         if (halo_ghost(a, r)) continue;
         const float4 p = a.pos[r];

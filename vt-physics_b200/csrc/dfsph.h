@@ -59,7 +59,8 @@ struct DfsphArgs {
     uint32_t ntiles;
     bool persistent;            // persistent grid over the tiles
     const SceneTiles *scene_tiles;  // [S]
-    const SolveState *state;    // [S] states of the running solve (stopped scenes are skipped)
+    const SolveState *state;    // [S] states of the running solve (stopped scenes are skipped); null in
+                                // solve_b: no scene has stopped (a one-scene loop ends when it stops)
     Scenes sc;                  // per-scene gravity
     uint32_t *status;
     uint64_t *tick;             // substep counter, advanced by the finalize pass

@@ -118,6 +118,8 @@ struct vtp_solver {
 
     // device state
     cudaStream_t st = nullptr, side = nullptr;
+    cudaStream_t side2 = nullptr;       // second branch of the one-scene solve-loop body (the stop test)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<SceneRec> scenes;       // scene 0 comes from setConfig, the rest from add_scene
     vtp::SceneGrid *d_sg = nullptr;     // [S]
     uint16_t *row_scene = nullptr;      // [n]
@@ -196,6 +198,9 @@ struct vtp_solver {
             if (e) cudaEventDestroy(e), e = nullptr;
         if (st) cudaStreamDestroy(st), st = nullptr;
         if (side) cudaStreamDestroy(side), side = nullptr;
+        if (side2) cudaStreamDestroy(side2), side2 = nullptr;
+        if (ev_fork) cudaEventDestroy(ev_fork), ev_fork = nullptr;
+        if (ev_join) cudaEventDestroy(ev_join), ev_join = nullptr;
         imm.reset();
         diff.reset();
         graphs_ready = false;
