@@ -311,13 +311,18 @@ def test_programmatic_launch_gives_identical_trajectories(vtp_gpu):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("scene", ["dam_break", "colliding_blocks", "staged"])
+@pytest.mark.parametrize("scene", ["dam_break", "colliding_blocks", "staged", "IMM", "IMMCT"])
 def test_dfsph_solve_loop_graph_equals_host_loop(vtp_gpu, scene):
     """The one-scene solve-loop graph runs the stop test beside solve_b: trajectories and
     iteration counts equal the host-driven loops' (stop test after solve_b), bit for bit,
-    with one and two fluid objects and with the staged solve."""
+    with one and two fluid objects, with the staged solve and for the mixture solvers."""
     vtp = vtp_gpu
-    sc = vtp.scenes.colliding_blocks() if scene == "colliding_blocks" else vtp.scenes.dam_break("DFSPH", 20000, seed=3)
+    if scene in ("IMM", "IMMCT"):
+        sc = vtp.scenes.layered_mixture(scene, 16, seed=3)
+    elif scene == "colliding_blocks":
+        sc = vtp.scenes.colliding_blocks()
+    else:
+        sc = vtp.scenes.dam_break("DFSPH", 20000, seed=3)
     base = {"stagedSolve": True} if scene == "staged" else {}
     out = []
     for extra in ({}, {"useGraphs": False}, {"useGraphs": False, "deviceLoop": False}):

@@ -768,26 +768,23 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         CU(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
         CU(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        if (type == VTP_SOLVER_DFSPH && scenes.size() == 1) {
-            // One scene: the stop test reads only solve_a's residual partials, so it runs as
-            // a second branch beside solve_b.  The loop ends when the scene stops, so solve_b
-            // (the iteration's last velocity update, as in vfsph_div) runs unconditionally.
-            vtp::dfsph_solve_a(side, a, block);
+        if (scenes.size() == 1) {
+            // One scene (every mixture solver, and DFSPH unbatched): the stop test reads only
+            // solve_a's residual partials, so it runs as a second branch beside solve_b.  The
+            // loop ends when the scene stops, so solve_b (the iteration's last velocity
+            // update, as in vfsph_div) runs unconditionally.
+            vtp::DfsphArgs sa = type == VTP_SOLVER_DFSPH ? a : immct_solve_args(*this, which);
+            vtp::dfsph_solve_a(side, sa, block);
             CU(cudaEventRecord(ev_fork, side));
             CU(cudaStreamWaitEvent(side2, ev_fork, 0));
             vtp::dfsph_solve_end(side2, solve_ctl(which, hnd, 1), partials, d_status);
-            vtp::DfsphArgs b = a;
-            b.state = nullptr;
-            vtp::dfsph_solve_b(side, b, block);
+            sa.state = nullptr;
+            vtp::dfsph_solve_b(side, sa, block);
             CU(cudaEventRecord(ev_join, side2));
             CU(cudaStreamWaitEvent(side, ev_join, 0));
         } else {
-            if (type == VTP_SOLVER_DFSPH) {
-                vtp::dfsph_solve_a(side, a, block);
-                vtp::dfsph_solve_b(side, a, block);
-            } else {
-                immct_solve_ab(*this, side, which);
-            }
+            vtp::dfsph_solve_a(side, a, block);
+            vtp::dfsph_solve_b(side, a, block);
             vtp::dfsph_solve_end(side, solve_ctl(which, hnd, 1), partials, d_status);
         }
         cudaGraph_t out;

@@ -1014,9 +1014,14 @@ void immct_color(vtp_solver &s, const float *frac_attach_order, float *rgb) {
         }
 }
 
-void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which) {
+vtp::DfsphArgs immct_solve_args(vtp_solver &s, int which) {
     vtp::DfsphArgs a = s.dfsph_args(which);
     a.rest_density = s.imm->rd;
+    return a;
+}
+
+void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which) {
+    const vtp::DfsphArgs a = immct_solve_args(s, which);
     vtp::dfsph_solve_a(st, a, s.block);
     vtp::dfsph_solve_b(st, a, s.block);
 }

@@ -7,6 +7,7 @@
 
 #include <nlohmann/json.hpp>
 
+#include "dfsph.h"
 #include "internal.h"
 
 struct vtp_solver;
@@ -22,6 +23,9 @@ int immct_alloc(vtp_solver &s);
 int immct_init(vtp_solver &s);
 int immct_enqueue_tick(vtp_solver &s, cudaStream_t st, bool capture);
 void immct_solve_ab(vtp_solver &s, cudaStream_t st, int which);
+// The pressure-solve arguments of a mixture solver: the DFSPH passes' with the per-row rest
+// density (mass = rest density x volume).
+vtp::DfsphArgs immct_solve_args(vtp_solver &s, int which);
 int immct_phase_count(const vtp_solver &s);
 int immct_get_field(vtp_solver &s, int field, float *dev_out, size_t elems);
 void immct_fill_carry(vtp_solver &s, vtp::Carry &carry);
