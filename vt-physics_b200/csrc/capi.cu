@@ -672,6 +672,7 @@ int vtp_solver::initialize() {
         AL(&inv_count, invc.size());
         AL(&obj_of, n);
         AL(&d_tiles, std::max<size_t>(tiles.size(), 1));
+        AL(&d_tile_ran, std::max<size_t>(tiles.size(), 1));
         AL(&d_scene_tiles, S);
         CU(cudaMemcpyAsync(inv_count, invc.data(), invc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(obj_of, objmap.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
@@ -783,9 +784,18 @@ int vtp_solver::enqueue_solve(cudaStream_t s, int which, bool capture) {
             CU(cudaEventRecord(ev_join, side2));
             CU(cudaStreamWaitEvent(side, ev_join, 0));
         } else {
-            vtp::dfsph_solve_a(side, a, block);
-            vtp::dfsph_solve_b(side, a, block);
-            vtp::dfsph_solve_end(side, solve_ctl(which, hnd, 1), partials, d_status);
+            // Batched scenes: the same fork; solve_b follows solve_a's record of the tiles it
+            // ran this iteration, since the stop test beside it may stop a scene whose tiles
+            // this iteration's solve_b must still update.
+            vtp::DfsphArgs sa = a;
+            sa.tile_ran = d_tile_ran;
+            vtp::dfsph_solve_a(side, sa, block);
+            CU(cudaEventRecord(ev_fork, side));
+            CU(cudaStreamWaitEvent(side2, ev_fork, 0));
+            vtp::dfsph_solve_end(side2, solve_ctl(which, hnd, 1), partials, d_status);
+            vtp::dfsph_solve_b(side, sa, block);
+            CU(cudaEventRecord(ev_join, side2));
+            CU(cudaStreamWaitEvent(side, ev_join, 0));
         }
         cudaGraph_t out;
         CU(cudaStreamEndCapture(side, &out));

@@ -158,7 +158,9 @@ __global__ void __launch_bounds__(256) k_solve_a(DfsphArgs a) {
     const StepDt T = step_dt(a);
     for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const uint4 tile = a.tiles[t];
-        if (a.state[tile.z].stopped) continue;
+        const bool stopped = a.state[tile.z].stopped != 0;
+        if (a.tile_ran && threadIdx.x == 0) a.tile_ran[t] = stopped ? 0u : 1u;
+        if (stopped) continue;
         const uint32_t r = tile.x + threadIdx.x;
         double contrib = 0.0;
         int obj = 0;
@@ -373,7 +375,8 @@ __global__ void __launch_bounds__(256) k_solve_b(DfsphArgs a) {
     const StepDt T = step_dt(a);
     for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const uint4 tile = a.tiles[t];
-        if ((a.state && a.state[tile.z].stopped) || threadIdx.x >= tile.y) continue;
+        const bool skip = a.tile_ran ? a.tile_ran[t] == 0u : (a.state && a.state[tile.z].stopped);
+        if (skip || threadIdx.x >= tile.y) continue;
         const uint32_t r = tile.x + threadIdx.x;
         if (halo_ghost(a, r)) continue;
         const float4 p = a.pos[r];

@@ -61,6 +61,9 @@ struct DfsphArgs {
     const SceneTiles *scene_tiles;  // [S]
     const SolveState *state;    // [S] states of the running solve (stopped scenes are skipped); null in
                                 // solve_b: no scene has stopped (a one-scene loop ends when it stops)
+    uint32_t *tile_ran;         // [tiles] or null: solve_a records whether it ran each tile and solve_b
+                                // follows that record, not the stop flags, which the stop test of the
+                                // same iteration may be writing beside solve_b
     Scenes sc;                  // per-scene gravity
     uint32_t *status;
     uint64_t *tick;             // substep counter, advanced by the finalize pass

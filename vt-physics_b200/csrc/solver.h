@@ -126,6 +126,7 @@ struct vtp_solver {
     uint32_t nbuckets = 0;              // cell buckets of all scenes incl. their outside buckets
     float d2max = 0.f;
     uint4 *d_tiles = nullptr;           // scene-offset tiles of the fluid rows
+    uint32_t *d_tile_ran = nullptr;     // batched solve-loop graph: tiles solve_a ran this iteration
     uint32_t ntiles = 0;
     vtp::SceneTiles *d_scene_tiles = nullptr;
     bool staged = false;                // staged solve in use (DFSPH, one scene, bricked order, merge mode 0 / 1)
