@@ -84,8 +84,6 @@ json default_config(int type) {
     return {{solver_key(type), {{"Required", req}, {"Optional", opt}}}, {"EXPORT", exp}};
 }
 
-inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
-
 // Wraps a launch with profiler events when per-kernel timing is active.
 #define PROF(self, name, call)                        \
     do {                                              \

@@ -282,36 +282,36 @@ __device__ __forceinline__ F4x2 ldg8(const float4 *p) {
 // which keeps FP32 accumulation order identical for every U.
 template <int U, class Load, class Use>
 __device__ __forceinline__ void nbr_loop(const uint32_t *__restrict__ lst, uint32_t cnt, Load load, Use use) {
-    if (U <= 1) {
+    if constexpr (U <= 1) {
         for (uint32_t t = 0; t < cnt; ++t) {
             const uint32_t j = __ldcs(lst + (size_t)t * 32u);
             use(j, load(j));
         }
-        return;
-    }
-    using T = decltype(load(0u));
-    uint32_t nxt[U];
+    } else {
+        using T = decltype(load(0u));
+        uint32_t nxt[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) nxt[u] = (uint32_t)u < cnt ? __ldcs(lst + (size_t)u * 32u) : 0u;
-    uint32_t t = 0;
-    for (; t + U <= cnt; t += U) {
-        uint32_t j[U];
+        for (int u = 0; u < U; ++u) nxt[u] = (uint32_t)u < cnt ? __ldcs(lst + (size_t)u * 32u) : 0u;
+        uint32_t t = 0;
+        for (; t + U <= cnt; t += U) {
+            uint32_t j[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) j[u] = nxt[u];
+            for (int u = 0; u < U; ++u) j[u] = nxt[u];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t tt = t + U + (uint32_t)u;
+                nxt[u] = tt < cnt ? __ldcs(lst + (size_t)tt * 32u) : 0u;
+            }
+            T d[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) d[u] = load(j[u]);
+#pragma unroll
+            for (int u = 0; u < U; ++u) use(j[u], d[u]);
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t tt = t + U + (uint32_t)u;
-            nxt[u] = tt < cnt ? __ldcs(lst + (size_t)tt * 32u) : 0u;
+            if (t + (uint32_t)u < cnt) use(nxt[u], load(nxt[u]));
         }
-        T d[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) d[u] = load(j[u]);
-#pragma unroll
-        for (int u = 0; u < U; ++u) use(j[u], d[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-        if (t + (uint32_t)u < cnt) use(nxt[u], load(nxt[u]));
     }
 }
 

@@ -298,30 +298,30 @@ __global__ void __launch_bounds__(256) k_vis(ImmArgs a) {
                         nz = __fmaf_rn(sn, gz, nz);
                     }
                 });
-    if (SPLIT) {
+    if constexpr (SPLIT) {
 #pragma unroll
         for (int k = 0; k < P; ++k) a.acc_tmp[k][r] = make_float4(acc[k].x, acc[k].y, acc[k].z, 0.f);
         a.normal[r] = make_float4(nx, ny, nz, 0.f);
         // rows for the tension pass: {x, V}, {n, rest density}
         a.pk_out[2 * (size_t)r] = p;
         a.pk_out[2 * (size_t)r + 1] = make_float4(nx, ny, nz, a.rd[r]);
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int k = 0; k < P; ++k) {
-        float4 vk = vk_i[k];
-        vk.x = __fmaf_rn(acc[k].x, a.dt, vk.x);
-        vk.y = __fmaf_rn(acc[k].y, a.dt, vk.y);
-        vk.z = __fmaf_rn(acc[k].z, a.dt, vk.z);
-        a.vph[k][r] = vk;
+        for (int k = 0; k < P; ++k) {
+            float4 vk = vk_i[k];
+            vk.x = __fmaf_rn(acc[k].x, a.dt, vk.x);
+            vk.y = __fmaf_rn(acc[k].y, a.dt, vk.y);
+            vk.z = __fmaf_rn(acc[k].z, a.dt, vk.z);
+            a.vph[k][r] = vk;
+        }
+        const float4 o = mix_velocity(a, r, vi);
+        a.vel_alt[r] = o;
+        a.vadv_alt[r] = o;
+        // rows for the conformation pass: {x, V}, {v, m / rho}
+        const float rdr = a.rd[r];
+        a.pk_out[2 * (size_t)r] = p;
+        a.pk_out[2 * (size_t)r + 1] = make_float4(o.x, o.y, o.z, (rdr * p.w) / rdr);
     }
-    const float4 o = mix_velocity(a, r, vi);
-    a.vel_alt[r] = o;
-    a.vadv_alt[r] = o;
-    // rows for the conformation pass: {x, V}, {v, m / rho}
-    const float rdr = a.rd[r];
-    a.pk_out[2 * (size_t)r] = p;
-    a.pk_out[2 * (size_t)r + 1] = make_float4(o.x, o.y, o.z, (rdr * p.w) / rdr);
 }
 
 struct TG {
