@@ -1529,12 +1529,16 @@ int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, c
     vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), first, count, s->pos.c(), s->vel.c(), s->vadv.c());
     if (s->cfl > 0.f) vtp::dfsph_cfl_refresh(s->st, s->dfsph_args(), s->d_vmax);
     CU(cudaGetLastError());
-    return s->tick_n(n_steps, [&]() -> int {
+    rc = s->tick_n(n_steps, [&]() -> int {
         vtp::scatter_state_range(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), first, count, p3, v3);
         CU(cudaMemcpyAsync(pos_out, p3, b, cudaMemcpyDeviceToHost, s->st));
         CU(cudaMemcpyAsync(vel_out, v3, b, cudaMemcpyDeviceToHost, s->st));
         return VTP_OK;
     });
+    // On an error the ticks may have returned before their readback: wait for the queued
+    // copies, so that the input buffers are read (and the outputs no longer written) on return.
+    if (rc) cudaStreamSynchronize(s->st);
+    return rc;
 }
 
 int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
