@@ -311,11 +311,13 @@ def test_programmatic_launch_gives_identical_trajectories(vtp_gpu):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("scene", ["dam_break", "colliding_blocks", "staged", "IMM", "IMMCT"])
+@pytest.mark.parametrize("scene", ["dam_break", "cfl", "colliding_blocks", "staged", "IMM", "IMMCT"])
 def test_dfsph_solve_loop_graph_equals_host_loop(vtp_gpu, scene):
     """The one-scene solve-loop graph runs the stop test beside solve_b: trajectories and
     iteration counts equal the host-driven loops' (stop test after solve_b), bit for bit,
-    with one and two fluid objects, with the staged solve and for the mixture solvers."""
+    with one and two fluid objects, with the staged solve, with an adaptive step that binds
+    (the captured substep computes it on a branch beside the list build) and for the mixture
+    solvers."""
     vtp = vtp_gpu
     if scene in ("IMM", "IMMCT"):
         sc = vtp.scenes.layered_mixture(scene, 16, seed=3)
@@ -323,7 +325,7 @@ def test_dfsph_solve_loop_graph_equals_host_loop(vtp_gpu, scene):
         sc = vtp.scenes.colliding_blocks()
     else:
         sc = vtp.scenes.dam_break("DFSPH", 20000, seed=3)
-    base = {"stagedSolve": True} if scene == "staged" else {}
+    base = {"stagedSolve": True} if scene == "staged" else {"cfl": 0.05} if scene == "cfl" else {}
     out = []
     for extra in ({}, {"useGraphs": False}, {"useGraphs": False, "deviceLoop": False}):
         s = vtp.solver_from_scene(sc, extra=dict(base, **extra))
