@@ -285,6 +285,104 @@ def test_library_domains_follow_the_decomposed_oracle(vtp_gpu, oracle_lib):
     assert np.abs(lib_out["vel"] - ora["vel"]).max() < 1e-4
 
 
+def _ipc_rank(rank, world, port, steps, q, kind):
+    """One process of the CUDA IPC test: the library's stages on cuda:0, peer-store halos
+    linked through IPC handles, exchanges over gloo (device tensors staged through the host,
+    the device synchronised before every collective, so a collective orders the ranks' kernels
+    as NCCL's on the stream would)."""
+    import datetime
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    sys.path[:0] = [str(root), str(root / "vt-physics_b200")]
+    import torch
+    import torch.distributed as dist
+    from vtp import domain as D, scenes as S
+
+    class GlooDeviceComm(D.TorchComm):
+        def exchange(self, sends, recvs):
+            torch.cuda.synchronize()
+            cs = {k: t.cpu() for k, t in sends.items()}
+            cr = {k: torch.empty(t.shape, dtype=t.dtype) for k, t in recvs.items()}
+            super().exchange(cs, cr)
+            for k, t in cr.items():
+                recvs[k].copy_(t)
+            return recvs
+
+        def counts(self, send_counts, device):
+            return super().counts(send_counts, "cpu")
+
+        def _reduce(self, t, op):
+            torch.cuda.synchronize()
+            c = t.cpu()
+            dist.all_reduce(c, op=op)
+            t.copy_(c)
+            return t
+
+        def allreduce_sum(self, t):
+            return self._reduce(t, dist.ReduceOp.SUM)
+
+        def allreduce_max(self, t):
+            return self._reduce(t, dist.ReduceOp.MAX)
+
+        def fence(self, device):
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(0)
+    r = None
+    try:
+        sc = S.colliding_blocks() if kind == "DFSPH" else S.dam_break("PBF", 8000, seed=21, spacing=0.1)
+        arrays = D.scene_arrays(sc)
+        plan = D.plan_slabs(arrays, world)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            r = D.DomainRank(arrays, plan, GlooDeviceComm(), halo="peer")
+            assert r.peer_mode
+            r.step(steps)
+            state = r.state()
+        torch.cuda.synchronize()
+        parts = [None] * world
+        dist.all_gather_object(parts, state)
+        if rank == 0:
+            q.put(D.merge_states(arrays, parts))
+    finally:
+        # every rank's kernels (and their stores into the peers) have finished before any
+        # worker, and the memory its peers map, is released
+        torch.cuda.synchronize()
+        dist.barrier()
+        if r is not None:
+            r.close()
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["DFSPH", "PBF"])
+def test_two_processes_store_halos_through_cuda_ipc(vtp_gpu, kind):
+    """Two ranks as two processes on one GPU, each worker's stage kernels storing the ghost
+    values into the other process's buffers through CUDA IPC mappings (the multi-GPU path,
+    without NVLink): the merged result equals the whole-scene library run bit for bit."""
+    steps = 25 if kind == "DFSPH" else 40
+    sc = scenes.colliding_blocks() if kind == "DFSPH" else scenes.dam_break("PBF", 8000, seed=21, spacing=0.1)
+    pos, vel, iters = _whole_library(sc, steps, {})
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ipc_rank, args=(r, 2, port, steps, q, kind)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = q.get(timeout=600)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    if kind == "DFSPH":
+        assert out["iters"] == iters
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
 @pytest.mark.gpu
 def test_dfsph_1m_in_four_slabs_equals_the_whole_scene(vtp_gpu):
     sc = scenes.dfsph_1m()
