@@ -99,6 +99,14 @@ def test_one_call_frame_equals_set_tick_get(vtp_gpu, kind, extra, steps):
         assert a.stats() == b.stats()
     assert a.step_state_range_ptr(0, 0, 0, 0, 1, 0, 0) and b.tickNsteps(1)   # count 0 only ticks
     assert np.array_equal(a.get_field("pos"), b.get_field("pos"))
+    # no substeps: the state goes in and comes back unchanged
+    a.get_state_range_ptr(0, nf, pa.ptr, va.ptr)
+    pin, vin = pa.array.copy(), va.array.copy()
+    pb.array[:] = 0.0
+    vb.array[:] = 0.0
+    assert a.step_state_range_ptr(0, nf, pa.ptr, va.ptr, 0, pb.ptr, vb.ptr), a.last_error
+    assert np.array_equal(pb.array, pin) and np.array_equal(vb.array, vin)
+    assert a.stats()["steps_done"] == b.stats()["steps_done"]
     with pytest.raises(vtp.VtpError):
         a.strict = True
         a.step_state_range_ptr(nf, sc.n_total, pa.ptr, va.ptr, 1, pa.ptr, va.ptr)
