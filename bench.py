@@ -386,6 +386,26 @@ def state_bytes(bufs) -> int:
     return int(sum(p.nbytes + v.nbytes for _, _, p, v in bufs))
 
 
+def frame_buffers(s, ranges):
+    """Page-locked host buffers holding the state (pos, vel) of several attach-order ranges back
+    to back, filled with the current state."""
+    import vtp
+    total = sum(c for _, c in ranges)
+    p, v = vtp.HostBuffer((total, 3)), vtp.HostBuffer((total, 3))
+    off = 0
+    for first, count in ranges:
+        s.get_state_range_ptr(first, count, p.ptr + 12 * off, v.ptr + 12 * off)
+        off += count
+    return ranges, p, v
+
+
+def frame_round_trip(s, fb):
+    """One e2e step of several ranges: one vtp_solver_step_state_ranges call (upload, one
+    substep, read back, one synchronisation)."""
+    ranges, p, v = fb
+    assert s.step_state_ranges_ptr(ranges, p.ptr, v.ptr, 1, p.ptr, v.ptr), s.last_error
+
+
 def state_round_trip(s, bufs):
     """One e2e step: fluid state host -> device, one substep, fluid state device -> host (one
     library call, vtp_solver_step_state_range, when the fluid is one attach-order range)."""
@@ -480,9 +500,17 @@ def run_batched(args, rank, world, local, dist, torch):
     d_ms, d_n, dom_name, d_kind, d_idx, d_b = max(cands, key=lambda c: c[0])
     roofline = batch_roofline(d_b, d_kind, [mix[k] for k in d_idx], dom_name, d_ms / max(d_n, 1), clocks)
 
-    # e2e through the public API: every batch's whole state (positions and velocities of all
-    # its particles) round-trips through pinned host memory each step (H2D, one substep, D2H).
-    hbuf = [state_buffers(b, [(0, b.counts()["total"])], torch) for _, _, b, _ in batches]
+    # e2e through the public API: every step each batch's fluid state (positions and velocities
+    # of the fluid objects of all its scenes; boundary particles are static scene data) goes
+    # host -> device, one substep runs, and the new state comes back: one
+    # vtp_solver_step_state_ranges call per batch and step.
+    def fluid_of(idx, ranges):
+        out = []
+        for k, (lo, _) in zip(idx, ranges):
+            out += [(lo + f, c) for f, c in fluid_ranges(mix[k])]
+        return out
+
+    hbuf = [frame_buffers(b, fluid_of(idx, ranges)) for _, idx, b, ranges in batches]
     e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 20)
     torch.cuda.synchronize()
     if dist:
@@ -492,10 +520,10 @@ def run_batched(args, rank, world, local, dist, torch):
     failures = []
 
     def e2e_run(k):
-        b, bufs = batches[k][2], hbuf[k]
+        b, fb = batches[k][2], hbuf[k]
         try:
             for _ in range(e2e_steps):
-                state_round_trip(b, bufs)
+                frame_round_trip(b, fb)
         except BaseException as e:
             failures.append(e)
 
@@ -511,7 +539,7 @@ def run_batched(args, rank, world, local, dist, torch):
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_val = nf_all * e2e_steps / float(te.item()) / 1e6
-    io_bytes = int(sum(state_bytes(bufs) for bufs in hbuf))
+    io_bytes = int(sum(p.nbytes + v.nbytes for _, p, v in hbuf))
     for _, _, b, _ in batches:
         b.destroy()
 

@@ -321,6 +321,14 @@ VTP_API int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t c
 VTP_API int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos_in,
                                         const float *vel_in, uint32_t n_steps, float *pos_out, float *vel_out);
 
+/* The same frame for several attach-order ranges [firsts[k], firsts[k] + counts[k]),
+ * ascending and disjoint (e.g. the fluid objects of a batched solver's scenes): the
+ * host buffers hold the ranges' particles back to back (sum of counts x float[3]
+ * each). */
+VTP_API int vtp_solver_step_state_ranges(vtp_solver *s, uint32_t nranges, const uint32_t *firsts,
+                                         const uint32_t *counts, const float *pos_in, const float *vel_in,
+                                         uint32_t n_steps, float *pos_out, float *vel_out);
+
 /* Neighbour lists in the reference's layout (UniformGridNeighborSearch.hpp:
  * 39-51): counts[n_total] (self included, 0 for particles outside the grid)
  * and nbrs[n_total * max_nbr] original indices, self first, UINT32_MAX padded. */

@@ -168,3 +168,55 @@ def test_batched_scenes_follow_the_fp64_oracle(vtp_gpu, oracle_lib, kind):
         dv = np.abs(vel[lo:hi][fm] - o.vel[fm]).max() / max(np.abs(o.vel[fm]).max(), v_floor)
         print(f"{kind} scene {k} ({sc.n_fluid} fluid): pos {dp:.2e} vel {dv:.2e}")
         assert dp < 1e-5 and dv < 1e-4, f"scene {k}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["PBF", "DFSPH"])
+def test_multi_range_frame_equals_per_range_calls(vtp_gpu, kind):
+    """vtp_solver_step_state_ranges on the fluid objects of every scene of a batch (ranges
+    separated by the scenes' boundaries, held back to back on the host) gives what
+    set_state_range per range, tickNsteps and get_state_range per range give."""
+    mix = _pbf_mix() if kind == "PBF" else _dfsph_mix()
+    a, ranges = vtp.solver_from_scenes(mix)
+    b, _ = vtp.solver_from_scenes(mix)
+    assert a.initialize() and b.initialize() and a.tickNsteps(2) and b.tickNsteps(2)
+    fl = []
+    for sc, (lo, _) in zip(mix, ranges):
+        start = lo
+        for o in sc.objects:
+            if o.material == 0:
+                fl.append((start, o.n))
+            start += o.n
+    total = sum(c for _, c in fl)
+    pa, va = vtp.HostBuffer((total, 3)), vtp.HostBuffer((total, 3))
+    off = 0
+    for first, count in fl:
+        a.get_state_range_ptr(first, count, pa.ptr + 12 * off, va.ptr + 12 * off)
+        off += count
+    pb, vb = pa.array.copy(), va.array.copy()
+    for frame in range(3):
+        va.array[::7] *= 0.5
+        vb[::7] *= 0.5
+        assert a.step_state_ranges_ptr(fl, pa.ptr, va.ptr, 1, pa.ptr, va.ptr), a.last_error
+        off = 0
+        for first, count in fl:
+            b.set_state_range_ptr(first, count, pb[off:off + count].ctypes.data, vb[off:off + count].ctypes.data)
+            off += count
+        assert b.tickNsteps(1), b.last_error
+        off = 0
+        for first, count in fl:
+            pc, vc = np.empty((count, 3), np.float32), np.empty((count, 3), np.float32)
+            b.get_state_range_ptr(first, count, pc.ctypes.data, vc.ctypes.data)
+            pb[off:off + count], vb[off:off + count] = pc, vc
+            off += count
+        assert np.array_equal(pa.array, pb) and np.array_equal(va.array, vb), frame
+    assert np.array_equal(a.get_field("pos"), b.get_field("pos"))
+    a.strict = True
+    with pytest.raises(vtp.VtpError, match="ascending and disjoint"):
+        a.step_state_ranges_ptr(fl[::-1], pa.ptr, va.ptr, 1, pa.ptr, va.ptr)
+    with pytest.raises(vtp.VtpError, match="ascending and disjoint"):
+        a.step_state_ranges_ptr([fl[1], (fl[1][0], 1)], pa.ptr, va.ptr, 1, pa.ptr, va.ptr)   # overlapping
+    pa.free()
+    va.free()
+    a.destroy()
+    b.destroy()

@@ -1512,25 +1512,58 @@ int vtp_solver_set_state_range(vtp_solver *s, uint32_t first, uint32_t count, co
     return e == cudaSuccess ? VTP_OK : fail(VTP_ERR_CUDA, cudaGetErrorString(e));
 }
 
-int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos_in,
-                                const float *vel_in, uint32_t n_steps, float *pos_out, float *vel_out) {
-    if (!s || ((!pos_in || !vel_in || !pos_out || !vel_out) && count)) return fail(VTP_ERR_ARG, "null argument");
+int vtp_solver_step_state_ranges(vtp_solver *s, uint32_t nranges, const uint32_t *firsts, const uint32_t *counts,
+                                 const float *pos_in, const float *vel_in, uint32_t n_steps, float *pos_out,
+                                 float *vel_out) {
+    if (!s || (nranges && (!firsts || !counts))) return fail(VTP_ERR_ARG, "null argument");
     if (!s->initialized) return fail(VTP_ERR_STATE, "step_state before initialize");
-    if ((uint64_t)first + count > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
-    if (!count) return s->tick_n(n_steps);
-    const size_t b = (size_t)count * 12;
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < nranges; ++k) {
+        if ((uint64_t)firsts[k] + counts[k] > s->L.n) return fail(VTP_ERR_ARG, "particle range out of bounds");
+        if (k && firsts[k] < (uint64_t)firsts[k - 1] + counts[k - 1])
+            return fail(VTP_ERR_ARG, "particle ranges must be ascending and disjoint");
+        total += counts[k];
+    }
+    if (!total) return s->tick_n(n_steps);
+    if (!pos_in || !vel_in || !pos_out || !vel_out) return fail(VTP_ERR_ARG, "null argument");
+    const size_t b = (size_t)total * 12;
     int rc = s->ensure_stage(2 * b);
     if (rc) return rc;
-    float *p3 = s->stage, *v3 = s->stage + (size_t)count * 3;
+    float *p3 = s->stage, *v3 = s->stage + (size_t)total * 3;
+    // One range goes by value; several through a {first, count, first slot} table on the device.
+    const bool one = nranges == 1;
+    if (!one) {
+        std::vector<uint32_t> tab(3 * (size_t)nranges);
+        uint32_t slot = 0;
+        for (uint32_t k = 0; k < nranges; ++k) {
+            tab[3 * (size_t)k] = firsts[k];
+            tab[3 * (size_t)k + 1] = counts[k];
+            tab[3 * (size_t)k + 2] = slot;
+            slot += counts[k];
+        }
+        if ((rc = s->ensure_ranges(nranges))) return rc;
+        // from pageable memory: the table is copied out before the call returns
+        CU(cudaMemcpyAsync(s->d_ranges, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->st));
+    }
     // set_state_range's copies and row gather, the substeps, get_state_range's row scatter and
     // copies, all in stream order; the tick's end-of-tick readback synchronises once for all.
     CU(cudaMemcpyAsync(p3, pos_in, b, cudaMemcpyHostToDevice, s->st));
     CU(cudaMemcpyAsync(v3, vel_in, b, cudaMemcpyHostToDevice, s->st));
-    vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), first, count, s->pos.c(), s->vel.c(), s->vadv.c());
+    if (one)
+        vtp::gather_state_range(s->st, s->L.nf, p3, v3, s->orig.c(), firsts[0], counts[0], s->pos.c(), s->vel.c(),
+                                s->vadv.c());
+    else
+        vtp::gather_state_ranges(s->st, s->L.nf, p3, v3, s->orig.c(), s->d_ranges, nranges, s->pos.c(), s->vel.c(),
+                                 s->vadv.c());
     if (s->cfl > 0.f) vtp::dfsph_cfl_refresh(s->st, s->dfsph_args(), s->d_vmax);
     CU(cudaGetLastError());
+    const uint32_t first0 = firsts[0], count0 = counts[0];
     rc = s->tick_n(n_steps, [&]() -> int {
-        vtp::scatter_state_range(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), first, count, p3, v3);
+        if (one)
+            vtp::scatter_state_range(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), first0, count0, p3, v3);
+        else
+            vtp::scatter_state_ranges(s->st, s->L.n, s->pos.c(), s->vel.c(), s->orig.c(), s->d_ranges, nranges, p3,
+                                      v3);
         CU(cudaMemcpyAsync(pos_out, p3, b, cudaMemcpyDeviceToHost, s->st));
         CU(cudaMemcpyAsync(vel_out, v3, b, cudaMemcpyDeviceToHost, s->st));
         return VTP_OK;
@@ -1539,6 +1572,11 @@ int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, c
     // copies, so that the input buffers are read (and the outputs no longer written) on return.
     if (rc) cudaStreamSynchronize(s->st);
     return rc;
+}
+
+int vtp_solver_step_state_range(vtp_solver *s, uint32_t first, uint32_t count, const float *pos_in,
+                                const float *vel_in, uint32_t n_steps, float *pos_out, float *vel_out) {
+    return vtp_solver_step_state_ranges(s, 1, &first, &count, pos_in, vel_in, n_steps, pos_out, vel_out);
 }
 
 int vtp_solver_get_neighbors(vtp_solver *s, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {

@@ -121,6 +121,12 @@ void scatter_state_range(cudaStream_t st, uint32_t n, const float4 *pos, const f
                          uint32_t first, uint32_t count, float *p3, float *v3);
 void gather_state_range(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
                         uint32_t first, uint32_t count, float4 *pos, float4 *vel, float4 *vadv);
+// The same for several attach-id ranges held back to back in p3 / v3: tab (device) holds
+// {first, count, first slot} per range, ascending and disjoint.
+void scatter_state_ranges(cudaStream_t st, uint32_t n, const float4 *pos, const float4 *vel, const uint32_t *orig,
+                          const uint32_t *tab, uint32_t nr, float *p3, float *v3);
+void gather_state_ranges(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
+                         const uint32_t *tab, uint32_t nr, float4 *pos, float4 *vel, float4 *vadv);
 void export_neighbors(cudaStream_t st, const Layout &L, uint32_t row0, uint32_t cnt, const uint32_t *nbr,
                       const uint32_t *ncnt, const uint32_t *orig, uint32_t maxnbr, uint32_t *out_cnt,
                       uint32_t *out_nbr);

@@ -164,6 +164,8 @@ struct vtp_solver {
     vtp::Profiler *prof = nullptr;      // set only while vtp_solver_profile_kernels runs
     float *stage = nullptr;             // device staging buffer for field I/O
     size_t stage_bytes = 0;
+    uint32_t *d_ranges = nullptr;       // {first, count, first slot} per range of a multi-range state frame
+    uint32_t ranges_cap = 0;
     float stage_ms[3] = {0, 0, 0};
 
     uint64_t steps_done = 0;
@@ -186,12 +188,22 @@ struct vtp_solver {
         return 0;
     }
 
+    int ensure_ranges(uint32_t nr) {
+        if (nr <= ranges_cap) return 0;
+        if (d_ranges) cudaFree(d_ranges), d_ranges = nullptr, ranges_cap = 0;
+        if (cudaMalloc((void **)&d_ranges, 3 * (size_t)nr * sizeof(uint32_t)) != cudaSuccess)
+            return vtp::fail(VTP_ERR_NOMEM, "range table");
+        ranges_cap = nr;
+        return 0;
+    }
+
     void release() {
         for (int p = 0; p < 2; ++p)
             if (gexec[p]) cudaGraphExecDestroy(gexec[p]), gexec[p] = nullptr;
         for (void *a : allocs) cudaFree(a);
         allocs.clear();
         if (stage) cudaFree(stage), stage = nullptr, stage_bytes = 0;
+        if (d_ranges) cudaFree(d_ranges), d_ranges = nullptr, ranges_cap = 0;
         if (d_cons) cudaFree(d_cons), d_cons = nullptr, cons_blocks = 0;
         if (h_pinned) cudaFreeHost(h_pinned), h_pinned = nullptr;
         if (h_tick) cudaFreeHost(h_tick), h_tick = nullptr, h_tick_bytes = 0;

@@ -777,6 +777,57 @@ __global__ void k_gather_state_range(uint32_t n, const float *__restrict__ p3, c
     }
 }
 
+// Slot of attach id `id` in buffers that hold several particle ranges back to back:
+// tab[3k], tab[3k + 1], tab[3k + 2] = first, count, first slot of range k, the ranges
+// ascending and disjoint; ~0u outside every range.
+__device__ __forceinline__ uint32_t range_slot(uint32_t id, const uint32_t *__restrict__ tab, uint32_t nr) {
+    uint32_t lo = 0, hi = nr;   // the first range that starts after id
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tab[3 * mid] <= id) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0) return ~0u;
+    const uint32_t k = lo - 1, d = id - tab[3 * k];
+    return d < tab[3 * k + 1] ? tab[3 * k + 2] + d : ~0u;
+}
+
+__global__ void k_scatter_state_ranges(uint32_t n, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
+                                       const uint32_t *__restrict__ orig, const uint32_t *__restrict__ tab,
+                                       uint32_t nr, float *__restrict__ p3, float *__restrict__ v3) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = range_slot(orig[i], tab, nr);
+    if (id == ~0u) return;
+    const float4 p = pos[i], v = vel[i];
+    p3[3 * (size_t)id] = p.x;
+    p3[3 * (size_t)id + 1] = p.y;
+    p3[3 * (size_t)id + 2] = p.z;
+    v3[3 * (size_t)id] = v.x;
+    v3[3 * (size_t)id + 1] = v.y;
+    v3[3 * (size_t)id + 2] = v.z;
+}
+
+__global__ void k_gather_state_ranges(uint32_t n, const float *__restrict__ p3, const float *__restrict__ v3,
+                                      const uint32_t *__restrict__ orig, const uint32_t *__restrict__ tab,
+                                      uint32_t nr, float4 *__restrict__ pos, float4 *__restrict__ vel,
+                                      float4 *__restrict__ vadv) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = range_slot(orig[i], tab, nr);
+    if (id == ~0u) return;
+    float4 p = pos[i], v = vel[i];
+    p.x = p3[3 * (size_t)id]; p.y = p3[3 * (size_t)id + 1]; p.z = p3[3 * (size_t)id + 2];
+    v.x = v3[3 * (size_t)id]; v.y = v3[3 * (size_t)id + 1]; v.z = v3[3 * (size_t)id + 2];
+    pos[i] = p;
+    vel[i] = v;
+    if (vadv) {
+        float4 w = vadv[i];
+        w.x = v.x; w.y = v.y; w.z = v.z;
+        vadv[i] = w;
+    }
+}
+
 __global__ void k_iota(uint32_t n, uint32_t *dst, uint32_t base) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = base + i;
@@ -992,6 +1043,14 @@ void scatter_state_range(cudaStream_t st, uint32_t n, const float4 *pos, const f
 void gather_state_range(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
                         uint32_t first, uint32_t count, float4 *pos, float4 *vel, float4 *vadv) {
     if (n) k_gather_state_range<<<nblk(n, 256), 256, 0, st>>>(n, p3, v3, orig, first, count, pos, vel, vadv);
+}
+void scatter_state_ranges(cudaStream_t st, uint32_t n, const float4 *pos, const float4 *vel, const uint32_t *orig,
+                          const uint32_t *tab, uint32_t nr, float *p3, float *v3) {
+    if (n) k_scatter_state_ranges<<<nblk(n, 256), 256, 0, st>>>(n, pos, vel, orig, tab, nr, p3, v3);
+}
+void gather_state_ranges(cudaStream_t st, uint32_t n, const float *p3, const float *v3, const uint32_t *orig,
+                         const uint32_t *tab, uint32_t nr, float4 *pos, float4 *vel, float4 *vadv) {
+    if (n) k_gather_state_ranges<<<nblk(n, 256), 256, 0, st>>>(n, p3, v3, orig, tab, nr, pos, vel, vadv);
 }
 void fill_iota(cudaStream_t st, uint32_t n, uint32_t *dst, uint32_t base) {
     if (n) k_iota<<<nblk(n, 256), 256, 0, st>>>(n, dst, base);

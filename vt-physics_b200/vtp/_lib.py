@@ -69,6 +69,7 @@ SIGNATURES = {
     "vtp_solver_get_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_set_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "vtp_solver_step_state_range": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P]),
+    "vtp_solver_step_state_ranges": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, C.c_uint32, _P, _P]),
     "vtp_solver_get_neighbors": (C.c_int, [_P, _P, _P, C.c_uint32]),
     "vtp_solver_get_sorted_order": (C.c_int, [_P, _P, _P]),
     "vtp_solver_get_stage_times": (C.c_int, [_P, _P]),

@@ -225,6 +225,15 @@ class Solver:
         return self._call(lib().vtp_solver_step_state_range(self._h, int(first), int(count), pos_in, vel_in, int(n),
                                                             pos_out, vel_out), "step_state_range")
 
+    def step_state_ranges_ptr(self, ranges, pos_in: int, vel_in: int, n: int, pos_out: int, vel_out: int) -> bool:
+        """step_state_range_ptr for several attach-order ranges [(first, count), ...], ascending and
+        disjoint, whose particles the host buffers hold back to back."""
+        firsts = (C.c_uint32 * max(len(ranges), 1))(*[int(f) for f, _ in ranges])
+        counts = (C.c_uint32 * max(len(ranges), 1))(*[int(c) for _, c in ranges])
+        return self._call(lib().vtp_solver_step_state_ranges(self._h, len(ranges), C.cast(firsts, C.c_void_p),
+                                                             C.cast(counts, C.c_void_p), pos_in, vel_in, int(n),
+                                                             pos_out, vel_out), "step_state_ranges")
+
     def get_field_range(self, name: str, first: int, count: int) -> np.ndarray:
         fid, width = FIELDS[name]
         w = width if isinstance(width, int) and width > 0 else 1
