@@ -74,6 +74,12 @@ def lib() -> C.CDLL:
                                           C.POINTER(C.c_double)]
         L.or_dfsph_solve_op.argtypes = [C.c_uint32, P, P, P, P, P, P, C.c_uint32, C.c_double, C.c_double, C.c_int,
                                          P, P]
+        L.or_dfsph_step_frozen.restype = None
+        L.or_dfsph_step_frozen.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph),
+                                           C.c_int, C.c_int]
+        L.or_dfsph_step_adjoint.restype = None
+        L.or_dfsph_step_adjoint.argtypes = [C.c_uint32, P, P, P, P, P, P, P, C.c_uint32, C.POINTER(OrDfsph),
+                                            C.c_int, C.c_int, P, P, C.POINTER(C.c_double)]
         L.or_imm_init.argtypes = [C.c_uint32, P, P, P, C.POINTER(OrGrid), C.POINTER(OrImm)]
         L.or_imm_step.argtypes = [C.c_uint32, P, P, C.c_int32, P, P, P, P, P, P, P, P, C.POINTER(OrGrid),
                                   C.POINTER(OrImm), C.POINTER(OrImmOut)]
@@ -385,6 +391,66 @@ class PbfDiff:
             cnt, nb = used[t]
             lib().or_pbf_step_adjoint(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.mass), _ptr(b.vol), _ptr(cnt),
                                       _ptr(nb), self.maxnbr, C.byref(self.p), _ptr(xb), _ptr(vb), C.byref(kb))
+        return xb, vb, kb.value
+
+
+class DfsphDiff:
+    """FP64 differentiable DFSPH rollout with frozen neighbour lists and iteration counts
+    (test infrastructure; no counterpart in the reference).
+
+    ``rollout`` advances (pos, vel) ``steps`` substeps (DFSPHSolver.cpp:339-406, surface
+    tension off); substep t uses ``lists[t]`` = (counts, nbrs) in the reference layout (e.g.
+    the GPU's lists of the same trajectory) or lists built from the FP32-rounded positions,
+    and exactly ``iters[t]`` = (divergence, density) pressure-solve iterations.  ``adjoint``
+    runs or_dfsph_step_adjoint backwards over a recorded rollout and returns
+    dL/d(pos0, vel0, fPartRestViscosity).
+    """
+
+    def __init__(self, scene, viscosity: float | None = None):
+        self.base = OracleSolver(scene)
+        if viscosity is not None:
+            self.base.p.vis = float(viscosity)
+        self.p = self.base.p
+        self.maxnbr = int(self.base.grid.maxnbr)
+        b = self.base
+        self.mass = np.where(b.mat == 0, b.rest_density * b.vol, 0.0).astype(np.float64)
+
+    @property
+    def fluid(self):
+        return self.base.mat == 0
+
+    def lists_of(self, pos):
+        cnt, nb, _, _ = neighbors(np.asarray(pos).astype(np.float32), self.base.grid)
+        return cnt, nb
+
+    def rollout(self, pos0, vel0, steps: int, iters, lists=None, record: bool = False):
+        b = self.base
+        pos = np.ascontiguousarray(pos0, np.float64).copy()
+        vel = np.ascontiguousarray(vel0, np.float64).copy()
+        states, used = [], []
+        for t in range(steps):
+            cnt, nb = lists[t] if lists is not None else self.lists_of(pos)
+            cnt = np.ascontiguousarray(cnt, np.uint32)
+            nb = np.ascontiguousarray(nb, np.uint32)
+            di, ii = (int(x) for x in iters[t])
+            if record:
+                states.append((pos.copy(), vel.copy()))
+                used.append((cnt, nb, di, ii))
+            lib().or_dfsph_step_frozen(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.vol), _ptr(self.mass),
+                                       _ptr(cnt), _ptr(nb), self.maxnbr, C.byref(self.p), di, ii)
+        return pos, vel, states, used
+
+    def adjoint(self, states, used, xbar, vbar):
+        b = self.base
+        xb = np.ascontiguousarray(xbar, np.float64).copy()
+        vb = np.ascontiguousarray(vbar, np.float64).copy()
+        kb = C.c_double(0.0)
+        for t in range(len(states) - 1, -1, -1):
+            pos, vel = states[t]
+            cnt, nb, di, ii = used[t]
+            lib().or_dfsph_step_adjoint(b.n, _ptr(b.mat), _ptr(pos), _ptr(vel), _ptr(b.vol), _ptr(self.mass),
+                                        _ptr(cnt), _ptr(nb), self.maxnbr, C.byref(self.p), di, ii, _ptr(xb),
+                                        _ptr(vb), C.byref(kb))
         return xb, vb, kb.value
 
 

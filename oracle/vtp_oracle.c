@@ -971,6 +971,260 @@ void or_dfsph_solve_op(uint32_t n, const int32_t *mat, const double *pos, const 
     free(mass); free(ratio); free(alpha); free(kappa); free(mask);
 }
 
+/* ------------------------------------------------------------------ differentiable DFSPH substep */
+
+/* One DFSPH substep (DFSPHSolver::tick, DFSPHSolver.cpp:339-406, surface tension off) over
+ * frozen lists with exactly div_iters / inc_iters iterations of the two pressure solves.
+ * With a tape, every quantity the adjoint reads is recorded: VS*[it] = v* entering iteration
+ * it, KA*[it] = its kappa, VP = the velocity after the divergence solve, ALPHA, A1 (the
+ * unclamped alpha's gradient sum). */
+typedef struct {
+    double *VSd, *KAd, *VSi, *KAi, *VP, *ALPHA, *A1;
+} df_tape;
+
+static void dfsph_frozen(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vol,
+                         const double *mass, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                         const or_dfsph_params *p, int div_iters, int inc_iters, df_tape *T) {
+    const double dt = p->dt;
+    const size_t nn = n ? n : 1, n3 = 3 * nn;
+    cubic_t k = cubic_make(p->h);
+    double *ratio = (double *)calloc(nn, sizeof(double));
+    double *alpha = (double *)calloc(nn, sizeof(double));
+    double *vadv = (double *)malloc(sizeof(double) * n3);
+    double *kappa = (double *)calloc(nn, sizeof(double));
+    double *delta = (double *)calloc(nn, sizeof(double));
+    double *acc = (double *)calloc(n3, sizeof(double));
+    double *nrm = (double *)calloc(n3, sizeof(double));
+    double *rest = (double *)calloc(nn, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) rest[i] = vol[i] > 0 ? mass[i] / vol[i] : 0.0;
+    or_dfsph_ratio_alpha(n, mat, pos, vol, mass, cnt, nbr, maxnbr, p->h, ratio, alpha);
+    if (T) {
+        memcpy(T->ALPHA, alpha, sizeof(double) * n);
+#pragma omp parallel for
+        for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            double a1[3] = {0, 0, 0}, r[3];
+            if (mat[i] == 0) {
+                FOR_LIST(cnt, nbr, maxnbr, i, j) {
+                    double gg = cubic_g(&k, rdiff(pos, i, j, r));
+                    for (int a = 0; a < 3; ++a) a1[a] += vol[j] * gg * r[a];
+                }
+            }
+            for (int a = 0; a < 3; ++a) T->A1[3 * (size_t)i + a] = a1[a];
+        }
+    }
+    memcpy(vadv, vel, sizeof(double) * 3 * n);
+    for (int s = 0; s < 2; ++s) {
+        const int iters = s == 0 ? div_iters : inc_iters;
+        for (int it = 0; it < iters; ++it) {
+            if (T) memcpy((s == 0 ? T->VSd : T->VSi) + n3 * it, vadv, sizeof(double) * 3 * n);
+            or_dfsph_solve_a(n, mat, pos, vol, ratio, alpha, vadv, cnt, nbr, maxnbr, p->h, dt, delta, kappa);
+            if (T) memcpy((s == 0 ? T->KAd : T->KAi) + nn * it, kappa, sizeof(double) * n);
+            or_dfsph_solve_b(n, mat, pos, vol, mass, kappa, cnt, nbr, maxnbr, p->h, dt, vadv);
+        }
+        if (s == 0) {
+            or_dfsph_pressure_apply(n, mat, vel, vadv, dt);
+            if (T) memcpy(T->VP, vel, sizeof(double) * 3 * n);
+            or_dfsph_forces(n, mat, pos, vel, mass, rest, cnt, nbr, maxnbr, p, acc, nrm);
+            or_dfsph_accelerate(n, mat, vel, vadv, acc, dt);
+        }
+    }
+    or_dfsph_advance(n, mat, pos, vel, vadv, dt);
+    free(ratio); free(alpha); free(vadv); free(kappa); free(delta); free(acc); free(nrm); free(rest);
+}
+
+void or_dfsph_step_frozen(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vol,
+                          const double *mass, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                          const or_dfsph_params *p, int div_iters, int inc_iters) {
+    dfsph_frozen(n, mat, pos, vel, vol, mass, cnt, nbr, maxnbr, p, div_iters, inc_iters, NULL);
+}
+
+/* Adjoint of one pressure-solve iteration v' = v - B(x) kappa, kappa_i = P_i max(0, ratio_i - 1
+ * + (A(x) v)_i) (DFSPHCudaImpl.cu:142-220): vb (adjoint of v') becomes the adjoint of v; the
+ * position adjoint and the adjoints of ratio and alpha are accumulated.  J_ij = g I + hh r r^T
+ * is the Jacobian of gradW_ij = g r with respect to r = x_i - x_j. */
+static void dfsph_iter_adjoint(uint32_t n, const int32_t *mat, const double *pos, const double *vol,
+                               const double *mass, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                               const cubic_t *k, double dt, const double *alpha, const double *vs,
+                               const double *kap, double *vb, double *xb, double *rb, double *ab, double *db) {
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        db[i] = 0.0;
+        if (mat[i] != 0) continue;
+        const double ci = dt * vol[i] / mass[i];
+        double kb = 0, xa[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            if (j == i) continue;
+            const double rl = rdiff(pos, i, j, r);
+            const double g = cubic_g(k, rl), hh = cubic_hh(k, rl);
+            const int fj = mat[j] == 0;
+            const double kj = fj ? kap[j] : 0.0;
+            double w[3], rw = 0;   /* w = c_j V_i vb_j - c_i V_j vb_i */
+            for (int a = 0; a < 3; ++a) {
+                w[a] = (fj ? dt * vol[j] / mass[j] * vol[i] * vb[3 * (size_t)j + a] : 0.0) -
+                       ci * vol[j] * vb[3 * (size_t)i + a];
+                rw += r[a] * w[a];
+            }
+            kb += g * rw;
+            const double kk = kap[i] + kj;
+            for (int a = 0; a < 3; ++a) xa[a] += kk * (g * w[a] + hh * r[a] * rw);
+        }
+        for (int a = 0; a < 3; ++a) xb[3 * (size_t)i + a] += xa[a];
+        const double P = 1.0 / (alpha[i] * dt * dt * vol[i]);
+        db[i] = kap[i] > 0 ? kb * P : 0.0;
+        ab[i] -= kb * kap[i] / alpha[i];
+        rb[i] += db[i];
+    }
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double va[3] = {0, 0, 0}, xa[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            if (j == i) continue;
+            const double rl = rdiff(pos, i, j, r);
+            const double g = cubic_g(k, rl), hh = cubic_hh(k, rl);
+            const double c = dt * (vol[j] * db[i] + (mat[j] == 0 ? vol[i] * db[j] : 0.0));
+            double u[3], ru = 0;
+            for (int a = 0; a < 3; ++a) {
+                u[a] = vs[3 * (size_t)i + a] - vs[3 * (size_t)j + a];
+                ru += r[a] * u[a];
+            }
+            for (int a = 0; a < 3; ++a) {
+                va[a] += c * g * r[a];
+                xa[a] += c * (g * u[a] + hh * r[a] * ru);
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            vb[3 * (size_t)i + a] += va[a];
+            xb[3 * (size_t)i + a] += xa[a];
+        }
+    }
+}
+
+void or_dfsph_step_adjoint(uint32_t n, const int32_t *mat, const double *pos_in, const double *vel_in,
+                           const double *vol, const double *mass, const uint32_t *cnt, const uint32_t *nbr,
+                           uint32_t maxnbr, const or_dfsph_params *p, int div_iters, int inc_iters, double *xbar,
+                           double *vbar, double *visbar) {
+    const double dt = p->dt;
+    const size_t nn = n ? n : 1, n3 = 3 * nn;
+    cubic_t k = cubic_make(p->h);
+    df_tape T;
+    T.VSd = (double *)malloc(sizeof(double) * n3 * (div_iters > 0 ? div_iters : 1));
+    T.VSi = (double *)malloc(sizeof(double) * n3 * (inc_iters > 0 ? inc_iters : 1));
+    T.KAd = (double *)malloc(sizeof(double) * nn * (div_iters > 0 ? div_iters : 1));
+    T.KAi = (double *)malloc(sizeof(double) * nn * (inc_iters > 0 ? inc_iters : 1));
+    T.VP = (double *)malloc(sizeof(double) * n3);
+    T.ALPHA = (double *)malloc(sizeof(double) * nn);
+    T.A1 = (double *)malloc(sizeof(double) * n3);
+    double *x = (double *)malloc(sizeof(double) * n3);
+    double *v = (double *)malloc(sizeof(double) * n3);
+    memcpy(x, pos_in, sizeof(double) * 3 * n);
+    memcpy(v, vel_in, sizeof(double) * 3 * n);
+    dfsph_frozen(n, mat, x, v, vol, mass, cnt, nbr, maxnbr, p, div_iters, inc_iters, &T);
+    const double *pos = pos_in;
+    double *xb = (double *)calloc(n3, sizeof(double));
+    double *vb = (double *)calloc(n3, sizeof(double));
+    double *vb2 = (double *)calloc(n3, sizeof(double));
+    double *rb = (double *)calloc(nn, sizeof(double));
+    double *ab = (double *)calloc(nn, sizeof(double));
+    double *db = (double *)calloc(nn, sizeof(double));
+    double *a1b = (double *)calloc(n3, sizeof(double));
+    /* position update: x' = x + dt v', v' = v* of the density solve */
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mat[i] != 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            xb[3 * (size_t)i + a] = xbar[3 * (size_t)i + a];
+            vb[3 * (size_t)i + a] = vbar[3 * (size_t)i + a] + dt * xbar[3 * (size_t)i + a];
+        }
+    }
+    for (int it = inc_iters - 1; it >= 0; --it)
+        dfsph_iter_adjoint(n, mat, pos, vol, mass, cnt, nbr, maxnbr, &k, dt, T.ALPHA, T.VSi + n3 * it,
+                           T.KAi + nn * it, vb, xb, rb, ab, db);
+    /* gravity + viscosity (dfsph_gravity_vis_surface, DFSPHCudaImpl.cu:523-554):
+     * v' = vp + dt (g + sum_j C (u.r) phi r), u = vp_i - vp_j, phi = g/(|r|^2 + 0.001 h^2),
+     * C = 10 nu m_j / rho_j (fluid neighbours only) */
+    const double eps = 0.001 * p->h * p->h;
+    double vsum = 0.0;
+#pragma omp parallel for reduction(+ : vsum)
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        for (int a = 0; a < 3; ++a) vb2[3 * (size_t)i + a] = vb[3 * (size_t)i + a];
+        if (mat[i] != 0) continue;
+        double va[3] = {0, 0, 0}, xa[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            if (j == i || mat[j] != 0) continue;
+            const double rl = rdiff(pos, i, j, r);
+            const double d2 = rl * rl;
+            const double g = cubic_g(&k, rl), hh = cubic_hh(&k, rl);
+            const double C = 10.0 * p->vis * mass[j] / (mass[j] / vol[j]);
+            const double phi = g / (d2 + eps);
+            const double psi = hh / (d2 + eps) - 2.0 * g / ((d2 + eps) * (d2 + eps));
+            double u[3], w[3], ru = 0, rw = 0, uw = 0;
+            for (int a = 0; a < 3; ++a) {
+                u[a] = T.VP[3 * (size_t)i + a] - T.VP[3 * (size_t)j + a];
+                w[a] = vb[3 * (size_t)i + a] - vb[3 * (size_t)j + a];
+                ru += r[a] * u[a];
+                rw += r[a] * w[a];
+            }
+            for (int a = 0; a < 3; ++a) {
+                va[a] += dt * C * phi * r[a] * rw;
+                xa[a] += dt * C * (phi * u[a] * rw + ru * (phi * w[a] + psi * r[a] * rw));
+                uw += vb[3 * (size_t)i + a] * r[a];
+            }
+            vsum += dt * 10.0 * mass[j] / (mass[j] / vol[j]) * ru * phi * uw;
+        }
+        for (int a = 0; a < 3; ++a) {
+            vb2[3 * (size_t)i + a] += va[a];
+            xb[3 * (size_t)i + a] += xa[a];
+        }
+    }
+    if (visbar) *visbar += vsum;
+    for (int it = div_iters - 1; it >= 0; --it)
+        dfsph_iter_adjoint(n, mat, pos, vol, mass, cnt, nbr, maxnbr, &k, dt, T.ALPHA, T.VSd + n3 * it,
+                           T.KAd + nn * it, vb2, xb, rb, ab, db);
+    /* compression ratio and alpha (DFSPHCudaImpl.cu:85-140): ratio_i = sum_j V_j W_ij,
+     * alpha_i = max(|a1_i|^2 / m_i + 1e-6 + sum_{fluid j} V_j^2 |gradW_ij|^2 / m_j, 1e-6),
+     * a1_i = sum_j V_j gradW_ij */
+    for (uint32_t i = 0; i < n; ++i) {
+        const int live = mat[i] == 0 && T.ALPHA[i] > 1e-6;
+        if (!live) ab[i] = 0.0;
+        for (int a = 0; a < 3; ++a) a1b[3 * (size_t)i + a] = live ? ab[i] * 2.0 * T.A1[3 * (size_t)i + a] / mass[i] : 0.0;
+    }
+#pragma omp parallel for
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint32_t i = (uint32_t)ii;
+        if (mat[i] != 0) continue;
+        double xa[3] = {0, 0, 0}, r[3];
+        FOR_LIST(cnt, nbr, maxnbr, i, j) {
+            if (j == i) continue;
+            const double rl = rdiff(pos, i, j, r);
+            const double g = cubic_g(&k, rl), hh = cubic_hh(&k, rl);
+            const int fj = mat[j] == 0;
+            const double cr = rb[i] * vol[j] + (fj ? rb[j] * vol[i] : 0.0);
+            double w[3], rw = 0;
+            for (int a = 0; a < 3; ++a) {
+                w[a] = vol[j] * a1b[3 * (size_t)i + a] - (fj ? vol[i] * a1b[3 * (size_t)j + a] : 0.0);
+                rw += r[a] * w[a];
+            }
+            const double c2 = fj ? 2.0 * g * (g + hh * rl * rl) *
+                                       (ab[i] * vol[j] * vol[j] / mass[j] + ab[j] * vol[i] * vol[i] / mass[i])
+                                 : 0.0;
+            for (int a = 0; a < 3; ++a) xa[a] += (cr * g + c2) * r[a] + g * w[a] + hh * r[a] * rw;
+        }
+        for (int a = 0; a < 3; ++a) xb[3 * (size_t)i + a] += xa[a];
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            xbar[3 * (size_t)i + a] = mat[i] == 0 ? xb[3 * (size_t)i + a] : 0.0;
+            vbar[3 * (size_t)i + a] = mat[i] == 0 ? vb2[3 * (size_t)i + a] : 0.0;
+        }
+    }
+    free(T.VSd); free(T.VSi); free(T.KAd); free(T.KAi); free(T.VP); free(T.ALPHA); free(T.A1);
+    free(x); free(v); free(xb); free(vb); free(vb2); free(rb); free(ab); free(db); free(a1b);
+}
+
 /* ------------------------------------------------------------------ IMM / IMM-CT */
 
 #define V3(a, i) (&(a)[3 * (size_t)(i)])

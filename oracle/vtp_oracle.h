@@ -101,6 +101,22 @@ void or_dfsph_solve_op(uint32_t n, const int32_t *mat, const double *pos, const 
                        const double *rest_density, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
                        double h, double dt, int iters, double *vadv, double *vbar);
 
+/* Differentiable DFSPH substep (no counterpart in the reference): one substep
+ * (DFSPHSolver.cpp:339-406, surface tension off) over frozen lists (cnt[n],
+ * nbr[n * maxnbr], layout of or_neighbors) with exactly div_iters / inc_iters
+ * pressure-solve iterations; mass = rest_density * vol for fluid particles.
+ * or_dfsph_step_adjoint recomputes that substep from (pos, vel) and maps the
+ * adjoint of its output state (xbar, vbar, in place) to the adjoint of its input
+ * state, the clamp patterns of the forward held fixed; *visbar accumulates
+ * dL/d(fPartRestViscosity). */
+void or_dfsph_step_frozen(uint32_t n, const int32_t *mat, double *pos, double *vel, const double *vol,
+                          const double *mass, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                          const or_dfsph_params *p, int div_iters, int inc_iters);
+void or_dfsph_step_adjoint(uint32_t n, const int32_t *mat, const double *pos, const double *vel, const double *vol,
+                           const double *mass, const uint32_t *cnt, const uint32_t *nbr, uint32_t maxnbr,
+                           const or_dfsph_params *p, int div_iters, int inc_iters, double *xbar, double *vbar,
+                           double *visbar);
+
 /* DFSPH (DFSPHSolver.cpp:339-406): obj[n] gives each particle's object index
  * and obj_is_fluid/obj_count describe the objects (residual = mean over fluid
  * objects of the object's mean clamped compression error). */
