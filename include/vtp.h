@@ -363,27 +363,35 @@ VTP_API int vtp_solver_profile_kernels(vtp_solver *s, uint32_t n, vtp_kernel_tim
  * tick_n_steps call. */
 VTP_API int vtp_solver_get_launch_count(vtp_solver *s, uint64_t *launches);
 
-/* Differentiable PBF (no counterpart in the reference; PBF solver, one scene).
+/* Differentiable rollouts (no counterpart in the reference; PBF or DFSPH
+ * solver, one scene; DFSPH: fixed time step, surface tension 0).
  *
  * vtp_solver_diff_forward runs n_steps ordinary substeps from the current
  * state, saving the fluid state every `checkpoint_every` substeps (and at
  * the end).  With keep_lists != 0 every substep's neighbour lists are kept
- * for vtp_solver_diff_lists (finite-difference checks with frozen lists).
+ * for vtp_solver_diff_lists (finite-difference checks with frozen lists) and,
+ * DFSPH, its pressure-solve iteration counts for vtp_solver_diff_iterations.
  *
  * vtp_solver_diff_backward takes dL/d(positions) and dL/d(velocities) of
  * the state after the recorded substeps (attach order, n_total x float[3];
  * NULL = zero) and returns dL/d(positions) and dL/d(velocities) of the state
- * before them (boundary rows 0) and dL/dXSPH_k (any output may be NULL).
- * Each checkpoint segment is recomputed with the substep kernels into a
- * tape (lists frozen per substep as the forward built them), then the
- * hand-written adjoint passes run in reverse.  The solver is left at the
- * forward's final state. */
+ * before them and the derivative with respect to the solver's scalar
+ * parameter (any output may be NULL): PBF dL/dXSPH_k, DFSPH
+ * dL/dfPartRestViscosity.  Each checkpoint segment is recomputed with the
+ * substep kernels into a tape (lists frozen per substep as the forward built
+ * them; DFSPH: the pressure solves' iteration counts and clamp patterns too),
+ * then the hand-written adjoint passes run in reverse.  The solver is left at
+ * the forward's final state. */
 VTP_API int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists);
 VTP_API int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
                                      float *dl_dvel0, double *dl_dxsph_k);
 /* Neighbour lists of recorded substep `step` in the layout of
- * vtp_solver_get_neighbors (built after the substep's external force). */
+ * vtp_solver_get_neighbors (PBF: built after the substep's external force;
+ * DFSPH: built from the substep's starting positions). */
 VTP_API int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr);
+/* DFSPH: divergence- and density-solve iteration counts of recorded substep
+ * `step` (a rollout recorded with keep_lists). */
+VTP_API int vtp_solver_diff_iterations(vtp_solver *s, uint32_t step, uint32_t *div_iters, uint32_t *inc_iters);
 
 /* DFSPH pressure solve as a differentiable operator (no counterpart in the
  * reference; DFSPH solver, one scene).

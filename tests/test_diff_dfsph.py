@@ -57,3 +57,110 @@ def test_oracle_dfsph_rollout_adjoint_matches_finite_differences(oracle_lib):
     e = d.p.vis * 1e-4
     fd = (L(x0, v0, d.p.vis + e) - L(x0, v0, d.p.vis - e)) / (2 * e)
     assert abs(gvis - fd) <= 1e-6 * abs(fd)
+
+
+# ---------------------------------------------------------------- GPU: the library's adjoint
+
+T_GPU, EVERY = 4, 2
+
+
+def gpu_case(seed=5, n=3000, vis=1e-2):
+    sc = scenes.dam_break("DFSPH", n, seed=seed)
+    sc.config["DFSPH"]["Required"]["fPartRestViscosity"] = vis
+    f = sc.objects[0]
+    rng = np.random.default_rng(seed)
+    f.velocity = rng.normal(0.0, 0.1, (f.n, 3)).astype(np.float32)
+    return sc
+
+
+def _rollout_gradients(vtp, sc, A, B, keep_lists, extra=None):
+    from vtp import diff
+    s = vtp.solver_from_scene(sc, extra=extra)
+    assert s.initialize()
+    x0, v0 = s.get_field("pos"), s.get_field("vel")
+    diff.diff_forward(s, T_GPU, EVERY, keep_lists=keep_lists)
+    out = diff.diff_backward(s, A.astype(np.float32), B.astype(np.float32))
+    return s, x0, v0, out
+
+
+@pytest.mark.gpu
+def test_gpu_dfsph_rollout_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib):
+    from vtp import diff
+    sc = gpu_case()
+    mask = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    n = mask.size
+    A, B = _linear_loss((n, 3), mask, 3)
+    s, x0, v0, (gx, gv, gvis) = _rollout_gradients(vtp_gpu, sc, A, B, keep_lists=True)
+    M = int(sc.config["DFSPH"]["Required"]["maxNeighborNum"])
+    lists = [diff.diff_lists(s, t, M) for t in range(T_GPU)]
+    iters = [diff.diff_iterations(s, t) for t in range(T_GPU)]
+    print("iterations per substep", iters)
+    assert all(1 <= a <= 101 and 1 <= b <= 101 for a, b in iters)
+    # the recording forward advanced the solver exactly as ordinary substeps do
+    b = vtp_gpu.solver_from_scene(sc)
+    assert b.initialize() and b.tickNsteps(T_GPU)
+    assert np.array_equal(s.get_field("pos"), b.get_field("pos"))
+    assert np.array_equal(s.get_field("vel"), b.get_field("vel"))
+    b.destroy()
+    # FP64 adjoint of the same discrete map: the GPU's lists and iteration counts
+    d = oracle_lib.DfsphDiff(sc)
+    xd, vd = x0.astype(np.float64), v0.astype(np.float64)
+    _, _, states, used = d.rollout(xd, vd, T_GPU, iters, lists=lists, record=True)
+    ox, ov, ovis = d.adjoint(states, used, A, B)
+    ex = np.linalg.norm(gx[mask] - ox[mask]) / np.linalg.norm(ox[mask])
+    ev = np.linalg.norm(gv[mask] - ov[mask]) / np.linalg.norm(ov[mask])
+    evis = abs(gvis - ovis) / abs(ovis)
+    print(f"GPU vs FP64 adjoint: positions {ex:.2e}, velocities {ev:.2e}, viscosity {evis:.2e}")
+    assert ex < TOL and ev < TOL and evis < TOL
+
+    def L(x, v):
+        xT, vT, _, _ = d.rollout(x, v, T_GPU, iters, lists=lists)
+        return float((A * xT).sum() + (B * vT).sum())
+
+    rng = np.random.default_rng(8)
+    for _ in range(2):
+        dv = rng.normal(size=(n, 3)) * mask[:, None]
+        fd = (L(xd, vd + 1e-7 * dv) - L(xd, vd - 1e-7 * dv)) / 2e-7
+        ad = float((gv.astype(np.float64) * dv).sum())
+        print(f"velocity direction: fd {fd:.6e} adjoint {ad:.6e}")
+        assert abs(ad - fd) <= TOL * abs(fd)
+        dx = rng.normal(size=(n, 3)) * mask[:, None]
+        fd = (L(xd + 1e-8 * dx, vd) - L(xd - 1e-8 * dx, vd)) / 2e-8
+        ad = float((gx.astype(np.float64) * dx).sum())
+        print(f"position direction: fd {fd:.6e} adjoint {ad:.6e}")
+        assert abs(ad - fd) <= TOL * abs(fd)
+    s.destroy()
+
+
+@pytest.mark.gpu
+def test_gpu_dfsph_rollout_adjoint_same_with_recomputed_segments(vtp_gpu):
+    """One resident tape (tapeBudgetMB 0): every earlier segment is recomputed from its
+    checkpoint, and the gradient is the bits of the all-resident run."""
+    sc = gpu_case(seed=6)
+    mask = np.concatenate([np.full(o.n, o.material == 0) for o in sc.objects])
+    A, B = _linear_loss((mask.size, 3), mask, 4)
+    s1, _, _, g1 = _rollout_gradients(vtp_gpu, sc, A, B, keep_lists=True)
+    s2, _, _, g2 = _rollout_gradients(vtp_gpu, sc, A, B, keep_lists=False, extra={"tapeBudgetMB": 0})
+    assert np.array_equal(g1[0], g2[0]) and np.array_equal(g1[1], g2[1]) and g1[2] == g2[2]
+    assert np.array_equal(s1.get_field("pos"), s2.get_field("pos"))
+    for s in (s1, s2):
+        s.destroy()
+
+
+@pytest.mark.gpu
+def test_gpu_dfsph_rollout_rejects_unsupported_settings(vtp_gpu):
+    from vtp import diff
+    sc = gpu_case(seed=7, n=1000)
+    s = vtp_gpu.solver_from_scene(sc)
+    with pytest.raises(vtp_gpu.VtpError, match="before diff_forward"):
+        diff.diff_backward(s, np.zeros((s.counts()["total"], 3), np.float32))
+    s.destroy()
+    s = vtp_gpu.solver_from_scene(sc, extra={"cfl": 0.4})
+    with pytest.raises(vtp_gpu.VtpError, match="fixed time step"):
+        diff.diff_forward(s, 2, 1)
+    s.destroy()
+    sc.config["DFSPH"]["Required"]["surfaceTensionCoefficient"] = 0.001
+    s = vtp_gpu.solver_from_scene(sc)
+    with pytest.raises(vtp_gpu.VtpError, match="surface-tension"):
+        diff.diff_forward(s, 2, 1)
+    s.destroy()

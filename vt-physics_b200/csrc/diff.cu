@@ -23,6 +23,7 @@
 // adjoint values of the previous pass.  Boundary rows are static and get no
 // adjoint.
 #include "solver.h"
+#include "diff_dfsph.h"
 
 #include <algorithm>
 #include <array>
@@ -523,6 +524,7 @@ int check_ready(vtp_solver *s) {
 extern "C" {
 
 int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists) {
+    if (s && s->type == VTP_SOLVER_DFSPH) return vtp::dfsph_diff_forward(s, n_steps, checkpoint_every, keep_lists);
     const vtp::NvtxRange nvtx_range("vtp diff forward");
     int rc = check_ready(s);
     if (rc) return rc;
@@ -678,6 +680,8 @@ extern "C" {
 
 int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
                              float *dl_dvel0, double *dl_dxsph_k) {
+    if (s && s->type == VTP_SOLVER_DFSPH)
+        return vtp::dfsph_diff_backward(s, dl_dpos, dl_dvel, dl_dpos0, dl_dvel0, dl_dxsph_k);
     const vtp::NvtxRange nvtx_range("vtp diff backward");
     int rc = check_ready(s);
     if (rc) return rc;
@@ -735,24 +739,37 @@ int vtp_solver_diff_backward(vtp_solver *s, const float *dl_dpos, const float *d
 }
 
 int vtp_solver_diff_lists(vtp_solver *s, uint32_t step, uint32_t *counts, uint32_t *nbrs, uint32_t max_nbr) {
-    int rc = check_ready(s);
-    if (rc) return rc;
-    if (!s->diff || !s->diff->keep_lists) return fail(VTP_ERR_STATE, "diff_lists needs diff_forward with keep_lists");
-    vtp::DiffState &d = *s->diff;
-    if (step >= d.steps) return fail(VTP_ERR_ARG, "step out of range");
+    const uint32_t *l_orig = nullptr, *l_nbr = nullptr, *l_cnt = nullptr;
+    uint32_t n = 0, nf = 0;
+    if (s && s->type == VTP_SOLVER_DFSPH) {
+        int rc = vtp::dfsph_diff_slot(s, step, &l_orig, &l_nbr, &l_cnt, nullptr, nullptr);
+        if (rc) return rc;
+        n = s->L.n;
+        nf = s->L.nf;
+    } else {
+        int rc = check_ready(s);
+        if (rc) return rc;
+        if (!s->diff || !s->diff->keep_lists) return fail(VTP_ERR_STATE, "diff_lists needs diff_forward with keep_lists");
+        vtp::DiffState &d = *s->diff;
+        if (step >= d.steps) return fail(VTP_ERR_ARG, "step out of range");
+        n = d.n;
+        nf = d.nf;
+        l_orig = d.kl_orig[step];
+        l_nbr = d.kl_nbr[step];
+        l_cnt = d.kl_cnt[step];
+    }
     if (!counts || !nbrs) return fail(VTP_ERR_ARG, "null argument");
     if (max_nbr != s->maxnbr) return fail(VTP_ERR_ARG, "max_nbr must equal maxNeighborNum");
-    const uint32_t n = d.n, nf = d.nf;
     // Row -> attach id map of that substep: fluid rows from the record, boundary rows static.
     uint32_t *omap = nullptr, *dc = nullptr, *dn = nullptr;
     CU(cudaMalloc(&omap, (size_t)n * 4));
     cudaError_t e = cudaMalloc(&dc, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&dn, (size_t)n * max_nbr * 4);
-    if (e == cudaSuccess && nf) e = cudaMemcpyAsync(omap, d.kl_orig[step], (size_t)nf * 4, cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess && nf) e = cudaMemcpyAsync(omap, l_orig, (size_t)nf * 4, cudaMemcpyDeviceToDevice, s->st);
     if (e == cudaSuccess && n > nf)
         e = cudaMemcpyAsync(omap + nf, s->orig.c() + nf, (size_t)(n - nf) * 4, cudaMemcpyDeviceToDevice, s->st);
     if (e == cudaSuccess) {
-        vtp::export_neighbors(s->st, s->L, 0, nf, d.kl_nbr[step], d.kl_cnt[step], omap, max_nbr, dc, dn);
+        vtp::export_neighbors(s->st, s->L, 0, nf, l_nbr, l_cnt, omap, max_nbr, dc, dn);
         vtp::export_neighbors(s->st, s->L, nf, n - nf, s->u.bnbr, s->u.bncnt, omap, max_nbr, dc, dn);
         e = cudaMemcpyAsync(counts, dc, (size_t)n * 4, cudaMemcpyDeviceToHost, s->st);
     }

@@ -1,0 +1,741 @@
+// Differentiable DFSPH rollout: a recorded forward with checkpoints and the
+// hand-written adjoint of the DFSPH substep (no counterpart in the reference).
+//
+// One substep (DFSPHSolver::tick, DFSPHSolver.cpp:339-406, as the library runs
+// it; surface tension off, fixed time step):
+//   lists from x;  ratio_i = V_i W0 + sum_j V_j W_ij,  a1_i = sum_j V_j gradW_ij,
+//   alpha_i = max(|a1_i|^2 / m + 1e-6 + sum_{fluid j} V_j^2 |gradW_ij|^2 / m, 1e-6)
+//   divergence solve, density solve: from v* = v, each iteration
+//     kappa_i = max(0, ratio_i - 1 + dt sum_j V_j gradW_ij.(v*_i - v*_j)) / (alpha_i dt^2 V_i)
+//     v*_i -= (dt V_i / m) sum_j V_j (kappa_i + kappa_j) gradW_ij      (kappa_j = 0 for boundary j)
+//   between them: v' = v* + dt (g + sum_{fluid j} C (u.r) gradW_ij / (|r|^2 + 0.001 h^2)),
+//     u = v*_i - v*_j, C = 10 nu V_j
+//   v_new = v*, x_new = x + dt v_new
+// with gradW_ij = g r (r = x_i - x_j) and d(g r)/dr = J = g I + hh r r^T.
+//
+// Forward (vtp_solver_diff_forward on a DFSPH solver): the ordinary substeps, with
+// the fluid state saved every k substeps; the last segments (as many as fit the tape
+// budget) run recording substeps: the substep's lists, positions, alpha, the velocity
+// after the divergence solve and, per pressure-solve iteration, {v* entering it, its
+// kappa}.  The solve loops of a recording substep are host-driven (one 4-byte
+// readback per iteration) because the tape needs one record per iteration.
+// Backward: the segments last to first, each recomputed from its checkpoint into a
+// tape unless the forward recorded it, then the adjoint substeps in reverse.  Every
+// adjoint neighbour sum is in gather form over the same symmetric lists, so no pass
+// uses atomics; the clamps (kappa > 0, alpha > 1e-6) of the forward are held fixed.
+#include "solver.h"
+#include "diff_dfsph.h"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+namespace vtp {
+
+struct DfTapeSlot {
+    uint32_t *orig = nullptr, *nbr = nullptr, *ncnt = nullptr;
+    float4 *x = nullptr;        // [n] positions, w = volume (boundary rows static)
+    float4 *vp = nullptr;       // [nf] velocity after the divergence solve
+    float *alpha = nullptr;     // [nf]
+    uint32_t iters[2] = {0, 0}; // divergence / density solve iterations
+    uint32_t first[2] = {0, 0}; // their first record in the tape's record pool
+};
+
+struct DfTape {
+    std::vector<DfTapeSlot> slots;
+    std::vector<float4 *> recs;   // [n] {v* entering the iteration, its kappa}; boundary rows {v_b, 0}
+};
+
+struct DfDiffState {
+    uint32_t steps = 0, every = 0, nf = 0, n = 0;
+    bool keep_lists = false;
+    std::vector<void *> mem;
+    std::vector<float4 *> ck_pos, ck_vel;
+    std::vector<uint32_t *> ck_orig;
+    std::vector<DfTape> tapes;
+    std::vector<int> taped;
+    float4 *bstat = nullptr;      // [n] boundary rows {v_b, 0}, copied into every record
+    // adjoint work arrays
+    float4 *xbar_a = nullptr, *vbar_a = nullptr;    // attach order [n]
+    float4 *xbar = nullptr, *vb[2] = {nullptr, nullptr}, *a1b = nullptr;
+    float *db = nullptr, *rbar = nullptr, *abar = nullptr;
+    double *vpart = nullptr, *vacc = nullptr;
+    uint32_t blocks = 0;
+
+    ~DfDiffState() {
+        for (void *p : mem) cudaFree(p);
+    }
+    template <class T>
+    int alloc(T **p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e != cudaSuccess)
+            return fail(VTP_ERR_NOMEM, std::string("differentiable DFSPH: ") + cudaGetErrorString(e));
+        mem.push_back(*p);
+        return VTP_OK;
+    }
+};
+
+namespace {
+
+inline unsigned nblk(uint32_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// g'(r) / r of the cubic spline's gradient factor (gradW = g r).
+__device__ __forceinline__ float cubic_hh(float d2, const Cubic &k) {
+    if (!(d2 > 0.f)) return 0.f;
+    const float r = sqrtf(d2);
+    const float q = r * k.invh;
+    if (q < 1e-6f || q > 1.f) return 0.f;
+    const float ih2 = k.invh * k.invh, ih4 = ih2 * ih2;
+    if (q <= 0.5f) return 18.f * k.sigma * ih4 / q;
+    return 6.f * k.sigma * ih4 * (1.f - q * q) / (q * q * q);
+}
+
+__device__ __forceinline__ double block_sum_d(double v) {
+    __shared__ double sm[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    double s = 0.0;
+    if (wid == 0) {
+        s = lane < nw ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    return s;
+}
+
+struct DfdArgs {
+    uint32_t nf, ell_stride;
+    Cubic k;
+    float dt, mass_f, vis10;   // vis10 = 10 nu V_f (the viscosity pair factor C)
+    float eps;                 // 0.001 h^2
+    const uint32_t *nbr, *ncnt, *orig;
+    const float4 *x;           // [n] w = volume
+    const float4 *rec;         // [n] {v*, kappa} of the iteration
+    const float4 *vp;          // [nf]
+    const float *alpha;        // [nf]
+    float4 *xbar, *vb, *vb_out, *a1b;
+    float *db, *rbar, *abar;
+    float4 *xbar_a, *vbar_a;
+    double *vpart;
+};
+
+// Recording: {v* entering the iteration, kappa} of every fluid row.
+__global__ void k_dfd_record(uint32_t nf, const float4 *__restrict__ vadv, const float *__restrict__ kappa,
+                             float4 *__restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nf) return;
+    const float4 v = vadv[r];
+    out[r] = make_float4(v.x, v.y, v.z, kappa[r]);
+}
+
+// Recording: the velocity after the divergence solve (second half of the packed rows).
+__global__ void k_dfd_vp(uint32_t nf, const float4 *__restrict__ pva, float4 *__restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nf) return;
+    out[r] = pva[2 * (size_t)r + 1];
+}
+
+// Attach order -> this substep's rows; the position update's adjoint (v-bar of the density
+// solve's output = v-bar + dt x-bar); the ratio / alpha adjoints start at zero.
+__global__ void k_dfd_gather(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const uint32_t id = a.orig[r];
+    const float4 xo = a.xbar_a[id], vo = a.vbar_a[id];
+    a.xbar[r] = xo;
+    a.vb[r] = make_float4(vo.x + a.dt * xo.x, vo.y + a.dt * xo.y, vo.z + a.dt * xo.z, 0.f);
+    a.rbar[r] = 0.f;
+    a.abar[r] = 0.f;
+}
+
+// Pressure-solve iteration adjoint, pass A: kappa-bar_i = sum_j gradW_ij.w_ij with
+// w_ij = c_j V_i vb_j - c_i V_j vb_i (c = dt V / m; the j term only for fluid j), then
+// delta-bar (clamp of the forward), ratio-bar and alpha-bar, and the position adjoint of
+// the velocity update: x-bar_i += sum_j (kappa_i + kappa_j) J_ij w_ij.
+__global__ void __launch_bounds__(256) k_dfd_iter_a(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.x[r], vi = a.vb[r];
+    const float ki = a.rec[r].w;
+    const float ci = a.dt * p.w / a.mass_f;
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    float kb = 0.f, xx = 0.f, xy = 0.f, xz = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = __ldg(a.x + j);
+        const bool fj = j < a.nf;
+        const float kj = __ldg(&a.rec[j].w);   // 0 for boundary rows
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float d2 = dist2(rx, ry, rz);
+        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+        float wx = -ci * q.w * vi.x, wy = -ci * q.w * vi.y, wz = -ci * q.w * vi.z;
+        if (fj) {
+            const float4 vj = __ldg(a.vb + j);
+            const float cj = a.dt * q.w / a.mass_f * p.w;
+            wx += cj * vj.x;
+            wy += cj * vj.y;
+            wz += cj * vj.z;
+        }
+        const float rw = rx * wx + ry * wy + rz * wz;
+        kb += g * rw;
+        const float kk = ki + kj;
+        xx += kk * (g * wx + hh * rx * rw);
+        xy += kk * (g * wy + hh * ry * rw);
+        xz += kk * (g * wz + hh * rz * rw);
+    }
+    float4 xb = a.xbar[r];
+    xb.x += xx; xb.y += xy; xb.z += xz;
+    a.xbar[r] = xb;
+    const float al = a.alpha[r];
+    const float d = ki > 0.f ? kb / (al * a.dt * a.dt * p.w) : 0.f;
+    a.db[r] = d;
+    a.rbar[r] += d;
+    a.abar[r] -= kb * ki / al;
+}
+
+// Pressure-solve iteration adjoint, pass B: the delta term's adjoints,
+// vb_i += dt sum_j (V_j db_i + V_i db_j) gradW_ij and
+// x-bar_i += dt sum_j (V_j db_i + V_i db_j) J_ij (v*_i - v*_j) (db_j only for fluid j).
+__global__ void __launch_bounds__(256) k_dfd_iter_b(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.x[r], si = a.rec[r];
+    const float di = a.db[r];
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = __ldg(a.x + j), sj = __ldg(a.rec + j);
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float d2 = dist2(rx, ry, rz);
+        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+        const float c = a.dt * (q.w * di + (j < a.nf ? p.w * __ldg(a.db + j) : 0.f));
+        const float ux = si.x - sj.x, uy = si.y - sj.y, uz = si.z - sj.z;
+        const float ru = rx * ux + ry * uy + rz * uz;
+        vx += c * g * rx;
+        vy += c * g * ry;
+        vz += c * g * rz;
+        xx += c * (g * ux + hh * rx * ru);
+        xy += c * (g * uy + hh * ry * ru);
+        xz += c * (g * uz + hh * rz * ru);
+    }
+    float4 v = a.vb[r];
+    v.x += vx; v.y += vy; v.z += vz;
+    a.vb[r] = v;
+    float4 xb = a.xbar[r];
+    xb.x += xx; xb.y += xy; xb.z += xz;
+    a.xbar[r] = xb;
+}
+
+// Gravity + viscosity adjoint: vb_out_i = vb_i + dt C sum_{fluid j} phi r (r.(vb_i - vb_j)),
+// x-bar_i += dt C sum_j [phi u (r.w) + (u.r)(phi w + psi r (r.w))] with u = vp_i - vp_j,
+// w = vb_i - vb_j, phi = g / (|r|^2 + eps), psi = 2 dphi/d|r|^2; block partials of
+// dL/dnu / V_f = sum_i dt vb_i . sum_j 10 (u.r) phi r.
+__global__ void __launch_bounds__(256) k_dfd_visc(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    double part = 0.0;
+    if (r < a.nf) {
+        const float4 p = a.x[r], ui = a.vp[r], wi = a.vb[r];
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f, ps = 0.f;
+        for (uint32_t t = 0; t + 1 < n; ++t) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            if (j >= a.nf) continue;   // same-material neighbours only
+            const float4 q = __ldg(a.x + j), uj = __ldg(a.vp + j), wj = __ldg(a.vb + j);
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float d2 = dist2(rx, ry, rz);
+            const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+            const float den = d2 + a.eps;
+            const float phi = g / den;
+            const float psi = hh / den - 2.f * g / (den * den);
+            const float ux = ui.x - uj.x, uy = ui.y - uj.y, uz = ui.z - uj.z;
+            const float wx = wi.x - wj.x, wy = wi.y - wj.y, wz = wi.z - wj.z;
+            const float ru = rx * ux + ry * uy + rz * uz, rw = rx * wx + ry * wy + rz * wz;
+            const float cv = a.dt * a.vis10 * phi * rw;
+            vx += cv * rx;
+            vy += cv * ry;
+            vz += cv * rz;
+            const float cx = a.dt * a.vis10;
+            xx += cx * (phi * ux * rw + ru * (phi * wx + psi * rx * rw));
+            xy += cx * (phi * uy * rw + ru * (phi * wy + psi * ry * rw));
+            xz += cx * (phi * uz * rw + ru * (phi * wz + psi * rz * rw));
+            ps += ru * phi * (rx * wi.x + ry * wi.y + rz * wi.z);
+        }
+        a.vb_out[r] = make_float4(wi.x + vx, wi.y + vy, wi.z + vz, 0.f);
+        float4 xb = a.xbar[r];
+        xb.x += xx; xb.y += xy; xb.z += xz;
+        a.xbar[r] = xb;
+        part = (double)a.dt * 10.0 * (double)ps;
+    }
+    const double s = block_sum_d(part);
+    if (threadIdx.x == 0) a.vpart[blockIdx.x] = s;
+}
+
+__global__ void k_dfd_vreduce(const double *part, uint32_t nb, double vol_f, double *acc) {
+    double s = 0.0;
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
+    s = block_sum_d(s);
+    if (threadIdx.x == 0) *acc += s * vol_f;
+}
+
+// alpha adjoint, pass 1: a1-bar_i = alpha-bar_i 2 a1_i / m (a1 recomputed), with
+// alpha-bar zeroed where the forward clamped alpha; stored {a1-bar, alpha-bar}.
+__global__ void __launch_bounds__(256) k_dfd_a1(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const bool live = a.alpha[r] > 1e-6f;
+    const float ab = live ? a.abar[r] : 0.f;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (live) {
+        const float4 p = a.x[r];
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        for (uint32_t t = 0; t + 1 < n; ++t) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = __ldg(a.x + j);
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float g = cubic_g(dist2(rx, ry, rz), a.k) * q.w;
+            ax += g * rx;
+            ay += g * ry;
+            az += g * rz;
+        }
+    }
+    const float c = 2.f * ab / a.mass_f;
+    a.a1b[r] = make_float4(c * ax, c * ay, c * az, ab);
+}
+
+// ratio / alpha adjoint, pass 2: x-bar_i += sum_j (ratio-bar_i V_j + ratio-bar_j V_i) g r
+// + J (V_j a1-bar_i - V_i a1-bar_j) + 2 g (g + hh |r|^2) (alpha-bar_i V_j^2 + alpha-bar_j V_i^2) / m r
+// (the j terms only for fluid j); then this substep's rows -> attach order.
+__global__ void __launch_bounds__(256) k_dfd_ratio_x(DfdArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nf) return;
+    const float4 p = a.x[r], Ai = a.a1b[r];
+    const float rbi = a.rbar[r];
+    const uint32_t n = a.ncnt[r];
+    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    const float im = 1.f / a.mass_f;
+    float xx = 0.f, xy = 0.f, xz = 0.f;
+    for (uint32_t t = 0; t + 1 < n; ++t) {
+        const uint32_t j = lst[(size_t)t * 32u];
+        const float4 q = __ldg(a.x + j);
+        const bool fj = j < a.nf;
+        const float4 Aj = fj ? __ldg(a.a1b + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float rbj = fj ? __ldg(a.rbar + j) : 0.f;
+        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+        const float d2 = dist2(rx, ry, rz);
+        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+        const float cr = rbi * q.w + rbj * p.w;
+        const float c2 = fj ? 2.f * g * (g + hh * d2) * (Ai.w * q.w * q.w + Aj.w * p.w * p.w) * im : 0.f;
+        const float wx = q.w * Ai.x - p.w * Aj.x, wy = q.w * Ai.y - p.w * Aj.y, wz = q.w * Ai.z - p.w * Aj.z;
+        const float rw = rx * wx + ry * wy + rz * wz;
+        const float s = cr * g + c2;
+        xx += s * rx + g * wx + hh * rx * rw;
+        xy += s * ry + g * wy + hh * ry * rw;
+        xz += s * rz + g * wz + hh * rz * rw;
+    }
+    float4 xb = a.xbar[r];
+    xb.x += xx; xb.y += xy; xb.z += xz;
+    const uint32_t id = a.orig[r];
+    a.xbar_a[id] = xb;
+    a.vbar_a[id] = a.vb[r];
+}
+
+__global__ void k_f3_to_f4(uint32_t n, const float *src, float4 *dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src ? make_float4(src[3 * (size_t)i], src[3 * (size_t)i + 1], src[3 * (size_t)i + 2], 0.f)
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void k_f4_to_f3(uint32_t n, const float4 *src, float *dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = src[i];
+    dst[3 * (size_t)i] = v.x;
+    dst[3 * (size_t)i + 1] = v.y;
+    dst[3 * (size_t)i + 2] = v.z;
+}
+
+__global__ void k_bstat(uint32_t nf, uint32_t n, const float4 *__restrict__ vadv, float4 *__restrict__ out) {
+    const uint32_t i = nf + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = vadv[i];
+    out[i] = make_float4(v.x, v.y, v.z, 0.f);
+}
+
+}  // namespace
+}  // namespace vtp
+
+using vtp::fail;
+
+#define CU(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(VTP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+using vtp::DfDiffState;
+using vtp::DfTape;
+using vtp::DfTapeSlot;
+
+int df_save(vtp_solver &s, float4 *p, float4 *v, uint32_t *o) {
+    const size_t nf = s.L.nf;
+    if (!nf) return VTP_OK;
+    CU(cudaMemcpyAsync(p, s.pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(v, s.vel.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(o, s.orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s.st));
+    return VTP_OK;
+}
+
+// A substep starts from v* = v (the finalize pass leaves them equal).
+int df_restore(vtp_solver &s, const float4 *p, const float4 *v, const uint32_t *o) {
+    const size_t nf = s.L.nf;
+    if (!nf) return VTP_OK;
+    CU(cudaMemcpyAsync(s.pos.c(), p, nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(s.vel.c(), v, nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(s.vadv.c(), v, nf * sizeof(float4), cudaMemcpyDeviceToDevice, s.st));
+    CU(cudaMemcpyAsync(s.orig.c(), o, nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s.st));
+    return VTP_OK;
+}
+
+// The record of iteration `k` of the tape's pool, allocated (with its static boundary rows) on
+// first use.
+int df_record_slot(vtp_solver &s, DfDiffState &d, DfTape &tape, uint32_t k, float4 **out) {
+    while (tape.recs.size() <= k) {
+        float4 *p = nullptr;
+        int rc = d.alloc(&p, d.n);
+        if (rc) return rc;
+        if (d.n > d.nf)
+            CU(cudaMemcpyAsync(p + d.nf, d.bstat + d.nf, (size_t)(d.n - d.nf) * sizeof(float4),
+                               cudaMemcpyDeviceToDevice, s.st));
+        tape.recs.push_back(p);
+    }
+    *out = tape.recs[k];
+    return VTP_OK;
+}
+
+// One pressure solve of a recording substep, host-driven, each iteration's {v*, kappa}
+// recorded.  The stop test is the solver's (its constant forced counts included; a
+// per-substep forced sequence is not followed).
+int df_record_solve(vtp_solver &s, DfDiffState &d, DfTape &tape, DfTapeSlot &slot, int which, uint32_t &pool) {
+    const vtp::NvtxRange nvtx_range(which == 0 ? "vtp divergence solve (recorded)" : "vtp density solve (recorded)");
+    vtp::DfsphArgs a = s.dfsph_args(which);
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::SolveCtl c = s.solve_ctl(which, cudaGraphConditionalHandle{}, 0);
+    c.force_iters = which == 0 ? s.force_div : s.force_inc;
+    c.force_seq = nullptr;
+    c.scene_tiles = s.d_scene_tiles;   // the unstaged passes write one residual partial per tile
+    vtp::dfsph_solve_begin(s.st, s.solve + (size_t)which * s.scenes.size(), s.loop + which, 1);
+    vtp::dfsph_solve_pack(s.st, a);
+    slot.first[which] = pool;
+    const uint32_t nf = s.L.nf;
+    uint32_t it = 0;
+    for (; it < 101; ++it) {
+        float4 *rec = nullptr;
+        int rc = df_record_slot(s, d, tape, pool++, &rec);
+        if (rc) return rc;
+        vtp::dfsph_solve_a(s.st, a, s.block);
+        if (nf) vtp::k_dfd_record<<<vtp::nblk(nf, 256), 256, 0, s.st>>>(nf, a.vadv, a.kappa, rec);
+        vtp::dfsph_solve_b(s.st, a, s.block);
+        vtp::dfsph_solve_end(s.st, c, s.partials, s.d_status);
+        CU(cudaMemcpyAsync(s.h_pinned + 2, &s.loop[which].running, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+        CU(cudaStreamSynchronize(s.st));
+        if (!s.h_pinned[2]) break;
+    }
+    slot.iters[which] = std::min<uint32_t>(it + 1, 101);
+    return VTP_OK;
+}
+
+// One DFSPH substep recording into `slot` (the buffer swaps of enqueue_tick, so the substep
+// graphs' parities stay valid).  recompute: leave the device substep counter alone (the
+// iteration counts come from the stop test, which sees the forward's bits again).
+int df_record_substep(vtp_solver &s, DfDiffState &d, DfTape &tape, DfTapeSlot &slot, uint32_t &pool,
+                      bool recompute) {
+    const vtp::NvtxRange nvtx_range("vtp DFSPH substep (recorded)");
+    const uint32_t nf = s.L.nf;
+    cudaStream_t st = s.st;
+    vtp::Carry carry{};
+    carry.nf4 = 1;
+    carry.src4[0] = s.vadv.c();
+    carry.dst4[0] = s.vadv.n();
+    vtp::ugns_sort(st, s.scn(), s.nbuckets, 0, nf, s.pos.c(), s.pos.n(), s.vel.c(), s.vel.n(), s.orig.c(),
+                   s.orig.n(), carry, 0.f, s.u, s.u.fstart);
+    s.pos.swap(); s.vel.swap(); s.orig.swap(); s.vadv.swap();
+    vtp::ugns_build_lists(st, s.scn(), s.L, 0, nf, s.pos.c(), s.orig.c(), s.u, slot.nbr, slot.ncnt, s.d_status,
+                          s.d_overflow, s.block);
+    if (nf) {
+        CU(cudaMemcpyAsync(slot.orig, s.orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(slot.x, s.pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    }
+    vtp::DfsphArgs a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::dfsph_ratio_alpha(st, a, s.block);
+    if (nf) CU(cudaMemcpyAsync(slot.alpha, s.alpha, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    int rc;
+    if ((rc = df_record_solve(s, d, tape, slot, 0, pool))) return rc;
+    a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::dfsph_pressure_pack(st, a);
+    if (nf) vtp::k_dfd_vp<<<vtp::nblk(nf, 256), 256, 0, st>>>(nf, s.pva, slot.vp);
+    vtp::dfsph_viscosity(st, a, s.block);
+    s.vel.swap(); s.vadv.swap();
+    if ((rc = df_record_solve(s, d, tape, slot, 1, pool))) return rc;
+    a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    if (recompute) a.tick = nullptr;
+    vtp::dfsph_finalize(st, a);
+    return VTP_OK;
+}
+
+int df_record_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool recompute) {
+    DfTape &tape = d.tapes[tp];
+    uint32_t pool = 0;
+    for (uint32_t t = 0; t < k; ++t) {
+        int rc = df_record_substep(s, d, tape, tape.slots[t], pool, recompute);
+        if (rc) return rc;
+    }
+    CU(cudaStreamSynchronize(s.st));
+    return s.check_status();
+}
+
+int df_adjoint_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp) {
+    const uint32_t nf = d.nf;
+    if (!nf) return VTP_OK;
+    const DfTape &tape = d.tapes[tp];
+    const unsigned G = vtp::nblk(nf, 256);
+    vtp::DfdArgs a{};
+    a.nf = nf; a.ell_stride = s.L.ell_stride; a.k = s.kc;
+    a.dt = s.dt; a.mass_f = s.rho_f * s.vol0;
+    a.vis10 = 10.f * ((s.viscosity + s.viscosity) / 2 * a.mass_f / s.rho_f);
+    a.eps = 0.001f * (s.h * s.h);
+    a.xbar = d.xbar; a.a1b = d.a1b; a.db = d.db; a.rbar = d.rbar; a.abar = d.abar;
+    a.xbar_a = d.xbar_a; a.vbar_a = d.vbar_a; a.vpart = d.vpart;
+    for (int t = (int)k - 1; t >= 0; --t) {
+        const DfTapeSlot &T = tape.slots[t];
+        a.nbr = T.nbr; a.ncnt = T.ncnt; a.orig = T.orig; a.x = T.x; a.vp = T.vp; a.alpha = T.alpha;
+        int cur = 0;
+        a.vb = d.vb[cur];
+        vtp::k_dfd_gather<<<G, 256, 0, s.st>>>(a);
+        for (int w = 1; w >= 0; --w) {
+            for (int it = (int)T.iters[w] - 1; it >= 0; --it) {
+                a.rec = tape.recs[T.first[w] + it];
+                vtp::k_dfd_iter_a<<<G, 256, 0, s.st>>>(a);
+                vtp::k_dfd_iter_b<<<G, 256, 0, s.st>>>(a);
+            }
+            if (w == 1) {
+                a.vb_out = d.vb[cur ^ 1];
+                vtp::k_dfd_visc<<<G, 256, 0, s.st>>>(a);
+                vtp::k_dfd_vreduce<<<1, 256, 0, s.st>>>(d.vpart, G, (double)s.vol0, d.vacc);
+                cur ^= 1;
+                a.vb = d.vb[cur];
+            }
+        }
+        vtp::k_dfd_a1<<<G, 256, 0, s.st>>>(a);
+        vtp::k_dfd_ratio_x<<<G, 256, 0, s.st>>>(a);
+    }
+    CU(cudaGetLastError());
+    return VTP_OK;
+}
+
+// Forward of a recorded rollout: checkpoint, then the ordinary substeps up to the next
+// checkpoint, or (the last segments) recording substeps into the tapes.
+int df_record_rollout(vtp_solver &s, DfDiffState &d) {
+    const uint32_t nchk = (d.steps + d.every - 1) / d.every;
+    const uint32_t ntapes = (uint32_t)d.tapes.size();
+    int rc;
+    d.taped.assign(nchk, -1);
+    for (uint32_t c = 0; c < nchk; ++c) {
+        if ((rc = df_save(s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
+        const uint32_t k = std::min(d.every, d.steps - c * d.every);
+        if (c + ntapes >= nchk) {
+            const int tp = (int)(c + ntapes - nchk);
+            if ((rc = df_record_segment(s, d, k, tp, false))) return rc;
+            for (uint32_t t = 0; t < k; ++t) {   // as tick_n advances them for the segments before
+                s.sim_time += s.dt;
+                ++s.steps_done;
+            }
+            s.stats.steps_done = s.steps_done;
+            s.stats.sim_time = s.sim_time;
+            d.taped[c] = tp;
+            continue;
+        }
+        if ((rc = s.tick_n(k))) return rc;
+    }
+    if ((rc = df_save(s, d.ck_pos[nchk], d.ck_vel[nchk], d.ck_orig[nchk]))) return rc;
+    CU(cudaStreamSynchronize(s.st));
+    return s.check_status();
+}
+
+}  // namespace
+
+namespace vtp {
+
+int dfsph_diff_ready(vtp_solver *s) {
+    if (s->nscenes() != 1) return fail(VTP_ERR_CONFIG, "differentiable mode runs a single scene");
+    if (s->cfl > 0.f) return fail(VTP_ERR_CONFIG, "differentiable DFSPH takes the fixed time step (no \"cfl\")");
+    if (s->gamma != 0.f)
+        return fail(VTP_ERR_CONFIG, "differentiable DFSPH has no surface-tension adjoint (surfaceTensionCoefficient must be 0)");
+    return VTP_OK;
+}
+
+int dfsph_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_every, int keep_lists) {
+    const NvtxRange nvtx_range("vtp DFSPH diff forward");
+    int rc = dfsph_diff_ready(s);
+    if (rc) return rc;
+    if (!s->initialized && (rc = s->initialize())) return rc;
+    if (s->crashed) return fail(VTP_ERR_STATE, "solver is crashed");
+    if (n_steps == 0 || checkpoint_every == 0) return fail(VTP_ERR_ARG, "n_steps and checkpoint_every must be > 0");
+    const uint32_t every = std::min(checkpoint_every, n_steps);
+    const uint32_t nchk = (n_steps + every - 1) / every;
+    const size_t nf = std::max<uint32_t>(s->L.nf, 1), n = std::max<uint32_t>(s->L.n, 1);
+    const size_t lrows = ((size_t)s->L.nf + 31) / 32 * 32 * s->L.ell_stride;
+    // Tapes kept resident: as many segments' as the budget and half the free memory allow
+    // (all of them with keep_lists), estimated at 8 iteration records per substep.
+    const size_t slot_bytes = 4 * nf * 2 + 4 * std::max<size_t>(lrows, 1) + 16 * n + 16 * nf + 4 * nf + 16 * n * 8;
+    const size_t tape_bytes = std::max<size_t>(slot_bytes * every, 1);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    const size_t budget = std::min<size_t>((size_t)s->tape_budget_mb << 20, free_b / 2);
+    const uint32_t ntapes =
+        keep_lists ? nchk : (uint32_t)std::min<size_t>(std::max<size_t>(budget / tape_bytes, 1), nchk);
+    // A rollout of the same shape as the previous one reuses its checkpoints, tapes and work
+    // arrays (the free memory the estimate reads has shrunk by them since).
+    if (s->dfdiff && s->dfdiff->steps == n_steps && s->dfdiff->every == every &&
+        s->dfdiff->keep_lists == (keep_lists != 0) && s->dfdiff->nf == s->L.nf && s->dfdiff->n == s->L.n)
+        return df_record_rollout(*s, *s->dfdiff);
+    auto d = std::make_shared<DfDiffState>();
+    d->steps = n_steps;
+    d->every = every;
+    d->keep_lists = keep_lists != 0;
+    d->nf = s->L.nf;
+    d->n = s->L.n;
+    d->ck_pos.resize(nchk + 1);
+    d->ck_vel.resize(nchk + 1);
+    d->ck_orig.resize(nchk + 1);
+    for (uint32_t c = 0; c <= nchk; ++c)
+        if ((rc = d->alloc(&d->ck_pos[c], nf)) || (rc = d->alloc(&d->ck_vel[c], nf)) ||
+            (rc = d->alloc(&d->ck_orig[c], nf)))
+            return rc;
+    if ((rc = d->alloc(&d->bstat, n))) return rc;
+    if (s->L.n > s->L.nf)
+        k_bstat<<<nblk(s->L.n - s->L.nf, 256), 256, 0, s->st>>>(s->L.nf, s->L.n, s->vadv.c(), d->bstat);
+    d->tapes.resize(ntapes);
+    for (auto &tape : d->tapes) {
+        tape.slots.resize(every);
+        for (auto &slot : tape.slots) {
+            if ((rc = d->alloc(&slot.orig, nf)) || (rc = d->alloc(&slot.nbr, std::max<size_t>(lrows, 1))) ||
+                (rc = d->alloc(&slot.ncnt, nf)) || (rc = d->alloc(&slot.x, n)) || (rc = d->alloc(&slot.vp, nf)) ||
+                (rc = d->alloc(&slot.alpha, nf)))
+                return rc;
+            if (s->L.nb)   // boundary rows are static: copy them once
+                CU(cudaMemcpyAsync(slot.x + s->L.nf, s->pos.c() + s->L.nf, (size_t)s->L.nb * sizeof(float4),
+                                   cudaMemcpyDeviceToDevice, s->st));
+        }
+    }
+    d->blocks = nblk((uint32_t)nf, 256);
+    if ((rc = d->alloc(&d->xbar_a, n)) || (rc = d->alloc(&d->vbar_a, n)) || (rc = d->alloc(&d->xbar, nf)) ||
+        (rc = d->alloc(&d->vb[0], nf)) || (rc = d->alloc(&d->vb[1], nf)) || (rc = d->alloc(&d->a1b, nf)) ||
+        (rc = d->alloc(&d->db, nf)) || (rc = d->alloc(&d->rbar, nf)) || (rc = d->alloc(&d->abar, nf)) ||
+        (rc = d->alloc(&d->vpart, d->blocks)) || (rc = d->alloc(&d->vacc, 1)))
+        return rc;
+    s->dfdiff.reset();
+    if ((rc = df_record_rollout(*s, *d))) return rc;
+    s->dfdiff = d;
+    return VTP_OK;
+}
+
+int dfsph_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dvel, float *dl_dpos0,
+                        float *dl_dvel0, double *dl_dvis) {
+    const NvtxRange nvtx_range("vtp DFSPH diff backward");
+    int rc = dfsph_diff_ready(s);
+    if (rc) return rc;
+    if (!s->dfdiff) return fail(VTP_ERR_STATE, "diff_backward before diff_forward");
+    DfDiffState &d = *s->dfdiff;
+    const uint32_t n = d.n;
+    const size_t n3 = (size_t)n * 3 * sizeof(float);
+    if ((rc = s->ensure_stage(n3))) return rc;
+    if (dl_dpos) CU(cudaMemcpyAsync(s->stage, dl_dpos, n3, cudaMemcpyHostToDevice, s->st));
+    k_f3_to_f4<<<nblk(n, 256), 256, 0, s->st>>>(n, dl_dpos ? s->stage : nullptr, d.xbar_a);
+    if (dl_dvel) CU(cudaMemcpyAsync(s->stage, dl_dvel, n3, cudaMemcpyHostToDevice, s->st));
+    k_f3_to_f4<<<nblk(n, 256), 256, 0, s->st>>>(n, dl_dvel ? s->stage : nullptr, d.vbar_a);
+    CU(cudaMemsetAsync(d.vacc, 0, sizeof(double), s->st));
+    const uint32_t nchk = (d.steps + d.every - 1) / d.every;
+    for (int c = (int)nchk - 1; c >= 0; --c) {
+        const uint32_t t0 = (uint32_t)c * d.every, k = std::min(d.every, d.steps - t0);
+        int tp = c < (int)d.taped.size() ? d.taped[c] : -1;
+        if (tp < 0) {
+            // Recompute the segment from its checkpoint into tape 0 (whose own segment, the
+            // earliest one the forward recorded, has been consumed already).  Its iteration
+            // counts come from the stop test, which sees the forward's bits again.
+            tp = 0;
+            if ((rc = df_restore(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
+            if ((rc = df_record_segment(*s, d, k, 0, true))) return rc;
+        }
+        if ((rc = df_adjoint_segment(*s, d, k, tp))) return rc;
+    }
+    if (!d.keep_lists) d.taped.assign(d.taped.size(), -1);   // tape 0 now holds the first segment's recompute
+    if (dl_dpos0) {
+        k_f4_to_f3<<<nblk(n, 256), 256, 0, s->st>>>(n, d.xbar_a, s->stage);
+        CU(cudaMemcpyAsync(dl_dpos0, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+    }
+    if (dl_dvel0) {
+        k_f4_to_f3<<<nblk(n, 256), 256, 0, s->st>>>(n, d.vbar_a, s->stage);
+        CU(cudaMemcpyAsync(dl_dvel0, s->stage, n3, cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+    }
+    double vb = 0.0;
+    CU(cudaMemcpyAsync(&vb, d.vacc, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    // Put the forward's final state back so the solver can continue.
+    if ((rc = df_restore(*s, d.ck_pos[nchk], d.ck_vel[nchk], d.ck_orig[nchk]))) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    if (dl_dvis) *dl_dvis = vb;
+    return s->check_status();
+}
+
+int dfsph_diff_slot(vtp_solver *s, uint32_t step, const uint32_t **orig, const uint32_t **nbr,
+                    const uint32_t **ncnt, uint32_t *div_iters, uint32_t *inc_iters) {
+    if (!s->dfdiff || !s->dfdiff->keep_lists)
+        return fail(VTP_ERR_STATE, "the substep records need diff_forward with keep_lists");
+    DfDiffState &d = *s->dfdiff;
+    if (step >= d.steps) return fail(VTP_ERR_ARG, "step out of range");
+    const uint32_t c = step / d.every, t = step % d.every;
+    const int tp = c < d.taped.size() ? d.taped[c] : -1;
+    if (tp < 0) return fail(VTP_ERR_STATE, "substep not recorded");
+    const DfTapeSlot &slot = d.tapes[tp].slots[t];
+    if (orig) *orig = slot.orig;
+    if (nbr) *nbr = slot.nbr;
+    if (ncnt) *ncnt = slot.ncnt;
+    if (div_iters) *div_iters = slot.iters[0];
+    if (inc_iters) *inc_iters = slot.iters[1];
+    return VTP_OK;
+}
+
+}  // namespace vtp
+
+extern "C" int vtp_solver_diff_iterations(vtp_solver *s, uint32_t step, uint32_t *div_iters, uint32_t *inc_iters) {
+    if (!s) return fail(VTP_ERR_ARG, "null solver");
+    if (s->type != VTP_SOLVER_DFSPH) return fail(VTP_ERR_CONFIG, "pressure-solve iteration counts are DFSPH records");
+    return vtp::dfsph_diff_slot(s, step, nullptr, nullptr, nullptr, div_iters, inc_iters);
+}

@@ -63,6 +63,7 @@ struct PbfTapeSlot {
 
 namespace vtp {
 struct DiffState;
+struct DfDiffState;
 }
 
 struct vtp_solver {
@@ -109,7 +110,7 @@ struct vtp_solver {
     int list_lanes = 0;       // neighbour-list builder lanes per row (0 = by row count)
     bool cell_cull = false;   // list builder skips neighbour cells beyond h (same lists)
     bool staged_solve = false;      // DFSPH pressure solve gathers from shared-memory cell-group copies
-    uint32_t tape_budget_mb = 8192;  // differentiable PBF: device memory for resident segment tapes
+    uint32_t tape_budget_mb = 8192;  // differentiable PBF / DFSPH: device memory for resident segment tapes
     int stage_rows = 2048;          // staged rows per brick at most
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn
     bool phase_retry_all = false;   // IMM phase-transfer retries: every row, or rows near new flags
@@ -152,6 +153,7 @@ struct vtp_solver {
     size_t h_tick_bytes = 0;
     std::shared_ptr<vtp::ImmState> imm;
     std::shared_ptr<vtp::DiffState> diff;
+    std::shared_ptr<vtp::DfDiffState> dfdiff;   // differentiable DFSPH rollout
 
     // graphs: two parities (double-buffer swaps alternate between substeps)
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -216,6 +218,7 @@ struct vtp_solver {
         if (ev_join) cudaEventDestroy(ev_join), ev_join = nullptr;
         imm.reset();
         diff.reset();
+        dfdiff.reset();
         graphs_ready = false;
         initialized = false;
     }

@@ -78,6 +78,7 @@ SIGNATURES = {
     "vtp_solver_diff_forward": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int]),
     "vtp_solver_diff_backward": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(C.c_double)]),
     "vtp_solver_diff_lists": (C.c_int, [_P, C.c_uint32, _P, _P, C.c_uint32]),
+    "vtp_solver_diff_iterations": (C.c_int, [_P, C.c_uint32, _P, _P]),
     "vtp_solver_dfsph_solve_forward": (C.c_int, [_P, C.c_int, _P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "vtp_solver_dfsph_solve_backward": (C.c_int, [_P, _P, _P]),
     "vtp_ugns_neighbors_noalloc": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,

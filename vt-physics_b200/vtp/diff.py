@@ -22,7 +22,8 @@ def diff_forward(s, steps: int, checkpoint_every: int = 20, keep_lists: bool = F
 
 
 def diff_backward(s, dl_dpos=None, dl_dvel=None):
-    """dL/d(final pos, vel) (n x 3, attach order) -> (dL/dpos0, dL/dvel0, dL/dXSPH_k)."""
+    """dL/d(final pos, vel) (n x 3, attach order) -> (dL/dpos0, dL/dvel0, dL/dparam), the
+    parameter being XSPH_k (PBF) or fPartRestViscosity (DFSPH)."""
     n = s.counts()["total"]
 
     def arr(a):
@@ -47,6 +48,13 @@ def diff_lists(s, step: int, max_nbr: int):
     nb = np.empty((n, max_nbr), np.uint32)
     check(lib().vtp_solver_diff_lists(s._h, int(step), cnt.ctypes.data, nb.ctypes.data, int(max_nbr)), "diff_lists")
     return cnt, nb
+
+
+def diff_iterations(s, step: int):
+    """DFSPH: (divergence, density) pressure-solve iterations of recorded substep `step`."""
+    di, ii = C.c_uint32(), C.c_uint32()
+    check(lib().vtp_solver_diff_iterations(s._h, int(step), C.byref(di), C.byref(ii)), "diff_iterations")
+    return di.value, ii.value
 
 
 def pbf_solver(scene, v0_fluid=None, xsph_k=None, extra=None):
