@@ -258,6 +258,22 @@ def diff_pbf(seed: int = 5005) -> Scene:
                               SceneObject("box", wall, EPM_BOUNDARY)])
 
 
+def diff_dfsph(seed: int = 5005) -> Scene:
+    """The differentiable DFSPH scene: a 40^3 lattice (spacing 0.01, lb 0.1, no jitter, 64,000
+    fluid particles) in a 3-layer [0, 0.6]^3 box, initial fluid velocities N(0, 0.1^2) per
+    component (SplitMix64 stream ``seed``, Box-Muller), DFSPH parameters of the dam break
+    (dt 1 ms fixed, thresholds 0.1 %, viscosity 1e-6, no surface tension)."""
+    r = 0.005
+    fluid = cube(r, (0.1, 0.1, 0.1), (0.4, 0.4, 0.4))
+    wall = box(r, (0.0, 0.0, 0.0), (0.6, 0.6, 0.6), 3)
+    u = splitmix64_uniform(seed, 2 * fluid.shape[0] * 3).reshape(2, -1)
+    z = np.sqrt(-2.0 * np.log1p(-u[0])) * np.cos(2.0 * np.pi * u[1])
+    v0 = (0.1 * z).reshape(-1, 3).astype(np.float32)
+    cfg = dfsph_config(dt=1e-3, r=r, lb=(-0.05, -0.05, -0.05), size=(0.7, 0.7, 0.7))
+    return Scene("DFSPH", cfg, [SceneObject("fluid", fluid, EPM_FLUID, export_flag=True, velocity=v0),
+                                SceneObject("box", wall, EPM_BOUNDARY)])
+
+
 def batched_scenes(count: int = 64, n_pbf: int = 48, seed: int = 4242, gravity_seed: int = 4243,
                    n_min: float = 4e3, n_max: float = 2.56e5, pbf_spacing: float | None = None) -> list:
     """The batched mix: ``count`` dam breaks, the first ``n_pbf`` PBF and the rest DFSPH.
