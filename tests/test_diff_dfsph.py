@@ -164,3 +164,32 @@ def test_gpu_dfsph_rollout_rejects_unsupported_settings(vtp_gpu):
     with pytest.raises(vtp_gpu.VtpError, match="surface-tension"):
         diff.diff_forward(s, 2, 1)
     s.destroy()
+
+
+@pytest.mark.gpu
+def test_torch_autograd_dfsph_rollout(vtp_gpu):
+    """The torch wrapper's gradients are the C ABI's for the same loss."""
+    import torch
+    from vtp import diff
+    sc = gpu_case(seed=9, n=2000)
+    mask = diff.fluid_mask(sc)
+    f = sc.objects[0]
+    roll = diff.make_dfsph_rollout(sc, steps=4, checkpoint_every=2)
+    x0 = torch.tensor(f.pos, requires_grad=True)
+    v0 = torch.tensor(f.velocity, requires_grad=True)
+    x, v = roll(x0, v0)
+    w = torch.linspace(-1.0, 1.0, 3, dtype=torch.float64)
+    loss = (x.double().mean(0) * w).sum() + (v.double() ** 2).sum() * 1e-3
+    loss.backward()
+    s = vtp_gpu.solver_from_scene(sc)
+    assert s.initialize()
+    diff.diff_forward(s, 4, 2)
+    n = mask.size
+    gx = np.zeros((n, 3), np.float32)
+    gv = np.zeros((n, 3), np.float32)
+    gx[mask] = np.broadcast_to((w.numpy() / mask.sum()).astype(np.float32), (mask.sum(), 3))
+    gv[mask] = 2e-3 * s.get_field("vel")[mask]
+    ox, ov, _ = diff.diff_backward(s, gx, gv)
+    s.destroy()
+    assert np.allclose(x0.grad.numpy(), ox[mask], rtol=1e-5, atol=1e-9)
+    assert np.allclose(v0.grad.numpy(), ov[mask], rtol=1e-5, atol=1e-9)

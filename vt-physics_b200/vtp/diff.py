@@ -1,4 +1,4 @@
-"""Differentiable PBF through the C ABI, and its torch.autograd wrapper.
+"""Differentiable PBF and DFSPH through the C ABI, and their torch.autograd wrappers.
 
 The adjoint itself is the library's (vtp_solver_diff_forward / _backward:
 checkpointed forward, per-segment recompute into a tape with the substep
@@ -115,6 +115,50 @@ def make_rollout(scene, steps: int, checkpoint_every: int = 20, extra=None):
             return torch.from_numpy(gv[mask].copy()).to(dev), torch.tensor(gk, dtype=torch.float32, device=dev)
 
     return PbfRollout.apply
+
+
+def make_dfsph_rollout(scene, steps: int, checkpoint_every: int = 10, extra=None):
+    """torch.autograd.Function: (fluid positions x0 [nf, 3], fluid velocities v0 [nf, 3]) ->
+    (fluid positions, fluid velocities) after `steps` DFSPH substeps; the backward is the
+    library's adjoint of the rollout (lists, iteration counts and clamps of the forward)."""
+    import torch
+
+    mask = fluid_mask(scene)
+
+    class DfsphRollout(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x0, v0):
+            from .solver import solver_from_scene
+            s = solver_from_scene(scene, extra=extra)
+            if not s.initialize():
+                raise RuntimeError(s.last_error)
+            for name, val in (("pos", x0), ("vel", v0)):
+                full = s.get_field(name)
+                full[mask] = val.detach().cpu().numpy()
+                s.set_field(name, full)
+            diff_forward(s, steps, checkpoint_every)
+            ctx.solver = s
+            dev = x0.device
+            return (torch.from_numpy(s.get_field("pos")[mask].copy()).to(dev),
+                    torch.from_numpy(s.get_field("vel")[mask].copy()).to(dev))
+
+        @staticmethod
+        def backward(ctx, gx, gv):
+            s = ctx.solver
+            n = s.counts()["total"]
+            dx = np.zeros((n, 3), np.float32)
+            dv = np.zeros((n, 3), np.float32)
+            if gx is not None:
+                dx[mask] = gx.detach().cpu().numpy()
+            if gv is not None:
+                dv[mask] = gv.detach().cpu().numpy()
+            ox, ov, _ = diff_backward(s, dx, dv)
+            s.destroy()
+            ctx.solver = None
+            dev = (gx if gx is not None else gv).device
+            return torch.from_numpy(ox[mask].copy()).to(dev), torch.from_numpy(ov[mask].copy()).to(dev)
+
+    return DfsphRollout.apply
 
 
 def dfsph_solve(s, v_in, which: int = 0, force_iters: int = 0):
