@@ -177,19 +177,27 @@ def test_torch_autograd_dfsph_rollout(vtp_gpu):
     roll = diff.make_dfsph_rollout(sc, steps=4, checkpoint_every=2)
     x0 = torch.tensor(f.pos, requires_grad=True)
     v0 = torch.tensor(f.velocity, requires_grad=True)
-    x, v = roll(x0, v0)
     w = torch.linspace(-1.0, 1.0, 3, dtype=torch.float64)
-    loss = (x.double().mean(0) * w).sum() + (v.double() ** 2).sum() * 1e-3
-    loss.backward()
+
+    def loss_of(x, v):
+        return (x.double().mean(0) * w).sum() + (v.double() ** 2).sum() * 1e-3
+
+    x, v = roll(x0, v0)
+    loss_of(x, v).backward()
+    # the same loss through the C ABI: dL/d(output) from torch, then the library's backward
     s = vtp_gpu.solver_from_scene(sc)
     assert s.initialize()
     diff.diff_forward(s, 4, 2)
+    xo = torch.tensor(s.get_field("pos")[mask], requires_grad=True)
+    vo = torch.tensor(s.get_field("vel")[mask], requires_grad=True)
+    assert torch.equal(xo, x.detach()) and torch.equal(vo, v.detach())
+    loss_of(xo, vo).backward()
     n = mask.size
     gx = np.zeros((n, 3), np.float32)
     gv = np.zeros((n, 3), np.float32)
-    gx[mask] = np.broadcast_to((w.numpy() / mask.sum()).astype(np.float32), (mask.sum(), 3))
-    gv[mask] = 2e-3 * s.get_field("vel")[mask]
+    gx[mask] = xo.grad.numpy()
+    gv[mask] = vo.grad.numpy()
     ox, ov, _ = diff.diff_backward(s, gx, gv)
     s.destroy()
-    assert np.allclose(x0.grad.numpy(), ox[mask], rtol=1e-5, atol=1e-9)
-    assert np.allclose(v0.grad.numpy(), ov[mask], rtol=1e-5, atol=1e-9)
+    assert np.array_equal(x0.grad.numpy(), ox[mask])
+    assert np.array_equal(v0.grad.numpy(), ov[mask])
