@@ -55,6 +55,7 @@ struct DfDiffState {
     std::vector<DfTape> tapes;
     std::vector<int> taped;
     float4 *bstat = nullptr;      // [n] boundary rows {v_b, 0}, copied into every record
+    uint32_t hint[2] = {2, 2};    // iterations of the last recorded divergence / density solve
     // adjoint work arrays
     float4 *xbar_a = nullptr, *vbar_a = nullptr;    // attach order [n]
     float4 *xbar = nullptr, *vb[2] = {nullptr, nullptr}, *a1b = nullptr;
@@ -155,42 +156,64 @@ __global__ void k_dfd_gather(DfdArgs a) {
     a.abar[r] = 0.f;
 }
 
+// The neighbour passes of the adjoint split each row's list over L lanes (consecutive
+// threads; lane l takes entries l, l + L, ...) and sum the lanes' partials with a shuffle
+// butterfly: at the tens of thousands of rows a differentiable scene has, one thread per
+// row leaves most warp slots of the GPU empty and every gather's latency exposed.
+template <int L>
+__device__ __forceinline__ float lanes_sum(float v) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Pressure-solve iteration adjoint, pass A: kappa-bar_i = sum_j gradW_ij.w_ij with
 // w_ij = c_j V_i vb_j - c_i V_j vb_i (c = dt V / m; the j term only for fluid j), then
 // delta-bar (clamp of the forward), ratio-bar and alpha-bar, and the position adjoint of
 // the velocity update: x-bar_i += sum_j (kappa_i + kappa_j) J_ij w_ij.
+template <int L>
 __global__ void __launch_bounds__(256) k_dfd_iter_a(DfdArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const float4 p = a.x[r], vi = a.vb[r];
-    const float ki = a.rec[r].w;
-    const float ci = a.dt * p.w / a.mass_f;
-    const uint32_t n = a.ncnt[r];
-    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    float kb = 0.f, xx = 0.f, xy = 0.f, xz = 0.f;
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = __ldg(a.x + j);
-        const bool fj = j < a.nf;
-        const float kj = __ldg(&a.rec[j].w);   // 0 for boundary rows
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float d2 = dist2(rx, ry, rz);
-        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
-        float wx = -ci * q.w * vi.x, wy = -ci * q.w * vi.y, wz = -ci * q.w * vi.z;
-        if (fj) {
-            const float4 vj = __ldg(a.vb + j);
-            const float cj = a.dt * q.w / a.mass_f * p.w;
-            wx += cj * vj.x;
-            wy += cj * vj.y;
-            wz += cj * vj.z;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = g / L, lane = g % L;
+    const bool live = r < a.nf;
+    float kb = 0.f, xx = 0.f, xy = 0.f, xz = 0.f, ki = 0.f;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        p = a.x[r];
+        const float4 vi = a.vb[r];
+        ki = a.rec[r].w;
+        const float ci = a.dt * p.w / a.mass_f;
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        for (uint32_t t = lane; t + 1 < n; t += L) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = __ldg(a.x + j);
+            const bool fj = j < a.nf;
+            const float kj = __ldg(&a.rec[j].w);   // 0 for boundary rows
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float d2 = dist2(rx, ry, rz);
+            const float gg = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+            float wx = -ci * q.w * vi.x, wy = -ci * q.w * vi.y, wz = -ci * q.w * vi.z;
+            if (fj) {
+                const float4 vj = __ldg(a.vb + j);
+                const float cj = a.dt * q.w / a.mass_f * p.w;
+                wx += cj * vj.x;
+                wy += cj * vj.y;
+                wz += cj * vj.z;
+            }
+            const float rw = rx * wx + ry * wy + rz * wz;
+            kb += gg * rw;
+            const float kk = ki + kj;
+            xx += kk * (gg * wx + hh * rx * rw);
+            xy += kk * (gg * wy + hh * ry * rw);
+            xz += kk * (gg * wz + hh * rz * rw);
         }
-        const float rw = rx * wx + ry * wy + rz * wz;
-        kb += g * rw;
-        const float kk = ki + kj;
-        xx += kk * (g * wx + hh * rx * rw);
-        xy += kk * (g * wy + hh * ry * rw);
-        xz += kk * (g * wz + hh * rz * rw);
     }
+    kb = lanes_sum<L>(kb);
+    xx = lanes_sum<L>(xx);
+    xy = lanes_sum<L>(xy);
+    xz = lanes_sum<L>(xz);
+    if (!live || lane != 0) return;
     float4 xb = a.xbar[r];
     xb.x += xx; xb.y += xy; xb.z += xz;
     a.xbar[r] = xb;
@@ -204,30 +227,41 @@ __global__ void __launch_bounds__(256) k_dfd_iter_a(DfdArgs a) {
 // Pressure-solve iteration adjoint, pass B: the delta term's adjoints,
 // vb_i += dt sum_j (V_j db_i + V_i db_j) gradW_ij and
 // x-bar_i += dt sum_j (V_j db_i + V_i db_j) J_ij (v*_i - v*_j) (db_j only for fluid j).
+template <int L>
 __global__ void __launch_bounds__(256) k_dfd_iter_b(DfdArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const float4 p = a.x[r], si = a.rec[r];
-    const float di = a.db[r];
-    const uint32_t n = a.ncnt[r];
-    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = g / L, lane = g % L;
+    const bool live = r < a.nf;
     float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f;
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = __ldg(a.x + j), sj = __ldg(a.rec + j);
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float d2 = dist2(rx, ry, rz);
-        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
-        const float c = a.dt * (q.w * di + (j < a.nf ? p.w * __ldg(a.db + j) : 0.f));
-        const float ux = si.x - sj.x, uy = si.y - sj.y, uz = si.z - sj.z;
-        const float ru = rx * ux + ry * uy + rz * uz;
-        vx += c * g * rx;
-        vy += c * g * ry;
-        vz += c * g * rz;
-        xx += c * (g * ux + hh * rx * ru);
-        xy += c * (g * uy + hh * ry * ru);
-        xz += c * (g * uz + hh * rz * ru);
+    if (live) {
+        const float4 p = a.x[r], si = a.rec[r];
+        const float di = a.db[r];
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        for (uint32_t t = lane; t + 1 < n; t += L) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = __ldg(a.x + j), sj = __ldg(a.rec + j);
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float d2 = dist2(rx, ry, rz);
+            const float gg = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+            const float c = a.dt * (q.w * di + (j < a.nf ? p.w * __ldg(a.db + j) : 0.f));
+            const float ux = si.x - sj.x, uy = si.y - sj.y, uz = si.z - sj.z;
+            const float ru = rx * ux + ry * uy + rz * uz;
+            vx += c * gg * rx;
+            vy += c * gg * ry;
+            vz += c * gg * rz;
+            xx += c * (gg * ux + hh * rx * ru);
+            xy += c * (gg * uy + hh * ry * ru);
+            xz += c * (gg * uz + hh * rz * ru);
+        }
     }
+    vx = lanes_sum<L>(vx);
+    vy = lanes_sum<L>(vy);
+    vz = lanes_sum<L>(vz);
+    xx = lanes_sum<L>(xx);
+    xy = lanes_sum<L>(xy);
+    xz = lanes_sum<L>(xz);
+    if (!live || lane != 0) return;
     float4 v = a.vb[r];
     v.x += vx; v.y += vy; v.z += vz;
     a.vb[r] = v;
@@ -240,24 +274,28 @@ __global__ void __launch_bounds__(256) k_dfd_iter_b(DfdArgs a) {
 // x-bar_i += dt C sum_j [phi u (r.w) + (u.r)(phi w + psi r (r.w))] with u = vp_i - vp_j,
 // w = vb_i - vb_j, phi = g / (|r|^2 + eps), psi = 2 dphi/d|r|^2; block partials of
 // dL/dnu / V_f = sum_i dt vb_i . sum_j 10 (u.r) phi r.
+template <int L>
 __global__ void __launch_bounds__(256) k_dfd_visc(DfdArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    double part = 0.0;
-    if (r < a.nf) {
-        const float4 p = a.x[r], ui = a.vp[r], wi = a.vb[r];
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = g / L, lane = g % L;
+    const bool live = r < a.nf;
+    float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f, ps = 0.f;
+    float4 wi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        const float4 p = a.x[r], ui = a.vp[r];
+        wi = a.vb[r];
         const uint32_t n = a.ncnt[r];
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f, ps = 0.f;
-        for (uint32_t t = 0; t + 1 < n; ++t) {
+        for (uint32_t t = lane; t + 1 < n; t += L) {
             const uint32_t j = lst[(size_t)t * 32u];
             if (j >= a.nf) continue;   // same-material neighbours only
             const float4 q = __ldg(a.x + j), uj = __ldg(a.vp + j), wj = __ldg(a.vb + j);
             const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
             const float d2 = dist2(rx, ry, rz);
-            const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+            const float gg = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
             const float den = d2 + a.eps;
-            const float phi = g / den;
-            const float psi = hh / den - 2.f * g / (den * den);
+            const float phi = gg / den;
+            const float psi = hh / den - 2.f * gg / (den * den);
             const float ux = ui.x - uj.x, uy = ui.y - uj.y, uz = ui.z - uj.z;
             const float wx = wi.x - wj.x, wy = wi.y - wj.y, wz = wi.z - wj.z;
             const float ru = rx * ux + ry * uy + rz * uz, rw = rx * wx + ry * wy + rz * wz;
@@ -271,6 +309,16 @@ __global__ void __launch_bounds__(256) k_dfd_visc(DfdArgs a) {
             xz += cx * (phi * uz * rw + ru * (phi * wz + psi * rz * rw));
             ps += ru * phi * (rx * wi.x + ry * wi.y + rz * wi.z);
         }
+    }
+    vx = lanes_sum<L>(vx);
+    vy = lanes_sum<L>(vy);
+    vz = lanes_sum<L>(vz);
+    xx = lanes_sum<L>(xx);
+    xy = lanes_sum<L>(xy);
+    xz = lanes_sum<L>(xz);
+    ps = lanes_sum<L>(ps);
+    double part = 0.0;
+    if (live && lane == 0) {
         a.vb_out[r] = make_float4(wi.x + vx, wi.y + vy, wi.z + vz, 0.f);
         float4 xb = a.xbar[r];
         xb.x += xx; xb.y += xy; xb.z += xz;
@@ -290,26 +338,31 @@ __global__ void k_dfd_vreduce(const double *part, uint32_t nb, double vol_f, dou
 
 // alpha adjoint, pass 1: a1-bar_i = alpha-bar_i 2 a1_i / m (a1 recomputed), with
 // alpha-bar zeroed where the forward clamped alpha; stored {a1-bar, alpha-bar}.
+template <int L>
 __global__ void __launch_bounds__(256) k_dfd_a1(DfdArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const bool live = a.alpha[r] > 1e-6f;
-    const float ab = live ? a.abar[r] : 0.f;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = g / L, lane = g % L;
+    const bool live = r < a.nf && a.alpha[r] > 1e-6f;
     float ax = 0.f, ay = 0.f, az = 0.f;
     if (live) {
         const float4 p = a.x[r];
         const uint32_t n = a.ncnt[r];
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        for (uint32_t t = 0; t + 1 < n; ++t) {
+        for (uint32_t t = lane; t + 1 < n; t += L) {
             const uint32_t j = lst[(size_t)t * 32u];
             const float4 q = __ldg(a.x + j);
             const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-            const float g = cubic_g(dist2(rx, ry, rz), a.k) * q.w;
-            ax += g * rx;
-            ay += g * ry;
-            az += g * rz;
+            const float gg = cubic_g(dist2(rx, ry, rz), a.k) * q.w;
+            ax += gg * rx;
+            ay += gg * ry;
+            az += gg * rz;
         }
     }
+    ax = lanes_sum<L>(ax);
+    ay = lanes_sum<L>(ay);
+    az = lanes_sum<L>(az);
+    if (r >= a.nf || lane != 0) return;
+    const float ab = live ? a.abar[r] : 0.f;
     const float c = 2.f * ab / a.mass_f;
     a.a1b[r] = make_float4(c * ax, c * ay, c * az, ab);
 }
@@ -317,33 +370,41 @@ __global__ void __launch_bounds__(256) k_dfd_a1(DfdArgs a) {
 // ratio / alpha adjoint, pass 2: x-bar_i += sum_j (ratio-bar_i V_j + ratio-bar_j V_i) g r
 // + J (V_j a1-bar_i - V_i a1-bar_j) + 2 g (g + hh |r|^2) (alpha-bar_i V_j^2 + alpha-bar_j V_i^2) / m r
 // (the j terms only for fluid j); then this substep's rows -> attach order.
+template <int L>
 __global__ void __launch_bounds__(256) k_dfd_ratio_x(DfdArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
-    const float4 p = a.x[r], Ai = a.a1b[r];
-    const float rbi = a.rbar[r];
-    const uint32_t n = a.ncnt[r];
-    const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-    const float im = 1.f / a.mass_f;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = g / L, lane = g % L;
+    const bool live = r < a.nf;
     float xx = 0.f, xy = 0.f, xz = 0.f;
-    for (uint32_t t = 0; t + 1 < n; ++t) {
-        const uint32_t j = lst[(size_t)t * 32u];
-        const float4 q = __ldg(a.x + j);
-        const bool fj = j < a.nf;
-        const float4 Aj = fj ? __ldg(a.a1b + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float rbj = fj ? __ldg(a.rbar + j) : 0.f;
-        const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
-        const float d2 = dist2(rx, ry, rz);
-        const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
-        const float cr = rbi * q.w + rbj * p.w;
-        const float c2 = fj ? 2.f * g * (g + hh * d2) * (Ai.w * q.w * q.w + Aj.w * p.w * p.w) * im : 0.f;
-        const float wx = q.w * Ai.x - p.w * Aj.x, wy = q.w * Ai.y - p.w * Aj.y, wz = q.w * Ai.z - p.w * Aj.z;
-        const float rw = rx * wx + ry * wy + rz * wz;
-        const float s = cr * g + c2;
-        xx += s * rx + g * wx + hh * rx * rw;
-        xy += s * ry + g * wy + hh * ry * rw;
-        xz += s * rz + g * wz + hh * rz * rw;
+    if (live) {
+        const float4 p = a.x[r], Ai = a.a1b[r];
+        const float rbi = a.rbar[r];
+        const uint32_t n = a.ncnt[r];
+        const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
+        const float im = 1.f / a.mass_f;
+        for (uint32_t t = lane; t + 1 < n; t += L) {
+            const uint32_t j = lst[(size_t)t * 32u];
+            const float4 q = __ldg(a.x + j);
+            const bool fj = j < a.nf;
+            const float4 Aj = fj ? __ldg(a.a1b + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float rbj = fj ? __ldg(a.rbar + j) : 0.f;
+            const float rx = p.x - q.x, ry = p.y - q.y, rz = p.z - q.z;
+            const float d2 = dist2(rx, ry, rz);
+            const float gg = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+            const float cr = rbi * q.w + rbj * p.w;
+            const float c2 = fj ? 2.f * gg * (gg + hh * d2) * (Ai.w * q.w * q.w + Aj.w * p.w * p.w) * im : 0.f;
+            const float wx = q.w * Ai.x - p.w * Aj.x, wy = q.w * Ai.y - p.w * Aj.y, wz = q.w * Ai.z - p.w * Aj.z;
+            const float rw = rx * wx + ry * wy + rz * wz;
+            const float s = cr * gg + c2;
+            xx += s * rx + gg * wx + hh * rx * rw;
+            xy += s * ry + gg * wy + hh * ry * rw;
+            xz += s * rz + gg * wz + hh * rz * rw;
+        }
     }
+    xx = lanes_sum<L>(xx);
+    xy = lanes_sum<L>(xy);
+    xz = lanes_sum<L>(xz);
+    if (!live || lane != 0) return;
     float4 xb = a.xbar[r];
     xb.x += xx; xb.y += xy; xb.z += xz;
     const uint32_t id = a.orig[r];
@@ -445,20 +506,34 @@ int df_record_solve(vtp_solver &s, DfDiffState &d, DfTape &tape, DfTapeSlot &slo
     vtp::dfsph_solve_pack(s.st, a);
     slot.first[which] = pool;
     const uint32_t nf = s.L.nf;
-    uint32_t it = 0;
-    for (; it < 101; ++it) {
-        float4 *rec = nullptr;
-        int rc = df_record_slot(s, d, tape, pool++, &rec);
-        if (rc) return rc;
-        vtp::dfsph_solve_a(s.st, a, s.block);
-        if (nf) vtp::k_dfd_record<<<vtp::nblk(nf, 256), 256, 0, s.st>>>(nf, a.vadv, a.kappa, rec);
-        vtp::dfsph_solve_b(s.st, a, s.block);
-        vtp::dfsph_solve_end(s.st, c, s.partials, s.d_status);
-        CU(cudaMemcpyAsync(s.h_pinned + 2, &s.loop[which].running, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+    // Iterations are enqueued in chunks and the stop flag read once per chunk: an iteration
+    // enqueued after the stop test has stopped the solve is a no-op (solve_a and solve_b skip a
+    // stopped scene's tiles, solve_end leaves its state alone), and its record lands in a slot
+    // past the solve's last, which the next solve overwrites.  The first chunk is as long as
+    // the previous substep's solve of this kind was.
+    const vtp::SolveState *state = s.solve + (size_t)which * s.scenes.size();
+    uint32_t issued = 0, iters = 0;
+    uint32_t chunk = std::max<uint32_t>(d.hint[which], 1u);
+    for (;;) {
+        for (uint32_t c2 = 0; c2 < chunk; ++c2, ++issued) {
+            float4 *rec = nullptr;
+            int rc = df_record_slot(s, d, tape, pool + issued, &rec);
+            if (rc) return rc;
+            vtp::dfsph_solve_a(s.st, a, s.block);
+            if (nf) vtp::k_dfd_record<<<vtp::nblk(nf, 256), 256, 0, s.st>>>(nf, a.vadv, a.kappa, rec);
+            vtp::dfsph_solve_b(s.st, a, s.block);
+            vtp::dfsph_solve_end(s.st, c, s.partials, s.d_status);
+        }
+        CU(cudaMemcpyAsync(s.h_pinned + 2, state, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
         CU(cudaStreamSynchronize(s.st));
-        if (!s.h_pinned[2]) break;
+        iters = s.h_pinned[2];
+        if (s.h_pinned[3] || issued >= 101) break;   // stopped (the stop test ends every solve by 101)
+        chunk = 2;
     }
-    slot.iters[which] = std::min<uint32_t>(it + 1, 101);
+    iters = std::min<uint32_t>(std::max<uint32_t>(iters, 1u), 101u);
+    pool += iters;
+    slot.iters[which] = iters;
+    d.hint[which] = iters;
     return VTP_OK;
 }
 
@@ -519,11 +594,20 @@ int df_record_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool re
     return s.check_status();
 }
 
-int df_adjoint_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp) {
+// Lanes per row of the adjoint's neighbour passes: enough rows x lanes to fill the GPU's
+// thread slots (148 SMs x 2048), at most 8.
+int df_lanes(uint32_t nf) {
+    const uint64_t slots = 148ull * 2048ull;
+    int l = 1;
+    while (l < 8 && (uint64_t)nf * l < slots) l *= 2;
+    return l;
+}
+
+template <int L>
+int df_adjoint_segment_l(vtp_solver &s, DfDiffState &d, uint32_t k, int tp) {
     const uint32_t nf = d.nf;
-    if (!nf) return VTP_OK;
     const DfTape &tape = d.tapes[tp];
-    const unsigned G = vtp::nblk(nf, 256);
+    const unsigned G = vtp::nblk(nf, 256), GL = vtp::nblk(nf * (uint32_t)L, 256);
     vtp::DfdArgs a{};
     a.nf = nf; a.ell_stride = s.L.ell_stride; a.k = s.kc;
     a.dt = s.dt; a.mass_f = s.rho_f * s.vol0;
@@ -540,22 +624,32 @@ int df_adjoint_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp) {
         for (int w = 1; w >= 0; --w) {
             for (int it = (int)T.iters[w] - 1; it >= 0; --it) {
                 a.rec = tape.recs[T.first[w] + it];
-                vtp::k_dfd_iter_a<<<G, 256, 0, s.st>>>(a);
-                vtp::k_dfd_iter_b<<<G, 256, 0, s.st>>>(a);
+                vtp::k_dfd_iter_a<L><<<GL, 256, 0, s.st>>>(a);
+                vtp::k_dfd_iter_b<L><<<GL, 256, 0, s.st>>>(a);
             }
             if (w == 1) {
                 a.vb_out = d.vb[cur ^ 1];
-                vtp::k_dfd_visc<<<G, 256, 0, s.st>>>(a);
-                vtp::k_dfd_vreduce<<<1, 256, 0, s.st>>>(d.vpart, G, (double)s.vol0, d.vacc);
+                vtp::k_dfd_visc<L><<<GL, 256, 0, s.st>>>(a);
+                vtp::k_dfd_vreduce<<<1, 256, 0, s.st>>>(d.vpart, GL, (double)s.vol0, d.vacc);
                 cur ^= 1;
                 a.vb = d.vb[cur];
             }
         }
-        vtp::k_dfd_a1<<<G, 256, 0, s.st>>>(a);
-        vtp::k_dfd_ratio_x<<<G, 256, 0, s.st>>>(a);
+        vtp::k_dfd_a1<L><<<GL, 256, 0, s.st>>>(a);
+        vtp::k_dfd_ratio_x<L><<<GL, 256, 0, s.st>>>(a);
     }
     CU(cudaGetLastError());
     return VTP_OK;
+}
+
+int df_adjoint_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp) {
+    if (!d.nf) return VTP_OK;
+    switch (df_lanes(d.nf)) {
+        case 1: return df_adjoint_segment_l<1>(s, d, k, tp);
+        case 2: return df_adjoint_segment_l<2>(s, d, k, tp);
+        case 4: return df_adjoint_segment_l<4>(s, d, k, tp);
+        default: return df_adjoint_segment_l<8>(s, d, k, tp);
+    }
 }
 
 // Forward of a recorded rollout: checkpoint, then the ordinary substeps up to the next
@@ -653,7 +747,7 @@ int dfsph_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_ever
                                    cudaMemcpyDeviceToDevice, s->st));
         }
     }
-    d->blocks = nblk((uint32_t)nf, 256);
+    d->blocks = nblk((uint32_t)nf * 8u, 256);   // viscosity partials: one per block at up to 8 lanes per row
     if ((rc = d->alloc(&d->xbar_a, n)) || (rc = d->alloc(&d->vbar_a, n)) || (rc = d->alloc(&d->xbar, nf)) ||
         (rc = d->alloc(&d->vb[0], nf)) || (rc = d->alloc(&d->vb[1], nf)) || (rc = d->alloc(&d->a1b, nf)) ||
         (rc = d->alloc(&d->db, nf)) || (rc = d->alloc(&d->rbar, nf)) || (rc = d->alloc(&d->abar, nf)) ||
