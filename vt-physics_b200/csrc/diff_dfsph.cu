@@ -41,9 +41,22 @@ struct DfTapeSlot {
     uint32_t first[2] = {0, 0}; // their first record in the tape's record pool
 };
 
+// Record pointers a tape's graph-recorded segment can address (the device table's size).
+constexpr uint32_t kRecTable = 8192;
+
 struct DfTape {
     std::vector<DfTapeSlot> slots;
     std::vector<float4 *> recs;   // [n] {v* entering the iteration, its kappa}; boundary rows {v_b, 0}
+    // Graph-recorded segments: the segment's substeps captured once into `exec` (buffer parity
+    // `par` at its start), the solve loops as WHILE nodes; each iteration's record is recs[pool +
+    // iteration], pool = ctl[0] (advanced by each solve's iteration count), up to cap[0] records.
+    float4 **d_recs = nullptr;    // [kRecTable] device copy of recs
+    uint32_t *d_cap = nullptr;    // [1] records d_recs holds
+    uint32_t *d_ctl = nullptr;    // [2] pool counter, overflow flag
+    uint32_t *d_info = nullptr;   // [slots][4] first record and iterations of each slot's two solves
+    uint32_t uploaded = 0;        // recs entries copied to d_recs
+    cudaGraphExec_t exec = nullptr;
+    int par[4] = {-1, -1, -1, -1};
 };
 
 struct DfDiffState {
@@ -63,8 +76,13 @@ struct DfDiffState {
     double *vpart = nullptr, *vacc = nullptr;
     uint32_t blocks = 0;
 
+    uint32_t *h_info = nullptr;   // page-locked: one tape's d_info and d_ctl after a graph-recorded segment
+
     ~DfDiffState() {
+        for (auto &t : tapes)
+            if (t.exec) cudaGraphExecDestroy(t.exec);
         for (void *p : mem) cudaFree(p);
+        if (h_info) cudaFreeHost(h_info);
     }
     template <class T>
     int alloc(T **p, size_t count) {
@@ -134,6 +152,35 @@ __global__ void k_dfd_record(uint32_t nf, const float4 *__restrict__ vadv, const
     if (r >= nf) return;
     const float4 v = vadv[r];
     out[r] = make_float4(v.x, v.y, v.z, kappa[r]);
+}
+
+// Graph-recorded solves: the record of the running iteration is recs[ctl[0] + st->iter] (the
+// solve's iterations so far); past the table's valid records the overflow flag is set and the
+// record skipped (the host grows the table and replays the segment).
+__global__ void k_dfd_record_dev(uint32_t nf, const float4 *__restrict__ vadv, const float *__restrict__ kappa,
+                                 const SolveState *st, float4 *const *recs, const uint32_t *cap, uint32_t *ctl) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t idx = ctl[0] + st->iter;
+    if (idx >= *cap) {
+        if (r == 0) ctl[1] = 1u;
+        return;
+    }
+    if (r >= nf) return;
+    const float4 v = vadv[r];
+    recs[idx][r] = make_float4(v.x, v.y, v.z, kappa[r]);
+}
+
+// After a graph-recorded solve: its first record and iteration count, and the pool advanced.
+__global__ void k_dfd_solve_done(const SolveState *st, uint32_t *ctl, uint32_t *info) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t it = st->iter;
+    info[0] = ctl[0];
+    info[1] = it;
+    ctl[0] += it;
+}
+
+__global__ void k_dfd_tick_add(uint64_t *tick, uint32_t k) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *tick += k;
 }
 
 // Recording: the velocity after the divergence solve (second half of the packed rows).
@@ -583,7 +630,8 @@ int df_record_substep(vtp_solver &s, DfDiffState &d, DfTape &tape, DfTapeSlot &s
     return VTP_OK;
 }
 
-int df_record_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool recompute) {
+// A segment recorded with host-driven solve loops.
+int df_record_segment_host(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool recompute) {
     DfTape &tape = d.tapes[tp];
     uint32_t pool = 0;
     for (uint32_t t = 0; t < k; ++t) {
@@ -592,6 +640,188 @@ int df_record_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool re
     }
     CU(cudaStreamSynchronize(s.st));
     return s.check_status();
+}
+
+// Copies the record pointers the host-side pool has gained to the tape's device table (rare:
+// only when the pool grows; synchronous).
+int df_upload_recs(vtp_solver &s, DfTape &tape) {
+    const uint32_t n = (uint32_t)std::min<size_t>(tape.recs.size(), vtp::kRecTable);
+    if (n == tape.uploaded) return VTP_OK;
+    CU(cudaStreamSynchronize(s.st));
+    CU(cudaMemcpy(tape.d_recs + tape.uploaded, tape.recs.data() + tape.uploaded,
+                  (size_t)(n - tape.uploaded) * sizeof(float4 *), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(tape.d_cap, &n, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    tape.uploaded = n;
+    return VTP_OK;
+}
+
+// One pressure solve of a graph-recorded substep (being captured on s.st): the solve loop as a
+// WHILE node whose body is solve_a, the record, solve_b and the stop test, then the solve's
+// first record and iteration count into `info`.
+int df_capture_solve(vtp_solver &s, DfTape &tape, DfTapeSlot &slot, int which, uint32_t *info) {
+    vtp::DfsphArgs a = s.dfsph_args(which);
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::SolveState *state = s.solve + (size_t)which * s.scenes.size();
+    vtp::dfsph_solve_begin(s.st, state, s.loop + which, 1);
+    vtp::dfsph_solve_pack(s.st, a);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CU(cudaStreamGetCaptureInfo(s.st, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphConditionalHandle hnd;
+    CU(cudaGraphConditionalHandleCreate(&hnd, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hnd;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CU(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CU(cudaStreamUpdateCaptureDependencies(s.st, &node, 1, cudaStreamSetCaptureDependencies));
+    CU(cudaStreamBeginCaptureToGraph(s.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    vtp::SolveCtl c = s.solve_ctl(which, hnd, 1);
+    c.force_iters = which == 0 ? s.force_div : s.force_inc;
+    c.force_seq = nullptr;
+    c.scene_tiles = s.d_scene_tiles;   // the unstaged passes write one residual partial per tile
+    const uint32_t nf = s.L.nf;
+    vtp::dfsph_solve_a(s.side, a, s.block);
+    if (nf)
+        vtp::k_dfd_record_dev<<<vtp::nblk(nf, 256), 256, 0, s.side>>>(nf, a.vadv, a.kappa, state, tape.d_recs,
+                                                                      tape.d_cap, tape.d_ctl);
+    vtp::dfsph_solve_b(s.side, a, s.block);
+    vtp::dfsph_solve_end(s.side, c, s.partials, s.d_status);
+    cudaGraph_t out;
+    CU(cudaStreamEndCapture(s.side, &out));
+    vtp::k_dfd_solve_done<<<1, 32, 0, s.st>>>(state, tape.d_ctl, info);
+    return VTP_OK;
+}
+
+// One substep of a graph-recorded segment (being captured): df_record_substep with the solve
+// loops as WHILE nodes and the device substep counter left alone.
+int df_capture_substep(vtp_solver &s, DfTape &tape, DfTapeSlot &slot, uint32_t *info) {
+    const uint32_t nf = s.L.nf;
+    cudaStream_t st = s.st;
+    vtp::Carry carry{};
+    carry.nf4 = 1;
+    carry.src4[0] = s.vadv.c();
+    carry.dst4[0] = s.vadv.n();
+    vtp::ugns_sort(st, s.scn(), s.nbuckets, 0, nf, s.pos.c(), s.pos.n(), s.vel.c(), s.vel.n(), s.orig.c(),
+                   s.orig.n(), carry, 0.f, s.u, s.u.fstart);
+    s.pos.swap(); s.vel.swap(); s.orig.swap(); s.vadv.swap();
+    vtp::ugns_build_lists(st, s.scn(), s.L, 0, nf, s.pos.c(), s.orig.c(), s.u, slot.nbr, slot.ncnt, s.d_status,
+                          s.d_overflow, s.block);
+    if (nf) {
+        CU(cudaMemcpyAsync(slot.orig, s.orig.c(), nf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(slot.x, s.pos.c(), nf * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    }
+    vtp::DfsphArgs a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::dfsph_ratio_alpha(st, a, s.block);
+    if (nf) CU(cudaMemcpyAsync(slot.alpha, s.alpha, nf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    int rc;
+    if ((rc = df_capture_solve(s, tape, slot, 0, info))) return rc;
+    a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.staged = 0;
+    vtp::dfsph_pressure_pack(st, a);
+    if (nf) vtp::k_dfd_vp<<<vtp::nblk(nf, 256), 256, 0, st>>>(nf, s.pva, slot.vp);
+    vtp::dfsph_viscosity(st, a, s.block);
+    s.vel.swap(); s.vadv.swap();
+    if ((rc = df_capture_solve(s, tape, slot, 1, info + 2))) return rc;
+    a = s.dfsph_args();
+    a.nbr = slot.nbr;
+    a.ncnt = slot.ncnt;
+    a.tick = nullptr;
+    vtp::dfsph_finalize(st, a);
+    return VTP_OK;
+}
+
+// A segment of `every` substeps (an even number, so it ends at the buffer parity it started
+// from) replayed from the tape's captured graph: no readback until its end, where the solves'
+// records and iteration counts come back.  If the record table ran out, it is grown to the
+// segment's iteration total and the segment replayed from its checkpoint (ck_*), which the
+// solver's state equals on entry.  Returns 1 (nothing done) when the graph path does not apply.
+int df_record_segment_graph(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, const float4 *ck_p,
+                            const float4 *ck_v, const uint32_t *ck_o) {
+    DfTape &tape = d.tapes[tp];
+    if (!s.use_graphs || k != d.every || k % 2 != 0 || !d.nf || !tape.d_recs) return 1;
+    const int par[4] = {s.pos.cur, s.vel.cur, s.orig.cur, s.vadv.cur};
+    int rc;
+    if (!tape.exec) {
+        // records for one iteration of each solve to start with; the table grows on overflow
+        float4 *rec = nullptr;
+        if ((rc = df_record_slot(s, d, tape, 2 * k - 1, &rec)) || (rc = df_upload_recs(s, tape))) return rc;
+        CU(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeRelaxed));
+        cudaMemsetAsync(tape.d_ctl, 0, 2 * sizeof(uint32_t), s.st);
+        rc = VTP_OK;
+        for (uint32_t t = 0; t < k && !rc; ++t) rc = df_capture_substep(s, tape, tape.slots[t], tape.d_info + 4 * (size_t)t);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s.st, &g);
+        const bool same = s.pos.cur == par[0] && s.vel.cur == par[1] && s.orig.cur == par[2] && s.vadv.cur == par[3];
+        s.pos.cur = par[0]; s.vel.cur = par[1]; s.orig.cur = par[2]; s.vadv.cur = par[3];
+        cudaError_t e = !rc && ec == cudaSuccess && same ? cudaGraphInstantiate(&tape.exec, g, 0) : cudaErrorInvalidValue;
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {   // record this tape's segments with host-driven solves instead
+            cudaGetLastError();
+            tape.exec = nullptr;
+            tape.d_recs = nullptr;
+            return 1;
+        }
+        std::copy(par, par + 4, tape.par);
+    }
+    if (!std::equal(par, par + 4, tape.par)) return 1;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        CU(cudaMemcpyAsync(s.h_pinned + 4, s.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+        CU(cudaMemcpyAsync(s.h_pinned + 5, s.d_overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+        CU(cudaGraphLaunch(tape.exec, s.st));
+        CU(cudaMemcpyAsync(d.h_info, tape.d_info, 4 * (size_t)k * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+        CU(cudaMemcpyAsync(d.h_info + 4 * (size_t)k, tape.d_ctl, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+        CU(cudaStreamSynchronize(s.st));
+        if (!d.h_info[4 * (size_t)k + 1]) break;   // every record fitted
+        // Grow the table to the segment's iteration total (the counts are right: only
+        // records were skipped) and replay from the checkpoint, status words restored.
+        const uint32_t total = d.h_info[4 * (size_t)k];
+        if (attempt == 1 || total > vtp::kRecTable) return 2;
+        float4 *rec = nullptr;
+        if ((rc = df_record_slot(s, d, tape, total - 1, &rec)) || (rc = df_upload_recs(s, tape))) return rc;
+        if ((rc = df_restore(s, ck_p, ck_v, ck_o))) return rc;
+        CU(cudaMemcpyAsync(s.d_status, s.h_pinned + 4, sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+        CU(cudaMemcpyAsync(s.d_overflow, s.h_pinned + 5, sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+    }
+    for (uint32_t t = 0; t < k; ++t)
+        for (int w = 0; w < 2; ++w) {
+            tape.slots[t].first[w] = d.h_info[4 * t + 2 * w];
+            tape.slots[t].iters[w] = std::min<uint32_t>(std::max<uint32_t>(d.h_info[4 * t + 2 * w + 1], 1u), 101u);
+        }
+    return VTP_OK;
+}
+
+// The k substeps of a checkpoint segment recorded into tape `tp`, from checkpoint (ck_*),
+// which the solver's state equals on entry: replayed from the tape's graph where that applies,
+// else with host-driven solve loops.  forward: the device substep counter advances by k.
+int df_record_segment(vtp_solver &s, DfDiffState &d, uint32_t k, int tp, bool forward, const float4 *ck_p,
+                      const float4 *ck_v, const uint32_t *ck_o) {
+    int rc = df_record_segment_graph(s, d, k, tp, ck_p, ck_v, ck_o);
+    if (rc == VTP_OK) {
+        if (forward && s.d_tick) vtp::k_dfd_tick_add<<<1, 32, 0, s.st>>>(s.d_tick, k);
+        CU(cudaStreamSynchronize(s.st));
+        return s.check_status();
+    }
+    if (rc == 2) {   // the record table cannot hold the segment: host-driven from the checkpoint
+        if ((rc = df_restore(s, ck_p, ck_v, ck_o))) return rc;
+        CU(cudaMemcpyAsync(s.d_status, s.h_pinned + 4, sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+        CU(cudaMemcpyAsync(s.d_overflow, s.h_pinned + 5, sizeof(uint32_t), cudaMemcpyHostToDevice, s.st));
+    } else if (rc != 1) {
+        return rc;
+    }
+    return df_record_segment_host(s, d, k, tp, !forward);
 }
 
 // Lanes per row of the adjoint's neighbour passes: enough rows x lanes to fill the GPU's
@@ -664,7 +894,7 @@ int df_record_rollout(vtp_solver &s, DfDiffState &d) {
         const uint32_t k = std::min(d.every, d.steps - c * d.every);
         if (c + ntapes >= nchk) {
             const int tp = (int)(c + ntapes - nchk);
-            if ((rc = df_record_segment(s, d, k, tp, false))) return rc;
+            if ((rc = df_record_segment(s, d, k, tp, true, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
             for (uint32_t t = 0; t < k; ++t) {   // as tick_n advances them for the segments before
                 s.sim_time += s.dt;
                 ++s.steps_done;
@@ -735,7 +965,15 @@ int dfsph_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint_ever
     if (s->L.n > s->L.nf)
         k_bstat<<<nblk(s->L.n - s->L.nf, 256), 256, 0, s->st>>>(s->L.nf, s->L.n, s->vadv.c(), d->bstat);
     d->tapes.resize(ntapes);
+    if (cudaMallocHost((void **)&d->h_info, (4 * (size_t)every + 2) * sizeof(uint32_t)) != cudaSuccess) {
+        d->h_info = nullptr;
+        return fail(VTP_ERR_NOMEM, "differentiable DFSPH: page-locked readback buffer");
+    }
     for (auto &tape : d->tapes) {
+        if ((rc = d->alloc(&tape.d_recs, kRecTable)) || (rc = d->alloc(&tape.d_cap, 1)) ||
+            (rc = d->alloc(&tape.d_ctl, 2)) || (rc = d->alloc(&tape.d_info, 4 * (size_t)every)))
+            return rc;
+        CU(cudaMemsetAsync(tape.d_cap, 0, sizeof(uint32_t), s->st));
         tape.slots.resize(every);
         for (auto &slot : tape.slots) {
             if ((rc = d->alloc(&slot.orig, nf)) || (rc = d->alloc(&slot.nbr, std::max<size_t>(lrows, 1))) ||
@@ -784,7 +1022,7 @@ int dfsph_diff_backward(vtp_solver *s, const float *dl_dpos, const float *dl_dve
             // counts come from the stop test, which sees the forward's bits again.
             tp = 0;
             if ((rc = df_restore(*s, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
-            if ((rc = df_record_segment(*s, d, k, 0, true))) return rc;
+            if ((rc = df_record_segment(*s, d, k, 0, false, d.ck_pos[c], d.ck_vel[c], d.ck_orig[c]))) return rc;
         }
         if ((rc = df_adjoint_segment(*s, d, k, tp))) return rc;
     }
