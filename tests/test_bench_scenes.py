@@ -303,3 +303,55 @@ def test_diff_dfsph_64k_adjoint_matches_fp64_adjoint_and_fd(vtp_gpu, oracle_lib)
     assert smooth.sum() >= DFSPH_FD_DIRECTIONS - 2
     assert np.all(e_gpu_fd[smooth] < 1e-3)
     assert np.all(np.abs(e_gpu_fd - e_adj_fd)[~smooth] < 1e-3)
+
+
+def test_diff_dfsph_1m_adjoint_within_the_rounding_conditioning(vtp_gpu, oracle_lib):
+    """The DFSPH rollout adjoint at the headline scale: the 1M-fluid scene from the seeded
+    lattice at rest, two substeps with the benchmark window's iteration counts forced (3
+    divergence, 1 density: the two substeps' 8 solve iterations outgrow the graph-recorded
+    segment's first record table, so the segment is replayed from its checkpoint), a random
+    linear loss on the final fluid positions and velocities; the GPU adjoint (x0, v0 fields)
+    against the FP64 oracle's adjoint of the same discrete map (the GPU's lists and
+    iteration counts).
+
+    At this scale the adjoint of the clamped solve is ill-conditioned with respect to
+    rounding: the scene at rest has compression errors near the clamp delta = max(delta, 0)
+    throughout its bulk, and where the FP32 and FP64 trajectories' clamp patterns differ
+    their linearizations differ.  The bar is therefore the FP64 adjoint's own sensitivity,
+    measured in the same run: the FP64 adjoint at x0 moved by 1e-7 max|x0| (the size of an
+    FP32 rounding of the positions) per component.  The GPU adjoint must be no farther from
+    the FP64 adjoint than that (measured: 1.3e-2 / 6.4e-3 against 6.5e-2 / 3.1e-2 for
+    positions / velocities).  With the natural counts (52 divergence iterations in the
+    second substep) the two adjoints differ by 46 %."""
+    from vtp import diff
+    sc = vtp_gpu.scenes.dfsph_1m()
+    mask = diff.fluid_mask(sc)
+    n = mask.size
+    s = vtp_gpu.solver_from_scene(sc, extra={"forceDivIterations": 3, "forceIncompIterations": 1})
+    assert s.initialize()
+    x0, v0 = s.get_field("pos").astype(np.float64), s.get_field("vel").astype(np.float64)
+    maxnbr = int(sc.config["DFSPH"]["Required"]["maxNeighborNum"])
+    T = 2
+    diff.diff_forward(s, T, 2, keep_lists=True)
+    iters = [diff.diff_iterations(s, t) for t in range(T)]
+    lists = [diff.diff_lists(s, t, maxnbr) for t in range(T)]
+    rng = np.random.default_rng(2002)
+    A = (rng.normal(size=(n, 3)) * mask[:, None]).astype(np.float32)
+    B = (rng.normal(size=(n, 3)) * mask[:, None]).astype(np.float32)
+    gx, gv, _ = diff.diff_backward(s, A, B)
+    s.destroy()
+    assert iters == [(3, 1), (3, 1)]
+    d = oracle_lib.DfsphDiff(sc)
+
+    def fp64_adjoint(x):
+        _, _, states, used = d.rollout(x, v0, T, iters, lists=lists, record=True)
+        return d.adjoint(states, used, A.astype(np.float64), B.astype(np.float64))[:2]
+
+    ox, ov = fp64_adjoint(x0)
+    px, pv = fp64_adjoint(x0 + 1e-7 * np.abs(x0).max() * rng.normal(size=x0.shape) * mask[:, None])
+    rel = lambda a, b: float(np.linalg.norm(a[mask] - b[mask]) / np.linalg.norm(b[mask]))
+    ex, ev = rel(gx, ox), rel(gv, ov)
+    cx, cv = rel(px, ox), rel(pv, ov)
+    print(f"diff DFSPH 1M, {T} substeps (iterations {iters}): GPU vs FP64 adjoint x0 {ex:.2e} v0 {ev:.2e}; "
+          f"FP64 adjoint under a 1e-7 perturbation of x0: x0 {cx:.2e} v0 {cv:.2e}")
+    assert ex <= cx and ev <= cv
