@@ -17,8 +17,10 @@
 // the fluid state saved every k substeps; the last segments (as many as fit the tape
 // budget) run recording substeps: the substep's lists, positions, alpha, the velocity
 // after the divergence solve and, per pressure-solve iteration, {v* entering it, its
-// kappa}.  The solve loops of a recording substep are host-driven (one 4-byte
-// readback per iteration) because the tape needs one record per iteration.
+// kappa}.  A segment of an even checkpoint interval replays a CUDA graph captured once
+// per tape, its solve loops WHILE nodes whose iterations address their records on the
+// device (one readback per segment); other segments run host-driven solve loops that
+// read the stop flag once per chunk of iterations.
 // Backward: the segments last to first, each recomputed from its checkpoint into a
 // tape unless the forward recorded it, then the adjoint substeps in reverse.  Every
 // adjoint neighbour sum is in gather form over the same symmetric lists, so no pass
