@@ -124,6 +124,10 @@ def test_bad_extension_values_are_rejected():
     assert not s.setConfig(cfg) and "listLanes" in s.last_error
     cfg["B200"] = {"rowLanes": 2}
     assert not s.setConfig(cfg) and "rowLanes" in s.last_error
+    cfg["B200"] = {"adjointLanes": 3}
+    assert not s.setConfig(cfg) and "adjointLanes" in s.last_error
+    cfg["B200"] = {"adjointLanes": 4}
+    assert s.setConfig(cfg), s.last_error
     cfg["B200"] = {"phaseRetry": "some"}
     assert not s.setConfig(cfg) and "phaseRetry" in s.last_error
     cfg["B200"] = {"cellOrder": "hilbert"}

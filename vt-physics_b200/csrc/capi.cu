@@ -174,7 +174,7 @@ int vtp_solver::parse_config(const json &c) {
         force_seq.clear();
         device_loop = true; use_graphs = true; stage_timers = false; stop_on_crash = true;
         block = 128; unroll = 4; persistent_tiles = false; cube_powf = false; list_lanes = 0; row_lanes = 1;
-        cell_cull = false; staged_solve = false; stage_rows = 2048; tape_budget_mb = 8192;
+        cell_cull = false; staged_solve = false; stage_rows = 2048; tape_budget_mb = 8192; adj_lanes = 1;
         cfl = 0.f;
         cell_order_brick = true;
         pbf_form = 0; pbf_eps = 1e-6f;
@@ -213,6 +213,9 @@ int vtp_solver::parse_config(const json &c) {
             cell_cull = b.value("cellCull", false);
             staged_solve = b.value("stagedSolve", false);
             tape_budget_mb = b.value("tapeBudgetMB", 8192u);
+            adj_lanes = b.value("adjointLanes", 1);
+            if (adj_lanes != 1 && adj_lanes != 2 && adj_lanes != 4 && adj_lanes != 8)
+                return fail(VTP_ERR_CONFIG, "adjointLanes must be 1, 2, 4 or 8");
             stage_rows = b.value("stageRows", 2048);
             if (stage_rows < 256 || stage_rows > (int)vtp::kStageMaxRows)
                 return fail(VTP_ERR_CONFIG, "stageRows must be in [256, 32767]");

@@ -161,80 +161,104 @@ __global__ void k_adj_gather(AdjArgs a) {
     a.abar[r] = make_float4(xo.x * a.dt + vo.x, xo.y * a.dt + vo.y, xo.z * a.dt + vo.z, 0.f);
 }
 
+// The three neighbour passes take L lanes per row ("adjointLanes"; lane_group_mask /
+// nbr_loop_lanes / lane_sum of common.cuh): with L = 1 one thread walks the row with four
+// neighbours' gathers in flight; with L > 1 the row's lanes take entries lane, lane + L, ...
+// (AU gathers in flight each, fewer registers) and a butterfly adds their partials.
+template <int L>
+constexpr int adj_unroll() { return L == 1 ? 4 : (L == 2 ? 2 : 1); }
+
 // XSPH adjoint; epilogue: Delta-bar of the last constraint iteration.
+template <int L>
 __global__ void __launch_bounds__(256) k_adj_xsph(AdjArgs a) {
     pdl_enter();
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
     double kl = 0.0;
     if (r < a.nf) {
         const float4 p = a.x[r], vi = a.v[r], ai = a.abar[r];
-        float4 xb = a.xbar[r], vb = a.vbar[r];
         const float Vi = a.vol[r];
         const uint32_t n = a.ncnt[r];
         const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
-        float ksum = 0.f;
-        // U = 4 neighbours' gathers in flight per thread (same order of accumulation)
-        nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
-                    [&](uint32_t j) {
-                        XN e;
-                        e.q = __ldg(a.x + j);
-                        e.v = __ldg(a.v + j);
-                        e.vol = __ldg(a.vol + j);
-                        e.a = j < a.nf ? __ldg(a.abar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-                        return e;
-                    },
-                    [&](uint32_t, const XN &e) {
-                        const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                        const float d2 = dist2(rx, ry, rz);
-                        const float w = cubic_w(d2, a.k), g = cubic_g(d2, a.k);
-                        const float Vj = e.vol;
-                        const float dx = e.v.x - vi.x, dy = e.v.y - vi.y, dz = e.v.z - vi.z;
-                        const float di = dx * ai.x + dy * ai.y + dz * ai.z;
-                        const float dj = dx * e.a.x + dy * e.a.y + dz * e.a.z;
-                        const float ci = -a.c * Vj * w, cj = a.c * Vi * w;
-                        vb.x += ci * ai.x + cj * e.a.x;
-                        vb.y += ci * ai.y + cj * e.a.y;
-                        vb.z += ci * ai.z + cj * e.a.z;
-                        const float s = a.c * g * (Vj * di - Vi * dj);
-                        xb.x += s * rx;
-                        xb.y += s * ry;
-                        xb.z += s * rz;
-                        ksum += Vj * w * di;
-                    });
-        a.xbar[r] = xb;
-        a.vbar[r] = vb;
-        a.Dcur[r] = make_float4(xb.x + vb.x * a.inv_dt, xb.y + vb.y * a.inv_dt, xb.z + vb.z * a.inv_dt, 0.f);
-        kl = (double)ksum;
+        float vx = 0.f, vy = 0.f, vz = 0.f, xx = 0.f, xy = 0.f, xz = 0.f, ksum = 0.f;
+        nbr_loop_lanes<adj_unroll<L>(), L>(lst, n > 0 ? n - 1 : 0, lane,
+                             [&](uint32_t j) {
+                                 XN e;
+                                 e.q = __ldg(a.x + j);
+                                 e.v = __ldg(a.v + j);
+                                 e.vol = __ldg(a.vol + j);
+                                 e.a = j < a.nf ? __ldg(a.abar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                                 return e;
+                             },
+                             [&](uint32_t, const XN &e) {
+                                 const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                                 const float d2 = dist2(rx, ry, rz);
+                                 const float w = cubic_w(d2, a.k), g = cubic_g(d2, a.k);
+                                 const float Vj = e.vol;
+                                 const float dx = e.v.x - vi.x, dy = e.v.y - vi.y, dz = e.v.z - vi.z;
+                                 const float di = dx * ai.x + dy * ai.y + dz * ai.z;
+                                 const float dj = dx * e.a.x + dy * e.a.y + dz * e.a.z;
+                                 const float ci = -a.c * Vj * w, cj = a.c * Vi * w;
+                                 vx += ci * ai.x + cj * e.a.x;
+                                 vy += ci * ai.y + cj * e.a.y;
+                                 vz += ci * ai.z + cj * e.a.z;
+                                 const float s = a.c * g * (Vj * di - Vi * dj);
+                                 xx += s * rx;
+                                 xy += s * ry;
+                                 xz += s * rz;
+                                 ksum += Vj * w * di;
+                             });
+        const unsigned m = lane_group_mask<L>();
+        vx = lane_sum<L>(vx, m); vy = lane_sum<L>(vy, m); vz = lane_sum<L>(vz, m);
+        xx = lane_sum<L>(xx, m); xy = lane_sum<L>(xy, m); xz = lane_sum<L>(xz, m);
+        ksum = lane_sum<L>(ksum, m);
+        if (lane == 0) {
+            float4 xb = a.xbar[r], vb = a.vbar[r];
+            xb.x += xx; xb.y += xy; xb.z += xz;
+            vb.x += vx; vb.y += vy; vb.z += vz;
+            a.xbar[r] = xb;
+            a.vbar[r] = vb;
+            a.Dcur[r] = make_float4(xb.x + vb.x * a.inv_dt, xb.y + vb.y * a.inv_dt, xb.z + vb.z * a.inv_dt, 0.f);
+            kl = (double)ksum;
+        }
     }
     const double s = block_sum_d(kl);
     if (threadIdx.x == 0) a.kpart[blockIdx.x] = s;
 }
 
 // Constraint iteration adjoint, pass A: lambda-bar -> s2-bar, rho-bar; G recomputed.
+template <int L>
 __global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
     pdl_enter();
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
+    if (r >= a.nf) return;   // the same for every lane of the row
     const float4 p = a.x[r], di = a.Dcur[r];
     const uint32_t n = a.ncnt[r];
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     const float ir = 1.f / a.rho0;
     float lb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, s2 = 0.f;
-    nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
-                [&](uint32_t j) {
-                    LN e;
-                    e.q = __ldg(a.x + j);
-                    e.d = j < a.nf ? __ldg(a.Dcur + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    return e;
-                },
-                [&](uint32_t, const LN &e) {
-                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                    const float g = cubic_g(dist2(rx, ry, rz), a.k) * ir;
-                    const float ex = g * rx, ey = g * ry, ez = g * rz;
-                    gx += ex; gy += ey; gz += ez;
-                    s2 += ex * ex + ey * ey + ez * ez;
-                    lb += ex * (di.x - e.d.x) + ey * (di.y - e.d.y) + ez * (di.z - e.d.z);
-                });
+    nbr_loop_lanes<adj_unroll<L>(), L>(lst, n > 0 ? n - 1 : 0, lane,
+                         [&](uint32_t j) {
+                             LN e;
+                             e.q = __ldg(a.x + j);
+                             e.d = j < a.nf ? __ldg(a.Dcur + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                             return e;
+                         },
+                         [&](uint32_t, const LN &e) {
+                             const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                             const float g = cubic_g(dist2(rx, ry, rz), a.k) * ir;
+                             const float ex = g * rx, ey = g * ry, ez = g * rz;
+                             gx += ex; gy += ey; gz += ez;
+                             s2 += ex * ex + ey * ey + ez * ez;
+                             lb += ex * (di.x - e.d.x) + ey * (di.y - e.d.y) + ez * (di.z - e.d.z);
+                         });
+    const unsigned m = lane_group_mask<L>();
+    lb = lane_sum<L>(lb, m); s2 = lane_sum<L>(s2, m);
+    gx = lane_sum<L>(gx, m); gy = lane_sum<L>(gy, m); gz = lane_sum<L>(gz, m);
+    if (lane != 0) return;
     s2 += gx * gx + gy * gy + gz * gz;
     const float den = s2 + a.eps;
     const float lam = a.lam[r];
@@ -245,54 +269,60 @@ __global__ void __launch_bounds__(256) k_adj_lambda(AdjArgs a) {
 
 // Constraint iteration adjoint, pass B: xbar of the iteration's input positions;
 // epilogue: Delta-bar of the previous iteration.
+template <int L>
 __global__ void __launch_bounds__(256) k_adj_dx(AdjArgs a) {
     pdl_enter();
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nf) return;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = gt / L;
+    const int lane = (int)(gt % L);
+    if (r >= a.nf) return;   // the same for every lane of the row
     const float4 p = a.x[r], di = a.Dcur[r], Ai = a.A2[r];
     const float li = a.lam[r], sbi = a.sbar[r];
     const uint32_t n = a.ncnt[r];
     const uint32_t *lst = a.nbr + ell_index(r, 0, a.ell_stride);
     const float ir = 1.f / a.rho0;
     float ax = 0.f, ay = 0.f, az = 0.f;
-    nbr_loop<4>(lst, n > 0 ? n - 1 : 0,
-                [&](uint32_t j) {
-                    DN e;
-                    e.q = __ldg(a.x + j);
-                    e.fj = j < a.nf;
-                    if (e.fj) {
-                        e.l = __ldg(a.lam + j);
-                        e.s = __ldg(a.sbar + j);
-                        e.d = __ldg(a.Dcur + j);
-                        e.A = __ldg(a.A2 + j);
-                    } else {
-                        e.l = e.s = 0.f;
-                        e.d = e.A = make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-                    return e;
-                },
-                [&](uint32_t, const DN &e) {
-                    const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
-                    const float d2 = dist2(rx, ry, rz);
-                    const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
-                    const float ex = g * rx * ir, ey = g * ry * ir, ez = g * rz * ir;
-                    const float ll = li + e.l;
-                    // e-bar of pair (i, j) minus e-bar of pair (j, i) (zero for a boundary j)
-                    float bx = ll * di.x + 2.f * sbi * (ex + Ai.x);
-                    float by = ll * di.y + 2.f * sbi * (ey + Ai.y);
-                    float bz = ll * di.z + 2.f * sbi * (ez + Ai.z);
-                    if (e.fj) {
-                        bx -= ll * e.d.x + 2.f * e.s * (e.A.x - ex);
-                        by -= ll * e.d.y + 2.f * e.s * (e.A.y - ey);
-                        bz -= ll * e.d.z + 2.f * e.s * (e.A.z - ez);
-                    }
-                    const float rdot = rx * bx + ry * by + rz * bz;
-                    const float dens = e.q.w * Ai.w + (e.fj ? p.w * e.A.w : 0.f);   // m_j rho-bar_i + m_i rho-bar_j
-                    const float cg = g * dens;
-                    ax += cg * rx + (g * bx + hh * rx * rdot) * ir;
-                    ay += cg * ry + (g * by + hh * ry * rdot) * ir;
-                    az += cg * rz + (g * bz + hh * rz * rdot) * ir;
-                });
+    nbr_loop_lanes<adj_unroll<L>(), L>(lst, n > 0 ? n - 1 : 0, lane,
+                         [&](uint32_t j) {
+                             DN e;
+                             e.q = __ldg(a.x + j);
+                             e.fj = j < a.nf;
+                             if (e.fj) {
+                                 e.l = __ldg(a.lam + j);
+                                 e.s = __ldg(a.sbar + j);
+                                 e.d = __ldg(a.Dcur + j);
+                                 e.A = __ldg(a.A2 + j);
+                             } else {
+                                 e.l = e.s = 0.f;
+                                 e.d = e.A = make_float4(0.f, 0.f, 0.f, 0.f);
+                             }
+                             return e;
+                         },
+                         [&](uint32_t, const DN &e) {
+                             const float rx = p.x - e.q.x, ry = p.y - e.q.y, rz = p.z - e.q.z;
+                             const float d2 = dist2(rx, ry, rz);
+                             const float g = cubic_g(d2, a.k), hh = cubic_hh(d2, a.k);
+                             const float ex = g * rx * ir, ey = g * ry * ir, ez = g * rz * ir;
+                             const float ll = li + e.l;
+                             // e-bar of pair (i, j) minus e-bar of pair (j, i) (zero for a boundary j)
+                             float bx = ll * di.x + 2.f * sbi * (ex + Ai.x);
+                             float by = ll * di.y + 2.f * sbi * (ey + Ai.y);
+                             float bz = ll * di.z + 2.f * sbi * (ez + Ai.z);
+                             if (e.fj) {
+                                 bx -= ll * e.d.x + 2.f * e.s * (e.A.x - ex);
+                                 by -= ll * e.d.y + 2.f * e.s * (e.A.y - ey);
+                                 bz -= ll * e.d.z + 2.f * e.s * (e.A.z - ez);
+                             }
+                             const float rdot = rx * bx + ry * by + rz * bz;
+                             const float dens = e.q.w * Ai.w + (e.fj ? p.w * e.A.w : 0.f);   // m_j rho-bar_i + m_i rho-bar_j
+                             const float cg = g * dens;
+                             ax += cg * rx + (g * bx + hh * rx * rdot) * ir;
+                             ay += cg * ry + (g * by + hh * ry * rdot) * ir;
+                             az += cg * rz + (g * bz + hh * rz * rdot) * ir;
+                         });
+    const unsigned m = lane_group_mask<L>();
+    ax = lane_sum<L>(ax, m); ay = lane_sum<L>(ay, m); az = lane_sum<L>(az, m);
+    if (lane != 0) return;
     float4 xb = a.xbar[r];
     xb.x += ax; xb.y += ay; xb.z += az;
     a.xbar[r] = xb;
@@ -442,9 +472,11 @@ int record_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, int tp) {
 
 // The adjoint substeps of a recorded segment of k substeps, last to first (programmatic
 // launch between their kernels, as in the forward substep).
-int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G, int tp) {
+template <int L>
+int adjoint_segment_l(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G, int tp) {
     const uint32_t nf = d.nf;
     const int I = s->iterations;
+    const unsigned GL = vtp::nblk(nf * (uint32_t)L, 256);
     const vtp::PdlScope pdl_scope(s->pdl);
     for (int t = (int)k - 1; t >= 0 && nf; --t) {
         const PbfTapeSlot &T = d.tapes[tp][t];
@@ -459,21 +491,30 @@ int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G, in
         a.x = T.x[I];
         a.Dcur = d.D[cur];
         vtp::launch(vtp::k_adj_gather, G, 256, 0, s->st, a);
-        vtp::launch(vtp::k_adj_xsph, G, 256, 0, s->st, a);
-        vtp::launch(vtp::k_adj_kreduce, 1, 256, 0, s->st, d.kpart, G, d.kacc);
+        vtp::launch(vtp::k_adj_xsph<L>, GL, 256, 0, s->st, a);
+        vtp::launch(vtp::k_adj_kreduce, 1, 256, 0, s->st, d.kpart, GL, d.kacc);
         for (int it = I - 1; it >= 0; --it) {
             a.x = T.x[it];
             a.lam = T.lam[it];
             a.rho = T.rho[it];
             a.Dcur = d.D[cur];
             a.Dnext = d.D[cur ^ 1];
-            vtp::launch(vtp::k_adj_lambda, G, 256, 0, s->st, a);
-            vtp::launch(vtp::k_adj_dx, G, 256, 0, s->st, a);
+            vtp::launch(vtp::k_adj_lambda<L>, GL, 256, 0, s->st, a);
+            vtp::launch(vtp::k_adj_dx<L>, GL, 256, 0, s->st, a);
             cur ^= 1;
         }
         vtp::launch(vtp::k_adj_force_scatter, G, 256, 0, s->st, a);
     }
     return VTP_OK;
+}
+
+int adjoint_segment(vtp_solver *s, vtp::DiffState &d, uint32_t k, unsigned G, int tp) {
+    switch (s->adj_lanes) {
+        case 2: return adjoint_segment_l<2>(s, d, k, G, tp);
+        case 4: return adjoint_segment_l<4>(s, d, k, G, tp);
+        case 8: return adjoint_segment_l<8>(s, d, k, G, tp);
+        default: return adjoint_segment_l<1>(s, d, k, G, tp);
+    }
 }
 
 // Runs `body` (enqueueing a full segment's work on s->st) through the graph `exec`, capturing
@@ -609,7 +650,7 @@ int vtp_solver_diff_forward(vtp_solver *s, uint32_t n_steps, uint32_t checkpoint
     d->rec_exec.assign(ntapes, nullptr);
     d->adj_exec.assign(ntapes, nullptr);
     d->rec_parity.assign(ntapes, {-1, -1, -1});
-    d->kblocks = vtp::nblk(std::max<uint32_t>(d->nf, 1), 256);
+    d->kblocks = vtp::nblk(std::max<uint32_t>(d->nf, 1) * 8u, 256);   // XSPH partials at up to 8 lanes per row
     if ((rc = d->alloc(&d->xbar_a, n)) || (rc = d->alloc(&d->vbar_a, n)) || (rc = d->alloc(&d->xbar, nf)) ||
         (rc = d->alloc(&d->vbar, nf)) || (rc = d->alloc(&d->abar, nf)) || (rc = d->alloc(&d->D[0], nf)) ||
         (rc = d->alloc(&d->D[1], nf)) || (rc = d->alloc(&d->A2, nf)) || (rc = d->alloc(&d->sbar, nf)) ||

@@ -111,6 +111,7 @@ struct vtp_solver {
     bool cell_cull = false;   // list builder skips neighbour cells beyond h (same lists)
     bool staged_solve = false;      // DFSPH pressure solve gathers from shared-memory cell-group copies
     uint32_t tape_budget_mb = 8192;  // differentiable PBF / DFSPH: device memory for resident segment tapes
+    int adj_lanes = 1;              // differentiable PBF: lanes per row of the adjoint's neighbour passes
     int stage_rows = 2048;          // staged rows per brick at most
     bool cube_powf = false;   // cubic W outer branch: powf (reference rounding) or cube_rn
     bool phase_retry_all = false;   // IMM phase-transfer retries: every row, or rows near new flags
