@@ -1,16 +1,20 @@
 #!/usr/bin/env python
 """Benchmark of the particle-fluid hot path: one step = one solver substep.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload dfsph_1m|pbf]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dfsph_1m|pbf|pbf_m1|immct_500k|batched|batched_m1|diff_pbf|diff_dfsph|dfsph_1m_dd]
 
 Default workload: DFSPH, 1,000,000 fluid particles (100^3 lattice, spacing 0.01,
-jitter +-0.05 spacing, seed 2002) in a 3-layer 2 x 1.5 x 1 box of 439,467
-boundary particles, dt = 1 ms, thresholds 0.1 %, seeded synthetic input.
-Metric: million fluid-particle substeps per second (whole job, all ranks).
+jitter +-0.05 spacing, seed 2002) in a 3-layer 2 x 1.5 x 1.06 box of 453,957
+boundary particles, dt = 1 ms (CFL 0.4 rule capped there), thresholds 0.1 %,
+seeded synthetic input.  Metric: million fluid-particle substeps per second
+(whole job, all ranks).  diff_pbf / diff_dfsph time a recorded forward plus
+its adjoint over a rollout (64k fluid particles each).
 
-Under torchrun every rank advances its own replica of the scene (the path
-has no exchange step: replicas only); timing is the max over ranks.
-Prints one JSON line on rank 0.
+With --gpus N (or under torchrun) one process per GPU: a single scene runs as
+replicas (the path has no exchange step), the batched mix is sharded over the
+ranks by longest-processing-time assignment, dfsph_1m_dd runs one slab per
+rank; timing is the max over ranks.  Prints one JSON line on rank 0.
 """
 from __future__ import annotations
 
