@@ -76,5 +76,25 @@ def test_committed_cache_is_well_formed():
     for gpu, table in cache.items():
         for key, entry in table.items():
             cfg = entry["B200"]
-            assert set(cfg) <= {"blockSize", "unroll", "rowLanes", "listLanes", "cellOrder", "stagedSolve"}
+            assert set(cfg) <= {"blockSize", "unroll", "rowLanes", "listLanes", "cellOrder", "stagedSolve",
+                                "adjointLanes"}
             assert cfg.get("cellOrder", "brick") in ("brick", "linear")
+
+
+def test_adjoint_lanes_are_tuned_on_their_own_measurement_and_keep_the_tuned_tile():
+    """The differentiable workload's second search: only "adjointLanes", whose config carries
+    no cell-tile keys, so merging it into the forward's tuned block keeps that block's tile."""
+    calls = []
+
+    def measure(cfg):
+        calls.append(dict(cfg))
+        assert set(cfg) == {"adjointLanes"}
+        return {1: 2.3, 2: 2.2, 4: 2.0, 8: 2.1}[cfg["adjointLanes"]]
+
+    res = A.tune(measure, "PBF", ("adjointLanes",))
+    assert res["best"] == {"adjointLanes": 4} and res["config"] == {"adjointLanes": 4}
+    assert len(calls) == 4
+    forward = {"blockSize": 256, "unroll": 4, "cellOrder": "linear", "stagedSolve": False}
+    forward.update(res["config"])
+    assert forward["cellOrder"] == "linear" and forward["adjointLanes"] == 4
+    assert A.DIMENSIONS["adjointLanes"] == (1, 2, 4, 8) and A.DEFAULTS["adjointLanes"] == 1

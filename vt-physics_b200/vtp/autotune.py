@@ -11,9 +11,13 @@ Tuned dimensions (keys of the solver config's "B200" block):
                  whose neighbourhoods the pressure solve copies into shared
                  memory; "cellOrder" / "stagedSolve" / "stageRows");
   * rowLanes   - threads per row of the PBF neighbour passes (1, 4, 8);
-  * listLanes  - threads per row of the list builder (0: by row count, 1, 8).
+  * listLanes  - threads per row of the list builder (0: by row count, 1, 8);
+  * adjointLanes - threads per row of the PBF adjoint's neighbour passes (1, 2,
+                 4, 8), tuned for the differentiable workload only, after the
+                 forward's keys, on the backward's wall-clock time.
 Every candidate is timed with the library's per-kernel CUDA-event profiler
-(the substep's kernel time), by coordinate descent from the current best:
+(the substep's kernel time; the adjoint's keys: a recorded rollout's backward),
+by coordinate descent from the current best:
 each dimension in turn is swept with the others fixed, until a full pass
 changes nothing.  `tune` takes the measurement as a function, so the search
 itself runs without a GPU (tests/test_autotune.py).
@@ -40,8 +44,9 @@ DIMENSIONS = {
     "cellTile": ("brick", "linear", "staged"),
     "rowLanes": (1, 4, 8),
     "listLanes": (0, 1, 8),
+    "adjointLanes": (1, 2, 4, 8),
 }
-DEFAULTS = {"blockSize": 128, "unroll": 4, "cellTile": "brick", "rowLanes": 1, "listLanes": 0}
+DEFAULTS = {"blockSize": 128, "unroll": 4, "cellTile": "brick", "rowLanes": 1, "listLanes": 0, "adjointLanes": 1}
 # Dimensions each solver type has (the others leave its kernels unchanged).
 SOLVER_DIMS = {
     "PBF": ("blockSize", "unroll", "cellTile", "rowLanes", "listLanes"),
@@ -52,11 +57,13 @@ SOLVER_DIMS = {
 
 
 def to_config(point: dict) -> dict:
-    """The "B200" config keys of a search point."""
-    out = {k: point[k] for k in ("blockSize", "unroll", "rowLanes", "listLanes") if k in point}
-    tile = point.get("cellTile", "brick")
-    out["cellOrder"] = "linear" if tile == "linear" else "brick"
-    out["stagedSolve"] = tile == "staged"
+    """The "B200" config keys of a search point (the cell tile's keys only when the point has
+    one, so a search over other keys leaves a tuned tile in place)."""
+    out = {k: point[k] for k in ("blockSize", "unroll", "rowLanes", "listLanes", "adjointLanes") if k in point}
+    if "cellTile" in point:
+        tile = point["cellTile"]
+        out["cellOrder"] = "linear" if tile == "linear" else "brick"
+        out["stagedSolve"] = tile == "staged"
     return out
 
 
@@ -142,6 +149,35 @@ def library_measure(scene, warmup: int = 3, steps: int = 3, base_extra: dict | N
     return measure
 
 
+def adjoint_measure(scene, steps: int = 20, checkpoint_every: int = 10, base_extra: dict | None = None):
+    """measure(config) for `tune` over the adjoint's keys: milliseconds per substep of the
+    backward of a recorded `steps`-substep rollout of the differentiable PBF `scene` (the
+    second of two, so that tapes and the backward's segment graphs exist), loss = mean fluid
+    position along (1, 1, 1)."""
+    import numpy as np
+
+    from . import diff
+
+    def measure(cfg: dict) -> float:
+        extra = dict(base_extra or {})
+        extra.update(cfg)
+        s = diff.pbf_solver(scene, extra=extra)
+        try:
+            mask = diff.fluid_mask(scene)
+            g = np.zeros((mask.size, 3), np.float32)
+            g[mask] = 1.0 / mask.sum()
+            best = math.inf
+            for _ in range(2):
+                diff.diff_forward(s, steps, checkpoint_every)
+                t0 = time.perf_counter()
+                diff.diff_backward(s, g, None)
+                best = min(best, 1e3 * (time.perf_counter() - t0) / steps)
+            return best
+        finally:
+            s.destroy()
+    return measure
+
+
 def workload_key(solver: str, n_fluid: int, name: str | None = None) -> str:
     """Cache key of a workload: a named workload, or the solver type and the fluid-particle
     count rounded to the nearest power of two."""
@@ -213,6 +249,11 @@ def main(argv=None):
         if a.workload == "dfsph_1m":
             base = {"cfl": 0.4}
     res = tune(library_measure(sc, base_extra=base), kind, dims_for(kind, not a.no_arithmetic), verbose=True)
+    if a.workload == "diff_pbf":
+        # the adjoint's lanes, on the backward, with the forward's tuned keys fixed
+        adj = tune(adjoint_measure(sc, base_extra=res["config"]), kind, ("adjointLanes",), verbose=True)
+        res["config"].update(adj["config"])
+        res["adjoint_ms_per_step"] = adj["ms_per_step"]
     print(json.dumps({k: res[k] for k in ("best", "config", "ms_per_step")}))
     if a.write:
         store(a.workload, res)
