@@ -171,3 +171,23 @@ def test_export_config_is_validated():
     del cfg["EXPORT"]["Common"]["exportTargetDir"]
     assert not s.setConfig(cfg) and "exportTargetDir" in s.last_error
     s.destroy()
+
+
+def test_product_path_fails_loudly_without_the_library(tmp_path):
+    """With no built library the solver API raises; nothing falls back to a CPU path."""
+    import os
+    import subprocess
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    code = ("import sys; sys.path.insert(0, 'vt-physics_b200')\n"
+            "import vtp\n"
+            "try:\n"
+            "    s = vtp.DFSPHSolver()\n"
+            "except RuntimeError as e:\n"
+            "    print('raised:', e)\n"
+            "    sys.exit(0)\n"
+            "sys.exit(3)\n")
+    env = dict(os.environ, VTP_LIBRARY=str(tmp_path / "absent" / "libvtp.so"))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "is missing" in r.stdout
